@@ -1,0 +1,252 @@
+"""Seeded synthetic configurations in LBIBCell's own text formats.
+
+Each configuration is four files:
+
+* ``parameters.txt`` -- the reference's global parameter file
+  (``libs/LbmLib/src/GlobalSimulationParameters.cpp:34-72``): ``CurrentIterations:``,
+  ``Iterations:``, ``ReportStep:``, ``SizeX:``, ``SizeY:``, ``tauFluid:``,
+  ``CDESolvers: name tau ...``.
+* ``geometry.txt`` -- the reference's txt geometry
+  (``libs/LbmLib/src/geometry/Geometry.cpp:99-160``): ``#Nodes`` lines ``id x y`` then
+  ``#Connection`` lines ``id1 id2 domainId [bsolver cdesolver]...``.  Cells are
+  counter-clockwise polygons, so that the inside is the domain side of each
+  connection (``libs/LbmLib/src/geometry/Connection.cpp:246-314``).
+* ``force.txt`` -- the reference's force file (``apps/config/force.txt``); comment
+  lines only unless a config adds static forces.
+* ``plugins.txt`` -- the solver plugins to register and their parameters.  The
+  reference hard-codes these constants inside each plugin; this file carries them
+  instead.  One plugin per line, tab separated::
+
+      MassSolver  MassSolverBoxOutlet
+      BioSolver   LbibAreaRegulator    factor F strength K maxsource M
+      BioSolver   LbibMembraneTension  force F frequency N
+      CDE         <species name>       init C0 decay D
+      CDESource   <species name>       <domainId> <rate> [<domainId> <rate> ...]
+
+  Bio solvers run in file order.  Species names are the ``CDESolvers:`` names of the
+  parameter file (``LbibCDESolverD2Q5_A``, ``_B``, ``_C``); the reference orders
+  species alphabetically (a ``std::map``).
+
+Node coordinates are written with 17 significant digits, so that every reader
+parses exactly the doubles that were generated.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+SPECIES_NAMES = ("LbibCDESolverD2Q5_A", "LbibCDESolverD2Q5_B", "LbibCDESolverD2Q5_C")
+
+
+@dataclass
+class Species:
+    name: str
+    tau: float
+    init: float = 0.0
+    decay: float = 0.0
+    source: Dict[int, float] = field(default_factory=dict)
+
+
+@dataclass
+class Config:
+    """A complete simulation set-up: lattice, cells, solvers."""
+
+    name: str
+    nx: int
+    ny: int
+    tau_fluid: float
+    iterations: int
+    report_step: int
+    cells: List[Tuple[int, np.ndarray]]  # (domainId, (n, 2) CCW vertices)
+    species: List[Species]
+    outlet: bool = True
+    tension: Optional[Tuple[float, int]] = (0.1, 10)  # (force, frequency)
+    area: Optional[Tuple[float, float, float]] = (1.2, 0.01, 0.004)  # factor, strength, maxsource
+    forces: List[str] = field(default_factory=list)
+
+    @property
+    def lattice_nodes(self) -> int:
+        return self.nx * self.ny
+
+    @property
+    def membrane_nodes(self) -> int:
+        return sum(len(v) for _, v in self.cells)
+
+    def write(self, directory: str) -> Dict[str, str]:
+        """Write the four files into ``directory``; returns their paths."""
+        os.makedirs(directory, exist_ok=True)
+        paths = {k: os.path.join(directory, k + ".txt") for k in ("parameters", "geometry", "force", "plugins")}
+        with open(paths["parameters"], "w") as f:
+            f.write("#Global Parameter file\n")
+            f.write("CurrentIterations:\t0\n")
+            f.write(f"Iterations:\t{self.iterations}\n")
+            f.write(f"ReportStep:\t{self.report_step}\n")
+            f.write(f"SizeX:\t{self.nx}\n")
+            f.write(f"SizeY:\t{self.ny}\n")
+            f.write(f"tauFluid:\t{self.tau_fluid!r}\n")
+            f.write("CDESolvers:")
+            for s in self.species:
+                f.write(f"\t{s.name}\t{s.tau!r}")
+            f.write("\n")
+        with open(paths["geometry"], "w") as f:
+            f.write("#Nodes (id\txPos\tyPos)\n")
+            nid = 1
+            conns = []
+            for dom, verts in self.cells:
+                first = nid
+                for x, y in verts:
+                    f.write(f"{nid}\t{float(x):.17g}\t{float(y):.17g}\n")
+                    nid += 1
+                ids = list(range(first, nid))
+                for i, a in enumerate(ids):
+                    conns.append((a, ids[(i + 1) % len(ids)], dom))
+            f.write("#Connection (nodeId1\tnodeId2\tdomainId\tbsolver\tcdesolver\t...)\n")
+            for a, b, d in conns:
+                f.write(f"{a}\t{b}\t{d}\n")
+        with open(paths["force"], "w") as f:
+            f.write("#Force 6 {type=6 id1 id2 f}\tmembrane tension (renewed by LbibMembraneTension)\n")
+            for line in self.forces:
+                f.write(line.rstrip("\n") + "\n")
+        with open(paths["plugins"], "w") as f:
+            f.write("#lbibcell_b200 plugin file\n")
+            if self.outlet:
+                f.write("MassSolver\tMassSolverBoxOutlet\n")
+            if self.area is not None:
+                fa, st, mx = self.area
+                f.write(f"BioSolver\tLbibAreaRegulator\tfactor\t{fa!r}\tstrength\t{st!r}\tmaxsource\t{mx!r}\n")
+            if self.tension is not None:
+                fo, fr = self.tension
+                f.write(f"BioSolver\tLbibMembraneTension\tforce\t{fo!r}\tfrequency\t{fr}\n")
+            for s in self.species:
+                f.write(f"CDE\t{s.name}\tinit\t{s.init!r}\tdecay\t{s.decay!r}\n")
+                if s.source:
+                    f.write(f"CDESource\t{s.name}")
+                    for d in sorted(s.source):
+                        f.write(f"\t{d}\t{s.source[d]!r}")
+                    f.write("\n")
+        return paths
+
+
+def circle(cx: float, cy: float, r: float, n: int, phase: float = 0.0) -> np.ndarray:
+    """n vertices at uniform angle, counter-clockwise."""
+    t = phase + 2.0 * math.pi * np.arange(n) / n
+    return np.stack([cx + r * np.cos(t), cy + r * np.sin(t)], axis=1)
+
+
+def config1(iterations: int = 2000, report_step: int = 500) -> Config:
+    """Single circular cell (tutorial_01 style): 200x200, r=20, 250 nodes, 1 species."""
+    return Config(
+        name="single_cell_200",
+        nx=200, ny=200, tau_fluid=1.0,
+        iterations=iterations, report_step=report_step,
+        cells=[(1, circle(100.0, 100.0, 20.0, 250))],
+        species=[Species(SPECIES_NAMES[0], 1.0, init=0.0, decay=0.0, source={1: 1e-3})],
+    )
+
+
+def toy(n: int = 64, r: float = 10.0, nodes: int = 100, iterations: int = 100, report_step: int = 25,
+        species: int = 1, tau_fluid: float = 1.0) -> Config:
+    """Small single-cell case for fast tests."""
+    taus = (1.0, 0.8, 1.2)
+    sp = [Species(SPECIES_NAMES[k], taus[k], init=0.0, decay=1e-4 * k, source={1: 1e-3 * (k + 1)})
+          for k in range(species)]
+    return Config(
+        name=f"toy_{n}", nx=n, ny=n, tau_fluid=tau_fluid,
+        iterations=iterations, report_step=report_step,
+        cells=[(1, circle(n / 2.0, n / 2.0, r, nodes))],
+        species=sp,
+    )
+
+
+def hex_tissue(nx: int, ny: int, spacing: float, r0: float, jitter: float, nodes_per_cell: int,
+               seed: int, margin: float = 6.0) -> List[Tuple[int, np.ndarray]]:
+    """Cells on a hexagonal grid with radius r0 + U(-jitter, jitter)."""
+    rng = np.random.default_rng(seed)
+    cells = []
+    dom = 1
+    dy = spacing * math.sqrt(3.0) / 2.0
+    row = 0
+    y = margin + r0 + jitter
+    while y + r0 + jitter + margin <= ny:
+        x = margin + r0 + jitter + (spacing / 2.0 if row % 2 else 0.0)
+        while x + r0 + jitter + margin <= nx:
+            r = r0 + rng.uniform(-jitter, jitter)
+            cells.append((dom, circle(x, y, r, nodes_per_cell, phase=rng.uniform(0, 2 * math.pi))))
+            dom += 1
+            x += spacing
+        y += dy
+        row += 1
+    return cells
+
+
+def config2(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> Config:
+    """1024x1024 tissue: ~400 cells on a hex grid (spacing 44), r=20+U(-2,2), 250 nodes/cell,
+    2 species (tau 0.8, 1.2), secretion 1e-3/step from a seeded 10% of the cells."""
+    cells = hex_tissue(1024, 1024, 44.0, 20.0, 2.0, 250, seed)
+    rng = np.random.default_rng(seed + 1)
+    doms = [d for d, _ in cells]
+    k = max(1, len(doms) // 10)
+    sec = sorted(rng.choice(doms, size=k, replace=False).tolist())
+    species = [Species(SPECIES_NAMES[0], 0.8, source={d: 1e-3 for d in sec}),
+               Species(SPECIES_NAMES[1], 1.2, source={d: 1e-3 for d in sec})]
+    return Config(name="tissue_1024", nx=1024, ny=1024, tau_fluid=1.0, iterations=iterations,
+                  report_step=report_step, cells=cells, species=species)
+
+
+def poisson_tissue(nx: int, ny: int, rmin: float, rmax: float, spacing: float, seed: int,
+                   margin: float = 6.0, gap: float = 3.0, max_cells: Optional[int] = None):
+    """Cells placed by seeded dart throwing (Poisson-disk), radii U(rmin, rmax),
+    membrane node spacing ``spacing``."""
+    rng = np.random.default_rng(seed)
+    cell_size = 2 * rmax + gap
+    gw, gh = int(nx // cell_size) + 1, int(ny // cell_size) + 1
+    grid: Dict[Tuple[int, int], List[int]] = {}
+    placed: List[Tuple[float, float, float]] = []
+    attempts = 0
+    limit = 60 * (nx * ny) // int(cell_size * cell_size)
+    while attempts < limit:
+        attempts += 1
+        r = rng.uniform(rmin, rmax)
+        x = rng.uniform(margin + r, nx - margin - r)
+        y = rng.uniform(margin + r, ny - margin - r)
+        gx, gy = int(x // cell_size), int(y // cell_size)
+        ok = True
+        for ix in range(gx - 1, gx + 2):
+            for iy in range(gy - 1, gy + 2):
+                for j in grid.get((ix, iy), ()):
+                    px, py, pr = placed[j]
+                    if (px - x) ** 2 + (py - y) ** 2 < (pr + r + gap) ** 2:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        grid.setdefault((gx, gy), []).append(len(placed))
+        placed.append((x, y, r))
+        if max_cells is not None and len(placed) >= max_cells:
+            break
+    cells = []
+    for i, (x, y, r) in enumerate(placed):
+        n = max(8, int(round(2 * math.pi * r / spacing)))
+        cells.append((i + 1, circle(x, y, r, n, phase=rng.uniform(0, 2 * math.pi))))
+    return cells
+
+
+def config3(iterations: int = 5000, report_step: int = 1000, seed: int = 0) -> Config:
+    """4096x4096 tissue: Poisson-disk cells r~U(10,16), node spacing 0.5, 3 species
+    (tau 0.55/1.0/1.5) with linear decay 1e-4."""
+    cells = poisson_tissue(4096, 4096, 10.0, 16.0, 0.5, seed)
+    species = [Species(SPECIES_NAMES[k], t, decay=1e-4, source={d: 1e-3 for d, _ in cells[::10]})
+               for k, t in enumerate((0.55, 1.0, 1.5))]
+    return Config(name="tissue_4096", nx=4096, ny=4096, tau_fluid=1.0, iterations=iterations,
+                  report_step=report_step, cells=cells, species=species)
+
+
+CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "toy": toy}
