@@ -1,0 +1,129 @@
+/* lbibcell.h — C ABI of the lbibcell_b200 device runtime (liblbibcuda.so).
+ *
+ * One handle owns one simulation: the lattice (D2Q9 fluid + up to three D2Q5
+ * species), the membrane (immersed-boundary nodes and connections), the force
+ * list and the registered mass/bio solvers, all resident on one GPU.  Host
+ * code (the Python mirror in lbibcell_b200/, or a C++ host) drives it through
+ * these calls.  All calls return 0 or an LBIB_ERR_* code and never throw or
+ * abort across the ABI; lbib_last_error() gives the message and the index of
+ * the node or connection involved.  The caller owns every host buffer; the
+ * handle owns every device buffer.  A handle uses one CUDA stream and is not
+ * thread-safe.
+ *
+ * The comment of each call names the reference interface it replaces (paths
+ * relative to the LBIBCell project root).
+ */
+#ifndef LBIBCELL_H
+#define LBIBCELL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbib_handle lbib_handle;
+
+/* Precision of the lattice. */
+#define LBIB_FP64 0          /* plain: bit-identical to the reference's double run */
+#define LBIB_FP32_SHIFTED 1  /* FP32 storage of f - w (deviation from rest), FP32 collision */
+
+/* Error codes. */
+#define LBIB_OK 0
+#define LBIB_ERR_EDGE_W 10        /* "geometry point moved too close to the west boundary" */
+#define LBIB_ERR_EDGE_S 11
+#define LBIB_ERR_EDGE_E 12
+#define LBIB_ERR_EDGE_N 13
+#define LBIB_ERR_SPEED 20         /* membrane speed^2 > CS (LagrangianPoint.cpp:96-102) */
+#define LBIB_ERR_LEFT_DOMAIN 30   /* "domainID at the left boundary must be 0." */
+#define LBIB_ERR_VERTICAL 40      /* non-finite connection slope (Connection.cpp:315-323) */
+#define LBIB_ERR_FORCE_NODE 50    /* force refers to a missing node (ForceStructs.hpp) */
+#define LBIB_ERR_STENCIL 60       /* membrane node stencil leaves the lattice */
+#define LBIB_ERR_CAPACITY 70      /* a per-step device list overflowed */
+#define LBIB_ERR_CUDA 80          /* CUDA runtime error */
+#define LBIB_ERR_INPUT 90         /* bad file or argument */
+#define LBIB_ERR_STATE 91         /* call not valid in the handle's state */
+
+/* Creates a simulation from the reference's own text files (parameter,
+ * geometry and force files) plus the plugin file that names the mass/bio
+ * solvers and species parameters (format: lbibcell_b200/configs.py).
+ * Replaces the set-up of apps/tutorial_01.cpp:59-143:
+ *   Parameters.loadGlobalSimulationParameters  (GlobalSimulationParameters.cpp:34-72)
+ *   geometry::Geometry(file) txt loader        (Geometry.cpp:99-160)
+ *   geometry::GeometryHandler(geo)             (GeometryHandler.cpp:51-56, cureLattice :149-170)
+ *   SimulationRunner(geohandler, reporter)     (SimulationRunner.cpp:50-64)
+ *   SimulationRunner::initSolvers()            (SimulationRunner.cpp:290-306)
+ *   SimulationRunner::initForceSolver(file)    (SimulationRunner.cpp:392-394)
+ *   SimulationRunner::addMassSolver / addBioSolver (SimulationRunner.cpp:401-408)
+ * `device` is the CUDA device ordinal. */
+int lbib_create_from_files(const char* parameters, const char* geometry, const char* force, const char* plugins,
+                           int precision, int device, lbib_handle** out);
+
+/* Releases every device and host resource of the handle. */
+int lbib_destroy(lbib_handle* h);
+
+/* Advances n time steps: the body of SimulationRunner::runSimulation
+ * (SimulationRunner.cpp:72-99) — force evaluation, spreading, fused
+ * stream-collide of fluid and species, interpolation and motion, crossings,
+ * domain ids and species reinitialisation, remeshing, coarsening every 10
+ * iterations, mass solvers, bio solvers.  Returns after the GPU finished. */
+int lbib_step(lbib_handle* h, int n);
+
+/* Lattice-only steps with the geometry held fixed: pull-stream + collide of
+ * fluid and species (FluidSolver/CDESolver advect+collide), then the box
+ * outlet when `outlet` is non-zero.  The force field, domain ids and mass
+ * sources stay as they are.  Stage-level parity and bandwidth measurement. */
+int lbib_lattice_step(lbib_handle* h, int n, int outlet);
+
+/* sizes[0..9] = nx, ny, S, M (membrane nodes), C (connections), iteration,
+ * precision, host interventions (perturbation/remesh/coarsen), steps done,
+ * number of cells. */
+int lbib_get_sizes(lbib_handle* h, long long* sizes);
+
+/* Lattice state in the reference's layout (SimulationRunner::writeSimulation's
+ * solver dump order, SimulationRunner.cpp:112-149): f[L][9] and g[S][L][5]
+ * in the slot convention after FluidSolver::localSwap, vel[L][2]
+ * (FluidSolver::velocity_), force[L][2] (FluidSolver::force_), dom[L]
+ * (PhysicalNode::domainIdentifier_), ctype[L] (PhysicalNode::cellType_).
+ * Any pointer may be NULL.  FP32-shifted state is converted to f = h + w. */
+int lbib_download_lattice(lbib_handle* h, double* f, double* g, double* vel, double* force, unsigned* dom,
+                          unsigned* ctype);
+
+/* Overwrites the distributions (reference slot layout) and, if non-NULL, the
+ * spread force field.  Replaces SimulationRunner::initSolvers(file)
+ * (SimulationRunner.cpp:151-182) for restarts and stage-level tests. */
+int lbib_upload_lattice(lbib_handle* h, const double* f, const double* g, const double* force);
+
+/* Membrane nodes in ascending id order (Geometry::getGeometryNodes):
+ * ids[M], state[M][6] = x, y, vx, vy, fx, fy. */
+int lbib_download_membrane(lbib_handle* h, unsigned* ids, double* state);
+
+/* Connections in Geometry::getConnections order: conn[C][3] = id1, id2, domain. */
+int lbib_download_connections(lbib_handle* h, unsigned* conn);
+
+/* Cell areas (GeometryHandler::computeAreas, GeometryHandler.cpp:101-134):
+ * dom[k], area[k] for k < return value (capped at cap). Negative on error. */
+int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
+
+/* Sets species k's production rate per domain id (rates[0..n), n <= number of
+ * domain ids), taking effect at the next step.  This is the per-domain table
+ * that a host BioSolver plugin would otherwise write node by node through
+ * CDESolver state (e.g. tutorial_01_CDESolverD2Q5_SIGNAL.cpp:92-100, where the
+ * production depends on the node's domain id). */
+int lbib_set_species_source(lbib_handle* h, int k, const double* rates, int n);
+
+/* Last error: code; message into buf; index of the node/connection involved. */
+int lbib_last_error(lbib_handle* h, char* buf, int len, long long* index);
+
+/* Timing of the last lbib_step / lbib_lattice_step call measured with CUDA
+ * events on the handle's stream: out[0] = total ms, out[1] = ms in the
+ * stream-collide kernel (summed over steps, when profiling is on), out[2] =
+ * stream-collide launches timed, out[3] = kernels launched in total. */
+int lbib_last_timing(lbib_handle* h, double* out);
+
+/* Enables or disables per-kernel timing of the stream-collide kernel. */
+int lbib_set_profiling(lbib_handle* h, int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBIBCELL_H */

@@ -1,0 +1,71 @@
+"""ctypes binding of liblbibcuda.so (the C ABI in include/lbibcell.h).
+
+The shared library is built in-tree by lbibcell_b200/build.py.  Loading fails
+loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbibcuda.so")
+
+#: symbols declared in include/lbibcell.h
+SYMBOLS = (
+    "lbib_create_from_files", "lbib_destroy", "lbib_step", "lbib_lattice_step", "lbib_get_sizes",
+    "lbib_download_lattice", "lbib_upload_lattice", "lbib_download_membrane", "lbib_download_connections",
+    "lbib_areas", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
+)
+
+_lib = None
+
+
+class LbibError(RuntimeError):
+    """An error code returned through the C ABI."""
+
+    def __init__(self, code: int, message: str, index: int = -1):
+        super().__init__(f"lbibcell error {code}: {message} (index {index})")
+        self.code = code
+        self.index = index
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m lbibcell_b200.build` "
+                          f"(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ip, cp = ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p
+    L.lbib_create_from_files.restype = ip
+    L.lbib_create_from_files.argtypes = [cp, cp, cp, cp, ip, ip, ctypes.POINTER(vp)]
+    L.lbib_destroy.restype = ip
+    L.lbib_destroy.argtypes = [vp]
+    L.lbib_step.restype = ip
+    L.lbib_step.argtypes = [vp, ip]
+    L.lbib_lattice_step.restype = ip
+    L.lbib_lattice_step.argtypes = [vp, ip, ip]
+    L.lbib_get_sizes.restype = ip
+    L.lbib_get_sizes.argtypes = [vp, vp]
+    L.lbib_download_lattice.restype = ip
+    L.lbib_download_lattice.argtypes = [vp] + [vp] * 6
+    L.lbib_upload_lattice.restype = ip
+    L.lbib_upload_lattice.argtypes = [vp, vp, vp, vp]
+    L.lbib_download_membrane.restype = ip
+    L.lbib_download_membrane.argtypes = [vp, vp, vp]
+    L.lbib_download_connections.restype = ip
+    L.lbib_download_connections.argtypes = [vp, vp]
+    L.lbib_areas.restype = ip
+    L.lbib_areas.argtypes = [vp, vp, vp, ip]
+    L.lbib_last_error.restype = ip
+    L.lbib_last_error.argtypes = [vp, cp, ip, ctypes.POINTER(ctypes.c_longlong)]
+    L.lbib_last_timing.restype = ip
+    L.lbib_last_timing.argtypes = [vp, vp]
+    L.lbib_set_species_source.restype = ip
+    L.lbib_set_species_source.argtypes = [vp, ip, vp, ip]
+    L.lbib_set_profiling.restype = ip
+    L.lbib_set_profiling.argtypes = [vp, ip]
+    _lib = L
+    return L

@@ -163,30 +163,31 @@ def toy(n: int = 64, r: float = 10.0, nodes: int = 100, iterations: int = 100, r
 
 
 def hex_tissue(nx: int, ny: int, spacing: float, r0: float, jitter: float, nodes_per_cell: int,
-               seed: int, margin: float = 6.0) -> List[Tuple[int, np.ndarray]]:
-    """Cells on a hexagonal grid with radius r0 + U(-jitter, jitter)."""
+               seed: int, cols: int, rows: int) -> List[Tuple[int, np.ndarray]]:
+    """cols x rows cells on a hexagonal grid (centred in the lattice), radius
+    r0 + U(-jitter, jitter), each with a random phase for its first node."""
     rng = np.random.default_rng(seed)
+    dy = spacing * math.sqrt(3.0) / 2.0
+    w = (cols - 1) * spacing + spacing / 2.0
+    h = (rows - 1) * dy
+    x0, y0 = (nx - w) / 2.0, (ny - h) / 2.0
     cells = []
     dom = 1
-    dy = spacing * math.sqrt(3.0) / 2.0
-    row = 0
-    y = margin + r0 + jitter
-    while y + r0 + jitter + margin <= ny:
-        x = margin + r0 + jitter + (spacing / 2.0 if row % 2 else 0.0)
-        while x + r0 + jitter + margin <= nx:
+    for row in range(rows):
+        for col in range(cols):
+            x = x0 + col * spacing + (spacing / 2.0 if row % 2 else 0.0)
+            y = y0 + row * dy
             r = r0 + rng.uniform(-jitter, jitter)
             cells.append((dom, circle(x, y, r, nodes_per_cell, phase=rng.uniform(0, 2 * math.pi))))
             dom += 1
-            x += spacing
-        y += dy
-        row += 1
     return cells
 
 
 def config2(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> Config:
-    """1024x1024 tissue: ~400 cells on a hex grid (spacing 44), r=20+U(-2,2), 250 nodes/cell,
-    2 species (tau 0.8, 1.2), secretion 1e-3/step from a seeded 10% of the cells."""
-    cells = hex_tissue(1024, 1024, 44.0, 20.0, 2.0, 250, seed)
+    """1024x1024 tissue: 400 cells (20 x 20) on a hex grid (spacing 44), r=20+U(-2,2),
+    250 nodes/cell, 2 species (tau 0.8, 1.2), secretion 1e-3/step from a seeded 10% of
+    the cells."""
+    cells = hex_tissue(1024, 1024, 44.0, 20.0, 2.0, 250, seed, cols=20, rows=20)
     rng = np.random.default_rng(seed + 1)
     doms = [d for d, _ in cells]
     k = max(1, len(doms) // 10)

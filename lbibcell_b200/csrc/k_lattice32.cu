@@ -1,0 +1,194 @@
+// k_lattice32.cu — FP32-shifted lattice kernels.
+//
+// Storage: h_q = f_q - w_q (deviation from the rest state rho0 = 1, u = 0) in
+// FP32; collision arithmetic in FP32.  Algebraically the same update as the
+// FP64 path (FluidSolver.cpp:103-183 with Luo1993ForceModel.cpp:29-70):
+//   rho_F = 1 + sum h                      (force term density, no rhoToAdd)
+//   rho   = rho_F + rhoToAdd
+//   u     = (sum c_q h_q) / rho
+//   h_q' = h_q + (heq_q - h_q)/tau + 3 w_q rho_F (c_q . F)
+//   heq_q = w_q (rho - 1) + w_q rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)
+//   u'    = u + (rho_F / rho) F            (= sum c_q f_q' / rho)
+// Species (rest state 0) are stored as g_q and updated as in
+// CDESolverD2Q5.cpp:75-107 with the dt*R/3, dt*R/6 source.
+#include "kernels.cuh"
+
+namespace lbib {
+
+__device__ __forceinline__ float reaction32(int kind, float src, float decay, uint32_t dom, unsigned iteration,
+                                            float C) {
+    if (kind == RX_LINEAR) return src - decay * C;
+    if (kind == RX_SIGNAL) return (dom == 1 && iteration < 5000u) ? 0.0001f : -0.00001f * C;
+    return 0.0f;
+}
+
+__global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
+    if (a.status->halt) return;
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.L) return;
+    const int nx = a.nx, ny = a.ny;
+    const int x = (int)(n % (size_t)nx), y = (int)(n / (size_t)nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const size_t L = a.L;
+    const size_t rC = (size_t)y * nx, rM = (size_t)ym * nx, rP = (size_t)yp * nx;
+    const float* fin = a.fin;
+    const float hT = fin[0 * L + rC + x];
+    const float hE = fin[1 * L + rC + xm];
+    const float hN = fin[2 * L + rM + x];
+    const float hW = fin[3 * L + rC + xp];
+    const float hS = fin[4 * L + rP + x];
+    const float hNE = fin[5 * L + rM + xm];
+    const float hNW = fin[6 * L + rM + xp];
+    const float hSW = fin[7 * L + rP + xp];
+    const float hSE = fin[8 * L + rP + xm];
+
+    const uint32_t dom = a.dom[n];
+    float rta = 0.0f;
+    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = (float)a.massTab[dom];
+    float Fx = 0.0f, Fy = 0.0f;
+    if (a.tileCount[(y / kTile) * a.tilesX + (x / kTile)] > 0) {
+        Fx = a.force[n];
+        Fy = a.force[L + n];
+    }
+    const float drho = ((hT + hE) + (hN + hW)) + ((hS + hNE) + (hNW + hSW)) + hSE;
+    const float dr = drho + rta;          // rho - 1
+    const float rhoF = 1.0f + drho;
+    const float rho = rhoF + rta;
+    const float jx = (hE - hW) + (hNE - hNW) + (hSE - hSW);
+    const float jy = (hN - hS) + (hNE - hSE) + (hNW - hSW);
+    const float rinv = 1.0f / rho;
+    const float ux = jx * rinv, uy = jy * rinv;
+    const float tauI = (float)(1.0 / a.tauF);
+    const float usq = 1.5f * (ux * ux + uy * uy);
+    const float w0 = 4.0f / 9.0f, w1 = 1.0f / 9.0f, w2 = 1.0f / 36.0f;
+    const float f3 = 3.0f * rhoF;
+    float* fo = a.fout;
+    // rest
+    {
+        const float heq = w0 * dr + w0 * rho * (-usq);
+        fo[0 * L + n] = hT + (heq - hT) * tauI;
+    }
+#define LBIB_Q(idx, h, w, cu, cf)                                                 \
+    {                                                                             \
+        const float c_u = (cu);                                                   \
+        const float heq = (w) * dr + (w) * rho * (3.0f * c_u + 4.5f * c_u * c_u - usq); \
+        fo[(idx) * L + n] = (h) + (heq - (h)) * tauI + (w) * f3 * (cf);           \
+    }
+    LBIB_Q(1, hE, w1, ux, Fx)
+    LBIB_Q(2, hN, w1, uy, Fy)
+    LBIB_Q(3, hW, w1, -ux, -Fx)
+    LBIB_Q(4, hS, w1, -uy, -Fy)
+    LBIB_Q(5, hNE, w2, ux + uy, Fx + Fy)
+    LBIB_Q(6, hNW, w2, -ux + uy, -Fx + Fy)
+    LBIB_Q(7, hSW, w2, -ux - uy, -Fx - Fy)
+    LBIB_Q(8, hSE, w2, ux - uy, Fx - Fy)
+#undef LBIB_Q
+    const float s = rhoF * rinv;
+    const float uxo = ux + s * Fx, uyo = uy + s * Fy;
+    a.u[n] = uxo;
+    a.u[L + n] = uyo;
+
+    for (int k = 0; k < a.S; ++k) {
+        const float* gin = a.gin + (size_t)k * 5 * L;
+        const float gT = gin[0 * L + rC + x];
+        const float gE = gin[1 * L + rC + xm];
+        const float gN = gin[2 * L + rM + x];
+        const float gW = gin[3 * L + rC + xp];
+        const float gS = gin[4 * L + rP + x];
+        const float C = ((gT + gE) + (gN + gW)) + gS;
+        const float tI = (float)(1.0 / a.sp[k].tau);
+        float src = 0.0f;
+        if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = (float)a.srcTab[(size_t)k * a.nDomains + dom];
+        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, a.iteration, C);
+        const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
+        const float e0 = C * (1.0f / 3.0f), e1 = C * (1.0f / 6.0f);
+        float* go = a.gout + (size_t)k * 5 * L;
+        go[0 * L + n] = gT + (e0 - gT) * tI + r0;
+        go[1 * L + n] = gE + (e1 * (1.0f + 3.0f * uxo) - gE) * tI + r1;
+        go[2 * L + n] = gN + (e1 * (1.0f + 3.0f * uyo) - gN) * tI + r1;
+        go[3 * L + n] = gW + (e1 * (1.0f - 3.0f * uxo) - gW) * tI + r1;
+        go[4 * L + n] = gS + (e1 * (1.0f - 3.0f * uyo) - gS) * tI + r1;
+    }
+}
+
+// MassSolverBoxOutlet in shifted storage: f' = f / rho, i.e.
+// h' = h / rho + w (1/rho - 1) = (h - w * drho) / rho with drho = sum h.
+__device__ __forceinline__ void rescale_node32(float* f, float* g, int S, size_t L, size_t n) {
+    const float wq[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
+                         1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
+    float drho = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) drho += f[(size_t)q * L + n];
+    const float rinv = 1.0f / (1.0f + drho);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float h = f[(size_t)q * L + n];
+        f[(size_t)q * L + n] = (h - wq[q] * drho) * rinv;
+    }
+    for (int k = 0; k < S; ++k)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] *= rinv;
+}
+
+__global__ void outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ny) {
+        rescale_node32(f, g, S, L, (size_t)i * nx);
+        if (i == 0) rescale_node32(f, g, S, L, 0);
+    } else if (i < ny + nx - 1) {
+        rescale_node32(f, g, S, L, (size_t)(i - ny + 1));
+    }
+}
+
+// Initial state: the FP64 initial collision (f_T = 1, zero force and mass)
+// converted to deviations, and the species' initial conditions.
+__global__ void init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1,
+                       double init2) {
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L) return;
+    const double wq[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                          1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+    const double tauI = 1.0 / tauF;
+    // f_q' = f_q - f_q/tau + w_q/tau with f = (1, 0, ..., 0), so h_q = (f_q - w_q)(1 - 1/tau).
+    for (int q = 0; q < 9; ++q) {
+        const double f0 = q == 0 ? 1.0 : 0.0;
+        f[(size_t)q * L + n] = (float)((f0 - wq[q]) * (1.0 - tauI));
+    }
+    u[n] = 0.0f;
+    u[L + n] = 0.0f;
+    const SpeciesConst sp[3] = {sp0, sp1, sp2};
+    const double init[3] = {init0, init1, init2};
+    for (int k = 0; k < S; ++k) {
+        double gi[5];
+        if (sp[k].kind == RX_NONE) {
+            const double tI = 1.0 / sp[k].tau;
+            gi[0] = 1.0 - tI + (1.0 / 3.0) * tI;
+            for (int q = 1; q < 5; ++q) gi[q] = (1.0 / 6.0) * tI;
+        } else if (sp[k].kind == RX_SIGNAL) {
+            for (int q = 0; q < 5; ++q) gi[q] = dom[n] == 0 ? 0.0 : 0.2;
+        } else {
+            for (int q = 0; q < 5; ++q) gi[q] = init[k] / 5.0;
+        }
+        for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] = (float)gi[q];
+    }
+}
+
+void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
+    stream_collide32<<<(unsigned)((a.L + 255) / 256), 256, 0, s>>>(a);
+}
+
+void launch_outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
+    const int n = nx + ny;
+    outlet32<<<(n + 255) / 256, 256, 0, s>>>(f, g, S, nx, ny, L, st);
+}
+
+void launch_init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+                   const SpeciesConst* sp, const double* init, cudaStream_t s) {
+    init32<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, S, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+                                                       init[1], init[2]);
+}
+
+}  // namespace lbib

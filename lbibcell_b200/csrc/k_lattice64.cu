@@ -1,0 +1,150 @@
+// k_lattice64.cu — FP64 (plain) lattice kernels.  Compiled with --fmad=false:
+// the results are bit-identical to the reference's double-precision run.
+//
+//   stream_collide64  fused pull streaming + D2Q9 BGK/Luo collision + S D2Q5
+//                     species with reaction.  Replaces FluidSolver::advect/collide
+//                     and CDESolver*::advect/collide (SimulationRunner.cpp:244-288).
+//                     Pull streaming f_q(x) <- f*_q(x - c_q) on the periodic
+//                     lattice (GeometryHandler.cpp:476-589) is the same
+//                     permutation as the reference's swap scheme
+//                     (FluidSolver.cpp:185-194, 259-264).
+//   outlet64          MassSolverBoxOutlet::calculateMass (MassSolverBoxOutlet.cpp:42-72).
+//   init64            SimulationRunner::initSolvers (SimulationRunner.cpp:290-306).
+#include "lattice_math.cuh"
+#include "kernels.cuh"
+
+namespace lbib {
+
+__global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
+    if (a.status->halt) return;
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.L) return;
+    const int nx = a.nx, ny = a.ny;
+    const int x = (int)(n % (size_t)nx), y = (int)(n / (size_t)nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const size_t L = a.L;
+    const size_t rC = (size_t)y * nx, rM = (size_t)ym * nx, rP = (size_t)yp * nx;
+    const double* fin = a.fin;
+    double f[9];
+    f[T] = fin[0 * L + rC + x];
+    f[E] = fin[1 * L + rC + xm];
+    f[N] = fin[2 * L + rM + x];
+    f[W] = fin[3 * L + rC + xp];
+    f[S] = fin[4 * L + rP + x];
+    f[NE] = fin[5 * L + rM + xm];
+    f[NW] = fin[6 * L + rM + xp];
+    f[SW] = fin[7 * L + rP + xp];
+    f[SE] = fin[8 * L + rP + xm];
+
+    const uint32_t dom = a.dom[n];
+    double rta = 0.0;
+    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
+    double fx = 0.0, fy = 0.0;
+    if (a.tileCount[(y / kTile) * a.tilesX + (x / kTile)] > 0) {
+        fx = a.force[n];
+        fy = a.force[L + n];
+    }
+    double ux, uy;
+    collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
+    a.u[n] = ux;
+    a.u[L + n] = uy;
+
+    for (int k = 0; k < a.S; ++k) {
+        const double* gin = a.gin + (size_t)k * 5 * L;
+        double g[5];
+        g[T] = gin[0 * L + rC + x];
+        g[E] = gin[1 * L + rC + xm];
+        g[N] = gin[2 * L + rM + x];
+        g[W] = gin[3 * L + rC + xp];
+        g[S] = gin[4 * L + rP + x];
+        double src = 0.0;
+        if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
+        collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.iteration);
+        double* gout = a.gout + (size_t)k * 5 * L;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) gout[q * L + n] = g[q];
+    }
+}
+
+// Column x=0 (all y) then row y=0 (all x); the corner (0,0) is rescaled
+// twice, first by the column pass.  rho is summed in the reference's slot
+// order after FluidSolver::localSwap: T, W, S, E, N, SW, SE, NE, NW.
+__device__ __forceinline__ void rescale_node64(double* f, double* g, int S, size_t L, size_t n) {
+    const int order[9] = {T, W, S, E, N, SW, SE, NE, NW};
+    double rho = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) rho += f[(size_t)order[i] * L + n];
+    const double sc = 1.0 / rho;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[(size_t)q * L + n] *= sc;
+    for (int k = 0; k < S; ++k)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] *= sc;
+}
+
+__global__ void outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // threads [0, ny): column nodes (0, i); thread 0 also runs the corner's
+    // row pass after its column pass.  threads [ny, ny + nx - 1): row nodes (x, 0), x >= 1.
+    if (i < ny) {
+        rescale_node64(f, g, S, L, (size_t)i * nx);
+        if (i == 0) rescale_node64(f, g, S, L, 0);
+    } else if (i < ny + nx - 1) {
+        const int x = i - ny + 1;
+        rescale_node64(f, g, S, L, (size_t)x);
+    }
+}
+
+// FluidSolver::initSolver (f_T = 1, then collide with zero force and mass)
+// and the species' initial conditions.
+__global__ void init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1, double init2) {
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L) return;
+    double fi[9] = {1.0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double ux, uy;
+    collide_fluid64(fi, 0.0, 0.0, 0.0, tauF, ux, uy);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[(size_t)q * L + n] = fi[q];
+    u[n] = ux;
+    u[L + n] = uy;
+    const SpeciesConst sp[3] = {sp0, sp1, sp2};
+    const double init[3] = {init0, init1, init2};
+    for (int k = 0; k < S; ++k) {
+        double gi[5];
+        if (sp[k].kind == RX_NONE) {
+            // CDESolverD2Q5::initSolver — CDESolverD2Q5.cpp:37-40
+            gi[0] = 1.0; gi[1] = gi[2] = gi[3] = gi[4] = 0.0;
+            collide_cde64(gi, ux, uy, sp[k].tau, RX_NONE, 0.0, 0.0, dom[n], 0);
+        } else if (sp[k].kind == RX_SIGNAL) {
+            // tutorial_01_CDESolverD2Q5_SIGNAL::initSolver — :46-57
+            const double v = dom[n] == 0 ? 0.0 : 1.0 / 5.0;
+            for (int q = 0; q < 5; ++q) gi[q] = v;
+        } else {
+            for (int q = 0; q < 5; ++q) gi[q] = init[k] / 5.0;
+        }
+        for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] = gi[q];
+    }
+}
+
+void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
+    const unsigned blocks = (unsigned)((a.L + 255) / 256);
+    stream_collide64<<<blocks, 256, 0, s>>>(a);
+}
+
+void launch_outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
+    const int n = nx + ny;
+    outlet64<<<(n + 255) / 256, 256, 0, s>>>(f, g, S, nx, ny, L, st);
+}
+
+void launch_init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+                   const SpeciesConst* sp, const double* init, cudaStream_t s) {
+    init64<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, S, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+                                                       init[1], init[2]);
+}
+
+}  // namespace lbib

@@ -1,0 +1,806 @@
+// k_membrane.cu — immersed-boundary and geometry kernels.  Compiled with
+// --fmad=false: every FP64 result is bit-identical to the reference.
+//
+//   force_eval       ForceSolver::calculateForce (ForceSolver.cpp:42-85) over a
+//                    per-node CSR of force records in insertion order
+//                    (ForceStructs.hpp:49-588).
+//   spread           SimulationRunner::distributeForce + GeometryNode::distributeForce
+//                    (SimulationRunner.cpp:425-453, GeometryNode.cpp:228-235) as a
+//                    deterministic gather: each 16x16 lattice tile collects the
+//                    membrane nodes whose 4x4 stencil overlaps it, sorts them by
+//                    id and every lattice node sums its contributions in id order
+//                    (the reference's serial map order).  No floating-point atomics.
+//   interp_move      GeometryNode::collectVelocity (GeometryNode.cpp:216-226, slot
+//                    order (4x+y) mod 16 from GeometryHandler.cpp:641), the speed
+//                    check (LagrangianPoint.cpp:92-103) and GeometryNode::move
+//                    (GeometryNode.cpp:245-254); positions that need the
+//                    reference's random perturbation (GeometryNode.cpp:153-214)
+//                    are flagged for the host, which owns the generator.
+//   crossings        Connection::generateBoundaryNodes / insertBoundaryNode
+//                    (Connection.cpp:181-324): every crossing of a connection with
+//                    a lattice line is a candidate for one (node, slot); the
+//                    closest wins, ties keep the earlier connection.
+//   reinit           PhysicalNode::updateDomainIdentifier + CDESolverD2Q5::reinitialise
+//                    (PhysicalNode.cpp:109-124, CDESolverD2Q5.cpp:156-228) in
+//                    row-major order semantics, processed in dependency rounds.
+//   domain_fill      GeometryHandler::updateAllDomainIdentifiers (GeometryHandler.cpp:68-85).
+#include <cub/cub.cuh>
+
+#include "kernels.cuh"
+#include "lattice_math.cuh"
+
+namespace lbib {
+
+// ---------------------------------------------------------------------------
+// fastCos and the Dirac weight: GeometryNode.cpp:55-94.
+__device__ __forceinline__ double fast_cos(const double x) {
+    const double halfPi = M_PI / 2.0;
+    const double doublePi = 2.0 * M_PI;
+    double cs;
+    double tempx = x + halfPi;
+    if (tempx > M_PI) tempx -= doublePi;
+    if (tempx < .00) {
+        cs = 1.27323954 * tempx + 0.405284735 * tempx * tempx;
+    } else {
+        cs = 1.27323954 * tempx - 0.405284735 * tempx * tempx;
+    }
+    if (cs < 0.0) {
+        cs = 0.225 * (cs * -cs - cs) + cs;
+    } else {
+        cs = 0.225 * (cs * cs - cs) + cs;
+    }
+    return cs;
+}
+
+__device__ __forceinline__ double dirac(const double dx, const double dy) {
+    const double halfPi = M_PI / 2.0;
+    return ((1.0 + fast_cos(halfPi * dx)) * (1.0 + fast_cos(halfPi * dy))) / 16.0;
+}
+
+// ---------------------------------------------------------------------------
+// Force evaluation
+__global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.M) return;
+    const double x1 = m.x[i], y1 = m.y[i];
+    double Fx = 0.0, Fy = 0.0;
+    const int r0 = m.foff[i], r1 = m.foff[i + 1];
+    for (int r = r0; r < r1; ++r) {
+        const int type = m.ftype[r];
+        const double* p = m.fpar + 4 * (size_t)r;
+        const int j = m.fpartner[r];
+        if ((type == 0 || type == 7 || type == 5 || type == 6) && (j < 0 || j >= m.M)) {
+            raise_error(st, ERR_FORCE_NODE, i, ST_FORCE);
+            return;
+        }
+        switch (type) {
+            case 0: case 7: {  // spring between two nodes: f = k(|d| - l0), along d
+                const double x2 = m.x[j], y2 = m.y[j];
+                const double dist = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+                const double f = p[0] * (dist - p[1]);
+                Fx += ((x2 - x1) * f) / dist;
+                Fy += ((y2 - y1) * f) / dist;
+                break;
+            }
+            case 1: {  // anchor spring to (x, y)
+                const double tx = p[0], ty = p[1];
+                const double dist = sqrt((tx - x1) * (tx - x1) + (ty - y1) * (ty - y1));
+                const double f = p[2] * (dist - p[3]);
+                if (dist != 0.0) {
+                    Fx += ((tx - x1) * f) / dist;
+                    Fy += ((ty - y1) * f) / dist;
+                }
+                break;
+            }
+            case 2:  // constant force
+                Fx += p[0];
+                Fy += p[1];
+                break;
+            case 3: {  // horizontal slider at y
+                const double dist = sqrt((x1 - x1) * (x1 - x1) + (p[0] - y1) * (p[0] - y1));
+                const double f = p[1] * (dist - p[2]);
+                Fx += 0.0;
+                Fy += (y1 < p[0]) ? f : -f;
+                break;
+            }
+            case 4: {  // vertical slider at x
+                const double dist = sqrt((p[0] - x1) * (p[0] - x1) + (y1 - y1) * (y1 - y1));
+                const double f = p[1] * (dist - p[2]);
+                Fx += (x1 < p[0]) ? f : -f;
+                Fy += 0.0;
+                break;
+            }
+            default: {  // 5, 6: constant-magnitude pull toward the partner
+                const double x2 = m.x[j], y2 = m.y[j];
+                const double dist = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+                Fx += ((x2 - x1) * p[0]) / dist;
+                Fy += ((y2 - y1) * p[0]) / dist;
+                break;
+            }
+        }
+    }
+    m.fx[i] = Fx;
+    m.fy[i] = Fy;
+}
+
+template <typename Real>
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
+    if (m.M == 0) return;
+    force_eval_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, st, iteration);
+}
+template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t);
+template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Spreading
+
+// Stencil origin of a membrane node: x in [ceil(X-2), floor(X+2)]
+// (GeometryHandler.cpp:613-643).  For a non-integer X the stencil is 4 wide.
+__device__ __forceinline__ bool stencil_origin(double X, double Y, int nx, int ny, int& x0, int& y0) {
+    x0 = (int)ceil(X - 2.0);
+    y0 = (int)ceil(Y - 2.0);
+    const int x1 = (int)floor(X + 2.0), y1 = (int)floor(Y + 2.0);
+    return x1 - x0 == 3 && y1 - y0 == 3 && x0 >= 0 && y0 >= 0 && x1 < nx && y1 < ny;
+}
+
+__global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st, int pass) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.M) return;
+    int x0, y0;
+    if (!stencil_origin(m.x[i], m.y[i], nx, ny, x0, y0)) {
+        raise_error(st, ERR_STENCIL, i, ST_SPREAD);
+        return;
+    }
+    const int tx0 = x0 / kTile, tx1 = (x0 + 3) / kTile, ty0 = y0 / kTile, ty1 = (y0 + 3) / kTile;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) {
+            const int tile = ty * t.tilesX + tx;
+            if (pass == 0) {
+                atomicAdd(&t.count[tile], 1);
+            } else {
+                const int slot = atomicAdd(&t.fill[tile], 1);
+                const int pos = t.start[tile] + slot;
+                if (pos < t.cap) t.list[pos] = i;
+            }
+        }
+}
+
+constexpr int kSpreadMax = 1024;  // membrane stencils per tile held in shared memory
+
+template <typename Real>
+__global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
+                                                     Status* st) {
+    if (st->halt) return;
+    const int tile = blockIdx.x;
+    const int cnt = t.count[tile];
+    if (cnt == 0) return;
+    if (cnt > kSpreadMax || t.start[tile] + cnt > t.cap) {
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
+        return;
+    }
+    __shared__ int idx[kSpreadMax];
+    __shared__ double sx[kSpreadMax], sy[kSpreadMax], sfx[kSpreadMax], sfy[kSpreadMax];
+    __shared__ int sx0[kSpreadMax], sy0[kSpreadMax];
+    int p2 = 1;
+    while (p2 < cnt) p2 <<= 1;
+    const int base = t.start[tile];
+    for (int k = threadIdx.x; k < p2; k += blockDim.x) idx[k] = k < cnt ? t.list[base + k] : 0x7fffffff;
+    __syncthreads();
+    // bitonic sort by membrane index (= id order)
+    for (int size = 2; size <= p2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = threadIdx.x; k < p2; k += blockDim.x) {
+                const int j = k ^ stride;
+                if (j > k) {
+                    const bool up = (k & size) == 0;
+                    const int a = idx[k], b = idx[j];
+                    if ((a > b) == up) { idx[k] = b; idx[j] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int i = idx[k];
+        sx[k] = m.x[i]; sy[k] = m.y[i]; sfx[k] = m.fx[i]; sfy[k] = m.fy[i];
+        sx0[k] = (int)ceil(sx[k] - 2.0);
+        sy0[k] = (int)ceil(sy[k] - 2.0);
+    }
+    __syncthreads();
+    const int tx = tile % t.tilesX, ty = tile / t.tilesX;
+    const int x = tx * kTile + (threadIdx.x & 15), y = ty * kTile + (threadIdx.x >> 4);
+    if (x >= nx || y >= ny) return;
+    double ax = 0.0, ay = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+        const int dx0 = x - sx0[k], dy0 = y - sy0[k];
+        if ((unsigned)dx0 < 4u && (unsigned)dy0 < 4u) {
+            const double dl = dirac((double)x - sx[k], (double)y - sy[k]);
+            ax += sfx[k] * dl;
+            ay += sfy[k] * dl;
+        }
+    }
+    const size_t n = (size_t)y * nx + x;
+    force[n] = (Real)ax;
+    force[L + n] = (Real)ay;
+}
+
+template <typename Real>
+void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
+                   unsigned iteration, cudaStream_t s) {
+    cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
+    cudaMemsetAsync(t.fill, 0, sizeof(int) * t.nTiles, s);
+    if (m.M == 0) return;
+    const int blocks = (m.M + 127) / 128;
+    tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
+    tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
+    spread_kernel<Real><<<t.nTiles, 256, 0, s>>>(m, t, force, nx, ny, L, st);
+}
+template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
+                                    cudaStream_t);
+template void launch_spread<float>(const MembraneDev&, TileDev&, float*, int, int, size_t, Status*, unsigned,
+                                   cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Interpolation and motion
+
+__device__ __forceinline__ bool needs_perturbation(double X, double Y) {
+    // The four tests of GeometryNode::perturbatePosition (GeometryNode.cpp:160, 174, 189, 202).
+    if (fabs((double)(int)X - X) <= kEPSILON) return true;
+    if (fabs((double)(int)Y - Y) <= kEPSILON) return true;
+    if (fabs(Y - floor(Y) - (X - floor(X))) <= kEPSILON) return true;
+    if (fabs(ceil(Y) - Y - (X - floor(X))) <= kEPSILON) return true;
+    return false;
+}
+
+template <typename Real>
+__global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny, size_t L, CrossDev c, Status* st,
+                                   unsigned iteration) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.M) return;
+    const double X = m.x[i], Y = m.y[i];
+    int x0, y0;
+    if (!stencil_origin(X, Y, nx, ny, x0, y0)) {
+        raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
+        return;
+    }
+    double vx = 0.0, vy = 0.0;
+    const int base = ((4 * x0 + y0) % 16 + 16) % 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int r = (k - base + 16) & 15;
+        const int xk = x0 + (r >> 2), yk = y0 + (r & 3);
+        const size_t n = (size_t)yk * nx + xk;
+        const double dl = dirac((double)xk - X, (double)yk - Y);
+        vx += (double)u[n] * dl;
+        vy += (double)u[L + n] * dl;
+    }
+    m.vx[i] = vx;
+    m.vy[i] = vy;
+    const double CS = 1 / sqrt(3.0);
+    if (((vx * vx) + (vy * vy)) > CS) {
+        raise_error(st, ERR_SPEED, i, ST_INTERP_MOVE);
+        return;
+    }
+    m.ox[i] = X;
+    m.oy[i] = Y;
+    const double Xn = X + vx, Yn = Y + vy;
+    m.x[i] = Xn;
+    m.y[i] = Yn;
+    if (needs_perturbation(Xn, Yn)) {
+        const int k = atomicAdd(&st->nPerturbNode, 1);
+        if (k < c.perturbCap) c.perturbList[k] = i;
+        raise_halt(st, ST_INTERP_MOVE);
+    }
+}
+
+template <typename Real>
+void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
+                        unsigned iteration, cudaStream_t s) {
+    if (m.M == 0) return;
+    interp_move_kernel<Real><<<(m.M + 127) / 128, 128, 0, s>>>(m, u, nx, ny, L, c, st, iteration);
+}
+template void launch_interp_move<double>(const MembraneDev&, const double*, int, int, size_t, CrossDev&, Status*,
+                                         unsigned, cudaStream_t);
+template void launch_interp_move<float>(const MembraneDev&, const float*, int, int, size_t, CrossDev&, Status*,
+                                        unsigned, cudaStream_t);
+
+// Connection::perturbConnection's tests (Connection.cpp:339, 363).
+__global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
+    if (st->halt) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.C) return;
+    const int a = m.ca[c], b = m.cb[c];
+    if (fabs(m.x[a] - m.x[b]) < kEPSILON || fabs(m.y[a] - m.y[b]) < kEPSILON) {
+        atomicAdd(&st->nPerturbConn, 1);
+        raise_halt(st, ST_PERTURB_CONN);
+    }
+}
+
+void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
+    if (m.C == 0) return;
+    perturb_conn_kernel<<<(m.C + 127) / 128, 128, 0, s>>>(m, st);
+}
+
+// ---------------------------------------------------------------------------
+// Crossings: three passes over the connections.
+//   pass 0: closest distance per (node, slot) by atomicMin on the distance bits
+//           (non-negative doubles order like their bit patterns);
+//   pass 1: among records at that distance, the earliest connection;
+//   pass 2: the winner writes its domain; the winner of a node's last present
+//           slot (order E,N,W,S = the reference's boundaryNodes_ scan order)
+//           decides the node's tentative domain (PhysicalNode.cpp:111-115).
+constexpr unsigned long long kEmpty = ~0ull;
+
+__device__ __forceinline__ int slot_code(int d) {  // E,N,W,S -> 0..3
+    return d - 1;
+}
+
+__device__ __forceinline__ void cross_record(const CrossDev& c, const uint32_t* dom, Status* st, int pass,
+                                             int conn, int nx, int ny, int px, int py, int dirSlot, double bx,
+                                             double by, uint32_t bdom) {
+    if (px < 0 || py < 0 || px >= nx || py >= ny) {
+        raise_error(st, ERR_EDGE_W, conn, ST_CROSSINGS);
+        return;
+    }
+    const size_t node = (size_t)py * nx + px;
+    const double d2 = ((double)px - bx) * ((double)px - bx) + ((double)py - by) * ((double)py - by);
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
+    const size_t key = node * 4 + slot_code(dirSlot);
+    if (pass == 0) {
+        const unsigned long long old = atomicMin(&c.bnDist[key], bits);
+        if (old == kEmpty) {
+            const int k = atomicAdd(&st->nRecords, 1);
+            if (k < c.touchedCap) c.touched[k] = (uint32_t)key;
+            else raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
+        }
+    } else if (pass == 1) {
+        if (c.bnDist[key] == bits) atomicMin(&c.bnConn[key], (uint32_t)conn);
+    } else {
+        if (c.bnDist[key] == bits && c.bnConn[key] == (uint32_t)conn) {
+            c.bnDom[key] = bdom;
+            const int s = slot_code(dirSlot);
+            if (s == 2) c.wDom[node] = bdom + 1;
+            bool last = true;
+            for (int s2 = s + 1; s2 < 4; ++s2)
+                if (c.bnDist[node * 4 + s2] != kEmpty) last = false;
+            if (last && bdom != dom[node]) {
+                const int k = atomicAdd(&st->nChanged, 1);
+                if (k < c.changedCap) {
+                    c.changedNode[k] = (uint32_t)node;
+                    c.changedDom[k] = bdom;
+                } else {
+                    raise_error(st, ERR_CAPACITY, (int)node, ST_CROSSINGS);
+                }
+            }
+        }
+    }
+}
+
+__global__ void crossings_kernel(MembraneDev m, CrossDev c, const uint32_t* dom, int nx, int ny, Status* st,
+                                 int pass) {
+    if (st->halt) return;
+    const int cn = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cn >= m.C) return;
+    const int a = m.ca[cn], b = m.cb[cn];
+    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+    const uint32_t D = m.cdom[cn];
+    const double maxX = x1 < x2 ? x2 : x1, maxY = y1 < y2 ? y2 : y1;
+    const double minX = x2 < x1 ? x2 : x1, minY = y2 < y1 ? y2 : y1;
+    const double mm = (y2 - y1) / (x2 - x1);
+    const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
+    if (!isfinite(mm)) {
+        raise_error(st, ERR_VERTICAL, cn, ST_CROSSINGS);
+        return;
+    }
+    // keeps the line loops bounded for positions off the lattice
+    if (!(minX >= -1.0 && maxX <= nx + 1.0 && minY >= -1.0 && maxY <= ny + 1.0)) {
+        raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
+        return;
+    }
+    if (pass == 0) {
+        const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
+        if (len > kMAXLENGTH) st->remesh = 1;
+    }
+    const bool eastward = x1 < x2, southward = y1 > y2;
+    for (int i = (int)ceil(minX); i <= (int)floor(maxX); i++) {
+        const double yc = mm * i + nn;
+        // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
+        cross_record(c, dom, st, pass, cn, nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D);
+        cross_record(c, dom, st, pass, cn, nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u);
+    }
+    for (int i = (int)ceil(minY); i <= (int)floor(maxY); i++) {
+        const double xc = (i - nn) / mm;
+        // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
+        cross_record(c, dom, st, pass, cn, nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D);
+        cross_record(c, dom, st, pass, cn, nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u);
+    }
+}
+
+// GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test for nodes
+// that left their previous unit cell (GeometryHandler.cpp:610-636,
+// GeometryNode.cpp:256-261, Rectangle.cpp pointWithinBounds).
+__global__ void edge_check_kernel(MembraneDev m, int nx, int ny, Status* st, int stage) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.M) return;
+    const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
+    const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
+    if (within) return;
+    if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, stage);
+    else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, stage);
+    else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, stage);
+    else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, stage);
+}
+
+template <typename Real>
+void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, int nx, int ny, size_t L, Status* st,
+                      unsigned iteration, cudaStream_t s) {
+    if (m.C == 0) return;
+    const int blocks = (m.C + 127) / 128;
+    for (int pass = 0; pass < 3; ++pass) crossings_kernel<<<blocks, 128, 0, s>>>(m, c, dom, nx, ny, st, pass);
+    edge_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_CROSSINGS);
+}
+template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
+                                       unsigned, cudaStream_t);
+template void launch_crossings<float>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
+                                      unsigned, cudaStream_t);
+
+void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigned iteration, cudaStream_t s) {
+    if (m.M == 0) return;
+    edge_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_REMESH);
+}
+
+// ---------------------------------------------------------------------------
+// Reinitialisation of the species at nodes whose domain changed.
+//
+// The reference visits all lattice nodes in row-major order; a changed node
+// takes its new domain and re-initialises from its E,N,W,S neighbours of the
+// same domain that have no boundary node on the link, reading neighbours that
+// come earlier in the order with their new state and later ones with their old
+// state.  Here one block sorts the changed nodes, records for each the earlier
+// changed nodes among its E,N,W,S,NE (read after write) and SW (write after
+// read) neighbours, and processes nodes in rounds once those are done.
+constexpr int kReinitMax = 1024;
+
+template <typename Real>
+__device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int S,
+                            const SpeciesConst* sp, const double* srcTab, int nDomains, const uint32_t* ctypeTab,
+                            int cellTypesCopied, const CrossDev& c, int nx, int ny, size_t L, Status* st,
+                            unsigned iteration) {
+    const uint32_t oldDom = dom[n];
+    dom[n] = newDom;
+    const int x = (int)(n % nx), y = (int)(n / nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const size_t nb[4] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x};
+    const size_t nNE = (size_t)yp * nx + xp;
+    bool hasBN[4];
+    for (int s = 0; s < 4; ++s) hasBN[s] = c.bnDist[n * 4 + s] != kEmpty;
+    // boundaryNodes_[NE] aliases (domainIdentifier_, cellType_): null only if both are 0.
+    const uint32_t ctype = cellTypesCopied ? (oldDom < (uint32_t)nDomains ? ctypeTab[oldDom] : 1u) : 0u;
+    const bool neNull = newDom == 0 && ctype == 0;
+    const double ux = (double)u[n], uy = (double)u[L + n];
+    for (int k = 0; k < S; ++k) {
+        Real* gk = g + (size_t)k * 5 * L;
+        double sumC = 0.0;
+        int counter = 0;
+        for (int s = 0; s < 4; ++s) {
+            const size_t mnode = nb[s];
+            if (!hasBN[s] && newDom == dom[mnode]) {
+                // getC() in slot order after localSwap: T, W, S, E, N
+                double C = 0.0;
+                C += (double)gk[0 * L + mnode];
+                C += (double)gk[3 * L + mnode];
+                C += (double)gk[4 * L + mnode];
+                C += (double)gk[1 * L + mnode];
+                C += (double)gk[2 * L + mnode];
+                sumC += C;
+                counter++;
+            }
+        }
+        if (counter == 0 && neNull && newDom == dom[nNE]) {
+            double C = 0.0;
+            C += (double)gk[0 * L + nNE];
+            C += (double)gk[3 * L + nNE];
+            C += (double)gk[4 * L + nNE];
+            C += (double)gk[1 * L + nNE];
+            C += (double)gk[2 * L + nNE];
+            sumC += C;
+            counter++;
+            atomicAdd(&st->nDiagReinit, 1);
+        }
+        if (counter == 0) atomicAdd(&st->nFailedReinit, 1);
+        sumC /= static_cast<double>(counter);
+        double gi[5];
+        for (int q = 0; q < 5; ++q) gi[q] = sumC / 5.0;
+        const double src = (srcTab != nullptr && newDom < (uint32_t)nDomains) ? srcTab[(size_t)k * nDomains + newDom]
+                                                                            : 0.0;
+        collide_cde64(gi, ux, uy, sp[k].tau, sp[k].kind, src, sp[k].decay, newDom, iteration);
+        for (int q = 0; q < 5; ++q) gk[(size_t)q * L + n] = (Real)gi[q];
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int S,
+                                                      SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2,
+                                                      const double* srcTab, int nDomains, const uint32_t* ctypeTab,
+                                                      int cellTypesCopied, int nx, int ny, size_t L, Status* st,
+                                                      unsigned iteration) {
+    if (st->halt) return;
+    const int cnt = st->nChanged;
+    if (cnt == 0) return;
+    if (cnt > kReinitMax || cnt > c.changedCap) {
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, cnt, ST_REINIT);
+        return;
+    }
+    const SpeciesConst sp[3] = {sp0, sp1, sp2};
+    __shared__ unsigned long long key[kReinitMax];  // node << 32 | newDom
+    __shared__ int deps[kReinitMax][6];
+    __shared__ unsigned char done[kReinitMax];
+    __shared__ int remaining;
+    int p2 = 1;
+    while (p2 < cnt) p2 <<= 1;
+    for (int k = threadIdx.x; k < p2; k += blockDim.x)
+        key[k] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
+    __syncthreads();
+    for (int size = 2; size <= p2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = threadIdx.x; k < p2; k += blockDim.x) {
+                const int j = k ^ stride;
+                if (j > k) {
+                    const bool up = (k & size) == 0;
+                    const unsigned long long a = key[k], b = key[j];
+                    if ((a > b) == up) { key[k] = b; key[j] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const size_t n = (size_t)(key[k] >> 32);
+        const int x = (int)(n % nx), y = (int)(n / nx);
+        const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+        const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+        const size_t nbs[6] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x,
+                               (size_t)yp * nx + xp, (size_t)ym * nx + xm};
+        for (int d = 0; d < 6; ++d) {
+            deps[k][d] = -1;
+            const size_t mnode = nbs[d];
+            if (mnode >= n) continue;
+            int lo = 0, hi = k - 1;
+            while (lo <= hi) {
+                const int mid = (lo + hi) >> 1;
+                const size_t v = (size_t)(key[mid] >> 32);
+                if (v == mnode) { deps[k][d] = mid; break; }
+                if (v < mnode) lo = mid + 1; else hi = mid - 1;
+            }
+        }
+        done[k] = 0;
+    }
+    if (threadIdx.x == 0) remaining = cnt;
+    __syncthreads();
+    int rounds = 0;
+    while (remaining > 0 && rounds < kReinitMax + 1) {
+        __shared__ int nowDone;
+        if (threadIdx.x == 0) nowDone = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+            if (done[k]) continue;
+            bool ready = true;
+            for (int d = 0; d < 6; ++d)
+                if (deps[k][d] >= 0 && done[deps[k][d]] != 1) ready = false;
+            if (ready) done[k] = 2;  // processing this round
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+            if (done[k] == 2) {
+                reinit_node<Real>((size_t)(key[k] >> 32), (uint32_t)(key[k] & 0xffffffffu), dom, g, u, S, sp, srcTab,
+                                  nDomains, ctypeTab, cellTypesCopied, c, nx, ny, L, st, iteration);
+                atomicAdd(&nowDone, 1);
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x)
+            if (done[k] == 2) done[k] = 1;
+        if (threadIdx.x == 0) remaining -= nowDone;
+        __syncthreads();
+        ++rounds;
+    }
+}
+
+template <typename Real>
+void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int S, const SpeciesConst* sp,
+                   const double* srcTab, int nDomains, const uint32_t* ctypeTab, int cellTypesCopied, int nx, int ny,
+                   size_t L, Status* st, unsigned iteration, cudaStream_t s) {
+    if (c.changedCap <= 0) return;
+    reinit_kernel<Real><<<1, 1024, 0, s>>>(c, dom, g, u, S, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
+                                           cellTypesCopied, nx, ny, L, st, iteration);
+}
+template void launch_reinit<double>(CrossDev&, uint32_t*, double*, const double*, int, const SpeciesConst*,
+                                    const double*, int, const uint32_t*, int, int, int, size_t, Status*, unsigned,
+                                    cudaStream_t);
+template void launch_reinit<float>(CrossDev&, uint32_t*, float*, const float*, int, const SpeciesConst*,
+                                   const double*, int, const uint32_t*, int, int, int, size_t, Status*, unsigned,
+                                   cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Domain fill: one block per row; the row's domain id at x >= 1 is the domain
+// of the last W-slot boundary node at x' in [1, x], else dom(0, y), which must
+// be 0 (GeometryHandler.cpp:68-85).  Reads and clears the W-slot plane.
+__global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* dom, int nx, int ny, Status* st) {
+    if (st->halt) return;
+    const int y = blockIdx.x;
+    const size_t row = (size_t)y * nx;
+    const uint32_t left = dom[row];
+    if (left != 0) {
+        if (threadIdx.x == 0) raise_error(st, ERR_LEFT_DOMAIN, y, ST_DOMAIN);
+        return;
+    }
+    const int chunk = (nx + blockDim.x - 1) / blockDim.x;
+    const int xb = threadIdx.x * chunk;
+    const int xe = min(nx, xb + chunk);
+    // last W mark in this thread's chunk (x >= 1): (x << 32 | value)
+    unsigned long long last = 0;
+    for (int x = max(xb, 1); x < xe; ++x) {
+        const uint32_t w = c.wDom[row + x];
+        if (w) last = ((unsigned long long)(x + 1) << 32) | (w - 1);
+    }
+    typedef cub::BlockScan<unsigned long long, 256> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    unsigned long long carry;
+    Scan(tmp).ExclusiveScan(last, carry, 0ull, cub::Max());
+    uint32_t cur = carry ? (uint32_t)(carry & 0xffffffffu) : left;
+    for (int x = max(xb, 1); x < xe; ++x) {
+        const uint32_t w = c.wDom[row + x];
+        if (w) {
+            cur = w - 1;
+            c.wDom[row + x] = 0;
+        }
+        dom[row + x] = cur;
+    }
+}
+
+// Resets the (node, slot) entries this step wrote.
+__global__ void cross_clear_kernel(CrossDev c, Status* st) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = min(st->nRecords, c.touchedCap);
+    if (k >= n) return;
+    const uint32_t key = c.touched[k];
+    c.bnDist[key] = kEmpty;
+    c.bnConn[key] = ~0u;
+}
+
+void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
+                        cudaStream_t s) {
+    domain_fill_kernel<<<ny, 256, 0, s>>>(c, dom, nx, ny, st);
+}
+
+void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s) {
+    if (c.touchedCap <= 0) return;
+    cross_clear_kernel<<<(c.touchedCap + 255) / 256, 256, 0, s>>>(c, st);
+}
+
+// ---------------------------------------------------------------------------
+// Topology checks
+
+__global__ void remesh_check_kernel(Status* st) {
+    if (st->halt) return;
+    if (st->remesh) raise_halt(st, ST_REMESH);
+}
+
+void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s) { remesh_check_kernel<<<1, 1, 0, s>>>(st); }
+
+// GeometryHandler::coarsenBoundary's test (GeometryHandler.cpp:444-449): the
+// span from the previous node to the next node is below MAXLENGTH.
+__global__ void coarsen_check_kernel(MembraneDev m, Status* st) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.M) return;
+    const int p = m.prev[i], q = m.next[i];
+    const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
+    const double length = sqrt(dx * dx + dy * dy);
+    if (length < kMAXLENGTH) {
+        st->coarsen = 1;
+        raise_halt(st, ST_COARSEN);
+    }
+}
+
+void launch_coarsen_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
+    if (m.M == 0) return;
+    coarsen_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, st);
+}
+
+__global__ void clear_forces_kernel(int* foff, int M) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= M) foff[i] = 0;
+}
+
+void launch_clear_forces(MembraneDev& m, cudaStream_t s) {
+    clear_forces_kernel<<<(m.M + 1 + 255) / 256, 256, 0, s>>>(m.foff, m.M);
+}
+
+// Tension renewal when the force list holds only tension pairs: node i gets
+// one type-6 record toward each ring neighbour, ordered by the position of the
+// contributing connection in the connection vector
+// (tutorial_01_BioSolverMembraneTension.cpp:52-73 adds them in that order).
+__global__ void tension_pos_kernel(MembraneDev m, int* outPos, int* inPos) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.C) return;
+    outPos[m.ca[c]] = c;
+    inPos[m.cb[c]] = c;
+}
+
+__global__ void tension_fill_kernel(MembraneDev m, const int* outPos, const int* inPos, double force) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m.M) return;
+    m.foff[i] = 2 * i;
+    if (i == m.M) return;
+    const int nextNode = m.cb[outPos[i]], prevNode = m.ca[inPos[i]];
+    const int first = outPos[i] < inPos[i] ? 0 : 1;
+    m.ftype[2 * i + first] = 6;
+    m.fpartner[2 * i + first] = nextNode;
+    m.ftype[2 * i + 1 - first] = 6;
+    m.fpartner[2 * i + 1 - first] = prevNode;
+    for (int q = 0; q < 4; ++q) {
+        m.fpar[4 * (2 * i) + q] = q == 0 ? force : 0.0;
+        m.fpar[4 * (2 * i + 1) + q] = q == 0 ? force : 0.0;
+    }
+}
+
+void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s) {
+    if (m.M == 0) return;
+    tension_pos_kernel<<<(m.C + 127) / 128, 128, 0, s>>>(m, outPos, inPos);
+    tension_fill_kernel<<<(m.M + 1 + 127) / 128, 128, 0, s>>>(m, outPos, inPos, force);
+}
+
+// ---------------------------------------------------------------------------
+// Areas (GeometryHandler::computeAreas, shoelace in ring order) and the
+// LbibAreaRegulator mass source per domain.
+__global__ void areas_kernel(MembraneDev m, double* area) {
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= m.nCells) return;
+    const int b = m.ringStart[cell], e = m.ringStart[cell + 1];
+    const int np = e - b;
+    double sum = 0.0;
+    for (int k = 0; k < np; ++k) {
+        const int i = m.ringNode[b + k];
+        const int j = m.ringNode[b + (k + 1 == np ? 0 : k + 1)];
+        sum += m.x[i] * m.y[j] - m.x[j] * m.y[i];
+    }
+    area[cell] = sum / 2.0;
+}
+
+__global__ void area_regulator_kernel(MembraneDev m, const double* area, double* target, double* massTab,
+                                      int nDomains, double factor, double strength, double maxsource,
+                                      const Status* st) {
+    if (st->halt) return;
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= m.nCells) return;
+    const double A = area[cell];
+    if (isnan(target[cell])) target[cell] = factor * A;
+    const double tgt = target[cell];
+    double r = strength * (tgt - A) / tgt;
+    if (r > maxsource) r = maxsource;
+    else if (r < -maxsource) r = -maxsource;
+    const uint32_t d = m.ringDom[cell];
+    if (d < (uint32_t)nDomains && d != 0) massTab[d] = r;
+}
+
+void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
+    if (m.nCells == 0) return;
+    areas_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area);
+}
+
+void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
+                           double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
+    if (m.nCells == 0) return;
+    areas_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area);
+    area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
+                                                                 strength, maxsource, st);
+}
+
+}  // namespace lbib

@@ -1,0 +1,96 @@
+// kernels.cuh — launch wrappers of the lbibcell_b200 device kernels.
+#pragma once
+
+#include "lbib_internal.cuh"
+
+namespace lbib {
+
+// Membrane state on the device (nodes in ascending id order).
+struct MembraneDev {
+    int M;          // membrane nodes
+    int C;          // connections
+    double* x; double* y;       // LagrangianPoint::position_
+    double* ox; double* oy;     // GeometryNode::oldPosition_
+    double* vx; double* vy;     // LagrangianPoint::velocity_
+    double* fx; double* fy;     // GeometryNode::force_
+    uint32_t* id;
+    int* prev; int* next;       // ring neighbours (node indices)
+    int* ca; int* cb;           // connection endpoints (node indices), vector order
+    uint32_t* cdom;             // connection domain ids
+    // force records (CSR by node, insertion order)
+    int* foff;                  // M+1
+    int* ftype; int* fpartner;  // records
+    double* fpar;               // 4 parameters per record
+    // rings for the area computation (GeometryHandler::computeAreas order)
+    int nCells;
+    int* ringStart;             // nCells+1
+    int* ringNode;              // node indices, ring order
+    uint32_t* ringDom;          // domain of each ring
+};
+
+// Crossing resolution buffers (dense per lattice node and slot E,N,W,S).
+struct CrossDev {
+    unsigned long long* bnDist;  // 4*L, EMPTY = ~0ull
+    uint32_t* bnConn;            // 4*L, ~0u
+    uint32_t* bnDom;             // 4*L
+    uint32_t* wDom;              // L, W-slot winner domain + 1 (0: none)
+    uint32_t* touched;           // capacity: node*4+slot keys written this step
+    int touchedCap;
+    uint32_t* changedNode;       // capacity: nodes whose domain changes
+    uint32_t* changedDom;
+    int changedCap;
+    int* perturbList;            // membrane node indices flagged for the host RNG
+    int perturbCap;
+};
+
+// Tiles for force spreading.
+struct TileDev {
+    int tilesX, tilesY, nTiles;
+    int* count;     // nTiles
+    int* fill;      // nTiles
+    int* start;     // nTiles + 1
+    int* list;      // capacity entries
+    int cap;
+    void* scanTmp;  // CUB temporary storage
+    size_t scanTmpBytes;
+};
+
+void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s);
+void launch_outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
+void launch_init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+                   const SpeciesConst* sp, const double* init, cudaStream_t s);
+
+void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s);
+void launch_outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
+void launch_init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+                   const SpeciesConst* sp, const double* init, cudaStream_t s);
+
+// Membrane pipeline.  `Real` is the lattice precision (velocity / force planes).
+template <typename Real>
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
+template <typename Real>
+void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
+                   unsigned iteration, cudaStream_t s);
+template <typename Real>
+void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
+                        unsigned iteration, cudaStream_t s);
+void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
+template <typename Real>
+void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, int nx, int ny, size_t L, Status* st,
+                      unsigned iteration, cudaStream_t s);
+template <typename Real>
+void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int S, const SpeciesConst* sp,
+                   const double* srcTab, int nDomains, const uint32_t* ctypeTab, int cellTypesCopied, int nx,
+                   int ny, size_t L, Status* st, unsigned iteration, cudaStream_t s);
+void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
+                        cudaStream_t s);
+void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigned iteration, cudaStream_t s);
+void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s);
+void launch_coarsen_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
+void launch_clear_forces(MembraneDev& m, cudaStream_t s);
+void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s);
+void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
+                           double factor, double strength, double maxsource, const Status* st, cudaStream_t s);
+void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
+
+}  // namespace lbib

@@ -1,0 +1,1463 @@
+// lbib_host.cu — host runtime of lbibcell_b200: loaders for the reference's
+// text formats, the device-resident simulation handle, the staged time step
+// and the C ABI declared in include/lbibcell.h.
+//
+// The time step is a fixed sequence of stage kernels on one stream (the order
+// of SimulationRunner::runSimulation, SimulationRunner.cpp:72-99).  Events that
+// only the host can handle — the reference's random perturbation of
+// positions (two std::mt19937(1) streams, GeometryNode.cpp:153-158 and
+// Connection.cpp:332-337), remeshing, coarsening — are detected on the device,
+// which then sets a halt word: every later stage kernel returns at once, the
+// host reads the status after the batch, applies the event in the reference's
+// order and resumes the step at the stage after the one that halted.  Steps
+// without such events run with no host round trip.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "../../include/lbibcell.h"
+#include "kernels.cuh"
+
+namespace lbib {
+
+void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s);
+
+struct HostFail {
+    int code;
+    std::string msg;
+    long long index;
+};
+
+[[noreturn]] static void fail(int code, const std::string& m, long long index = -1) {
+    throw HostFail{code, m, index};
+}
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) ::lbib::fail(::lbib::ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct HConn {
+    uint32_t id1, id2, dom;
+    std::string desc;
+};
+
+struct HForce {
+    uint32_t type, id1, id2;
+    double p[4];
+};
+
+struct Species {
+    std::string name;
+    SpeciesConst c;
+    double init = 0.0;
+    std::map<uint32_t, double> source;
+};
+
+template <typename T>
+static T* dalloc(size_t n) {
+    T* p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    return p;
+}
+
+struct Handle {
+    // parameters
+    int nx = 0, ny = 0, S = 0;
+    size_t L = 0;
+    int precision = 0;
+    int device = 0;
+    double tauF = 1.0;
+    unsigned iteration = 0, iterations = 0, reportStep = 1;
+    std::vector<Species> sp;
+    bool outlet = false;
+    std::vector<int> bio;  // 1 tension, 2 area regulator
+    double tensionForce = 0.01;
+    unsigned tensionFreq = 10;
+    double areaFactor = 1.2, areaStrength = 0.01, areaMax = 0.004;
+
+    // lattice buffers
+    void* f[2] = {nullptr, nullptr};
+    void* g[2] = {nullptr, nullptr};
+    void* u = nullptr;
+    void* force = nullptr;
+    uint32_t* dom = nullptr;
+    int cur = 0;
+    int nDomains = 1;
+    double* massTab = nullptr;
+    double* srcTab = nullptr;
+    uint32_t* ctypeTab = nullptr;
+    std::vector<uint32_t> ctypeHost;
+    bool cellTypesCopied = false;
+
+    // membrane (host mirror of the topology; positions live on the device)
+    std::vector<uint32_t> ids;
+    std::vector<HConn> conns;
+    std::map<uint32_t, std::vector<HForce>> forcemap;
+    bool forcesPure = true;  // device force list = tension pairs from the last renewal (or empty)
+    MembraneDev m{};
+    int Mcap = 0, Ccap = 0, Fcap = 0, cellCap = 0;
+    int* outPos = nullptr;
+    int* inPos = nullptr;
+    double* area = nullptr;
+    double* target = nullptr;
+    std::vector<double> targetHost;  // per cell, survives ring rebuilds
+    std::vector<uint32_t> ringDomHost;
+
+    TileDev tiles{};
+    CrossDev cross{};
+    Status* st = nullptr;
+    Status* stHost = nullptr;
+    cudaStream_t stream = nullptr;
+
+    std::mt19937 genNode{1};
+    std::mt19937 genConn{1};
+    std::uniform_real_distribution<> dis{-kPERTURBATION, kPERTURBATION};
+
+    long long hostEvents = 0;
+    long long launches = 0;  // kernels launched by the last lbib_step / lbib_lattice_step
+    long long stepsDone = 0;
+
+    // errors
+    int err = 0;
+    std::string msg;
+    long long errIndex = -1;
+
+    // timing
+    bool profiling = false;
+    cudaEvent_t evA = nullptr, evB = nullptr;
+    std::vector<cudaEvent_t> kEvents;
+    double lastTotalMs = 0, lastCollideMs = 0;
+    long long lastCollideLaunches = 0;
+
+    ~Handle();
+};
+
+Handle::~Handle() {
+    cudaSetDevice(device);
+    auto fr = [](void* p) { if (p) cudaFree(p); };
+    for (int i = 0; i < 2; ++i) { fr(f[i]); fr(g[i]); }
+    fr(u); fr(force); fr(dom); fr(massTab); fr(srcTab); fr(ctypeTab);
+    fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id);
+    fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
+    fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
+    fr(outPos); fr(inPos); fr(area); fr(target);
+    fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
+    fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.touched);
+    fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
+    fr(st);
+    if (stHost) cudaFreeHost(stHost);
+    if (evA) cudaEventDestroy(evA);
+    if (evB) cudaEventDestroy(evB);
+    for (auto e : kEvents) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// ---------------------------------------------------------------------------
+// Loaders for the reference formats.
+
+// GlobalSimulationParameters::loadGlobalSimulationParameters (GlobalSimulationParameters.cpp:34-72).
+// Species are kept in the parameter map's (alphabetical) order.
+static void load_parameters(Handle& h, const std::string& fn) {
+    std::ifstream in(fn);
+    if (!in.is_open()) fail(ERR_INPUT, "Cannot find the parameter file.");
+    std::string line;
+    std::map<std::string, double> cdes;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::stringstream ls(line);
+        std::string key;
+        ls >> key;
+        if (key == "CurrentIterations:") ls >> h.iteration;
+        else if (key == "Iterations:") ls >> h.iterations;
+        else if (key == "ReportStep:") ls >> h.reportStep;
+        else if (key == "SizeX:") ls >> h.nx;
+        else if (key == "SizeY:") ls >> h.ny;
+        else if (key == "tauFluid:") ls >> h.tauF;
+        else if (key == "CDESolvers:") {
+            std::string nm; double tau;
+            while (ls >> nm >> tau) cdes[nm] = tau;
+        } else fail(ERR_INPUT, "An unknown parameter was passed in the global Parameter file");
+    }
+    for (auto& kv : cdes) {
+        Species s;
+        s.name = kv.first;
+        s.c.tau = kv.second;
+        s.c.decay = 0.0;
+        if (kv.first == "CDESolverD2Q5") s.c.kind = RX_NONE;
+        else if (kv.first == "tutorial_01_CDESolverD2Q5_SIGNAL") s.c.kind = RX_SIGNAL;
+        else s.c.kind = RX_LINEAR;
+        h.sp.push_back(s);
+    }
+    h.S = (int)h.sp.size();
+    if (h.S > kMaxSpecies) fail(ERR_INPUT, "at most 3 CDE species are supported");
+    if (h.nx < 8 || h.ny < 8) fail(ERR_INPUT, "lattice too small");
+}
+
+static void load_plugins(Handle& h, const std::string& fn) {
+    if (fn.empty()) return;
+    std::ifstream in(fn);
+    if (!in.is_open()) fail(ERR_INPUT, "Cannot find the plugin file.");
+    std::string line;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::stringstream ls(line);
+        std::string kind, name;
+        ls >> kind >> name;
+        std::map<std::string, double> kv;
+        if (kind == "MassSolver") {
+            if (name == "MassSolverBoxOutlet") h.outlet = true;
+            else fail(ERR_INPUT, "unknown mass solver " + name);
+        } else if (kind == "BioSolver") {
+            std::string k; double v;
+            while (ls >> k >> v) kv[k] = v;
+            if (name == "LbibMembraneTension") {
+                h.bio.push_back(1);
+                if (kv.count("force")) h.tensionForce = kv["force"];
+                if (kv.count("frequency")) h.tensionFreq = (unsigned)kv["frequency"];
+                if (h.tensionFreq == 0) fail(ERR_INPUT, "tension frequency must be positive");
+            } else if (name == "LbibAreaRegulator") {
+                h.bio.push_back(2);
+                if (kv.count("factor")) h.areaFactor = kv["factor"];
+                if (kv.count("strength")) h.areaStrength = kv["strength"];
+                if (kv.count("maxsource")) h.areaMax = kv["maxsource"];
+            } else fail(ERR_INPUT, "unknown bio solver " + name);
+        } else if (kind == "CDE") {
+            std::string k; double v;
+            while (ls >> k >> v) kv[k] = v;
+            for (auto& s : h.sp)
+                if (s.name == name) {
+                    if (kv.count("init")) s.init = kv["init"];
+                    if (kv.count("decay")) s.c.decay = kv["decay"];
+                }
+        } else if (kind == "CDESource") {
+            uint32_t d; double r;
+            while (ls >> d >> r)
+                for (auto& s : h.sp)
+                    if (s.name == name) s.source[d] = r;
+        } else fail(ERR_INPUT, "unknown plugin line " + kind);
+    }
+}
+
+// ForceSolver::addForce text format (ForceSolver.cpp:107-139; ForceStructs.hpp).
+static void add_force_line(Handle& h, const std::string& line) {
+    std::stringstream ls(line);
+    HForce f{};
+    ls >> f.type;
+    switch (f.type) {
+        case 0: case 7: ls >> f.id1 >> f.id2 >> f.p[0] >> f.p[1]; break;
+        case 1: ls >> f.id1 >> f.p[0] >> f.p[1] >> f.p[2] >> f.p[3]; break;
+        case 2: ls >> f.id1 >> f.p[0] >> f.p[1]; break;
+        case 3: case 4: ls >> f.id1 >> f.p[0] >> f.p[1] >> f.p[2]; break;
+        case 5: case 6: ls >> f.id1 >> f.id2 >> f.p[0]; break;
+        default: fail(ERR_INPUT, "Invalid force solver type found.");
+    }
+    h.forcemap[f.id1].push_back(f);
+}
+
+// ---------------------------------------------------------------------------
+// Host copies of the membrane arrays (used by the host-side events).
+
+struct HostMembrane {
+    std::vector<double> x, y, ox, oy, vx, vy, fx, fy;
+};
+
+static void download_membrane(Handle& h, HostMembrane& hm) {
+    const int M = h.m.M;
+    hm.x.resize(M); hm.y.resize(M); hm.ox.resize(M); hm.oy.resize(M);
+    hm.vx.resize(M); hm.vy.resize(M); hm.fx.resize(M); hm.fy.resize(M);
+    if (M == 0) return;
+    const size_t b = sizeof(double) * M;
+    CK(cudaMemcpyAsync(hm.x.data(), h.m.x, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.y.data(), h.m.y, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.ox.data(), h.m.ox, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.oy.data(), h.m.oy, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.vx.data(), h.m.vx, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.vy.data(), h.m.vy, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.fx.data(), h.m.fx, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.fy.data(), h.m.fy, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+static void ensure_capacity(Handle& h, int M, int C, int F, int cells);
+
+// Uploads node arrays, connections, ring order, neighbour indices and the
+// force records, after any change of the host topology mirror.
+static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces) {
+    const int M = (int)h.ids.size();
+    const int C = (int)h.conns.size();
+    std::map<uint32_t, int> index;
+    for (int i = 0; i < M; ++i) index[h.ids[i]] = i;
+    std::vector<int> ca(C), cb(C), prev(M, -1), next(M, -1);
+    std::vector<uint32_t> cdom(C);
+    for (int c = 0; c < C; ++c) {
+        ca[c] = index.at(h.conns[c].id1);
+        cb[c] = index.at(h.conns[c].id2);
+        cdom[c] = h.conns[c].dom;
+        next[ca[c]] = cb[c];
+        prev[cb[c]] = ca[c];
+    }
+    for (int i = 0; i < M; ++i)
+        if (prev[i] < 0 || next[i] < 0) fail(ERR_INPUT, "Geometry::checkGeometryIntegrity: open membrane", i);
+    // rings: GeometryHandler::computeAreas (GeometryHandler.cpp:112-126):
+    // per domain (ascending), start at the first connection with that domain
+    // and follow the second node's outgoing connection.
+    std::map<uint32_t, int> first;
+    for (int c = 0; c < C; ++c)
+        if (!first.count(cdom[c])) first[cdom[c]] = c;
+    std::vector<int> outConn(M, -1);
+    for (int c = 0; c < C; ++c) outConn[ca[c]] = c;
+    std::vector<int> ringStart, ringNode;
+    std::vector<uint32_t> ringDom;
+    for (auto& kv : first) {
+        ringStart.push_back((int)ringNode.size());
+        ringDom.push_back(kv.first);
+        int c = kv.second;
+        int guard = 0;
+        do {
+            ringNode.push_back(cb[c]);
+            c = outConn[cb[c]];
+            if (++guard > C) fail(ERR_INPUT, "broken ring", kv.first);
+        } while (c != kv.second);
+    }
+    ringStart.push_back((int)ringNode.size());
+    const int cells = (int)ringDom.size();
+    // force records
+    std::vector<int> foff(M + 1, 0), ftype, fpart;
+    std::vector<double> fpar;
+    if (uploadForces) {
+        for (int i = 0; i < M; ++i) {
+            foff[i] = (int)ftype.size();
+            auto it = h.forcemap.find(h.ids[i]);
+            if (it == h.forcemap.end()) continue;
+            for (const HForce& f : it->second) {
+                ftype.push_back((int)f.type);
+                int j = -1;
+                if (f.type == 0 || f.type == 7 || f.type == 5 || f.type == 6) {
+                    auto jt = index.find(f.id2);
+                    j = jt == index.end() ? -1 : jt->second;
+                }
+                fpart.push_back(j);
+                for (int q = 0; q < 4; ++q) fpar.push_back(f.p[q]);
+            }
+        }
+        foff[M] = (int)ftype.size();
+        // forces on ids that are not membrane nodes fail like nodes.at() would
+        for (auto& kv : h.forcemap)
+            if (!kv.second.empty() && !index.count(kv.first)) fail(ERR_FORCE_NODE, "Could not compute and set the forces.", kv.first);
+    }
+    const int F = std::max((int)ftype.size(), 2 * M);
+    ensure_capacity(h, M, C, F, cells);
+    h.m.M = M;
+    h.m.C = C;
+    h.m.nCells = cells;
+    const size_t bd = sizeof(double) * M;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h.stream));
+    };
+    up(h.m.x, hm.x.data(), bd); up(h.m.y, hm.y.data(), bd);
+    up(h.m.ox, hm.ox.data(), bd); up(h.m.oy, hm.oy.data(), bd);
+    up(h.m.vx, hm.vx.data(), bd); up(h.m.vy, hm.vy.data(), bd);
+    up(h.m.fx, hm.fx.data(), bd); up(h.m.fy, hm.fy.data(), bd);
+    up(h.m.id, h.ids.data(), sizeof(uint32_t) * M);
+    up(h.m.prev, prev.data(), sizeof(int) * M);
+    up(h.m.next, next.data(), sizeof(int) * M);
+    up(h.m.ca, ca.data(), sizeof(int) * C);
+    up(h.m.cb, cb.data(), sizeof(int) * C);
+    up(h.m.cdom, cdom.data(), sizeof(uint32_t) * C);
+    up(h.m.ringStart, ringStart.data(), sizeof(int) * ringStart.size());
+    up(h.m.ringNode, ringNode.data(), sizeof(int) * ringNode.size());
+    up(h.m.ringDom, ringDom.data(), sizeof(uint32_t) * cells);
+    if (uploadForces) {
+        up(h.m.foff, foff.data(), sizeof(int) * (M + 1));
+        up(h.m.ftype, ftype.data(), sizeof(int) * ftype.size());
+        up(h.m.fpartner, fpart.data(), sizeof(int) * fpart.size());
+        up(h.m.fpar, fpar.data(), sizeof(double) * fpar.size());
+    }
+    // per-cell area targets follow their domain across ring rebuilds
+    std::map<uint32_t, double> tgt;
+    for (size_t c = 0; c < h.ringDomHost.size(); ++c) tgt[h.ringDomHost[c]] = h.targetHost[c];
+    std::vector<double> tnew(cells);
+    for (int c = 0; c < cells; ++c) tnew[c] = tgt.count(ringDom[c]) ? tgt[ringDom[c]] : NAN;
+    h.ringDomHost = ringDom;
+    h.targetHost = tnew;
+    up(h.target, tnew.data(), sizeof(double) * cells);
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+// Copies the device's area targets to the host mirror (they are set on the
+// device by the first area-regulator call).
+static void sync_targets(Handle& h) {
+    if (h.m.nCells == 0) return;
+    h.targetHost.resize(h.m.nCells);
+    CK(cudaMemcpyAsync(h.targetHost.data(), h.target, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
+    auto grow = [&](int need, int& cap) { if (need <= cap) return false; cap = std::max(need + need / 2, 64); return true; };
+    int oldM = h.Mcap;
+    if (grow(M, h.Mcap)) {
+        // membrane arrays are rewritten by every upload_topology; no copy needed
+        auto fr = [](void* p) { if (p) cudaFree(p); };
+        fr(h.m.x); fr(h.m.y); fr(h.m.ox); fr(h.m.oy); fr(h.m.vx); fr(h.m.vy); fr(h.m.fx); fr(h.m.fy);
+        fr(h.m.id); fr(h.m.prev); fr(h.m.next); fr(h.outPos); fr(h.inPos); fr(h.cross.perturbList);
+        fr(h.m.foff); fr(h.m.ringNode); fr(h.tiles.list);
+        const int n = h.Mcap;
+        h.m.x = dalloc<double>(n); h.m.y = dalloc<double>(n); h.m.ox = dalloc<double>(n); h.m.oy = dalloc<double>(n);
+        h.m.vx = dalloc<double>(n); h.m.vy = dalloc<double>(n); h.m.fx = dalloc<double>(n); h.m.fy = dalloc<double>(n);
+        h.m.id = dalloc<uint32_t>(n); h.m.prev = dalloc<int>(n); h.m.next = dalloc<int>(n);
+        h.outPos = dalloc<int>(n); h.inPos = dalloc<int>(n);
+        h.cross.perturbList = dalloc<int>(n); h.cross.perturbCap = n;
+        h.m.foff = dalloc<int>(n + 1);
+        h.m.ringNode = dalloc<int>(n);
+        h.tiles.cap = 4 * n;
+        h.tiles.list = dalloc<int>(h.tiles.cap);
+        // the force records survive a growth only when the force list is rebuilt
+        if (oldM > 0 && h.forcesPure) {
+            // re-create the empty/pure state: offsets are re-filled by the caller
+        }
+    }
+    if (grow(C, h.Ccap)) {
+        auto fr = [](void* p) { if (p) cudaFree(p); };
+        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.cross.touched); fr(h.cross.changedNode); fr(h.cross.changedDom);
+        const int n = h.Ccap;
+        h.m.ca = dalloc<int>(n); h.m.cb = dalloc<int>(n); h.m.cdom = dalloc<uint32_t>(n);
+        // each connection of length <= MAXLENGTH crosses at most one line per axis
+        // (two records each); longer ones exist only between the move and the remesh
+        h.cross.touchedCap = 16 * n + 1024;
+        h.cross.touched = dalloc<uint32_t>(h.cross.touchedCap);
+        h.cross.changedCap = 8 * n + 1024;
+        h.cross.changedNode = dalloc<uint32_t>(h.cross.changedCap);
+        h.cross.changedDom = dalloc<uint32_t>(h.cross.changedCap);
+    }
+    if (grow(F, h.Fcap)) {
+        auto fr = [](void* p) { if (p) cudaFree(p); };
+        fr(h.m.ftype); fr(h.m.fpartner); fr(h.m.fpar);
+        h.m.ftype = dalloc<int>(h.Fcap); h.m.fpartner = dalloc<int>(h.Fcap); h.m.fpar = dalloc<double>(4 * (size_t)h.Fcap);
+    }
+    if (grow(cells, h.cellCap)) {
+        auto fr = [](void* p) { if (p) cudaFree(p); };
+        fr(h.m.ringStart); fr(h.m.ringDom); fr(h.area); fr(h.target);
+        h.m.ringStart = dalloc<int>(h.cellCap + 1); h.m.ringDom = dalloc<uint32_t>(h.cellCap);
+        h.area = dalloc<double>(h.cellCap); h.target = dalloc<double>(h.cellCap);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side events, in the reference's order.
+
+// GeometryNode::perturbatePosition (GeometryNode.cpp:153-214).  The two draws
+// of one setPos(x + dis(gen), y + dis(gen)) are taken y-first: g++ evaluates
+// those arguments right to left, which is what the reference build does.
+static void perturbate(Handle& h, double& x, double& y) {
+    double r;
+    if (std::abs(static_cast<int>(x) - x) <= kEPSILON) {
+        r = 0.0;
+        while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genNode);
+        x = x + r;
+    }
+    if (std::abs(static_cast<int>(y) - y) <= kEPSILON) {
+        r = 0.0;
+        while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genNode);
+        y = y + r;
+    }
+    if (std::abs(y - std::floor(y) - (x - std::floor(x))) <= kEPSILON) {
+        const double ry = h.dis(h.genNode);
+        const double rx = h.dis(h.genNode);
+        x = x + rx; y = y + ry;
+    }
+    if (std::abs(std::ceil(y) - y - (x - std::floor(x))) <= kEPSILON) {
+        const double ry = h.dis(h.genNode);
+        const double rx = h.dis(h.genNode);
+        x = x + rx; y = y + ry;
+    }
+}
+
+// GeometryHandler::perturbConnections + Connection::perturbConnection
+// (GeometryHandler.cpp:326-356, Connection.cpp:332-387) on the host copy.
+static void perturb_connections(Handle& h, HostMembrane& hm) {
+    std::map<uint32_t, int> index;
+    for (size_t i = 0; i < h.ids.size(); ++i) index[h.ids[i]] = (int)i;
+    std::map<uint32_t, int> first;
+    for (size_t c = 0; c < h.conns.size(); ++c)
+        if (!first.count(h.conns[c].dom)) first[h.conns[c].dom] = (int)c;
+    std::vector<int> outConn(h.ids.size(), -1);
+    for (size_t c = 0; c < h.conns.size(); ++c) outConn[index.at(h.conns[c].id1)] = (int)c;
+    for (auto& kv : first) {
+        int c = kv.second;
+        do {
+            const int a = index.at(h.conns[c].id1), b = index.at(h.conns[c].id2);
+            double r;
+            if (std::abs(hm.x[a] - hm.x[b]) < kEPSILON) {
+                r = 0.0;
+                while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genConn);
+                hm.x[a] = hm.x[a] + r;
+                perturbate(h, hm.x[a], hm.y[a]);
+            }
+            if (std::abs(hm.y[a] - hm.y[b]) < kEPSILON) {
+                r = 0.0;
+                while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genConn);
+                hm.y[a] = hm.y[a] + r;
+                perturbate(h, hm.x[a], hm.y[a]);
+            }
+            c = outConn[b];
+        } while (c != kv.second);
+    }
+}
+
+// GeometryHandler::remeshBoundary loop (GeometryHandler.cpp:385-431,
+// SimulationRunner.cpp:190-199) with Geometry::addGeometryNode /
+// eraseConnection / addConnection (Geometry.cpp:382-452).  One pass visits
+// the connections present at its start, in vector order; each long one gets a
+// new node at its midpoint (next id, perturbed on creation) and is replaced by
+// two connections appended at the end of the vector.
+static bool remesh(Handle& h, HostMembrane& hm) {
+    bool any = false;
+    for (;;) {
+        std::map<uint32_t, int> index;
+        for (size_t i = 0; i < h.ids.size(); ++i) index[h.ids[i]] = (int)i;
+        std::vector<HConn> kept, added;
+        kept.reserve(h.conns.size());
+        for (const HConn& c : h.conns) {
+            const int a = index.at(c.id1), b = index.at(c.id2);
+            const double len = std::sqrt((hm.x[a] - hm.x[b]) * (hm.x[a] - hm.x[b]) +
+                                         (hm.y[a] - hm.y[b]) * (hm.y[a] - hm.y[b]));
+            if (len > kMAXLENGTH) {
+                const uint32_t nid = h.ids.back() + 1;
+                double nx = (hm.x[a] + hm.x[b]) / 2, ny = (hm.y[a] + hm.y[b]) / 2;
+                const double ox = nx - 5.0, oy = ny - 5.0;
+                perturbate(h, nx, ny);
+                h.ids.push_back(nid);
+                hm.x.push_back(nx); hm.y.push_back(ny);
+                hm.ox.push_back(ox); hm.oy.push_back(oy);
+                hm.vx.push_back(0.0); hm.vy.push_back(0.0);
+                hm.fx.push_back(0.0); hm.fy.push_back(0.0);
+                added.push_back(HConn{c.id1, nid, c.dom, c.desc});
+                added.push_back(HConn{nid, c.id2, c.dom, c.desc});
+            } else {
+                kept.push_back(c);
+            }
+        }
+        if (added.empty()) break;
+        kept.insert(kept.end(), added.begin(), added.end());
+        h.conns.swap(kept);
+        any = true;
+    }
+    return any;
+}
+
+// GeometryHandler::coarsenBoundary + Geometry::removeGeometryNode
+// (GeometryHandler.cpp:433-461, Geometry.cpp:402-431): nodes in id order; a
+// node whose neighbours are closer than MAXLENGTH is removed, its two
+// connections are erased and one from its predecessor to its successor is
+// appended.  Connections are kept in an append-only list with liveness flags
+// and per-node incoming/outgoing indices, compacted at the end.
+static bool coarsen(Handle& h, HostMembrane& hm) {
+    std::vector<HConn> list = h.conns;
+    std::vector<char> alive(list.size(), 1);
+    std::map<uint32_t, int> inC, outC, pos;
+    for (size_t c = 0; c < list.size(); ++c) {
+        outC[list[c].id1] = (int)c;
+        inC[list[c].id2] = (int)c;
+    }
+    for (size_t i = 0; i < h.ids.size(); ++i) pos[h.ids[i]] = (int)i;
+    std::vector<char> removed(h.ids.size(), 0);
+    bool any = false;
+    for (size_t i = 0; i < h.ids.size(); ++i) {
+        const uint32_t id = h.ids[i];
+        auto ii = inC.find(id), oo = outC.find(id);
+        if (ii == inC.end() || oo == outC.end()) fail(ERR_INPUT, "Geometry::removeGeometryNode: open membrane", id);
+        const int cin = ii->second, cout = oo->second;
+        const uint32_t n1 = list[cin].id1, n2 = list[cout].id2;
+        const int p1 = pos.at(n1), p2 = pos.at(n2);
+        const double length = std::sqrt((hm.x[p2] - hm.x[p1]) * (hm.x[p2] - hm.x[p1]) +
+                                        (hm.y[p2] - hm.y[p1]) * (hm.y[p2] - hm.y[p1]));
+        if (length < kMAXLENGTH) {
+            alive[cin] = 0;
+            alive[cout] = 0;
+            list.push_back(HConn{n1, n2, list[cin].dom, list[cin].desc});
+            alive.push_back(1);
+            outC[n1] = (int)list.size() - 1;
+            inC[n2] = (int)list.size() - 1;
+            inC.erase(id);
+            outC.erase(id);
+            removed[i] = 1;
+            any = true;
+        }
+    }
+    if (!any) return false;
+    std::vector<HConn> conns;
+    for (size_t c = 0; c < list.size(); ++c)
+        if (alive[c]) conns.push_back(list[c]);
+    h.conns.swap(conns);
+    size_t w = 0;
+    for (size_t i = 0; i < h.ids.size(); ++i) {
+        if (removed[i]) continue;
+        h.ids[w] = h.ids[i];
+        hm.x[w] = hm.x[i]; hm.y[w] = hm.y[i]; hm.ox[w] = hm.ox[i]; hm.oy[w] = hm.oy[i];
+        hm.vx[w] = hm.vx[i]; hm.vy[w] = hm.vy[i]; hm.fx[w] = hm.fx[i]; hm.fy[w] = hm.fy[i];
+        ++w;
+    }
+    h.ids.resize(w);
+    hm.x.resize(w); hm.y.resize(w); hm.ox.resize(w); hm.oy.resize(w);
+    hm.vx.resize(w); hm.vy.resize(w); hm.fx.resize(w); hm.fy.resize(w);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Stage launcher
+
+template <typename Real>
+static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity) {
+    LatticeArgs<Real> a{};
+    a.nx = h.nx; a.ny = h.ny; a.L = h.L; a.S = h.S;
+    a.fin = (const Real*)h.f[parity];
+    a.fout = (Real*)h.f[1 - parity];
+    a.gin = (const Real*)h.g[parity];
+    a.gout = (Real*)h.g[1 - parity];
+    a.u = (Real*)h.u;
+    a.force = (const Real*)h.force;
+    a.tileCount = h.tiles.count;
+    a.tilesX = h.tiles.tilesX;
+    a.dom = h.dom;
+    bool area = false;
+    for (int b : h.bio) area |= (b == 2);
+    a.massTab = area ? h.massTab : nullptr;
+    a.nDomains = h.nDomains;
+    a.srcTab = h.srcTab;
+    a.tauF = h.tauF;
+    for (int k = 0; k < h.S; ++k) a.sp[k] = h.sp[k].c;
+    a.iteration = iteration;
+    a.status = h.st;
+    return a;
+}
+
+__global__ void step_begin_kernel(Status* st) {
+    if (st->halt) return;
+    st->nPerturbNode = 0;
+    st->nPerturbConn = 0;
+    st->nChanged = 0;
+    st->nRecords = 0;
+    st->remesh = 0;
+    st->coarsen = 0;
+}
+
+__global__ void step_end_kernel(Status* st) {
+    if (st->halt) return;
+    st->pad[0] += 1;  // steps completed in this batch
+}
+
+template <typename Real>
+static void launch_stages(Handle& h, unsigned iteration, int parity, int fromStage, bool firstStepOfRun,
+                          cudaEvent_t evCollideA, cudaEvent_t evCollideB) {
+    cudaStream_t s = h.stream;
+    Real* fcur = (Real*)h.f[1 - parity];
+    Real* gcur = (Real*)h.g[1 - parity];
+    const bool hasM = h.m.M > 0;
+    long long& k = h.launches;
+    if (fromStage <= ST_FORCE) {
+        step_begin_kernel<<<1, 1, 0, s>>>(h.st);
+        launch_force_eval<Real>(h.m, h.st, iteration, s);
+        k += 1 + hasM;
+    }
+    if (fromStage <= ST_SPREAD) {
+        launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, iteration, s);
+        k += hasM ? 5 : 0;
+    }
+    if (fromStage <= ST_COLLIDE) {
+        if (evCollideA) cudaEventRecord(evCollideA, s);
+        if (sizeof(Real) == 8) {
+            const LatticeArgs<double> a = lattice_args<double>(h, iteration, parity);
+            launch_stream_collide64(a, s);
+        } else {
+            const LatticeArgs<float> a = lattice_args<float>(h, iteration, parity);
+            launch_stream_collide32(a, s);
+        }
+        if (evCollideB) cudaEventRecord(evCollideB, s);
+        k += 1;
+    }
+    if (fromStage <= ST_INTERP_MOVE) {
+        launch_interp_move<Real>(h.m, (const Real*)h.u, h.nx, h.ny, h.L, h.cross, h.st, iteration, s);
+        k += hasM;
+    }
+    if (fromStage <= ST_PERTURB_CONN) {
+        launch_perturb_conn_check(h.m, h.st, iteration, s);
+        k += hasM;
+    }
+    if (fromStage <= ST_CROSSINGS) {
+        launch_crossings<Real>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
+        k += hasM ? 4 : 0;
+    }
+    if (fromStage <= ST_REINIT) {
+        SpeciesConst spc[kMaxSpecies] = {};
+        for (int k = 0; k < h.S; ++k) spc[k] = h.sp[k].c;
+        const int copied = (h.cellTypesCopied || !firstStepOfRun) ? 1 : 0;
+        launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, copied,
+                            h.nx, h.ny, h.L, h.st, iteration, s);
+        k += 1;
+    }
+    if (fromStage <= ST_DOMAIN) {
+        launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
+        launch_cross_clear(h.cross, h.st, s);
+        k += 2;
+    }
+    if (fromStage <= ST_REMESH) {
+        launch_remesh_check(h.st, iteration, s);
+        k += 1;
+    }
+    if (fromStage <= ST_COARSEN && iteration % 10 == 0) {
+        launch_clear_forces(h.m, s);
+        launch_coarsen_check(h.m, h.st, iteration, s);
+        k += 1 + hasM;
+    }
+    if (fromStage <= ST_OUTLET && h.outlet) {
+        if (sizeof(Real) == 8) launch_outlet64((double*)fcur, (double*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
+        else launch_outlet32((float*)fcur, (float*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
+        k += 1;
+    }
+    if (fromStage <= ST_BIO) {
+        for (int b : h.bio) {
+            if (b == 2) {
+                launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor, h.areaStrength,
+                                      h.areaMax, h.st, s);
+                k += h.m.nCells > 0 ? 2 : 0;
+            } else if (b == 1 && iteration % h.tensionFreq == 0) {
+                launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
+                k += hasM ? 2 : 0;
+            }
+        }
+    }
+    step_end_kernel<<<1, 1, 0, s>>>(h.st);
+    k += 1;
+}
+
+// The stage the host resumes at after handling the halt of `stage`.
+static int resume_stage(int stage) {
+    switch (stage) {
+        case ST_INTERP_MOVE: return ST_PERTURB_CONN;
+        case ST_PERTURB_CONN: return ST_CROSSINGS;
+        case ST_REMESH: return ST_COARSEN;
+        case ST_COARSEN: return ST_OUTLET;
+        default: return -1;
+    }
+}
+
+static void read_status(Handle& h) {
+    CK(cudaMemcpyAsync(h.stHost, h.st, sizeof(Status), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+static void write_status(Handle& h) {
+    CK(cudaMemcpyAsync(h.st, h.stHost, sizeof(Status), cudaMemcpyHostToDevice, h.stream));
+}
+
+// Bookkeeping the host does for a step it launches (the force list's state).
+static void host_step_bookkeeping(Handle& h, unsigned iteration) {
+    if (iteration % 10 == 0) {
+        h.forcemap.clear();
+        h.forcesPure = true;
+    }
+    for (int b : h.bio)
+        if (b == 1 && iteration % h.tensionFreq == 0 && !h.forcesPure)
+            fail(ERR_STATE, "tension renewal on a non-tension force list is not supported on the device");
+}
+
+template <typename Real>
+static void run_steps(Handle& h, int n) {
+    const int kBatch = 64;
+    int fromStage = ST_FORCE;
+    while (n > 0) {
+        const int B = std::min(n, kBatch);
+        std::memset(h.stHost, 0, sizeof(Status));
+        write_status(h);
+        const bool prof = h.profiling;
+        while ((int)h.kEvents.size() < 2 * B) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            h.kEvents.push_back(e);
+        }
+        for (int b = 0; b < B; ++b) {
+            const unsigned it = h.iteration + b;
+            host_step_bookkeeping(h, it);
+            const int parity = (h.cur + b) & 1;
+            const bool first = (h.stepsDone + b) == 0;
+            launch_stages<Real>(h, it, parity, b == 0 ? fromStage : ST_FORCE, first,
+                                prof && (b > 0 || fromStage <= ST_COLLIDE) ? h.kEvents[2 * b] : nullptr,
+                                prof && (b > 0 || fromStage <= ST_COLLIDE) ? h.kEvents[2 * b + 1] : nullptr);
+        }
+        CK(cudaGetLastError());
+        read_status(h);
+        Status& st = *h.stHost;
+        const int done = st.pad[0];
+        if (prof) {
+            for (int b = 0; b < std::min(done, B); ++b) {
+                if (b == 0 && fromStage > ST_COLLIDE) continue;
+                float ms = 0;
+                if (cudaEventElapsedTime(&ms, h.kEvents[2 * b], h.kEvents[2 * b + 1]) == cudaSuccess) {
+                    h.lastCollideMs += ms;
+                    h.lastCollideLaunches += 1;
+                }
+            }
+        }
+        if (!st.halt) {
+            h.cur = (h.cur + B) & 1;
+            h.iteration += B;
+            h.stepsDone += B;
+            h.cellTypesCopied = true;
+            n -= B;
+            fromStage = ST_FORCE;
+            continue;
+        }
+        // steps before the halted one completed; the halted step ran up to st.haltStage
+        h.cur = (h.cur + done) & 1;
+        h.iteration += done;
+        h.stepsDone += done;
+        n -= done;
+        if (done > 0) h.cellTypesCopied = true;
+        if (st.err) {
+            h.err = st.err;
+            h.errIndex = st.errIndex;
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "device error %d at stage %d, iteration %u", st.err, st.haltStage, h.iteration);
+            h.msg = buf;
+            fail(st.err, h.msg, st.errIndex);
+        }
+        const int stage = st.haltStage;
+        const unsigned it = h.iteration;
+        const int parity = h.cur;
+        h.hostEvents++;
+        HostMembrane hm;
+        if (stage == ST_INTERP_MOVE) {
+            // positions that need GeometryNode::perturbatePosition, in id order
+            std::vector<int> list(std::min(st.nPerturbNode, h.cross.perturbCap));
+            if (st.nPerturbNode > h.cross.perturbCap) fail(ERR_CAPACITY, "perturbation list overflow");
+            CK(cudaMemcpyAsync(list.data(), h.cross.perturbList, sizeof(int) * list.size(), cudaMemcpyDeviceToHost, h.stream));
+            download_membrane(h, hm);
+            std::sort(list.begin(), list.end());
+            for (int i : list) perturbate(h, hm.x[i], hm.y[i]);
+            CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
+        } else if (stage == ST_PERTURB_CONN) {
+            download_membrane(h, hm);
+            perturb_connections(h, hm);
+            CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
+        } else if (stage == ST_REMESH) {
+            download_membrane(h, hm);
+            sync_targets(h);
+            const int Mold = (int)h.ids.size();
+            remesh(h, hm);
+            // the force list keeps its records; new nodes have none
+            std::vector<int> foff(Mold + 1);
+            CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (Mold + 1), cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+            const int nrec = foff[Mold];
+            std::vector<int> ftype(nrec), fpart(nrec);
+            std::vector<double> fpar(4 * (size_t)nrec);
+            if (nrec) {
+                CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+                CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+                CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
+                CK(cudaStreamSynchronize(h.stream));
+            }
+            upload_topology(h, hm, false);
+            foff.resize(h.m.M + 1, nrec);
+            CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
+            if (nrec) {
+                CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+                CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+                CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * 4 * nrec, cudaMemcpyHostToDevice, h.stream));
+            }
+            // new nodes are bound to the lattice now (GeometryHandler.cpp:427-428)
+            std::memset(h.stHost, 0, sizeof(Status));
+            write_status(h);
+            launch_edge_check(h.m, h.nx, h.ny, h.st, it, h.stream);
+            read_status(h);
+            if (h.stHost->err) fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
+        } else if (stage == ST_COARSEN) {
+            download_membrane(h, hm);
+            sync_targets(h);
+            coarsen(h, hm);
+            upload_topology(h, hm, true);  // the force list is empty at a coarsening step
+        } else {
+            fail(ERR_STATE, "unexpected halt stage");
+        }
+        // resume the halted step
+        std::memset(h.stHost, 0, sizeof(Status));
+        write_status(h);
+        const int from = resume_stage(stage);
+        const bool first = h.stepsDone == 0;
+        launch_stages<Real>(h, it, parity, from, first, nullptr, nullptr);
+        read_status(h);
+        if (h.stHost->halt) {
+            // a second event in the same step: handle it by looping with this step resumed
+            const int st2 = h.stHost->haltStage;
+            if (h.stHost->err) fail(h.stHost->err, "device error after resume", h.stHost->errIndex);
+            // re-enter the loop at the halted stage of the same step
+            fromStage = -st2;  // marker handled below
+        } else {
+            h.cur = (h.cur + 1) & 1;
+            h.iteration += 1;
+            h.stepsDone += 1;
+            h.cellTypesCopied = true;
+            n -= 1;
+            fromStage = ST_FORCE;
+        }
+        while (fromStage < 0) {
+            // a further halt inside the resumed step
+            const int stage2 = -fromStage;
+            h.hostEvents++;
+            HostMembrane hm2;
+            if (stage2 == ST_PERTURB_CONN) {
+                download_membrane(h, hm2);
+                perturb_connections(h, hm2);
+                CK(cudaMemcpyAsync(h.m.x, hm2.x.data(), sizeof(double) * hm2.x.size(), cudaMemcpyHostToDevice, h.stream));
+                CK(cudaMemcpyAsync(h.m.y, hm2.y.data(), sizeof(double) * hm2.y.size(), cudaMemcpyHostToDevice, h.stream));
+            } else if (stage2 == ST_REMESH || stage2 == ST_COARSEN) {
+                download_membrane(h, hm2);
+                sync_targets(h);
+                if (stage2 == ST_REMESH) {
+                    const int Mold = (int)h.ids.size();
+                    std::vector<int> foff(Mold + 1);
+                    CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (Mold + 1), cudaMemcpyDeviceToHost, h.stream));
+                    CK(cudaStreamSynchronize(h.stream));
+                    const int nrec = foff[Mold];
+                    std::vector<int> ftype(nrec), fpart(nrec);
+                    std::vector<double> fpar(4 * (size_t)nrec);
+                    if (nrec) {
+                        CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+                        CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+                        CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
+                        CK(cudaStreamSynchronize(h.stream));
+                    }
+                    remesh(h, hm2);
+                    upload_topology(h, hm2, false);
+                    foff.resize(h.m.M + 1, nrec);
+                    CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
+                    if (nrec) {
+                        CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+                        CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+                        CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * 4 * nrec, cudaMemcpyHostToDevice, h.stream));
+                    }
+                    std::memset(h.stHost, 0, sizeof(Status));
+                    write_status(h);
+                    launch_edge_check(h.m, h.nx, h.ny, h.st, it, h.stream);
+                    read_status(h);
+                    if (h.stHost->err) fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
+                } else {
+                    coarsen(h, hm2);
+                    upload_topology(h, hm2, true);
+                }
+            } else {
+                fail(ERR_STATE, "unexpected halt stage after resume");
+            }
+            std::memset(h.stHost, 0, sizeof(Status));
+            write_status(h);
+            launch_stages<Real>(h, it, parity, resume_stage(stage2), h.stepsDone == 0, nullptr, nullptr);
+            read_status(h);
+            if (h.stHost->err) fail(h.stHost->err, "device error after resume", h.stHost->errIndex);
+            if (h.stHost->halt) {
+                fromStage = -h.stHost->haltStage;
+            } else {
+                h.cur = (h.cur + 1) & 1;
+                h.iteration += 1;
+                h.stepsDone += 1;
+                h.cellTypesCopied = true;
+                n -= 1;
+                fromStage = ST_FORCE;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Construction
+
+static void cure_lattice(Handle& h, HostMembrane& hm);
+
+static void create(Handle& h, const std::string& params, const std::string& geom, const std::string& forceFile,
+                   const std::string& plugins) {
+    CK(cudaSetDevice(h.device));
+    CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h.evA));
+    CK(cudaEventCreate(&h.evB));
+    load_parameters(h, params);
+    load_plugins(h, plugins);
+    h.L = (size_t)h.nx * h.ny;
+    const size_t rs = h.precision == LBIB_FP64 ? sizeof(double) : sizeof(float);
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaMalloc(&h.f[i], 9 * h.L * rs));
+        CK(cudaMalloc(&h.g[i], std::max(1, h.S) * 5 * h.L * rs));
+    }
+    CK(cudaMalloc(&h.u, 2 * h.L * rs));
+    CK(cudaMalloc(&h.force, 2 * h.L * rs));
+    CK(cudaMemsetAsync(h.force, 0, 2 * h.L * rs, h.stream));
+    h.dom = dalloc<uint32_t>(h.L);
+    CK(cudaMemsetAsync(h.dom, 0, sizeof(uint32_t) * h.L, h.stream));
+    CK(cudaMalloc(&h.st, sizeof(Status)));
+    CK(cudaMallocHost(&h.stHost, sizeof(Status)));
+    std::memset(h.stHost, 0, sizeof(Status));
+    write_status(h);
+
+    // tiles
+    h.tiles.tilesX = (h.nx + kTile - 1) / kTile;
+    h.tiles.tilesY = (h.ny + kTile - 1) / kTile;
+    h.tiles.nTiles = h.tiles.tilesX * h.tiles.tilesY;
+    // count has one extra zero entry: the exclusive scan over nTiles + 1
+    // items yields start[nTiles] = total
+    h.tiles.count = dalloc<int>(h.tiles.nTiles + 1);
+    h.tiles.fill = dalloc<int>(h.tiles.nTiles);
+    h.tiles.start = dalloc<int>(h.tiles.nTiles + 1);
+    CK(cudaMemsetAsync(h.tiles.count, 0, sizeof(int) * (h.tiles.nTiles + 1), h.stream));
+    cub::DeviceScan::ExclusiveSum(nullptr, h.tiles.scanTmpBytes, h.tiles.count, h.tiles.start, h.tiles.nTiles + 1, h.stream);
+    CK(cudaMalloc(&h.tiles.scanTmp, std::max<size_t>(h.tiles.scanTmpBytes, 16)));
+
+    // crossing planes
+    h.cross.bnDist = dalloc<unsigned long long>(4 * h.L);
+    h.cross.bnConn = dalloc<uint32_t>(4 * h.L);
+    h.cross.bnDom = dalloc<uint32_t>(4 * h.L);
+    h.cross.wDom = dalloc<uint32_t>(h.L);
+    CK(cudaMemsetAsync(h.cross.bnDist, 0xff, sizeof(unsigned long long) * 4 * h.L, h.stream));
+    CK(cudaMemsetAsync(h.cross.bnConn, 0xff, sizeof(uint32_t) * 4 * h.L, h.stream));
+    CK(cudaMemsetAsync(h.cross.wDom, 0, sizeof(uint32_t) * h.L, h.stream));
+
+    // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160); each new
+    // GeometryNode runs perturbatePosition (GeometryNode.cpp:98-117).
+    std::ifstream in(geom);
+    if (!in.is_open()) fail(ERR_INPUT, "Cannot find the geometry.txt file.");
+    std::map<uint32_t, std::pair<double, double>> nodes;
+    std::map<uint32_t, uint32_t> ctypes;
+    ctypes[0] = 0;
+    std::string line;
+    bool readingNodes = true;
+    uint32_t maxDom = 0;
+    while (std::getline(in, line)) {
+        if (line.empty()) continue;
+        if (line.find("#Connection") != std::string::npos) readingNodes = false;
+        if (line[0] == '#') continue;
+        std::stringstream ls(line);
+        if (readingNodes) {
+            uint32_t id; double x, y;
+            ls >> id >> x >> y;
+            perturbate(h, x, y);
+            nodes[id] = {x, y};
+        } else {
+            HConn c;
+            ls >> c.id1 >> c.id2 >> c.dom;
+            std::string a, b;
+            while (ls >> a >> b) c.desc += "\t" + a + "\t" + b;
+            ctypes[c.dom] = 1;
+            maxDom = std::max(maxDom, c.dom);
+            h.conns.push_back(c);
+        }
+    }
+    HostMembrane hm;
+    for (auto& kv : nodes) {
+        h.ids.push_back(kv.first);
+        hm.x.push_back(kv.second.first);
+        hm.y.push_back(kv.second.second);
+        hm.ox.push_back(kv.second.first - 5.0);
+        hm.oy.push_back(kv.second.second - 5.0);
+        hm.vx.push_back(0.0); hm.vy.push_back(0.0); hm.fx.push_back(0.0); hm.fy.push_back(0.0);
+    }
+    // tables indexed by domain id
+    for (auto& s : h.sp)
+        for (auto& kv : s.source) maxDom = std::max(maxDom, kv.first);
+    h.nDomains = (int)maxDom + 1;
+    h.massTab = dalloc<double>(h.nDomains);
+    CK(cudaMemsetAsync(h.massTab, 0, sizeof(double) * h.nDomains, h.stream));
+    std::vector<double> src((size_t)std::max(1, h.S) * h.nDomains, 0.0);
+    for (int k = 0; k < h.S; ++k)
+        for (auto& kv : h.sp[k].source) src[(size_t)k * h.nDomains + kv.first] = kv.second;
+    h.srcTab = dalloc<double>(src.size());
+    CK(cudaMemcpyAsync(h.srcTab, src.data(), sizeof(double) * src.size(), cudaMemcpyHostToDevice, h.stream));
+    h.ctypeHost.assign(h.nDomains, 1);
+    for (auto& kv : ctypes)
+        if (kv.first < (uint32_t)h.nDomains) h.ctypeHost[kv.first] = kv.second;
+    h.ctypeTab = dalloc<uint32_t>(h.nDomains);
+    CK(cudaMemcpyAsync(h.ctypeTab, h.ctypeHost.data(), sizeof(uint32_t) * h.nDomains, cudaMemcpyHostToDevice, h.stream));
+
+    if (!forceFile.empty()) {
+        std::ifstream fin(forceFile);
+        if (!fin.is_open()) fail(ERR_INPUT, "Cannot find the force solver file.");
+        while (std::getline(fin, line)) {
+            if (line.empty()) fail(ERR_INPUT, "empty line in the force file");
+            if (line[0] == '#') continue;
+            add_force_line(h, line);
+        }
+    }
+    h.forcesPure = h.forcemap.empty();
+
+    upload_topology(h, hm, false);
+    {
+        std::vector<int> z(h.m.M + 1, 0);
+        CK(cudaMemcpyAsync(h.m.foff, z.data(), sizeof(int) * z.size(), cudaMemcpyHostToDevice, h.stream));
+    }
+    cure_lattice(h, hm);
+
+    // SimulationRunner::initSolvers (SimulationRunner.cpp:290-306)
+    SpeciesConst spc[kMaxSpecies] = {};
+    double init[kMaxSpecies] = {0, 0, 0};
+    for (int k = 0; k < h.S; ++k) { spc[k] = h.sp[k].c; init[k] = h.sp[k].init; }
+    if (h.precision == LBIB_FP64)
+        launch_init64((double*)h.f[0], (double*)h.g[0], (double*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
+    else
+        launch_init32((float*)h.f[0], (float*)h.g[0], (float*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
+    h.cur = 0;
+    // SimulationRunner::initForceSolver: the force list
+    if (!h.forcemap.empty()) upload_topology(h, hm, true);
+    CK(cudaStreamSynchronize(h.stream));
+    CK(cudaGetLastError());
+}
+
+// GeometryHandler::cureLattice (GeometryHandler.cpp:149-170): perturb the
+// connections, bind the stencils (edge test), generate the crossings and set
+// every domain id by the row scan.  No species reinitialisation happens here.
+static void cure_lattice(Handle& h, HostMembrane& hm) {
+    perturb_connections(h, hm);
+    CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
+    std::memset(h.stHost, 0, sizeof(Status));
+    write_status(h);
+    launch_edge_check(h.m, h.nx, h.ny, h.st, 0, h.stream);
+    if (h.precision == LBIB_FP64) launch_crossings<double>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
+    else launch_crossings<float>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
+    launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
+    launch_cross_clear(h.cross, h.st, h.stream);
+    read_status(h);
+    if (h.stHost->err) fail(h.stHost->err, "lattice set-up failed", h.stHost->errIndex);
+    std::memset(h.stHost, 0, sizeof(Status));
+    write_status(h);
+}
+
+}  // namespace lbib
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+using lbib::Handle;
+using lbib::HostFail;
+
+struct lbib_handle {
+    Handle h;
+};
+
+#define API_BEGIN(hh)                                    \
+    if (!(hh)) return LBIB_ERR_STATE;                    \
+    Handle& h = (hh)->h;                                 \
+    if (h.err) return h.err;                             \
+    try {                                                \
+        cudaSetDevice(h.device);
+#define API_END                                          \
+    } catch (const HostFail& e) {                        \
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index; \
+        return e.code;                                   \
+    } catch (const std::exception& e) {                  \
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();        \
+        return h.err;                                    \
+    }                                                    \
+    return LBIB_OK;
+
+extern "C" {
+
+int lbib_create_from_files(const char* parameters, const char* geometry, const char* force, const char* plugins,
+                           int precision, int device, lbib_handle** out) {
+    if (!out || !parameters || !geometry) return LBIB_ERR_INPUT;
+    if (precision != LBIB_FP64 && precision != LBIB_FP32_SHIFTED) return LBIB_ERR_INPUT;
+    lbib_handle* hh = new lbib_handle();
+    *out = hh;
+    Handle& h = hh->h;
+    h.precision = precision;
+    h.device = device;
+    try {
+        lbib::create(h, parameters, geometry, force ? force : "", plugins ? plugins : "");
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index;
+        return e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return h.err;
+    }
+    return LBIB_OK;
+}
+
+int lbib_destroy(lbib_handle* hh) {
+    delete hh;
+    return LBIB_OK;
+}
+
+int lbib_step(lbib_handle* hh, int n) {
+    API_BEGIN(hh)
+    if (n < 0) lbib::fail(LBIB_ERR_INPUT, "negative step count");
+    h.lastCollideMs = 0;
+    h.lastCollideLaunches = 0;
+    h.launches = 0;
+    CK(cudaEventRecord(h.evA, h.stream));
+    if (h.precision == LBIB_FP64) lbib::run_steps<double>(h, n);
+    else lbib::run_steps<float>(h, n);
+    CK(cudaEventRecord(h.evB, h.stream));
+    CK(cudaEventSynchronize(h.evB));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
+    h.lastTotalMs = ms;
+    API_END
+}
+
+int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
+    API_BEGIN(hh)
+    if (n < 0) lbib::fail(LBIB_ERR_INPUT, "negative step count");
+    std::memset(h.stHost, 0, sizeof(lbib::Status));
+    lbib::write_status(h);
+    h.lastCollideMs = 0;
+    h.lastCollideLaunches = 0;
+    h.launches = (long long)n * (outlet ? 2 : 1);
+    while ((int)h.kEvents.size() < 2 * n) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        h.kEvents.push_back(e);
+    }
+    CK(cudaEventRecord(h.evA, h.stream));
+    for (int i = 0; i < n; ++i) {
+        const int p = h.cur;
+        if (h.profiling) CK(cudaEventRecord(h.kEvents[2 * i], h.stream));
+        if (h.precision == LBIB_FP64) {
+            auto a = lbib::lattice_args<double>(h, h.iteration, p);
+            lbib::launch_stream_collide64(a, h.stream);
+        } else {
+            auto a = lbib::lattice_args<float>(h, h.iteration, p);
+            lbib::launch_stream_collide32(a, h.stream);
+        }
+        if (h.profiling) CK(cudaEventRecord(h.kEvents[2 * i + 1], h.stream));
+        h.cur = 1 - p;
+        if (outlet) {
+            if (h.precision == LBIB_FP64)
+                lbib::launch_outlet64((double*)h.f[h.cur], (double*)h.g[h.cur], h.S, h.nx, h.ny, h.L, h.st, h.stream);
+            else
+                lbib::launch_outlet32((float*)h.f[h.cur], (float*)h.g[h.cur], h.S, h.nx, h.ny, h.L, h.st, h.stream);
+        }
+        h.iteration++;
+    }
+    CK(cudaEventRecord(h.evB, h.stream));
+    CK(cudaEventSynchronize(h.evB));
+    CK(cudaGetLastError());
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
+    h.lastTotalMs = ms;
+    if (h.profiling)
+        for (int i = 0; i < n; ++i) {
+            float k = 0;
+            CK(cudaEventElapsedTime(&k, h.kEvents[2 * i], h.kEvents[2 * i + 1]));
+            h.lastCollideMs += k;
+            h.lastCollideLaunches++;
+        }
+    API_END
+}
+
+int lbib_get_sizes(lbib_handle* hh, long long* s) {
+    if (!hh || !s) return LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    s[0] = h.nx; s[1] = h.ny; s[2] = h.S; s[3] = (long long)h.ids.size(); s[4] = (long long)h.conns.size();
+    s[5] = h.iteration; s[6] = h.precision; s[7] = h.hostEvents; s[8] = h.stepsDone; s[9] = h.m.nCells;
+    return LBIB_OK;
+}
+
+int lbib_download_lattice(lbib_handle* hh, double* f, double* g, double* vel, double* force, unsigned* dom,
+                          unsigned* ctype) {
+    API_BEGIN(hh)
+    const size_t L = h.L;
+    const int S = h.S;
+    const bool fp64 = h.precision == LBIB_FP64;
+    const size_t rs = fp64 ? 8 : 4;
+    std::vector<char> buf;
+    auto fetch = [&](const void* src, size_t count) {
+        buf.resize(count * rs);
+        CK(cudaMemcpyAsync(buf.data(), src, count * rs, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    };
+    auto val = [&](size_t i) -> double {
+        return fp64 ? ((const double*)buf.data())[i] : (double)((const float*)buf.data())[i];
+    };
+    static const int INV9[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+    static const int INV5[5] = {0, 3, 4, 1, 2};
+    static const double W9[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                                 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+    if (f) {
+        fetch(h.f[h.cur], 9 * L);
+        for (size_t n = 0; n < L; ++n)
+            for (int d = 0; d < 9; ++d) {
+                const int q = INV9[d];
+                f[n * 9 + d] = fp64 ? val(q * L + n) : val(q * L + n) + W9[q];
+            }
+    }
+    if (g && S > 0) {
+        fetch(h.g[h.cur], (size_t)S * 5 * L);
+        for (int k = 0; k < S; ++k)
+            for (size_t n = 0; n < L; ++n)
+                for (int d = 0; d < 5; ++d) g[((size_t)k * L + n) * 5 + d] = val(((size_t)k * 5 + INV5[d]) * L + n);
+    }
+    if (vel) {
+        fetch(h.u, 2 * L);
+        for (size_t n = 0; n < L; ++n) { vel[2 * n] = val(n); vel[2 * n + 1] = val(L + n); }
+    }
+    if (force) {
+        fetch(h.force, 2 * L);
+        std::vector<int> tc(h.tiles.nTiles);
+        CK(cudaMemcpyAsync(tc.data(), h.tiles.count, sizeof(int) * tc.size(), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        for (size_t n = 0; n < L; ++n) {
+            const int x = (int)(n % h.nx), y = (int)(n / h.nx);
+            const bool act = tc[(y / lbib::kTile) * h.tiles.tilesX + x / lbib::kTile] > 0;
+            force[2 * n] = act ? val(n) : 0.0;
+            force[2 * n + 1] = act ? val(L + n) : 0.0;
+        }
+    }
+    if (dom || ctype) {
+        std::vector<uint32_t> d(L);
+        CK(cudaMemcpyAsync(d.data(), h.dom, sizeof(uint32_t) * L, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        for (size_t n = 0; n < L; ++n) {
+            if (dom) dom[n] = d[n];
+            if (ctype) ctype[n] = h.cellTypesCopied ? (d[n] < h.ctypeHost.size() ? h.ctypeHost[d[n]] : 1u) : 0u;
+        }
+    }
+    API_END
+}
+
+int lbib_upload_lattice(lbib_handle* hh, const double* f, const double* g, const double* force) {
+    API_BEGIN(hh)
+    const size_t L = h.L;
+    const bool fp64 = h.precision == LBIB_FP64;
+    static const int INV9[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+    static const int INV5[5] = {0, 3, 4, 1, 2};
+    static const double W9[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                                 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+    auto put = [&](void* dst, const std::vector<double>& v) {
+        if (fp64) {
+            CK(cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+        } else {
+            std::vector<float> fv(v.begin(), v.end());
+            CK(cudaMemcpyAsync(dst, fv.data(), fv.size() * 4, cudaMemcpyHostToDevice, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+        }
+    };
+    if (f) {
+        std::vector<double> v(9 * L);
+        for (size_t n = 0; n < L; ++n)
+            for (int d = 0; d < 9; ++d) {
+                const int q = INV9[d];
+                v[q * L + n] = fp64 ? f[n * 9 + d] : f[n * 9 + d] - W9[q];
+            }
+        put(h.f[h.cur], v);
+    }
+    if (g && h.S > 0) {
+        std::vector<double> v((size_t)h.S * 5 * L);
+        for (int k = 0; k < h.S; ++k)
+            for (size_t n = 0; n < L; ++n)
+                for (int d = 0; d < 5; ++d) v[((size_t)k * 5 + INV5[d]) * L + n] = g[((size_t)k * L + n) * 5 + d];
+        put(h.g[h.cur], v);
+    }
+    if (force) {
+        std::vector<double> v(2 * L);
+        for (size_t n = 0; n < L; ++n) { v[n] = force[2 * n]; v[L + n] = force[2 * n + 1]; }
+        put(h.force, v);
+        // mark every tile active so that the lattice kernels read the field
+        std::vector<int> ones(h.tiles.nTiles, 1);
+        CK(cudaMemcpyAsync(h.tiles.count, ones.data(), sizeof(int) * ones.size(), cudaMemcpyHostToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    }
+    API_END
+}
+
+int lbib_download_membrane(lbib_handle* hh, unsigned* ids, double* state) {
+    API_BEGIN(hh)
+    lbib::HostMembrane hm;
+    lbib::download_membrane(h, hm);
+    for (size_t i = 0; i < h.ids.size(); ++i) {
+        if (ids) ids[i] = h.ids[i];
+        if (state) {
+            double* o = state + 6 * i;
+            o[0] = hm.x[i]; o[1] = hm.y[i]; o[2] = hm.vx[i]; o[3] = hm.vy[i]; o[4] = hm.fx[i]; o[5] = hm.fy[i];
+        }
+    }
+    API_END
+}
+
+int lbib_download_connections(lbib_handle* hh, unsigned* conn) {
+    API_BEGIN(hh)
+    for (size_t c = 0; c < h.conns.size(); ++c) {
+        conn[3 * c] = h.conns[c].id1; conn[3 * c + 1] = h.conns[c].id2; conn[3 * c + 2] = h.conns[c].dom;
+    }
+    API_END
+}
+
+int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    try {
+        cudaSetDevice(h.device);
+        lbib::launch_areas(h.m, h.area, h.stream);
+        std::vector<double> a(h.m.nCells);
+        if (h.m.nCells)
+            CK(cudaMemcpyAsync(a.data(), h.area, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        for (int c = 0; c < h.m.nCells && c < cap; ++c) {
+            dom[c] = h.ringDomHost[c];
+            area[c] = a[c];
+        }
+        return h.m.nCells;
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg;
+        return -e.code;
+    }
+}
+
+int lbib_set_species_source(lbib_handle* hh, int k, const double* rates, int n) {
+    API_BEGIN(hh)
+    if (k < 0 || k >= h.S || n < 0 || n > h.nDomains || (n > 0 && !rates))
+        lbib::fail(LBIB_ERR_INPUT, "bad species index or table size");
+    if (n > 0)
+        CK(cudaMemcpyAsync(h.srcTab + (size_t)k * h.nDomains, rates, sizeof(double) * n, cudaMemcpyHostToDevice,
+                           h.stream));
+    API_END
+}
+
+int lbib_last_error(lbib_handle* hh, char* buf, int len, long long* index) {
+    if (!hh) return LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (buf && len > 0) std::snprintf(buf, len, "%s", h.msg.c_str());
+    if (index) *index = h.errIndex;
+    return h.err;
+}
+
+int lbib_last_timing(lbib_handle* hh, double* out) {
+    if (!hh || !out) return LBIB_ERR_STATE;
+    out[0] = hh->h.lastTotalMs;
+    out[1] = hh->h.lastCollideMs;
+    out[2] = (double)hh->h.lastCollideLaunches;
+    out[3] = (double)hh->h.launches;
+    return LBIB_OK;
+}
+
+int lbib_set_profiling(lbib_handle* hh, int on) {
+    if (!hh) return LBIB_ERR_STATE;
+    hh->h.profiling = on != 0;
+    return LBIB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// lbib_internal.cuh — shared definitions of the lbibcell_b200 device runtime.
+//
+// Lattice layout in HBM (structure of arrays, one plane per direction):
+//   distributions  f[q][n], q = 0..8 in the reference's D2Q9 order
+//                  T,E,N,W,S,NE,NW,SW,SE (libs/LbmLib/include/Direction.hpp:34-44),
+//                  n = y*nx + x.  Two copies (A/B) for the pull scheme; each
+//                  copy holds the post-collision values of one step in natural
+//                  direction order (the reference stores them under the
+//                  inverse direction after FluidSolver::localSwap).
+//   species        g[k][q][n], q = 0..4 (T,E,N,W,S), two copies.
+//   velocity       u[2][n]  (post-collision fluid velocity, FluidSolver::velocity_)
+//   force          F[2][n]  (spread IBM force, FluidSolver::force_), written and
+//                  read only inside tiles that hold membrane stencils.
+//   domain         dom[n] (u32, PhysicalNode::domainIdentifier_)
+// FP64 mode stores f; FP32-shifted mode stores f - w_q (rest state rho0 = 1).
+//
+// Membrane (nodes kept in ascending id order, the reference's std::map order):
+//   x, y, ox, oy, vx, vy, fx, fy (FP64), id (u32)
+// Connections in Geometry::connections_ order: a[c], b[c] node indices, dom[c].
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lbib {
+
+// Direction tables: libs/LbmLib/include/Direction.hpp:34-44 and
+// libs/LbmLib/src/Direction.cpp:27-61.
+enum Dir { T = 0, E = 1, N = 2, W = 3, S = 4, NE = 5, NW = 6, SW = 7, SE = 8 };
+
+// Constants: libs/LbmLib/include/Constants.hpp:31-49.
+constexpr double kEPSILON = 10E-10;
+constexpr double kPERTURBATION = 10E-7;
+constexpr double kMAXLENGTH = 0.5;
+
+// Status word shared by all stage kernels (device memory, one per handle).
+struct Status {
+    int halt;          // non-zero: later stage kernels return immediately
+    int haltStage;     // stage that raised the halt
+    int err;           // LBIB_ERR_* (0 = none)
+    int errIndex;      // node / connection index of the first error
+    int nPerturbNode;  // membrane nodes whose position needs the host RNG
+    int nPerturbConn;  // connections that need Connection::perturbConnection
+    int nChanged;      // lattice nodes whose domain id changed (reinit list)
+    int nRecords;      // crossing records this step
+    int remesh;        // a connection is longer than MAXLENGTH
+    int coarsen;       // a node is a coarsening candidate
+    int nDiagReinit;   // reinit from diagonal neighbours
+    int nFailedReinit; // reinit without any neighbour (division by zero)
+    int pad[4];
+};
+
+// Stage numbers (halt points), in the reference's order of
+// SimulationRunner::runSimulation (SimulationRunner.cpp:72-99).
+enum Stage {
+    ST_FORCE = 1,
+    ST_SPREAD = 2,
+    ST_COLLIDE = 3,
+    ST_INTERP_MOVE = 4,
+    ST_PERTURB_CONN = 5,
+    ST_CROSSINGS = 6,
+    ST_REINIT = 7,
+    ST_DOMAIN = 8,
+    ST_REMESH = 9,
+    ST_COARSEN = 10,
+    ST_OUTLET = 11,
+    ST_BIO = 12,
+    ST_DONE = 13,
+};
+
+// Error codes (also returned through the C ABI, include/lbibcell.h).
+enum Err {
+    ERR_OK = 0,
+    ERR_EDGE_W = 10, ERR_EDGE_S = 11, ERR_EDGE_E = 12, ERR_EDGE_N = 13,
+    ERR_SPEED = 20,
+    ERR_LEFT_DOMAIN = 30,
+    ERR_VERTICAL = 40,
+    ERR_FORCE_NODE = 50,
+    ERR_STENCIL = 60,
+    ERR_CAPACITY = 70,
+    ERR_CUDA = 80,
+    ERR_INPUT = 90,
+    ERR_STATE = 91,
+};
+
+__device__ __forceinline__ void raise_error(Status* st, int code, int index, int stage) {
+    if (atomicCAS(&st->err, 0, code) == 0) st->errIndex = index;
+    atomicExch(&st->halt, 1);
+    atomicCAS(&st->haltStage, 0, stage);
+}
+
+__device__ __forceinline__ void raise_halt(Status* st, int stage) {
+    atomicExch(&st->halt, 1);
+    atomicCAS(&st->haltStage, 0, stage);
+}
+
+// Reaction kinds of the CDE species.
+enum Reaction { RX_NONE = 0, RX_LINEAR = 1, RX_SIGNAL = 2 };
+
+constexpr int kMaxSpecies = 3;
+
+// Per-species constants for the lattice kernels.
+struct SpeciesConst {
+    int kind;
+    double tau;
+    double decay;
+};
+
+// Everything the fused stream-collide kernel reads besides the planes.
+template <typename Real>
+struct LatticeArgs {
+    int nx, ny;
+    size_t L;
+    int S;
+    const Real* fin;      // 9*L
+    Real* fout;           // 9*L
+    const Real* gin;      // S*5*L
+    Real* gout;           // S*5*L
+    Real* u;              // 2*L
+    const Real* force;    // 2*L (valid where tileCount > 0)
+    const int* tileCount; // per 16x16 tile: membrane stencils overlapping it
+    int tilesX;
+    const uint32_t* dom;  // L
+    const double* massTab;     // per-domain rhoToAdd (nullptr: none)
+    int nDomains;              // entries in massTab / srcTab rows
+    const double* srcTab;      // [S][nDomains] production per step
+    double tauF;
+    SpeciesConst sp[kMaxSpecies];
+    unsigned iteration;
+    const Status* status;
+};
+
+constexpr int kTile = 16;  // force tiles are 16x16 lattice nodes
+
+}  // namespace lbib

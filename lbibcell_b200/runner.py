@@ -1,0 +1,151 @@
+"""Host-side mirror of LBIBCell's simulation interface over the C ABI.
+
+``Simulation`` stands for the objects a reference application builds
+(apps/tutorial_01.cpp:59-143): the global ``Parameters``, ``Geometry`` +
+``GeometryHandler`` and ``SimulationRunner`` with its mass and bio solvers.  It
+is created from the same files the reference reads, plus the plugin file of
+lbibcell_b200/configs.py.  Every call goes to liblbibcuda.so; state lives on
+the GPU.
+
+Method map (reference -> here):
+    SimulationRunner::runSimulation loop body   -> step(n)
+    SimulationRunner::writeSimulation solvers   -> lattice() (same slot layout)
+    SimulationRunner::initSolvers(file)         -> set_lattice()
+    Geometry::getGeometryNodes                  -> membrane()
+    Geometry::getConnections                    -> connections()
+    GeometryHandler::computeAreas               -> areas()
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Dict, Optional
+
+import numpy as np
+
+from ._lib import LbibError, load
+
+FP64 = 0
+FP32_SHIFTED = 1
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class LatticeState:
+    f: np.ndarray       # (L, 9) reference slot convention
+    g: np.ndarray       # (S, L, 5)
+    vel: np.ndarray     # (L, 2)
+    force: np.ndarray   # (L, 2)
+    dom: np.ndarray     # (L,) uint32
+    ctype: np.ndarray   # (L,) uint32
+
+
+class Simulation:
+    """One GPU-resident LBIBCell simulation."""
+
+    def __init__(self, paths: Dict[str, str], precision: int = FP64, device: int = 0):
+        self._L = load()
+        h = ctypes.c_void_p()
+        rc = self._L.lbib_create_from_files(paths["parameters"].encode(), paths["geometry"].encode(),
+                                            paths.get("force", "").encode(), paths.get("plugins", "").encode(),
+                                            int(precision), int(device), ctypes.byref(h))
+        self._h = h
+        if rc:
+            err = self._error()
+            self.close()
+            raise err
+        self.precision = precision
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.lbib_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _error(self) -> LbibError:
+        buf = ctypes.create_string_buffer(512)
+        idx = ctypes.c_longlong(-1)
+        code = self._L.lbib_last_error(self._h, buf, 512, ctypes.byref(idx))
+        return LbibError(code, buf.value.decode(), idx.value)
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise self._error()
+
+    # -- stepping -------------------------------------------------------------
+    def step(self, n: int = 1) -> None:
+        """n iterations of SimulationRunner::runSimulation's loop body."""
+        self._check(self._L.lbib_step(self._h, int(n)))
+
+    def lattice_step(self, n: int = 1, outlet: bool = True) -> None:
+        """n stream-collide steps with the geometry, forces and domains fixed."""
+        self._check(self._L.lbib_lattice_step(self._h, int(n), 1 if outlet else 0))
+
+    def set_species_source(self, k: int, rates: np.ndarray) -> None:
+        """Per-domain production rate of species k (index = domain id)."""
+        r = np.ascontiguousarray(rates, np.float64)
+        self._check(self._L.lbib_set_species_source(self._h, int(k), _p(r), int(r.size)))
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self._L.lbib_set_profiling(self._h, 1 if on else 0))
+
+    def last_timing(self) -> Dict[str, float]:
+        out = np.zeros(4)
+        self._check(self._L.lbib_last_timing(self._h, _p(out)))
+        return {"total_ms": float(out[0]), "collide_ms": float(out[1]), "collide_launches": int(out[2]),
+                "launches": int(out[3])}
+
+    # -- state ----------------------------------------------------------------
+    def sizes(self) -> Dict[str, int]:
+        s = np.zeros(10, np.int64)
+        self._check(self._L.lbib_get_sizes(self._h, _p(s)))
+        keys = ("nx", "ny", "S", "M", "C", "iteration", "precision", "host_events", "steps", "cells")
+        return {k: int(v) for k, v in zip(keys, s)}
+
+    def lattice(self) -> LatticeState:
+        z = self.sizes()
+        L, S = z["nx"] * z["ny"], z["S"]
+        f = np.zeros((L, 9)); g = np.zeros((S, L, 5)); vel = np.zeros((L, 2)); force = np.zeros((L, 2))
+        dom = np.zeros(L, np.uint32); ctype = np.zeros(L, np.uint32)
+        self._check(self._L.lbib_download_lattice(self._h, _p(f), _p(g), _p(vel), _p(force), _p(dom), _p(ctype)))
+        return LatticeState(f, g, vel, force, dom, ctype)
+
+    def set_lattice(self, f=None, g=None, force=None) -> None:
+        args = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (f, g, force)]
+        self._check(self._L.lbib_upload_lattice(self._h, *[_p(a) for a in args]))
+
+    def membrane(self):
+        """(ids[M], state[M, 6]) with state = x, y, vx, vy, fx, fy, in id order."""
+        M = self.sizes()["M"]
+        ids = np.zeros(M, np.uint32); st = np.zeros((M, 6))
+        self._check(self._L.lbib_download_membrane(self._h, _p(ids), _p(st)))
+        return ids, st
+
+    def connections(self) -> np.ndarray:
+        C = self.sizes()["C"]
+        c = np.zeros((C, 3), np.uint32)
+        self._check(self._L.lbib_download_connections(self._h, _p(c)))
+        return c
+
+    def areas(self) -> Dict[int, float]:
+        cap = max(1, self.sizes()["cells"])
+        d = np.zeros(cap, np.uint32); a = np.zeros(cap)
+        n = self._L.lbib_areas(self._h, _p(d), _p(a), cap)
+        if n < 0:
+            raise self._error()
+        return {int(d[i]): float(a[i]) for i in range(n)}

@@ -8,9 +8,11 @@
 // A report functor (the reference's own reporter API,
 // AbstractReportFunctor.hpp) dumps the state every ReportStep iterations.
 //
-// usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir [timing]
-//   With "timing" as the sixth argument no reporter is registered and the
-//   wall time of runSimulation() is printed as JSON (the CPU baseline).
+// usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir [timing W K]
+//   With "timing W K" no reporter is registered: runSimulation() runs W
+//   untimed iterations, then K iterations whose wall time is printed as JSON
+//   (the CPU baseline).  The log goes to outdir/log.txt as in
+//   apps/tutorial_01.cpp:47-57.
 //
 // Dump file outdir/dump_<t>.bin (little endian):
 //   int64 hdr[8] = {0x4c424942, t, nx, ny, S, M, C, currentIteration}
@@ -200,8 +202,12 @@ int main(int argc, char** argv) {
         std::cerr << "usage: ref_driver params geometry force plugins outdir [timing]\n";
         return 2;
     }
-    const bool timing = argc > 6 && std::string(argv[6]) == "timing";
+    const bool timing = argc > 8 && std::string(argv[6]) == "timing";
+    const unsigned warm = timing ? (unsigned)std::stoul(argv[7]) : 0;
+    const unsigned steps = timing ? (unsigned)std::stoul(argv[8]) : 0;
     try {
+        std::shared_ptr<std::ostream> logStream(new std::ofstream(std::string(argv[5]) + "/log.txt"));
+        UtilLib::Log::setStream(logStream);
         PluginList pl = loadPlugins(argv[4]);
         LbmLib::Parameters.loadGlobalSimulationParameters(argv[1]);
         LbmLib::geometry::Geometry geo(argv[2]);
@@ -215,14 +221,19 @@ int main(int argc, char** argv) {
         simRunner.initForceSolver(argv[3]);
         if (pl.outlet) simRunner.addMassSolver("MassSolverBoxOutlet");
         for (const auto& b : pl.bio) simRunner.addBioSolver(b);
-        const auto t0 = std::chrono::steady_clock::now();
-        simRunner.runSimulation();
-        const auto t1 = std::chrono::steady_clock::now();
-        if (timing) {
+        if (!timing) {
+            simRunner.runSimulation();
+        } else {
+            LbmLib::Parameters.iterations_ = warm;
+            if (warm) simRunner.runSimulation();
+            LbmLib::Parameters.iterations_ = steps;
+            const auto t0 = std::chrono::steady_clock::now();
+            simRunner.runSimulation();
+            const auto t1 = std::chrono::steady_clock::now();
             const double sec = std::chrono::duration<double>(t1 - t0).count();
-            std::printf("{\"seconds\": %.6f, \"iterations\": %u, \"nx\": %u, \"ny\": %u, \"threads\": %d}\n", sec,
-                        LbmLib::Parameters.getIterations(), LbmLib::Parameters.getSizeX(),
-                        LbmLib::Parameters.getSizeY(), omp_get_max_threads());
+            std::fprintf(stderr, "{\"seconds\": %.6f, \"iterations\": %u, \"warmup\": %u, \"nx\": %u, \"ny\": %u, \"threads\": %d}\n",
+                         sec, steps, warm, LbmLib::Parameters.getSizeX(), LbmLib::Parameters.getSizeY(),
+                         omp_get_max_threads());
         }
     } catch (const std::exception& e) {
         std::cerr << "reference run failed: " << e.what() << "\n";

@@ -1,0 +1,141 @@
+"""Parity of the CUDA path with the CPU oracle (itself pinned bit-exact to the
+reference build).  FP64 results must be identical; FP32-shifted results are
+checked against the FP64 path with stated tolerances."""
+import json
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from lbibcell_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def lbib():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from lbibcell_b200 import build, runner
+    build.build()
+    return runner
+
+
+def _cmp_exact(a, b, what):
+    assert a.shape == b.shape, (what, a.shape, b.shape)
+    if not np.array_equal(a, b):
+        d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+        i = np.unravel_index(np.argmax(d), d.shape)
+        raise AssertionError(f"{what}: max |diff| {d.max():.3e} at {i}: {a[i]} vs {b[i]}")
+
+
+def _compare_state(sim, st, with_force=True):
+    lat = sim.lattice()
+    _cmp_exact(lat.f, st.f, "f")
+    _cmp_exact(lat.g, st.g, "g")
+    _cmp_exact(lat.vel, st.vel, "vel")
+    if with_force:
+        _cmp_exact(lat.force, st.force, "force")
+    _cmp_exact(lat.dom, st.dom, "dom")
+    _cmp_exact(lat.ctype, st.ctype, "ctype")
+    ids, node = sim.membrane()
+    _cmp_exact(ids, st.ids, "ids")
+    _cmp_exact(node, st.node, "node")
+    _cmp_exact(sim.connections(), st.conn, "conn")
+
+
+def test_initial_state_fp64(lbib, oracle_mod, tmp_path):
+    paths = configs.toy(n=48, r=8.0, nodes=80, iterations=60, report_step=30).write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    _compare_state(sim, o.state())
+
+
+def test_lattice_only_fp64_random_force(lbib, oracle_mod, tmp_path):
+    """Fused pull stream-collide of fluid + 2 species and the box outlet, with a
+    random force field, against the oracle's swap-scheme advect/collide."""
+    paths = configs.toy(n=64, r=10.0, nodes=100, species=2).write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    rng = np.random.default_rng(7)
+    force = rng.normal(0, 1e-4, size=(64 * 64, 2))
+    st = o.state()
+    f = st.f + rng.normal(0, 1e-3, size=st.f.shape)
+    sim.set_lattice(f=f, g=st.g, force=force)
+    o.set_lattice(f=f, g=st.g, force=force)
+    sim.lattice_step(25, outlet=True)
+    o.lattice_step(25, outlet=True)
+    a, b = sim.lattice(), o.state()
+    _cmp_exact(a.f, b.f, "f")
+    _cmp_exact(a.g, b.g, "g")
+    _cmp_exact(a.vel, b.vel, "vel")
+
+
+def test_toy48_full_steps_fp64(lbib, oracle_mod, tmp_path):
+    """The whole reference step (IBM, crossings, domain ids, reinit, remesh,
+    coarsening, outlet, plugins) for 60 steps: identical to the oracle."""
+    paths = configs.toy(n=48, r=8.0, nodes=80, iterations=60, report_step=30).write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    for n in (1, 9, 20, 30):
+        sim.step(n)
+        o.step(n)
+        _compare_state(sim, o.state())
+
+
+def test_toy_two_species_fp64(lbib, oracle_mod, tmp_path):
+    paths = configs.toy(n=64, r=12.0, nodes=120, iterations=200, species=2).write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    for n in (50, 150):
+        sim.step(n)
+        o.step(n)
+        _compare_state(sim, o.state())
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_config1_fp64_matches_reference_digests(lbib, tmp_path):
+    """200x200 single cell, 2000 steps: every array identical to the reference
+    build's (golden digests from oracle/_ref)."""
+    dig = json.load(open(os.path.join(GOLD, "config1_digest.json")))
+    sim = lbib.Simulation(configs.config1().write(str(tmp_path)), lbib.FP64)
+    prev = 0
+    for t in (0, 500, 1000, 1500, 2000):
+        sim.step(t - prev)
+        prev = t
+        lat = sim.lattice()
+        ids, node = sim.membrane()
+        got = {"f": lat.f, "g": lat.g, "vel": lat.vel, "force": lat.force, "dom": lat.dom, "ctype": lat.ctype,
+               "ids": ids, "node": node, "conn": sim.connections()}
+        for k, v in got.items():
+            assert _digest(v) == dig[str(t)][k], (t, k)
+
+
+def test_fp32_shifted_error_config1(lbib, tmp_path):
+    """FP32-shifted vs FP64 on the 200x200 single cell after 500 steps: relative
+    max-norm errors (rho-1 by max|rho-1|, u by max|u|, c by max c) <= 1e-5;
+    membrane positions within 1e-6 lu."""
+    paths = configs.config1().write(str(tmp_path))
+    a = lbib.Simulation(paths, lbib.FP64)
+    b = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    a.step(500)
+    b.step(500)
+    la, lb = a.lattice(), b.lattice()
+    ra, rb = la.f.sum(1) - 1.0, lb.f.sum(1) - 1.0
+    e_rho = np.abs(ra - rb).max() / np.abs(ra).max()
+    e_u = np.abs(la.vel - lb.vel).max() / np.abs(la.vel).max()
+    ca, cb = la.g.sum(2), lb.g.sum(2)
+    e_c = np.abs(ca - cb).max() / np.abs(ca).max()
+    _, na = a.membrane()
+    _, nb = b.membrane()
+    e_x = np.abs(na[:, :2] - nb[:, :2]).max() if na.shape == nb.shape else np.inf
+    print(f"FP32-shifted vs FP64: rho {e_rho:.2e} u {e_u:.2e} c {e_c:.2e} x {e_x:.2e}")
+    assert e_rho <= 1e-5 and e_u <= 1e-5 and e_c <= 1e-5
+    assert e_x <= 1e-6
