@@ -21,6 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 UNITS = [
     ("k_lattice64.cu", ["--fmad=false"]),
     ("k_membrane.cu", ["--fmad=false"]),
+    ("k_topology.cu", ["--fmad=false"]),
     ("lbib_host.cu", ["--fmad=false"]),
     ("k_lattice32.cu", []),
 ]
@@ -51,7 +52,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
         subprocess.run(cmd, check=True)
         objs.append(obj)
     cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
-        "-Xcompiler", "-static-libstdc++", "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-Bsymbolic",
+        "-Xcompiler", "-static-libstdc++", "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-Bsymbolic", "-Xlinker", "--no-undefined",
         "-cudart", "static"]
     if verbose:
         print(" ".join(cmd))

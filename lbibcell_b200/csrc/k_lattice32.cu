@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
 
 // MassSolverBoxOutlet in shifted storage: f' = f / rho, i.e.
 // h' = h / rho + w (1/rho - 1) = (h - w * drho) / rho with drho = sum h.
-__device__ __forceinline__ void rescale_node32(float* f, float* g, int S, size_t L, size_t n) {
+__device__ __forceinline__ void rescale_node32(float* f, float* g, int nS, size_t L, size_t n) {
     const float wq[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
                          1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
     float drho = 0.0f;
@@ -126,25 +126,25 @@ __device__ __forceinline__ void rescale_node32(float* f, float* g, int S, size_t
         const float h = f[(size_t)q * L + n];
         f[(size_t)q * L + n] = (h - wq[q] * drho) * rinv;
     }
-    for (int k = 0; k < S; ++k)
+    for (int k = 0; k < nS; ++k)
 #pragma unroll
         for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] *= rinv;
 }
 
-__global__ void outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st) {
+__global__ void outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ny) {
-        rescale_node32(f, g, S, L, (size_t)i * nx);
-        if (i == 0) rescale_node32(f, g, S, L, 0);
+        rescale_node32(f, g, nS, L, (size_t)i * nx);
+        if (i == 0) rescale_node32(f, g, nS, L, 0);
     } else if (i < ny + nx - 1) {
-        rescale_node32(f, g, S, L, (size_t)(i - ny + 1));
+        rescale_node32(f, g, nS, L, (size_t)(i - ny + 1));
     }
 }
 
 // Initial state: the FP64 initial collision (f_T = 1, zero force and mass)
 // converted to deviations, and the species' initial conditions.
-__global__ void init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+__global__ void init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                        SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1,
                        double init2) {
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,7 +161,7 @@ __global__ void init32(float* f, float* g, float* u, int S, size_t L, double tau
     u[L + n] = 0.0f;
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
     const double init[3] = {init0, init1, init2};
-    for (int k = 0; k < S; ++k) {
+    for (int k = 0; k < nS; ++k) {
         double gi[5];
         if (sp[k].kind == RX_NONE) {
             const double tI = 1.0 / sp[k].tau;
@@ -180,14 +180,14 @@ void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
     stream_collide32<<<(unsigned)((a.L + 255) / 256), 256, 0, s>>>(a);
 }
 
-void launch_outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
+void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
     const int n = nx + ny;
-    outlet32<<<(n + 255) / 256, 256, 0, s>>>(f, g, S, nx, ny, L, st);
+    outlet32<<<(n + 255) / 256, 256, 0, s>>>(f, g, nS, nx, ny, L, st);
 }
 
-void launch_init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s) {
-    init32<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, S, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+    init32<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
                                                        init[1], init[2]);
 }
 

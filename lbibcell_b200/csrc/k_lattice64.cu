@@ -72,36 +72,36 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
 // Column x=0 (all y) then row y=0 (all x); the corner (0,0) is rescaled
 // twice, first by the column pass.  rho is summed in the reference's slot
 // order after FluidSolver::localSwap: T, W, S, E, N, SW, SE, NE, NW.
-__device__ __forceinline__ void rescale_node64(double* f, double* g, int S, size_t L, size_t n) {
-    const int order[9] = {T, W, S, E, N, SW, SE, NE, NW};
+__device__ __forceinline__ void rescale_node64(double* f, double* g, int nS, size_t L, size_t n) {
+    const int order[9] = {Dir::T, Dir::W, Dir::S, Dir::E, Dir::N, Dir::SW, Dir::SE, Dir::NE, Dir::NW};
     double rho = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) rho += f[(size_t)order[i] * L + n];
     const double sc = 1.0 / rho;
 #pragma unroll
     for (int q = 0; q < 9; ++q) f[(size_t)q * L + n] *= sc;
-    for (int k = 0; k < S; ++k)
+    for (int k = 0; k < nS; ++k)
 #pragma unroll
         for (int q = 0; q < 5; ++q) g[((size_t)k * 5 + q) * L + n] *= sc;
 }
 
-__global__ void outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st) {
+__global__ void outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     // threads [0, ny): column nodes (0, i); thread 0 also runs the corner's
     // row pass after its column pass.  threads [ny, ny + nx - 1): row nodes (x, 0), x >= 1.
     if (i < ny) {
-        rescale_node64(f, g, S, L, (size_t)i * nx);
-        if (i == 0) rescale_node64(f, g, S, L, 0);
+        rescale_node64(f, g, nS, L, (size_t)i * nx);
+        if (i == 0) rescale_node64(f, g, nS, L, 0);
     } else if (i < ny + nx - 1) {
         const int x = i - ny + 1;
-        rescale_node64(f, g, S, L, (size_t)x);
+        rescale_node64(f, g, nS, L, (size_t)x);
     }
 }
 
 // FluidSolver::initSolver (f_T = 1, then collide with zero force and mass)
 // and the species' initial conditions.
-__global__ void init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+__global__ void init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                        SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1, double init2) {
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L) return;
@@ -114,7 +114,7 @@ __global__ void init64(double* f, double* g, double* u, int S, size_t L, double 
     u[L + n] = uy;
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
     const double init[3] = {init0, init1, init2};
-    for (int k = 0; k < S; ++k) {
+    for (int k = 0; k < nS; ++k) {
         double gi[5];
         if (sp[k].kind == RX_NONE) {
             // CDESolverD2Q5::initSolver — CDESolverD2Q5.cpp:37-40
@@ -136,14 +136,14 @@ void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
     stream_collide64<<<blocks, 256, 0, s>>>(a);
 }
 
-void launch_outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
+void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
     const int n = nx + ny;
-    outlet64<<<(n + 255) / 256, 256, 0, s>>>(f, g, S, nx, ny, L, st);
+    outlet64<<<(n + 255) / 256, 256, 0, s>>>(f, g, nS, nx, ny, L, st);
 }
 
-void launch_init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s) {
-    init64<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, S, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+    init64<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
                                                        init[1], init[2]);
 }
 

@@ -62,7 +62,7 @@ __device__ __forceinline__ double dirac(const double dx, const double dy) {
 __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.M) return;
+    if (i >= m.topo->M) return;
     const double x1 = m.x[i], y1 = m.y[i];
     double Fx = 0.0, Fy = 0.0;
     const int r0 = m.foff[i], r1 = m.foff[i + 1];
@@ -70,7 +70,7 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration)
         const int type = m.ftype[r];
         const double* p = m.fpar + 4 * (size_t)r;
         const int j = m.fpartner[r];
-        if ((type == 0 || type == 7 || type == 5 || type == 6) && (j < 0 || j >= m.M)) {
+        if ((type == 0 || type == 7 || type == 5 || type == 6) && (j < 0 || j >= m.topo->M)) {
             raise_error(st, ERR_FORCE_NODE, i, ST_FORCE);
             return;
         }
@@ -126,8 +126,8 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration)
 
 template <typename Real>
 void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
-    if (m.M == 0) return;
-    force_eval_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, st, iteration);
+    if (m.Mcap == 0) return;
+    force_eval_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, st, iteration);
 }
 template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t);
 template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t);
@@ -135,25 +135,61 @@ template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cu
 // ---------------------------------------------------------------------------
 // Spreading
 
-// Stencil origin of a membrane node: x in [ceil(X-2), floor(X+2)]
-// (GeometryHandler.cpp:613-643).  For a non-integer X the stencil is 4 wide.
-__device__ __forceinline__ bool stencil_origin(double X, double Y, int nx, int ny, int& x0, int& y0) {
-    x0 = (int)ceil(X - 2.0);
-    y0 = (int)ceil(Y - 2.0);
-    const int x1 = (int)floor(X + 2.0), y1 = (int)floor(Y + 2.0);
-    return x1 - x0 == 3 && y1 - y0 == 3 && x0 >= 0 && y0 >= 0 && x1 < nx && y1 < ny;
+// Stencil of a membrane node (GeometryHandler.cpp:613-643): the loop
+//   for x in [ceil(X-2), floor(X+2)], for y in [ceil(Y-2), floor(Y+2)]:
+//       slot[(4x + y) % 16] = node(x, y)
+// binds 16 slots.  The ranges are 4 wide, except when rounding of X+2 or X-2
+// makes them 5 wide (e.g. X = 32 - 1 ulp); then later writes replace earlier
+// ones with the same slot, and the bound set is what the last writers leave.
+struct Stencil {
+    int x0, x1, y0, y1;
+};
+
+__device__ __forceinline__ bool stencil_range(double X, double Y, int nx, int ny, Stencil& s) {
+    s.x0 = (int)ceil(X - 2.0);
+    s.y0 = (int)ceil(Y - 2.0);
+    s.x1 = (int)floor(X + 2.0);
+    s.y1 = (int)floor(Y + 2.0);
+    const int wx = s.x1 - s.x0, wy = s.y1 - s.y0;
+    return wx >= 3 && wx <= 4 && wy >= 3 && wy <= 4 && s.x0 >= 0 && s.y0 >= 0 && s.x1 < nx && s.y1 < ny;
+}
+
+// Is lattice node (x, y) bound by the stencil (the last writer of its slot)?
+__device__ __forceinline__ bool in_stencil(const Stencil& s, int x, int y) {
+    if (x < s.x0 || x > s.x1 || y < s.y0 || y > s.y1) return false;
+    if (s.x1 - s.x0 == 3 && s.y1 - s.y0 == 3) return true;
+    const int slot = (4 * x + y) & 15;
+    for (int xp = x; xp <= s.x1; ++xp)
+        for (int yp = (xp == x ? y + 1 : s.y0); yp <= s.y1; ++yp)
+            if (((4 * xp + yp) & 15) == slot) return false;
+    return true;
+}
+
+// The lattice node bound to slot k (k = 0..15).
+__device__ __forceinline__ void stencil_slot(const Stencil& s, int k, int& xk, int& yk) {
+    if (s.x1 - s.x0 == 3 && s.y1 - s.y0 == 3) {
+        const int base = ((4 * s.x0 + s.y0) % 16 + 16) % 16;
+        const int r = (k - base + 16) & 15;
+        xk = s.x0 + (r >> 2);
+        yk = s.y0 + (r & 3);
+        return;
+    }
+    xk = -1; yk = -1;
+    for (int x = s.x0; x <= s.x1; ++x)
+        for (int y = s.y0; y <= s.y1; ++y)
+            if (((4 * x + y) & 15) == k) { xk = x; yk = y; }
 }
 
 __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st, int pass) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.M) return;
-    int x0, y0;
-    if (!stencil_origin(m.x[i], m.y[i], nx, ny, x0, y0)) {
+    if (i >= m.topo->M) return;
+    Stencil sc;
+    if (!stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_SPREAD);
         return;
     }
-    const int tx0 = x0 / kTile, tx1 = (x0 + 3) / kTile, ty0 = y0 / kTile, ty1 = (y0 + 3) / kTile;
+    const int tx0 = sc.x0 / kTile, tx1 = sc.x1 / kTile, ty0 = sc.y0 / kTile, ty1 = sc.y1 / kTile;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
             const int tile = ty * t.tilesX + tx;
@@ -180,9 +216,14 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
         return;
     }
-    __shared__ int idx[kSpreadMax];
-    __shared__ double sx[kSpreadMax], sy[kSpreadMax], sfx[kSpreadMax], sfy[kSpreadMax];
-    __shared__ int sx0[kSpreadMax], sy0[kSpreadMax];
+    // dynamic shared memory: kSpreadMax x (4 doubles + stencil + index)
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sx = (double*)smem;
+    double* sy = sx + kSpreadMax;
+    double* sfx = sy + kSpreadMax;
+    double* sfy = sfx + kSpreadMax;
+    Stencil* sst = (Stencil*)(sfy + kSpreadMax);
+    int* idx = (int*)(sst + kSpreadMax);
     int p2 = 1;
     while (p2 < cnt) p2 <<= 1;
     const int base = t.start[tile];
@@ -205,8 +246,7 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
         const int i = idx[k];
         sx[k] = m.x[i]; sy[k] = m.y[i]; sfx[k] = m.fx[i]; sfy[k] = m.fy[i];
-        sx0[k] = (int)ceil(sx[k] - 2.0);
-        sy0[k] = (int)ceil(sy[k] - 2.0);
+        stencil_range(sx[k], sy[k], nx, ny, sst[k]);
     }
     __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
@@ -214,8 +254,7 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     if (x >= nx || y >= ny) return;
     double ax = 0.0, ay = 0.0;
     for (int k = 0; k < cnt; ++k) {
-        const int dx0 = x - sx0[k], dy0 = y - sy0[k];
-        if ((unsigned)dx0 < 4u && (unsigned)dy0 < 4u) {
+        if (in_stencil(sst[k], x, y)) {
             const double dl = dirac((double)x - sx[k], (double)y - sy[k]);
             ax += sfx[k] * dl;
             ay += sfy[k] * dl;
@@ -231,12 +270,18 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
                    unsigned iteration, cudaStream_t s) {
     cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
     cudaMemsetAsync(t.fill, 0, sizeof(int) * t.nTiles, s);
-    if (m.M == 0) return;
-    const int blocks = (m.M + 127) / 128;
+    if (m.Mcap == 0) return;
+    const int blocks = (m.Mcap + 127) / 128;
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
-    spread_kernel<Real><<<t.nTiles, 256, 0, s>>>(m, t, force, nx, ny, L, st);
+    constexpr size_t smemBytes = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(Stencil) + sizeof(int));
+    static bool attrSet = false;
+    if (!attrSet) {
+        cudaFuncSetAttribute(spread_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+        attrSet = true;
+    }
+    spread_kernel<Real><<<t.nTiles, 256, smemBytes, s>>>(m, t, force, nx, ny, L, st);
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
                                     cudaStream_t);
@@ -260,19 +305,17 @@ __global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny,
                                    unsigned iteration) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.M) return;
+    if (i >= m.topo->M) return;
     const double X = m.x[i], Y = m.y[i];
-    int x0, y0;
-    if (!stencil_origin(X, Y, nx, ny, x0, y0)) {
+    Stencil sc;
+    if (!stencil_range(X, Y, nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
         return;
     }
     double vx = 0.0, vy = 0.0;
-    const int base = ((4 * x0 + y0) % 16 + 16) % 16;
-#pragma unroll
     for (int k = 0; k < 16; ++k) {
-        const int r = (k - base + 16) & 15;
-        const int xk = x0 + (r >> 2), yk = y0 + (r & 3);
+        int xk, yk;
+        stencil_slot(sc, k, xk, yk);
         const size_t n = (size_t)yk * nx + xk;
         const double dl = dirac((double)xk - X, (double)yk - Y);
         vx += (double)u[n] * dl;
@@ -300,8 +343,8 @@ __global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny,
 template <typename Real>
 void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
                         unsigned iteration, cudaStream_t s) {
-    if (m.M == 0) return;
-    interp_move_kernel<Real><<<(m.M + 127) / 128, 128, 0, s>>>(m, u, nx, ny, L, c, st, iteration);
+    if (m.Mcap == 0) return;
+    interp_move_kernel<Real><<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, u, nx, ny, L, c, st, iteration);
 }
 template void launch_interp_move<double>(const MembraneDev&, const double*, int, int, size_t, CrossDev&, Status*,
                                          unsigned, cudaStream_t);
@@ -312,7 +355,7 @@ template void launch_interp_move<float>(const MembraneDev&, const float*, int, i
 __global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.C) return;
+    if (c >= m.topo->C) return;
     const int a = m.ca[c], b = m.cb[c];
     if (fabs(m.x[a] - m.x[b]) < kEPSILON || fabs(m.y[a] - m.y[b]) < kEPSILON) {
         atomicAdd(&st->nPerturbConn, 1);
@@ -321,8 +364,8 @@ __global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
 }
 
 void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
-    if (m.C == 0) return;
-    perturb_conn_kernel<<<(m.C + 127) / 128, 128, 0, s>>>(m, st);
+    if (m.Ccap == 0) return;
+    perturb_conn_kernel<<<(m.Ccap + 127) / 128, 128, 0, s>>>(m, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,7 +427,7 @@ __global__ void crossings_kernel(MembraneDev m, CrossDev c, const uint32_t* dom,
                                  int pass) {
     if (st->halt) return;
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cn >= m.C) return;
+    if (cn >= m.topo->C) return;
     const int a = m.ca[cn], b = m.cb[cn];
     const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
     const uint32_t D = m.cdom[cn];
@@ -426,7 +469,7 @@ __global__ void crossings_kernel(MembraneDev m, CrossDev c, const uint32_t* dom,
 __global__ void edge_check_kernel(MembraneDev m, int nx, int ny, Status* st, int stage) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.M) return;
+    if (i >= m.topo->M) return;
     const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
     const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
     if (within) return;
@@ -439,10 +482,10 @@ __global__ void edge_check_kernel(MembraneDev m, int nx, int ny, Status* st, int
 template <typename Real>
 void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, int nx, int ny, size_t L, Status* st,
                       unsigned iteration, cudaStream_t s) {
-    if (m.C == 0) return;
-    const int blocks = (m.C + 127) / 128;
+    if (m.Ccap == 0) return;
+    const int blocks = (m.Ccap + 127) / 128;
     for (int pass = 0; pass < 3; ++pass) crossings_kernel<<<blocks, 128, 0, s>>>(m, c, dom, nx, ny, st, pass);
-    edge_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_CROSSINGS);
+    edge_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_CROSSINGS);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
                                        unsigned, cudaStream_t);
@@ -450,8 +493,8 @@ template void launch_crossings<float>(const MembraneDev&, CrossDev&, const uint3
                                       unsigned, cudaStream_t);
 
 void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigned iteration, cudaStream_t s) {
-    if (m.M == 0) return;
-    edge_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_REMESH);
+    if (m.Mcap == 0) return;
+    edge_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_REMESH);
 }
 
 // ---------------------------------------------------------------------------
@@ -467,7 +510,7 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 constexpr int kReinitMax = 1024;
 
 template <typename Real>
-__device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int S,
+__device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int nS,
                             const SpeciesConst* sp, const double* srcTab, int nDomains, const uint32_t* ctypeTab,
                             int cellTypesCopied, const CrossDev& c, int nx, int ny, size_t L, Status* st,
                             unsigned iteration) {
@@ -484,7 +527,7 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     const uint32_t ctype = cellTypesCopied ? (oldDom < (uint32_t)nDomains ? ctypeTab[oldDom] : 1u) : 0u;
     const bool neNull = newDom == 0 && ctype == 0;
     const double ux = (double)u[n], uy = (double)u[L + n];
-    for (int k = 0; k < S; ++k) {
+    for (int k = 0; k < nS; ++k) {
         Real* gk = g + (size_t)k * 5 * L;
         double sumC = 0.0;
         int counter = 0;
@@ -525,7 +568,7 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int S,
+__global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int nS,
                                                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2,
                                                       const double* srcTab, int nDomains, const uint32_t* ctypeTab,
                                                       int cellTypesCopied, int nx, int ny, size_t L, Status* st,
@@ -598,7 +641,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         __syncthreads();
         for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
             if (done[k] == 2) {
-                reinit_node<Real>((size_t)(key[k] >> 32), (uint32_t)(key[k] & 0xffffffffu), dom, g, u, S, sp, srcTab,
+                reinit_node<Real>((size_t)(key[k] >> 32), (uint32_t)(key[k] & 0xffffffffu), dom, g, u, nS, sp, srcTab,
                                   nDomains, ctypeTab, cellTypesCopied, c, nx, ny, L, st, iteration);
                 atomicAdd(&nowDone, 1);
             }
@@ -613,11 +656,11 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
 }
 
 template <typename Real>
-void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int S, const SpeciesConst* sp,
+void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, const SpeciesConst* sp,
                    const double* srcTab, int nDomains, const uint32_t* ctypeTab, int cellTypesCopied, int nx, int ny,
                    size_t L, Status* st, unsigned iteration, cudaStream_t s) {
     if (c.changedCap <= 0) return;
-    reinit_kernel<Real><<<1, 1024, 0, s>>>(c, dom, g, u, S, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
+    reinit_kernel<Real><<<1, 1024, 0, s>>>(c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
                                            cellTypesCopied, nx, ny, L, st, iteration);
 }
 template void launch_reinit<double>(CrossDev&, uint32_t*, double*, const double*, int, const SpeciesConst*,
@@ -699,7 +742,7 @@ void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s) { remes
 __global__ void coarsen_check_kernel(MembraneDev m, Status* st) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.M) return;
+    if (i >= m.topo->M) return;
     const int p = m.prev[i], q = m.next[i];
     const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
     const double length = sqrt(dx * dx + dy * dy);
@@ -710,17 +753,17 @@ __global__ void coarsen_check_kernel(MembraneDev m, Status* st) {
 }
 
 void launch_coarsen_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
-    if (m.M == 0) return;
-    coarsen_check_kernel<<<(m.M + 127) / 128, 128, 0, s>>>(m, st);
+    if (m.Mcap == 0) return;
+    coarsen_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, st);
 }
 
-__global__ void clear_forces_kernel(int* foff, int M) {
+__global__ void clear_forces_kernel(MembraneDev m) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i <= M) foff[i] = 0;
+    if (i <= m.topo->M) m.foff[i] = 0;
 }
 
 void launch_clear_forces(MembraneDev& m, cudaStream_t s) {
-    clear_forces_kernel<<<(m.M + 1 + 255) / 256, 256, 0, s>>>(m.foff, m.M);
+    clear_forces_kernel<<<(m.Mcap + 1 + 255) / 256, 256, 0, s>>>(m);
 }
 
 // Tension renewal when the force list holds only tension pairs: node i gets
@@ -729,16 +772,16 @@ void launch_clear_forces(MembraneDev& m, cudaStream_t s) {
 // (tutorial_01_BioSolverMembraneTension.cpp:52-73 adds them in that order).
 __global__ void tension_pos_kernel(MembraneDev m, int* outPos, int* inPos) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.C) return;
+    if (c >= m.topo->C) return;
     outPos[m.ca[c]] = c;
     inPos[m.cb[c]] = c;
 }
 
 __global__ void tension_fill_kernel(MembraneDev m, const int* outPos, const int* inPos, double force) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > m.M) return;
+    if (i > m.topo->M) return;
     m.foff[i] = 2 * i;
-    if (i == m.M) return;
+    if (i == m.topo->M) return;
     const int nextNode = m.cb[outPos[i]], prevNode = m.ca[inPos[i]];
     const int first = outPos[i] < inPos[i] ? 0 : 1;
     m.ftype[2 * i + first] = 6;
@@ -752,9 +795,9 @@ __global__ void tension_fill_kernel(MembraneDev m, const int* outPos, const int*
 }
 
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s) {
-    if (m.M == 0) return;
-    tension_pos_kernel<<<(m.C + 127) / 128, 128, 0, s>>>(m, outPos, inPos);
-    tension_fill_kernel<<<(m.M + 1 + 127) / 128, 128, 0, s>>>(m, outPos, inPos, force);
+    if (m.Mcap == 0) return;
+    tension_pos_kernel<<<(m.Ccap + 127) / 128, 128, 0, s>>>(m, outPos, inPos);
+    tension_fill_kernel<<<(m.Mcap + 1 + 127) / 128, 128, 0, s>>>(m, outPos, inPos, force);
 }
 
 // ---------------------------------------------------------------------------

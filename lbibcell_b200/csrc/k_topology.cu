@@ -1,0 +1,464 @@
+// k_topology.cu — membrane topology edits on the device.
+//
+//   remesh    GeometryHandler::remeshBoundary (GeometryHandler.cpp:385-431) as
+//             scan + scatter: every connection longer than MAXLENGTH gets a new
+//             node at its midpoint; the new node ids continue from the largest
+//             id in connection order (Geometry::addGeometryNode,
+//             Geometry.cpp:382-400); the split connection leaves the vector and
+//             its two halves are appended (Geometry::eraseConnection /
+//             addConnection, Geometry.cpp:433-452).  Up to two passes run on
+//             the device (SimulationRunner.cpp:190-199 repeats until nothing is
+//             split); a third pass that would still split, a new node that
+//             needs the random perturbation, or a full buffer hands the step to
+//             the host.
+//   coarsen   GeometryHandler::coarsenBoundary (GeometryHandler.cpp:433-461):
+//             nodes are visited in id order and removed when their neighbours
+//             are closer than MAXLENGTH; a removal erases the node's two
+//             connections and appends one from its predecessor to its successor
+//             (Geometry::removeGeometryNode, Geometry.cpp:402-431).  Removals
+//             only interact along a ring, so one thread per cell runs the
+//             id-ordered visit over that cell's candidates (a node is a
+//             candidate if it is one at the start or a smaller-id neighbour
+//             was removed); the new connections are appended in removal order.
+//   rings     the node order of GeometryHandler::computeAreas (first connection
+//             of each domain in vector order, then the second node's outgoing
+//             connection) by pointer jumping, one block per cell.
+#include <cub/cub.cuh>
+
+#include "kernels.cuh"
+
+namespace lbib {
+
+size_t topo_scan_bytes(int n) {
+    size_t b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, n, (cudaStream_t)0);
+    return b;
+}
+
+// Perturbation tests of a new node (GeometryNode.cpp:160, 174, 189, 202).
+__device__ __forceinline__ bool new_node_needs_rng(double X, double Y) {
+    if (fabs((double)(int)X - X) <= kEPSILON) return true;
+    if (fabs((double)(int)Y - Y) <= kEPSILON) return true;
+    if (fabs(Y - floor(Y) - (X - floor(X))) <= kEPSILON) return true;
+    if (fabs(ceil(Y) - Y - (X - floor(X))) <= kEPSILON) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Remesh
+
+__global__ void remesh_flag_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > m.Ccap) return;
+    int f = 0;
+    if (!st->halt && c < m.topo->C) {
+        const int a = m.ca[c], b = m.cb[c];
+        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+        // Connection::getLength (Connection.cpp:389-394)
+        const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
+        if (len > kMAXLENGTH) {
+            f = 1;
+            if (new_node_needs_rng((x1 + x2) / 2, (y1 + y2) / 2)) atomicAdd(nRng, 1);
+        }
+    }
+    t.flag[c] = f;
+}
+
+// Decides the pass: K = number of splits; hands over to the host when the
+// pass would overflow a buffer, needs the random generator, or is a third one.
+__global__ void remesh_decide_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng, int lastPass) {
+    if (st->halt) return;
+    Topo* T = m.topo;
+    const int C = T->C;
+    const int K = t.rank[m.Ccap];  // exclusive scan over Ccap + 1 flags: the total
+    T->K = 0;
+    if (K == 0) return;
+    if (lastPass || *nRng > 0 || T->M + K > m.Mcap || C + K > m.Ccap) {
+        raise_halt(st, ST_REMESH);
+        return;
+    }
+    T->K = K;
+}
+
+__global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const Topo* T = m.topo;
+    const int K = T->K;
+    if (K == 0 || c >= T->C) return;
+    const int C = T->C, M = T->M;
+    const int r = t.rank[c];
+    if (!t.flag[c]) {
+        const int dst = c - r;
+        t.ca2[dst] = m.ca[c]; t.cb2[dst] = m.cb[c]; t.cdom2[dst] = m.cdom[c]; t.cdesc2[dst] = m.cdesc[c];
+        return;
+    }
+    const int a = m.ca[c], b = m.cb[c];
+    const int j = M + r;
+    const double x = (m.x[a] + m.x[b]) / 2, y = (m.y[a] + m.y[b]) / 2;
+    m.x[j] = x; m.y[j] = y;
+    m.ox[j] = x - 5.0; m.oy[j] = y - 5.0;   // GeometryNode.cpp:98-103
+    m.vx[j] = 0.0; m.vy[j] = 0.0; m.fx[j] = 0.0; m.fy[j] = 0.0;
+    m.id[j] = T->maxId + 1 + (unsigned)r;
+    m.next[a] = j; m.prev[j] = a; m.next[j] = b; m.prev[b] = j;
+    m.foff[j + 1] = m.foff[M];              // new nodes carry no forces
+    const int base = C - K + 2 * r;
+    t.ca2[base] = a; t.cb2[base] = j; t.cdom2[base] = m.cdom[c]; t.cdesc2[base] = m.cdesc[c];
+    t.ca2[base + 1] = j; t.cb2[base + 1] = b; t.cdom2[base + 1] = m.cdom[c]; t.cdesc2[base + 1] = m.cdesc[c];
+}
+
+__global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const Topo* T = m.topo;
+    if (T->K == 0 || c >= T->C + T->K) return;
+    m.ca[c] = t.ca2[c]; m.cb[c] = t.cb2[c]; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
+}
+
+__global__ void remesh_commit_kernel(MembraneDev m, Status* st) {
+    if (st->halt) return;
+    Topo* T = m.topo;
+    const int K = T->K;
+    if (K == 0) return;
+    T->M += K;
+    T->C += K;
+    T->maxId += K;
+    T->changed = 1;
+    T->K = 0;
+}
+
+// New nodes are bound to the lattice at once (GeometryHandler.cpp:427-428):
+// their old position is 5 lu away, so the edge test of
+// connectGeometryNodesToPhysicalNodes applies (GeometryHandler.cpp:618-636).
+__global__ void new_node_edge_kernel(MembraneDev m, int nx, int ny, Status* st, int from) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
+    const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
+    if (within) return;
+    if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
+    else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
+    else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
+    else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
+}
+
+int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
+    if (m.Ccap == 0) return 0;
+    int n = 0;
+    int* nRng = &st->pad[1];
+    const int cb = (m.Ccap + 1 + 255) / 256;
+    for (int pass = 0; pass < 3; ++pass) {
+        cudaMemsetAsync(nRng, 0, sizeof(int), s);
+        remesh_flag_kernel<<<cb, 256, 0, s>>>(m, t, st, nRng);
+        cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
+        remesh_decide_kernel<<<1, 1, 0, s>>>(m, t, st, nRng, pass == 2);
+        n += 4;
+        if (pass == 2) break;
+        remesh_apply_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
+        remesh_copy_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
+        remesh_commit_kernel<<<1, 1, 0, s>>>(m, st);
+        n += 3;
+    }
+    new_node_edge_kernel<<<(m.Mcap + 255) / 256, 256, 0, s>>>(m, nx, ny, st, 0);
+    return n + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Coarsen
+
+// Node -> its incoming / outgoing connection; node -> cell; candidates.
+__global__ void conn_links_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.topo->C) return;
+    t.outConn[m.ca[c]] = c;
+    t.inConn[m.cb[c]] = c;
+    t.connAlive[c] = 1;
+}
+
+__global__ void coarsen_cand_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    t.removed[i] = 0;
+    t.ncAlive[i] = 0;
+    const int p = m.prev[i], q = m.next[i];
+    const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
+    if (sqrt(dx * dx + dy * dy) < kMAXLENGTH) {
+        const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
+        atomicAdd(&t.cellCount[cell], 1);
+        atomicAdd(&m.topo->nCand, 1);
+    }
+}
+
+__global__ void coarsen_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt || m.topo->nCand == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const int p = m.prev[i], q = m.next[i];
+    const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
+    if (sqrt(dx * dx + dy * dy) < kMAXLENGTH) {
+        const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
+        const int k = atomicAdd(&t.cellFill[cell], 1);
+        t.members[t.cellStart[cell] + k] = i;
+    }
+}
+
+constexpr int kCoarsenLocal = 256;  // pending nodes per cell held by one thread
+
+// Handles: h < Ccap is connection index h; h >= Ccap is the connection made by
+// removing node h - Ccap.
+__global__ void coarsen_cell_kernel(MembraneDev m, TopoDev t, Status* st, int nCells) {
+    if (st->halt || m.topo->nCand == 0) return;
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= nCells) return;
+    const int b = t.cellStart[cell], cnt = t.cellCount[cell];
+    if (cnt == 0) return;
+    int pend[kCoarsenLocal];
+    int np = 0;
+    if (cnt > kCoarsenLocal) {
+        raise_error(st, ERR_CAPACITY, cell, ST_COARSEN);
+        return;
+    }
+    for (int k = 0; k < cnt; ++k) {
+        // insertion into the ascending pending list
+        const int v = t.members[b + k];
+        int j = np++;
+        while (j > 0 && pend[j - 1] > v) { pend[j] = pend[j - 1]; --j; }
+        pend[j] = v;
+    }
+    const int Ccap = m.Ccap;
+    int removedHere = 0;
+    int head = 0;
+    while (head < np) {
+        const int i = pend[head++];
+        if (t.removed[i]) continue;
+        const int p = m.prev[i], q = m.next[i];
+        const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
+        if (!(sqrt(dx * dx + dy * dy) < kMAXLENGTH)) continue;
+        t.removed[i] = 1;
+        ++removedHere;
+        const int hin = t.inConn[i], hout = t.outConn[i];
+        uint32_t dom;
+        int desc;
+        if (hin < Ccap) { t.connAlive[hin] = 0; dom = m.cdom[hin]; desc = m.cdesc[hin]; }
+        else { t.ncAlive[hin - Ccap] = 0; dom = t.ncDom[hin - Ccap]; desc = t.ncDesc[hin - Ccap]; }
+        if (hout < Ccap) t.connAlive[hout] = 0;
+        else t.ncAlive[hout - Ccap] = 0;
+        t.ncA[i] = p; t.ncB[i] = q; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
+        m.next[p] = q; m.prev[q] = p;
+        t.outConn[p] = Ccap + i; t.inConn[q] = Ccap + i;
+        // neighbours with a larger id get visited at their turn with the new links
+        const int nb[2] = {p, q};
+        for (int u = 0; u < 2; ++u) {
+            const int v = nb[u];
+            if (v <= i) continue;
+            bool present = false;
+            for (int k = head; k < np; ++k) if (pend[k] == v) { present = true; break; }
+            if (present) continue;
+            if (np >= kCoarsenLocal) {
+                raise_error(st, ERR_CAPACITY, cell, ST_COARSEN);
+                return;
+            }
+            int j = np++;
+            while (j > head && pend[j - 1] > v) { pend[j] = pend[j - 1]; --j; }
+            pend[j] = v;
+        }
+    }
+    if (removedHere) atomicAdd(&m.topo->removed, removedHere);
+}
+
+// Compaction flags: kept nodes; alive original connections; alive new ones.
+__global__ void coarsen_flags_kernel(MembraneDev m, TopoDev t, Status* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const Topo* T = m.topo;
+    if (i <= m.Mcap) t.nflag[i] = (!st->halt && T->removed && i < T->M && !t.removed[i]) ? 1 : 0;
+    if (i <= m.Ccap) t.flag[i] = (!st->halt && T->removed && i < T->C && t.connAlive[i]) ? 1 : 0;
+}
+
+// Gathers the kept nodes and the alive connections into the scratch copies.
+__global__ void coarsen_gather_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt || m.topo->removed == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int M = m.topo->M, C = m.topo->C;
+    if (i < M && !t.removed[i]) {
+        const int d = t.nrank[i];
+        double* a = t.dalt;
+        const size_t cap = (size_t)m.Mcap;
+        a[0 * cap + d] = m.x[i]; a[1 * cap + d] = m.y[i]; a[2 * cap + d] = m.ox[i]; a[3 * cap + d] = m.oy[i];
+        a[4 * cap + d] = m.vx[i]; a[5 * cap + d] = m.vy[i]; a[6 * cap + d] = m.fx[i]; a[7 * cap + d] = m.fy[i];
+        t.id2[d] = m.id[i];
+        t.prev2[d] = t.nrank[m.prev[i]];
+        t.next2[d] = t.nrank[m.next[i]];
+    }
+    const int Calive = t.rank[m.Ccap];
+    if (i < C && t.connAlive[i]) {
+        const int d = t.rank[i];
+        t.ca2[d] = t.nrank[m.ca[i]]; t.cb2[d] = t.nrank[m.cb[i]]; t.cdom2[d] = m.cdom[i]; t.cdesc2[d] = m.cdesc[i];
+    }
+    if (i < M && t.ncAlive[i]) {
+        // new connections follow the alive originals, in removal (= id) order
+        const int d = Calive + t.succ[i];
+        t.ca2[d] = t.nrank[t.ncA[i]]; t.cb2[d] = t.nrank[t.ncB[i]]; t.cdom2[d] = t.ncDom[i]; t.cdesc2[d] = t.ncDesc[i];
+    }
+}
+
+__global__ void coarsen_scatter_back_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt || m.topo->removed == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int M = m.topo->M, C = m.topo->C;
+    const int Mn = t.nrank[m.Mcap];
+    const int Cn = t.rank[m.Ccap] + t.succ[m.Mcap];
+    (void)C;
+    if (i < Mn) {
+        const double* a = t.dalt;
+        const size_t cap = (size_t)m.Mcap;
+        m.x[i] = a[0 * cap + i]; m.y[i] = a[1 * cap + i]; m.ox[i] = a[2 * cap + i]; m.oy[i] = a[3 * cap + i];
+        m.vx[i] = a[4 * cap + i]; m.vy[i] = a[5 * cap + i]; m.fx[i] = a[6 * cap + i]; m.fy[i] = a[7 * cap + i];
+        m.id[i] = t.id2[i]; m.prev[i] = t.prev2[i]; m.next[i] = t.next2[i];
+    }
+    if (i <= Mn) m.foff[i] = 0;  // the force list is empty at a coarsening step
+    if (i < Cn) { m.ca[i] = t.ca2[i]; m.cb[i] = t.cb2[i]; m.cdom[i] = t.cdom2[i]; m.cdesc[i] = t.cdesc2[i]; }
+}
+
+__global__ void coarsen_commit_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (st->halt) return;
+    Topo* T = m.topo;
+    if (T->removed == 0) { T->nCand = 0; return; }
+    const int Mn = t.nrank[m.Mcap];
+    T->M = Mn;
+    T->C = t.rank[m.Ccap] + t.succ[m.Mcap];
+    if (Mn > 0) T->maxId = m.id[Mn - 1];
+    T->changed = 1;
+    T->removed = 0;
+    T->nCand = 0;
+}
+
+// ncAlive as an int flag array for the scan of new connections
+__global__ void coarsen_ncflag_kernel(MembraneDev m, TopoDev t, Status* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m.Mcap) return;
+    t.dist[i] = (!st->halt && m.topo->removed && i < m.topo->M && t.ncAlive[i]) ? 1 : 0;
+}
+
+int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
+    const int nCells = t.nCellsCap;
+    if (m.Mcap == 0 || nCells == 0) return 0;
+    const int mb = (m.Mcap + 1 + 255) / 256, cbk = (m.Ccap + 1 + 255) / 256;
+    const int gb = ((m.Mcap > m.Ccap ? m.Mcap : m.Ccap) + 1 + 255) / 256;
+    cudaMemsetAsync(t.cellCount, 0, sizeof(int) * (nCells + 1), s);
+    cudaMemsetAsync(t.cellFill, 0, sizeof(int) * nCells, s);
+    conn_links_kernel<<<cbk, 256, 0, s>>>(m, t, st);
+    coarsen_cand_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.cellCount, t.cellStart, nCells + 1, s);
+    coarsen_fill_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    coarsen_cell_kernel<<<(nCells + 63) / 64, 64, 0, s>>>(m, t, st, nCells);
+    coarsen_flags_kernel<<<gb, 256, 0, s>>>(m, t, st);
+    coarsen_ncflag_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.nflag, t.nrank, m.Mcap + 1, s);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.dist, t.succ, m.Mcap + 1, s);
+    coarsen_gather_kernel<<<gb, 256, 0, s>>>(m, t, st);
+    coarsen_scatter_back_kernel<<<gb, 256, 0, s>>>(m, t, st);
+    coarsen_commit_kernel<<<1, 1, 0, s>>>(m, t, st);
+    return 17;
+}
+
+// ---------------------------------------------------------------------------
+// Rings
+
+__global__ void ring_first_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (!m.topo->changed) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.topo->C) return;
+    t.outConn[m.ca[c]] = c;
+    atomicMin(&t.firstConn[m.cdom[c]], c);
+}
+
+__global__ void ring_count_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (!m.topo->changed) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
+    atomicAdd(&t.cellCount[cell], 1);
+}
+
+__global__ void ring_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (!m.topo->changed) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const uint32_t d = m.cdom[t.outConn[i]];
+    const int cell = t.cellOfDom[d];
+    const int k = atomicAdd(&t.cellFill[cell], 1);
+    t.members[t.cellStart[cell] + k] = i;
+    const int start = m.cb[t.firstConn[d]];
+    // break the ring before its start node: the node whose successor is the start is last
+    t.succ[i] = m.next[i] == start ? -1 : m.next[i];
+    t.dist[i] = m.next[i] == start ? 0 : 1;
+}
+
+constexpr int kRingPerThread = 16;  // 256 threads x 16 = 4096 nodes per ring
+
+__global__ void __launch_bounds__(256) ring_rank_kernel(MembraneDev m, TopoDev t, Status* st) {
+    if (!m.topo->changed) return;
+    const int cell = blockIdx.x;
+    const int b = t.cellStart[cell], len = t.cellCount[cell];
+    if (len > 256 * kRingPerThread) {
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, cell, ST_BIO);
+        return;
+    }
+    int ns[kRingPerThread], nd[kRingPerThread];
+    for (int round = 0; (1 << round) < len; ++round) {
+        for (int k = 0; k < kRingPerThread; ++k) {
+            const int idx = threadIdx.x + k * 256;
+            if (idx >= len) break;
+            const int i = t.members[b + idx];
+            const int sc = t.succ[i];
+            if (sc >= 0) { nd[k] = t.dist[i] + t.dist[sc]; ns[k] = t.succ[sc]; }
+            else { nd[k] = t.dist[i]; ns[k] = -1; }
+        }
+        __syncthreads();
+        for (int k = 0; k < kRingPerThread; ++k) {
+            const int idx = threadIdx.x + k * 256;
+            if (idx >= len) break;
+            const int i = t.members[b + idx];
+            t.succ[i] = ns[k];
+            t.dist[i] = nd[k];
+        }
+        __syncthreads();
+    }
+    for (int k = 0; k < kRingPerThread; ++k) {
+        const int idx = threadIdx.x + k * 256;
+        if (idx >= len) break;
+        const int i = t.members[b + idx];
+        const int d = t.dist[i];
+        if (d >= 0 && d < len) m.ringNode[b + (len - 1 - d)] = i;
+        else raise_error(st, ERR_STATE, i, ST_BIO);
+    }
+    if (threadIdx.x == 0) m.ringStart[cell] = b;
+    if (threadIdx.x == 0 && cell == gridDim.x - 1) m.ringStart[cell + 1] = b + len;
+}
+
+__global__ void ring_done_kernel(MembraneDev m, TopoDev t) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < t.nDomains) t.firstConn[d] = 0x7fffffff;
+    if (d == 0) m.topo->changed = 0;
+}
+
+int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
+    const int nCells = t.nCellsCap;
+    if (m.Mcap == 0 || nCells == 0) return 0;
+    const int mb = (m.Mcap + 255) / 256, cbk = (m.Ccap + 255) / 256;
+    cudaMemsetAsync(t.cellCount, 0, sizeof(int) * (nCells + 1), s);
+    cudaMemsetAsync(t.cellFill, 0, sizeof(int) * nCells, s);
+    ring_first_kernel<<<cbk, 256, 0, s>>>(m, t, st);
+    ring_count_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.cellCount, t.cellStart, nCells + 1, s);
+    ring_fill_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    ring_rank_kernel<<<nCells, 256, 0, s>>>(m, t, st);
+    ring_done_kernel<<<(t.nDomains + 255) / 256, 256, 0, s>>>(m, t);
+    return 7;
+}
+
+}  // namespace lbib

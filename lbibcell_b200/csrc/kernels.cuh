@@ -5,10 +5,25 @@
 
 namespace lbib {
 
+// Membrane counts live in device memory: remeshing and coarsening change them
+// on the device, and kernels launched ahead of time size their work from here.
+struct Topo {
+    int M;            // membrane nodes
+    int C;            // connections
+    unsigned maxId;   // id of the last node (ids ascend with the index)
+    int changed;      // the topology changed: rings must be rebuilt
+    int K;            // connections split by the current remesh pass
+    int removed;      // nodes removed by the current coarsening
+    int nCand;        // coarsening candidates
+    int pad;
+};
+
 // Membrane state on the device (nodes in ascending id order).
 struct MembraneDev {
-    int M;          // membrane nodes
-    int C;          // connections
+    Topo* topo;     // device counts
+    int Mcap, Ccap; // capacities (launch grids)
+    int M;          // host view of the node count (valid after a pull)
+    int C;          // host view of the connection count
     double* x; double* y;       // LagrangianPoint::position_
     double* ox; double* oy;     // GeometryNode::oldPosition_
     double* vx; double* vy;     // LagrangianPoint::velocity_
@@ -17,6 +32,7 @@ struct MembraneDev {
     int* prev; int* next;       // ring neighbours (node indices)
     int* ca; int* cb;           // connection endpoints (node indices), vector order
     uint32_t* cdom;             // connection domain ids
+    int* cdesc;                 // connection boundary-descriptor index (host string table)
     // force records (CSR by node, insertion order)
     int* foff;                  // M+1
     int* ftype; int* fpartner;  // records
@@ -55,14 +71,40 @@ struct TileDev {
     size_t scanTmpBytes;
 };
 
+// Scratch of the device-side topology edits and the ring ranking.
+struct TopoDev {
+    int* flag;          // Ccap + 1
+    int* rank;          // Ccap + 1
+    int* nflag;         // Mcap + 1
+    int* nrank;         // Mcap + 1
+    int* ca2; int* cb2; uint32_t* cdom2; int* cdesc2;    // Ccap
+    double* dalt;       // 8 * Mcap node doubles
+    uint32_t* id2; int* prev2; int* next2;                // Mcap
+    int* inConn; int* outConn;                            // Mcap
+    unsigned char* removed;                               // Mcap
+    int* connAlive;                                       // Ccap
+    int* ncA; int* ncB; uint32_t* ncDom; int* ncDesc; int* ncAlive;  // Mcap
+    int nCellsCap;
+    int* cellOfDom;     // nDomains (cell index of a domain id, -1 none)
+    int* firstConn;     // nDomains
+    int* cellCount;     // nCells + 1
+    int* cellStart;     // nCells + 1
+    int* cellFill;      // nCells
+    int* members;       // Mcap
+    int* succ; int* dist;                                 // Mcap
+    int* startNode;     // nCells
+    void* scanTmp; size_t scanTmpBytes;
+    int nDomains;
+};
+
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s);
-void launch_outlet64(double* f, double* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
-void launch_init64(double* f, double* g, double* u, int S, size_t L, double tauF, const uint32_t* dom,
+void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
+void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s);
 
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s);
-void launch_outlet32(float* f, float* g, int S, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
-void launch_init32(float* f, float* g, float* u, int S, size_t L, double tauF, const uint32_t* dom,
+void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
+void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s);
 
 // Membrane pipeline.  `Real` is the lattice precision (velocity / force planes).
@@ -79,7 +121,7 @@ template <typename Real>
 void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, int nx, int ny, size_t L, Status* st,
                       unsigned iteration, cudaStream_t s);
 template <typename Real>
-void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int S, const SpeciesConst* sp,
+void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, const SpeciesConst* sp,
                    const double* srcTab, int nDomains, const uint32_t* ctypeTab, int cellTypesCopied, int nx,
                    int ny, size_t L, Status* st, unsigned iteration, cudaStream_t s);
 void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
@@ -92,5 +134,12 @@ void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double forc
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s);
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
+
+// Device-side topology edits (k_topology.cu).  Each returns the number of
+// kernels it launched.
+int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s);
+int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
+int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
+size_t topo_scan_bytes(int n);
 
 }  // namespace lbib

@@ -119,6 +119,8 @@ struct Handle {
 
     TileDev tiles{};
     CrossDev cross{};
+    TopoDev td{};
+    std::vector<std::string> descTable;  // boundary-descriptor strings of the connections
     Status* st = nullptr;
     Status* stHost = nullptr;
     cudaStream_t stream = nullptr;
@@ -158,6 +160,12 @@ Handle::~Handle() {
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.touched);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
+    fr(m.topo); fr(m.cdesc);
+    fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
+    fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
+    fr(td.connAlive); fr(td.ncA); fr(td.ncB); fr(td.ncDom); fr(td.ncDesc); fr(td.ncAlive); fr(td.cellOfDom);
+    fr(td.firstConn); fr(td.cellCount); fr(td.cellStart); fr(td.cellFill); fr(td.members); fr(td.succ);
+    fr(td.dist); fr(td.startNode); fr(td.scanTmp);
     fr(st);
     if (stHost) cudaFreeHost(stHost);
     if (evA) cudaEventDestroy(evA);
@@ -301,12 +309,15 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
     const int C = (int)h.conns.size();
     std::map<uint32_t, int> index;
     for (int i = 0; i < M; ++i) index[h.ids[i]] = i;
-    std::vector<int> ca(C), cb(C), prev(M, -1), next(M, -1);
+    std::vector<int> ca(C), cb(C), prev(M, -1), next(M, -1), cdesc(C);
     std::vector<uint32_t> cdom(C);
     for (int c = 0; c < C; ++c) {
         ca[c] = index.at(h.conns[c].id1);
         cb[c] = index.at(h.conns[c].id2);
         cdom[c] = h.conns[c].dom;
+        auto dt = std::find(h.descTable.begin(), h.descTable.end(), h.conns[c].desc);
+        if (dt == h.descTable.end()) { h.descTable.push_back(h.conns[c].desc); dt = h.descTable.end() - 1; }
+        cdesc[c] = (int)(dt - h.descTable.begin());
         next[ca[c]] = cb[c];
         prev[cb[c]] = ca[c];
     }
@@ -359,7 +370,8 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
         for (auto& kv : h.forcemap)
             if (!kv.second.empty() && !index.count(kv.first)) fail(ERR_FORCE_NODE, "Could not compute and set the forces.", kv.first);
     }
-    const int F = std::max((int)ftype.size(), 2 * M);
+    ensure_capacity(h, M, C, 1, cells);
+    const int F = std::max((int)ftype.size(), 2 * h.Mcap);
     ensure_capacity(h, M, C, F, cells);
     h.m.M = M;
     h.m.C = C;
@@ -378,6 +390,25 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
     up(h.m.ca, ca.data(), sizeof(int) * C);
     up(h.m.cb, cb.data(), sizeof(int) * C);
     up(h.m.cdom, cdom.data(), sizeof(uint32_t) * C);
+    up(h.m.cdesc, cdesc.data(), sizeof(int) * C);
+    {
+        // device counts, domain -> cell table, ring bookkeeping
+        Topo tp{};
+        tp.M = M; tp.C = C; tp.maxId = M ? h.ids.back() : 0u; tp.changed = 0;
+        up(h.m.topo, &tp, sizeof(Topo));
+        std::vector<int> cellOf(h.nDomains, -1);
+        for (int c = 0; c < cells; ++c)
+            if (ringDom[c] < (uint32_t)h.nDomains) cellOf[ringDom[c]] = c;
+        if (!h.td.cellOfDom) {
+            h.td.cellOfDom = dalloc<int>(h.nDomains);
+            h.td.firstConn = dalloc<int>(h.nDomains);
+            h.td.nDomains = h.nDomains;
+        }
+        up(h.td.cellOfDom, cellOf.data(), sizeof(int) * h.nDomains);
+        std::vector<int> big(h.nDomains, 0x7fffffff);
+        up(h.td.firstConn, big.data(), sizeof(int) * h.nDomains);
+        h.td.nCellsCap = cells;
+    }
     up(h.m.ringStart, ringStart.data(), sizeof(int) * ringStart.size());
     up(h.m.ringNode, ringNode.data(), sizeof(int) * ringNode.size());
     up(h.m.ringDom, ringDom.data(), sizeof(uint32_t) * cells);
@@ -398,6 +429,32 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
     CK(cudaStreamSynchronize(h.stream));
 }
 
+// Refreshes the host mirror of the topology (node ids, connection vector)
+// from the device, which edits it when remeshing and coarsening.
+static void pull_topology(Handle& h) {
+    Topo tp{};
+    CK(cudaMemcpyAsync(&tp, h.m.topo, sizeof(Topo), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    const int M = tp.M, C = tp.C;
+    std::vector<int> ca(C), cb(C), cdesc(C);
+    std::vector<uint32_t> cdom(C);
+    h.ids.resize(M);
+    if (M) CK(cudaMemcpyAsync(h.ids.data(), h.m.id, sizeof(uint32_t) * M, cudaMemcpyDeviceToHost, h.stream));
+    if (C) {
+        CK(cudaMemcpyAsync(ca.data(), h.m.ca, sizeof(int) * C, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(cb.data(), h.m.cb, sizeof(int) * C, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(cdom.data(), h.m.cdom, sizeof(uint32_t) * C, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(cdesc.data(), h.m.cdesc, sizeof(int) * C, cudaMemcpyDeviceToHost, h.stream));
+    }
+    CK(cudaStreamSynchronize(h.stream));
+    h.conns.resize(C);
+    for (int c = 0; c < C; ++c)
+        h.conns[c] = HConn{h.ids[ca[c]], h.ids[cb[c]], cdom[c],
+                           cdesc[c] >= 0 && cdesc[c] < (int)h.descTable.size() ? h.descTable[cdesc[c]] : std::string()};
+    h.m.M = M;
+    h.m.C = C;
+}
+
 // Copies the device's area targets to the host mirror (they are set on the
 // device by the first area-regulator call).
 static void sync_targets(Handle& h) {
@@ -408,7 +465,9 @@ static void sync_targets(Handle& h) {
 }
 
 static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
-    auto grow = [&](int need, int& cap) { if (need <= cap) return false; cap = std::max(need + need / 2, 64); return true; };
+    // headroom for remeshing on the device: node and connection buffers hold
+    // twice the current counts before the host has to grow them
+    auto grow = [&](int need, int& cap) { if (need <= cap) return false; cap = std::max(2 * need + 1024, 64); return true; };
     int oldM = h.Mcap;
     if (grow(M, h.Mcap)) {
         // membrane arrays are rewritten by every upload_topology; no copy needed
@@ -416,7 +475,20 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         fr(h.m.x); fr(h.m.y); fr(h.m.ox); fr(h.m.oy); fr(h.m.vx); fr(h.m.vy); fr(h.m.fx); fr(h.m.fy);
         fr(h.m.id); fr(h.m.prev); fr(h.m.next); fr(h.outPos); fr(h.inPos); fr(h.cross.perturbList);
         fr(h.m.foff); fr(h.m.ringNode); fr(h.tiles.list);
+        fr(h.td.nflag); fr(h.td.nrank); fr(h.td.dalt); fr(h.td.id2); fr(h.td.prev2); fr(h.td.next2);
+        fr(h.td.inConn); fr(h.td.outConn); fr(h.td.removed); fr(h.td.ncA); fr(h.td.ncB); fr(h.td.ncDom);
+        fr(h.td.ncDesc); fr(h.td.ncAlive); fr(h.td.members); fr(h.td.succ); fr(h.td.dist);
         const int n = h.Mcap;
+        h.td.nflag = dalloc<int>(n + 1); h.td.nrank = dalloc<int>(n + 1);
+        h.td.dalt = dalloc<double>(8 * (size_t)n);
+        h.td.id2 = dalloc<uint32_t>(n); h.td.prev2 = dalloc<int>(n); h.td.next2 = dalloc<int>(n);
+        h.td.inConn = dalloc<int>(n); h.td.outConn = dalloc<int>(n);
+        h.td.removed = dalloc<unsigned char>(n);
+        CK(cudaMemsetAsync(h.td.removed, 0, n, h.stream));
+        h.td.ncA = dalloc<int>(n); h.td.ncB = dalloc<int>(n); h.td.ncDom = dalloc<uint32_t>(n);
+        h.td.ncDesc = dalloc<int>(n); h.td.ncAlive = dalloc<int>(n + 1);
+        CK(cudaMemsetAsync(h.td.ncAlive, 0, sizeof(int) * (n + 1), h.stream));
+        h.td.members = dalloc<int>(n); h.td.succ = dalloc<int>(n + 1); h.td.dist = dalloc<int>(n + 1);
         h.m.x = dalloc<double>(n); h.m.y = dalloc<double>(n); h.m.ox = dalloc<double>(n); h.m.oy = dalloc<double>(n);
         h.m.vx = dalloc<double>(n); h.m.vy = dalloc<double>(n); h.m.fx = dalloc<double>(n); h.m.fy = dalloc<double>(n);
         h.m.id = dalloc<uint32_t>(n); h.m.prev = dalloc<int>(n); h.m.next = dalloc<int>(n);
@@ -433,9 +505,14 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.cross.touched); fr(h.cross.changedNode); fr(h.cross.changedDom);
+        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.touched); fr(h.cross.changedNode);
+        fr(h.cross.changedDom);
+        fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
         const int n = h.Ccap;
-        h.m.ca = dalloc<int>(n); h.m.cb = dalloc<int>(n); h.m.cdom = dalloc<uint32_t>(n);
+        h.m.ca = dalloc<int>(n); h.m.cb = dalloc<int>(n); h.m.cdom = dalloc<uint32_t>(n); h.m.cdesc = dalloc<int>(n);
+        h.td.flag = dalloc<int>(n + 1); h.td.rank = dalloc<int>(n + 1);
+        h.td.ca2 = dalloc<int>(n); h.td.cb2 = dalloc<int>(n); h.td.cdom2 = dalloc<uint32_t>(n);
+        h.td.cdesc2 = dalloc<int>(n); h.td.connAlive = dalloc<int>(n);
         // each connection of length <= MAXLENGTH crosses at most one line per axis
         // (two records each); longer ones exist only between the move and the remesh
         h.cross.touchedCap = 16 * n + 1024;
@@ -452,9 +529,21 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     if (grow(cells, h.cellCap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(h.m.ringStart); fr(h.m.ringDom); fr(h.area); fr(h.target);
+        fr(h.td.cellCount); fr(h.td.cellStart); fr(h.td.cellFill); fr(h.td.startNode);
         h.m.ringStart = dalloc<int>(h.cellCap + 1); h.m.ringDom = dalloc<uint32_t>(h.cellCap);
         h.area = dalloc<double>(h.cellCap); h.target = dalloc<double>(h.cellCap);
+        h.td.cellCount = dalloc<int>(h.cellCap + 1); h.td.cellStart = dalloc<int>(h.cellCap + 1);
+        h.td.cellFill = dalloc<int>(h.cellCap); h.td.startNode = dalloc<int>(h.cellCap);
     }
+    // scan scratch for the largest scan (nodes, connections or cells)
+    const size_t need = topo_scan_bytes(std::max(std::max(h.Mcap, h.Ccap), h.cellCap) + 1);
+    if (need > h.td.scanTmpBytes) {
+        if (h.td.scanTmp) cudaFree(h.td.scanTmp);
+        CK(cudaMalloc(&h.td.scanTmp, need));
+        h.td.scanTmpBytes = need;
+    }
+    h.m.Mcap = h.Mcap;
+    h.m.Ccap = h.Ccap;
 }
 
 // ---------------------------------------------------------------------------
@@ -667,16 +756,16 @@ static void launch_stages(Handle& h, unsigned iteration, int parity, int fromSta
     cudaStream_t s = h.stream;
     Real* fcur = (Real*)h.f[1 - parity];
     Real* gcur = (Real*)h.g[1 - parity];
-    const bool hasM = h.m.M > 0;
-    long long& k = h.launches;
+    const bool hasM = h.m.Mcap > 0;
+    long long& nl = h.launches;
     if (fromStage <= ST_FORCE) {
         step_begin_kernel<<<1, 1, 0, s>>>(h.st);
         launch_force_eval<Real>(h.m, h.st, iteration, s);
-        k += 1 + hasM;
+        nl += 1 + hasM;
     }
     if (fromStage <= ST_SPREAD) {
         launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, iteration, s);
-        k += hasM ? 5 : 0;
+        nl += hasM ? 5 : 0;
     }
     if (fromStage <= ST_COLLIDE) {
         if (evCollideA) cudaEventRecord(evCollideA, s);
@@ -688,19 +777,19 @@ static void launch_stages(Handle& h, unsigned iteration, int parity, int fromSta
             launch_stream_collide32(a, s);
         }
         if (evCollideB) cudaEventRecord(evCollideB, s);
-        k += 1;
+        nl += 1;
     }
     if (fromStage <= ST_INTERP_MOVE) {
         launch_interp_move<Real>(h.m, (const Real*)h.u, h.nx, h.ny, h.L, h.cross, h.st, iteration, s);
-        k += hasM;
+        nl += hasM;
     }
     if (fromStage <= ST_PERTURB_CONN) {
         launch_perturb_conn_check(h.m, h.st, iteration, s);
-        k += hasM;
+        nl += hasM;
     }
     if (fromStage <= ST_CROSSINGS) {
         launch_crossings<Real>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
-        k += hasM ? 4 : 0;
+        nl += hasM ? 4 : 0;
     }
     if (fromStage <= ST_REINIT) {
         SpeciesConst spc[kMaxSpecies] = {};
@@ -708,41 +797,39 @@ static void launch_stages(Handle& h, unsigned iteration, int parity, int fromSta
         const int copied = (h.cellTypesCopied || !firstStepOfRun) ? 1 : 0;
         launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, copied,
                             h.nx, h.ny, h.L, h.st, iteration, s);
-        k += 1;
+        nl += 1;
     }
     if (fromStage <= ST_DOMAIN) {
         launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
         launch_cross_clear(h.cross, h.st, s);
-        k += 2;
+        nl += 2;
     }
-    if (fromStage <= ST_REMESH) {
-        launch_remesh_check(h.st, iteration, s);
-        k += 1;
-    }
+    if (fromStage <= ST_REMESH) nl += launch_remesh(h.m, h.td, h.nx, h.ny, h.st, s);
     if (fromStage <= ST_COARSEN && iteration % 10 == 0) {
+        // SimulationRunner.cpp:84-87: ForceSolver::deleteAllForces, then coarsenBoundary
         launch_clear_forces(h.m, s);
-        launch_coarsen_check(h.m, h.st, iteration, s);
-        k += 1 + hasM;
+        nl += 1 + launch_coarsen(h.m, h.td, h.st, s);
     }
     if (fromStage <= ST_OUTLET && h.outlet) {
         if (sizeof(Real) == 8) launch_outlet64((double*)fcur, (double*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
         else launch_outlet32((float*)fcur, (float*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
-        k += 1;
+        nl += 1;
     }
     if (fromStage <= ST_BIO) {
+        nl += launch_rings(h.m, h.td, h.st, s);
         for (int b : h.bio) {
             if (b == 2) {
                 launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor, h.areaStrength,
                                       h.areaMax, h.st, s);
-                k += h.m.nCells > 0 ? 2 : 0;
+                nl += h.m.nCells > 0 ? 2 : 0;
             } else if (b == 1 && iteration % h.tensionFreq == 0) {
                 launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
-                k += hasM ? 2 : 0;
+                nl += hasM ? 2 : 0;
             }
         }
     }
     step_end_kernel<<<1, 1, 0, s>>>(h.st);
-    k += 1;
+    nl += 1;
 }
 
 // The stage the host resumes at after handling the halt of `stage`.
@@ -840,6 +927,7 @@ static void run_steps(Handle& h, int n) {
         const unsigned it = h.iteration;
         const int parity = h.cur;
         h.hostEvents++;
+        pull_topology(h);
         HostMembrane hm;
         if (stage == ST_INTERP_MOVE) {
             // positions that need GeometryNode::perturbatePosition, in id order
@@ -921,6 +1009,7 @@ static void run_steps(Handle& h, int n) {
             // a further halt inside the resumed step
             const int stage2 = -fromStage;
             h.hostEvents++;
+            pull_topology(h);
             HostMembrane hm2;
             if (stage2 == ST_PERTURB_CONN) {
                 download_membrane(h, hm2);
@@ -1034,6 +1123,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.cross.bnDist, 0xff, sizeof(unsigned long long) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.bnConn, 0xff, sizeof(uint32_t) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.wDom, 0, sizeof(uint32_t) * h.L, h.stream));
+
+    h.m.topo = dalloc<Topo>(1);
 
     // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160); each new
     // GeometryNode runs perturbatePosition (GeometryNode.cpp:98-117).
@@ -1270,6 +1361,13 @@ int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
 int lbib_get_sizes(lbib_handle* hh, long long* s) {
     if (!hh || !s) return LBIB_ERR_STATE;
     Handle& h = hh->h;
+    if (!h.err) {
+        try {
+            lbib::pull_topology(h);
+        } catch (const HostFail& e) {
+            h.err = e.code; h.msg = e.msg;
+        }
+    }
     s[0] = h.nx; s[1] = h.ny; s[2] = h.S; s[3] = (long long)h.ids.size(); s[4] = (long long)h.conns.size();
     s[5] = h.iteration; s[6] = h.precision; s[7] = h.hostEvents; s[8] = h.stepsDone; s[9] = h.m.nCells;
     return LBIB_OK;
@@ -1385,6 +1483,7 @@ int lbib_upload_lattice(lbib_handle* hh, const double* f, const double* g, const
 
 int lbib_download_membrane(lbib_handle* hh, unsigned* ids, double* state) {
     API_BEGIN(hh)
+    lbib::pull_topology(h);
     lbib::HostMembrane hm;
     lbib::download_membrane(h, hm);
     for (size_t i = 0; i < h.ids.size(); ++i) {
@@ -1399,6 +1498,7 @@ int lbib_download_membrane(lbib_handle* hh, unsigned* ids, double* state) {
 
 int lbib_download_connections(lbib_handle* hh, unsigned* conn) {
     API_BEGIN(hh)
+    lbib::pull_topology(h);
     for (size_t c = 0; c < h.conns.size(); ++c) {
         conn[3 * c] = h.conns[c].id1; conn[3 * c + 1] = h.conns[c].id2; conn[3 * c + 2] = h.conns[c].dom;
     }
