@@ -194,8 +194,13 @@ def config2(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> 
     sec = sorted(rng.choice(doms, size=k, replace=False).tolist())
     species = [Species(SPECIES_NAMES[0], 0.8, source={d: 1e-3 for d in sec}),
                Species(SPECIES_NAMES[1], 1.2, source={d: 1e-3 for d in sec})]
+    # Cells of radius up to 22 on a 44 lu grid already touch; a growth target
+    # would press neighbours into each other (and the reference's species
+    # re-initialisation divides by zero for nodes trapped between two
+    # membranes, CDESolverD2Q5.cpp:223).  The area regulator holds each cell's
+    # initial area here.
     return Config(name="tissue_1024", nx=1024, ny=1024, tau_fluid=1.0, iterations=iterations,
-                  report_step=report_step, cells=cells, species=species)
+                  report_step=report_step, cells=cells, species=species, area=(1.0, 0.01, 0.004))
 
 
 def poisson_tissue(nx: int, ny: int, rmin: float, rmax: float, spacing: float, seed: int,

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         const float tI = (float)(1.0 / a.sp[k].tau);
         float src = 0.0f;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = (float)a.srcTab[(size_t)k * a.nDomains + dom];
-        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, a.iteration, C);
+        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, a.status->iteration, C);
         const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
         const float e0 = C * (1.0f / 3.0f), e1 = C * (1.0f / 6.0f);
         float* go = a.gout + (size_t)k * 5 * L;

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         g[S] = gin[4 * L + rP + x];
         double src = 0.0;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
-        collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.iteration);
+        collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.status->iteration);
         double* gout = a.gout + (size_t)k * 5 * L;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gout[q * L + n] = g[q];

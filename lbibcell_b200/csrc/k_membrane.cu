@@ -204,6 +204,7 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
 }
 
 constexpr int kSpreadMax = 1024;  // membrane stencils per tile held in shared memory
+constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(Stencil) + sizeof(int));
 
 template <typename Real>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
@@ -251,15 +252,21 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int x = tx * kTile + (threadIdx.x & 15), y = ty * kTile + (threadIdx.x >> 4);
-    if (x >= nx || y >= ny) return;
+    const bool inside = x < nx && y < ny;
     double ax = 0.0, ay = 0.0;
+    // a warp covers two rows of the tile: entries whose stencil rows miss
+    // both are skipped by a warp-uniform test
+    const int yA = ty * kTile + ((threadIdx.x >> 5) << 1);
     for (int k = 0; k < cnt; ++k) {
-        if (in_stencil(sst[k], x, y)) {
+        const Stencil sc = sst[k];
+        if (sc.y1 < yA || sc.y0 > yA + 1) continue;
+        if (in_stencil(sc, x, y)) {
             const double dl = dirac((double)x - sx[k], (double)y - sy[k]);
             ax += sfx[k] * dl;
             ay += sfy[k] * dl;
         }
     }
+    if (!inside) return;
     const size_t n = (size_t)y * nx + x;
     force[n] = (Real)ax;
     force[L + n] = (Real)ay;
@@ -275,12 +282,7 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
-    constexpr size_t smemBytes = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(Stencil) + sizeof(int));
-    static bool attrSet = false;
-    if (!attrSet) {
-        cudaFuncSetAttribute(spread_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
-        attrSet = true;
-    }
+    constexpr size_t smemBytes = kSpreadSmem;
     spread_kernel<Real><<<t.nTiles, 256, smemBytes, s>>>(m, t, force, nx, ny, L, st);
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
@@ -382,9 +384,11 @@ __device__ __forceinline__ int slot_code(int d) {  // E,N,W,S -> 0..3
     return d - 1;
 }
 
-__device__ __forceinline__ void cross_record(const CrossDev& c, const uint32_t* dom, Status* st, int pass,
-                                             int conn, int nx, int ny, int px, int py, int dirSlot, double bx,
-                                             double by, uint32_t bdom) {
+// Pass 0, per crossing: closest distance by atomicMin; the record is kept
+// for passes 1 and 2; the first writer of a (node, slot) key lists it for
+// the reset at the end of the step.
+__device__ __forceinline__ void cross_record(const CrossDev& c, Status* st, int conn, int nx, int ny, int px,
+                                             int py, int dirSlot, double bx, double by, uint32_t bdom) {
     if (px < 0 || py < 0 || px >= nx || py >= ny) {
         raise_error(st, ERR_EDGE_W, conn, ST_CROSSINGS);
         return;
@@ -392,39 +396,22 @@ __device__ __forceinline__ void cross_record(const CrossDev& c, const uint32_t* 
     const size_t node = (size_t)py * nx + px;
     const double d2 = ((double)px - bx) * ((double)px - bx) + ((double)py - by) * ((double)py - by);
     const unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
-    const size_t key = node * 4 + slot_code(dirSlot);
-    if (pass == 0) {
-        const unsigned long long old = atomicMin(&c.bnDist[key], bits);
-        if (old == kEmpty) {
-            const int k = atomicAdd(&st->nRecords, 1);
-            if (k < c.touchedCap) c.touched[k] = (uint32_t)key;
-            else raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
-        }
-    } else if (pass == 1) {
-        if (c.bnDist[key] == bits) atomicMin(&c.bnConn[key], (uint32_t)conn);
+    const uint32_t key = (uint32_t)(node * 4 + slot_code(dirSlot));
+    const unsigned long long old = atomicMin(&c.bnDist[key], bits);
+    if (old == kEmpty) {
+        const int k = atomicAdd(&st->nRecords, 1);
+        if (k < c.touchedCap) c.touched[k] = key;
+        else raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
+    }
+    const int r = atomicAdd(&st->pad[2], 1);
+    if (r < c.recCap) {
+        c.recKey[r] = key; c.recConn[r] = (uint32_t)conn; c.recDom[r] = bdom; c.recDist[r] = bits;
     } else {
-        if (c.bnDist[key] == bits && c.bnConn[key] == (uint32_t)conn) {
-            c.bnDom[key] = bdom;
-            const int s = slot_code(dirSlot);
-            if (s == 2) c.wDom[node] = bdom + 1;
-            bool last = true;
-            for (int s2 = s + 1; s2 < 4; ++s2)
-                if (c.bnDist[node * 4 + s2] != kEmpty) last = false;
-            if (last && bdom != dom[node]) {
-                const int k = atomicAdd(&st->nChanged, 1);
-                if (k < c.changedCap) {
-                    c.changedNode[k] = (uint32_t)node;
-                    c.changedDom[k] = bdom;
-                } else {
-                    raise_error(st, ERR_CAPACITY, (int)node, ST_CROSSINGS);
-                }
-            }
-        }
+        raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
     }
 }
 
-__global__ void crossings_kernel(MembraneDev m, CrossDev c, const uint32_t* dom, int nx, int ny, Status* st,
-                                 int pass) {
+__global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Status* st) {
     if (st->halt) return;
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
     if (cn >= m.topo->C) return;
@@ -444,22 +431,57 @@ __global__ void crossings_kernel(MembraneDev m, CrossDev c, const uint32_t* dom,
         raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
         return;
     }
-    if (pass == 0) {
-        const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
-        if (len > kMAXLENGTH) st->remesh = 1;
-    }
     const bool eastward = x1 < x2, southward = y1 > y2;
     for (int i = (int)ceil(minX); i <= (int)floor(maxX); i++) {
         const double yc = mm * i + nn;
         // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
-        cross_record(c, dom, st, pass, cn, nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D);
-        cross_record(c, dom, st, pass, cn, nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u);
+        cross_record(c, st, cn, nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D);
+        cross_record(c, st, cn, nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u);
     }
     for (int i = (int)ceil(minY); i <= (int)floor(maxY); i++) {
         const double xc = (i - nn) / mm;
         // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
-        cross_record(c, dom, st, pass, cn, nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D);
-        cross_record(c, dom, st, pass, cn, nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u);
+        cross_record(c, st, cn, nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D);
+        cross_record(c, st, cn, nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u);
+    }
+}
+
+// Pass 1: among records at the closest distance, the earliest connection.
+__global__ void cross_tie_kernel(CrossDev c, Status* st) {
+    if (st->halt) return;
+    const int n = min(st->pad[2], c.recCap);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t key = c.recKey[r];
+        if (c.bnDist[key] == c.recDist[r]) atomicMin(&c.bnConn[key], c.recConn[r]);
+    }
+}
+
+// Pass 2: the winner writes its domain; the winner of a node's last present
+// slot (order E,N,W,S = the reference's boundaryNodes_ scan order) decides the
+// node's tentative domain (PhysicalNode.cpp:111-115).
+__global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
+    if (st->halt) return;
+    const int n = min(st->pad[2], c.recCap);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t key = c.recKey[r];
+        if (c.bnDist[key] != c.recDist[r] || c.bnConn[key] != c.recConn[r]) continue;
+        const uint32_t bdom = c.recDom[r];
+        const size_t node = key >> 2;
+        const int s = (int)(key & 3u);
+        c.bnDom[key] = bdom;
+        if (s == 2) c.wDom[node] = bdom + 1;
+        bool last = true;
+        for (int s2 = s + 1; s2 < 4; ++s2)
+            if (c.bnDist[node * 4 + s2] != kEmpty) last = false;
+        if (last && bdom != dom[node]) {
+            const int k = atomicAdd(&st->nChanged, 1);
+            if (k < c.changedCap) {
+                c.changedNode[k] = (uint32_t)node;
+                c.changedDom[k] = bdom;
+            } else {
+                raise_error(st, ERR_CAPACITY, (int)node, ST_CROSSINGS);
+            }
+        }
     }
 }
 
@@ -484,7 +506,10 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
                       unsigned iteration, cudaStream_t s) {
     if (m.Ccap == 0) return;
     const int blocks = (m.Ccap + 127) / 128;
-    for (int pass = 0; pass < 3; ++pass) crossings_kernel<<<blocks, 128, 0, s>>>(m, c, dom, nx, ny, st, pass);
+    cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
+    crossings_kernel<<<blocks, 128, 0, s>>>(m, c, nx, ny, st);
+    cross_tie_kernel<<<296, 256, 0, s>>>(c, st);
+    cross_win_kernel<<<296, 256, 0, s>>>(c, dom, st);
     edge_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_CROSSINGS);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
@@ -507,7 +532,8 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 // state.  Here one block sorts the changed nodes, records for each the earlier
 // changed nodes among its E,N,W,S,NE (read after write) and SW (write after
 // read) neighbours, and processes nodes in rounds once those are done.
-constexpr int kReinitMax = 1024;
+constexpr int kReinitMax = 4096;  // changed nodes per step (dynamic shared memory)
+constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1);
 
 template <typename Real>
 __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int nS,
@@ -581,9 +607,10 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         return;
     }
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
-    __shared__ unsigned long long key[kReinitMax];  // node << 32 | newDom
-    __shared__ int deps[kReinitMax][6];
-    __shared__ unsigned char done[kReinitMax];
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* key = (unsigned long long*)smem;  // node << 32 | newDom
+    int(*deps)[6] = (int(*)[6])(key + kReinitMax);
+    unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
     int p2 = 1;
     while (p2 < cnt) p2 <<= 1;
@@ -642,7 +669,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
             if (done[k] == 2) {
                 reinit_node<Real>((size_t)(key[k] >> 32), (uint32_t)(key[k] & 0xffffffffu), dom, g, u, nS, sp, srcTab,
-                                  nDomains, ctypeTab, cellTypesCopied, c, nx, ny, L, st, iteration);
+                                  nDomains, ctypeTab, st->cellTypesCopied, c, nx, ny, L, st, st->iteration);
                 atomicAdd(&nowDone, 1);
             }
         }
@@ -660,7 +687,8 @@ void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, c
                    const double* srcTab, int nDomains, const uint32_t* ctypeTab, int cellTypesCopied, int nx, int ny,
                    size_t L, Status* st, unsigned iteration, cudaStream_t s) {
     if (c.changedCap <= 0) return;
-    reinit_kernel<Real><<<1, 1024, 0, s>>>(c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
+    constexpr size_t smemBytes = kReinitSmem;
+    reinit_kernel<Real><<<1, 1024, smemBytes, s>>>(c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
                                            cellTypesCopied, nx, ny, L, st, iteration);
 }
 template void launch_reinit<double>(CrossDev&, uint32_t*, double*, const double*, int, const SpeciesConst*,
@@ -707,14 +735,15 @@ __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* 
     }
 }
 
-// Resets the (node, slot) entries this step wrote.
+// Resets the (node, slot) entries this step wrote (grid-stride over the
+// step's count, which lives on the device).
 __global__ void cross_clear_kernel(CrossDev c, Status* st) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = min(st->nRecords, c.touchedCap);
-    if (k >= n) return;
-    const uint32_t key = c.touched[k];
-    c.bnDist[key] = kEmpty;
-    c.bnConn[key] = ~0u;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t key = c.touched[k];
+        c.bnDist[key] = kEmpty;
+        c.bnConn[key] = ~0u;
+    }
 }
 
 void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
@@ -724,7 +753,7 @@ void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, St
 
 void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s) {
     if (c.touchedCap <= 0) return;
-    cross_clear_kernel<<<(c.touchedCap + 255) / 256, 256, 0, s>>>(c, st);
+    cross_clear_kernel<<<296, 256, 0, s>>>(c, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -803,18 +832,31 @@ void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double forc
 // ---------------------------------------------------------------------------
 // Areas (GeometryHandler::computeAreas, shoelace in ring order) and the
 // LbibAreaRegulator mass source per domain.
-__global__ void areas_kernel(MembraneDev m, double* area) {
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= m.nCells) return;
+// One block per cell: the terms x_i y_j - x_j y_i are formed in parallel;
+// one thread adds them in ring order (the summation order of the shoelace
+// sum is part of the result).
+constexpr int kAreaMax = 4096;
+
+__global__ void __launch_bounds__(256) areas_kernel(MembraneDev m, double* area, Status* st) {
+    const int cell = blockIdx.x;
     const int b = m.ringStart[cell], e = m.ringStart[cell + 1];
     const int np = e - b;
-    double sum = 0.0;
-    for (int k = 0; k < np; ++k) {
+    __shared__ double terms[kAreaMax];
+    if (np > kAreaMax) {
+        if (threadIdx.x == 0 && st) raise_error(st, ERR_CAPACITY, cell, ST_BIO);
+        return;
+    }
+    for (int k = threadIdx.x; k < np; k += blockDim.x) {
         const int i = m.ringNode[b + k];
         const int j = m.ringNode[b + (k + 1 == np ? 0 : k + 1)];
-        sum += m.x[i] * m.y[j] - m.x[j] * m.y[i];
+        terms[k] = m.x[i] * m.y[j] - m.x[j] * m.y[i];
     }
-    area[cell] = sum / 2.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int k = 0; k < np; ++k) sum += terms[k];
+        area[cell] = sum / 2.0;
+    }
 }
 
 __global__ void area_regulator_kernel(MembraneDev m, const double* area, double* target, double* massTab,
@@ -835,15 +877,27 @@ __global__ void area_regulator_kernel(MembraneDev m, const double* area, double*
 
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
     if (m.nCells == 0) return;
-    areas_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area);
+    areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, nullptr);
 }
 
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
-    areas_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area);
+    areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, (Status*)st);
     area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
                                                                  strength, maxsource, st);
+}
+
+}  // namespace lbib
+
+namespace lbib {
+
+void init_kernel_attributes() {
+    cudaFuncSetAttribute(spread_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpreadSmem);
+    cudaFuncSetAttribute(spread_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpreadSmem);
+    cudaFuncSetAttribute(reinit_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
+    cudaFuncSetAttribute(reinit_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
+    init_kernel_attributes_topology();
 }
 
 }  // namespace lbib

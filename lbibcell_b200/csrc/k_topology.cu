@@ -44,6 +44,26 @@ __device__ __forceinline__ bool new_node_needs_rng(double X, double Y) {
     return false;
 }
 
+// Warp-aggregated atomics: lanes with the same key share one atomic.
+__device__ __forceinline__ int agg_add(int* addr, int key) {
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(addr, __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    return base + __popc(grp & ((1u << lane) - 1u));
+}
+
+// Minimum of v per key, where v increases with the lane (a warp's
+// connection indices): the group's lowest lane holds the group's minimum.
+__device__ __forceinline__ void agg_min(int* addr, int key, int v) {
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, key);
+    if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicMin(addr, v);
+}
+
 // ---------------------------------------------------------------------------
 // Remesh
 
@@ -143,25 +163,32 @@ __global__ void new_node_edge_kernel(MembraneDev m, int nx, int ny, Status* st, 
     else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
 }
 
+// After the device pass: a connection still longer than MAXLENGTH (a split
+// half of one longer than 2 * MAXLENGTH) needs another pass; that rare case
+// goes to the host, which repeats passes like SimulationRunner.cpp:190-199.
+__global__ void remesh_again_kernel(MembraneDev m, Status* st) {
+    if (st->halt) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.topo->C) return;
+    const int a = m.ca[c], b = m.cb[c];
+    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+    if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
+}
+
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
     if (m.Ccap == 0) return 0;
-    int n = 0;
     int* nRng = &st->pad[1];
     const int cb = (m.Ccap + 1 + 255) / 256;
-    for (int pass = 0; pass < 3; ++pass) {
-        cudaMemsetAsync(nRng, 0, sizeof(int), s);
-        remesh_flag_kernel<<<cb, 256, 0, s>>>(m, t, st, nRng);
-        cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
-        remesh_decide_kernel<<<1, 1, 0, s>>>(m, t, st, nRng, pass == 2);
-        n += 4;
-        if (pass == 2) break;
-        remesh_apply_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
-        remesh_copy_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
-        remesh_commit_kernel<<<1, 1, 0, s>>>(m, st);
-        n += 3;
-    }
+    cudaMemsetAsync(nRng, 0, sizeof(int), s);
+    remesh_flag_kernel<<<cb, 256, 0, s>>>(m, t, st, nRng);
+    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
+    remesh_decide_kernel<<<1, 1, 0, s>>>(m, t, st, nRng, 0);
+    remesh_apply_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
+    remesh_copy_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
+    remesh_commit_kernel<<<1, 1, 0, s>>>(m, st);
+    remesh_again_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, st);
     new_node_edge_kernel<<<(m.Mcap + 255) / 256, 256, 0, s>>>(m, nx, ny, st, 0);
-    return n + 1;
+    return 9;
 }
 
 // ---------------------------------------------------------------------------
@@ -185,88 +212,123 @@ __global__ void coarsen_cand_kernel(MembraneDev m, TopoDev t, Status* st) {
     t.ncAlive[i] = 0;
     const int p = m.prev[i], q = m.next[i];
     const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
-    if (sqrt(dx * dx + dy * dy) < kMAXLENGTH) {
-        const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
-        atomicAdd(&t.cellCount[cell], 1);
-        atomicAdd(&m.topo->nCand, 1);
-    }
+    const bool cand = sqrt(dx * dx + dy * dy) < kMAXLENGTH;
+    const unsigned bal = __ballot_sync(__activemask(), cand);
+    if (cand && (threadIdx.x & 31) == __ffs(bal) - 1) atomicAdd(&m.topo->nCand, __popc(bal));
 }
 
-__global__ void coarsen_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
-    if (st->halt || m.topo->nCand == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.topo->M) return;
-    const int p = m.prev[i], q = m.next[i];
-    const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
-    if (sqrt(dx * dx + dy * dy) < kMAXLENGTH) {
-        const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
-        const int k = atomicAdd(&t.cellFill[cell], 1);
-        t.members[t.cellStart[cell] + k] = i;
-    }
-}
+constexpr int kCoarsenMax = 2048;  // nodes of one ring held in shared memory
+constexpr size_t kCoarsenSmem = (size_t)kCoarsenMax * (2 * sizeof(double) + sizeof(unsigned long long) +
+                                                       5 * sizeof(int) + 2);
 
-constexpr int kCoarsenLocal = 256;  // pending nodes per cell held by one thread
-
+// One block per cell.  The ring (in ring order, rebuilt just before) is
+// loaded into shared memory as a circular list; thread 0 then visits the
+// ring's nodes in id order like GeometryHandler::coarsenBoundary, testing
+// only nodes whose span is short at the start or whose neighbour was removed
+// (every other node keeps a span >= MAXLENGTH and stays).
 // Handles: h < Ccap is connection index h; h >= Ccap is the connection made by
 // removing node h - Ccap.
-__global__ void coarsen_cell_kernel(MembraneDev m, TopoDev t, Status* st, int nCells) {
+__global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDev t, Status* st) {
     if (st->halt || m.topo->nCand == 0) return;
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= nCells) return;
-    const int b = t.cellStart[cell], cnt = t.cellCount[cell];
-    if (cnt == 0) return;
-    int pend[kCoarsenLocal];
-    int np = 0;
-    if (cnt > kCoarsenLocal) {
-        raise_error(st, ERR_CAPACITY, cell, ST_COARSEN);
+    const int cell = blockIdx.x;
+    const int b = m.ringStart[cell], len = m.ringStart[cell + 1] - b;
+    if (len > kCoarsenMax) {
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, cell, ST_COARSEN);
         return;
     }
-    for (int k = 0; k < cnt; ++k) {
-        // insertion into the ascending pending list
-        const int v = t.members[b + k];
-        int j = np++;
-        while (j > 0 && pend[j - 1] > v) { pend[j] = pend[j - 1]; --j; }
-        pend[j] = v;
-    }
-    const int Ccap = m.Ccap;
-    int removedHere = 0;
-    int head = 0;
-    while (head < np) {
-        const int i = pend[head++];
-        if (t.removed[i]) continue;
-        const int p = m.prev[i], q = m.next[i];
-        const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
-        if (!(sqrt(dx * dx + dy * dy) < kMAXLENGTH)) continue;
-        t.removed[i] = 1;
-        ++removedHere;
-        const int hin = t.inConn[i], hout = t.outConn[i];
-        uint32_t dom;
-        int desc;
-        if (hin < Ccap) { t.connAlive[hin] = 0; dom = m.cdom[hin]; desc = m.cdesc[hin]; }
-        else { t.ncAlive[hin - Ccap] = 0; dom = t.ncDom[hin - Ccap]; desc = t.ncDesc[hin - Ccap]; }
-        if (hout < Ccap) t.connAlive[hout] = 0;
-        else t.ncAlive[hout - Ccap] = 0;
-        t.ncA[i] = p; t.ncB[i] = q; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
-        m.next[p] = q; m.prev[q] = p;
-        t.outConn[p] = Ccap + i; t.inConn[q] = Ccap + i;
-        // neighbours with a larger id get visited at their turn with the new links
-        const int nb[2] = {p, q};
-        for (int u = 0; u < 2; ++u) {
-            const int v = nb[u];
-            if (v <= i) continue;
-            bool present = false;
-            for (int k = head; k < np; ++k) if (pend[k] == v) { present = true; break; }
-            if (present) continue;
-            if (np >= kCoarsenLocal) {
-                raise_error(st, ERR_CAPACITY, cell, ST_COARSEN);
-                return;
-            }
-            int j = np++;
-            while (j > head && pend[j - 1] > v) { pend[j] = pend[j - 1]; --j; }
-            pend[j] = v;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sx = (double*)smem;
+    double* sy = sx + kCoarsenMax;
+    unsigned long long* ord = (unsigned long long*)(sy + kCoarsenMax);
+    int* node = (int*)(ord + kCoarsenMax);
+    int* pl = node + kCoarsenMax;
+    int* nl = pl + kCoarsenMax;
+    int* hin = nl + kCoarsenMax;
+    int* hout = hin + kCoarsenMax;
+    unsigned char* dirty = (unsigned char*)(hout + kCoarsenMax);
+    unsigned char* gone = dirty + kCoarsenMax;
+    __shared__ int anyDirty;
+    if (threadIdx.x == 0) anyDirty = 0;
+    int p2 = 1;
+    while (p2 < len) p2 <<= 1;
+    __syncthreads();
+    for (int k = threadIdx.x; k < p2; k += blockDim.x) {
+        if (k < len) {
+            const int i = m.ringNode[b + k];
+            node[k] = i;
+            sx[k] = m.x[i];
+            sy[k] = m.y[i];
+            pl[k] = k == 0 ? len - 1 : k - 1;
+            nl[k] = k == len - 1 ? 0 : k + 1;
+            hin[k] = t.inConn[i];
+            hout[k] = t.outConn[i];
+            ord[k] = ((unsigned long long)i << 32) | (unsigned)k;
+            gone[k] = 0;
+        } else {
+            ord[k] = ~0ull;
         }
     }
-    if (removedHere) atomicAdd(&m.topo->removed, removedHere);
+    __syncthreads();
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+        const int p = pl[k], q = nl[k];
+        const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
+        dirty[k] = sqrt(dx * dx + dy * dy) < kMAXLENGTH;
+        if (dirty[k]) anyDirty = 1;
+    }
+    __syncthreads();
+    if (!anyDirty) {
+        for (int k = threadIdx.x; k < len; k += blockDim.x) t.removed[node[k]] = 0;
+        return;
+    }
+    // id order of the ring's nodes
+    for (int size = 2; size <= p2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = threadIdx.x; k < p2; k += blockDim.x) {
+                const int j = k ^ stride;
+                if (j > k) {
+                    const bool up = (k & size) == 0;
+                    const unsigned long long x = ord[k], y = ord[j];
+                    if ((x > y) == up) { ord[k] = y; ord[j] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        const int Ccap = m.Ccap;
+        int removedHere = 0;
+        for (int j = 0; j < len; ++j) {
+            const int k = (int)(ord[j] & 0xffffffffu);
+            if (!dirty[k]) continue;
+            const int p = pl[k], q = nl[k];
+            const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
+            if (!(sqrt(dx * dx + dy * dy) < kMAXLENGTH)) continue;
+            gone[k] = 1;
+            ++removedHere;
+            const int i = node[k];
+            const int h1 = hin[k], h2 = hout[k];
+            uint32_t dom;
+            int desc;
+            if (h1 < Ccap) { t.connAlive[h1] = 0; dom = m.cdom[h1]; desc = m.cdesc[h1]; }
+            else { t.ncAlive[h1 - Ccap] = 0; dom = t.ncDom[h1 - Ccap]; desc = t.ncDesc[h1 - Ccap]; }
+            if (h2 < Ccap) t.connAlive[h2] = 0;
+            else t.ncAlive[h2 - Ccap] = 0;
+            t.ncA[i] = node[p]; t.ncB[i] = node[q]; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
+            nl[p] = q; pl[q] = p;
+            hout[p] = Ccap + i; hin[q] = Ccap + i;
+            dirty[p] = 1; dirty[q] = 1;
+        }
+        if (removedHere) atomicAdd(&m.topo->removed, removedHere);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+        const int i = node[k];
+        t.removed[i] = gone[k];
+        if (!gone[k]) {
+            m.prev[i] = node[pl[k]];
+            m.next[i] = node[nl[k]];
+        }
+    }
 }
 
 // Compaction flags: kept nodes; alive original connections; alive new ones.
@@ -347,13 +409,11 @@ int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     if (m.Mcap == 0 || nCells == 0) return 0;
     const int mb = (m.Mcap + 1 + 255) / 256, cbk = (m.Ccap + 1 + 255) / 256;
     const int gb = ((m.Mcap > m.Ccap ? m.Mcap : m.Ccap) + 1 + 255) / 256;
-    cudaMemsetAsync(t.cellCount, 0, sizeof(int) * (nCells + 1), s);
-    cudaMemsetAsync(t.cellFill, 0, sizeof(int) * nCells, s);
+    int n = launch_rings(m, t, st, s);  // ring order after this step's remeshing
     conn_links_kernel<<<cbk, 256, 0, s>>>(m, t, st);
     coarsen_cand_kernel<<<mb, 256, 0, s>>>(m, t, st);
-    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.cellCount, t.cellStart, nCells + 1, s);
-    coarsen_fill_kernel<<<mb, 256, 0, s>>>(m, t, st);
-    coarsen_cell_kernel<<<(nCells + 63) / 64, 64, 0, s>>>(m, t, st, nCells);
+    constexpr size_t smemBytes = kCoarsenSmem;
+    coarsen_cell_kernel<<<nCells, 256, smemBytes, s>>>(m, t, st);
     coarsen_flags_kernel<<<gb, 256, 0, s>>>(m, t, st);
     coarsen_ncflag_kernel<<<mb, 256, 0, s>>>(m, t, st);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.nflag, t.nrank, m.Mcap + 1, s);
@@ -362,7 +422,7 @@ int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     coarsen_gather_kernel<<<gb, 256, 0, s>>>(m, t, st);
     coarsen_scatter_back_kernel<<<gb, 256, 0, s>>>(m, t, st);
     coarsen_commit_kernel<<<1, 1, 0, s>>>(m, t, st);
-    return 17;
+    return n + 15;
 }
 
 // ---------------------------------------------------------------------------
@@ -373,7 +433,7 @@ __global__ void ring_first_kernel(MembraneDev m, TopoDev t, Status* st) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
     t.outConn[m.ca[c]] = c;
-    atomicMin(&t.firstConn[m.cdom[c]], c);
+    agg_min(&t.firstConn[m.cdom[c]], (int)m.cdom[c], c);
 }
 
 __global__ void ring_count_kernel(MembraneDev m, TopoDev t, Status* st) {
@@ -381,7 +441,7 @@ __global__ void ring_count_kernel(MembraneDev m, TopoDev t, Status* st) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
     const int cell = t.cellOfDom[m.cdom[t.outConn[i]]];
-    atomicAdd(&t.cellCount[cell], 1);
+    agg_add(&t.cellCount[cell], cell);
 }
 
 __global__ void ring_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
@@ -390,7 +450,7 @@ __global__ void ring_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
     if (i >= m.topo->M) return;
     const uint32_t d = m.cdom[t.outConn[i]];
     const int cell = t.cellOfDom[d];
-    const int k = atomicAdd(&t.cellFill[cell], 1);
+    const int k = agg_add(&t.cellFill[cell], cell);
     t.members[t.cellStart[cell] + k] = i;
     const int start = m.cb[t.firstConn[d]];
     // break the ring before its start node: the node whose successor is the start is last
@@ -459,6 +519,14 @@ int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     ring_rank_kernel<<<nCells, 256, 0, s>>>(m, t, st);
     ring_done_kernel<<<(t.nDomains + 255) / 256, 256, 0, s>>>(m, t);
     return 7;
+}
+
+}  // namespace lbib
+
+namespace lbib {
+
+void init_kernel_attributes_topology() {
+    cudaFuncSetAttribute(coarsen_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarsenSmem);
 }
 
 }  // namespace lbib

@@ -57,6 +57,9 @@ struct CrossDev {
     int changedCap;
     int* perturbList;            // membrane node indices flagged for the host RNG
     int perturbCap;
+    // crossing records of this step (one per candidate node-slot pair)
+    uint32_t* recKey; uint32_t* recConn; uint32_t* recDom; unsigned long long* recDist;
+    int recCap;
 };
 
 // Tiles for force spreading.
@@ -141,5 +144,10 @@ int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaSt
 int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 size_t topo_scan_bytes(int n);
+
+// Opt-in shared-memory sizes of the kernels that need more than 48 KB; called
+// once before any launch (and so before any stream capture).
+void init_kernel_attributes();
+void init_kernel_attributes_topology();
 
 }  // namespace lbib

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -130,7 +131,16 @@ struct Handle {
     std::uniform_real_distribution<> dis{-kPERTURBATION, kPERTURBATION};
 
     long long hostEvents = 0;
-    long long launches = 0;  // kernels launched by the last lbib_step / lbib_lattice_step
+    long long launches = 0;
+    // CUDA graphs of one step, keyed by (buffer parity, coarsening step,
+    // tension renewal); rebuilt when a buffer is reallocated
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+    };
+    StepGraph graphs[8];
+    bool useGraphs = true;
+    long long graphEpoch = 0, graphBuiltEpoch = 0;  // kernels launched by the last lbib_step / lbib_lattice_step
     long long stepsDone = 0;
 
     // errors
@@ -160,6 +170,7 @@ Handle::~Handle() {
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.touched);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
+    fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist);
     fr(m.topo); fr(m.cdesc);
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
     fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
@@ -171,6 +182,8 @@ Handle::~Handle() {
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
     for (auto e : kEvents) cudaEventDestroy(e);
+    for (auto& g : graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -467,7 +480,12 @@ static void sync_targets(Handle& h) {
 static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     // headroom for remeshing on the device: node and connection buffers hold
     // twice the current counts before the host has to grow them
-    auto grow = [&](int need, int& cap) { if (need <= cap) return false; cap = std::max(2 * need + 1024, 64); return true; };
+    auto grow = [&](int need, int& cap) {
+        if (need <= cap) return false;
+        cap = std::max(2 * need + 1024, 64);
+        h.graphEpoch++;
+        return true;
+    };
     int oldM = h.Mcap;
     if (grow(M, h.Mcap)) {
         // membrane arrays are rewritten by every upload_topology; no copy needed
@@ -506,6 +524,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.touched); fr(h.cross.changedNode);
+        fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
         fr(h.cross.changedDom);
         fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
         const int n = h.Ccap;
@@ -518,6 +537,11 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.cross.touchedCap = 16 * n + 1024;
         h.cross.touched = dalloc<uint32_t>(h.cross.touchedCap);
         h.cross.changedCap = 8 * n + 1024;
+        h.cross.recCap = 16 * n + 1024;
+        h.cross.recKey = dalloc<uint32_t>(h.cross.recCap);
+        h.cross.recConn = dalloc<uint32_t>(h.cross.recCap);
+        h.cross.recDom = dalloc<uint32_t>(h.cross.recCap);
+        h.cross.recDist = dalloc<unsigned long long>(h.cross.recCap);
         h.cross.changedNode = dalloc<uint32_t>(h.cross.changedCap);
         h.cross.changedDom = dalloc<uint32_t>(h.cross.changedCap);
     }
@@ -730,7 +754,6 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     a.srcTab = h.srcTab;
     a.tauF = h.tauF;
     for (int k = 0; k < h.S; ++k) a.sp[k] = h.sp[k].c;
-    a.iteration = iteration;
     a.status = h.st;
     return a;
 }
@@ -748,64 +771,72 @@ __global__ void step_begin_kernel(Status* st) {
 __global__ void step_end_kernel(Status* st) {
     if (st->halt) return;
     st->pad[0] += 1;  // steps completed in this batch
+    st->iteration += 1;  // Parameters++ (SimulationRunner.cpp:98)
+    st->cellTypesCopied = 1;
 }
 
+__global__ void iteration_inc_kernel(Status* st) { st->iteration += 1; }
+
+// Launches the stage kernels of one step from `fromStage` on.  `coarsenStep`
+// (Parameters' iteration % 10 == 0) and `renewal` (the tension plugin's
+// frequency) are the only host decisions; everything else reads device state.
+// Returns the number of kernels launched.
 template <typename Real>
-static void launch_stages(Handle& h, unsigned iteration, int parity, int fromStage, bool firstStepOfRun,
-                          cudaEvent_t evCollideA, cudaEvent_t evCollideB) {
+static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int parity, int fromStage,
+                               cudaEvent_t evCollideA, cudaEvent_t evCollideB) {
     cudaStream_t s = h.stream;
     Real* fcur = (Real*)h.f[1 - parity];
     Real* gcur = (Real*)h.g[1 - parity];
     const bool hasM = h.m.Mcap > 0;
-    long long& nl = h.launches;
+    const unsigned it = 0;  // kernels read the iteration from the status word
+    long long nl = 0;
     if (fromStage <= ST_FORCE) {
         step_begin_kernel<<<1, 1, 0, s>>>(h.st);
-        launch_force_eval<Real>(h.m, h.st, iteration, s);
+        launch_force_eval<Real>(h.m, h.st, it, s);
         nl += 1 + hasM;
     }
     if (fromStage <= ST_SPREAD) {
-        launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, iteration, s);
+        launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s);
         nl += hasM ? 5 : 0;
     }
     if (fromStage <= ST_COLLIDE) {
         if (evCollideA) cudaEventRecord(evCollideA, s);
         if (sizeof(Real) == 8) {
-            const LatticeArgs<double> a = lattice_args<double>(h, iteration, parity);
+            const LatticeArgs<double> a = lattice_args<double>(h, it, parity);
             launch_stream_collide64(a, s);
         } else {
-            const LatticeArgs<float> a = lattice_args<float>(h, iteration, parity);
+            const LatticeArgs<float> a = lattice_args<float>(h, it, parity);
             launch_stream_collide32(a, s);
         }
         if (evCollideB) cudaEventRecord(evCollideB, s);
         nl += 1;
     }
     if (fromStage <= ST_INTERP_MOVE) {
-        launch_interp_move<Real>(h.m, (const Real*)h.u, h.nx, h.ny, h.L, h.cross, h.st, iteration, s);
+        launch_interp_move<Real>(h.m, (const Real*)h.u, h.nx, h.ny, h.L, h.cross, h.st, it, s);
         nl += hasM;
     }
     if (fromStage <= ST_PERTURB_CONN) {
-        launch_perturb_conn_check(h.m, h.st, iteration, s);
+        launch_perturb_conn_check(h.m, h.st, it, s);
         nl += hasM;
     }
     if (fromStage <= ST_CROSSINGS) {
-        launch_crossings<Real>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
+        launch_crossings<Real>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
         nl += hasM ? 4 : 0;
     }
     if (fromStage <= ST_REINIT) {
         SpeciesConst spc[kMaxSpecies] = {};
         for (int k = 0; k < h.S; ++k) spc[k] = h.sp[k].c;
-        const int copied = (h.cellTypesCopied || !firstStepOfRun) ? 1 : 0;
-        launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, copied,
-                            h.nx, h.ny, h.L, h.st, iteration, s);
+        launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, 0,
+                            h.nx, h.ny, h.L, h.st, it, s);
         nl += 1;
     }
     if (fromStage <= ST_DOMAIN) {
-        launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, iteration, s);
+        launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
         launch_cross_clear(h.cross, h.st, s);
         nl += 2;
     }
     if (fromStage <= ST_REMESH) nl += launch_remesh(h.m, h.td, h.nx, h.ny, h.st, s);
-    if (fromStage <= ST_COARSEN && iteration % 10 == 0) {
+    if (fromStage <= ST_COARSEN && coarsenStep) {
         // SimulationRunner.cpp:84-87: ForceSolver::deleteAllForces, then coarsenBoundary
         launch_clear_forces(h.m, s);
         nl += 1 + launch_coarsen(h.m, h.td, h.st, s);
@@ -822,7 +853,7 @@ static void launch_stages(Handle& h, unsigned iteration, int parity, int fromSta
                 launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor, h.areaStrength,
                                       h.areaMax, h.st, s);
                 nl += h.m.nCells > 0 ? 2 : 0;
-            } else if (b == 1 && iteration % h.tensionFreq == 0) {
+            } else if (b == 1 && renewal) {
                 launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
                 nl += hasM ? 2 : 0;
             }
@@ -830,6 +861,7 @@ static void launch_stages(Handle& h, unsigned iteration, int parity, int fromSta
     }
     step_end_kernel<<<1, 1, 0, s>>>(h.st);
     nl += 1;
+    return nl;
 }
 
 // The stage the host resumes at after handling the halt of `stage`.
@@ -838,7 +870,6 @@ static int resume_stage(int stage) {
         case ST_INTERP_MOVE: return ST_PERTURB_CONN;
         case ST_PERTURB_CONN: return ST_CROSSINGS;
         case ST_REMESH: return ST_COARSEN;
-        case ST_COARSEN: return ST_OUTLET;
         default: return -1;
     }
 }
@@ -852,6 +883,14 @@ static void write_status(Handle& h) {
     CK(cudaMemcpyAsync(h.st, h.stHost, sizeof(Status), cudaMemcpyHostToDevice, h.stream));
 }
 
+// Clears the status word for a run that starts at Parameters' iteration `it`.
+static void reset_status(Handle& h, unsigned it, bool cellTypesCopied) {
+    std::memset(h.stHost, 0, sizeof(Status));
+    h.stHost->iteration = it;
+    h.stHost->cellTypesCopied = cellTypesCopied ? 1 : 0;
+    write_status(h);
+}
+
 // Bookkeeping the host does for a step it launches (the force list's state).
 static void host_step_bookkeeping(Handle& h, unsigned iteration) {
     if (iteration % 10 == 0) {
@@ -863,14 +902,96 @@ static void host_step_bookkeeping(Handle& h, unsigned iteration) {
             fail(ERR_STATE, "tension renewal on a non-tension force list is not supported on the device");
 }
 
+static bool renewal_step(const Handle& h, unsigned it) {
+    for (int b : h.bio)
+        if (b == 1 && it % h.tensionFreq == 0) return true;
+    return false;
+}
+
+// The host side of a halted stage, in the reference's order.
+static void handle_halt(Handle& h, int stage) {
+    h.hostEvents++;
+    pull_topology(h);
+    HostMembrane hm;
+    if (stage == ST_INTERP_MOVE) {
+        // positions that need GeometryNode::perturbatePosition, in id order
+        const int cnt = h.stHost->nPerturbNode;
+        if (cnt > h.cross.perturbCap) fail(ERR_CAPACITY, "perturbation list overflow");
+        std::vector<int> list(cnt);
+        if (cnt) CK(cudaMemcpyAsync(list.data(), h.cross.perturbList, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h.stream));
+        download_membrane(h, hm);
+        std::sort(list.begin(), list.end());
+        for (int i : list) perturbate(h, hm.x[i], hm.y[i]);
+        CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
+    } else if (stage == ST_PERTURB_CONN) {
+        download_membrane(h, hm);
+        perturb_connections(h, hm);
+        CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
+    } else if (stage == ST_REMESH) {
+        download_membrane(h, hm);
+        sync_targets(h);
+        const int Mold = (int)h.ids.size();
+        // the force list keeps its records; new nodes have none
+        std::vector<int> foff(Mold + 1);
+        CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (Mold + 1), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        const int nrec = foff[Mold];
+        std::vector<int> ftype(nrec), fpart(nrec);
+        std::vector<double> fpar(4 * (size_t)nrec);
+        if (nrec) {
+            CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+        }
+        remesh(h, hm);
+        upload_topology(h, hm, false);
+        foff.resize(h.m.M + 1, nrec);
+        CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
+        if (nrec) {
+            CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * 4 * nrec, cudaMemcpyHostToDevice, h.stream));
+        }
+        // new nodes are bound to the lattice now (GeometryHandler.cpp:427-428)
+        reset_status(h, h.iteration, true);
+        launch_edge_check(h.m, h.nx, h.ny, h.st, 0, h.stream);
+        read_status(h);
+        if (h.stHost->err) fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
+    } else {
+        fail(ERR_STATE, "unexpected halt stage");
+    }
+}
+
+template <typename Real>
+static void launch_step_graph(Handle& h, int parity, bool coarsenStep, bool renewal) {
+    const int key = parity * 4 + (coarsenStep ? 2 : 0) + (renewal ? 1 : 0);
+    if (h.graphEpoch != h.graphBuiltEpoch) {
+        for (auto& g : h.graphs)
+            if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+        h.graphBuiltEpoch = h.graphEpoch;
+    }
+    Handle::StepGraph& g = h.graphs[key];
+    if (!g.exec) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+        g.launches = launch_stages<Real>(h, coarsenStep, renewal, parity, ST_FORCE, nullptr, nullptr);
+        CK(cudaStreamEndCapture(h.stream, &graph));
+        CK(cudaGraphInstantiate(&g.exec, graph, 0));
+        CK(cudaGraphDestroy(graph));
+    }
+    CK(cudaGraphLaunch(g.exec, h.stream));
+    h.launches += g.launches;
+}
+
 template <typename Real>
 static void run_steps(Handle& h, int n) {
     const int kBatch = 64;
-    int fromStage = ST_FORCE;
     while (n > 0) {
         const int B = std::min(n, kBatch);
-        std::memset(h.stHost, 0, sizeof(Status));
-        write_status(h);
+        reset_status(h, h.iteration, h.cellTypesCopied);
         const bool prof = h.profiling;
         while ((int)h.kEvents.size() < 2 * B) {
             cudaEvent_t e;
@@ -881,18 +1002,19 @@ static void run_steps(Handle& h, int n) {
             const unsigned it = h.iteration + b;
             host_step_bookkeeping(h, it);
             const int parity = (h.cur + b) & 1;
-            const bool first = (h.stepsDone + b) == 0;
-            launch_stages<Real>(h, it, parity, b == 0 ? fromStage : ST_FORCE, first,
-                                prof && (b > 0 || fromStage <= ST_COLLIDE) ? h.kEvents[2 * b] : nullptr,
-                                prof && (b > 0 || fromStage <= ST_COLLIDE) ? h.kEvents[2 * b + 1] : nullptr);
+            if (prof || !h.useGraphs)
+                h.launches += launch_stages<Real>(h, it % 10 == 0, renewal_step(h, it), parity, ST_FORCE,
+                                                  prof ? h.kEvents[2 * b] : nullptr,
+                                                  prof ? h.kEvents[2 * b + 1] : nullptr);
+            else
+                launch_step_graph<Real>(h, parity, it % 10 == 0, renewal_step(h, it));
         }
         CK(cudaGetLastError());
         read_status(h);
-        Status& st = *h.stHost;
+        const Status st = *h.stHost;
         const int done = st.pad[0];
         if (prof) {
             for (int b = 0; b < std::min(done, B); ++b) {
-                if (b == 0 && fromStage > ST_COLLIDE) continue;
                 float ms = 0;
                 if (cudaEventElapsedTime(&ms, h.kEvents[2 * b], h.kEvents[2 * b + 1]) == cudaSuccess) {
                     h.lastCollideMs += ms;
@@ -900,21 +1022,12 @@ static void run_steps(Handle& h, int n) {
                 }
             }
         }
-        if (!st.halt) {
-            h.cur = (h.cur + B) & 1;
-            h.iteration += B;
-            h.stepsDone += B;
-            h.cellTypesCopied = true;
-            n -= B;
-            fromStage = ST_FORCE;
-            continue;
-        }
-        // steps before the halted one completed; the halted step ran up to st.haltStage
         h.cur = (h.cur + done) & 1;
         h.iteration += done;
         h.stepsDone += done;
-        n -= done;
         if (done > 0) h.cellTypesCopied = true;
+        n -= done;
+        if (!st.halt) continue;
         if (st.err) {
             h.err = st.err;
             h.errIndex = st.errIndex;
@@ -923,153 +1036,29 @@ static void run_steps(Handle& h, int n) {
             h.msg = buf;
             fail(st.err, h.msg, st.errIndex);
         }
-        const int stage = st.haltStage;
+        // the halted step ran up to st.haltStage: serve the host event, resume
+        int stage = st.haltStage;
         const unsigned it = h.iteration;
-        const int parity = h.cur;
-        h.hostEvents++;
-        pull_topology(h);
-        HostMembrane hm;
-        if (stage == ST_INTERP_MOVE) {
-            // positions that need GeometryNode::perturbatePosition, in id order
-            std::vector<int> list(std::min(st.nPerturbNode, h.cross.perturbCap));
-            if (st.nPerturbNode > h.cross.perturbCap) fail(ERR_CAPACITY, "perturbation list overflow");
-            CK(cudaMemcpyAsync(list.data(), h.cross.perturbList, sizeof(int) * list.size(), cudaMemcpyDeviceToHost, h.stream));
-            download_membrane(h, hm);
-            std::sort(list.begin(), list.end());
-            for (int i : list) perturbate(h, hm.x[i], hm.y[i]);
-            CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
-            CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
-        } else if (stage == ST_PERTURB_CONN) {
-            download_membrane(h, hm);
-            perturb_connections(h, hm);
-            CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
-            CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
-        } else if (stage == ST_REMESH) {
-            download_membrane(h, hm);
-            sync_targets(h);
-            const int Mold = (int)h.ids.size();
-            remesh(h, hm);
-            // the force list keeps its records; new nodes have none
-            std::vector<int> foff(Mold + 1);
-            CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (Mold + 1), cudaMemcpyDeviceToHost, h.stream));
-            CK(cudaStreamSynchronize(h.stream));
-            const int nrec = foff[Mold];
-            std::vector<int> ftype(nrec), fpart(nrec);
-            std::vector<double> fpar(4 * (size_t)nrec);
-            if (nrec) {
-                CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
-                CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
-                CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
-                CK(cudaStreamSynchronize(h.stream));
-            }
-            upload_topology(h, hm, false);
-            foff.resize(h.m.M + 1, nrec);
-            CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
-            if (nrec) {
-                CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
-                CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
-                CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * 4 * nrec, cudaMemcpyHostToDevice, h.stream));
-            }
-            // new nodes are bound to the lattice now (GeometryHandler.cpp:427-428)
-            std::memset(h.stHost, 0, sizeof(Status));
-            write_status(h);
-            launch_edge_check(h.m, h.nx, h.ny, h.st, it, h.stream);
+        for (;;) {
+            handle_halt(h, stage);
+            const int from = resume_stage(stage);
+            if (from < 0) fail(ERR_STATE, "unexpected halt stage");
+            reset_status(h, it, h.cellTypesCopied);
+            h.launches += launch_stages<Real>(h, it % 10 == 0, renewal_step(h, it), h.cur, from, nullptr, nullptr);
             read_status(h);
-            if (h.stHost->err) fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
-        } else if (stage == ST_COARSEN) {
-            download_membrane(h, hm);
-            sync_targets(h);
-            coarsen(h, hm);
-            upload_topology(h, hm, true);  // the force list is empty at a coarsening step
-        } else {
-            fail(ERR_STATE, "unexpected halt stage");
-        }
-        // resume the halted step
-        std::memset(h.stHost, 0, sizeof(Status));
-        write_status(h);
-        const int from = resume_stage(stage);
-        const bool first = h.stepsDone == 0;
-        launch_stages<Real>(h, it, parity, from, first, nullptr, nullptr);
-        read_status(h);
-        if (h.stHost->halt) {
-            // a second event in the same step: handle it by looping with this step resumed
-            const int st2 = h.stHost->haltStage;
-            if (h.stHost->err) fail(h.stHost->err, "device error after resume", h.stHost->errIndex);
-            // re-enter the loop at the halted stage of the same step
-            fromStage = -st2;  // marker handled below
-        } else {
-            h.cur = (h.cur + 1) & 1;
-            h.iteration += 1;
-            h.stepsDone += 1;
-            h.cellTypesCopied = true;
-            n -= 1;
-            fromStage = ST_FORCE;
-        }
-        while (fromStage < 0) {
-            // a further halt inside the resumed step
-            const int stage2 = -fromStage;
-            h.hostEvents++;
-            pull_topology(h);
-            HostMembrane hm2;
-            if (stage2 == ST_PERTURB_CONN) {
-                download_membrane(h, hm2);
-                perturb_connections(h, hm2);
-                CK(cudaMemcpyAsync(h.m.x, hm2.x.data(), sizeof(double) * hm2.x.size(), cudaMemcpyHostToDevice, h.stream));
-                CK(cudaMemcpyAsync(h.m.y, hm2.y.data(), sizeof(double) * hm2.y.size(), cudaMemcpyHostToDevice, h.stream));
-            } else if (stage2 == ST_REMESH || stage2 == ST_COARSEN) {
-                download_membrane(h, hm2);
-                sync_targets(h);
-                if (stage2 == ST_REMESH) {
-                    const int Mold = (int)h.ids.size();
-                    std::vector<int> foff(Mold + 1);
-                    CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (Mold + 1), cudaMemcpyDeviceToHost, h.stream));
-                    CK(cudaStreamSynchronize(h.stream));
-                    const int nrec = foff[Mold];
-                    std::vector<int> ftype(nrec), fpart(nrec);
-                    std::vector<double> fpar(4 * (size_t)nrec);
-                    if (nrec) {
-                        CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
-                        CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
-                        CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
-                        CK(cudaStreamSynchronize(h.stream));
-                    }
-                    remesh(h, hm2);
-                    upload_topology(h, hm2, false);
-                    foff.resize(h.m.M + 1, nrec);
-                    CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
-                    if (nrec) {
-                        CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
-                        CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * nrec, cudaMemcpyHostToDevice, h.stream));
-                        CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * 4 * nrec, cudaMemcpyHostToDevice, h.stream));
-                    }
-                    std::memset(h.stHost, 0, sizeof(Status));
-                    write_status(h);
-                    launch_edge_check(h.m, h.nx, h.ny, h.st, it, h.stream);
-                    read_status(h);
-                    if (h.stHost->err) fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
-                } else {
-                    coarsen(h, hm2);
-                    upload_topology(h, hm2, true);
-                }
-            } else {
-                fail(ERR_STATE, "unexpected halt stage after resume");
+            if (h.stHost->err) {
+                h.err = h.stHost->err;
+                h.errIndex = h.stHost->errIndex;
+                fail(h.stHost->err, "device error after a host event", h.stHost->errIndex);
             }
-            std::memset(h.stHost, 0, sizeof(Status));
-            write_status(h);
-            launch_stages<Real>(h, it, parity, resume_stage(stage2), h.stepsDone == 0, nullptr, nullptr);
-            read_status(h);
-            if (h.stHost->err) fail(h.stHost->err, "device error after resume", h.stHost->errIndex);
-            if (h.stHost->halt) {
-                fromStage = -h.stHost->haltStage;
-            } else {
-                h.cur = (h.cur + 1) & 1;
-                h.iteration += 1;
-                h.stepsDone += 1;
-                h.cellTypesCopied = true;
-                n -= 1;
-                fromStage = ST_FORCE;
-            }
+            if (!h.stHost->halt) break;
+            stage = h.stHost->haltStage;
         }
+        h.cur = (h.cur + 1) & 1;
+        h.iteration += 1;
+        h.stepsDone += 1;
+        h.cellTypesCopied = true;
+        n -= 1;
     }
 }
 
@@ -1099,6 +1088,9 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.dom, 0, sizeof(uint32_t) * h.L, h.stream));
     CK(cudaMalloc(&h.st, sizeof(Status)));
     CK(cudaMallocHost(&h.stHost, sizeof(Status)));
+    init_kernel_attributes();
+    // LBIB_NO_GRAPHS=1 launches every stage kernel directly (no CUDA graphs)
+    if (const char* e = std::getenv("LBIB_NO_GRAPHS")) h.useGraphs = !(e[0] == '1');
     std::memset(h.stHost, 0, sizeof(Status));
     write_status(h);
 
@@ -1311,8 +1303,7 @@ int lbib_step(lbib_handle* hh, int n) {
 int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
     API_BEGIN(hh)
     if (n < 0) lbib::fail(LBIB_ERR_INPUT, "negative step count");
-    std::memset(h.stHost, 0, sizeof(lbib::Status));
-    lbib::write_status(h);
+    lbib::reset_status(h, h.iteration, h.cellTypesCopied);
     h.lastCollideMs = 0;
     h.lastCollideLaunches = 0;
     h.launches = (long long)n * (outlet ? 2 : 1);
@@ -1340,6 +1331,7 @@ int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
             else
                 lbib::launch_outlet32((float*)h.f[h.cur], (float*)h.g[h.cur], h.S, h.nx, h.ny, h.L, h.st, h.stream);
         }
+        lbib::iteration_inc_kernel<<<1, 1, 0, h.stream>>>(h.st);
         h.iteration++;
     }
     CK(cudaEventRecord(h.evB, h.stream));

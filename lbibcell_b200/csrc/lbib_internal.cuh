@@ -47,7 +47,9 @@ struct Status {
     int coarsen;       // a node is a coarsening candidate
     int nDiagReinit;   // reinit from diagonal neighbours
     int nFailedReinit; // reinit without any neighbour (division by zero)
-    int pad[4];
+    unsigned iteration;   // Parameters' current iteration of the step being run
+    int cellTypesCopied;  // copyCellTypeToPhysicalNodes has run (after the first step)
+    int pad[4];           // [0] steps completed in a batch, [1] remesh RNG needs, [2] crossing records
 };
 
 // Stage numbers (halt points), in the reference's order of
@@ -126,7 +128,6 @@ struct LatticeArgs {
     const double* srcTab;      // [S][nDomains] production per step
     double tauF;
     SpeciesConst sp[kMaxSpecies];
-    unsigned iteration;
     const Status* status;
 };
 

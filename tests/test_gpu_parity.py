@@ -139,3 +139,24 @@ def test_fp32_shifted_error_config1(lbib, tmp_path):
     print(f"FP32-shifted vs FP64: rho {e_rho:.2e} u {e_u:.2e} c {e_c:.2e} x {e_x:.2e}")
     assert e_rho <= 1e-5 and e_u <= 1e-5 and e_c <= 1e-5
     assert e_x <= 1e-6
+
+
+def _hex25(tmp_path, iterations=120):
+    cells = configs.hex_tissue(320, 320, 44.0, 20.0, 2.0, 250, 0, cols=5, rows=5)
+    cfg = configs.Config(name="hex25", nx=320, ny=320, tau_fluid=1.0, iterations=iterations, report_step=60,
+                         cells=cells,
+                         species=[configs.Species(configs.SPECIES_NAMES[0], 0.8, source={1: 1e-3, 7: 1e-3}),
+                                  configs.Species(configs.SPECIES_NAMES[1], 1.2, decay=1e-4, source={3: 2e-3})])
+    return cfg.write(str(tmp_path))
+
+
+def test_hex25_tissue_fp64(lbib, oracle_mod, tmp_path):
+    """25 cells growing on a 320x320 lattice: remeshing on most steps and
+    coarsening every 10 on the device, 2 species; identical to the oracle."""
+    paths = _hex25(tmp_path)
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    for n in (1, 10, 49, 60):
+        sim.step(n)
+        o.step(n)
+        _compare_state(sim, o.state())
