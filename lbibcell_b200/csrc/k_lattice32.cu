@@ -88,6 +88,20 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const float uxo = ux + s * Fx, uyo = uy + s * Fy;
     a.u[n] = uxo;
     a.u[L + n] = uyo;
+    // MassSolverBoxOutlet on the x=0 column and the y=0 row (the corner twice),
+    // fused here as in the FP64 kernel: f' = f / rho, i.e.
+    // h' = (h - w * dh) / (1 + dh) with dh = sum h.
+    const int passes = a.outlet ? (x == 0) + (y == 0) : 0;
+    float rs[2] = {1.0f, 1.0f};
+    for (int p = 0; p < passes; ++p) {
+        const float wq[9] = {w0, w1, w1, w1, w1, w2, w2, w2, w2};
+        float dh = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dh += fo[q * L + n];
+        rs[p] = 1.0f / (1.0f + dh);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) fo[q * L + n] = (fo[q * L + n] - wq[q] * dh) * rs[p];
+    }
 
     for (int k = 0; k < a.S; ++k) {
         const float* gin = a.gin + (size_t)k * 5 * L;
@@ -103,12 +117,18 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, a.status->iteration, C);
         const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
         const float e0 = C * (1.0f / 3.0f), e1 = C * (1.0f / 6.0f);
-        float* go = a.gout + (size_t)k * 5 * L;
-        go[0 * L + n] = gT + (e0 - gT) * tI + r0;
-        go[1 * L + n] = gE + (e1 * (1.0f + 3.0f * uxo) - gE) * tI + r1;
-        go[2 * L + n] = gN + (e1 * (1.0f + 3.0f * uyo) - gN) * tI + r1;
-        go[3 * L + n] = gW + (e1 * (1.0f - 3.0f * uxo) - gW) * tI + r1;
-        go[4 * L + n] = gS + (e1 * (1.0f - 3.0f * uyo) - gS) * tI + r1;
+        float go[5];
+        go[0] = gT + (e0 - gT) * tI + r0;
+        go[1] = gE + (e1 * (1.0f + 3.0f * uxo) - gE) * tI + r1;
+        go[2] = gN + (e1 * (1.0f + 3.0f * uyo) - gN) * tI + r1;
+        go[3] = gW + (e1 * (1.0f - 3.0f * uxo) - gW) * tI + r1;
+        go[4] = gS + (e1 * (1.0f - 3.0f * uyo) - gS) * tI + r1;
+        for (int p = 0; p < passes; ++p)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) go[q] *= rs[p];
+        float* gop = a.gout + (size_t)k * 5 * L;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) gop[q * L + n] = go[q];
     }
 }
 

@@ -47,10 +47,25 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
     }
     double ux, uy;
     collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
     a.u[n] = ux;
     a.u[L + n] = uy;
+    // MassSolverBoxOutlet (MassSolverBoxOutlet.cpp:42-72) on the x=0 column and
+    // the y=0 row: fused here because no later stage of the step touches those
+    // nodes (membrane nodes keep 2 lu from the edges, GeometryHandler.cpp:618-636).
+    // The corner is rescaled twice, as the column pass and then the row pass do.
+    const int passes = a.outlet ? (x == 0) + (y == 0) : 0;
+    double sc[2] = {1.0, 1.0};
+    for (int p = 0; p < passes; ++p) {
+        // rho in the reference's slot order after localSwap: T, W, S, E, N, SW, SE, NE, NW
+        double rho = 0.0;
+        rho += f[T]; rho += f[W]; rho += f[S]; rho += f[E]; rho += f[N];
+        rho += f[SW]; rho += f[SE]; rho += f[NE]; rho += f[NW];
+        sc[p] = 1.0 / rho;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] *= sc[p];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
 
     for (int k = 0; k < a.S; ++k) {
         const double* gin = a.gin + (size_t)k * 5 * L;
@@ -63,6 +78,9 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         double src = 0.0;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
         collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.status->iteration);
+        for (int p = 0; p < passes; ++p)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) g[q] *= sc[p];
         double* gout = a.gout + (size_t)k * 5 * L;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gout[q * L + n] = g[q];

@@ -180,35 +180,57 @@ __device__ __forceinline__ void stencil_slot(const Stencil& s, int k, int& xk, i
             if (((4 * x + y) & 15) == k) { xk = x; yk = y; }
 }
 
+// Lanes with the same tile share one atomic.
+__device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid) {
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, valid ? tile : -1);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (valid && lane == leader) base = atomicAdd(&arr[tile], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    return base + __popc(grp & ((1u << lane) - 1u));
+}
+
 __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st, int pass) {
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.topo->M) return;
-    Stencil sc;
-    if (!stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
+    bool ok = i < m.topo->M;
+    Stencil sc{0, 0, 0, 0};
+    if (ok && !stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_SPREAD);
-        return;
+        ok = false;
     }
     const int tx0 = sc.x0 / kTile, tx1 = sc.x1 / kTile, ty0 = sc.y0 / kTile, ty1 = sc.y1 / kTile;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) {
-            const int tile = ty * t.tilesX + tx;
-            if (pass == 0) {
-                atomicAdd(&t.count[tile], 1);
-            } else {
-                const int slot = atomicAdd(&t.fill[tile], 1);
+    // up to 2 x 2 tiles per stencil; all lanes run the four rounds together
+    for (int j = 0; j < 4; ++j) {
+        const int tx = tx0 + (j & 1), ty = ty0 + (j >> 1);
+        const bool v = ok && tx <= tx1 && ty <= ty1;
+        const int tile = v ? ty * t.tilesX + tx : -1;
+        if (pass == 0) {
+            tile_agg_add(t.count, tile, v);
+        } else {
+            const int slot = tile_agg_add(t.fill, tile, v);
+            if (v) {
                 const int pos = t.start[tile] + slot;
                 if (pos < t.cap) t.list[pos] = i;
             }
         }
+    }
 }
 
 constexpr int kSpreadMax = 1024;  // membrane stencils per tile held in shared memory
-constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(Stencil) + sizeof(int));
+constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(int));
+
+// Per-tile entry: the stencil origin relative to the tile (+4) and the stencil
+// widths, packed in one word: ox | oy << 8 | (x1-x0) << 16 | (y1-y0) << 20.
+__device__ __forceinline__ int pack_stencil(const Stencil& s, int tileX0, int tileY0) {
+    return (s.x0 - tileX0 + 4) | ((s.y0 - tileY0 + 4) << 8) | ((s.x1 - s.x0) << 16) | ((s.y1 - s.y0) << 20);
+}
 
 template <typename Real>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
-                                                     Status* st) {
+                                                     Status* st, int sortBits) {
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
@@ -217,50 +239,59 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
         return;
     }
-    // dynamic shared memory: kSpreadMax x (4 doubles + stencil + index)
+    // dynamic shared memory: kSpreadMax x (4 doubles + packed stencil)
     extern __shared__ __align__(16) unsigned char smem[];
     double* sx = (double*)smem;
     double* sy = sx + kSpreadMax;
     double* sfx = sy + kSpreadMax;
     double* sfy = sfx + kSpreadMax;
-    Stencil* sst = (Stencil*)(sfy + kSpreadMax);
-    int* idx = (int*)(sst + kSpreadMax);
-    int p2 = 1;
-    while (p2 < cnt) p2 <<= 1;
+    int* code = (int*)(sfy + kSpreadMax);
+    typedef cub::BlockRadixSort<int, 256, kSpreadMax / 256> Sort;
+    __shared__ typename Sort::TempStorage sortTmp;
     const int base = t.start[tile];
-    for (int k = threadIdx.x; k < p2; k += blockDim.x) idx[k] = k < cnt ? t.list[base + k] : 0x7fffffff;
-    __syncthreads();
-    // bitonic sort by membrane index (= id order)
-    for (int size = 2; size <= p2; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int k = threadIdx.x; k < p2; k += blockDim.x) {
-                const int j = k ^ stride;
-                if (j > k) {
-                    const bool up = (k & size) == 0;
-                    const int a = idx[k], b = idx[j];
-                    if ((a > b) == up) { idx[k] = b; idx[j] = a; }
-                }
-            }
-            __syncthreads();
+    int keys[kSpreadMax / 256];
+#pragma unroll
+    for (int j = 0; j < kSpreadMax / 256; ++j) {
+        const int k = threadIdx.x * (kSpreadMax / 256) + j;
+        keys[j] = k < cnt ? t.list[base + k] : 0x7fffffff;
+    }
+    // membrane indices in ascending order = id order
+    Sort(sortTmp).Sort(keys, 0, sortBits);
+    const int tx = tile % t.tilesX, ty = tile / t.tilesX;
+    const int tileX0 = tx * kTile, tileY0 = ty * kTile;
+#pragma unroll
+    for (int j = 0; j < kSpreadMax / 256; ++j) {
+        const int k = threadIdx.x * (kSpreadMax / 256) + j;
+        if (k < cnt) {
+            const int i = keys[j];
+            sx[k] = m.x[i]; sy[k] = m.y[i]; sfx[k] = m.fx[i]; sfy[k] = m.fy[i];
+            Stencil sc;
+            stencil_range(sx[k], sy[k], nx, ny, sc);
+            code[k] = pack_stencil(sc, tileX0, tileY0);
         }
     }
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-        const int i = idx[k];
-        sx[k] = m.x[i]; sy[k] = m.y[i]; sfx[k] = m.fx[i]; sfy[k] = m.fy[i];
-        stencil_range(sx[k], sy[k], nx, ny, sst[k]);
-    }
     __syncthreads();
-    const int tx = tile % t.tilesX, ty = tile / t.tilesX;
-    const int x = tx * kTile + (threadIdx.x & 15), y = ty * kTile + (threadIdx.x >> 4);
+    const int lx = threadIdx.x & 15, ly = threadIdx.x >> 4;
+    const int x = tileX0 + lx, y = tileY0 + ly;
     const bool inside = x < nx && y < ny;
     double ax = 0.0, ay = 0.0;
-    // a warp covers two rows of the tile: entries whose stencil rows miss
-    // both are skipped by a warp-uniform test
-    const int yA = ty * kTile + ((threadIdx.x >> 5) << 1);
+    // a warp covers local rows wy0, wy0+1 (+4 offset): entries whose stencil
+    // rows miss both are skipped by a warp-uniform test
+    const int wy0 = ((threadIdx.x >> 5) << 1) + 4;
     for (int k = 0; k < cnt; ++k) {
-        const Stencil sc = sst[k];
-        if (sc.y1 < yA || sc.y0 > yA + 1) continue;
-        if (in_stencil(sc, x, y)) {
+        const int c = code[k];
+        const int oy = (c >> 8) & 0xff, hy = (c >> 20) & 0xf;
+        if (oy + hy < wy0 || oy > wy0 + 1) continue;
+        const int ox = c & 0xff, hx = (c >> 16) & 0xf;
+        const int dx = lx + 4 - ox, dy = ly + 4 - oy;
+        bool hit;
+        if (hx == 3 && hy == 3) {
+            hit = (unsigned)dx < 4u && (unsigned)dy < 4u;
+        } else {
+            Stencil sc{ox - 4 + tileX0, ox - 4 + tileX0 + hx, oy - 4 + tileY0, oy - 4 + tileY0 + hy};
+            hit = in_stencil(sc, x, y);
+        }
+        if (hit) {
             const double dl = dirac((double)x - sx[k], (double)y - sy[k]);
             ax += sfx[k] * dl;
             ay += sfy[k] * dl;
@@ -283,7 +314,9 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
     constexpr size_t smemBytes = kSpreadSmem;
-    spread_kernel<Real><<<t.nTiles, 256, smemBytes, s>>>(m, t, force, nx, ny, L, st);
+    int bits = 1;
+    while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
+    spread_kernel<Real><<<t.nTiles, 256, smemBytes, s>>>(m, t, force, nx, ny, L, st, bits);
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
                                     cudaStream_t);
@@ -384,65 +417,113 @@ __device__ __forceinline__ int slot_code(int d) {  // E,N,W,S -> 0..3
     return d - 1;
 }
 
-// Pass 0, per crossing: closest distance by atomicMin; the record is kept
-// for passes 1 and 2; the first writer of a (node, slot) key lists it for
-// the reset at the end of the step.
-__device__ __forceinline__ void cross_record(const CrossDev& c, Status* st, int conn, int nx, int ny, int px,
-                                             int py, int dirSlot, double bx, double by, uint32_t bdom) {
-    if (px < 0 || py < 0 || px >= nx || py >= ny) {
-        raise_error(st, ERR_EDGE_W, conn, ST_CROSSINGS);
-        return;
-    }
+// Pass 0: every crossing of a connection with a lattice line is a candidate
+// boundary node for one (node, slot) key.  The closest distance per key is
+// found by atomicMin on the distance's bits; each candidate is recorded for
+// passes 1 and 2; a key's first writer lists it for the reset at the end of
+// the step.  A warp reserves its records and listings with one atomic each.
+constexpr int kRecPerConn = 16;
+
+struct CrossRec {
+    uint32_t key;
+    uint32_t dom;
+    unsigned long long bits;
+};
+
+__device__ __forceinline__ bool make_record(int nx, int ny, int px, int py, int dirSlot, double bx, double by,
+                                            uint32_t bdom, CrossRec& r) {
+    if (px < 0 || py < 0 || px >= nx || py >= ny) return false;
     const size_t node = (size_t)py * nx + px;
     const double d2 = ((double)px - bx) * ((double)px - bx) + ((double)py - by) * ((double)py - by);
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
-    const uint32_t key = (uint32_t)(node * 4 + slot_code(dirSlot));
-    const unsigned long long old = atomicMin(&c.bnDist[key], bits);
-    if (old == kEmpty) {
-        const int k = atomicAdd(&st->nRecords, 1);
-        if (k < c.touchedCap) c.touched[k] = key;
-        else raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
+    r.bits = (unsigned long long)__double_as_longlong(d2);
+    r.key = (uint32_t)(node * 4 + slot_code(dirSlot));
+    r.dom = bdom;
+    return true;
+}
+
+// Exclusive prefix of `count` over the active lanes plus one atomicAdd per warp.
+__device__ __forceinline__ int warp_reserve(int* counter, int count) {
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
+    int incl = count;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(act, incl, off);
+        if (lane >= off && ((act >> (lane - off)) & 1u)) incl += v;
     }
-    const int r = atomicAdd(&st->pad[2], 1);
-    if (r < c.recCap) {
-        c.recKey[r] = key; c.recConn[r] = (uint32_t)conn; c.recDom[r] = bdom; c.recDist[r] = bits;
-    } else {
-        raise_error(st, ERR_CAPACITY, conn, ST_CROSSINGS);
-    }
+    const int last = 31 - __clz(act);
+    const int total = __shfl_sync(act, incl, last);
+    const int leader = __ffs(act) - 1;
+    int base = 0;
+    if (lane == leader && total > 0) base = atomicAdd(counter, total);
+    base = __shfl_sync(act, base, leader);
+    return base + incl - count;
 }
 
 __global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Status* st) {
     if (st->halt) return;
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cn >= m.topo->C) return;
-    const int a = m.ca[cn], b = m.cb[cn];
-    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-    const uint32_t D = m.cdom[cn];
-    const double maxX = x1 < x2 ? x2 : x1, maxY = y1 < y2 ? y2 : y1;
-    const double minX = x2 < x1 ? x2 : x1, minY = y2 < y1 ? y2 : y1;
-    const double mm = (y2 - y1) / (x2 - x1);
-    const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
-    if (!isfinite(mm)) {
-        raise_error(st, ERR_VERTICAL, cn, ST_CROSSINGS);
-        return;
+    CrossRec rec[kRecPerConn];
+    int nrec = 0;
+    bool bad = false;
+    if (cn < m.topo->C) {
+        const int a = m.ca[cn], b = m.cb[cn];
+        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+        const uint32_t D = m.cdom[cn];
+        const double maxX = x1 < x2 ? x2 : x1, maxY = y1 < y2 ? y2 : y1;
+        const double minX = x2 < x1 ? x2 : x1, minY = y2 < y1 ? y2 : y1;
+        const double mm = (y2 - y1) / (x2 - x1);
+        const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
+        if (!isfinite(mm)) {
+            raise_error(st, ERR_VERTICAL, cn, ST_CROSSINGS);
+            bad = true;
+        } else if (!(minX >= -1.0 && maxX <= nx + 1.0 && minY >= -1.0 && maxY <= ny + 1.0)) {
+            // keeps the line loops bounded for positions off the lattice
+            raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
+            bad = true;
+        } else {
+            const bool eastward = x1 < x2, southward = y1 > y2;
+            for (int i = (int)ceil(minX); i <= (int)floor(maxX) && !bad; i++) {
+                const double yc = mm * i + nn;
+                // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
+                if (nrec + 2 > kRecPerConn) { bad = true; break; }
+                if (!make_record(nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D, rec[nrec])) bad = true;
+                else ++nrec;
+                if (!bad && !make_record(nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u, rec[nrec])) bad = true;
+                else if (!bad) ++nrec;
+            }
+            for (int i = (int)ceil(minY); i <= (int)floor(maxY) && !bad; i++) {
+                const double xc = (i - nn) / mm;
+                // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
+                if (nrec + 2 > kRecPerConn) { bad = true; break; }
+                if (!make_record(nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D, rec[nrec])) bad = true;
+                else ++nrec;
+                if (!bad && !make_record(nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u, rec[nrec])) bad = true;
+                else if (!bad) ++nrec;
+            }
+            if (bad) raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
+        }
     }
-    // keeps the line loops bounded for positions off the lattice
-    if (!(minX >= -1.0 && maxX <= nx + 1.0 && minY >= -1.0 && maxY <= ny + 1.0)) {
-        raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
-        return;
+    if (bad) nrec = 0;
+    // closest distance per key; first writers of a key
+    int firsts = 0;
+    uint32_t firstKey[kRecPerConn];
+    for (int k = 0; k < nrec; ++k) {
+        const unsigned long long old = atomicMin(&c.bnDist[rec[k].key], rec[k].bits);
+        if (old == kEmpty) firstKey[firsts++] = rec[k].key;
     }
-    const bool eastward = x1 < x2, southward = y1 > y2;
-    for (int i = (int)ceil(minX); i <= (int)floor(maxX); i++) {
-        const double yc = mm * i + nn;
-        // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
-        cross_record(c, st, cn, nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D);
-        cross_record(c, st, cn, nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u);
+    const int rb = warp_reserve(&st->pad[2], nrec);
+    const int fb = warp_reserve(&st->nRecords, firsts);
+    for (int k = 0; k < nrec; ++k) {
+        const int r = rb + k;
+        if (r < c.recCap) {
+            c.recKey[r] = rec[k].key; c.recConn[r] = (uint32_t)cn; c.recDom[r] = rec[k].dom; c.recDist[r] = rec[k].bits;
+        } else {
+            raise_error(st, ERR_CAPACITY, cn, ST_CROSSINGS);
+        }
     }
-    for (int i = (int)ceil(minY); i <= (int)floor(maxY); i++) {
-        const double xc = (i - nn) / mm;
-        // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
-        cross_record(c, st, cn, nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D);
-        cross_record(c, st, cn, nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u);
+    for (int k = 0; k < firsts; ++k) {
+        if (fb + k < c.touchedCap) c.touched[fb + k] = firstKey[k];
+        else raise_error(st, ERR_CAPACITY, cn, ST_CROSSINGS);
     }
 }
 
@@ -612,23 +693,20 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[6] = (int(*)[6])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    int p2 = 1;
-    while (p2 < cnt) p2 <<= 1;
-    for (int k = threadIdx.x; k < p2; k += blockDim.x)
-        key[k] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
-    __syncthreads();
-    for (int size = 2; size <= p2; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int k = threadIdx.x; k < p2; k += blockDim.x) {
-                const int j = k ^ stride;
-                if (j > k) {
-                    const bool up = (k & size) == 0;
-                    const unsigned long long a = key[k], b = key[j];
-                    if ((a > b) == up) { key[k] = b; key[j] = a; }
-                }
-            }
-            __syncthreads();
+    {
+        // sort by node index (row-major order): keys node << 32 | newDom
+        typedef cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024> Sort;
+        __shared__ typename Sort::TempStorage sortTmp;
+        unsigned long long kv[kReinitMax / 1024];
+#pragma unroll
+        for (int j = 0; j < kReinitMax / 1024; ++j) {
+            const int k = threadIdx.x * (kReinitMax / 1024) + j;
+            kv[j] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
         }
+        Sort(sortTmp).Sort(kv, 32, 64);
+#pragma unroll
+        for (int j = 0; j < kReinitMax / 1024; ++j) key[threadIdx.x * (kReinitMax / 1024) + j] = kv[j];
+        __syncthreads();
     }
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
         const size_t n = (size_t)(key[k] >> 32);

@@ -755,6 +755,7 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     a.tauF = h.tauF;
     for (int k = 0; k < h.S; ++k) a.sp[k] = h.sp[k].c;
     a.status = h.st;
+    a.outlet = h.outlet ? 1 : 0;
     return a;
 }
 
@@ -841,11 +842,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
         launch_clear_forces(h.m, s);
         nl += 1 + launch_coarsen(h.m, h.td, h.st, s);
     }
-    if (fromStage <= ST_OUTLET && h.outlet) {
-        if (sizeof(Real) == 8) launch_outlet64((double*)fcur, (double*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
-        else launch_outlet32((float*)fcur, (float*)gcur, h.S, h.nx, h.ny, h.L, h.st, s);
-        nl += 1;
-    }
+    // ST_OUTLET: MassSolverBoxOutlet runs inside the stream-collide kernel
     if (fromStage <= ST_BIO) {
         nl += launch_rings(h.m, h.td, h.st, s);
         for (int b : h.bio) {
@@ -1306,7 +1303,7 @@ int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
     lbib::reset_status(h, h.iteration, h.cellTypesCopied);
     h.lastCollideMs = 0;
     h.lastCollideLaunches = 0;
-    h.launches = (long long)n * (outlet ? 2 : 1);
+    h.launches = (long long)n * 2;
     while ((int)h.kEvents.size() < 2 * n) {
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
@@ -1318,19 +1315,15 @@ int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
         if (h.profiling) CK(cudaEventRecord(h.kEvents[2 * i], h.stream));
         if (h.precision == LBIB_FP64) {
             auto a = lbib::lattice_args<double>(h, h.iteration, p);
+            a.outlet = outlet ? 1 : 0;
             lbib::launch_stream_collide64(a, h.stream);
         } else {
             auto a = lbib::lattice_args<float>(h, h.iteration, p);
+            a.outlet = outlet ? 1 : 0;
             lbib::launch_stream_collide32(a, h.stream);
         }
         if (h.profiling) CK(cudaEventRecord(h.kEvents[2 * i + 1], h.stream));
         h.cur = 1 - p;
-        if (outlet) {
-            if (h.precision == LBIB_FP64)
-                lbib::launch_outlet64((double*)h.f[h.cur], (double*)h.g[h.cur], h.S, h.nx, h.ny, h.L, h.st, h.stream);
-            else
-                lbib::launch_outlet32((float*)h.f[h.cur], (float*)h.g[h.cur], h.S, h.nx, h.ny, h.L, h.st, h.stream);
-        }
         lbib::iteration_inc_kernel<<<1, 1, 0, h.stream>>>(h.st);
         h.iteration++;
     }

@@ -129,6 +129,7 @@ struct LatticeArgs {
     double tauF;
     SpeciesConst sp[kMaxSpecies];
     const Status* status;
+    int outlet;                // MassSolverBoxOutlet registered: rescale x=0 / y=0 nodes
 };
 
 constexpr int kTile = 16;  // force tiles are 16x16 lattice nodes
