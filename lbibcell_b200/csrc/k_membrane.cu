@@ -219,8 +219,8 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
     }
 }
 
-constexpr int kSpreadMax = 1024;  // membrane stencils per tile held in shared memory
-constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (4 * sizeof(double) + sizeof(int));
+constexpr int kSpreadMax = 768;  // membrane stencils per tile held in shared memory
+constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (12 * sizeof(double) + 2 * sizeof(int) + 8 * sizeof(unsigned short));
 
 // Per-tile entry: the stencil origin relative to the tile (+4) and the stencil
 // widths, packed in one word: ox | oy << 8 | (x1-x0) << 16 | (y1-y0) << 20.
@@ -228,6 +228,31 @@ __device__ __forceinline__ int pack_stencil(const Stencil& s, int tileX0, int ti
     return (s.x0 - tileX0 + 4) | ((s.y0 - tileY0 + 4) << 8) | ((s.x1 - s.x0) << 16) | ((s.y1 - s.y0) << 20);
 }
 
+// Sorts the tile's membrane indices ascending (= id order) into `out`.
+template <int ITEMS>
+__device__ __forceinline__ void sort_tile_list(const int* list, int cnt, int sortBits, int* out, void* tmp) {
+    typedef cub::BlockRadixSort<int, 256, ITEMS> Sort;
+    int keys[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int k = threadIdx.x * ITEMS + j;
+        keys[j] = k < cnt ? list[k] : 0x7fffffff;
+    }
+    Sort(*(typename Sort::TempStorage*)tmp).Sort(keys, 0, sortBits);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int k = threadIdx.x * ITEMS + j;
+        if (k < cnt) out[k] = keys[j];
+    }
+}
+
+// Each 16x16 tile: its membrane nodes sorted by id; per node the Dirac factors
+// A_i = 1 + fastCos(pi/2 (x0 + i - X)) and B_j = 1 + fastCos(pi/2 (y0 + j - Y)),
+// so that the weight of lattice node (x0+i, y0+j) is (A_i * B_j) / 16, the same
+// expression as calculateDiscreteDeltaDirac (GeometryNode.cpp:89-94).  Each warp
+// covers two rows of the tile and first collects, in id order, the entries
+// whose stencil rows meet its rows; every lattice node then adds its
+// contributions in id order.
 template <typename Real>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
                                                      Status* st, int sortBits) {
@@ -239,50 +264,63 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
         return;
     }
-    // dynamic shared memory: kSpreadMax x (4 doubles + packed stencil)
     extern __shared__ __align__(16) unsigned char smem[];
-    double* sx = (double*)smem;
-    double* sy = sx + kSpreadMax;
-    double* sfx = sy + kSpreadMax;
+    double* fac = (double*)smem;                          // kSpreadMax x 10: A[5], B[5]
+    double* sfx = fac + 10 * kSpreadMax;
     double* sfy = sfx + kSpreadMax;
     int* code = (int*)(sfy + kSpreadMax);
-    typedef cub::BlockRadixSort<int, 256, kSpreadMax / 256> Sort;
-    __shared__ typename Sort::TempStorage sortTmp;
-    const int base = t.start[tile];
-    int keys[kSpreadMax / 256];
-#pragma unroll
-    for (int j = 0; j < kSpreadMax / 256; ++j) {
-        const int k = threadIdx.x * (kSpreadMax / 256) + j;
-        keys[j] = k < cnt ? t.list[base + k] : 0x7fffffff;
-    }
-    // membrane indices in ascending order = id order
-    Sort(sortTmp).Sort(keys, 0, sortBits);
+    int* order = code + kSpreadMax;                      // sorted membrane indices
+    unsigned short* wlist = (unsigned short*)(order + kSpreadMax);  // 8 warps x kSpreadMax
+    __shared__ __align__(16) unsigned char sortTmp[sizeof(typename cub::BlockRadixSort<int, 256, kSpreadMax / 256>::TempStorage)];
+    const int* list = t.list + t.start[tile];
+    if (cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
+    else if (cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
+    else sort_tile_list<kSpreadMax / 256>(list, cnt, sortBits, order, sortTmp);
+    __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
+    const double halfPi = M_PI / 2.0;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int i = order[k];
+        const double X = m.x[i], Y = m.y[i];
+        sfx[k] = m.fx[i];
+        sfy[k] = m.fy[i];
+        Stencil sc;
+        stencil_range(X, Y, nx, ny, sc);
+        code[k] = pack_stencil(sc, tileX0, tileY0);
+        double* f = fac + 10 * k;
 #pragma unroll
-    for (int j = 0; j < kSpreadMax / 256; ++j) {
-        const int k = threadIdx.x * (kSpreadMax / 256) + j;
-        if (k < cnt) {
-            const int i = keys[j];
-            sx[k] = m.x[i]; sy[k] = m.y[i]; sfx[k] = m.fx[i]; sfy[k] = m.fy[i];
-            Stencil sc;
-            stencil_range(sx[k], sy[k], nx, ny, sc);
-            code[k] = pack_stencil(sc, tileX0, tileY0);
+        for (int q = 0; q < 5; ++q) {
+            f[q] = 1.0 + fast_cos(halfPi * ((double)(sc.x0 + q) - X));
+            f[5 + q] = 1.0 + fast_cos(halfPi * ((double)(sc.y0 + q) - Y));
         }
     }
     __syncthreads();
-    const int lx = threadIdx.x & 15, ly = threadIdx.x >> 4;
+    // per-warp list of the entries whose stencil rows meet the warp's rows
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wy0 = (warp << 1) + 4;  // local rows + 4
+    unsigned short* wl = wlist + warp * kSpreadMax;
+    int wn = 0;
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int k = k0 + lane;
+        bool rel = false;
+        if (k < cnt) {
+            const int c = code[k];
+            const int oy = (c >> 8) & 0xff, hy = (c >> 20) & 0xf;
+            rel = !(oy + hy < wy0 || oy > wy0 + 1);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, rel);
+        if (rel) wl[wn + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)k;
+        wn += __popc(bal);
+    }
+    __syncwarp();
+    const int lx = lane & 15, ly = threadIdx.x >> 4;
     const int x = tileX0 + lx, y = tileY0 + ly;
-    const bool inside = x < nx && y < ny;
     double ax = 0.0, ay = 0.0;
-    // a warp covers local rows wy0, wy0+1 (+4 offset): entries whose stencil
-    // rows miss both are skipped by a warp-uniform test
-    const int wy0 = ((threadIdx.x >> 5) << 1) + 4;
-    for (int k = 0; k < cnt; ++k) {
+    for (int e = 0; e < wn; ++e) {
+        const int k = wl[e];
         const int c = code[k];
-        const int oy = (c >> 8) & 0xff, hy = (c >> 20) & 0xf;
-        if (oy + hy < wy0 || oy > wy0 + 1) continue;
-        const int ox = c & 0xff, hx = (c >> 16) & 0xf;
+        const int ox = c & 0xff, oy = (c >> 8) & 0xff, hx = (c >> 16) & 0xf, hy = (c >> 20) & 0xf;
         const int dx = lx + 4 - ox, dy = ly + 4 - oy;
         bool hit;
         if (hx == 3 && hy == 3) {
@@ -292,12 +330,13 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
             hit = in_stencil(sc, x, y);
         }
         if (hit) {
-            const double dl = dirac((double)x - sx[k], (double)y - sy[k]);
+            const double* f = fac + 10 * k;
+            const double dl = (f[dx] * f[5 + dy]) / 16.0;
             ax += sfx[k] * dl;
             ay += sfy[k] * dl;
         }
     }
-    if (!inside) return;
+    if (x >= nx || y >= ny) return;
     const size_t n = (size_t)y * nx + x;
     force[n] = (Real)ax;
     force[L + n] = (Real)ay;
@@ -614,7 +653,8 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 // changed nodes among its E,N,W,S,NE (read after write) and SW (write after
 // read) neighbours, and processes nodes in rounds once those are done.
 constexpr int kReinitMax = 4096;  // changed nodes per step (dynamic shared memory)
-constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1);
+constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1) +
+                                sizeof(cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024>::TempStorage) + 16;
 
 template <typename Real>
 __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int nS,
@@ -674,6 +714,24 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     }
 }
 
+typedef cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024> ReinitSortMax;
+
+template <int ITEMS>
+__device__ __forceinline__ void reinit_sort(const CrossDev& c, int cnt, unsigned long long* key, void* tmp) {
+    typedef cub::BlockRadixSort<unsigned long long, 1024, ITEMS> Sort;
+    typename Sort::TempStorage& sortTmp = *(typename Sort::TempStorage*)tmp;
+    unsigned long long kv[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int k = threadIdx.x * ITEMS + j;
+        kv[j] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
+    }
+    Sort(sortTmp).Sort(kv, 32, 64);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) key[threadIdx.x * ITEMS + j] = kv[j];
+    __syncthreads();
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int nS,
                                                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2,
@@ -693,21 +751,9 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[6] = (int(*)[6])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    {
-        // sort by node index (row-major order): keys node << 32 | newDom
-        typedef cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024> Sort;
-        __shared__ typename Sort::TempStorage sortTmp;
-        unsigned long long kv[kReinitMax / 1024];
-#pragma unroll
-        for (int j = 0; j < kReinitMax / 1024; ++j) {
-            const int k = threadIdx.x * (kReinitMax / 1024) + j;
-            kv[j] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
-        }
-        Sort(sortTmp).Sort(kv, 32, 64);
-#pragma unroll
-        for (int j = 0; j < kReinitMax / 1024; ++j) key[threadIdx.x * (kReinitMax / 1024) + j] = kv[j];
-        __syncthreads();
-    }
+    // sort by node index (row-major order): keys node << 32 | newDom
+    if (cnt <= 1024) reinit_sort<1>(c, cnt, key, done + kReinitMax);
+    else reinit_sort<kReinitMax / 1024>(c, cnt, key, done + kReinitMax);
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
         const size_t n = (size_t)(key[k] >> 32);
         const int x = (int)(n % nx), y = (int)(n / nx);
