@@ -219,8 +219,13 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
     }
 }
 
-constexpr int kSpreadMax = 768;  // membrane stencils per tile held in shared memory
-constexpr size_t kSpreadSmem = (size_t)kSpreadMax * (12 * sizeof(double) + 2 * sizeof(int) + 8 * sizeof(unsigned short));
+// Membrane stencils per tile held in shared memory: most tiles hold fewer than
+// kSpreadSmall; the others go to the kSpreadLarge variant.
+constexpr int kSpreadSmall = 256;
+constexpr int kSpreadLarge = 768;
+constexpr size_t spread_smem(int cap) {
+    return (size_t)cap * (12 * sizeof(double) + 2 * sizeof(int) + 8 * sizeof(unsigned short));
+}
 
 // Per-tile entry: the stencil origin relative to the tile (+4) and the stencil
 // widths, packed in one word: ox | oy << 8 | (x1-x0) << 16 | (y1-y0) << 20.
@@ -253,13 +258,14 @@ __device__ __forceinline__ void sort_tile_list(const int* list, int cnt, int sor
 // covers two rows of the tile and first collects, in id order, the entries
 // whose stencil rows meet its rows; every lattice node then adds its
 // contributions in id order.
-template <typename Real>
+template <typename Real, int kSpreadMax, int kMinCount>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
                                                      Status* st, int sortBits) {
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
-    if (cnt == 0) return;
+    // each size class handles the tiles whose count it fits best
+    if (cnt == 0 || cnt < kMinCount || (kMinCount == 0 && cnt > kSpreadMax)) return;
     if (cnt > kSpreadMax || t.start[tile] + cnt > t.cap) {
         if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
         return;
@@ -271,11 +277,11 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     int* code = (int*)(sfy + kSpreadMax);
     int* order = code + kSpreadMax;                      // sorted membrane indices
     unsigned short* wlist = (unsigned short*)(order + kSpreadMax);  // 8 warps x kSpreadMax
-    __shared__ __align__(16) unsigned char sortTmp[sizeof(typename cub::BlockRadixSort<int, 256, kSpreadMax / 256>::TempStorage)];
+    __shared__ __align__(16) unsigned char sortTmp[sizeof(typename cub::BlockRadixSort<int, 256, (kSpreadMax + 255) / 256>::TempStorage)];
     const int* list = t.list + t.start[tile];
-    if (cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
-    else if (cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
-    else sort_tile_list<kSpreadMax / 256>(list, cnt, sortBits, order, sortTmp);
+    if (kSpreadMax <= 256 || cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
+    else if (kSpreadMax <= 512 || cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
+    else sort_tile_list<(kSpreadMax + 255) / 256>(list, cnt, sortBits, order, sortTmp);
     __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
@@ -352,10 +358,10 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
-    constexpr size_t smemBytes = kSpreadSmem;
     int bits = 1;
     while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
-    spread_kernel<Real><<<t.nTiles, 256, smemBytes, s>>>(m, t, force, nx, ny, L, st, bits);
+    spread_kernel<Real, kSpreadSmall, 0><<<t.nTiles, 256, spread_smem(kSpreadSmall), s>>>(m, t, force, nx, ny, L, st, bits);
+    spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1><<<t.nTiles, 256, spread_smem(kSpreadLarge), s>>>(m, t, force, nx, ny, L, st, bits);
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
                                     cudaStream_t);
@@ -1017,8 +1023,10 @@ void launch_area_regulator(const MembraneDev& m, double* area, double* target, d
 namespace lbib {
 
 void init_kernel_attributes() {
-    cudaFuncSetAttribute(spread_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpreadSmem);
-    cudaFuncSetAttribute(spread_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpreadSmem);
+    cudaFuncSetAttribute(spread_kernel<double, kSpreadSmall, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadSmall));
+    cudaFuncSetAttribute(spread_kernel<float, kSpreadSmall, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadSmall));
+    cudaFuncSetAttribute(spread_kernel<double, kSpreadLarge, kSpreadSmall + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadLarge));
+    cudaFuncSetAttribute(spread_kernel<float, kSpreadLarge, kSpreadSmall + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadLarge));
     cudaFuncSetAttribute(reinit_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
     cudaFuncSetAttribute(reinit_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
     init_kernel_attributes_topology();
