@@ -103,6 +103,23 @@ int lbib_download_connections(lbib_handle* h, unsigned* conn);
  * dom[k], area[k] for k < return value (capped at cap). Negative on error. */
 int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
 
+/* The same cell areas as lbib_areas, computed without any allocation: no
+ * cudaMalloc, no host heap.  No counterpart in the reference.  For callers
+ * that must not allocate while a run is under way, such as a host that
+ * reserved the device memory for itself, or a tight per-step loop where an
+ * allocator call (and the synchronisation it can bring) is not acceptable.
+ * The per-cell sums go to one fixed array in device memory of 16384 doubles
+ * (128 KB); a simulation with more cells is rejected with
+ * -LBIB_ERR_CAPACITY, its message readable by lbib_last_error, and the
+ * handle stays usable.  Every call on a device, from any handle, shares
+ * that one array: each call writes every entry it reads, so nothing in it
+ * needs to start at zero, but calls that overlap in time (two threads, or
+ * two handles on different streams) race on it and must be serialised by
+ * the caller.  The first call on a device looks up the array's address;
+ * make that call before any stream capture.  Returns the number of cells,
+ * as lbib_areas. */
+int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
+
 /* Sets species k's production rate per domain id (rates[0..n), n <= number of
  * domain ids), taking effect at the next step.  This is the per-domain table
  * that a host BioSolver plugin would otherwise write node by node through

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "liblbibcuda.so")
 SYMBOLS = (
     "lbib_create_from_files", "lbib_destroy", "lbib_step", "lbib_lattice_step", "lbib_get_sizes",
     "lbib_download_lattice", "lbib_upload_lattice", "lbib_download_membrane", "lbib_download_connections",
-    "lbib_areas", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
+    "lbib_areas", "lbib_areas_static", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
 )
 
 _lib = None
@@ -59,6 +59,8 @@ def load() -> ctypes.CDLL:
     L.lbib_download_connections.argtypes = [vp, vp]
     L.lbib_areas.restype = ip
     L.lbib_areas.argtypes = [vp, vp, vp, ip]
+    L.lbib_areas_static.restype = ip
+    L.lbib_areas_static.argtypes = [vp, vp, vp, ip]
     L.lbib_last_error.restype = ip
     L.lbib_last_error.argtypes = [vp, cp, ip, ctypes.POINTER(ctypes.c_longlong)]
     L.lbib_last_timing.restype = ip

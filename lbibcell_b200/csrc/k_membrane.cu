@@ -1010,6 +1010,14 @@ void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
     areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, nullptr);
 }
 
+// The fixed device array of lbib_areas_static: the per-cell sums of one call.
+// Every call on a device writes and reads this same array.
+static __device__ __align__(256) double g_areaScratch[kStaticAreaCells];
+
+cudaError_t static_area_scratch(double** ptr) {
+    return cudaGetSymbolAddress((void**)ptr, g_areaScratch);
+}
+
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;

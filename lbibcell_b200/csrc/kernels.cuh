@@ -138,6 +138,11 @@ void launch_area_regulator(const MembraneDev& m, double* area, double* target, d
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s);
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
 
+// Cells that fit the fixed device array of lbib_areas_static (16384 doubles,
+// 128 KB), and the address of that array on the current device.
+constexpr int kStaticAreaCells = 16384;
+cudaError_t static_area_scratch(double** ptr);
+
 // Device-side topology edits (k_topology.cu).  Each returns the number of
 // kernels it launched.
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s);

@@ -19,6 +19,7 @@
 #include <fstream>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <sstream>
 #include <stdexcept>
@@ -1505,6 +1506,63 @@ int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
             dom[c] = h.ringDomHost[c];
             area[c] = a[c];
         }
+        return h.m.nCells;
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg;
+        return -e.code;
+    }
+}
+
+}  // extern "C"
+
+namespace {
+
+// Address of the fixed area array on each device, looked up once per device
+// with that device current.
+constexpr int kStaticDevices = 64;
+std::mutex g_staticMu;
+double* g_staticArea[kStaticDevices] = {};
+
+cudaError_t static_area_address(int device, double** out) {
+    if (device < 0 || device >= kStaticDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_staticMu);
+    if (!g_staticArea[device]) {
+        double* p = nullptr;
+        const cudaError_t e = lbib::static_area_scratch(&p);
+        if (e != cudaSuccess) return e;
+        g_staticArea[device] = p;
+    }
+    *out = g_staticArea[device];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbib_areas_static(lbib_handle* hh, unsigned* dom, double* area, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    if (h.m.nCells > lbib::kStaticAreaCells) {
+        h.msg = "lbib_areas_static: " + std::to_string(h.m.nCells) + " cells exceed the fixed device array of " +
+                std::to_string(lbib::kStaticAreaCells) + " cells (use lbib_areas)";
+        return -LBIB_ERR_CAPACITY;
+    }
+    if (cap < 0 || (cap > 0 && (!dom || !area))) {
+        h.msg = "lbib_areas_static: bad output buffers";
+        return -LBIB_ERR_INPUT;
+    }
+    try {
+        CK(cudaSetDevice(h.device));
+        double* scratch = nullptr;
+        CK(static_area_address(h.device, &scratch));
+        lbib::launch_areas(h.m, scratch, h.stream);
+        CK(cudaGetLastError());
+        const int n = std::min(h.m.nCells, cap);
+        if (n > 0) CK(cudaMemcpyAsync(area, scratch, sizeof(double) * n, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        for (int c = 0; c < n; ++c) dom[c] = h.ringDomHost[c];
         return h.m.nCells;
     } catch (const HostFail& e) {
         h.err = e.code; h.msg = e.msg;
