@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -263,13 +264,13 @@ def main():
     peak, peak_kind = measured_peaks()
     avg_ms = tp_["collide_ms"] / max(1, tp_["collide_launches"])
     achieved = bytes_per_node * L / (avg_ms / 1e3) / 1e9
+    # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
+    # same kernel on this workload, from its committed summary
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    tp = os.path.join(ROOT, "profiles", "stream_collide32_tissue_1024.md")
     if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("stream_collide32_tissue_1024")
-        except (ValueError, OSError):
-            traffic = None
+        m = re.search(r"\|\s*traffic_bytes_per_launch\s*\|\s*(\d+)", open(tp).read())
+        traffic = int(m.group(1)) if m else None
 
     # ---- end to end through the public API, host buffers each step ---------
     # every step: H2D of both species' per-domain secretion tables (what a host
