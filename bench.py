@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiated-run timing")
+    ap.add_argument("--adjoint-steps", type=int, default=2000, help="T of the differentiated run")
     return ap.parse_args()
 
 
@@ -329,6 +331,33 @@ def main():
         a.close()
         b.close()
 
+    # ---- differentiated run: adjoint/forward time on the adjoint workload ----
+    adjoint = None
+    if not args.no_adjoint:
+        acfg = configs.config4()
+        apaths = acfg.write(os.path.join(tmp, f"adj_rank{rank}"))
+        T, K = args.adjoint_steps, max(1, args.adjoint_steps // 20)
+        d = runner.Simulation(apaths, runner.FP64, device=local)
+        d.step(3)  # membrane forces of a force evaluation become the default parameters
+        d.diff_begin(T, K)
+        seed = np.random.default_rng(0).normal(size=(len(acfg.species), acfg.nx * acfg.ny))
+        d.diff_forward()  # untimed: first touch of the checkpoint memory
+        d.diff_backward(seed)
+        torch.cuda.synchronize()
+        d.diff_forward()
+        fwd_ms = dist_max(d.last_timing()["total_ms"], world)
+        g = d.diff_backward(seed)
+        bwd_ms = dist_max(d.last_timing()["total_ms"], world)
+        d.diff_end()
+        d.close()
+        AL = acfg.nx * acfg.ny
+        adjoint = {"workload": f"{acfg.name}: {acfg.nx}x{acfg.ny}, {len(acfg.cells)} cells, "
+                               f"{len(acfg.species)} species, frozen geometry, FP64",
+                   "T": T, "K": K, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                   "forward_mlups": world * AL * T / (fwd_ms / 1e3) / 1e6,
+                   "backward_note": "segment recompute from checkpoints + adjoint steps",
+                   "grad_finite": bool(np.isfinite(g["force"]).all() and np.isfinite(g["tau"]).all())}
+
     if rank != 0:
         return
     cpu = None
@@ -361,7 +390,8 @@ def main():
                      "launches_timed": tp_["collide_launches"], "peak_source": peak_kind},
         "fp64": fp64,
         "fp32_over_fp64": (value / fp64["mlups"]) if fp64 else None,
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": (adjoint["backward_ms"] / adjoint["forward_ms"]) if adjoint else None,
+        "adjoint": adjoint,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(tm["launches"]),

@@ -127,6 +127,53 @@ int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
  * production depends on the node's domain id). */
 int lbib_set_species_source(lbib_handle* h, int k, const double* rates, int n);
 
+/* Number of domain ids (rows of the per-domain source and mass tables). */
+int lbib_get_domain_count(lbib_handle* h, int* n);
+
+/* Differentiated runs (no counterpart in the reference).  FP64 handles only.
+ *
+ * A differentiated run advances the lattice T steps with the geometry frozen
+ * at its state when lbib_diff_begin is called: the membrane positions (so the
+ * Dirac weights of the spread), the domain ids and the per-domain mass table
+ * stay fixed, exactly as in lbib_lattice_step.  Each step is the pull-stream
+ * + collide of the fluid (Luo force) and the species (with their reaction),
+ * then the box outlet when enabled.  Its parameters are the membrane node
+ * forces F_i (spread once into the force field), the relaxation times
+ * (tauFluid and each species' tau) and the per-domain production rates of the
+ * linear-source species.  The reverse pass gives the gradients of a scalar
+ * loss L of the final concentrations C_k(x) = sum of species k's five
+ * distributions, from the caller's dL/dC_k(x).
+ *
+ * lbib_diff_begin snapshots the current lattice as the run's initial state
+ * and allocates the checkpoints: one state every K steps (K <= 0 picks
+ * ceil(sqrt(T))) plus K-1 states of the segment being reversed; each state is
+ * (9 + 5 S) * Nx * Ny doubles.  The defaults of the parameters are the
+ * handle's: the membrane forces of the last force evaluation, the relaxation
+ * times and source rates of the files. */
+int lbib_diff_begin(lbib_handle* h, int T, int K);
+
+/* Runs the T forward steps from the snapshot, storing the checkpoints.
+ * memForce[M][2] (node order of lbib_download_membrane), tau[1 + S]
+ * (tauFluid, then the species in parameter-file order) and rates[S][n_domains]
+ * replace the current parameters when non-NULL and stay in effect for later
+ * calls.  outlet != 0 applies the box outlet after each step.  The final state
+ * and the spread force field become the handle's lattice
+ * (lbib_download_lattice). */
+int lbib_diff_forward(lbib_handle* h, const double* memForce, const double* tau, const double* rates, int outlet);
+
+/* Reverse pass of the last lbib_diff_forward: recomputes each segment of K
+ * steps from its checkpoint and runs the adjoint steps backwards.  dLdC[S][L]
+ * (L = Nx * Ny, node y * Nx + x) is dL/dC_k(x) at the final step.  Outputs
+ * (any may be NULL): gForce[M][2] = dL/dF_i, gTau[1 + S] = dL/dtau,
+ * gRates[S][n_domains] = dL/d rate (zero for species without a linear source).
+ * Per-domain and relaxation-time gradients are sums of atomic adds: their
+ * last bits can differ between calls. */
+int lbib_diff_backward(lbib_handle* h, const double* dLdC, double* gForce, double* gTau, double* gRates);
+
+/* Restores the snapshot taken by lbib_diff_begin (distributions, velocity and
+ * force planes) and frees the run's device memory. */
+int lbib_diff_end(lbib_handle* h);
+
 /* Last error: code; message into buf; index of the node/connection involved. */
 int lbib_last_error(lbib_handle* h, char* buf, int len, long long* index);
 

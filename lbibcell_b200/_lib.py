@@ -16,6 +16,7 @@ SYMBOLS = (
     "lbib_create_from_files", "lbib_destroy", "lbib_step", "lbib_lattice_step", "lbib_get_sizes",
     "lbib_download_lattice", "lbib_upload_lattice", "lbib_download_membrane", "lbib_download_connections",
     "lbib_areas", "lbib_areas_static", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
+    "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
 )
 
 _lib = None
@@ -69,5 +70,15 @@ def load() -> ctypes.CDLL:
     L.lbib_set_species_source.argtypes = [vp, ip, vp, ip]
     L.lbib_set_profiling.restype = ip
     L.lbib_set_profiling.argtypes = [vp, ip]
+    L.lbib_get_domain_count.restype = ip
+    L.lbib_get_domain_count.argtypes = [vp, ctypes.POINTER(ip)]
+    L.lbib_diff_begin.restype = ip
+    L.lbib_diff_begin.argtypes = [vp, ip, ip]
+    L.lbib_diff_forward.restype = ip
+    L.lbib_diff_forward.argtypes = [vp, vp, vp, vp, ip]
+    L.lbib_diff_backward.restype = ip
+    L.lbib_diff_backward.argtypes = [vp, vp, vp, vp, vp]
+    L.lbib_diff_end.restype = ip
+    L.lbib_diff_end.argtypes = [vp]
     _lib = L
     return L

@@ -24,6 +24,7 @@ UNITS = [
     ("k_topology.cu", ["--fmad=false"]),
     ("lbib_host.cu", ["--fmad=false"]),
     ("k_lattice32.cu", []),
+    ("k_adjoint.cu", []),
 ]
 
 

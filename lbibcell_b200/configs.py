@@ -255,4 +255,30 @@ def config3(iterations: int = 5000, report_step: int = 1000, seed: int = 0) -> C
                   report_step=report_step, cells=cells, species=species)
 
 
-CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "toy": toy}
+def config4(iterations: int = 2000, report_step: int = 1000, seed: int = 0) -> Config:
+    """Adjoint workload, 512x512: 50 Poisson-disk cells r~U(12,18), node spacing
+    0.5, one species (tau 0.8) produced in every cell at a seeded per-cell
+    rate U(0.5, 1.5) * 1e-3.  Differentiated over T=2000 steps with a
+    checkpoint every 100."""
+    cells = poisson_tissue(512, 512, 12.0, 18.0, 0.5, seed, max_cells=50)
+    rng = np.random.default_rng(seed + 4)
+    rates = {d: float(1e-3 * rng.uniform(0.5, 1.5)) for d, _ in cells}
+    species = [Species(SPECIES_NAMES[0], 0.8, source=rates)]
+    return Config(name="adjoint_512", nx=512, ny=512, tau_fluid=1.0, iterations=iterations,
+                  report_step=report_step, cells=cells, species=species, area=None)
+
+
+def config5(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> Config:
+    """Adjoint workload, 2048x2048: 1000 Poisson-disk cells r~U(10,16), two
+    species (tau 0.8, 1.2) with seeded per-cell rates.  Differentiated over
+    T=10000 steps with sqrt(T) checkpoints."""
+    cells = poisson_tissue(2048, 2048, 10.0, 16.0, 0.5, seed, max_cells=1000)
+    rng = np.random.default_rng(seed + 5)
+    species = [Species(SPECIES_NAMES[k], t, source={d: float(1e-3 * rng.uniform(0.5, 1.5)) for d, _ in cells})
+               for k, t in enumerate((0.8, 1.2))]
+    return Config(name="adjoint_2048", nx=2048, ny=2048, tau_fluid=1.0, iterations=iterations,
+                  report_step=report_step, cells=cells, species=species, area=None)
+
+
+CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "config4": config4, "config5": config5,
+           "toy": toy}

@@ -431,6 +431,38 @@ template void launch_interp_move<double>(const MembraneDev&, const double*, int,
 template void launch_interp_move<float>(const MembraneDev&, const float*, int, int, size_t, CrossDev&, Status*,
                                         unsigned, cudaStream_t);
 
+// Adjoint of the spread for a differentiated run with frozen positions.  The
+// spread adds dirac(x - X_i) * F_i to every lattice node x of node i's stencil
+// (GeometryNode::distributeForce, GeometryNode.cpp:228-235), so
+// dL/dF_i = sum over the same 16 slots of dirac * dL/dF(x): the interpolation
+// of collectVelocity (GeometryNode.cpp:216-226) applied to G = dL/dF.
+__global__ void force_adjoint_kernel(MembraneDev m, const double* G, int nx, int ny, size_t L, double* gfx,
+                                     double* gfy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const double X = m.x[i], Y = m.y[i];
+    Stencil sc;
+    double gx = 0.0, gy = 0.0;
+    if (stencil_range(X, Y, nx, ny, sc)) {
+        for (int k = 0; k < 16; ++k) {
+            int xk, yk;
+            stencil_slot(sc, k, xk, yk);
+            const size_t n = (size_t)yk * nx + xk;
+            const double dl = dirac((double)xk - X, (double)yk - Y);
+            gx += G[n] * dl;
+            gy += G[L + n] * dl;
+        }
+    }
+    gfx[i] = gx;
+    gfy[i] = gy;
+}
+
+void launch_force_adjoint(const MembraneDev& m, const double* G, int nx, int ny, size_t L, double* gfx,
+                          double* gfy, cudaStream_t s) {
+    if (m.Mcap == 0) return;
+    force_adjoint_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, G, nx, ny, L, gfx, gfy);
+}
+
 // Connection::perturbConnection's tests (Connection.cpp:339, 363).
 __global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
     if (st->halt) return;

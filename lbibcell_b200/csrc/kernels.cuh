@@ -150,6 +150,40 @@ int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 size_t topo_scan_bytes(int n);
 
+// Adjoint of one FP64 lattice step of a differentiated run (k_adjoint.cu).
+struct AdjointArgs {
+    int nx, ny;
+    size_t L;
+    int S;
+    const double* fprev;   // 9*L      state after step t-1
+    const double* gprev;   // S*5*L
+    const double* pf;      // 9*L      adjoint planes of step t+1 (unused with seed)
+    const double* pg;      // S*5*L
+    const double* seed;    // S*L      dL/dC_k at the final step, or nullptr
+    double* qf;            // 9*L      adjoint planes of step t (output)
+    double* qg;            // S*5*L
+    const double* force;   // 2*L      spread force field (valid where tileCount > 0)
+    const int* tileCount;
+    int tilesX;
+    const uint32_t* dom;
+    const double* massTab; // per-domain rhoToAdd, or nullptr
+    int nDomains;
+    const double* srcTab;  // [S][nDomains]
+    double tauF;
+    SpeciesConst sp[kMaxSpecies];
+    unsigned iteration;    // iteration counter during step t
+    int outlet;
+    double* G;             // 2*L      dL/dF(x), summed over steps
+    double* grad;          // 1 + S + S*nDomains
+};
+void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s);
+void launch_set_iteration(Status* st, unsigned it, cudaStream_t s);
+
+// Transpose of the spread under fixed positions: gf[i] = sum over node i's 16
+// stencil slots of dirac * G(x) (k_membrane.cu).
+void launch_force_adjoint(const MembraneDev& m, const double* G, int nx, int ny, size_t L, double* gfx,
+                          double* gfy, cudaStream_t s);
+
 // Opt-in shared-memory sizes of the kernels that need more than 48 KB; called
 // once before any launch (and so before any stream capture).
 void init_kernel_attributes();

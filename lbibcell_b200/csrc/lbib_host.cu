@@ -76,6 +76,41 @@ static T* dalloc(size_t n) {
     return p;
 }
 
+// Device state of a differentiated run (lbib_diff_*): the snapshot it starts
+// from, the checkpoints of the forward pass, one segment of recomputed states,
+// the adjoint planes and the gradient accumulators.  A "state" is the fluid
+// planes (9*L) followed by the species planes (S*5*L), FP64.
+struct DiffCtx {
+    int T = 0, K = 0, nSeg = 0;
+    size_t stateDoubles = 0;
+    double* x0 = nullptr;     // state at step 0
+    double* u0 = nullptr;     // velocity and force planes at step 0 (restored by lbib_diff_end), 4*L
+    double* ck = nullptr;     // states at steps K, 2K, ... (nSeg - 1 of them)
+    double* seg = nullptr;    // states base+1 .. base+K-1 of the segment being reversed
+    double* P[2] = {nullptr, nullptr};
+    double* G = nullptr;      // 2*L
+    double* force = nullptr;  // 2*L spread of the parameter forces
+    double* fxp = nullptr;    // membrane forces (parameters), Mcap each
+    double* fyp = nullptr;
+    double* gfx = nullptr;
+    double* gfy = nullptr;
+    double* srcTab = nullptr; // S*nDomains
+    double* seed = nullptr;   // S*L
+    double* grad = nullptr;   // 1 + S + S*nDomains
+    Status* st = nullptr;
+    double tauF = 1.0;
+    double tau[kMaxSpecies] = {1.0, 1.0, 1.0};
+    int outlet = 0;
+    unsigned it0 = 0;
+    bool forwardDone = false;
+    double* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateDoubles; }
+    ~DiffCtx() {
+        auto fr = [](void* p) { if (p) cudaFree(p); };
+        fr(x0); fr(u0); fr(ck); fr(seg); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(fxp); fr(fyp); fr(gfx); fr(gfy);
+        fr(srcTab); fr(seed); fr(grad); fr(st);
+    }
+};
+
 struct Handle {
     // parameters
     int nx = 0, ny = 0, S = 0;
@@ -156,11 +191,14 @@ struct Handle {
     double lastTotalMs = 0, lastCollideMs = 0;
     long long lastCollideLaunches = 0;
 
+    DiffCtx* diff = nullptr;
+
     ~Handle();
 };
 
 Handle::~Handle() {
     cudaSetDevice(device);
+    delete diff;
     auto fr = [](void* p) { if (p) cudaFree(p); };
     for (int i = 0; i < 2; ++i) { fr(f[i]); fr(g[i]); }
     fr(u); fr(force); fr(dom); fr(massTab); fr(srcTab); fr(ctypeTab);
@@ -1225,6 +1263,167 @@ static void cure_lattice(Handle& h, HostMembrane& hm) {
     write_status(h);
 }
 
+// ---------------------------------------------------------------------------
+// Differentiated runs (lbib_diff_*): frozen geometry, FP64, checkpoints every
+// K steps and segment-by-segment recomputation in the backward pass.
+
+static void diff_begin(Handle& h, int T, int K) {
+    delete h.diff;
+    h.diff = nullptr;
+    pull_topology(h);
+    const size_t L = h.L;
+    const int S = h.S;
+    const int nSeg = (T + K - 1) / K;
+    const size_t stateDoubles = (size_t)(9 + 5 * S) * L;
+    const size_t states = 1 + (size_t)(nSeg - 1) + (size_t)(K - 1) + 2;
+    const size_t bytes = sizeof(double) * (states * stateDoubles + 10 * L + (size_t)S * L + 4 * (size_t)h.Mcap +
+                                           2 * (size_t)S * h.nDomains + 1 + S);
+    size_t freeB = 0, totalB = 0;
+    CK(cudaMemGetInfo(&freeB, &totalB));
+    if (bytes + (256u << 20) > freeB)
+        fail(ERR_CAPACITY, "differentiated run needs " + std::to_string(bytes >> 20) + " MiB of device memory, " +
+                               std::to_string(freeB >> 20) + " MiB free (raise K or lower T)");
+    std::unique_ptr<DiffCtx> d(new DiffCtx());
+    d->T = T; d->K = K; d->nSeg = nSeg; d->stateDoubles = stateDoubles;
+    d->x0 = dalloc<double>(stateDoubles);
+    d->u0 = dalloc<double>(4 * L);
+    d->ck = dalloc<double>((size_t)(nSeg - 1) * stateDoubles);
+    d->seg = dalloc<double>((size_t)(K - 1) * stateDoubles);
+    d->P[0] = dalloc<double>(stateDoubles);
+    d->P[1] = dalloc<double>(stateDoubles);
+    d->G = dalloc<double>(2 * L);
+    d->force = dalloc<double>(2 * L);
+    d->fxp = dalloc<double>(h.Mcap); d->fyp = dalloc<double>(h.Mcap);
+    d->gfx = dalloc<double>(h.Mcap); d->gfy = dalloc<double>(h.Mcap);
+    d->srcTab = dalloc<double>((size_t)S * h.nDomains);
+    d->seed = dalloc<double>((size_t)S * L);
+    d->grad = dalloc<double>(1 + S + (size_t)S * h.nDomains);
+    d->st = dalloc<Status>(1);
+    CK(cudaMemsetAsync(d->st, 0, sizeof(Status), h.stream));
+    CK(cudaMemsetAsync(d->force, 0, sizeof(double) * 2 * L, h.stream));
+    // snapshot of the lattice and the run's default parameters
+    CK(cudaMemcpyAsync(d->x0, h.f[h.cur], sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
+    if (S) CK(cudaMemcpyAsync(d->x0 + 9 * L, h.g[h.cur], sizeof(double) * 5 * S * L, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(d->u0, h.u, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(d->u0 + 2 * L, h.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    if (S) CK(cudaMemcpyAsync(d->srcTab, h.srcTab, sizeof(double) * S * h.nDomains, cudaMemcpyDeviceToDevice, h.stream));
+    if (h.m.M) {
+        CK(cudaMemcpyAsync(d->fxp, h.m.fx, sizeof(double) * h.m.M, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaMemcpyAsync(d->fyp, h.m.fy, sizeof(double) * h.m.M, cudaMemcpyDeviceToDevice, h.stream));
+    }
+    d->tauF = h.tauF;
+    for (int k = 0; k < S; ++k) d->tau[k] = h.sp[k].c.tau;
+    d->outlet = h.outlet ? 1 : 0;
+    d->it0 = h.iteration;
+    CK(cudaStreamSynchronize(h.stream));
+    h.diff = d.release();
+}
+
+static bool diff_needs_iteration(const Handle& h) {
+    for (int k = 0; k < h.S; ++k)
+        if (h.sp[k].c.kind == RX_SIGNAL) return true;
+    return false;
+}
+
+// Forward step t of the differentiated run: state `in` (after step t-1) to `out`.
+static void diff_forward_step(Handle& h, DiffCtx& d, const double* in, double* out, int t) {
+    const unsigned it = d.it0 + (unsigned)(t - 1);
+    if (diff_needs_iteration(h)) launch_set_iteration(d.st, it, h.stream);
+    LatticeArgs<double> a = lattice_args<double>(h, it, h.cur);
+    a.fin = in; a.fout = out;
+    a.gin = in + 9 * h.L; a.gout = out + 9 * h.L;
+    a.force = d.force;
+    a.srcTab = d.srcTab;
+    a.tauF = d.tauF;
+    for (int k = 0; k < h.S; ++k) a.sp[k].tau = d.tau[k];
+    a.status = d.st;
+    a.outlet = d.outlet;
+    launch_stream_collide64(a, h.stream);
+}
+
+static void diff_check_status(Handle& h, DiffCtx& d) {
+    Status st{};
+    CK(cudaMemcpyAsync(&st, d.st, sizeof(Status), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    if (st.err) fail(st.err, "differentiated run: device error in the force spread", st.errIndex);
+}
+
+static void diff_forward(Handle& h, DiffCtx& d) {
+    const size_t L = h.L;
+    MembraneDev mp = h.m;
+    mp.fx = d.fxp;
+    mp.fy = d.fyp;
+    launch_spread<double>(mp, h.tiles, d.force, h.nx, h.ny, L, d.st, d.it0, h.stream);
+    const double* in = d.x0;
+    double* out = nullptr;
+    for (int t = 1; t <= d.T; ++t) {
+        out = (t % d.K == 0 && t < d.T) ? d.state(t / d.K) : d.P[t & 1];
+        diff_forward_step(h, d, in, out, t);
+        in = out;
+    }
+    // the final state and the force field become the handle's lattice, for
+    // lbib_download_lattice
+    CK(cudaMemcpyAsync(h.force, d.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.f[h.cur], in, sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
+    if (h.S)
+        CK(cudaMemcpyAsync(h.g[h.cur], in + 9 * L, sizeof(double) * 5 * h.S * L, cudaMemcpyDeviceToDevice,
+                           h.stream));
+    CK(cudaGetLastError());
+    diff_check_status(h, d);
+    d.forwardDone = true;
+}
+
+static void diff_backward(Handle& h, DiffCtx& d) {
+    const size_t L = h.L;
+    const int S = h.S;
+    CK(cudaMemsetAsync(d.G, 0, sizeof(double) * 2 * L, h.stream));
+    CK(cudaMemsetAsync(d.grad, 0, sizeof(double) * (1 + S + (size_t)S * h.nDomains), h.stream));
+    bool area = false;
+    for (int b : h.bio) area |= (b == 2);
+    AdjointArgs a{};
+    a.nx = h.nx; a.ny = h.ny; a.L = L; a.S = S;
+    a.force = d.force;
+    a.tileCount = h.tiles.count;
+    a.tilesX = h.tiles.tilesX;
+    a.dom = h.dom;
+    a.massTab = area ? h.massTab : nullptr;
+    a.nDomains = h.nDomains;
+    a.srcTab = d.srcTab;
+    a.tauF = d.tauF;
+    for (int k = 0; k < S; ++k) {
+        a.sp[k] = h.sp[k].c;
+        a.sp[k].tau = d.tau[k];
+    }
+    a.outlet = d.outlet;
+    a.G = d.G;
+    a.grad = d.grad;
+    for (int s = d.nSeg - 1; s >= 0; --s) {
+        const int base = s * d.K;
+        const int len = std::min(d.K, d.T - base);
+        // recompute states base+1 .. base+len-1 from the checkpoint
+        auto segState = [&](int j) -> double* {  // state base + j, 0 <= j < len
+            return j == 0 ? d.state(s) : d.seg + (size_t)(j - 1) * d.stateDoubles;
+        };
+        for (int j = 1; j < len; ++j) diff_forward_step(h, d, segState(j - 1), segState(j), base + j);
+        for (int t = base + len; t > base; --t) {
+            const double* prev = segState(t - 1 - base);
+            a.fprev = prev;
+            a.gprev = prev + 9 * L;
+            const bool seedStep = t == d.T;
+            const double* pin = d.P[(t + 1) & 1];
+            a.pf = seedStep ? nullptr : pin;
+            a.pg = seedStep ? nullptr : pin + 9 * L;
+            a.seed = seedStep ? d.seed : nullptr;
+            a.qf = d.P[t & 1];
+            a.qg = d.P[t & 1] + 9 * L;
+            a.iteration = d.it0 + (unsigned)(t - 1);
+            launch_adjoint_step64(a, h.stream);
+        }
+    }
+    launch_force_adjoint(h.m, d.G, h.nx, h.ny, L, d.gfx, d.gfy, h.stream);
+    CK(cudaGetLastError());
+}
+
 }  // namespace lbib
 
 // ---------------------------------------------------------------------------
@@ -1601,6 +1800,113 @@ int lbib_set_profiling(lbib_handle* hh, int on) {
     if (!hh) return LBIB_ERR_STATE;
     hh->h.profiling = on != 0;
     return LBIB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiated runs.
+
+extern "C" {
+
+int lbib_get_domain_count(lbib_handle* hh, int* n) {
+    API_BEGIN(hh)
+    if (!n) lbib::fail(LBIB_ERR_INPUT, "lbib_get_domain_count: NULL output");
+    *n = h.nDomains;
+    API_END
+}
+
+int lbib_diff_begin(lbib_handle* hh, int T, int K) {
+    API_BEGIN(hh)
+    if (h.precision != LBIB_FP64) lbib::fail(LBIB_ERR_STATE, "differentiated runs need an FP64 handle");
+    if (T < 1) lbib::fail(LBIB_ERR_INPUT, "differentiated run: T must be at least 1");
+    if (K <= 0) K = (int)std::ceil(std::sqrt((double)T));
+    if (K > T) K = T;
+    lbib::diff_begin(h, T, K);
+    API_END
+}
+
+int lbib_diff_forward(lbib_handle* hh, const double* memForce, const double* tau, const double* rates, int outlet) {
+    API_BEGIN(hh)
+    if (!h.diff) lbib::fail(LBIB_ERR_STATE, "lbib_diff_forward before lbib_diff_begin");
+    lbib::DiffCtx& d = *h.diff;
+    if (tau) {
+        for (int k = 0; k <= h.S; ++k)
+            if (!(tau[k] > 0.5)) lbib::fail(LBIB_ERR_INPUT, "relaxation times must exceed 0.5", k);
+        d.tauF = tau[0];
+        for (int k = 0; k < h.S; ++k) d.tau[k] = tau[1 + k];
+    }
+    if (rates && h.S)
+        CK(cudaMemcpyAsync(d.srcTab, rates, sizeof(double) * h.S * h.nDomains, cudaMemcpyHostToDevice, h.stream));
+    const int M = h.m.M;
+    if (memForce && M) {
+        std::vector<double> fx(M), fy(M);
+        for (int i = 0; i < M; ++i) { fx[i] = memForce[2 * i]; fy[i] = memForce[2 * i + 1]; }
+        CK(cudaMemcpyAsync(d.fxp, fx.data(), sizeof(double) * M, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(d.fyp, fy.data(), sizeof(double) * M, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    }
+    d.outlet = outlet ? 1 : 0;
+    CK(cudaEventRecord(h.evA, h.stream));
+    lbib::diff_forward(h, d);
+    CK(cudaEventRecord(h.evB, h.stream));
+    CK(cudaEventSynchronize(h.evB));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
+    h.lastTotalMs = ms;
+    API_END
+}
+
+int lbib_diff_backward(lbib_handle* hh, const double* dLdC, double* gForce, double* gTau, double* gRates) {
+    API_BEGIN(hh)
+    if (!h.diff || !h.diff->forwardDone) lbib::fail(LBIB_ERR_STATE, "lbib_diff_backward before lbib_diff_forward");
+    if (!dLdC && h.S) lbib::fail(LBIB_ERR_INPUT, "lbib_diff_backward: dLdC is NULL");
+    lbib::DiffCtx& d = *h.diff;
+    const size_t L = h.L;
+    if (h.S) CK(cudaMemcpyAsync(d.seed, dLdC, sizeof(double) * h.S * L, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    CK(cudaEventRecord(h.evA, h.stream));
+    lbib::diff_backward(h, d);
+    CK(cudaEventRecord(h.evB, h.stream));
+    CK(cudaEventSynchronize(h.evB));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
+    h.lastTotalMs = ms;
+    const size_t nG = 1 + h.S + (size_t)h.S * h.nDomains;
+    std::vector<double> grad(nG);
+    CK(cudaMemcpy(grad.data(), d.grad, sizeof(double) * nG, cudaMemcpyDeviceToHost));
+    if (gTau) {
+        gTau[0] = -grad[0] / (d.tauF * d.tauF);
+        for (int k = 0; k < h.S; ++k) gTau[1 + k] = -grad[1 + k] / (d.tau[k] * d.tau[k]);
+    }
+    if (gRates)
+        for (size_t i = 0; i < (size_t)h.S * h.nDomains; ++i) gRates[i] = grad[1 + h.S + i];
+    const int M = h.m.M;
+    if (gForce && M) {
+        std::vector<double> gx(M), gy(M);
+        CK(cudaMemcpy(gx.data(), d.gfx, sizeof(double) * M, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gy.data(), d.gfy, sizeof(double) * M, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < M; ++i) { gForce[2 * i] = gx[i]; gForce[2 * i + 1] = gy[i]; }
+    }
+    API_END
+}
+
+int lbib_diff_end(lbib_handle* hh) {
+    API_BEGIN(hh)
+    if (h.diff) {
+        lbib::DiffCtx& d = *h.diff;
+        const size_t L = h.L;
+        CK(cudaMemcpyAsync(h.f[h.cur], d.x0, sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
+        if (h.S)
+            CK(cudaMemcpyAsync(h.g[h.cur], d.x0 + 9 * L, sizeof(double) * 5 * h.S * L, cudaMemcpyDeviceToDevice,
+                               h.stream));
+        CK(cudaMemcpyAsync(h.u, d.u0, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.force, d.u0 + 2 * L, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        delete h.diff;
+        h.diff = nullptr;
+    }
+    API_END
 }
 
 }  // extern "C"

@@ -149,3 +149,39 @@ class Simulation:
         if n < 0:
             raise self._error()
         return {int(d[i]): float(a[i]) for i in range(n)}
+
+    # -- differentiated runs (frozen geometry, FP64) -----------------------------
+    def domain_count(self) -> int:
+        n = ctypes.c_int(0)
+        self._check(self._L.lbib_get_domain_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def diff_begin(self, T: int, K: int = 0) -> None:
+        """Snapshot the lattice as the initial state of a T-step differentiated
+        run with a checkpoint every K steps (K <= 0: ceil(sqrt(T)))."""
+        self._check(self._L.lbib_diff_begin(self._h, int(T), int(K)))
+
+    def diff_forward(self, forces=None, tau=None, rates=None, outlet: bool = True) -> None:
+        """T forward steps from the snapshot.  forces (M, 2) membrane node
+        forces, tau (1 + S,) relaxation times, rates (S, n_domains) source rates;
+        None keeps the current values."""
+        args = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (forces, tau, rates)]
+        self._check(self._L.lbib_diff_forward(self._h, *[_p(a) for a in args], 1 if outlet else 0))
+
+    def diff_backward(self, dLdC) -> Dict[str, np.ndarray]:
+        """Gradients of L from dL/dC (S, Nx*Ny) at the final step:
+        {"force": (M, 2), "tau": (1 + S,), "rates": (S, n_domains)}."""
+        z = self.sizes()
+        S, M = z["S"], z["M"]
+        seed = np.ascontiguousarray(np.asarray(dLdC, np.float64).reshape(S, z["nx"] * z["ny"]))
+        gF = np.zeros((M, 2)); gT = np.zeros(1 + S); gR = np.zeros((S, self.domain_count()))
+        self._check(self._L.lbib_diff_backward(self._h, _p(seed), _p(gF), _p(gT), _p(gR)))
+        return {"force": gF, "tau": gT, "rates": gR}
+
+    def diff_end(self) -> None:
+        """Restore the snapshot and free the run's checkpoints."""
+        self._check(self._L.lbib_diff_end(self._h))
+
+    def concentrations(self) -> np.ndarray:
+        """C_k(x) = sum of species k's distributions, shape (S, Nx*Ny)."""
+        return self.lattice().g.sum(axis=2)

@@ -1,0 +1,229 @@
+"""Differentiated lattice runs (lbib_diff_*): the hand-written adjoint against
+central finite differences of the FP64 forward and of the oracle (the CPU
+restatement of the reference's lattice step), checkpoint-interval
+invariance, and the torch.autograd.Function wrapper of the test harness.
+
+Tolerance: adjoint vs central difference within 1e-4 relative (plus a floor of
+1e-7 of the gradient's scale for components that are nearly zero)."""
+import numpy as np
+import pytest
+
+from lbibcell_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def lbib():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from lbibcell_b200 import build, runner
+    build.build()
+    return runner
+
+
+def _cfg(n=64, species=2, tau_fluid=0.9, rates=None):
+    cfg = configs.toy(n=n, r=10.0, nodes=100, iterations=100, species=species, tau_fluid=tau_fluid)
+    cfg.area = None  # no mass source: the lattice step then matches the oracle's
+    if rates is not None:
+        for k, sp in enumerate(cfg.species):
+            sp.source = {d: float(rates[k, d]) for d in range(rates.shape[1])}
+    return cfg
+
+
+def _close(adj, fd, scale, what):
+    err = abs(adj - fd)
+    assert err <= RTOL * abs(fd) + 1e-7 * scale, f"{what}: adjoint {adj:.10e} vs central difference {fd:.10e}"
+
+
+class _Problem:
+    """A differentiated run with parameters p = (forces, tau, rates) and the
+    loss L = sum(w * C) of the final concentrations."""
+
+    def __init__(self, runner, paths, T, K, seed=0, steps_before=0):
+        self.sim = runner.Simulation(paths, runner.FP64)
+        if steps_before:
+            self.sim.step(steps_before)
+        z = self.sim.sizes()
+        self.S, self.M, self.L = z["S"], z["M"], z["nx"] * z["ny"]
+        self.nD = self.sim.domain_count()
+        rng = np.random.default_rng(seed)
+        self.F = rng.normal(0.0, 2e-3, (self.M, 2))
+        self.tau = np.array([0.9, 1.1, 0.8][: 1 + self.S])
+        self.rates = rng.uniform(0.5e-3, 2e-3, (self.S, self.nD))
+        self.w = rng.normal(size=(self.S, self.L))
+        self.sim.diff_begin(T, K)
+
+    def loss(self, F=None, tau=None, rates=None):
+        self.sim.diff_forward(self.F if F is None else F, self.tau if tau is None else tau,
+                              self.rates if rates is None else rates)
+        return float((self.sim.concentrations() * self.w).sum())
+
+    def grads(self):
+        self.loss()
+        return self.sim.diff_backward(self.w)
+
+
+def test_adjoint_vs_central_differences_fp64(lbib, tmp_path):
+    """Two species with linear sources and decay, box outlet, a membrane that
+    has moved for 3 full steps; T=24 with a checkpoint every 5 steps (last
+    segment partial)."""
+    paths = _cfg().write(str(tmp_path))
+    P = _Problem(lbib, paths, T=24, K=5, steps_before=3)
+    g = P.grads()
+    # relaxation times
+    for i in range(1 + P.S):
+        h = 1e-5
+        tp, tm = P.tau.copy(), P.tau.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (P.loss(tau=tp) - P.loss(tau=tm)) / (2 * h)
+        _close(g["tau"][i], fd, np.abs(g["tau"]).max(), f"dL/dtau[{i}]")
+    # source rates of the exterior (0) and the cell (1), both species
+    for k in range(P.S):
+        for d in (0, 1):
+            h = 1e-5
+            rp, rm = P.rates.copy(), P.rates.copy()
+            rp[k, d] += h
+            rm[k, d] -= h
+            fd = (P.loss(rates=rp) - P.loss(rates=rm)) / (2 * h)
+            _close(g["rates"][k, d], fd, np.abs(g["rates"]).max(), f"dL/drate[{k},{d}]")
+    # membrane node forces: single components and one random direction
+    scaleF = np.abs(g["force"]).max()
+    assert scaleF > 0
+    for i, c in ((0, 0), (P.M // 3, 1), (int(np.argmax(np.abs(g["force"][:, 0]))), 0)):
+        h = 1e-5
+        Fp, Fm = P.F.copy(), P.F.copy()
+        Fp[i, c] += h
+        Fm[i, c] -= h
+        fd = (P.loss(F=Fp) - P.loss(F=Fm)) / (2 * h)
+        _close(g["force"][i, c], fd, scaleF, f"dL/dF[{i},{c}]")
+    v = np.random.default_rng(7).normal(size=P.F.shape)
+    h = 1e-5
+    fd = (P.loss(F=P.F + h * v) - P.loss(F=P.F - h * v)) / (2 * h)
+    _close(float((g["force"] * v).sum()), fd, np.abs(g["force"] * v).sum(), "dL/dF . v")
+    P.sim.diff_end()
+
+
+def test_adjoint_vs_central_differences_oracle(lbib, oracle_mod, tmp_path):
+    """The differentiated forward is the oracle's lattice step bit for bit, and
+    the adjoint matches central differences taken through the oracle."""
+    T = 16
+    base = _cfg()
+    paths = base.write(str(tmp_path / "base"))
+    P = _Problem(lbib, paths, T=T, K=4)
+    lat0 = P.sim.lattice()
+    g = P.grads()
+    C_gpu = P.sim.concentrations()
+    force = P.sim.lattice().force
+
+    def oracle_loss(tau, rates, tag):
+        cfg = _cfg(tau_fluid=float(tau[0]), rates=rates)
+        for k, sp in enumerate(cfg.species):
+            sp.tau = float(tau[1 + k])
+        o = oracle_mod.Oracle(cfg.write(str(tmp_path / tag)))
+        o.set_lattice(lat0.f, lat0.g, force)
+        o.lattice_step(T, outlet=True)
+        C = o.state().g.sum(axis=2)
+        return C, float((C * P.w).sum())
+
+    C_cpu, _ = oracle_loss(P.tau, P.rates, "same")
+    np.testing.assert_array_equal(C_cpu, C_gpu)
+    h = 1e-5
+    for i in range(1 + P.S):
+        tp, tm = P.tau.copy(), P.tau.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (oracle_loss(tp, P.rates, f"tp{i}")[1] - oracle_loss(tm, P.rates, f"tm{i}")[1]) / (2 * h)
+        _close(g["tau"][i], fd, np.abs(g["tau"]).max(), f"oracle dL/dtau[{i}]")
+    for k in range(P.S):
+        rp, rm = P.rates.copy(), P.rates.copy()
+        rp[k, 1] += h
+        rm[k, 1] -= h
+        fd = (oracle_loss(P.tau, rp, f"rp{k}")[1] - oracle_loss(P.tau, rm, f"rm{k}")[1]) / (2 * h)
+        _close(g["rates"][k, 1], fd, np.abs(g["rates"]).max(), f"oracle dL/drate[{k},1]")
+    P.sim.diff_end()
+
+
+def test_checkpoint_interval_and_restore(lbib, tmp_path):
+    """Gradients do not depend on the checkpoint interval; lbib_diff_end puts
+    the snapshot back."""
+    paths = _cfg(species=1).write(str(tmp_path))
+    ref = None
+    for K in (1, 4, 0, 13):
+        P = _Problem(lbib, paths, T=13, K=K, steps_before=2)
+        before = P.sim.lattice()
+        g = P.grads()
+        if ref is None:
+            ref = g
+        else:
+            np.testing.assert_array_equal(g["force"], ref["force"])
+            np.testing.assert_allclose(g["tau"], ref["tau"], rtol=1e-12)
+            np.testing.assert_allclose(g["rates"], ref["rates"], rtol=1e-12, atol=1e-300)
+        P.sim.diff_end()
+        after = P.sim.lattice()
+        for name in ("f", "g", "vel", "force", "dom"):
+            np.testing.assert_array_equal(getattr(after, name), getattr(before, name), err_msg=name)
+        P.sim.close()
+
+
+def test_diff_rejects_fp32_and_order(lbib, tmp_path):
+    paths = _cfg(species=1).write(str(tmp_path))
+    s32 = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    with pytest.raises(lbib.LbibError) as e:
+        s32.diff_begin(4)
+    assert e.value.code == 91
+    s64 = lbib.Simulation(paths, lbib.FP64)
+    s64.diff_begin(4)
+    with pytest.raises(lbib.LbibError) as e:
+        s64.diff_backward(np.zeros((1, 64 * 64)))
+    assert e.value.code == 91
+
+
+def test_autograd_function_wrapper(lbib, tmp_path):
+    """The torch.autograd.Function of the harness: a nonlinear loss of the
+    concentrations, gradients for all three parameter groups at once, checked
+    along a random direction by a central difference."""
+    import torch
+
+    paths = _cfg().write(str(tmp_path))
+    P = _Problem(lbib, paths, T=20, K=6, steps_before=2)
+    sim = P.sim
+
+    class LatticeRun(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, forces, tau, rates):
+            sim.diff_forward(forces.detach().numpy(), tau.detach().numpy(), rates.detach().numpy())
+            return torch.from_numpy(sim.concentrations())
+
+        @staticmethod
+        def backward(ctx, gC):
+            g = sim.diff_backward(gC.detach().numpy())
+            return torch.from_numpy(g["force"]), torch.from_numpy(g["tau"]), torch.from_numpy(g["rates"])
+
+    w = torch.from_numpy(P.w)
+
+    def loss_of(F, tau, rates):
+        C = LatticeRun.apply(F, tau, rates)
+        return (w * C).sum() + 50.0 * (C * C).sum()
+
+    F = torch.tensor(P.F, requires_grad=True)
+    tau = torch.tensor(P.tau, requires_grad=True)
+    rates = torch.tensor(P.rates, requires_grad=True)
+    loss = loss_of(F, tau, rates)
+    loss.backward()
+    rng = np.random.default_rng(3)
+    vF = torch.from_numpy(rng.normal(size=P.F.shape) * 1e-3)
+    vT = torch.from_numpy(rng.normal(size=P.tau.shape) * 1e-2)
+    vR = torch.from_numpy(rng.normal(size=P.rates.shape) * 1e-4)
+    directional = float((F.grad * vF).sum() + (tau.grad * vT).sum() + (rates.grad * vR).sum())
+    h = 1e-3
+    with torch.no_grad():
+        lp = float(loss_of(F + h * vF, tau + h * vT, rates + h * vR))
+        lm = float(loss_of(F - h * vF, tau - h * vT, rates - h * vR))
+    fd = (lp - lm) / (2 * h)
+    _close(directional, fd, abs(fd), "autograd directional derivative")
+    sim.diff_end()
