@@ -20,11 +20,14 @@
 // At the final step the adjoint of the stored state is the seed dL/dC_k(x)
 // (C_k = sum of the species' five values) for every species direction.
 //
-// Parameter gradients accumulate in `grad`:
-//   grad[0]                     dL/d(1/tauF)
-//   grad[1 + k]                 dL/d(1/tau_k)
-//   grad[1 + S + k*nDom + d]    dL/d source_k[d]   (RX_LINEAR species)
-// and dL/dF(x) of the force field in G (summed over steps, force tiles only).
+// Parameter gradients, accumulated without contended atomics:
+//   part[b][0], part[b][1 + k]  dL/d(1/tauF), dL/d(1/tau_k) summed by thread
+//                               block b (each block owns its slots; the same
+//                               blocks cover the same nodes every step),
+//   racc[k][x]                  dL/d source_k at node x (RX_LINEAR species),
+//   G[x]                        dL/dF(x) of the force field,
+// all summed over the steps; launch_adjoint_finish reduces part and racc into
+// grad[0..S] and grad[1 + S + k*nDomains + domain].
 #include "kernels.cuh"
 
 namespace lbib {
@@ -45,6 +48,12 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Adds v into grad[key] once per group of lanes with the same key (lanes with
 // key < 0 add nothing).  Every lane of the warp calls it.
 __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) {
+    const int key0 = __shfl_sync(0xffffffffu, key, 0);
+    if (__all_sync(0xffffffffu, key == key0)) {  // the usual case: one domain per warp
+        const double sum = warp_sum(v);
+        if ((threadIdx.x & 31) == 0 && key0 >= 0 && sum != 0.0) atomicAdd(grad + key0, sum);
+        return;
+    }
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     double sum = 0.0;
 #pragma unroll 4
@@ -58,35 +67,61 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) adjoint_step64(AdjointArgs a) {
-    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = n < a.L;
-    const size_t nn = valid ? n : 0;
+// NS = number of species (compile-time, so that every input of a node is
+// loaded before any arithmetic).  Grid (ceil(nx / 256), ny).
+template <int NS>
+__global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
-    const int x = (int)(nn % (size_t)nx), y = (int)(nn / (size_t)nx);
+    const int xr = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = xr < nx;
+    const int x = valid ? xr : nx - 1, y = blockIdx.y;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-    const size_t rC = (size_t)y * nx, rM = (size_t)ym * nx, rP = (size_t)yp * nx;
-    // forward pull sources x - c_q and adjoint gather sources x + c_q
-    const size_t pull[9] = {rC + x, rC + xm, rM + x, rC + xp, rP + x, rM + xm, rM + xp, rP + xp, rP + xm};
-    const size_t push[9] = {rC + x, rC + xp, rP + x, rC + xm, rM + x, rP + xp, rP + xm, rM + xm, rM + xp};
+    const unsigned rC = (unsigned)y * nx, rM = (unsigned)ym * nx, rP = (unsigned)yp * nx;
+    const unsigned n = rC + x;
+    // forward pull sources x - c_q and adjoint gather sources x + c_q (offsets within a plane)
+    const unsigned pull[9] = {rC + x, rC + xm, rM + x, rC + xp, rP + x, rM + xm, rM + xp, rP + xp, rP + xm};
+    const unsigned push[9] = {rC + x, rC + xp, rP + x, rC + xm, rM + x, rP + xp, rP + xm, rM + xm, rM + xp};
 
-    // ---- forward recomputation of the fluid collision -------------------
-    double f[9];
+    // ---- every input of the node, loaded before any arithmetic -----------
+    const double* __restrict__ fprev = a.fprev;
+    double f[9], lf[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = a.fprev[(size_t)q * L + pull[q]];
-    const uint32_t dom = a.dom[nn];
+    for (int q = 0; q < 9; ++q) f[q] = fprev[(size_t)q * L + pull[q]];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) lf[q] = a.seed ? 0.0 : a.pf[(size_t)q * L + push[q]];
+    double gA[NS > 0 ? NS : 1][5], muA[NS > 0 ? NS : 1][5];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const double* gp = a.gprev + (size_t)k * 5 * L;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) gA[k][q] = gp[(size_t)q * L + pull[q]];
+        if (a.seed) {
+            const double sd = a.seed[(size_t)k * L + n];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) muA[k][q] = sd;
+        } else {
+            const double* pg = a.pg + (size_t)k * 5 * L;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) muA[k][q] = pg[(size_t)q * L + push[q]];
+        }
+    }
+    const uint32_t dom = a.dom[n];
+    // The force field of a differentiated run is zero outside the force tiles,
+    // so it and G are read and written everywhere: no load waits on another.
+    const double fx = a.force[n], fy = a.force[L + n];
+    const double Gx = a.G[n], Gy = a.G[L + n];
+    double raccA[NS > 0 ? NS : 1];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) raccA[k] = a.racc[(size_t)k * L + n];
+    double gTauK[NS > 0 ? NS : 1];
     double rta = 0.0;
     if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
     if (!isfinite(rta)) rta = 0.0;
-    const bool tile = a.tileCount[(y / kTile) * a.tilesX + (x / kTile)] > 0;
-    double fx = 0.0, fy = 0.0;
-    if (tile) {
-        fx = a.force[nn];
-        fy = a.force[L + nn];
-    }
-    const double tauI = 1.0 / a.tauF;
+
+    // ---- forward recomputation of the fluid collision --------------------
+    const double tauI = a.tauIF;
     double rhoF = 0.0;
 #pragma unroll
     for (int q = 0; q < 9; ++q) rhoF += f[q];
@@ -97,99 +132,88 @@ __global__ void __launch_bounds__(256) adjoint_step64(AdjointArgs a) {
         jx += kCX[q] * f[q];
         jy += kCY[q] * f[q];
     }
-    const double ux = jx / rho, uy = jy / rho;
+    const double rhoI = 1.0 / rho;
+    const double ux = jx * rhoI, uy = jy * rhoI;
     const double lastTerm = 1.5 * (ux * ux + uy * uy);
-    double fs[9], feqw[9];
+    // equilibrium and post-collision value of direction q
+    auto feqw = [&](int q) {
+        const double cu = kCX[q] * ux + kCY[q] * uy;
+        return weight9(q) * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - lastTerm);
+    };
+    auto fs = [&](int q) {
+        return f[q] - f[q] * tauI + feqw(q) * tauI + 3.0 * weight9(q) * rhoF * (kCX[q] * fx + kCY[q] * fy);
+    };
     double jox = 0.0, joy = 0.0;
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        const double w = weight9(q);
-        const double cu = kCX[q] * ux + kCY[q] * uy;
-        feqw[q] = w * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - lastTerm);
-        fs[q] = f[q] - f[q] * tauI + feqw[q] * tauI + 3.0 * w * rhoF * (kCX[q] * fx + kCY[q] * fy);
-        jox += kCX[q] * fs[q];
-        joy += kCY[q] * fs[q];
+        const double v = fs(q);
+        jox += kCX[q] * v;
+        joy += kCY[q] * v;
     }
-    const double uox = jox / rho, uoy = joy / rho;  // FluidSolver::velocity_ after collide
+    const double uox = jox * rhoI, uoy = joy * rhoI;  // FluidSolver::velocity_ after collide
     // box outlet: node-local rescale(s) by 1/sum(f) on x = 0 and y = 0 (corner twice)
     const int passes = a.outlet ? (x == 0) + (y == 0) : 0;
     double s1 = 1.0, s2 = 1.0;
     if (passes >= 1) {
         double r = 0.0;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) r += fs[q];
+        for (int q = 0; q < 9; ++q) r += fs(q);
         s1 = 1.0 / r;
     }
     if (passes == 2) {
         double r = 0.0;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) r += fs[q] * s1;
+        for (int q = 0; q < 9; ++q) r += fs(q) * s1;
         s2 = 1.0 / r;
     }
 
-    // ---- adjoint of the stored fluid state ------------------------------
-    double lf[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) lf[q] = a.seed ? 0.0 : a.pf[(size_t)q * L + push[q]];
-
-    double D1 = 0.0, D2 = 0.0;    // dL/ds1, dL/ds2 from the species
+    // ---- species, backwards (their velocity and outlet terms feed the fluid)
+    double D1 = 0.0, D2 = 0.0;      // dL/ds1, dL/ds2 from the species
     double muox = 0.0, muoy = 0.0;  // dL/d(post-collision velocity)
-    for (int k = 0; k < a.S; ++k) {
-        const double* gp = a.gprev + (size_t)k * 5 * L;
-        double g[5];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) g[q] = gp[(size_t)q * L + pull[q]];
+    for (int k = 0; k < NS; ++k) {
+        double* g = gA[k];
+        double* mu = muA[k];
         const SpeciesConst sp = a.sp[k];
-        const double tauIk = 1.0 / sp.tau;
+        const double tauIk = a.tauI[k];
         const double C = g[0] + g[1] + g[2] + g[3] + g[4];
+        const double C3 = C * (1.0 / 3.0), C6 = C * (1.0 / 6.0);
         double temp[5];
-        temp[0] = C / 3.0;
-        temp[1] = C / 6.0 * (1.0 + 3.0 * uox);
-        temp[2] = C / 6.0 * (1.0 + 3.0 * uoy);
-        temp[3] = C / 6.0 * (1.0 - 3.0 * uox);
-        temp[4] = C / 6.0 * (1.0 - 3.0 * uoy);
-        double R = 0.0, dRdC = 0.0;
-        if (sp.kind == RX_LINEAR) {
-            double src = 0.0;
-            if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
-            R = src - sp.decay * C;
-            dRdC = -sp.decay;
-        } else if (sp.kind == RX_SIGNAL) {
-            if (dom == 1 && a.iteration < 5000u) {
-                R = 0.0001;
-            } else {
-                R = -0.00001 * C;
-                dRdC = -0.00001;
-            }
-        }
+        temp[0] = C3;
+        temp[1] = C6 * (1.0 + 3.0 * uox);
+        temp[2] = C6 * (1.0 + 3.0 * uoy);
+        temp[3] = C6 * (1.0 - 3.0 * uox);
+        temp[4] = C6 * (1.0 - 3.0 * uoy);
+        // dR/dC; the reaction value R itself only enters the outlet terms
+        double dRdC = 0.0;
+        if (sp.kind == RX_LINEAR) dRdC = -sp.decay;
+        else if (sp.kind == RX_SIGNAL && !(dom == 1 && a.iteration < 5000u)) dRdC = -0.00001;
         const bool react = sp.kind != RX_NONE;
-        double gs[5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q)
-            gs[q] = g[q] - g[q] * tauIk + temp[q] * tauIk + (react ? R * (q == 0 ? 1.0 / 3.0 : 1.0 / 6.0) : 0.0);
-
-        double mu[5];
-        if (a.seed) {
-            const double sd = a.seed[(size_t)k * L + nn];
-#pragma unroll
-            for (int q = 0; q < 5; ++q) mu[q] = sd;
-        } else {
-            const double* pg = a.pg + (size_t)k * 5 * L;
-#pragma unroll
-            for (int q = 0; q < 5; ++q) mu[q] = pg[(size_t)q * L + push[q]];
-        }
+        auto reaction = [&]() {
+            if (sp.kind == RX_LINEAR) {
+                double src = 0.0;
+                if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
+                return src - sp.decay * C;
+            }
+            if (sp.kind == RX_SIGNAL) return (dom == 1 && a.iteration < 5000u) ? 0.0001 : -0.00001 * C;
+            return 0.0;
+        };
+        const double R = passes ? reaction() : 0.0;
+        auto gs = [&](int q) {
+            return g[q] - g[q] * tauIk + temp[q] * tauIk + (react ? R * (q == 0 ? (1.0 / 3.0) : (1.0 / 6.0)) : 0.0);
+        };
         // outlet rescales of the species (same factors as the fluid)
         if (passes == 2) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                D2 += mu[q] * (gs[q] * s1);
+                D2 += mu[q] * (gs(q) * s1);
                 mu[q] *= s2;
             }
         }
         if (passes >= 1) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                D1 += mu[q] * gs[q];
+                D1 += mu[q] * gs(q);
                 mu[q] *= s1;
             }
         }
@@ -197,9 +221,10 @@ __global__ void __launch_bounds__(256) adjoint_step64(AdjointArgs a) {
         double gTau = 0.0;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gTau += mu[q] * (temp[q] - g[q]);
-        const double mR = react ? (mu[0] / 3.0 + (mu[1] + mu[2] + mu[3] + mu[4]) / 6.0) : 0.0;
-        const double mC = tauIk * (mu[0] / 3.0 + (mu[1] * (1.0 + 3.0 * uox) + mu[2] * (1.0 + 3.0 * uoy) +
-                                                  mu[3] * (1.0 - 3.0 * uox) + mu[4] * (1.0 - 3.0 * uoy)) / 6.0) +
+        const double mR = react ? (mu[0] * (1.0 / 3.0) + (mu[1] + mu[2] + mu[3] + mu[4]) * (1.0 / 6.0)) : 0.0;
+        const double mC = tauIk * (mu[0] * (1.0 / 3.0) +
+                                   (mu[1] * (1.0 + 3.0 * uox) + mu[2] * (1.0 + 3.0 * uoy) +
+                                    mu[3] * (1.0 - 3.0 * uox) + mu[4] * (1.0 - 3.0 * uoy)) * (1.0 / 6.0)) +
                           dRdC * mR;
         muox += tauIk * C * 0.5 * (mu[1] - mu[3]);
         muoy += tauIk * C * 0.5 * (mu[2] - mu[4]);
@@ -208,39 +233,36 @@ __global__ void __launch_bounds__(256) adjoint_step64(AdjointArgs a) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) qg[(size_t)q * L + n] = (1.0 - tauIk) * mu[q] + mC;
         }
-        const double gt = warp_sum(valid ? gTau : 0.0);
-        if ((threadIdx.x & 31) == 0 && gt != 0.0) atomicAdd(a.grad + 1 + k, gt);
-        if (sp.kind == RX_LINEAR && a.srcTab != nullptr) {
-            const int key = (valid && dom < (uint32_t)a.nDomains) ? 1 + a.S + k * a.nDomains + (int)dom : -1;
-            warp_keyed_add(a.grad, key, valid ? mR : 0.0);
-        }
+        gTauK[k] = valid ? gTau : 0.0;
+        if (valid && sp.kind == RX_LINEAR) a.racc[(size_t)k * L + n] = raccA[k] + mR;
     }
 
     // ---- fluid: outlet, velocity output and collide, backwards -----------
     if (passes == 2) {
         double d = D2;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) d += lf[q] * (fs[q] * s1);
+        for (int q = 0; q < 9; ++q) d += lf[q] * (fs(q) * s1);
 #pragma unroll
         for (int q = 0; q < 9; ++q) lf[q] = s2 * lf[q] - s2 * s2 * d;
     }
     if (passes >= 1) {
         double d = D1;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) d += lf[q] * fs[q];
+        for (int q = 0; q < 9; ++q) d += lf[q] * fs(q);
 #pragma unroll
         for (int q = 0; q < 9; ++q) lf[q] = s1 * lf[q] - s1 * s1 * d;
     }
     // post-collision velocity uo = (sum c_q fs_q) / rho
-    double mrho = -(uox * muox + uoy * muoy) / rho;
+    double mrho = -(uox * muox + uoy * muoy) * rhoI;
+    const double mjox = muox * rhoI, mjoy = muoy * rhoI;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) lf[q] += (kCX[q] * muox + kCY[q] * muoy) / rho;
+    for (int q = 0; q < 9; ++q) lf[q] += kCX[q] * mjox + kCY[q] * mjoy;
 
     double gTauF = 0.0, mrhoF = 0.0, mfx = 0.0, mfy = 0.0, mux = 0.0, muy = 0.0, mlast = 0.0;
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         const double w = weight9(q);
-        gTauF += lf[q] * (feqw[q] - f[q]);
+        gTauF += lf[q] * (feqw(q) - f[q]);
         const double mfeq = lf[q] * tauI;
         mrhoF += lf[q] * 3.0 * w * (kCX[q] * fx + kCY[q] * fy);
         mfx += lf[q] * 3.0 * w * rhoF * kCX[q];
@@ -254,26 +276,84 @@ __global__ void __launch_bounds__(256) adjoint_step64(AdjointArgs a) {
     }
     mux += mlast * 3.0 * ux;
     muy += mlast * 3.0 * uy;
-    const double mjx = mux / rho, mjy = muy / rho;
-    mrho -= (ux * mux + uy * muy) / rho;
+    const double mjx = mux * rhoI, mjy = muy * rhoI;
+    mrho -= (ux * mux + uy * muy) * rhoI;
     mrhoF += mrho;
     if (valid) {
 #pragma unroll
         for (int q = 0; q < 9; ++q) a.qf[(size_t)q * L + n] = (1.0 - tauI) * lf[q] + mrhoF + kCX[q] * mjx + kCY[q] * mjy;
-        if (tile) {
-            a.G[n] += mfx;
-            a.G[L + n] += mfy;
-        }
+        a.G[n] = Gx + mfx;
+        a.G[L + n] = Gy + mfy;
     }
-    const double gt = warp_sum(valid ? gTauF : 0.0);
-    if ((threadIdx.x & 31) == 0 && gt != 0.0) atomicAdd(a.grad, gt);
+    // relaxation-time gradients: block sums into this block's own slots (the
+    // same slots every step), reduced over blocks once at the end of the pass
+    __shared__ double red[8][1 + kMaxSpecies];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double v0 = warp_sum(valid ? gTauF : 0.0);
+    if (lane == 0) red[warp][0] = v0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const double v = warp_sum(gTauK[k]);
+        if (lane == 0) red[warp][1 + k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x <= NS) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+        double* slot = a.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * (1 + NS) + threadIdx.x;
+        *slot += t;
+    }
+}
+
+// Sums the per-block relaxation-time partials (nBlocks x width) into grad[0..width).
+__global__ void adjoint_part_reduce(const double* part, int nBlocks, int width, double* grad) {
+    __shared__ double red[8];
+    for (int j = 0; j < width; ++j) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < nBlocks; b += blockDim.x) t += part[(size_t)b * width + j];
+        t = warp_sum(t);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+            grad[j] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Sums the per-node source-rate partials into grad[1 + S + k*nDomains + dom].
+__global__ void adjoint_rate_reduce(const double* racc, const uint32_t* dom, size_t L, int S, int nDomains,
+                                    double* grad) {
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = n < L;
+    const uint32_t d = valid ? dom[n] : 0u;
+    for (int k = 0; k < S; ++k) {
+        const int key = (valid && d < (uint32_t)nDomains) ? 1 + S + k * nDomains + (int)d : -1;
+        warp_keyed_add(grad, key, valid ? racc[(size_t)k * L + n] : 0.0);
+    }
 }
 
 __global__ void set_iteration_kernel(Status* st, unsigned it) { st->iteration = it; }
 
+int adjoint_blocks(int nx, int ny) { return ((nx + 255) / 256) * ny; }
+
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
-    const unsigned blocks = (unsigned)((a.L + 255) / 256);
-    adjoint_step64<<<blocks, 256, 0, s>>>(a);
+    const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
+    switch (a.S) {
+        case 0: adjoint_step64<0><<<grid, 256, 0, s>>>(a); break;
+        case 1: adjoint_step64<1><<<grid, 256, 0, s>>>(a); break;
+        case 2: adjoint_step64<2><<<grid, 256, 0, s>>>(a); break;
+        default: adjoint_step64<3><<<grid, 256, 0, s>>>(a); break;
+    }
+}
+
+void launch_adjoint_finish(const AdjointArgs& a, cudaStream_t s) {
+    adjoint_part_reduce<<<1, 256, 0, s>>>(a.part, adjoint_blocks(a.nx, a.ny), 1 + a.S, a.grad);
+    if (a.S > 0 && a.srcTab != nullptr)
+        adjoint_rate_reduce<<<(unsigned)((a.L + 255) / 256), 256, 0, s>>>(a.racc, a.dom, a.L, a.S, a.nDomains,
+                                                                          a.grad);
 }
 
 void launch_set_iteration(Status* st, unsigned it, cudaStream_t s) { set_iteration_kernel<<<1, 1, 0, s>>>(st, it); }

@@ -22,17 +22,21 @@ __device__ __forceinline__ float reaction32(int kind, float src, float decay, ui
     return 0.0f;
 }
 
+// NS = number of species, a compile-time constant so that every input of a
+// node (9 + 5 NS values) is loaded before any arithmetic.  Grid (nx/256, ny).
+template <int NS>
 __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     if (a.status->halt) return;
-    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= a.L) return;
     const int nx = a.nx, ny = a.ny;
-    const int x = (int)(n % (size_t)nx), y = (int)(n / (size_t)nx);
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nx) return;
+    const int y = blockIdx.y;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const size_t L = a.L;
-    const size_t rC = (size_t)y * nx, rM = (size_t)ym * nx, rP = (size_t)yp * nx;
-    const float* fin = a.fin;
+    const unsigned rC = (unsigned)y * nx, rM = (unsigned)ym * nx, rP = (unsigned)yp * nx;
+    const unsigned n = rC + x;
+    const float* __restrict__ fin = a.fin;
     const float hT = fin[0 * L + rC + x];
     const float hE = fin[1 * L + rC + xm];
     const float hN = fin[2 * L + rM + x];
@@ -42,7 +46,16 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const float hNW = fin[6 * L + rM + xp];
     const float hSW = fin[7 * L + rP + xp];
     const float hSE = fin[8 * L + rP + xm];
-
+    float gi[NS > 0 ? NS : 1][5];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const float* __restrict__ gin = a.gin + (size_t)k * 5 * L;
+        gi[k][0] = gin[0 * L + rC + x];
+        gi[k][1] = gin[1 * L + rC + xm];
+        gi[k][2] = gin[2 * L + rM + x];
+        gi[k][3] = gin[3 * L + rC + xp];
+        gi[k][4] = gin[4 * L + rP + x];
+    }
     const uint32_t dom = a.dom[n];
     float rta = 0.0f;
     if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = (float)a.massTab[dom];
@@ -63,17 +76,13 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const float usq = 1.5f * (ux * ux + uy * uy);
     const float w0 = 4.0f / 9.0f, w1 = 1.0f / 9.0f, w2 = 1.0f / 36.0f;
     const float f3 = 3.0f * rhoF;
-    float* fo = a.fout;
-    // rest
-    {
-        const float heq = w0 * dr + w0 * rho * (-usq);
-        fo[0 * L + n] = hT + (heq - hT) * tauI;
-    }
+    float ho[9];
+    ho[0] = hT + (w0 * dr + w0 * rho * (-usq) - hT) * tauI;
 #define LBIB_Q(idx, h, w, cu, cf)                                                 \
     {                                                                             \
         const float c_u = (cu);                                                   \
         const float heq = (w) * dr + (w) * rho * (3.0f * c_u + 4.5f * c_u * c_u - usq); \
-        fo[(idx) * L + n] = (h) + (heq - (h)) * tauI + (w) * f3 * (cf);           \
+        ho[idx] = (h) + (heq - (h)) * tauI + (w) * f3 * (cf);                     \
     }
     LBIB_Q(1, hE, w1, ux, Fx)
     LBIB_Q(2, hN, w1, uy, Fy)
@@ -97,24 +106,24 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         const float wq[9] = {w0, w1, w1, w1, w1, w2, w2, w2, w2};
         float dh = 0.0f;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) dh += fo[q * L + n];
+        for (int q = 0; q < 9; ++q) dh += ho[q];
         rs[p] = 1.0f / (1.0f + dh);
 #pragma unroll
-        for (int q = 0; q < 9; ++q) fo[q * L + n] = (fo[q * L + n] - wq[q] * dh) * rs[p];
+        for (int q = 0; q < 9; ++q) ho[q] = (ho[q] - wq[q] * dh) * rs[p];
     }
+    float* __restrict__ fo = a.fout;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[q * L + n] = ho[q];
 
-    for (int k = 0; k < a.S; ++k) {
-        const float* gin = a.gin + (size_t)k * 5 * L;
-        const float gT = gin[0 * L + rC + x];
-        const float gE = gin[1 * L + rC + xm];
-        const float gN = gin[2 * L + rM + x];
-        const float gW = gin[3 * L + rC + xp];
-        const float gS = gin[4 * L + rP + x];
+    const unsigned iteration = NS > 0 ? a.status->iteration : 0u;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const float gT = gi[k][0], gE = gi[k][1], gN = gi[k][2], gW = gi[k][3], gS = gi[k][4];
         const float C = ((gT + gE) + (gN + gW)) + gS;
         const float tI = (float)(1.0 / a.sp[k].tau);
         float src = 0.0f;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = (float)a.srcTab[(size_t)k * a.nDomains + dom];
-        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, a.status->iteration, C);
+        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, iteration, C);
         const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
         const float e0 = C * (1.0f / 3.0f), e1 = C * (1.0f / 6.0f);
         float go[5];
@@ -126,7 +135,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         for (int p = 0; p < passes; ++p)
 #pragma unroll
             for (int q = 0; q < 5; ++q) go[q] *= rs[p];
-        float* gop = a.gout + (size_t)k * 5 * L;
+        float* __restrict__ gop = a.gout + (size_t)k * 5 * L;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gop[q * L + n] = go[q];
     }
@@ -197,7 +206,13 @@ __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double ta
 }
 
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
-    stream_collide32<<<(unsigned)((a.L + 255) / 256), 256, 0, s>>>(a);
+    const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
+    switch (a.S) {
+        case 0: stream_collide32<0><<<grid, 256, 0, s>>>(a); break;
+        case 1: stream_collide32<1><<<grid, 256, 0, s>>>(a); break;
+        case 2: stream_collide32<2><<<grid, 256, 0, s>>>(a); break;
+        default: stream_collide32<3><<<grid, 256, 0, s>>>(a); break;
+    }
 }
 
 void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {

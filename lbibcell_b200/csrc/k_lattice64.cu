@@ -17,14 +17,16 @@ namespace lbib {
 
 __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
     if (a.status->halt) return;
-    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= a.L) return;
+    // grid (nx/256, ny): one lattice node per thread
     const int nx = a.nx, ny = a.ny;
-    const int x = (int)(n % (size_t)nx), y = (int)(n / (size_t)nx);
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nx) return;
+    const int y = blockIdx.y;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const size_t L = a.L;
-    const size_t rC = (size_t)y * nx, rM = (size_t)ym * nx, rP = (size_t)yp * nx;
+    const unsigned rC = (unsigned)y * nx, rM = (unsigned)ym * nx, rP = (unsigned)yp * nx;
+    const unsigned n = rC + x;
     const double* fin = a.fin;
     double f[9];
     f[T] = fin[0 * L + rC + x];
@@ -150,8 +152,8 @@ __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double
 }
 
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
-    const unsigned blocks = (unsigned)((a.L + 255) / 256);
-    stream_collide64<<<blocks, 256, 0, s>>>(a);
+    const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
+    stream_collide64<<<grid, 256, 0, s>>>(a);
 }
 
 void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {

@@ -162,21 +162,26 @@ struct AdjointArgs {
     const double* seed;    // S*L      dL/dC_k at the final step, or nullptr
     double* qf;            // 9*L      adjoint planes of step t (output)
     double* qg;            // S*5*L
-    const double* force;   // 2*L      spread force field (valid where tileCount > 0)
-    const int* tileCount;
-    int tilesX;
+    const double* force;   // 2*L      spread force field (zero outside the force tiles)
     const uint32_t* dom;
     const double* massTab; // per-domain rhoToAdd, or nullptr
     int nDomains;
     const double* srcTab;  // [S][nDomains]
-    double tauF;
+    double tauIF;              // 1 / tauFluid
+    double tauI[kMaxSpecies];  // 1 / tau of each species
     SpeciesConst sp[kMaxSpecies];
     unsigned iteration;    // iteration counter during step t
     int outlet;
     double* G;             // 2*L      dL/dF(x), summed over steps
-    double* grad;          // 1 + S + S*nDomains
+    double* racc;          // S*L      dL/d source at each node, summed over steps
+    double* part;          // adjoint_blocks * (1 + S): per-block relaxation-time partials
+    double* grad;          // 1 + S + S*nDomains (written by launch_adjoint_finish)
 };
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s);
+// Thread blocks of one adjoint launch (the rows of AdjointArgs::part).
+int adjoint_blocks(int nx, int ny);
+// Reduces the per-block and per-node partials into grad.
+void launch_adjoint_finish(const AdjointArgs& a, cudaStream_t s);
 void launch_set_iteration(Status* st, unsigned it, cudaStream_t s);
 
 // Transpose of the spread under fixed positions: gf[i] = sum over node i's 16

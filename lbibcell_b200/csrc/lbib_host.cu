@@ -97,6 +97,8 @@ struct DiffCtx {
     double* srcTab = nullptr; // S*nDomains
     double* seed = nullptr;   // S*L
     double* grad = nullptr;   // 1 + S + S*nDomains
+    double* racc = nullptr;   // S*L
+    double* part = nullptr;   // adjoint blocks * (1 + S)
     Status* st = nullptr;
     double tauF = 1.0;
     double tau[kMaxSpecies] = {1.0, 1.0, 1.0};
@@ -107,7 +109,7 @@ struct DiffCtx {
     ~DiffCtx() {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(x0); fr(u0); fr(ck); fr(seg); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(fxp); fr(fyp); fr(gfx); fr(gfy);
-        fr(srcTab); fr(seed); fr(grad); fr(st);
+        fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st);
     }
 };
 
@@ -1276,7 +1278,8 @@ static void diff_begin(Handle& h, int T, int K) {
     const int nSeg = (T + K - 1) / K;
     const size_t stateDoubles = (size_t)(9 + 5 * S) * L;
     const size_t states = 1 + (size_t)(nSeg - 1) + (size_t)(K - 1) + 2;
-    const size_t bytes = sizeof(double) * (states * stateDoubles + 10 * L + (size_t)S * L + 4 * (size_t)h.Mcap +
+    const size_t nPart = (size_t)adjoint_blocks(h.nx, h.ny) * (1 + S);
+    const size_t bytes = sizeof(double) * (states * stateDoubles + 10 * L + 2 * (size_t)S * L + nPart + 4 * (size_t)h.Mcap +
                                            2 * (size_t)S * h.nDomains + 1 + S);
     size_t freeB = 0, totalB = 0;
     CK(cudaMemGetInfo(&freeB, &totalB));
@@ -1298,6 +1301,8 @@ static void diff_begin(Handle& h, int T, int K) {
     d->srcTab = dalloc<double>((size_t)S * h.nDomains);
     d->seed = dalloc<double>((size_t)S * L);
     d->grad = dalloc<double>(1 + S + (size_t)S * h.nDomains);
+    d->racc = dalloc<double>((size_t)S * L);
+    d->part = dalloc<double>(nPart);
     d->st = dalloc<Status>(1);
     CK(cudaMemsetAsync(d->st, 0, sizeof(Status), h.stream));
     CK(cudaMemsetAsync(d->force, 0, sizeof(double) * 2 * L, h.stream));
@@ -1378,24 +1383,27 @@ static void diff_backward(Handle& h, DiffCtx& d) {
     const int S = h.S;
     CK(cudaMemsetAsync(d.G, 0, sizeof(double) * 2 * L, h.stream));
     CK(cudaMemsetAsync(d.grad, 0, sizeof(double) * (1 + S + (size_t)S * h.nDomains), h.stream));
+    if (S) CK(cudaMemsetAsync(d.racc, 0, sizeof(double) * S * L, h.stream));
+    CK(cudaMemsetAsync(d.part, 0, sizeof(double) * adjoint_blocks(h.nx, h.ny) * (1 + S), h.stream));
     bool area = false;
     for (int b : h.bio) area |= (b == 2);
     AdjointArgs a{};
     a.nx = h.nx; a.ny = h.ny; a.L = L; a.S = S;
     a.force = d.force;
-    a.tileCount = h.tiles.count;
-    a.tilesX = h.tiles.tilesX;
     a.dom = h.dom;
     a.massTab = area ? h.massTab : nullptr;
     a.nDomains = h.nDomains;
     a.srcTab = d.srcTab;
-    a.tauF = d.tauF;
+    a.tauIF = 1.0 / d.tauF;
     for (int k = 0; k < S; ++k) {
         a.sp[k] = h.sp[k].c;
         a.sp[k].tau = d.tau[k];
+        a.tauI[k] = 1.0 / d.tau[k];
     }
     a.outlet = d.outlet;
     a.G = d.G;
+    a.racc = d.racc;
+    a.part = d.part;
     a.grad = d.grad;
     for (int s = d.nSeg - 1; s >= 0; --s) {
         const int base = s * d.K;
@@ -1420,6 +1428,7 @@ static void diff_backward(Handle& h, DiffCtx& d) {
             launch_adjoint_step64(a, h.stream);
         }
     }
+    launch_adjoint_finish(a, h.stream);
     launch_force_adjoint(h.m, d.G, h.nx, h.ny, L, d.gfx, d.gfy, h.stream);
     CK(cudaGetLastError());
 }
