@@ -227,3 +227,35 @@ def test_autograd_function_wrapper(lbib, tmp_path):
     fd = (lp - lm) / (2 * h)
     _close(directional, fd, abs(fd), "autograd directional derivative")
     sim.diff_end()
+
+
+@pytest.mark.parametrize("nx", [520, 63])
+def test_adjoint_row_blocks(lbib, tmp_path, nx):
+    """Lattice widths that exercise every kind of row block of the adjoint
+    step: 520 = two full blocks of 256 nodes (one of them away from the
+    periodic x boundary) and a partial block of 8; 63 (odd) takes the
+    direct-load kernel."""
+    ny = 40
+    sp = [configs.Species(configs.SPECIES_NAMES[k], t, decay=1e-4 * k, source={1: 1e-3})
+          for k, t in enumerate((1.0, 0.8))]
+    cfg = configs.Config(name=f"wide_{nx}", nx=nx, ny=ny, tau_fluid=0.9, iterations=100, report_step=50,
+                         cells=[(1, configs.circle(nx / 2.0 + 0.3, ny / 2.0 + 0.2, 9.0, 90))], species=sp,
+                         area=None)
+    P = _Problem(lbib, cfg.write(str(tmp_path)), T=12, K=5, steps_before=2)
+    g = P.grads()
+    h = 1e-5
+    for i in range(1 + P.S):
+        tp, tm = P.tau.copy(), P.tau.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (P.loss(tau=tp) - P.loss(tau=tm)) / (2 * h)
+        _close(g["tau"][i], fd, np.abs(g["tau"]).max(), f"dL/dtau[{i}]")
+    rp, rm = P.rates.copy(), P.rates.copy()
+    rp[1, 1] += h
+    rm[1, 1] -= h
+    fd = (P.loss(rates=rp) - P.loss(rates=rm)) / (2 * h)
+    _close(g["rates"][1, 1], fd, np.abs(g["rates"]).max(), "dL/drate[1,1]")
+    v = np.random.default_rng(11).normal(size=P.F.shape)
+    fd = (P.loss(F=P.F + h * v) - P.loss(F=P.F - h * v)) / (2 * h)
+    _close(float((g["force"] * v).sum()), fd, np.abs(g["force"] * v).sum(), "dL/dF . v")
+    P.sim.diff_end()
