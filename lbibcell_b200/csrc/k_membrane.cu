@@ -258,9 +258,16 @@ __device__ __forceinline__ void sort_tile_list(const int* list, int cnt, int sor
 // covers two rows of the tile and first collects, in id order, the entries
 // whose stencil rows meet its rows; every lattice node then adds its
 // contributions in id order.
+//
+// FP64 runs add in id order, the reference's summation order.  FP32-shifted
+// runs skip the sort: each contribution is rounded to 64-bit fixed point
+// (2^-44) and the integer sums do not depend on the order, so the field is
+// still deterministic; the rounding is far below FP32 resolution.
+constexpr double kForceFix = 17592186044416.0;  // 2^44
 template <typename Real, int kSpreadMax, int kMinCount>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
                                                      Status* st, int sortBits) {
+    constexpr bool kExactOrder = sizeof(Real) == 8;
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
@@ -279,9 +286,13 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     unsigned short* wlist = (unsigned short*)(order + kSpreadMax);  // 8 warps x kSpreadMax
     __shared__ __align__(16) unsigned char sortTmp[sizeof(typename cub::BlockRadixSort<int, 256, (kSpreadMax + 255) / 256>::TempStorage)];
     const int* list = t.list + t.start[tile];
-    if (kSpreadMax <= 256 || cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
-    else if (kSpreadMax <= 512 || cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
-    else sort_tile_list<(kSpreadMax + 255) / 256>(list, cnt, sortBits, order, sortTmp);
+    if constexpr (kExactOrder) {
+        if (kSpreadMax <= 256 || cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
+        else if (kSpreadMax <= 512 || cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
+        else sort_tile_list<(kSpreadMax + 255) / 256>(list, cnt, sortBits, order, sortTmp);
+    } else {
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) order[k] = list[k];
+    }
     __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
@@ -323,6 +334,7 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     const int lx = lane & 15, ly = threadIdx.x >> 4;
     const int x = tileX0 + lx, y = tileY0 + ly;
     double ax = 0.0, ay = 0.0;
+    long long qx = 0, qy = 0;  // fixed-point sums (FP32-shifted runs)
     for (int e = 0; e < wn; ++e) {
         const int k = wl[e];
         const int c = code[k];
@@ -338,12 +350,21 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         if (hit) {
             const double* f = fac + 10 * k;
             const double dl = (f[dx] * f[5 + dy]) / 16.0;
-            ax += sfx[k] * dl;
-            ay += sfy[k] * dl;
+            if constexpr (kExactOrder) {
+                ax += sfx[k] * dl;
+                ay += sfy[k] * dl;
+            } else {
+                qx += __double2ll_rn(sfx[k] * dl * kForceFix);
+                qy += __double2ll_rn(sfy[k] * dl * kForceFix);
+            }
         }
     }
     if (x >= nx || y >= ny) return;
     const size_t n = (size_t)y * nx + x;
+    if constexpr (!kExactOrder) {
+        ax = (double)qx * (1.0 / kForceFix);
+        ay = (double)qy * (1.0 / kForceFix);
+    }
     force[n] = (Real)ax;
     force[L + n] = (Real)ay;
 }
@@ -1037,6 +1058,39 @@ __global__ void area_regulator_kernel(MembraneDev m, const double* area, double*
     if (d < (uint32_t)nDomains && d != 0) massTab[d] = r;
 }
 
+// FP32-shifted runs: the per-cell shoelace sums over the connections in any
+// order, each term x_a y_b - x_b y_a (a -> b along the ring) rounded to 64-bit
+// fixed point (2^-24), so that the integer sums are exact and independent of
+// the order; no ring ranking is needed.  FP64 runs keep the ring-ordered sum.
+constexpr double kAreaFix = 16777216.0;  // 2^24
+__global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDomains, unsigned long long* acc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int cell = -1;
+    long long v = 0;
+    if (c < m.topo->C) {
+        const int a = m.ca[c], b = m.cb[c];
+        const uint32_t d = m.cdom[c];
+        if (d < (uint32_t)nDomains) cell = cellOfDom[d];
+        v = __double2ll_rn((m.x[a] * m.y[b] - m.x[b] * m.y[a]) * kAreaFix);
+    }
+    // one atomic per run of equal cells in the warp (connections of a cell are mostly contiguous)
+    const unsigned peers = __match_any_sync(0xffffffffu, cell);
+    long long sum = 0;
+    for (int l = 0; l < 32; ++l) {
+        const long long t = __shfl_sync(0xffffffffu, v, l);
+        if ((peers >> l) & 1u) sum += t;
+    }
+    if (cell >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+        atomicAdd(acc + cell, (unsigned long long)sum);
+}
+
+__global__ void areas_fixed_finish(unsigned long long* acc, int nCells, double* area) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nCells) return;
+    area[c] = (double)(long long)acc[c] * (1.0 / kAreaFix) / 2.0;
+    acc[c] = 0ull;
+}
+
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
     if (m.nCells == 0) return;
     areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, nullptr);
@@ -1054,6 +1108,16 @@ void launch_area_regulator(const MembraneDev& m, double* area, double* target, d
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
     areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, (Status*)st);
+    area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
+                                                                 strength, maxsource, st);
+}
+
+void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
+                                 double* target, double* massTab, int nDomains, double factor, double strength,
+                                 double maxsource, const Status* st, cudaStream_t s) {
+    if (m.nCells == 0 || m.Ccap == 0) return;
+    areas_fixed_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, cellOfDom, nDomains, acc);
+    areas_fixed_finish<<<(m.nCells + 127) / 128, 128, 0, s>>>(acc, m.nCells, area);
     area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
                                                                  strength, maxsource, st);
 }

@@ -137,6 +137,11 @@ void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double forc
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s);
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
+// FP32-shifted runs: areas from the connections in fixed point (no ring order
+// needed), then the regulator.  acc (nCells) must start at zero; it is left zero.
+void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
+                                 double* target, double* massTab, int nDomains, double factor, double strength,
+                                 double maxsource, const Status* st, cudaStream_t s);
 
 // Cells that fit the fixed device array of lbib_areas_static (16384 doubles,
 // 128 KB), and the address of that array on the current device.

@@ -153,6 +153,7 @@ struct Handle {
     int* inPos = nullptr;
     double* area = nullptr;
     double* target = nullptr;
+    unsigned long long* areaAcc = nullptr;  // fixed-point area sums of FP32-shifted runs
     std::vector<double> targetHost;  // per cell, survives ring rebuilds
     std::vector<uint32_t> ringDomHost;
 
@@ -207,7 +208,7 @@ Handle::~Handle() {
     fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id);
     fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
-    fr(outPos); fr(inPos); fr(area); fr(target);
+    fr(outPos); fr(inPos); fr(area); fr(target); fr(areaAcc);
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.touched);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
@@ -593,10 +594,12 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(cells, h.cellCap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ringStart); fr(h.m.ringDom); fr(h.area); fr(h.target);
+        fr(h.m.ringStart); fr(h.m.ringDom); fr(h.area); fr(h.target); fr(h.areaAcc);
         fr(h.td.cellCount); fr(h.td.cellStart); fr(h.td.cellFill); fr(h.td.startNode);
         h.m.ringStart = dalloc<int>(h.cellCap + 1); h.m.ringDom = dalloc<uint32_t>(h.cellCap);
         h.area = dalloc<double>(h.cellCap); h.target = dalloc<double>(h.cellCap);
+        h.areaAcc = dalloc<unsigned long long>(h.cellCap);
+        CK(cudaMemset(h.areaAcc, 0, sizeof(unsigned long long) * h.cellCap));
         h.td.cellCount = dalloc<int>(h.cellCap + 1); h.td.cellStart = dalloc<int>(h.cellCap + 1);
         h.td.cellFill = dalloc<int>(h.cellCap); h.td.startNode = dalloc<int>(h.cellCap);
     }
@@ -885,12 +888,21 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
     }
     // ST_OUTLET: MassSolverBoxOutlet runs inside the stream-collide kernel
     if (fromStage <= ST_BIO) {
-        nl += launch_rings(h.m, h.td, h.st, s);
+        // FP64 runs sum the areas in ring order (the reference's order), so the
+        // rings are re-ranked after any topology change; FP32-shifted runs sum
+        // in exact fixed point and need no ring order here
+        if (sizeof(Real) == 8) nl += launch_rings(h.m, h.td, h.st, s);
         for (int b : h.bio) {
             if (b == 2) {
-                launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor, h.areaStrength,
-                                      h.areaMax, h.st, s);
-                nl += h.m.nCells > 0 ? 2 : 0;
+                if (sizeof(Real) == 8) {
+                    launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor,
+                                          h.areaStrength, h.areaMax, h.st, s);
+                    nl += h.m.nCells > 0 ? 2 : 0;
+                } else {
+                    launch_area_regulator_fixed(h.m, h.td.cellOfDom, h.areaAcc, h.area, h.target, h.massTab,
+                                                h.nDomains, h.areaFactor, h.areaStrength, h.areaMax, h.st, s);
+                    nl += h.m.nCells > 0 ? 3 : 0;
+                }
             } else if (b == 1 && renewal) {
                 launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
                 nl += hasM ? 2 : 0;
@@ -1705,6 +1717,7 @@ int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
     if (h.err) return -h.err;
     try {
         cudaSetDevice(h.device);
+        lbib::launch_rings(h.m, h.td, h.st, h.stream);  // FP32-shifted steps leave the ring order stale
         lbib::launch_areas(h.m, h.area, h.stream);
         std::vector<double> a(h.m.nCells);
         if (h.m.nCells)
@@ -1765,6 +1778,7 @@ int lbib_areas_static(lbib_handle* hh, unsigned* dom, double* area, int cap) {
         CK(cudaSetDevice(h.device));
         double* scratch = nullptr;
         CK(static_area_address(h.device, &scratch));
+        lbib::launch_rings(h.m, h.td, h.st, h.stream);  // FP32-shifted steps leave the ring order stale
         lbib::launch_areas(h.m, scratch, h.stream);
         CK(cudaGetLastError());
         const int n = std::min(h.m.nCells, cap);
