@@ -258,16 +258,10 @@ __device__ __forceinline__ void sort_tile_list(const int* list, int cnt, int sor
 // covers two rows of the tile and first collects, in id order, the entries
 // whose stencil rows meet its rows; every lattice node then adds its
 // contributions in id order.
-//
-// FP64 runs add in id order, the reference's summation order.  FP32-shifted
-// runs skip the sort: each contribution is rounded to 64-bit fixed point
-// (2^-44) and the integer sums do not depend on the order, so the field is
-// still deterministic; the rounding is far below FP32 resolution.
-constexpr double kForceFix = 17592186044416.0;  // 2^44
+// Used by FP64 runs, whose summation order must be the reference's.
 template <typename Real, int kSpreadMax, int kMinCount>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
                                                      Status* st, int sortBits) {
-    constexpr bool kExactOrder = sizeof(Real) == 8;
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
@@ -286,13 +280,9 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     unsigned short* wlist = (unsigned short*)(order + kSpreadMax);  // 8 warps x kSpreadMax
     __shared__ __align__(16) unsigned char sortTmp[sizeof(typename cub::BlockRadixSort<int, 256, (kSpreadMax + 255) / 256>::TempStorage)];
     const int* list = t.list + t.start[tile];
-    if constexpr (kExactOrder) {
-        if (kSpreadMax <= 256 || cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
-        else if (kSpreadMax <= 512 || cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
-        else sort_tile_list<(kSpreadMax + 255) / 256>(list, cnt, sortBits, order, sortTmp);
-    } else {
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x) order[k] = list[k];
-    }
+    if (kSpreadMax <= 256 || cnt <= 256) sort_tile_list<1>(list, cnt, sortBits, order, sortTmp);
+    else if (kSpreadMax <= 512 || cnt <= 512) sort_tile_list<2>(list, cnt, sortBits, order, sortTmp);
+    else sort_tile_list<(kSpreadMax + 255) / 256>(list, cnt, sortBits, order, sortTmp);
     __syncthreads();
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
@@ -334,7 +324,6 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
     const int lx = lane & 15, ly = threadIdx.x >> 4;
     const int x = tileX0 + lx, y = tileY0 + ly;
     double ax = 0.0, ay = 0.0;
-    long long qx = 0, qy = 0;  // fixed-point sums (FP32-shifted runs)
     for (int e = 0; e < wn; ++e) {
         const int k = wl[e];
         const int c = code[k];
@@ -350,23 +339,91 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         if (hit) {
             const double* f = fac + 10 * k;
             const double dl = (f[dx] * f[5 + dy]) / 16.0;
-            if constexpr (kExactOrder) {
-                ax += sfx[k] * dl;
-                ay += sfy[k] * dl;
-            } else {
-                qx += __double2ll_rn(sfx[k] * dl * kForceFix);
-                qy += __double2ll_rn(sfy[k] * dl * kForceFix);
-            }
+            ax += sfx[k] * dl;
+            ay += sfy[k] * dl;
         }
     }
     if (x >= nx || y >= ny) return;
     const size_t n = (size_t)y * nx + x;
-    if constexpr (!kExactOrder) {
-        ax = (double)qx * (1.0 / kForceFix);
-        ay = (double)qy * (1.0 / kForceFix);
-    }
     force[n] = (Real)ax;
     force[L + n] = (Real)ay;
+}
+
+// FP32-shifted runs: each 16x16 tile scatters the contributions of the
+// membrane nodes listed for it into 64-bit fixed-point accumulators (2^-44) in
+// shared memory.  Each contribution dirac * F_i is formed in FP64 exactly as in
+// the ordered gather and rounded once; the integer sums are exact, so the
+// field does not depend on the order of the list (it is deterministic) and no
+// sort is needed.  The rounding is far below FP32 resolution.
+constexpr double kForceFix = 17592186044416.0;  // 2^44
+constexpr int kScatterChunk = 256;
+__global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDev t, float* force, int nx, int ny,
+                                                           size_t L, Status* st) {
+    if (st->halt) return;
+    const int tile = blockIdx.x;
+    const int cnt = t.count[tile];
+    if (cnt == 0) return;
+    if (t.start[tile] + cnt > t.cap) {
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
+        return;
+    }
+    __shared__ unsigned long long acc[2][kTile * kTile];
+    __shared__ double fa[kScatterChunk][5], fb[kScatterChunk][5], sF[2][kScatterChunk];
+    __shared__ int org[kScatterChunk];
+    for (int j = threadIdx.x; j < kTile * kTile; j += blockDim.x) acc[0][j] = acc[1][j] = 0ull;
+    const int tx = tile % t.tilesX, ty = tile / t.tilesX;
+    const int tileX0 = tx * kTile, tileY0 = ty * kTile;
+    const int* list = t.list + t.start[tile];
+    const double halfPi = M_PI / 2.0;
+    for (int c0 = 0; c0 < cnt; c0 += kScatterChunk) {
+        const int nc = min(kScatterChunk, cnt - c0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nc; e += blockDim.x) {
+            const int i = list[c0 + e];
+            const double X = m.x[i], Y = m.y[i];
+            Stencil sc;
+            stencil_range(X, Y, nx, ny, sc);
+            org[e] = pack_stencil(sc, tileX0, tileY0);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                fa[e][q] = 1.0 + fast_cos(halfPi * ((double)(sc.x0 + q) - X));
+                fb[e][q] = 1.0 + fast_cos(halfPi * ((double)(sc.y0 + q) - Y));
+            }
+            sF[0][e] = m.fx[i];
+            sF[1][e] = m.fy[i];
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < 16 * nc; j += blockDim.x) {
+            const int e = j >> 4, k = j & 15;
+            const int c = org[e];
+            const int ox = (c & 0xff) - 4, oy = ((c >> 8) & 0xff) - 4, hx = (c >> 16) & 0xf, hy = (c >> 20) & 0xf;
+            int dx, dy;  // node of item k relative to the stencil origin
+            if (hx == 3 && hy == 3) {
+                dx = k >> 2;
+                dy = k & 3;
+            } else {
+                // wider stencil: the node bound to slot k (last writer of the slot)
+                const Stencil sc{ox + tileX0, ox + tileX0 + hx, oy + tileY0, oy + tileY0 + hy};
+                int xk, yk;
+                stencil_slot(sc, k, xk, yk);
+                if (xk < 0) continue;
+                dx = xk - sc.x0;
+                dy = yk - sc.y0;
+            }
+            const int lx = ox + dx, ly = oy + dy;
+            if ((unsigned)lx >= (unsigned)kTile || (unsigned)ly >= (unsigned)kTile) continue;
+            const double dl = (fa[e][dx] * fb[e][dy]) / 16.0;
+            atomicAdd(&acc[0][ly * kTile + lx], (unsigned long long)__double2ll_rn(sF[0][e] * dl * kForceFix));
+            atomicAdd(&acc[1][ly * kTile + lx], (unsigned long long)__double2ll_rn(sF[1][e] * dl * kForceFix));
+        }
+    }
+    __syncthreads();
+    const int lx = threadIdx.x & 15, ly = threadIdx.x >> 4;
+    const int x = tileX0 + lx, y = tileY0 + ly;
+    if (x >= nx || y >= ny) return;
+    const size_t n = (size_t)y * nx + x;
+    force[n] = (float)((double)(long long)acc[0][threadIdx.x] * (1.0 / kForceFix));
+    force[L + n] = (float)((double)(long long)acc[1][threadIdx.x] * (1.0 / kForceFix));
 }
 
 template <typename Real>
@@ -379,10 +436,16 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
     tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
-    int bits = 1;
-    while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
-    spread_kernel<Real, kSpreadSmall, 0><<<t.nTiles, 256, spread_smem(kSpreadSmall), s>>>(m, t, force, nx, ny, L, st, bits);
-    spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1><<<t.nTiles, 256, spread_smem(kSpreadLarge), s>>>(m, t, force, nx, ny, L, st, bits);
+    if constexpr (sizeof(Real) == 4) {
+        spread_fixed_kernel<<<t.nTiles, 256, 0, s>>>(m, t, (float*)force, nx, ny, L, st);
+    } else {
+        int bits = 1;
+        while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
+        spread_kernel<Real, kSpreadSmall, 0><<<t.nTiles, 256, spread_smem(kSpreadSmall), s>>>(m, t, force, nx, ny, L,
+                                                                                         st, bits);
+        spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1><<<t.nTiles, 256, spread_smem(kSpreadLarge), s>>>(
+            m, t, force, nx, ny, L, st, bits);
+    }
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
                                     cudaStream_t);
@@ -1128,9 +1191,7 @@ namespace lbib {
 
 void init_kernel_attributes() {
     cudaFuncSetAttribute(spread_kernel<double, kSpreadSmall, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadSmall));
-    cudaFuncSetAttribute(spread_kernel<float, kSpreadSmall, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadSmall));
     cudaFuncSetAttribute(spread_kernel<double, kSpreadLarge, kSpreadSmall + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadLarge));
-    cudaFuncSetAttribute(spread_kernel<float, kSpreadLarge, kSpreadSmall + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread_smem(kSpreadLarge));
     cudaFuncSetAttribute(reinit_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
     cudaFuncSetAttribute(reinit_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReinitSmem);
     init_kernel_attributes_topology();

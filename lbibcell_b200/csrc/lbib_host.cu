@@ -842,7 +842,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
     }
     if (fromStage <= ST_SPREAD) {
         launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s);
-        nl += hasM ? 6 : 0;
+        nl += hasM ? (sizeof(Real) == 8 ? 6 : 5) : 0;
     }
     if (fromStage <= ST_COLLIDE) {
         if (evCollideA) cudaEventRecord(evCollideA, s);
