@@ -476,12 +476,24 @@ __global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny,
         raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
         return;
     }
+    // the Dirac factors of the stencil's columns and rows, each formed once:
+    // (fa * fb) / 16 is calculateDiscreteDeltaDirac's expression
+    const double halfPi = M_PI / 2.0;
+    double fa[5], fb[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        fa[q] = 1.0 + fast_cos(halfPi * ((double)(sc.x0 + q) - X));
+        fb[q] = 1.0 + fast_cos(halfPi * ((double)(sc.y0 + q) - Y));
+    }
+    auto pick = [](const double* v, int i) {
+        return i == 0 ? v[0] : i == 1 ? v[1] : i == 2 ? v[2] : i == 3 ? v[3] : v[4];
+    };
     double vx = 0.0, vy = 0.0;
     for (int k = 0; k < 16; ++k) {
         int xk, yk;
         stencil_slot(sc, k, xk, yk);
         const size_t n = (size_t)yk * nx + xk;
-        const double dl = dirac((double)xk - X, (double)yk - Y);
+        const double dl = (pick(fa, xk - sc.x0) * pick(fb, yk - sc.y0)) / 16.0;
         vx += (double)u[n] * dl;
         vy += (double)u[L + n] * dl;
     }
@@ -581,8 +593,8 @@ __device__ __forceinline__ int slot_code(int d) {  // E,N,W,S -> 0..3
 // Pass 0: every crossing of a connection with a lattice line is a candidate
 // boundary node for one (node, slot) key.  The closest distance per key is
 // found by atomicMin on the distance's bits; each candidate is recorded for
-// passes 1 and 2; a key's first writer lists it for the reset at the end of
-// the step.  A warp reserves its records and listings with one atomic each.
+// passes 1 and 2 and for the reset of its key at the end of the step.  A warp
+// reserves its records with one atomic.
 constexpr int kRecPerConn = 16;
 
 struct CrossRec {
@@ -620,71 +632,81 @@ __device__ __forceinline__ int warp_reserve(int* counter, int count) {
     return base + incl - count;
 }
 
+// Calls fn(k, record) for the candidate records of connection cn in a fixed
+// order (k = 0, 1, ...); returns the number of records, or -1 after raising
+// the error of a connection that cannot be processed.  The kernel enumerates
+// three times (count, emit, list first writers) so that no per-thread record
+// array is needed.
+template <class Fn>
+__device__ __forceinline__ int for_each_record(const MembraneDev& m, int cn, int nx, int ny, Status* st, bool report,
+                                               Fn fn) {
+    const int a = m.ca[cn], b = m.cb[cn];
+    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+    const uint32_t D = m.cdom[cn];
+    const double maxX = x1 < x2 ? x2 : x1, maxY = y1 < y2 ? y2 : y1;
+    const double minX = x2 < x1 ? x2 : x1, minY = y2 < y1 ? y2 : y1;
+    const double mm = (y2 - y1) / (x2 - x1);
+    const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
+    if (!isfinite(mm)) {
+        if (report) raise_error(st, ERR_VERTICAL, cn, ST_CROSSINGS);
+        return -1;
+    }
+    if (!(minX >= -1.0 && maxX <= nx + 1.0 && minY >= -1.0 && maxY <= ny + 1.0)) {
+        // keeps the line loops bounded for positions off the lattice
+        if (report) raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
+        return -1;
+    }
+    const bool eastward = x1 < x2, southward = y1 > y2;
+    int k = 0;
+    CrossRec r;
+    for (int i = (int)ceil(minX); i <= (int)floor(maxX); i++) {
+        const double yc = mm * i + nn;
+        // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
+        if (k + 2 > kRecPerConn) break;
+        if (!make_record(nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D, r)) break;
+        fn(k++, r);
+        if (!make_record(nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u, r)) break;
+        fn(k++, r);
+    }
+    for (int i = (int)ceil(minY); i <= (int)floor(maxY); i++) {
+        const double xc = (i - nn) / mm;
+        // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
+        if (k + 2 > kRecPerConn) break;
+        if (!make_record(nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D, r)) break;
+        fn(k++, r);
+        if (!make_record(nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u, r)) break;
+        fn(k++, r);
+    }
+    const int want = 2 * (max(0, (int)floor(maxX) - (int)ceil(minX) + 1) + max(0, (int)floor(maxY) - (int)ceil(minY) + 1));
+    if (k != want) {
+        if (report) raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
+        return -1;
+    }
+    return k;
+}
+
 __global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Status* st) {
     if (st->halt) return;
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
-    CrossRec rec[kRecPerConn];
+    const bool live = cn < m.topo->C;
     int nrec = 0;
-    bool bad = false;
-    if (cn < m.topo->C) {
-        const int a = m.ca[cn], b = m.cb[cn];
-        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-        const uint32_t D = m.cdom[cn];
-        const double maxX = x1 < x2 ? x2 : x1, maxY = y1 < y2 ? y2 : y1;
-        const double minX = x2 < x1 ? x2 : x1, minY = y2 < y1 ? y2 : y1;
-        const double mm = (y2 - y1) / (x2 - x1);
-        const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
-        if (!isfinite(mm)) {
-            raise_error(st, ERR_VERTICAL, cn, ST_CROSSINGS);
-            bad = true;
-        } else if (!(minX >= -1.0 && maxX <= nx + 1.0 && minY >= -1.0 && maxY <= ny + 1.0)) {
-            // keeps the line loops bounded for positions off the lattice
-            raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
-            bad = true;
-        } else {
-            const bool eastward = x1 < x2, southward = y1 > y2;
-            for (int i = (int)ceil(minX); i <= (int)floor(maxX) && !bad; i++) {
-                const double yc = mm * i + nn;
-                // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
-                if (nrec + 2 > kRecPerConn) { bad = true; break; }
-                if (!make_record(nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D, rec[nrec])) bad = true;
-                else ++nrec;
-                if (!bad && !make_record(nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u, rec[nrec])) bad = true;
-                else if (!bad) ++nrec;
-            }
-            for (int i = (int)ceil(minY); i <= (int)floor(maxY) && !bad; i++) {
-                const double xc = (i - nn) / mm;
-                // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
-                if (nrec + 2 > kRecPerConn) { bad = true; break; }
-                if (!make_record(nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D, rec[nrec])) bad = true;
-                else ++nrec;
-                if (!bad && !make_record(nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u, rec[nrec])) bad = true;
-                else if (!bad) ++nrec;
-            }
-            if (bad) raise_error(st, ERR_EDGE_W, cn, ST_CROSSINGS);
-        }
+    if (live) {
+        nrec = for_each_record(m, cn, nx, ny, st, true, [](int, const CrossRec&) {});
+        if (nrec < 0) nrec = 0;
     }
-    if (bad) nrec = 0;
-    // closest distance per key; first writers of a key
-    int firsts = 0;
-    uint32_t firstKey[kRecPerConn];
-    for (int k = 0; k < nrec; ++k) {
-        const unsigned long long old = atomicMin(&c.bnDist[rec[k].key], rec[k].bits);
-        if (old == kEmpty) firstKey[firsts++] = rec[k].key;
-    }
+    // records of this step (they also list the keys to reset at the end of
+    // the step) and the closest distance per key
     const int rb = warp_reserve(&st->pad[2], nrec);
-    const int fb = warp_reserve(&st->nRecords, firsts);
-    for (int k = 0; k < nrec; ++k) {
-        const int r = rb + k;
-        if (r < c.recCap) {
-            c.recKey[r] = rec[k].key; c.recConn[r] = (uint32_t)cn; c.recDom[r] = rec[k].dom; c.recDist[r] = rec[k].bits;
-        } else {
-            raise_error(st, ERR_CAPACITY, cn, ST_CROSSINGS);
-        }
-    }
-    for (int k = 0; k < firsts; ++k) {
-        if (fb + k < c.touchedCap) c.touched[fb + k] = firstKey[k];
-        else raise_error(st, ERR_CAPACITY, cn, ST_CROSSINGS);
+    if (nrec > 0) {
+        for_each_record(m, cn, nx, ny, st, false, [&](int k, const CrossRec& r) {
+            const int idx = rb + k;
+            if (idx < c.recCap) {
+                c.recKey[idx] = r.key; c.recConn[idx] = (uint32_t)cn; c.recDom[idx] = r.dom; c.recDist[idx] = r.bits;
+            } else {
+                raise_error(st, ERR_CAPACITY, cn, ST_CROSSINGS);
+            }
+            atomicMin(&c.bnDist[r.key], r.bits);
+        });
     }
 }
 
@@ -775,8 +797,7 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 // changed nodes among its E,N,W,S,NE (read after write) and SW (write after
 // read) neighbours, and processes nodes in rounds once those are done.
 constexpr int kReinitMax = 4096;  // changed nodes per step (dynamic shared memory)
-constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1) +
-                                sizeof(cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024>::TempStorage) + 16;
+constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1) + 16;
 
 template <typename Real>
 __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int nS,
@@ -836,24 +857,6 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     }
 }
 
-typedef cub::BlockRadixSort<unsigned long long, 1024, kReinitMax / 1024> ReinitSortMax;
-
-template <int ITEMS>
-__device__ __forceinline__ void reinit_sort(const CrossDev& c, int cnt, unsigned long long* key, void* tmp) {
-    typedef cub::BlockRadixSort<unsigned long long, 1024, ITEMS> Sort;
-    typename Sort::TempStorage& sortTmp = *(typename Sort::TempStorage*)tmp;
-    unsigned long long kv[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const int k = threadIdx.x * ITEMS + j;
-        kv[j] = k < cnt ? (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k] : ~0ull;
-    }
-    Sort(sortTmp).Sort(kv, 32, 64);
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) key[threadIdx.x * ITEMS + j] = kv[j];
-    __syncthreads();
-}
-
 template <typename Real>
 __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int nS,
                                                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2,
@@ -873,9 +876,13 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[6] = (int(*)[6])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    // sort by node index (row-major order): keys node << 32 | newDom
-    if (cnt <= 1024) reinit_sort<1>(c, cnt, key, done + kReinitMax);
-    else reinit_sort<kReinitMax / 1024>(c, cnt, key, done + kReinitMax);
+    // keys node << 32 | newDom in list order; mark[node] = position + 1 lets
+    // each node find its changed neighbours without sorting
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        key[k] = (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k];
+        c.mark[c.changedNode[k]] = k + 1;
+    }
+    __syncthreads();
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
         const size_t n = (size_t)(key[k] >> 32);
         const int x = (int)(n % nx), y = (int)(n / nx);
@@ -887,13 +894,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
             deps[k][d] = -1;
             const size_t mnode = nbs[d];
             if (mnode >= n) continue;
-            int lo = 0, hi = k - 1;
-            while (lo <= hi) {
-                const int mid = (lo + hi) >> 1;
-                const size_t v = (size_t)(key[mid] >> 32);
-                if (v == mnode) { deps[k][d] = mid; break; }
-                if (v < mnode) lo = mid + 1; else hi = mid - 1;
-            }
+            deps[k][d] = c.mark[mnode] - 1;
         }
         done[k] = 0;
     }
@@ -926,6 +927,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         __syncthreads();
         ++rounds;
     }
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) c.mark[(size_t)(key[k] >> 32)] = 0;
 }
 
 template <typename Real>
@@ -983,10 +985,11 @@ __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* 
 
 // Resets the (node, slot) entries this step wrote (grid-stride over the
 // step's count, which lives on the device).
+// Resets the keys written this step (every written key has a record).
 __global__ void cross_clear_kernel(CrossDev c, Status* st) {
-    const int n = min(st->nRecords, c.touchedCap);
+    const int n = min(st->pad[2], c.recCap);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t key = c.touched[k];
+        const uint32_t key = c.recKey[k];
         c.bnDist[key] = kEmpty;
         c.bnConn[key] = ~0u;
     }
@@ -998,7 +1001,7 @@ void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, St
 }
 
 void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s) {
-    if (c.touchedCap <= 0) return;
+    if (c.recCap <= 0) return;
     cross_clear_kernel<<<296, 256, 0, s>>>(c, st);
 }
 

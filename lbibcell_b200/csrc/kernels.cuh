@@ -50,8 +50,7 @@ struct CrossDev {
     uint32_t* bnConn;            // 4*L, ~0u
     uint32_t* bnDom;             // 4*L
     uint32_t* wDom;              // L, W-slot winner domain + 1 (0: none)
-    uint32_t* touched;           // capacity: node*4+slot keys written this step
-    int touchedCap;
+    int* mark;                   // L, position + 1 of a node in this step's changed list (0: none)
     uint32_t* changedNode;       // capacity: nodes whose domain changes
     uint32_t* changedDom;
     int changedCap;

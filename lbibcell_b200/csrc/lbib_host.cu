@@ -210,7 +210,7 @@ Handle::~Handle() {
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
     fr(outPos); fr(inPos); fr(area); fr(target); fr(areaAcc);
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
-    fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.touched);
+    fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
     fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist);
     fr(m.topo); fr(m.cdesc);
@@ -565,7 +565,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.touched); fr(h.cross.changedNode);
+        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode);
         fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
         fr(h.cross.changedDom);
         fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
@@ -576,8 +576,6 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.td.cdesc2 = dalloc<int>(n); h.td.connAlive = dalloc<int>(n);
         // each connection of length <= MAXLENGTH crosses at most one line per axis
         // (two records each); longer ones exist only between the move and the remesh
-        h.cross.touchedCap = 16 * n + 1024;
-        h.cross.touched = dalloc<uint32_t>(h.cross.touchedCap);
         h.cross.changedCap = 8 * n + 1024;
         h.cross.recCap = 16 * n + 1024;
         h.cross.recKey = dalloc<uint32_t>(h.cross.recCap);
@@ -1162,6 +1160,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     h.cross.bnConn = dalloc<uint32_t>(4 * h.L);
     h.cross.bnDom = dalloc<uint32_t>(4 * h.L);
     h.cross.wDom = dalloc<uint32_t>(h.L);
+    h.cross.mark = dalloc<int>(h.L);
+    CK(cudaMemsetAsync(h.cross.mark, 0, sizeof(int) * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.bnDist, 0xff, sizeof(unsigned long long) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.bnConn, 0xff, sizeof(uint32_t) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.wDom, 0, sizeof(uint32_t) * h.L, h.stream));
