@@ -71,6 +71,7 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 // loaded before any arithmetic).  Grid (ceil(nx / 256), ny).
 template <int NS>
 __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
+    pdl_wait();
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
     const int xr = blockIdx.x * blockDim.x + threadIdx.x;
@@ -307,6 +308,7 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
 
 // Sums the per-block relaxation-time partials (nBlocks x width) into grad[0..width).
 __global__ void adjoint_part_reduce(const double* part, int nBlocks, int width, double* grad) {
+    pdl_wait();
     __shared__ double red[8];
     for (int j = 0; j < width; ++j) {
         double t = 0.0;
@@ -326,6 +328,7 @@ __global__ void adjoint_part_reduce(const double* part, int nBlocks, int width, 
 // Sums the per-node source-rate partials into grad[1 + S + k*nDomains + dom].
 __global__ void adjoint_rate_reduce(const double* racc, const uint32_t* dom, size_t L, int S, int nDomains,
                                     double* grad) {
+    pdl_wait();
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = n < L;
     const uint32_t d = valid ? dom[n] : 0u;
@@ -335,27 +338,28 @@ __global__ void adjoint_rate_reduce(const double* racc, const uint32_t* dom, siz
     }
 }
 
-__global__ void set_iteration_kernel(Status* st, unsigned it) { st->iteration = it; }
+__global__ void set_iteration_kernel(Status* st, unsigned it) {
+    pdl_wait(); st->iteration = it; }
 
 int adjoint_blocks(int nx, int ny) { return ((nx + 255) / 256) * ny; }
 
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     switch (a.S) {
-        case 0: adjoint_step64<0><<<grid, 256, 0, s>>>(a); break;
-        case 1: adjoint_step64<1><<<grid, 256, 0, s>>>(a); break;
-        case 2: adjoint_step64<2><<<grid, 256, 0, s>>>(a); break;
-        default: adjoint_step64<3><<<grid, 256, 0, s>>>(a); break;
+        case 0: launch_pdl(adjoint_step64<0>, grid, 256, 0, s, a); break;
+        case 1: launch_pdl(adjoint_step64<1>, grid, 256, 0, s, a); break;
+        case 2: launch_pdl(adjoint_step64<2>, grid, 256, 0, s, a); break;
+        default: launch_pdl(adjoint_step64<3>, grid, 256, 0, s, a); break;
     }
 }
 
 void launch_adjoint_finish(const AdjointArgs& a, cudaStream_t s) {
-    adjoint_part_reduce<<<1, 256, 0, s>>>(a.part, adjoint_blocks(a.nx, a.ny), 1 + a.S, a.grad);
+    launch_pdl(adjoint_part_reduce, 1, 256, 0, s, a.part, adjoint_blocks(a.nx, a.ny), 1 + a.S, a.grad);
     if (a.S > 0 && a.srcTab != nullptr)
-        adjoint_rate_reduce<<<(unsigned)((a.L + 255) / 256), 256, 0, s>>>(a.racc, a.dom, a.L, a.S, a.nDomains,
+        launch_pdl(adjoint_rate_reduce, (unsigned)((a.L + 255) / 256), 256, 0, s, a.racc, a.dom, a.L, a.S, a.nDomains,
                                                                           a.grad);
 }
 
-void launch_set_iteration(Status* st, unsigned it, cudaStream_t s) { set_iteration_kernel<<<1, 1, 0, s>>>(st, it); }
+void launch_set_iteration(Status* st, unsigned it, cudaStream_t s) { launch_pdl(set_iteration_kernel, 1, 1, 0, s, st, it); }
 
 }  // namespace lbib

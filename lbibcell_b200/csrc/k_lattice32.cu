@@ -26,6 +26,7 @@ __device__ __forceinline__ float reaction32(int kind, float src, float decay, ui
 // node (9 + 5 NS values) is loaded before any arithmetic.  Grid (nx/256, ny).
 template <int NS>
 __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
+    pdl_wait();
     if (a.status->halt) return;
     const int nx = a.nx, ny = a.ny;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,6 +162,7 @@ __device__ __forceinline__ void rescale_node32(float* f, float* g, int nS, size_
 }
 
 __global__ void outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ny) {
@@ -176,6 +178,7 @@ __global__ void outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, c
 __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                        SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1,
                        double init2) {
+    pdl_wait();
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L) return;
     const double wq[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
@@ -208,21 +211,21 @@ __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double ta
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     switch (a.S) {
-        case 0: stream_collide32<0><<<grid, 256, 0, s>>>(a); break;
-        case 1: stream_collide32<1><<<grid, 256, 0, s>>>(a); break;
-        case 2: stream_collide32<2><<<grid, 256, 0, s>>>(a); break;
-        default: stream_collide32<3><<<grid, 256, 0, s>>>(a); break;
+        case 0: launch_pdl(stream_collide32<0>, grid, 256, 0, s, a); break;
+        case 1: launch_pdl(stream_collide32<1>, grid, 256, 0, s, a); break;
+        case 2: launch_pdl(stream_collide32<2>, grid, 256, 0, s, a); break;
+        default: launch_pdl(stream_collide32<3>, grid, 256, 0, s, a); break;
     }
 }
 
 void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
     const int n = nx + ny;
-    outlet32<<<(n + 255) / 256, 256, 0, s>>>(f, g, nS, nx, ny, L, st);
+    launch_pdl(outlet32, (n + 255) / 256, 256, 0, s, f, g, nS, nx, ny, L, st);
 }
 
 void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s) {
-    init32<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+    launch_pdl(init32, (unsigned)((L + 255) / 256), 256, 0, s, f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
                                                        init[1], init[2]);
 }
 

@@ -16,6 +16,7 @@
 namespace lbib {
 
 __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
+    pdl_wait();
     if (a.status->halt) return;
     // grid (nx/256, ny): one lattice node per thread
     const int nx = a.nx, ny = a.ny;
@@ -106,6 +107,7 @@ __device__ __forceinline__ void rescale_node64(double* f, double* g, int nS, siz
 }
 
 __global__ void outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     // threads [0, ny): column nodes (0, i); thread 0 also runs the corner's
@@ -123,6 +125,7 @@ __global__ void outlet64(double* f, double* g, int nS, int nx, int ny, size_t L,
 // and the species' initial conditions.
 __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                        SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1, double init2) {
+    pdl_wait();
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L) return;
     double fi[9] = {1.0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -153,17 +156,17 @@ __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double
 
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
-    stream_collide64<<<grid, 256, 0, s>>>(a);
+    launch_pdl(stream_collide64, grid, 256, 0, s, a);
 }
 
 void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {
     const int n = nx + ny;
-    outlet64<<<(n + 255) / 256, 256, 0, s>>>(f, g, nS, nx, ny, L, st);
+    launch_pdl(outlet64, (n + 255) / 256, 256, 0, s, f, g, nS, nx, ny, L, st);
 }
 
 void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s) {
-    init64<<<(unsigned)((L + 255) / 256), 256, 0, s>>>(f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
+    launch_pdl(init64, (unsigned)((L + 255) / 256), 256, 0, s, f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
                                                        init[1], init[2]);
 }
 

@@ -60,6 +60,7 @@ __device__ __forceinline__ double dirac(const double dx, const double dy) {
 // ---------------------------------------------------------------------------
 // Force evaluation
 __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -127,7 +128,7 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration)
 template <typename Real>
 void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    force_eval_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, st, iteration);
+    launch_pdl(force_eval_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st, iteration);
 }
 template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t);
 template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t);
@@ -193,6 +194,7 @@ __device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid) {
 }
 
 __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st, int pass) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool ok = i < m.topo->M;
@@ -262,6 +264,7 @@ __device__ __forceinline__ void sort_tile_list(const int* list, int cnt, int sor
 template <typename Real, int kSpreadMax, int kMinCount>
 __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, Real* force, int nx, int ny, size_t L,
                                                      Status* st, int sortBits) {
+    pdl_wait();
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
@@ -359,6 +362,7 @@ constexpr double kForceFix = 17592186044416.0;  // 2^44
 constexpr int kScatterChunk = 256;
 __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDev t, float* force, int nx, int ny,
                                                            size_t L, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int tile = blockIdx.x;
     const int cnt = t.count[tile];
@@ -433,17 +437,17 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     cudaMemsetAsync(t.fill, 0, sizeof(int) * t.nTiles, s);
     if (m.Mcap == 0) return;
     const int blocks = (m.Mcap + 127) / 128;
-    tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 0);
+    launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 0);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
-    tile_count_kernel<<<blocks, 128, 0, s>>>(m, t, nx, ny, st, 1);
+    launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 1);
     if constexpr (sizeof(Real) == 4) {
-        spread_fixed_kernel<<<t.nTiles, 256, 0, s>>>(m, t, (float*)force, nx, ny, L, st);
+        launch_pdl(spread_fixed_kernel, t.nTiles, 256, 0, s, m, t, (float*)force, nx, ny, L, st);
     } else {
         int bits = 1;
         while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
-        spread_kernel<Real, kSpreadSmall, 0><<<t.nTiles, 256, spread_smem(kSpreadSmall), s>>>(m, t, force, nx, ny, L,
+        launch_pdl(spread_kernel<Real, kSpreadSmall, 0>, t.nTiles, 256, spread_smem(kSpreadSmall), s, m, t, force, nx, ny, L,
                                                                                          st, bits);
-        spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1><<<t.nTiles, 256, spread_smem(kSpreadLarge), s>>>(
+        launch_pdl(spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1>, t.nTiles, 256, spread_smem(kSpreadLarge), s, 
             m, t, force, nx, ny, L, st, bits);
     }
 }
@@ -467,6 +471,7 @@ __device__ __forceinline__ bool needs_perturbation(double X, double Y) {
 template <typename Real>
 __global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny, size_t L, CrossDev c, Status* st,
                                    unsigned iteration) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -520,7 +525,7 @@ template <typename Real>
 void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
                         unsigned iteration, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    interp_move_kernel<Real><<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, u, nx, ny, L, c, st, iteration);
+    launch_pdl(interp_move_kernel<Real>, (m.Mcap + 127) / 128, 128, 0, s, m, u, nx, ny, L, c, st, iteration);
 }
 template void launch_interp_move<double>(const MembraneDev&, const double*, int, int, size_t, CrossDev&, Status*,
                                          unsigned, cudaStream_t);
@@ -534,6 +539,7 @@ template void launch_interp_move<float>(const MembraneDev&, const float*, int, i
 // of collectVelocity (GeometryNode.cpp:216-226) applied to G = dL/dF.
 __global__ void force_adjoint_kernel(MembraneDev m, const double* G, int nx, int ny, size_t L, double* gfx,
                                      double* gfy) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
     const double X = m.x[i], Y = m.y[i];
@@ -556,11 +562,12 @@ __global__ void force_adjoint_kernel(MembraneDev m, const double* G, int nx, int
 void launch_force_adjoint(const MembraneDev& m, const double* G, int nx, int ny, size_t L, double* gfx,
                           double* gfy, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    force_adjoint_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, G, nx, ny, L, gfx, gfy);
+    launch_pdl(force_adjoint_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, G, nx, ny, L, gfx, gfy);
 }
 
 // Connection::perturbConnection's tests (Connection.cpp:339, 363).
 __global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
@@ -573,7 +580,7 @@ __global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
 
 void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
     if (m.Ccap == 0) return;
-    perturb_conn_kernel<<<(m.Ccap + 127) / 128, 128, 0, s>>>(m, st);
+    launch_pdl(perturb_conn_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -686,6 +693,7 @@ __device__ __forceinline__ int for_each_record(const MembraneDev& m, int cn, int
 }
 
 __global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = cn < m.topo->C;
@@ -712,6 +720,7 @@ __global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Stat
 
 // Pass 1: among records at the closest distance, the earliest connection.
 __global__ void cross_tie_kernel(CrossDev c, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int n = min(st->pad[2], c.recCap);
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -724,6 +733,7 @@ __global__ void cross_tie_kernel(CrossDev c, Status* st) {
 // slot (order E,N,W,S = the reference's boundaryNodes_ scan order) decides the
 // node's tentative domain (PhysicalNode.cpp:111-115).
 __global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int n = min(st->pad[2], c.recCap);
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -753,6 +763,7 @@ __global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
 // that left their previous unit cell (GeometryHandler.cpp:610-636,
 // GeometryNode.cpp:256-261, Rectangle.cpp pointWithinBounds).
 __global__ void edge_check_kernel(MembraneDev m, int nx, int ny, Status* st, int stage) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -771,10 +782,10 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     if (m.Ccap == 0) return;
     const int blocks = (m.Ccap + 127) / 128;
     cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
-    crossings_kernel<<<blocks, 128, 0, s>>>(m, c, nx, ny, st);
-    cross_tie_kernel<<<296, 256, 0, s>>>(c, st);
-    cross_win_kernel<<<296, 256, 0, s>>>(c, dom, st);
-    edge_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_CROSSINGS);
+    launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
+    launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
+    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, dom, st);
+    launch_pdl(edge_check_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, nx, ny, st, ST_CROSSINGS);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
                                        unsigned, cudaStream_t);
@@ -783,7 +794,7 @@ template void launch_crossings<float>(const MembraneDev&, CrossDev&, const uint3
 
 void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigned iteration, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    edge_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, nx, ny, st, ST_REMESH);
+    launch_pdl(edge_check_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, nx, ny, st, ST_REMESH);
 }
 
 // ---------------------------------------------------------------------------
@@ -863,6 +874,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
                                                       const double* srcTab, int nDomains, const uint32_t* ctypeTab,
                                                       int cellTypesCopied, int nx, int ny, size_t L, Status* st,
                                                       unsigned iteration) {
+    pdl_wait();
     if (st->halt) return;
     const int cnt = st->nChanged;
     if (cnt == 0) return;
@@ -936,7 +948,7 @@ void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, c
                    size_t L, Status* st, unsigned iteration, cudaStream_t s) {
     if (c.changedCap <= 0) return;
     constexpr size_t smemBytes = kReinitSmem;
-    reinit_kernel<Real><<<1, 1024, smemBytes, s>>>(c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
+    launch_pdl(reinit_kernel<Real>, 1, 1024, smemBytes, s, c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
                                            cellTypesCopied, nx, ny, L, st, iteration);
 }
 template void launch_reinit<double>(CrossDev&, uint32_t*, double*, const double*, int, const SpeciesConst*,
@@ -951,6 +963,7 @@ template void launch_reinit<float>(CrossDev&, uint32_t*, float*, const float*, i
 // of the last W-slot boundary node at x' in [1, x], else dom(0, y), which must
 // be 0 (GeometryHandler.cpp:68-85).  Reads and clears the W-slot plane.
 __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* dom, int nx, int ny, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int y = blockIdx.x;
     const size_t row = (size_t)y * nx;
@@ -987,6 +1000,7 @@ __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* 
 // step's count, which lives on the device).
 // Resets the keys written this step (every written key has a record).
 __global__ void cross_clear_kernel(CrossDev c, Status* st) {
+    pdl_wait();
     const int n = min(st->pad[2], c.recCap);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t key = c.recKey[k];
@@ -997,27 +1011,29 @@ __global__ void cross_clear_kernel(CrossDev c, Status* st) {
 
 void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
                         cudaStream_t s) {
-    domain_fill_kernel<<<ny, 256, 0, s>>>(c, dom, nx, ny, st);
+    launch_pdl(domain_fill_kernel, ny, 256, 0, s, c, dom, nx, ny, st);
 }
 
 void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s) {
     if (c.recCap <= 0) return;
-    cross_clear_kernel<<<296, 256, 0, s>>>(c, st);
+    launch_pdl(cross_clear_kernel, 296, 256, 0, s, c, st);
 }
 
 // ---------------------------------------------------------------------------
 // Topology checks
 
 __global__ void remesh_check_kernel(Status* st) {
+    pdl_wait();
     if (st->halt) return;
     if (st->remesh) raise_halt(st, ST_REMESH);
 }
 
-void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s) { remesh_check_kernel<<<1, 1, 0, s>>>(st); }
+void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s) { launch_pdl(remesh_check_kernel, 1, 1, 0, s, st); }
 
 // GeometryHandler::coarsenBoundary's test (GeometryHandler.cpp:444-449): the
 // span from the previous node to the next node is below MAXLENGTH.
 __global__ void coarsen_check_kernel(MembraneDev m, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -1032,16 +1048,17 @@ __global__ void coarsen_check_kernel(MembraneDev m, Status* st) {
 
 void launch_coarsen_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    coarsen_check_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, st);
+    launch_pdl(coarsen_check_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st);
 }
 
 __global__ void clear_forces_kernel(MembraneDev m) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i <= m.topo->M) m.foff[i] = 0;
 }
 
 void launch_clear_forces(MembraneDev& m, cudaStream_t s) {
-    clear_forces_kernel<<<(m.Mcap + 1 + 255) / 256, 256, 0, s>>>(m);
+    launch_pdl(clear_forces_kernel, (m.Mcap + 1 + 255) / 256, 256, 0, s, m);
 }
 
 // Tension renewal when the force list holds only tension pairs: node i gets
@@ -1049,6 +1066,7 @@ void launch_clear_forces(MembraneDev& m, cudaStream_t s) {
 // contributing connection in the connection vector
 // (tutorial_01_BioSolverMembraneTension.cpp:52-73 adds them in that order).
 __global__ void tension_pos_kernel(MembraneDev m, int* outPos, int* inPos) {
+    pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
     outPos[m.ca[c]] = c;
@@ -1056,6 +1074,7 @@ __global__ void tension_pos_kernel(MembraneDev m, int* outPos, int* inPos) {
 }
 
 __global__ void tension_fill_kernel(MembraneDev m, const int* outPos, const int* inPos, double force) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m.topo->M) return;
     m.foff[i] = 2 * i;
@@ -1074,8 +1093,8 @@ __global__ void tension_fill_kernel(MembraneDev m, const int* outPos, const int*
 
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s) {
     if (m.Mcap == 0) return;
-    tension_pos_kernel<<<(m.Ccap + 127) / 128, 128, 0, s>>>(m, outPos, inPos);
-    tension_fill_kernel<<<(m.Mcap + 1 + 127) / 128, 128, 0, s>>>(m, outPos, inPos, force);
+    launch_pdl(tension_pos_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, outPos, inPos);
+    launch_pdl(tension_fill_kernel, (m.Mcap + 1 + 127) / 128, 128, 0, s, m, outPos, inPos, force);
 }
 
 // ---------------------------------------------------------------------------
@@ -1087,6 +1106,7 @@ void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double forc
 constexpr int kAreaMax = 4096;
 
 __global__ void __launch_bounds__(256) areas_kernel(MembraneDev m, double* area, Status* st) {
+    pdl_wait();
     const int cell = blockIdx.x;
     const int b = m.ringStart[cell], e = m.ringStart[cell + 1];
     const int np = e - b;
@@ -1111,6 +1131,7 @@ __global__ void __launch_bounds__(256) areas_kernel(MembraneDev m, double* area,
 __global__ void area_regulator_kernel(MembraneDev m, const double* area, double* target, double* massTab,
                                       int nDomains, double factor, double strength, double maxsource,
                                       const Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= m.nCells) return;
@@ -1130,6 +1151,7 @@ __global__ void area_regulator_kernel(MembraneDev m, const double* area, double*
 // the order; no ring ranking is needed.  FP64 runs keep the ring-ordered sum.
 constexpr double kAreaFix = 16777216.0;  // 2^24
 __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDomains, unsigned long long* acc) {
+    pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     int cell = -1;
     long long v = 0;
@@ -1151,6 +1173,7 @@ __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDom
 }
 
 __global__ void areas_fixed_finish(unsigned long long* acc, int nCells, double* area) {
+    pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCells) return;
     area[c] = (double)(long long)acc[c] * (1.0 / kAreaFix) / 2.0;
@@ -1159,7 +1182,7 @@ __global__ void areas_fixed_finish(unsigned long long* acc, int nCells, double* 
 
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
     if (m.nCells == 0) return;
-    areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, nullptr);
+    launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, nullptr);
 }
 
 // The fixed device array of lbib_areas_static: the per-cell sums of one call.
@@ -1173,8 +1196,8 @@ cudaError_t static_area_scratch(double** ptr) {
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
-    areas_kernel<<<m.nCells, 256, 0, s>>>(m, area, (Status*)st);
-    area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
+    launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, (Status*)st);
+    launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
                                                                  strength, maxsource, st);
 }
 
@@ -1182,9 +1205,9 @@ void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, uns
                                  double* target, double* massTab, int nDomains, double factor, double strength,
                                  double maxsource, const Status* st, cudaStream_t s) {
     if (m.nCells == 0 || m.Ccap == 0) return;
-    areas_fixed_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, cellOfDom, nDomains, acc);
-    areas_fixed_finish<<<(m.nCells + 127) / 128, 128, 0, s>>>(acc, m.nCells, area);
-    area_regulator_kernel<<<(m.nCells + 127) / 128, 128, 0, s>>>(m, area, target, massTab, nDomains, factor,
+    launch_pdl(areas_fixed_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, cellOfDom, nDomains, acc);
+    launch_pdl(areas_fixed_finish, (m.nCells + 127) / 128, 128, 0, s, acc, m.nCells, area);
+    launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
                                                                  strength, maxsource, st);
 }
 

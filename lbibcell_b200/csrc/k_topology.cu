@@ -68,6 +68,7 @@ __device__ __forceinline__ void agg_min(int* addr, int key, int v) {
 // Remesh
 
 __global__ void remesh_flag_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng) {
+    pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c > m.Ccap) return;
     int f = 0;
@@ -87,6 +88,7 @@ __global__ void remesh_flag_kernel(MembraneDev m, TopoDev t, Status* st, int* nR
 // Decides the pass: K = number of splits; hands over to the host when the
 // pass would overflow a buffer, needs the random generator, or is a third one.
 __global__ void remesh_decide_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng, int lastPass) {
+    pdl_wait();
     if (st->halt) return;
     Topo* T = m.topo;
     const int C = T->C;
@@ -101,6 +103,7 @@ __global__ void remesh_decide_kernel(MembraneDev m, TopoDev t, Status* st, int* 
 }
 
 __global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const Topo* T = m.topo;
@@ -128,6 +131,7 @@ __global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const Topo* T = m.topo;
@@ -136,6 +140,7 @@ __global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void remesh_commit_kernel(MembraneDev m, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     Topo* T = m.topo;
     const int K = T->K;
@@ -151,6 +156,7 @@ __global__ void remesh_commit_kernel(MembraneDev m, Status* st) {
 // their old position is 5 lu away, so the edge test of
 // connectGeometryNodesToPhysicalNodes applies (GeometryHandler.cpp:618-636).
 __global__ void new_node_edge_kernel(MembraneDev m, int nx, int ny, Status* st, int from) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -167,6 +173,7 @@ __global__ void new_node_edge_kernel(MembraneDev m, int nx, int ny, Status* st, 
 // half of one longer than 2 * MAXLENGTH) needs another pass; that rare case
 // goes to the host, which repeats passes like SimulationRunner.cpp:190-199.
 __global__ void remesh_again_kernel(MembraneDev m, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
@@ -180,14 +187,14 @@ int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaSt
     int* nRng = &st->pad[1];
     const int cb = (m.Ccap + 1 + 255) / 256;
     cudaMemsetAsync(nRng, 0, sizeof(int), s);
-    remesh_flag_kernel<<<cb, 256, 0, s>>>(m, t, st, nRng);
+    launch_pdl(remesh_flag_kernel, cb, 256, 0, s, m, t, st, nRng);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
-    remesh_decide_kernel<<<1, 1, 0, s>>>(m, t, st, nRng, 0);
-    remesh_apply_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
-    remesh_copy_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, t, st);
-    remesh_commit_kernel<<<1, 1, 0, s>>>(m, st);
-    remesh_again_kernel<<<(m.Ccap + 255) / 256, 256, 0, s>>>(m, st);
-    new_node_edge_kernel<<<(m.Mcap + 255) / 256, 256, 0, s>>>(m, nx, ny, st, 0);
+    launch_pdl(remesh_decide_kernel, 1, 1, 0, s, m, t, st, nRng, 0);
+    launch_pdl(remesh_apply_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
+    launch_pdl(remesh_copy_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
+    launch_pdl(remesh_commit_kernel, 1, 1, 0, s, m, st);
+    launch_pdl(remesh_again_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, st);
+    launch_pdl(new_node_edge_kernel, (m.Mcap + 255) / 256, 256, 0, s, m, nx, ny, st, 0);
     return 9;
 }
 
@@ -196,6 +203,7 @@ int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaSt
 
 // Node -> its incoming / outgoing connection; node -> cell; candidates.
 __global__ void conn_links_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
@@ -205,6 +213,7 @@ __global__ void conn_links_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void coarsen_cand_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -229,6 +238,7 @@ constexpr size_t kCoarsenSmem = (size_t)kCoarsenMax * (2 * sizeof(double) + size
 // Handles: h < Ccap is connection index h; h >= Ccap is the connection made by
 // removing node h - Ccap.
 __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt || m.topo->nCand == 0) return;
     const int cell = blockIdx.x;
     const int b = m.ringStart[cell], len = m.ringStart[cell + 1] - b;
@@ -333,6 +343,7 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
 
 // Compaction flags: kept nodes; alive original connections; alive new ones.
 __global__ void coarsen_flags_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const Topo* T = m.topo;
     if (i <= m.Mcap) t.nflag[i] = (!st->halt && T->removed && i < T->M && !t.removed[i]) ? 1 : 0;
@@ -341,6 +352,7 @@ __global__ void coarsen_flags_kernel(MembraneDev m, TopoDev t, Status* st) {
 
 // Gathers the kept nodes and the alive connections into the scratch copies.
 __global__ void coarsen_gather_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt || m.topo->removed == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int M = m.topo->M, C = m.topo->C;
@@ -367,6 +379,7 @@ __global__ void coarsen_gather_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void coarsen_scatter_back_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt || m.topo->removed == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int M = m.topo->M, C = m.topo->C;
@@ -385,6 +398,7 @@ __global__ void coarsen_scatter_back_kernel(MembraneDev m, TopoDev t, Status* st
 }
 
 __global__ void coarsen_commit_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (st->halt) return;
     Topo* T = m.topo;
     if (T->removed == 0) { T->nCand = 0; return; }
@@ -399,6 +413,7 @@ __global__ void coarsen_commit_kernel(MembraneDev m, TopoDev t, Status* st) {
 
 // ncAlive as an int flag array for the scan of new connections
 __global__ void coarsen_ncflag_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m.Mcap) return;
     t.dist[i] = (!st->halt && m.topo->removed && i < m.topo->M && t.ncAlive[i]) ? 1 : 0;
@@ -410,18 +425,18 @@ int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     const int mb = (m.Mcap + 1 + 255) / 256, cbk = (m.Ccap + 1 + 255) / 256;
     const int gb = ((m.Mcap > m.Ccap ? m.Mcap : m.Ccap) + 1 + 255) / 256;
     int n = launch_rings(m, t, st, s);  // ring order after this step's remeshing
-    conn_links_kernel<<<cbk, 256, 0, s>>>(m, t, st);
-    coarsen_cand_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    launch_pdl(conn_links_kernel, cbk, 256, 0, s, m, t, st);
+    launch_pdl(coarsen_cand_kernel, mb, 256, 0, s, m, t, st);
     constexpr size_t smemBytes = kCoarsenSmem;
-    coarsen_cell_kernel<<<nCells, 256, smemBytes, s>>>(m, t, st);
-    coarsen_flags_kernel<<<gb, 256, 0, s>>>(m, t, st);
-    coarsen_ncflag_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    launch_pdl(coarsen_cell_kernel, nCells, 256, smemBytes, s, m, t, st);
+    launch_pdl(coarsen_flags_kernel, gb, 256, 0, s, m, t, st);
+    launch_pdl(coarsen_ncflag_kernel, mb, 256, 0, s, m, t, st);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.nflag, t.nrank, m.Mcap + 1, s);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.dist, t.succ, m.Mcap + 1, s);
-    coarsen_gather_kernel<<<gb, 256, 0, s>>>(m, t, st);
-    coarsen_scatter_back_kernel<<<gb, 256, 0, s>>>(m, t, st);
-    coarsen_commit_kernel<<<1, 1, 0, s>>>(m, t, st);
+    launch_pdl(coarsen_gather_kernel, gb, 256, 0, s, m, t, st);
+    launch_pdl(coarsen_scatter_back_kernel, gb, 256, 0, s, m, t, st);
+    launch_pdl(coarsen_commit_kernel, 1, 1, 0, s, m, t, st);
     return n + 15;
 }
 
@@ -429,6 +444,7 @@ int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
 // Rings
 
 __global__ void ring_first_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (!m.topo->changed) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
@@ -437,6 +453,7 @@ __global__ void ring_first_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void ring_count_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (!m.topo->changed) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -445,6 +462,7 @@ __global__ void ring_count_kernel(MembraneDev m, TopoDev t, Status* st) {
 }
 
 __global__ void ring_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (!m.topo->changed) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
@@ -461,6 +479,7 @@ __global__ void ring_fill_kernel(MembraneDev m, TopoDev t, Status* st) {
 constexpr int kRingPerThread = 16;  // 256 threads x 16 = 4096 nodes per ring
 
 __global__ void __launch_bounds__(256) ring_rank_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
     if (!m.topo->changed) return;
     const int cell = blockIdx.x;
     const int b = t.cellStart[cell], len = t.cellCount[cell];
@@ -501,6 +520,7 @@ __global__ void __launch_bounds__(256) ring_rank_kernel(MembraneDev m, TopoDev t
 }
 
 __global__ void ring_done_kernel(MembraneDev m, TopoDev t) {
+    pdl_wait();
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d < t.nDomains) t.firstConn[d] = 0x7fffffff;
     if (d == 0) m.topo->changed = 0;
@@ -512,12 +532,12 @@ int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     const int mb = (m.Mcap + 255) / 256, cbk = (m.Ccap + 255) / 256;
     cudaMemsetAsync(t.cellCount, 0, sizeof(int) * (nCells + 1), s);
     cudaMemsetAsync(t.cellFill, 0, sizeof(int) * nCells, s);
-    ring_first_kernel<<<cbk, 256, 0, s>>>(m, t, st);
-    ring_count_kernel<<<mb, 256, 0, s>>>(m, t, st);
+    launch_pdl(ring_first_kernel, cbk, 256, 0, s, m, t, st);
+    launch_pdl(ring_count_kernel, mb, 256, 0, s, m, t, st);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.cellCount, t.cellStart, nCells + 1, s);
-    ring_fill_kernel<<<mb, 256, 0, s>>>(m, t, st);
-    ring_rank_kernel<<<nCells, 256, 0, s>>>(m, t, st);
-    ring_done_kernel<<<(t.nDomains + 255) / 256, 256, 0, s>>>(m, t);
+    launch_pdl(ring_fill_kernel, mb, 256, 0, s, m, t, st);
+    launch_pdl(ring_rank_kernel, nCells, 256, 0, s, m, t, st);
+    launch_pdl(ring_done_kernel, (t.nDomains + 255) / 256, 256, 0, s, m, t);
     return 7;
 }
 

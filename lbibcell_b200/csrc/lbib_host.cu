@@ -802,6 +802,7 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
 }
 
 __global__ void step_begin_kernel(Status* st) {
+    pdl_wait();
     if (st->halt) return;
     st->nPerturbNode = 0;
     st->nPerturbConn = 0;
@@ -812,13 +813,15 @@ __global__ void step_begin_kernel(Status* st) {
 }
 
 __global__ void step_end_kernel(Status* st) {
+    pdl_wait();
     if (st->halt) return;
     st->pad[0] += 1;  // steps completed in this batch
     st->iteration += 1;  // Parameters++ (SimulationRunner.cpp:98)
     st->cellTypesCopied = 1;
 }
 
-__global__ void iteration_inc_kernel(Status* st) { st->iteration += 1; }
+__global__ void iteration_inc_kernel(Status* st) {
+    pdl_wait(); st->iteration += 1; }
 
 // Launches the stage kernels of one step from `fromStage` on.  `coarsenStep`
 // (Parameters' iteration % 10 == 0) and `renewal` (the tension plugin's
@@ -834,7 +837,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
     const unsigned it = 0;  // kernels read the iteration from the status word
     long long nl = 0;
     if (fromStage <= ST_FORCE) {
-        step_begin_kernel<<<1, 1, 0, s>>>(h.st);
+        launch_pdl(step_begin_kernel, 1, 1, 0, s, h.st);
         launch_force_eval<Real>(h.m, h.st, it, s);
         nl += 1 + hasM;
     }
@@ -907,7 +910,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
             }
         }
     }
-    step_end_kernel<<<1, 1, 0, s>>>(h.st);
+    launch_pdl(step_end_kernel, 1, 1, 0, s, h.st);
     nl += 1;
     return nl;
 }
@@ -1545,7 +1548,7 @@ int lbib_lattice_step(lbib_handle* hh, int n, int outlet) {
         }
         if (h.profiling) CK(cudaEventRecord(h.kEvents[2 * i + 1], h.stream));
         h.cur = 1 - p;
-        lbib::iteration_inc_kernel<<<1, 1, 0, h.stream>>>(h.st);
+        launch_pdl(lbib::iteration_inc_kernel, 1, 1, 0, h.stream, h.st);
         h.iteration++;
     }
     CK(cudaEventRecord(h.evB, h.stream));

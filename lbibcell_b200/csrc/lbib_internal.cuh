@@ -20,9 +20,45 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace lbib {
+
+// Programmatic dependent launch.  The stage kernels of a step are short and
+// many; launching each with programmatic stream serialization lets the
+// launch and block scheduling of a kernel overlap the end of the previous
+// one.  No kernel triggers its dependents early, so a kernel's blocks start
+// only once every block of the previous kernel has exited, and each kernel
+// begins with griddepcontrol.wait, which returns once the previous grid has
+// completed and its memory operations are visible.  Ordering is therefore the
+// same as plain stream order.  LBIB_NO_PDL=1 launches without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("LBIB_NO_PDL");
+        return !(e && e[0] == '1');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Direction tables: libs/LbmLib/include/Direction.hpp:34-44 and
 // libs/LbmLib/src/Direction.cpp:27-61.
