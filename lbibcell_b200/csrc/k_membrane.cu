@@ -371,10 +371,21 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
         if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
         return;
     }
-    __shared__ unsigned long long acc[2][kTile * kTile];
+    // each 64-bit fixed-point sum is kept as a signed high part (bits 22..63)
+    // and an unsigned low part (bits 0..21), each summed with 32-bit integer
+    // atomics: the low parts of up to 1024 contributions cannot overflow
+    __shared__ int accHi[2][kTile * kTile];
+    __shared__ unsigned accLo[2][kTile * kTile];
     __shared__ double fa[kScatterChunk][5], fb[kScatterChunk][5], sF[2][kScatterChunk];
     __shared__ int org[kScatterChunk];
-    for (int j = threadIdx.x; j < kTile * kTile; j += blockDim.x) acc[0][j] = acc[1][j] = 0ull;
+    for (int j = threadIdx.x; j < kTile * kTile; j += blockDim.x) {
+        accHi[0][j] = accHi[1][j] = 0;
+        accLo[0][j] = accLo[1][j] = 0u;
+    }
+    if (cnt > 1024) {  // the low parts would overflow
+        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
+        return;
+    }
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
     const int* list = t.list + t.start[tile];
@@ -417,8 +428,13 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
             const int lx = ox + dx, ly = oy + dy;
             if ((unsigned)lx >= (unsigned)kTile || (unsigned)ly >= (unsigned)kTile) continue;
             const double dl = (fa[e][dx] * fb[e][dy]) / 16.0;
-            atomicAdd(&acc[0][ly * kTile + lx], (unsigned long long)__double2ll_rn(sF[0][e] * dl * kForceFix));
-            atomicAdd(&acc[1][ly * kTile + lx], (unsigned long long)__double2ll_rn(sF[1][e] * dl * kForceFix));
+            const long long vx = __double2ll_rn(sF[0][e] * dl * kForceFix);
+            const long long vy = __double2ll_rn(sF[1][e] * dl * kForceFix);
+            const int node = ly * kTile + lx;
+            atomicAdd(&accHi[0][node], (int)(vx >> 22));
+            atomicAdd(&accLo[0][node], (unsigned)(vx & 0x3fffff));
+            atomicAdd(&accHi[1][node], (int)(vy >> 22));
+            atomicAdd(&accLo[1][node], (unsigned)(vy & 0x3fffff));
         }
     }
     __syncthreads();
@@ -426,8 +442,10 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
     const int x = tileX0 + lx, y = tileY0 + ly;
     if (x >= nx || y >= ny) return;
     const size_t n = (size_t)y * nx + x;
-    force[n] = (float)((double)(long long)acc[0][threadIdx.x] * (1.0 / kForceFix));
-    force[L + n] = (float)((double)(long long)acc[1][threadIdx.x] * (1.0 / kForceFix));
+    const long long sx = (long long)accHi[0][threadIdx.x] * (1ll << 22) + (long long)accLo[0][threadIdx.x];
+    const long long sy = (long long)accHi[1][threadIdx.x] * (1ll << 22) + (long long)accLo[1][threadIdx.x];
+    force[n] = (float)((double)sx * (1.0 / kForceFix));
+    force[L + n] = (float)((double)sy * (1.0 / kForceFix));
 }
 
 template <typename Real>
