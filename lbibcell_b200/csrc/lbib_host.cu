@@ -1571,13 +1571,19 @@ int lbib_get_sizes(lbib_handle* hh, long long* s) {
     if (!hh || !s) return LBIB_ERR_STATE;
     Handle& h = hh->h;
     if (!h.err) {
-        try {
-            lbib::pull_topology(h);
-        } catch (const HostFail& e) {
-            h.err = e.code; h.msg = e.msg;
+        // the counts only: one small read, not the whole topology
+        lbib::Topo tp{};
+        if (cudaSetDevice(h.device) == cudaSuccess &&
+            cudaMemcpyAsync(&tp, h.m.topo, sizeof(tp), cudaMemcpyDeviceToHost, h.stream) == cudaSuccess &&
+            cudaStreamSynchronize(h.stream) == cudaSuccess) {
+            h.m.M = tp.M;
+            h.m.C = tp.C;
+        } else {
+            h.err = LBIB_ERR_CUDA;
+            h.msg = "lbib_get_sizes: reading the membrane counts failed";
         }
     }
-    s[0] = h.nx; s[1] = h.ny; s[2] = h.S; s[3] = (long long)h.ids.size(); s[4] = (long long)h.conns.size();
+    s[0] = h.nx; s[1] = h.ny; s[2] = h.S; s[3] = h.m.M; s[4] = h.m.C;
     s[5] = h.iteration; s[6] = h.precision; s[7] = h.hostEvents; s[8] = h.stepsDone; s[9] = h.m.nCells;
     return LBIB_OK;
 }
