@@ -211,6 +211,13 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
         const int tile = v ? ty * t.tilesX + tx : -1;
         if (pass == 0) {
             tile_agg_add(t.count, tile, v);
+        } else if (pass == 2) {
+            // FP32-shifted runs: one pass into fixed-size per-tile slots
+            const int slot = tile_agg_add(t.count, tile, v);
+            if (v) {
+                if (slot < kTileSlots) t.slots[(size_t)tile * kTileSlots + slot] = i;
+                else raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
+            }
         } else {
             const int slot = tile_agg_add(t.fill, tile, v);
             if (v) {
@@ -365,12 +372,8 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
     pdl_wait();
     if (st->halt) return;
     const int tile = blockIdx.x;
-    const int cnt = t.count[tile];
+    const int cnt = min(t.count[tile], kTileSlots);
     if (cnt == 0) return;
-    if (t.start[tile] + cnt > t.cap) {
-        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
-        return;
-    }
     // each 64-bit fixed-point sum is kept as a signed high part (bits 22..63)
     // and an unsigned low part (bits 0..21), each summed with 32-bit integer
     // atomics: the low parts of up to 1024 contributions cannot overflow
@@ -382,13 +385,10 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
         accHi[0][j] = accHi[1][j] = 0;
         accLo[0][j] = accLo[1][j] = 0u;
     }
-    if (cnt > 1024) {  // the low parts would overflow
-        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
-        return;
-    }
+
     const int tx = tile % t.tilesX, ty = tile / t.tilesX;
     const int tileX0 = tx * kTile, tileY0 = ty * kTile;
-    const int* list = t.list + t.start[tile];
+    const int* list = t.slots + (size_t)tile * kTileSlots;
     const double halfPi = M_PI / 2.0;
     for (int c0 = 0; c0 < cnt; c0 += kScatterChunk) {
         const int nc = min(kScatterChunk, cnt - c0);
@@ -452,21 +452,24 @@ template <typename Real>
 void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
                    unsigned iteration, cudaStream_t s) {
     cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
-    cudaMemsetAsync(t.fill, 0, sizeof(int) * t.nTiles, s);
     if (m.Mcap == 0) return;
     const int blocks = (m.Mcap + 127) / 128;
-    launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 0);
-    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
-    launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 1);
     if constexpr (sizeof(Real) == 4) {
+        // one pass into fixed per-tile slots, then the fixed-point scatter
+        launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 2);
         launch_pdl(spread_fixed_kernel, t.nTiles, 256, 0, s, m, t, (float*)force, nx, ny, L, st);
     } else {
+        // exact lists (count, scan, fill), then the ordered gather
+        cudaMemsetAsync(t.fill, 0, sizeof(int) * t.nTiles, s);
+        launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 0);
+        cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.count, t.start, t.nTiles + 1, s);
+        launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 1);
         int bits = 1;
         while ((1 << bits) < m.Mcap + 1 && bits < 31) ++bits;
-        launch_pdl(spread_kernel<Real, kSpreadSmall, 0>, t.nTiles, 256, spread_smem(kSpreadSmall), s, m, t, force, nx, ny, L,
-                                                                                         st, bits);
-        launch_pdl(spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1>, t.nTiles, 256, spread_smem(kSpreadLarge), s, 
-            m, t, force, nx, ny, L, st, bits);
+        launch_pdl(spread_kernel<Real, kSpreadSmall, 0>, t.nTiles, 256, spread_smem(kSpreadSmall), s, m, t, force, nx,
+                   ny, L, st, bits);
+        launch_pdl(spread_kernel<Real, kSpreadLarge, kSpreadSmall + 1>, t.nTiles, 256, spread_smem(kSpreadLarge), s, m,
+                   t, force, nx, ny, L, st, bits);
     }
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
@@ -886,6 +889,56 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     }
 }
 
+// The earlier changed nodes a changed node n waits for: its E,N,W,S (read
+// after write: n reads their new state) and NE / SW neighbours (SW reads n's
+// old state through its NE fallback) with a smaller row-major index; -1 none.
+__device__ __forceinline__ void reinit_deps(const CrossDev& c, size_t n, int nx, int ny, int* deps) {
+    const int x = (int)(n % nx), y = (int)(n / nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const size_t nbs[6] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x,
+                           (size_t)yp * nx + xp, (size_t)ym * nx + xm};
+#pragma unroll
+    for (int d = 0; d < 6; ++d) deps[d] = nbs[d] < n ? c.mark[nbs[d]] - 1 : -1;
+}
+
+// Re-initialisation, step 1: every changed node marks its position in the list.
+__global__ void reinit_mark_kernel(CrossDev c, Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    const int cnt = st->nChanged;
+    if (cnt > kReinitMax || cnt > c.changedCap) return;  // reported by the block kernel
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+        c.mark[c.changedNode[k]] = k + 1;
+}
+
+// Step 2, across the whole GPU: the nodes that wait for no other changed node
+// (almost all of them) are re-initialised at once.  No two such nodes read
+// each other (a changed neighbour in any of the six directions makes one of
+// the two wait for the other), so the order among them does not matter.
+template <typename Real>
+__global__ void reinit_free_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int nS, SpeciesConst sp0,
+                                   SpeciesConst sp1, SpeciesConst sp2, const double* srcTab, int nDomains,
+                                   const uint32_t* ctypeTab, int nx, int ny, size_t L, Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    const int cnt = st->nChanged;
+    if (cnt > kReinitMax || cnt > c.changedCap) return;  // reported by the block kernel
+    const SpeciesConst sp[3] = {sp0, sp1, sp2};
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const size_t n = c.changedNode[k];
+        int deps[6];
+        reinit_deps(c, n, nx, ny, deps);
+        bool free = true;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) free &= deps[d] < 0;
+        c.reinitDone[k] = free ? 1 : 0;
+        if (free)
+            reinit_node<Real>(n, c.changedDom[k], dom, g, u, nS, sp, srcTab, nDomains, ctypeTab, st->cellTypesCopied,
+                              c, nx, ny, L, st, st->iteration);
+    }
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom, Real* g, const Real* u, int nS,
                                                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2,
@@ -906,29 +959,16 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[6] = (int(*)[6])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    // keys node << 32 | newDom in list order; mark[node] = position + 1 lets
-    // each node find its changed neighbours without sorting
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-        key[k] = (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k];
-        c.mark[c.changedNode[k]] = k + 1;
-    }
+    // Step 3, one block: the nodes that wait for others, in dependency rounds
+    // (the marks and the free nodes' results come from steps 1 and 2)
+    if (threadIdx.x == 0) remaining = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-        const size_t n = (size_t)(key[k] >> 32);
-        const int x = (int)(n % nx), y = (int)(n / nx);
-        const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
-        const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-        const size_t nbs[6] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x,
-                               (size_t)yp * nx + xp, (size_t)ym * nx + xm};
-        for (int d = 0; d < 6; ++d) {
-            deps[k][d] = -1;
-            const size_t mnode = nbs[d];
-            if (mnode >= n) continue;
-            deps[k][d] = c.mark[mnode] - 1;
-        }
-        done[k] = 0;
+        key[k] = (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k];
+        reinit_deps(c, (size_t)c.changedNode[k], nx, ny, deps[k]);
+        done[k] = c.reinitDone[k];
+        if (!done[k]) atomicAdd(&remaining, 1);
     }
-    if (threadIdx.x == 0) remaining = cnt;
     __syncthreads();
     int rounds = 0;
     while (remaining > 0 && rounds < kReinitMax + 1) {
@@ -966,6 +1006,9 @@ void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, c
                    size_t L, Status* st, unsigned iteration, cudaStream_t s) {
     if (c.changedCap <= 0) return;
     constexpr size_t smemBytes = kReinitSmem;
+    launch_pdl(reinit_mark_kernel, 148, 256, 0, s, c, st);
+    launch_pdl(reinit_free_kernel<Real>, 148, 256, 0, s, c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains,
+               ctypeTab, nx, ny, L, st);
     launch_pdl(reinit_kernel<Real>, 1, 1024, smemBytes, s, c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
                                            cellTypesCopied, nx, ny, L, st, iteration);
 }

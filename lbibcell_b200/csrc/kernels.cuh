@@ -51,6 +51,7 @@ struct CrossDev {
     uint32_t* bnDom;             // 4*L
     uint32_t* wDom;              // L, W-slot winner domain + 1 (0: none)
     int* mark;                   // L, position + 1 of a node in this step's changed list (0: none)
+    unsigned char* reinitDone;   // changedCap: re-initialised by the wide pass
     uint32_t* changedNode;       // capacity: nodes whose domain changes
     uint32_t* changedDom;
     int changedCap;
@@ -71,7 +72,12 @@ struct TileDev {
     int cap;
     void* scanTmp;  // CUB temporary storage
     size_t scanTmpBytes;
+    int* slots;     // FP32-shifted runs: nTiles x kTileSlots membrane indices (unordered)
 };
+
+// Entries a tile's slot list holds (the fixed-point spread's 32-bit low parts
+// cannot overflow below 1024 contributions per lattice node either).
+constexpr int kTileSlots = 1024;
 
 // Scratch of the device-side topology edits and the ring ranking.
 struct TopoDev {

@@ -209,9 +209,9 @@ Handle::~Handle() {
     fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
     fr(outPos); fr(inPos); fr(area); fr(target); fr(areaAcc);
-    fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp);
+    fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp); fr(tiles.slots);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
-    fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList);
+    fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
     fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist);
     fr(m.topo); fr(m.cdesc);
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
@@ -565,7 +565,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode);
+        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode); fr(h.cross.reinitDone);
         fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
         fr(h.cross.changedDom);
         fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
@@ -583,6 +583,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.cross.recDom = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDist = dalloc<unsigned long long>(h.cross.recCap);
         h.cross.changedNode = dalloc<uint32_t>(h.cross.changedCap);
+        h.cross.reinitDone = dalloc<unsigned char>(h.cross.changedCap);
         h.cross.changedDom = dalloc<uint32_t>(h.cross.changedCap);
     }
     if (grow(F, h.Fcap)) {
@@ -843,7 +844,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
     }
     if (fromStage <= ST_SPREAD) {
         launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s);
-        nl += hasM ? (sizeof(Real) == 8 ? 6 : 5) : 0;
+        nl += hasM ? (sizeof(Real) == 8 ? 6 : 2) : 0;
     }
     if (fromStage <= ST_COLLIDE) {
         if (evCollideA) cudaEventRecord(evCollideA, s);
@@ -874,7 +875,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
         for (int k = 0; k < h.S; ++k) spc[k] = h.sp[k].c;
         launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, 0,
                             h.nx, h.ny, h.L, h.st, it, s);
-        nl += 1;
+        nl += 3;
     }
     if (fromStage <= ST_DOMAIN) {
         launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
@@ -1157,6 +1158,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.tiles.count, 0, sizeof(int) * (h.tiles.nTiles + 1), h.stream));
     cub::DeviceScan::ExclusiveSum(nullptr, h.tiles.scanTmpBytes, h.tiles.count, h.tiles.start, h.tiles.nTiles + 1, h.stream);
     CK(cudaMalloc(&h.tiles.scanTmp, std::max<size_t>(h.tiles.scanTmpBytes, 16)));
+    if (h.precision == LBIB_FP32_SHIFTED) h.tiles.slots = dalloc<int>((size_t)h.tiles.nTiles * kTileSlots);
 
     // crossing planes
     h.cross.bnDist = dalloc<unsigned long long>(4 * h.L);
