@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) f[q] = fprev[(size_t)q * L + pull[q]];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) lf[q] = a.seed ? 0.0 : a.pf[(size_t)q * L + push[q]];
+    for (int q = 0; q < 9; ++q) lf[q] = a.seed ? 0.0 : (double)a.pf[(size_t)q * L + push[q]];
     double gA[NS > 0 ? NS : 1][5], muA[NS > 0 ? NS : 1][5];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -103,9 +103,9 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) muA[k][q] = sd;
         } else {
-            const double* pg = a.pg + (size_t)k * 5 * L;
+            const float* pg = a.pg + (size_t)k * 5 * L;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) muA[k][q] = pg[(size_t)q * L + push[q]];
+            for (int q = 0; q < 5; ++q) muA[k][q] = (double)pg[(size_t)q * L + push[q]];
         }
     }
     const uint32_t dom = a.dom[n];
@@ -230,9 +230,9 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
         muox += tauIk * C * 0.5 * (mu[1] - mu[3]);
         muoy += tauIk * C * 0.5 * (mu[2] - mu[4]);
         if (valid) {
-            double* qg = a.qg + (size_t)k * 5 * L;
+            float* qg = a.qg + (size_t)k * 5 * L;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) qg[(size_t)q * L + n] = (1.0 - tauIk) * mu[q] + mC;
+            for (int q = 0; q < 5; ++q) qg[(size_t)q * L + n] = (float)((1.0 - tauIk) * mu[q] + mC);
         }
         gTauK[k] = valid ? gTau : 0.0;
         if (valid && sp.kind == RX_LINEAR) a.racc[(size_t)k * L + n] = raccA[k] + mR;
@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
     mrhoF += mrho;
     if (valid) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) a.qf[(size_t)q * L + n] = (1.0 - tauI) * lf[q] + mrhoF + kCX[q] * mjx + kCY[q] * mjy;
+        for (int q = 0; q < 9; ++q)
+            a.qf[(size_t)q * L + n] = (float)((1.0 - tauI) * lf[q] + mrhoF + kCX[q] * mjx + kCY[q] * mjy);
         a.G[n] = Gx + mfx;
         a.G[L + n] = Gy + mfy;
     }

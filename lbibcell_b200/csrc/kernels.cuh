@@ -167,11 +167,11 @@ struct AdjointArgs {
     int S;
     const double* fprev;   // 9*L      state after step t-1
     const double* gprev;   // S*5*L
-    const double* pf;      // 9*L      adjoint planes of step t+1 (unused with seed)
-    const double* pg;      // S*5*L
+    const float* pf;       // 9*L      adjoint planes of step t+1 (unused with seed), FP32
+    const float* pg;       // S*5*L
     const double* seed;    // S*L      dL/dC_k at the final step, or nullptr
-    double* qf;            // 9*L      adjoint planes of step t (output)
-    double* qg;            // S*5*L
+    float* qf;             // 9*L      adjoint planes of step t (output), FP32
+    float* qg;             // S*5*L
     const double* force;   // 2*L      spread force field (zero outside the force tiles)
     const uint32_t* dom;
     const double* massTab; // per-domain rhoToAdd, or nullptr

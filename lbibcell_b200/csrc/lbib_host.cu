@@ -1435,12 +1435,13 @@ static void diff_backward(Handle& h, DiffCtx& d) {
             a.fprev = prev;
             a.gprev = prev + 9 * L;
             const bool seedStep = t == d.T;
-            const double* pin = d.P[(t + 1) & 1];
+            // the adjoint planes are FP32 (in the first half of the state-sized buffers)
+            const float* pin = (const float*)d.P[(t + 1) & 1];
             a.pf = seedStep ? nullptr : pin;
             a.pg = seedStep ? nullptr : pin + 9 * L;
             a.seed = seedStep ? d.seed : nullptr;
-            a.qf = d.P[t & 1];
-            a.qg = d.P[t & 1] + 9 * L;
+            a.qf = (float*)d.P[t & 1];
+            a.qg = (float*)d.P[t & 1] + 9 * L;
             a.iteration = d.it0 + (unsigned)(t - 1);
             launch_adjoint_step64(a, h.stream);
         }
