@@ -127,6 +127,25 @@ int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
  * production depends on the node's domain id). */
 int lbib_set_species_source(lbib_handle* h, int k, const double* rates, int n);
 
+/* Writes the simulation in the reference's four text formats, as
+ * SimulationRunner::writeSimulation does (SimulationRunner.cpp:112-149):
+ * the force list (ForceSolver::writeForceSolver, ForceSolver.cpp:141-156),
+ * the geometry (Geometry::writeGeometry, Geometry.cpp:77-95), the global
+ * parameters with the current iteration (GlobalSimulationParameters.cpp:74-97)
+ * and the solver dump (distributions per node, rows y then x, in the stored
+ * slot order).  Numbers are written with 17 significant digits, so a restart
+ * from these files continues with the same values; the reference's loaders
+ * read them unchanged.  Any file name may be NULL or empty to skip it. */
+int lbib_write_simulation(lbib_handle* h, const char* forceFile, const char* geometryFile, const char* parameterFile,
+                          const char* solverFile);
+
+/* Loads the distributions of a solver dump (SimulationRunner::initSolvers(file),
+ * SimulationRunner.cpp:151-182) into the lattice: the nodes the file lists take
+ * its values, the others keep theirs.  With lbib_create_from_files on the
+ * written parameter, geometry and force files this restarts a run, from a
+ * dump of this library or of the reference. */
+int lbib_load_solvers(lbib_handle* h, const char* solverFile);
+
 /* Number of domain ids (rows of the per-domain source and mass tables). */
 int lbib_get_domain_count(lbib_handle* h, int* n);
 

@@ -17,6 +17,7 @@ SYMBOLS = (
     "lbib_download_lattice", "lbib_upload_lattice", "lbib_download_membrane", "lbib_download_connections",
     "lbib_areas", "lbib_areas_static", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
     "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
+    "lbib_write_simulation", "lbib_load_solvers",
 )
 
 _lib = None
@@ -80,5 +81,9 @@ def load() -> ctypes.CDLL:
     L.lbib_diff_backward.argtypes = [vp, vp, vp, vp, vp]
     L.lbib_diff_end.restype = ip
     L.lbib_diff_end.argtypes = [vp]
+    L.lbib_write_simulation.restype = ip
+    L.lbib_write_simulation.argtypes = [vp, cp, cp, cp, cp]
+    L.lbib_load_solvers.restype = ip
+    L.lbib_load_solvers.argtypes = [vp, cp]
     _lib = L
     return L

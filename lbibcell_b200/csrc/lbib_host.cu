@@ -1945,3 +1945,170 @@ int lbib_diff_end(lbib_handle* hh) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoint files in the reference's formats.
+
+namespace {
+
+std::string g17(double v) {
+    char b[40];
+    std::snprintf(b, sizeof b, "%.17g", v);
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbib_write_simulation(lbib_handle* hh, const char* forceFile, const char* geometryFile, const char* parameterFile,
+                          const char* solverFile) {
+    API_BEGIN(hh)
+    lbib::pull_topology(h);
+    const int M = (int)h.ids.size();
+    const size_t L = h.L;
+    if (geometryFile && *geometryFile) {
+        // Geometry::writeGeometry (Geometry.cpp:77-95), nodes in id order
+        std::vector<double> x(M), y(M);
+        if (M) {
+            CK(cudaMemcpyAsync(x.data(), h.m.x, sizeof(double) * M, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(y.data(), h.m.y, sizeof(double) * M, cudaMemcpyDeviceToHost, h.stream));
+        }
+        CK(cudaStreamSynchronize(h.stream));
+        std::ofstream o(geometryFile);
+        if (!o.is_open()) lbib::fail(LBIB_ERR_INPUT, std::string("cannot open ") + geometryFile);
+        o << "#Nodes (id\txPos\tyPos)\n";
+        for (int i = 0; i < M; ++i) o << h.ids[i] << '\t' << g17(x[i]) << '\t' << g17(y[i]) << '\n';
+        o << "#Connection (nodeId1\tnodeId2\tdomainId\tbsolver\tcdesolver\t...)\n";
+        for (const auto& c : h.conns) o << c.id1 << '\t' << c.id2 << '\t' << c.dom << c.desc << '\n';
+    }
+    if (forceFile && *forceFile) {
+        // ForceSolver::writeForceSolver (ForceSolver.cpp:141-156): per node in id
+        // order, its forces in insertion order, each as ForceStructs.hpp writes it
+        std::vector<int> foff(M + 1, 0);
+        if (M) CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (M + 1), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        const int nrec = foff[M];
+        std::vector<int> ftype(nrec), fpart(nrec);
+        std::vector<double> fpar(4 * (size_t)nrec);
+        if (nrec) {
+            CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * 4 * nrec, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+        }
+        std::ofstream o(forceFile);
+        if (!o.is_open()) lbib::fail(LBIB_ERR_INPUT, std::string("cannot open ") + forceFile);
+        for (int i = 0; i < M; ++i)
+            for (int r = foff[i]; r < foff[i + 1]; ++r) {
+                const int t = ftype[r];
+                const double* p = &fpar[4 * (size_t)r];
+                const unsigned partner = fpart[r] >= 0 && fpart[r] < M ? h.ids[fpart[r]] : 0u;
+                o << t << '\t' << h.ids[i];
+                switch (t) {
+                    case 0: case 7: o << '\t' << partner << '\t' << g17(p[0]) << '\t' << g17(p[1]); break;
+                    case 1: o << '\t' << g17(p[0]) << '\t' << g17(p[1]) << '\t' << g17(p[2]) << '\t' << g17(p[3]); break;
+                    case 2: o << '\t' << g17(p[0]) << '\t' << g17(p[1]); break;
+                    case 3: case 4: o << '\t' << g17(p[0]) << '\t' << g17(p[1]) << '\t' << g17(p[2]); break;
+                    default: o << '\t' << partner << '\t' << g17(p[0]); break;  // 5, 6
+                }
+                o << '\n';
+            }
+    }
+    if (parameterFile && *parameterFile) {
+        // GlobalSimulationParameters::writeGlobalSimulationParameters (GlobalSimulationParameters.cpp:74-97)
+        std::ofstream o(parameterFile);
+        if (!o.is_open()) lbib::fail(LBIB_ERR_INPUT, std::string("cannot open ") + parameterFile);
+        o << "#Global Parameter file\n";
+        o << "CurrentIterations:\t" << h.iteration << "\n";
+        o << "Iterations:\t" << h.iterations << "\n";
+        o << "ReportStep:\t" << h.reportStep << "\n";
+        o << "SizeX:\t" << h.nx << "\n";
+        o << "SizeY:\t" << h.ny << "\n";
+        o << "tauFluid:\t" << g17(h.tauF) << "\n";
+        o << "CDESolvers:";
+        for (const auto& sp : h.sp) o << '\t' << sp.name << '\t' << g17(sp.c.tau);
+        o << "\n";
+    }
+    if (solverFile && *solverFile) {
+        // SimulationRunner::writeSimulation's solver dump (SimulationRunner.cpp:121-145):
+        // rows y, then x; distributions in the stored (post-swap) slot order
+        std::vector<double> f(9 * L), g(5 * (size_t)h.S * L);
+        const int rc = lbib_download_lattice(hh, f.data(), h.S ? g.data() : nullptr, nullptr, nullptr, nullptr, nullptr);
+        if (rc) return rc;
+        std::ofstream o(solverFile);
+        if (!o.is_open()) lbib::fail(LBIB_ERR_INPUT, std::string("cannot open ") + solverFile);
+        o << "#Solvers (xPos\tyPos\tDistributions...)\n";
+        o << "#BEGIN FluidSolver\n";
+        for (int y = 0; y < h.ny; ++y)
+            for (int x = 0; x < h.nx; ++x) {
+                const size_t n = (size_t)y * h.nx + x;
+                o << x << '\t' << y;
+                for (int q = 0; q < 9; ++q) o << '\t' << g17(f[9 * n + q]);
+                o << '\n';
+            }
+        o << "#END FluidSolver\n";
+        for (int k = 0; k < h.S; ++k) {
+            o << "#BEGIN " << h.sp[k].name << "\n";
+            for (int y = 0; y < h.ny; ++y)
+                for (int x = 0; x < h.nx; ++x) {
+                    const size_t n = (size_t)y * h.nx + x;
+                    o << x << '\t' << y;
+                    for (int q = 0; q < 5; ++q) o << '\t' << g17(g[((size_t)k * L + n) * 5 + q]);
+                    o << '\n';
+                }
+            o << "#END " << h.sp[k].name << "\n";
+        }
+    }
+    API_END
+}
+
+int lbib_load_solvers(lbib_handle* hh, const char* solverFile) {
+    API_BEGIN(hh)
+    // SimulationRunner::initSolvers(file) (SimulationRunner.cpp:151-182): nodes
+    // listed in the file take its distributions, the others keep theirs
+    std::ifstream in(solverFile ? solverFile : "");
+    if (!in.is_open()) lbib::fail(LBIB_ERR_INPUT, "Cannot find the solver file.");
+    const size_t L = h.L;
+    std::vector<double> f(9 * L), g(5 * (size_t)h.S * L);
+    int rc = lbib_download_lattice(hh, f.data(), h.S ? g.data() : nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    std::string line, solver;
+    int k = -1;
+    while (std::getline(in, line)) {
+        if (line.empty()) continue;
+        std::stringstream ls(line);
+        if (line[0] == '#') {
+            std::string tag;
+            if (line.find("#BEGIN") != std::string::npos) {
+                ls >> tag >> solver;
+                k = -1;
+                if (solver != "FluidSolver") {
+                    for (int j = 0; j < h.S; ++j)
+                        if (h.sp[j].name == solver) k = j;
+                    if (k < 0) lbib::fail(LBIB_ERR_INPUT, "unknown CDE solver in the solver file: " + solver);
+                }
+            } else if (line.find("#END") != std::string::npos) {
+                solver.clear();
+            }
+            continue;
+        }
+        int x, y;
+        ls >> x >> y;
+        if (!ls || x < 0 || y < 0 || x >= h.nx || y >= h.ny) lbib::fail(LBIB_ERR_INPUT, "bad node in the solver file: " + line);
+        const size_t n = (size_t)y * h.nx + x;
+        if (solver == "FluidSolver") {
+            for (int q = 0; q < 9; ++q) ls >> f[9 * n + q];
+        } else if (k >= 0) {
+            for (int q = 0; q < 5; ++q) ls >> g[((size_t)k * L + n) * 5 + q];
+        } else {
+            lbib::fail(LBIB_ERR_INPUT, "solver file line outside a #BEGIN/#END block: " + line);
+        }
+        if (!ls) lbib::fail(LBIB_ERR_INPUT, "bad distributions in the solver file: " + line);
+    }
+    rc = lbib_upload_lattice(hh, f.data(), h.S ? g.data() : nullptr, nullptr);
+    if (rc) return rc;
+    API_END
+}
+
+}  // extern "C"

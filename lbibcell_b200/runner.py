@@ -150,6 +150,19 @@ class Simulation:
             raise self._error()
         return {int(d[i]): float(a[i]) for i in range(n)}
 
+    # -- checkpoint files (the reference's formats) ------------------------------
+    def write_simulation(self, prefix: str) -> Dict[str, str]:
+        """SimulationRunner::writeSimulation into prefix_{force,geometry,parameters,solver}.txt;
+        returns the paths (keys as the configuration files)."""
+        paths = {k: f"{prefix}_{k}.txt" for k in ("force", "geometry", "parameters", "solver")}
+        self._check(self._L.lbib_write_simulation(self._h, *[paths[k].encode() for k in
+                                                                ("force", "geometry", "parameters", "solver")]))
+        return paths
+
+    def load_solvers(self, solver_file: str) -> None:
+        """SimulationRunner::initSolvers(file): the distributions of a solver dump."""
+        self._check(self._L.lbib_load_solvers(self._h, solver_file.encode()))
+
     # -- differentiated runs (frozen geometry, FP64) -----------------------------
     def domain_count(self) -> int:
         n = ctypes.c_int(0)

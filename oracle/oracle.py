@@ -182,11 +182,14 @@ def read_dump(path: str) -> State:
     return State(t, nx, ny, S, it, f, g, vel, force, dom, ctype, ids, node, conn, counters)
 
 
-def run_reference(paths: Dict[str, str], outdir: str, driver: str = REF_DRIVER, timeout: float = 3600) -> Dict[int, State]:
-    """Run the reference build on a configuration; returns its dumps by time."""
+def run_reference(paths: Dict[str, str], outdir: str, driver: str = REF_DRIVER, timeout: float = 3600,
+                  extra=()) -> Dict[int, State]:
+    """Run the reference build on a configuration; returns its dumps by time.
+    ``extra``: further driver arguments ("restart", solver file; "write", prefix)."""
     os.makedirs(outdir, exist_ok=True)
     env = dict(os.environ, OMP_NUM_THREADS="1")
-    r = subprocess.run([driver, paths["parameters"], paths["geometry"], paths["force"], paths["plugins"], outdir],
+    r = subprocess.run([driver, paths["parameters"], paths["geometry"], paths["force"], paths["plugins"], outdir]
+                       + [str(a) for a in extra],
                        cwd=outdir, env=env, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"reference run failed: {r.stderr}{r.stdout}")

@@ -8,11 +8,15 @@
 // A report functor (the reference's own reporter API,
 // AbstractReportFunctor.hpp) dumps the state every ReportStep iterations.
 //
-// usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir [timing W K]
+// usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir
+//                   [timing W K] [restart SOLVERFILE] [write PREFIX]
 //   With "timing W K" no reporter is registered: runSimulation() runs W
 //   untimed iterations, then K iterations whose wall time is printed as JSON
-//   (the CPU baseline).  The log goes to outdir/log.txt as in
-//   apps/tutorial_01.cpp:47-57.
+//   (the CPU baseline).  "restart SOLVERFILE" loads the distributions with
+//   SimulationRunner::initSolvers(file) after initSolvers(); "write PREFIX"
+//   calls SimulationRunner::writeSimulation at the end, into PREFIX_force.txt,
+//   PREFIX_geometry.txt, PREFIX_parameters.txt and PREFIX_solver.txt.  The log
+//   goes to outdir/log.txt as in apps/tutorial_01.cpp:47-57.
 //
 // Dump file outdir/dump_<t>.bin (little endian):
 //   int64 hdr[8] = {0x4c424942, t, nx, ny, S, M, C, currentIteration}
@@ -202,9 +206,25 @@ int main(int argc, char** argv) {
         std::cerr << "usage: ref_driver params geometry force plugins outdir [timing]\n";
         return 2;
     }
-    const bool timing = argc > 8 && std::string(argv[6]) == "timing";
-    const unsigned warm = timing ? (unsigned)std::stoul(argv[7]) : 0;
-    const unsigned steps = timing ? (unsigned)std::stoul(argv[8]) : 0;
+    bool timing = false;
+    unsigned warm = 0, steps = 0;
+    std::string restartFile, writePrefix;
+    for (int a = 6; a < argc; ++a) {
+        const std::string k = argv[a];
+        if (k == "timing" && a + 2 < argc) {
+            timing = true;
+            warm = (unsigned)std::stoul(argv[a + 1]);
+            steps = (unsigned)std::stoul(argv[a + 2]);
+            a += 2;
+        } else if (k == "restart" && a + 1 < argc) {
+            restartFile = argv[++a];
+        } else if (k == "write" && a + 1 < argc) {
+            writePrefix = argv[++a];
+        } else {
+            std::cerr << "unknown argument " << k << "\n";
+            return 2;
+        }
+    }
     try {
         std::shared_ptr<std::ostream> logStream(new std::ofstream(std::string(argv[5]) + "/log.txt"));
         UtilLib::Log::setStream(logStream);
@@ -218,11 +238,15 @@ int main(int argc, char** argv) {
             reporter.registerReporter(std::unique_ptr<LbmLib::reportHandler::AbstractReportFunctor>(
                 new DumpReporter(geohandler, argv[5])));
         simRunner.initSolvers();
+        if (!restartFile.empty()) simRunner.initSolvers(restartFile);
         simRunner.initForceSolver(argv[3]);
         if (pl.outlet) simRunner.addMassSolver("MassSolverBoxOutlet");
         for (const auto& b : pl.bio) simRunner.addBioSolver(b);
         if (!timing) {
             simRunner.runSimulation();
+            if (!writePrefix.empty())
+                simRunner.writeSimulation(writePrefix + "_force.txt", writePrefix + "_geometry.txt",
+                                          writePrefix + "_parameters.txt", writePrefix + "_solver.txt");
         } else {
             LbmLib::Parameters.iterations_ = warm;
             if (warm) simRunner.runSimulation();
