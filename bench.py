@@ -117,15 +117,21 @@ class ClockSampler:
 
 
 def dist_setup(n):
+    """One process per GPU (replicas: the ranks share only the barrier around
+    the timed region and the max of the timings).  NCCL on GPUs, gloo without."""
     rank, world, local = 0, 1, 0
     if n > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1:
-        import torch.distributed as dist
         import datetime
+        import torch
+        import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
         local = int(os.environ.get("LOCAL_RANK", "0"))
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -134,7 +140,8 @@ def dist_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -401,4 +408,9 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    try:
+        main()
+    finally:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
