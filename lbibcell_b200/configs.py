@@ -67,6 +67,9 @@ class Config:
     tension: Optional[Tuple[float, int]] = (0.1, 10)  # (force, frequency)
     area: Optional[Tuple[float, float, float]] = (1.2, 0.01, 0.004)  # factor, strength, maxsource
     forces: List[str] = field(default_factory=list)
+    # boundary solvers on every connection: (bsolver, cdesolver) pairs, as the
+    # reference's geometry files list them (apps/config/tutorial_02_geometry.txt)
+    boundary: List[Tuple[str, str]] = field(default_factory=list)
 
     @property
     def lattice_nodes(self) -> int:
@@ -105,8 +108,9 @@ class Config:
                 for i, a in enumerate(ids):
                     conns.append((a, ids[(i + 1) % len(ids)], dom))
             f.write("#Connection (nodeId1\tnodeId2\tdomainId\tbsolver\tcdesolver\t...)\n")
+            desc = "".join(f"\t{bs}\t{cde}" for bs, cde in self.boundary)
             for a, b, d in conns:
-                f.write(f"{a}\t{b}\t{d}\n")
+                f.write(f"{a}\t{b}\t{d}{desc}\n")
         with open(paths["force"], "w") as f:
             f.write("#Force 6 {type=6 id1 id2 f}\tmembrane tension (renewed by LbibMembraneTension)\n")
             for line in self.forces:

@@ -12,6 +12,7 @@
 // Species (rest state 0) are stored as g_q and updated as in
 // CDESolverD2Q5.cpp:75-107 with the dt*R/3, dt*R/6 source.
 #include "kernels.cuh"
+#include "lattice_math.cuh"
 
 namespace lbib {
 
@@ -96,6 +97,8 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
 #undef LBIB_Q
     const float s = rhoF * rinv;
     const float uxo = ux + s * Fx, uyo = uy + s * Fy;
+    if (NS > 0 && a.nfTab != nullptr)  // boundary solvers read the previous step's velocity
+        apply_noflux<float, float>(a, n, (double)a.u[n], (double)a.u[L + n], gi);
     a.u[n] = uxo;
     a.u[L + n] = uyo;
     // MassSolverBoxOutlet on the x=0 column and the y=0 row (the corner twice),

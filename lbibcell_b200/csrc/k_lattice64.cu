@@ -48,6 +48,8 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         fx = a.force[n];
         fy = a.force[L + n];
     }
+    // the fluid velocity of the previous step, for the boundary solvers
+    const double uPrevX = a.nfTab != nullptr ? a.u[n] : 0.0, uPrevY = a.nfTab != nullptr ? a.u[L + n] : 0.0;
     double ux, uy;
     collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
     a.u[n] = ux;
@@ -70,14 +72,18 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
 
+    double gAll[kMaxSpecies][5];
     for (int k = 0; k < a.S; ++k) {
         const double* gin = a.gin + (size_t)k * 5 * L;
-        double g[5];
-        g[T] = gin[0 * L + rC + x];
-        g[E] = gin[1 * L + rC + xm];
-        g[N] = gin[2 * L + rM + x];
-        g[W] = gin[3 * L + rC + xp];
-        g[S] = gin[4 * L + rP + x];
+        gAll[k][T] = gin[0 * L + rC + x];
+        gAll[k][E] = gin[1 * L + rC + xm];
+        gAll[k][N] = gin[2 * L + rM + x];
+        gAll[k][W] = gin[3 * L + rC + xp];
+        gAll[k][S] = gin[4 * L + rP + x];
+    }
+    if (a.nfTab != nullptr) apply_noflux<double, double>(a, n, uPrevX, uPrevY, gAll);
+    for (int k = 0; k < a.S; ++k) {
+        double* g = gAll[k];
         double src = 0.0;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
         collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.status->iteration);

@@ -753,7 +753,40 @@ __global__ void cross_tie_kernel(CrossDev c, Status* st) {
 // Pass 2: the winner writes its domain; the winner of a node's last present
 // slot (order E,N,W,S = the reference's boundaryNodes_ scan order) decides the
 // node's tentative domain (PhysicalNode.cpp:111-115).
-__global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
+// The boundary node of a winning record whose connection carries boundary
+// solvers: its position on the lattice line (BoundaryNode(i, getYPos(m, i, n))
+// or BoundaryNode(getXPos(m, i, n), i), Connection.cpp:243-312) and its
+// velocity, interpolated along the connection (Connection::calculateVelocity,
+// Connection.cpp:146-168), kept for the next step's no-flux solvers.
+__device__ __forceinline__ void record_noflux(const MembraneDev& m, CrossDev& c, int conn, uint32_t key, int nx) {
+    const int desc = m.cdesc[conn];
+    if (desc < 0 || c.nfTab[desc].nSolvers == 0) return;
+    const int a = m.ca[conn], b = m.cb[conn];
+    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+    const double mm = (y2 - y1) / (x2 - x1);
+    const double nn = y1 - (y2 - y1) / (x2 - x1) * x1;
+    const size_t node = key >> 2;
+    const int s = (int)(key & 3u);  // E, N, W, S
+    const int px = (int)(node % (size_t)nx), py = (int)(node / (size_t)nx);
+    double bx, by;
+    if (s == 1 || s == 3) {  // N / S slot: a crossing with the vertical line x = px
+        bx = (double)px;
+        by = mm * px + nn;
+    } else {                 // E / W slot: a crossing with the horizontal line y = py
+        bx = (py - nn) / mm;
+        by = (double)py;
+    }
+    const double l = sqrt((x1 - bx) * (x1 - bx) + (y1 - by) * (y1 - by));
+    const double Lc = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+    const double vx1 = m.vx[a], vy1 = m.vy[a], vx2 = m.vx[b], vy2 = m.vy[b];
+    c.nfU[2 * (size_t)key] = (vx2 - vx1) * l / Lc + vx1;
+    c.nfU[2 * (size_t)key + 1] = (vy2 - vy1) * l / Lc + vy1;
+    c.nfSpec[key] = (uint8_t)(desc + 1);
+    const int k = atomicAdd(c.nfN, 1);
+    if (k < c.nfCap) c.nfKeys[k] = key;
+}
+
+__global__ void cross_win_kernel(CrossDev c, MembraneDev m, const uint32_t* dom, int nx, Status* st) {
     pdl_wait();
     if (st->halt) return;
     const int n = min(st->pad[2], c.recCap);
@@ -764,6 +797,7 @@ __global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
         const size_t node = key >> 2;
         const int s = (int)(key & 3u);
         c.bnDom[key] = bdom;
+        if (c.nfTab != nullptr) record_noflux(m, c, (int)c.recConn[r], key, nx);
         if (s == 2) c.wDom[node] = bdom + 1;
         bool last = true;
         for (int s2 = s + 1; s2 < 4; ++s2)
@@ -778,6 +812,16 @@ __global__ void cross_win_kernel(CrossDev c, const uint32_t* dom, Status* st) {
             }
         }
     }
+}
+
+// Clears the previous step's no-flux boundary nodes (after the stream-collide
+// that used them, before this step's crossings set the new ones).
+__global__ void noflux_reset_kernel(CrossDev c) {
+    pdl_wait();
+    const int n = min(*c.nfN, c.nfCap);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) c.nfSpec[c.nfKeys[k]] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) *c.nfN = 0;
 }
 
 // GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test for nodes
@@ -802,10 +846,11 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
                       unsigned iteration, cudaStream_t s) {
     if (m.Ccap == 0) return;
     const int blocks = (m.Ccap + 127) / 128;
+    if (c.nfTab != nullptr) launch_pdl(noflux_reset_kernel, 1, 1024, 0, s, c);
     cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
     launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
-    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, dom, st);
+    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, st);
     launch_pdl(edge_check_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, nx, ny, st, ST_CROSSINGS);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,

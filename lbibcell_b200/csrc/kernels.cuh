@@ -60,6 +60,14 @@ struct CrossDev {
     // crossing records of this step (one per candidate node-slot pair)
     uint32_t* recKey; uint32_t* recConn; uint32_t* recDom; unsigned long long* recDist;
     int recCap;
+    // boundary nodes with boundary solvers, for the next step's stream-collide
+    // (nfTab == nullptr when no connection has one)
+    const NfSpec* nfTab;         // per connection descriptor index
+    uint8_t* nfSpec;             // 4*L, descriptor index + 1 (0: none)
+    double* nfU;                 // 8*L, boundary node velocity (x, y)
+    uint32_t* nfKeys;            // keys set in nfSpec, for the reset
+    int* nfN;                    // number of nfKeys
+    int nfCap;
 };
 
 // Tiles for force spreading.

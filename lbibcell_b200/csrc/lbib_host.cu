@@ -161,6 +161,7 @@ struct Handle {
     CrossDev cross{};
     TopoDev td{};
     std::vector<std::string> descTable;  // boundary-descriptor strings of the connections
+    NfSpec* nfTabDev = nullptr;          // boundary solvers per descriptor (device), nullptr: none
     Status* st = nullptr;
     Status* stHost = nullptr;
     cudaStream_t stream = nullptr;
@@ -212,7 +213,8 @@ Handle::~Handle() {
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp); fr(tiles.slots);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
-    fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist);
+    fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys);
+    fr(cross.nfSpec); fr(cross.nfU); fr(cross.nfN); fr(nfTabDev);
     fr(m.topo); fr(m.cdesc);
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
     fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
@@ -566,7 +568,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode); fr(h.cross.reinitDone);
-        fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
+        fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist); fr(h.cross.nfKeys);
         fr(h.cross.changedDom);
         fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
         const int n = h.Ccap;
@@ -579,6 +581,8 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.cross.changedCap = 8 * n + 1024;
         h.cross.recCap = 16 * n + 1024;
         h.cross.recKey = dalloc<uint32_t>(h.cross.recCap);
+        h.cross.nfKeys = dalloc<uint32_t>(h.cross.recCap);  // no more boundary nodes than records
+        h.cross.nfCap = h.cross.recCap;
         h.cross.recConn = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDom = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDist = dalloc<unsigned long long>(h.cross.recCap);
@@ -799,6 +803,11 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     for (int k = 0; k < h.S; ++k) a.sp[k] = h.sp[k].c;
     a.status = h.st;
     a.outlet = h.outlet ? 1 : 0;
+    if (h.cross.nfTab != nullptr) {
+        a.nfSpec = h.cross.nfSpec;
+        a.nfU = h.cross.nfU;
+        a.nfTab = h.cross.nfTab;
+    }
     return a;
 }
 
@@ -1118,6 +1127,7 @@ static void run_steps(Handle& h, int n) {
 // Construction
 
 static void cure_lattice(Handle& h, HostMembrane& hm);
+static void setup_boundary_solvers(Handle& h);
 
 static void create(Handle& h, const std::string& params, const std::string& geom, const std::string& forceFile,
                    const std::string& plugins) {
@@ -1245,6 +1255,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
         std::vector<int> z(h.m.M + 1, 0);
         CK(cudaMemcpyAsync(h.m.foff, z.data(), sizeof(int) * z.size(), cudaMemcpyHostToDevice, h.stream));
     }
+    setup_boundary_solvers(h);
     cure_lattice(h, hm);
 
     // SimulationRunner::initSolvers (SimulationRunner.cpp:290-306)
@@ -1265,6 +1276,50 @@ static void create(Handle& h, const std::string& params, const std::string& geom
 // GeometryHandler::cureLattice (GeometryHandler.cpp:149-170): perturb the
 // connections, bind the stencils (edge test), generate the crossings and set
 // every domain id by the row scan.  No species reinitialisation happens here.
+// The boundary solvers named on the connections ("bsolver cdesolver" pairs,
+// Geometry.cpp:122-151; Connection::connectionType_ is a map from solver name
+// to the CDE solvers in file order; BoundaryNode creates the solvers in the
+// map's name order, BoundaryNode.cpp:35-46).  Unknown names fail like the
+// reference's factories and getCDESolverSlow.
+static void setup_boundary_solvers(Handle& h) {
+    std::vector<NfSpec> tab(h.descTable.size());
+    bool any = false;
+    for (size_t i = 0; i < h.descTable.size(); ++i) {
+        std::map<std::string, std::vector<std::string>> type;
+        std::stringstream ls(h.descTable[i]);
+        std::string bs, cde;
+        while (ls >> bs >> cde) type[bs].push_back(cde);
+        NfSpec sp{};
+        for (const auto& kv : type) {
+            if (sp.nSolvers == 2) fail(ERR_INPUT, "more than two boundary solvers on a connection");
+            NfSolver& so = sp.s[sp.nSolvers++];
+            if (kv.first == "BoundarySolverNoFlux") so.kind = NF_NOFLUX;
+            else if (kv.first == "BoundarySolverNoFluxD2Q5") so.kind = NF_NOFLUX_D2Q5;
+            else fail(ERR_INPUT, "unknown boundary solver " + kv.first);
+            if (kv.second.size() > 4) fail(ERR_INPUT, "more than four CDE solvers for one boundary solver");
+            for (const auto& name : kv.second) {
+                int k = -1;
+                for (int j = 0; j < h.S; ++j)
+                    if (h.sp[j].name == name) k = j;
+                if (k < 0) fail(ERR_INPUT, "boundary solver for an unknown CDE solver " + name);
+                so.cde[so.nCde++] = k;
+            }
+        }
+        any |= sp.nSolvers > 0;
+        tab[i] = sp;
+    }
+    if (!any) return;
+    if (tab.size() > 255) fail(ERR_INPUT, "more than 255 distinct connection descriptors");
+    h.nfTabDev = dalloc<NfSpec>(tab.size());
+    CK(cudaMemcpyAsync(h.nfTabDev, tab.data(), sizeof(NfSpec) * tab.size(), cudaMemcpyHostToDevice, h.stream));
+    h.cross.nfTab = h.nfTabDev;
+    h.cross.nfSpec = dalloc<uint8_t>(4 * h.L);
+    CK(cudaMemsetAsync(h.cross.nfSpec, 0, 4 * h.L, h.stream));
+    h.cross.nfU = dalloc<double>(8 * h.L);
+    h.cross.nfN = dalloc<int>(1);
+    CK(cudaMemsetAsync(h.cross.nfN, 0, sizeof(int), h.stream));
+}
+
 static void cure_lattice(Handle& h, HostMembrane& hm) {
     perturb_connections(h, hm);
     CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
@@ -1854,6 +1909,8 @@ int lbib_get_domain_count(lbib_handle* hh, int* n) {
 int lbib_diff_begin(lbib_handle* hh, int T, int K) {
     API_BEGIN(hh)
     if (h.precision != LBIB_FP64) lbib::fail(LBIB_ERR_STATE, "differentiated runs need an FP64 handle");
+    if (h.cross.nfTab != nullptr)
+        lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover boundary solvers on connections");
     if (T < 1) lbib::fail(LBIB_ERR_INPUT, "differentiated run: T must be at least 1");
     if (K <= 0) K = (int)std::ceil(std::sqrt((double)T));
     if (K > T) K = T;

@@ -144,6 +144,21 @@ struct SpeciesConst {
     double decay;
 };
 
+// Boundary solvers on connections (the "bsolver cdesolver" pairs of a
+// geometry file's connection lines, Geometry.cpp:122-151), per distinct list
+// of pairs: the solvers in name order (BoundaryNode's std::map), each with its
+// CDE solvers in file order.
+enum NoFluxKind { NF_NOFLUX = 1, NF_NOFLUX_D2Q5 = 2 };  // BoundarySolverNoFlux, BoundarySolverNoFluxD2Q5
+struct NfSolver {
+    int kind;
+    int nCde;
+    int cde[4];  // species indices
+};
+struct NfSpec {
+    int nSolvers;
+    NfSolver s[2];
+};
+
 // Everything the fused stream-collide kernel reads besides the planes.
 template <typename Real>
 struct LatticeArgs {
@@ -166,6 +181,10 @@ struct LatticeArgs {
     SpeciesConst sp[kMaxSpecies];
     const Status* status;
     int outlet;                // MassSolverBoxOutlet registered: rescale x=0 / y=0 nodes
+    // no-flux boundary nodes of the previous step's crossings (nullptr: none)
+    const uint8_t* nfSpec;     // 4*L: descriptor index + 1 per (node, slot E,N,W,S), 0 none
+    const double* nfU;         // 8*L: the boundary node's velocity per (node, slot)
+    const NfSpec* nfTab;
 };
 
 constexpr int kTile = 16;  // force tiles are 16x16 lattice nodes
