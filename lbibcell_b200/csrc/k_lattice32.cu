@@ -97,8 +97,6 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
 #undef LBIB_Q
     const float s = rhoF * rinv;
     const float uxo = ux + s * Fx, uyo = uy + s * Fy;
-    if (NS > 0 && a.nfTab != nullptr)  // boundary solvers read the previous step's velocity
-        apply_noflux<float, float>(a, n, (double)a.u[n], (double)a.u[L + n], gi);
     a.u[n] = uxo;
     a.u[L + n] = uyo;
     // MassSolverBoxOutlet on the x=0 column and the y=0 row (the corner twice),
@@ -119,6 +117,9 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) fo[q * L + n] = ho[q];
 
+    // Species: e0 = C - 4 e1 rather than C/3, so that the equilibrium sums to C
+    // exactly up to one rounding: with C/3 and C/6 each rounded in FP32 the
+    // relaxation adds a systematic 3e-8 C / tau per step.
     const unsigned iteration = NS > 0 ? a.status->iteration : 0u;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = (float)a.srcTab[(size_t)k * a.nDomains + dom];
         const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, iteration, C);
         const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
-        const float e0 = C * (1.0f / 3.0f), e1 = C * (1.0f / 6.0f);
+        const float e1 = C * (1.0f / 6.0f), e0 = C - 4.0f * e1;
         float go[5];
         go[0] = gT + (e0 - gT) * tI + r0;
         go[1] = gE + (e1 * (1.0f + 3.0f * uxo) - gE) * tI + r1;
@@ -213,6 +214,7 @@ __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double ta
 
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
+    if (a.nfTab != nullptr) launch_noflux<float>(a, s);
     switch (a.S) {
         case 0: launch_pdl(stream_collide32<0>, grid, 256, 0, s, a); break;
         case 1: launch_pdl(stream_collide32<1>, grid, 256, 0, s, a); break;

@@ -15,6 +15,9 @@
 
 namespace lbib {
 
+// NS = number of species (a.S), a compile-time constant so that the pulled
+// species values stay in registers.
+template <int NS>
 __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
     pdl_wait();
     if (a.status->halt) return;
@@ -48,8 +51,6 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         fx = a.force[n];
         fy = a.force[L + n];
     }
-    // the fluid velocity of the previous step, for the boundary solvers
-    const double uPrevX = a.nfTab != nullptr ? a.u[n] : 0.0, uPrevY = a.nfTab != nullptr ? a.u[L + n] : 0.0;
     double ux, uy;
     collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
     a.u[n] = ux;
@@ -72,8 +73,9 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
 
-    double gAll[kMaxSpecies][5];
-    for (int k = 0; k < a.S; ++k) {
+    double gAll[NS > 0 ? NS : 1][5];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
         const double* gin = a.gin + (size_t)k * 5 * L;
         gAll[k][T] = gin[0 * L + rC + x];
         gAll[k][E] = gin[1 * L + rC + xm];
@@ -81,8 +83,8 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         gAll[k][W] = gin[3 * L + rC + xp];
         gAll[k][S] = gin[4 * L + rP + x];
     }
-    if (a.nfTab != nullptr) apply_noflux<double, double>(a, n, uPrevX, uPrevY, gAll);
-    for (int k = 0; k < a.S; ++k) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
         double* g = gAll[k];
         double src = 0.0;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
@@ -160,9 +162,120 @@ __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double
     }
 }
 
+// The boundary solvers of the boundary nodes recorded by the previous step's
+// crossings: BoundarySolverNoFlux(D2Q5)::preAdvect, then postAdvect
+// (BoundarySolverNoFlux.cpp:36-105, BoundarySolverNoFluxD2Q5.cpp:37-106), as
+// two passes over the (node, slot) list before the stream-collide kernel.
+//
+// A boundary node in slot d (E, N, W, S) of lattice node n lies between n and
+// its neighbour n + c_d; the population it acts on is direction dir =
+// inverse(d), which node n pulls from n + c_d.  preAdvect forms, from node n's
+// state before the step and the boundary node's velocity, D = feq_b(dir) +
+// (g_dir(n) - feq_n(dir)) for the first CDE solver each boundary solver serves
+// (its loop returns after that one).  postAdvect then swaps D into the
+// post-advect value of direction dir of each served species in turn, so the
+// first gets D and each further one the previous one's value.  Pulling makes
+// "post-advect value of dir at n" the stored slot (dir, n + c_d), which no
+// other node reads: the swap writes there, and the stream-collide kernel pulls
+// the result.  The first pass only reads (every D sees the state before any
+// swap, as all preAdvects run before the advection); the second only swaps.
+template <typename Real>
+__global__ void noflux_pre_kernel(LatticeArgs<Real> a) {
+    pdl_wait();
+    if (a.status->halt) return;
+    const int cnt = min(*a.nfN, a.nfCap);
+    const size_t L = a.L;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const uint32_t key = a.nfKeys[e];
+        const size_t n = key >> 2;
+        const int d = (int)(key & 3u) + 1;                             // E, N, W, S
+        const int dir = d == E ? W : (d == N ? S : (d == W ? E : N));  // boundary node -> n
+        const NfSpec& sp = a.nfTab[a.nfSpec[key] - 1];
+        const double ub = a.nfU[2 * (size_t)key], vb = a.nfU[2 * (size_t)key + 1];
+        const double uPrevX = a.u[n], uPrevY = a.u[L + n];  // the fluid velocity of the previous step
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (j >= sp.nSolvers) break;
+            const Real* gk = a.gin + (size_t)sp.s[j].cde[0] * 5 * L;
+            // CDESolverD2Q5::getC over the stored slots (T, W, S, E, N directions)
+            double C = 0.0;
+            C += (double)gk[(size_t)T * L + n];
+            C += (double)gk[(size_t)W * L + n];
+            C += (double)gk[(size_t)S * L + n];
+            C += (double)gk[(size_t)E * L + n];
+            C += (double)gk[(size_t)N * L + n];
+            const bool d2q5 = sp.s[j].kind == NF_NOFLUX_D2Q5;
+            const double Cf = d2q5 ? C / 6.0 : C / 4.0;
+            const double c3 = d2q5 ? 3.0 : 2.0;
+            double feq;
+            if (dir == E) feq = Cf * (1 + c3 * ub);
+            else if (dir == N) feq = Cf * (1 + c3 * vb);
+            else if (dir == W) feq = Cf * (1 - c3 * ub);
+            else feq = Cf * (1 - c3 * vb);
+            // CDESolverD2Q5::calculateEquilibrium(dir) (CDESolverD2Q5.cpp:109-135)
+            const double w1 = C / 6.0;
+            double eq;
+            if (dir == E) eq = w1 * (1.0 + uPrevX * 3.0);
+            else if (dir == N) eq = w1 * (1.0 + uPrevY * 3.0);
+            else if (dir == W) eq = w1 * (1.0 + (-uPrevX) * 3.0);
+            else eq = w1 * (1.0 + (-uPrevY) * 3.0);
+            const double fneq = (double)gk[(size_t)dir * L + n] - eq;
+            a.nfD[2 * (size_t)e + j] = feq + fneq;
+        }
+    }
+}
+
+template <typename Real>
+__global__ void noflux_post_kernel(LatticeArgs<Real> a) {
+    pdl_wait();
+    if (a.status->halt) return;
+    const int cnt = min(*a.nfN, a.nfCap);
+    const size_t L = a.L;
+    const int nx = a.nx, ny = a.ny;
+    Real* g = const_cast<Real*>(a.gin);  // the current state, before this step's pull
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const uint32_t key = a.nfKeys[e];
+        const size_t n = key >> 2;
+        const int d = (int)(key & 3u) + 1;
+        const int dir = d == E ? W : (d == N ? S : (d == W ? E : N));
+        const NfSpec& sp = a.nfTab[a.nfSpec[key] - 1];
+        int x = (int)(n % (size_t)nx), y = (int)(n / (size_t)nx);
+        if (d == E) x = x == nx - 1 ? 0 : x + 1;
+        else if (d == N) y = y == ny - 1 ? 0 : y + 1;
+        else if (d == W) x = x == 0 ? nx - 1 : x - 1;
+        else y = y == 0 ? ny - 1 : y - 1;
+        const size_t from = (size_t)y * nx + x;  // node n pulls direction dir from here
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (j >= sp.nSolvers) break;
+            double cur = a.nfD[2 * (size_t)e + j];
+            for (int c = 0; c < sp.s[j].nCde; ++c) {
+                Real* slot = g + ((size_t)sp.s[j].cde[c] * 5 + dir) * L + from;
+                const double t = (double)*slot;
+                *slot = (Real)cur;
+                cur = t;
+            }
+        }
+    }
+}
+
+template <typename Real>
+void launch_noflux(const LatticeArgs<Real>& a, cudaStream_t s) {
+    launch_pdl(noflux_pre_kernel<Real>, 296, 256, 0, s, a);
+    launch_pdl(noflux_post_kernel<Real>, 296, 256, 0, s, a);
+}
+template void launch_noflux<double>(const LatticeArgs<double>&, cudaStream_t);
+template void launch_noflux<float>(const LatticeArgs<float>&, cudaStream_t);
+
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
-    launch_pdl(stream_collide64, grid, 256, 0, s, a);
+    if (a.nfTab != nullptr) launch_noflux<double>(a, s);
+    switch (a.S) {
+        case 0: launch_pdl(stream_collide64<0>, grid, 256, 0, s, a); break;
+        case 1: launch_pdl(stream_collide64<1>, grid, 256, 0, s, a); break;
+        case 2: launch_pdl(stream_collide64<2>, grid, 256, 0, s, a); break;
+        default: launch_pdl(stream_collide64<3>, grid, 256, 0, s, a); break;
+    }
 }
 
 void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s) {

@@ -382,10 +382,8 @@ __global__ void coarsen_scatter_back_kernel(MembraneDev m, TopoDev t, Status* st
     pdl_wait();
     if (st->halt || m.topo->removed == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int M = m.topo->M, C = m.topo->C;
     const int Mn = t.nrank[m.Mcap];
     const int Cn = t.rank[m.Ccap] + t.succ[m.Mcap];
-    (void)C;
     if (i < Mn) {
         const double* a = t.dalt;
         const size_t cap = (size_t)m.Mcap;

@@ -66,6 +66,7 @@ struct CrossDev {
     uint8_t* nfSpec;             // 4*L, descriptor index + 1 (0: none)
     double* nfU;                 // 8*L, boundary node velocity (x, y)
     uint32_t* nfKeys;            // keys set in nfSpec, for the reset
+    double* nfD;                 // 2 per key, scratch of the boundary solvers
     int* nfN;                    // number of nfKeys
     int nfCap;
 };
@@ -114,6 +115,10 @@ struct TopoDev {
 };
 
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s);
+// The membrane boundary solvers (2 launches, before the stream-collide kernel
+// of the same state); the stream-collide launchers call it when a.nfTab is set.
+template <typename Real>
+void launch_noflux(const LatticeArgs<Real>& a, cudaStream_t s);
 void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
 void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
                    const SpeciesConst* sp, const double* init, cudaStream_t s);

@@ -113,72 +113,3 @@ __host__ __device__ __forceinline__ void collide_cde64(double* gi, double ux, do
 }
 
 }  // namespace lbib
-
-namespace lbib {
-
-// The boundary solvers of the boundary nodes next to lattice node n, from
-// the previous step's crossings: BoundarySolverNoFlux(D2Q5)::preAdvect then
-// postAdvect (BoundarySolverNoFlux.cpp:36-105, BoundarySolverNoFluxD2Q5.cpp:37-106).
-// For a boundary node in slot d of node n (direction dir = inverse(d) from the
-// boundary node to n), preAdvect forms, from node n's state before the step
-// (stored planes `gin`, fluid velocity uPrev) and the boundary node's
-// velocity, the value D = feq_b(dir) + (f_dir(n) - feq_n(dir)) of the first CDE
-// solver it serves (its loop returns after that one); postAdvect then swaps D
-// into the post-advect value of direction dir of each served species in turn,
-// so the first gets D and each further one gets the previous one's value.
-// `G[k][q]` holds the pulled (post-advect) values of species k at node n.
-template <typename Real, typename V>
-__device__ __forceinline__ void apply_noflux(const LatticeArgs<Real>& a, size_t n, double uPrevX, double uPrevY,
-                                             V (*G)[5]) {
-    const uint32_t packed = *(const uint32_t*)(a.nfSpec + 4 * n);
-    if (packed == 0u) return;
-    const size_t L = a.L;
-    for (int s = 0; s < 4; ++s) {
-        const int spec = (int)((packed >> (8 * s)) & 0xffu);
-        if (spec == 0) continue;
-        const NfSpec& sp = a.nfTab[spec - 1];
-        const int d = s + 1;                                          // E, N, W, S
-        const int dir = d == E ? W : (d == N ? S : (d == W ? E : N));  // boundary node -> n
-        const double ub = a.nfU[2 * (4 * n + s)], vb = a.nfU[2 * (4 * n + s) + 1];
-        double D[2] = {0.0, 0.0};
-        for (int j = 0; j < sp.nSolvers; ++j) {
-            const int k1 = sp.s[j].cde[0];
-            const Real* gk = a.gin + (size_t)k1 * 5 * L;
-            // CDESolverD2Q5::getC over the stored slots (T, W, S, E, N directions)
-            double C = 0.0;
-            C += (double)gk[(size_t)T * L + n];
-            C += (double)gk[(size_t)W * L + n];
-            C += (double)gk[(size_t)S * L + n];
-            C += (double)gk[(size_t)E * L + n];
-            C += (double)gk[(size_t)N * L + n];
-            const bool d2q5 = sp.s[j].kind == NF_NOFLUX_D2Q5;
-            const double Cf = d2q5 ? C / 6.0 : C / 4.0;
-            const double c3 = d2q5 ? 3.0 : 2.0;
-            double feq;
-            if (dir == E) feq = Cf * (1 + c3 * ub);
-            else if (dir == N) feq = Cf * (1 + c3 * vb);
-            else if (dir == W) feq = Cf * (1 - c3 * ub);
-            else feq = Cf * (1 - c3 * vb);
-            // CDESolverD2Q5::calculateEquilibrium(dir) (CDESolverD2Q5.cpp:109-135)
-            const double w1 = C / 6.0;
-            double eq;
-            if (dir == E) eq = w1 * (1.0 + uPrevX * 3.0);
-            else if (dir == N) eq = w1 * (1.0 + uPrevY * 3.0);
-            else if (dir == W) eq = w1 * (1.0 + (-uPrevX) * 3.0);
-            else eq = w1 * (1.0 + (-uPrevY) * 3.0);
-            const double fneq = (double)gk[(size_t)dir * L + n] - eq;
-            D[j] = feq + fneq;
-        }
-        for (int j = 0; j < sp.nSolvers; ++j) {
-            double cur = D[j];
-            for (int c = 0; c < sp.s[j].nCde; ++c) {
-                const int k = sp.s[j].cde[c];
-                const double t = (double)G[k][dir];
-                G[k][dir] = (V)cur;
-                cur = t;
-            }
-        }
-    }
-}
-
-}  // namespace lbib

@@ -213,7 +213,7 @@ Handle::~Handle() {
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp); fr(tiles.slots);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
-    fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys);
+    fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys); fr(cross.nfD);
     fr(cross.nfSpec); fr(cross.nfU); fr(cross.nfN); fr(nfTabDev);
     fr(m.topo); fr(m.cdesc);
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
@@ -568,8 +568,13 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode); fr(h.cross.reinitDone);
-        fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist); fr(h.cross.nfKeys);
+        fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
         fr(h.cross.changedDom);
+        // the boundary-node list of the last crossings is still to be used by
+        // the next stream-collide and cleared after it: carried over
+        uint32_t* oldKeys = h.cross.nfKeys;
+        double* oldD = h.cross.nfD;
+        const int oldCap = h.cross.nfCap;
         fr(h.td.flag); fr(h.td.rank); fr(h.td.ca2); fr(h.td.cb2); fr(h.td.cdom2); fr(h.td.cdesc2); fr(h.td.connAlive);
         const int n = h.Ccap;
         h.m.ca = dalloc<int>(n); h.m.cb = dalloc<int>(n); h.m.cdom = dalloc<uint32_t>(n); h.m.cdesc = dalloc<int>(n);
@@ -582,7 +587,12 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.cross.recCap = 16 * n + 1024;
         h.cross.recKey = dalloc<uint32_t>(h.cross.recCap);
         h.cross.nfKeys = dalloc<uint32_t>(h.cross.recCap);  // no more boundary nodes than records
+        h.cross.nfD = dalloc<double>(2 * (size_t)h.cross.recCap);
         h.cross.nfCap = h.cross.recCap;
+        if (oldKeys != nullptr && oldCap > 0)
+            CK(cudaMemcpyAsync(h.cross.nfKeys, oldKeys, sizeof(uint32_t) * oldCap, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        fr(oldKeys); fr(oldD);
         h.cross.recConn = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDom = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDist = dalloc<unsigned long long>(h.cross.recCap);
@@ -720,64 +730,6 @@ static bool remesh(Handle& h, HostMembrane& hm) {
     return any;
 }
 
-// GeometryHandler::coarsenBoundary + Geometry::removeGeometryNode
-// (GeometryHandler.cpp:433-461, Geometry.cpp:402-431): nodes in id order; a
-// node whose neighbours are closer than MAXLENGTH is removed, its two
-// connections are erased and one from its predecessor to its successor is
-// appended.  Connections are kept in an append-only list with liveness flags
-// and per-node incoming/outgoing indices, compacted at the end.
-static bool coarsen(Handle& h, HostMembrane& hm) {
-    std::vector<HConn> list = h.conns;
-    std::vector<char> alive(list.size(), 1);
-    std::map<uint32_t, int> inC, outC, pos;
-    for (size_t c = 0; c < list.size(); ++c) {
-        outC[list[c].id1] = (int)c;
-        inC[list[c].id2] = (int)c;
-    }
-    for (size_t i = 0; i < h.ids.size(); ++i) pos[h.ids[i]] = (int)i;
-    std::vector<char> removed(h.ids.size(), 0);
-    bool any = false;
-    for (size_t i = 0; i < h.ids.size(); ++i) {
-        const uint32_t id = h.ids[i];
-        auto ii = inC.find(id), oo = outC.find(id);
-        if (ii == inC.end() || oo == outC.end()) fail(ERR_INPUT, "Geometry::removeGeometryNode: open membrane", id);
-        const int cin = ii->second, cout = oo->second;
-        const uint32_t n1 = list[cin].id1, n2 = list[cout].id2;
-        const int p1 = pos.at(n1), p2 = pos.at(n2);
-        const double length = std::sqrt((hm.x[p2] - hm.x[p1]) * (hm.x[p2] - hm.x[p1]) +
-                                        (hm.y[p2] - hm.y[p1]) * (hm.y[p2] - hm.y[p1]));
-        if (length < kMAXLENGTH) {
-            alive[cin] = 0;
-            alive[cout] = 0;
-            list.push_back(HConn{n1, n2, list[cin].dom, list[cin].desc});
-            alive.push_back(1);
-            outC[n1] = (int)list.size() - 1;
-            inC[n2] = (int)list.size() - 1;
-            inC.erase(id);
-            outC.erase(id);
-            removed[i] = 1;
-            any = true;
-        }
-    }
-    if (!any) return false;
-    std::vector<HConn> conns;
-    for (size_t c = 0; c < list.size(); ++c)
-        if (alive[c]) conns.push_back(list[c]);
-    h.conns.swap(conns);
-    size_t w = 0;
-    for (size_t i = 0; i < h.ids.size(); ++i) {
-        if (removed[i]) continue;
-        h.ids[w] = h.ids[i];
-        hm.x[w] = hm.x[i]; hm.y[w] = hm.y[i]; hm.ox[w] = hm.ox[i]; hm.oy[w] = hm.oy[i];
-        hm.vx[w] = hm.vx[i]; hm.vy[w] = hm.vy[i]; hm.fx[w] = hm.fx[i]; hm.fy[w] = hm.fy[i];
-        ++w;
-    }
-    h.ids.resize(w);
-    hm.x.resize(w); hm.y.resize(w); hm.ox.resize(w); hm.oy.resize(w);
-    hm.vx.resize(w); hm.vy.resize(w); hm.fx.resize(w); hm.fy.resize(w);
-    return true;
-}
-
 // ---------------------------------------------------------------------------
 // Stage launcher
 
@@ -807,6 +759,10 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
         a.nfSpec = h.cross.nfSpec;
         a.nfU = h.cross.nfU;
         a.nfTab = h.cross.nfTab;
+        a.nfKeys = h.cross.nfKeys;
+        a.nfN = h.cross.nfN;
+        a.nfCap = h.cross.nfCap;
+        a.nfD = h.cross.nfD;
     }
     return a;
 }
@@ -841,7 +797,6 @@ template <typename Real>
 static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int parity, int fromStage,
                                cudaEvent_t evCollideA, cudaEvent_t evCollideB) {
     cudaStream_t s = h.stream;
-    Real* fcur = (Real*)h.f[1 - parity];
     Real* gcur = (Real*)h.g[1 - parity];
     const bool hasM = h.m.Mcap > 0;
     const unsigned it = 0;  // kernels read the iteration from the status word
@@ -865,7 +820,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
             launch_stream_collide32(a, s);
         }
         if (evCollideB) cudaEventRecord(evCollideB, s);
-        nl += 1;
+        nl += 1 + (h.cross.nfTab != nullptr ? 2 : 0);
     }
     if (fromStage <= ST_INTERP_MOVE) {
         launch_interp_move<Real>(h.m, (const Real*)h.u, h.nx, h.ny, h.L, h.cross, h.st, it, s);

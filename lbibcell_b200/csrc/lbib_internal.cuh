@@ -185,6 +185,10 @@ struct LatticeArgs {
     const uint8_t* nfSpec;     // 4*L: descriptor index + 1 per (node, slot E,N,W,S), 0 none
     const double* nfU;         // 8*L: the boundary node's velocity per (node, slot)
     const NfSpec* nfTab;
+    const uint32_t* nfKeys;    // the (node, slot) keys set in nfSpec
+    const int* nfN;            // number of nfKeys
+    int nfCap;
+    double* nfD;               // 2 per key: preAdvect's value of each solver
 };
 
 constexpr int kTile = 16;  // force tiles are 16x16 lattice nodes
