@@ -98,7 +98,10 @@ def test_toy_two_species_fp64(lbib, oracle_mod, tmp_path):
 
 
 def _digest(a):
-    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    a = np.ascontiguousarray(a)
+    if a.dtype.kind == "f" and np.isnan(a).any():
+        a = np.where(np.isnan(a), np.nan, a)  # one canonical NaN (x86 and CUDA differ in the sign bit)
+    return hashlib.sha256(a.tobytes()).hexdigest()
 
 
 def test_config1_fp64_matches_reference_digests(lbib, tmp_path):
@@ -112,6 +115,27 @@ def test_config1_fp64_matches_reference_digests(lbib, tmp_path):
         prev = t
         lat = sim.lattice()
         ids, node = sim.membrane()
+        got = {"f": lat.f, "g": lat.g, "vel": lat.vel, "force": lat.force, "dom": lat.dom, "ctype": lat.ctype,
+               "ids": ids, "node": node, "conn": sim.connections()}
+        for k, v in got.items():
+            assert _digest(v) == dig[str(t)][k], (t, k)
+
+
+def test_tissue1024_fp64_matches_reference_digests(lbib, tmp_path):
+    """The benchmark workload at full size (1024x1024, 400 cells, 2 species):
+    every array identical to the reference build's at t = 0, 70, 80, including
+    the NaN that the reference's species re-initialisation produces between 70
+    and 80 for a node trapped between two touching membranes."""
+    dig = json.load(open(os.path.join(GOLD, "tissue1024_digest.json")))
+    sim = lbib.Simulation(configs.config2(iterations=80, report_step=10).write(str(tmp_path)), lbib.FP64)
+    prev = 0
+    for t in (0, 70, 80):
+        sim.step(t - prev)
+        prev = t
+        lat = sim.lattice()
+        ids, node = sim.membrane()
+        assert ids.shape[0] == dig[str(t)]["M"]
+        assert int((~np.isfinite(lat.g)).sum()) == dig[str(t)]["nonfinite_g"]
         got = {"f": lat.f, "g": lat.g, "vel": lat.vel, "force": lat.force, "dom": lat.dom, "ctype": lat.ctype,
                "ids": ids, "node": node, "conn": sim.connections()}
         for k, v in got.items():
