@@ -22,6 +22,7 @@ UNITS = [
     ("k_lattice64.cu", ["--fmad=false"]),
     ("k_membrane.cu", ["--fmad=false"]),
     ("k_topology.cu", ["--fmad=false"]),
+    ("k_forces.cu", ["--fmad=false"]),
     ("lbib_host.cu", ["--fmad=false"]),
     ("k_lattice32.cu", []),
     ("k_adjoint.cu", []),

@@ -70,6 +70,10 @@ class Config:
     # boundary solvers on every connection: (bsolver, cdesolver) pairs, as the
     # reference's geometry files list them (apps/config/tutorial_02_geometry.txt)
     boundary: List[Tuple[str, str]] = field(default_factory=list)
+    # further bio solvers by name (e.g. "tutorial_01_BioSolverCellJunction"),
+    # registered before (bio_first) or after the area regulator and tension
+    bio: List[str] = field(default_factory=list)
+    bio_first: bool = False
 
     @property
     def lattice_nodes(self) -> int:
@@ -119,12 +123,18 @@ class Config:
             f.write("#lbibcell_b200 plugin file\n")
             if self.outlet:
                 f.write("MassSolver\tMassSolverBoxOutlet\n")
+            if self.bio_first:
+                for name in self.bio:
+                    f.write(f"BioSolver\t{name}\n")
             if self.area is not None:
                 fa, st, mx = self.area
                 f.write(f"BioSolver\tLbibAreaRegulator\tfactor\t{fa!r}\tstrength\t{st!r}\tmaxsource\t{mx!r}\n")
             if self.tension is not None:
                 fo, fr = self.tension
                 f.write(f"BioSolver\tLbibMembraneTension\tforce\t{fo!r}\tfrequency\t{fr}\n")
+            if not self.bio_first:
+                for name in self.bio:
+                    f.write(f"BioSolver\t{name}\n")
             for s in self.species:
                 f.write(f"CDE\t{s.name}\tinit\t{s.init!r}\tdecay\t{s.decay!r}\n")
                 if s.source:
@@ -139,6 +149,20 @@ def circle(cx: float, cy: float, r: float, n: int, phase: float = 0.0) -> np.nda
     """n vertices at uniform angle, counter-clockwise."""
     t = phase + 2.0 * math.pi * np.arange(n) / n
     return np.stack([cx + r * np.cos(t), cy + r * np.sin(t)], axis=1)
+
+
+def junction_quad(iterations: int = 60, report_step: int = 30, tension: Tuple[float, int] = (0.1, 10),
+                  bio_first: bool = False, name: str = "tutorial_01_BioSolverCellJunction") -> Config:
+    """Four cells of radius 19.6 on a 40 lu square grid in a 124x124 lattice:
+    neighbouring membranes 0.8 lu apart, within the junction radius (1 lu) of
+    the cell-junction solver, which is registered with them."""
+    cells = []
+    for k, (cx, cy) in enumerate([(42.0, 42.0), (82.0, 42.0), (42.0, 82.0), (82.0, 82.0)]):
+        cells.append((k + 1, circle(cx, cy, 19.6, 240, phase=0.1 * (k + 1))))
+    return Config(name="junction_quad", nx=124, ny=124, tau_fluid=1.0, iterations=iterations,
+                  report_step=report_step, cells=cells,
+                  species=[Species(SPECIES_NAMES[0], 1.0, source={1: 1e-3, 4: 1e-3})],
+                  tension=tension, bio=[name], bio_first=bio_first)
 
 
 def config1(iterations: int = 2000, report_step: int = 500) -> Config:

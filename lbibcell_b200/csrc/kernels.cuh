@@ -44,6 +44,26 @@ struct MembraneDev {
     uint32_t* ringDom;          // domain of each ring
 };
 
+// Scratch of the device force-list edits and of the cell-junction search.
+enum ForceGen { GEN_TENSION = 1, GEN_JUNCTION = 2 };
+// Force-list operations of one bio solver in one step (2 bits per solver).
+enum BioOp { BIO_NONE = 0, BIO_TENSION_FILL = 1, BIO_TENSION_EDIT = 2, BIO_JUNCTIONS = 3 };
+struct ForceScratch {
+    int Fcap;                   // capacity of the force records
+    int* foffS;                 // Mcap+1: offsets before the edit
+    int* ftypeS; int* fpartnerS; double* fparS;  // Fcap: records before the edit
+    int* cnt;                   // Mcap+1: records per node after the edit
+    void* scanTmp; size_t scanTmpBytes;
+    int* outPos; int* inPos;    // Mcap: a node's outgoing / incoming connection
+    // cell junctions
+    unsigned* binKey; unsigned* binKeySorted;  // Mcap: cell-list bin of each node
+    int* binIdx; int* binIdxSorted;            // Mcap: node index
+    void* sortTmp; size_t sortTmpBytes;
+    int* closest;               // Mcap: closest node of another cell within the radius, -1: none
+    int* inCnt; int* inOff;     // Mcap+1: nodes that found node i, and their offsets
+    int* inList; int* inFill;   // Mcap
+};
+
 // Crossing resolution buffers (dense per lattice node and slot E,N,W,S).
 struct CrossDev {
     unsigned long long* bnDist;  // 4*L, EMPTY = ~0ull
@@ -151,6 +171,14 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 void launch_remesh_check(Status* st, unsigned iteration, cudaStream_t s);
 void launch_coarsen_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
 void launch_clear_forces(MembraneDev& m, cudaStream_t s);
+// ForceSolver::deleteForceType(6) + the membrane-tension records, on a list that
+// holds other forces too (launches returned).
+int launch_tension_edit(MembraneDev& m, ForceScratch& fs, double force, Status* st, cudaStream_t s);
+// The cell-junction bio solver (launches returned).
+int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double radius, double K, double L0,
+                     Status* st, cudaStream_t s);
+size_t force_scan_bytes(int n);
+size_t junction_sort_bytes(int n);
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s);
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s);

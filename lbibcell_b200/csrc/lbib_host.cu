@@ -123,9 +123,11 @@ struct Handle {
     unsigned iteration = 0, iterations = 0, reportStep = 1;
     std::vector<Species> sp;
     bool outlet = false;
-    std::vector<int> bio;  // 1 tension, 2 area regulator
+    std::vector<int> bio;  // 1 tension, 2 area regulator, 3 cell junctions
     double tensionForce = 0.01;
     unsigned tensionFreq = 10;
+    // tutorial_01_BioSolverCellJunction.cpp:37-41
+    double junctionRadius = 1.0, junctionK = 0.02, junctionL0 = 0.5;
     double areaFactor = 1.2, areaStrength = 0.01, areaMax = 0.004;
 
     // lattice buffers
@@ -146,7 +148,14 @@ struct Handle {
     std::vector<uint32_t> ids;
     std::vector<HConn> conns;
     std::map<uint32_t, std::vector<HForce>> forcemap;
-    bool forcesPure = true;  // device force list = tension pairs from the last renewal (or empty)
+    // The force list as loaded (from the force file or a restart) holds no
+    // records: until the first deleteAllForces, tension renewals may rebuild it
+    // whole.  forceListIt: the iteration of the first step on that list.
+    bool forcesPureAtLoad = true;
+    unsigned forceListIt = 0;
+    ForceScratch fs{};
+    int fsMcap = 0, fsFcap = 0;  // capacities the scratch was allocated for
+    int keepRecords = 0;         // force records the host re-uploads after a topology upload
     MembraneDev m{};
     int Mcap = 0, Ccap = 0, Fcap = 0, cellCap = 0;
     int* outPos = nullptr;
@@ -172,13 +181,13 @@ struct Handle {
 
     long long hostEvents = 0;
     long long launches = 0;
-    // CUDA graphs of one step, keyed by (buffer parity, coarsening step,
-    // tension renewal); rebuilt when a buffer is reallocated
+    // CUDA graphs of one step, keyed by (buffer parity, coarsening step, bio
+    // solvers' force-list operations); rebuilt when a buffer is reallocated
     struct StepGraph {
         cudaGraphExec_t exec = nullptr;
         long long launches = 0;
     };
-    StepGraph graphs[8];
+    std::map<int, StepGraph> graphs;
     bool useGraphs = true;
     long long graphEpoch = 0, graphBuiltEpoch = 0;  // kernels launched by the last lbib_step / lbib_lattice_step
     long long stepsDone = 0;
@@ -226,8 +235,11 @@ Handle::~Handle() {
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
     for (auto e : kEvents) cudaEventDestroy(e);
-    for (auto& g : graphs)
-        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& kv : graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
+    fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
+    fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -294,12 +306,19 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 if (kv.count("force")) h.tensionForce = kv["force"];
                 if (kv.count("frequency")) h.tensionFreq = (unsigned)kv["frequency"];
                 if (h.tensionFreq == 0) fail(ERR_INPUT, "tension frequency must be positive");
+            } else if (name == "tutorial_01_BioSolverCellJunction" || name == "tutorial_02_BioSolverCellJunction" ||
+                       name == "BioSolverCellJunction") {
+                h.bio.push_back(3);
+                if (kv.count("radius")) h.junctionRadius = kv["radius"];
+                if (kv.count("k")) h.junctionK = kv["k"];
+                if (kv.count("l0")) h.junctionL0 = kv["l0"];
             } else if (name == "LbibAreaRegulator") {
                 h.bio.push_back(2);
                 if (kv.count("factor")) h.areaFactor = kv["factor"];
                 if (kv.count("strength")) h.areaStrength = kv["strength"];
                 if (kv.count("maxsource")) h.areaMax = kv["maxsource"];
             } else fail(ERR_INPUT, "unknown bio solver " + name);
+            if (h.bio.size() > 8) fail(ERR_INPUT, "more than 8 bio solvers");
         } else if (kind == "CDE") {
             std::string k; double v;
             while (ls >> k >> v) kv[k] = v;
@@ -315,6 +334,10 @@ static void load_plugins(Handle& h, const std::string& fn) {
                     if (s.name == name) s.source[d] = r;
         } else fail(ERR_INPUT, "unknown plugin line " + kind);
     }
+}
+
+static bool has_junctions(const Handle& h) {
+    return std::find(h.bio.begin(), h.bio.end(), 3) != h.bio.end();
 }
 
 // ForceSolver::addForce text format (ForceSolver.cpp:107-139; ForceStructs.hpp).
@@ -428,7 +451,9 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
             if (!kv.second.empty() && !index.count(kv.first)) fail(ERR_FORCE_NODE, "Could not compute and set the forces.", kv.first);
     }
     ensure_capacity(h, M, C, 1, cells);
-    const int F = std::max((int)ftype.size(), 2 * h.Mcap);
+    // room for the loaded records plus the bio solvers' own: two tension records
+    // per node, and with junctions up to two springs per node
+    const int F = std::max((int)ftype.size(), h.keepRecords) + (has_junctions(h) ? 4 : 2) * h.Mcap;
     ensure_capacity(h, M, C, F, cells);
     h.m.M = M;
     h.m.C = C;
@@ -521,6 +546,45 @@ static void sync_targets(Handle& h) {
     CK(cudaStreamSynchronize(h.stream));
 }
 
+// Scratch of the device force-list edits (membrane tension on a list with other
+// forces, cell junctions), sized for the node and record capacities.
+static void ensure_force_scratch(Handle& h) {
+    const bool tension = std::find(h.bio.begin(), h.bio.end(), 1) != h.bio.end();
+    const bool junction = has_junctions(h);
+    h.fs.outPos = h.outPos;
+    h.fs.inPos = h.inPos;
+    if (!(tension || junction) || (h.fsMcap == h.Mcap && h.fsFcap == h.Fcap)) return;
+    auto fr = [](void* p) { if (p) cudaFree(p); };
+    ForceScratch& fs = h.fs;
+    fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
+    fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
+    fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
+    fs = ForceScratch{};
+    fs.outPos = h.outPos;
+    fs.inPos = h.inPos;
+    const int n = h.Mcap;
+    fs.Fcap = h.Fcap;
+    fs.foffS = dalloc<int>(n + 1);
+    fs.cnt = dalloc<int>(n + 1);
+    fs.ftypeS = dalloc<int>(h.Fcap);
+    fs.fpartnerS = dalloc<int>(h.Fcap);
+    fs.fparS = dalloc<double>(4 * (size_t)h.Fcap);
+    fs.scanTmpBytes = force_scan_bytes(n + 1);
+    CK(cudaMalloc(&fs.scanTmp, fs.scanTmpBytes));
+    if (junction) {
+        fs.binKey = dalloc<unsigned>(n); fs.binKeySorted = dalloc<unsigned>(n);
+        fs.binIdx = dalloc<int>(n); fs.binIdxSorted = dalloc<int>(n);
+        fs.sortTmpBytes = junction_sort_bytes(n);
+        CK(cudaMalloc(&fs.sortTmp, fs.sortTmpBytes));
+        fs.closest = dalloc<int>(n);
+        fs.inCnt = dalloc<int>(n + 1); fs.inOff = dalloc<int>(n + 1);
+        fs.inList = dalloc<int>(n); fs.inFill = dalloc<int>(n);
+    }
+    h.fsMcap = h.Mcap;
+    h.fsFcap = h.Fcap;
+    h.graphEpoch++;
+}
+
 static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     // headroom for remeshing on the device: node and connection buffers hold
     // twice the current counts before the host has to grow them
@@ -530,7 +594,6 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.graphEpoch++;
         return true;
     };
-    int oldM = h.Mcap;
     if (grow(M, h.Mcap)) {
         // membrane arrays are rewritten by every upload_topology; no copy needed
         auto fr = [](void* p) { if (p) cudaFree(p); };
@@ -560,10 +623,6 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.m.ringNode = dalloc<int>(n);
         h.tiles.cap = 4 * n;
         h.tiles.list = dalloc<int>(h.tiles.cap);
-        // the force records survive a growth only when the force list is rebuilt
-        if (oldM > 0 && h.forcesPure) {
-            // re-create the empty/pure state: offsets are re-filled by the caller
-        }
     }
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
@@ -616,6 +675,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.td.cellCount = dalloc<int>(h.cellCap + 1); h.td.cellStart = dalloc<int>(h.cellCap + 1);
         h.td.cellFill = dalloc<int>(h.cellCap); h.td.startNode = dalloc<int>(h.cellCap);
     }
+    ensure_force_scratch(h);
     // scan scratch for the largest scan (nodes, connections or cells)
     const size_t need = topo_scan_bytes(std::max(std::max(h.Mcap, h.Ccap), h.cellCap) + 1);
     if (need > h.td.scanTmpBytes) {
@@ -790,11 +850,11 @@ __global__ void iteration_inc_kernel(Status* st) {
     pdl_wait(); st->iteration += 1; }
 
 // Launches the stage kernels of one step from `fromStage` on.  `coarsenStep`
-// (Parameters' iteration % 10 == 0) and `renewal` (the tension plugin's
-// frequency) are the only host decisions; everything else reads device state.
-// Returns the number of kernels launched.
+// (Parameters' iteration % 10 == 0) and `bioOps` (which bio solvers change the
+// force list, step_bio_ops) are the only host decisions; everything else reads
+// device state.  Returns the number of kernels launched.
 template <typename Real>
-static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int parity, int fromStage,
+static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int parity, int fromStage,
                                cudaEvent_t evCollideA, cudaEvent_t evCollideB) {
     cudaStream_t s = h.stream;
     Real* gcur = (Real*)h.g[1 - parity];
@@ -858,7 +918,8 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
         // rings are re-ranked after any topology change; FP32-shifted runs sum
         // in exact fixed point and need no ring order here
         if (sizeof(Real) == 8) nl += launch_rings(h.m, h.td, h.st, s);
-        for (int b : h.bio) {
+        for (size_t q = 0; q < h.bio.size(); ++q) {
+            const int b = h.bio[q], op = (bioOps >> (2 * q)) & 3;
             if (b == 2) {
                 if (sizeof(Real) == 8) {
                     launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor,
@@ -869,9 +930,13 @@ static long long launch_stages(Handle& h, bool coarsenStep, bool renewal, int pa
                                                 h.nDomains, h.areaFactor, h.areaStrength, h.areaMax, h.st, s);
                     nl += h.m.nCells > 0 ? 3 : 0;
                 }
-            } else if (b == 1 && renewal) {
+            } else if (b == 1 && op == BIO_TENSION_FILL) {
                 launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
                 nl += hasM ? 2 : 0;
+            } else if (b == 1 && op == BIO_TENSION_EDIT) {
+                nl += launch_tension_edit(h.m, h.fs, h.tensionForce, h.st, s);
+            } else if (b == 3 && op == BIO_JUNCTIONS) {
+                nl += launch_junctions(h.m, h.fs, h.nx, h.ny, h.junctionRadius, h.junctionK, h.junctionL0, h.st, s);
             }
         }
     }
@@ -907,21 +972,40 @@ static void reset_status(Handle& h, unsigned it, bool cellTypesCopied) {
     write_status(h);
 }
 
-// Bookkeeping the host does for a step it launches (the force list's state).
+// Bookkeeping the host does for a step it launches: the loaded force list is
+// gone after the step's ForceSolver::deleteAllForces.
 static void host_step_bookkeeping(Handle& h, unsigned iteration) {
-    if (iteration % 10 == 0) {
-        h.forcemap.clear();
-        h.forcesPure = true;
-    }
-    for (int b : h.bio)
-        if (b == 1 && iteration % h.tensionFreq == 0 && !h.forcesPure)
-            fail(ERR_STATE, "tension renewal on a non-tension force list is not supported on the device");
+    if (iteration % 10 == 0) h.forcemap.clear();
 }
 
-static bool renewal_step(const Handle& h, unsigned it) {
-    for (int b : h.bio)
-        if (b == 1 && it % h.tensionFreq == 0) return true;
-    return false;
+// What the bio solvers of step `it` do to the force list, 2 bits per solver in
+// registration order (SimulationRunner::applyBioSolvers):
+//   BIO_TENSION_FILL  the membrane-tension renewal on a list of tension records
+//                     only (or none): the list is rebuilt whole;
+//   BIO_TENSION_EDIT  the same renewal on a list that holds other forces:
+//                     deleteForceType(6), then the new records appended;
+//   BIO_JUNCTIONS     the cell-junction solver (every 10th iteration).
+// Before the bio stage, the list holds only tension records when the step's
+// own coarsening stage cleared it (iteration % 10 == 0), or when it was
+// cleared at an earlier multiple of 10 and no junction solver added springs,
+// or, before any clearing, when it was loaded empty.
+static int step_bio_ops(const Handle& h, unsigned it) {
+    bool pure;
+    if (it % 10 == 0) pure = true;
+    else if (it - it % 10 >= h.forceListIt) pure = !has_junctions(h);
+    else pure = h.forcesPureAtLoad;
+    int ops = 0;
+    for (size_t q = 0; q < h.bio.size(); ++q) {
+        int op = 0;
+        if (h.bio[q] == 1 && it % h.tensionFreq == 0) {
+            op = pure ? BIO_TENSION_FILL : BIO_TENSION_EDIT;
+        } else if (h.bio[q] == 3 && it % 10 == 0) {
+            op = BIO_JUNCTIONS;
+            pure = false;
+        }
+        ops |= op << (2 * q);
+    }
+    return ops;
 }
 
 // The host side of a halted stage, in the reference's order.
@@ -963,7 +1047,9 @@ static void handle_halt(Handle& h, int stage) {
             CK(cudaStreamSynchronize(h.stream));
         }
         remesh(h, hm);
+        h.keepRecords = nrec;
         upload_topology(h, hm, false);
+        h.keepRecords = 0;
         foff.resize(h.m.M + 1, nrec);
         CK(cudaMemcpyAsync(h.m.foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h.stream));
         if (nrec) {
@@ -982,18 +1068,18 @@ static void handle_halt(Handle& h, int stage) {
 }
 
 template <typename Real>
-static void launch_step_graph(Handle& h, int parity, bool coarsenStep, bool renewal) {
-    const int key = parity * 4 + (coarsenStep ? 2 : 0) + (renewal ? 1 : 0);
+static void launch_step_graph(Handle& h, int parity, bool coarsenStep, int bioOps) {
+    const int key = (bioOps << 2) | (coarsenStep ? 2 : 0) | parity;
     if (h.graphEpoch != h.graphBuiltEpoch) {
-        for (auto& g : h.graphs)
-            if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+        for (auto& kv : h.graphs)
+            if (kv.second.exec) { cudaGraphExecDestroy(kv.second.exec); kv.second.exec = nullptr; }
         h.graphBuiltEpoch = h.graphEpoch;
     }
     Handle::StepGraph& g = h.graphs[key];
     if (!g.exec) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
-        g.launches = launch_stages<Real>(h, coarsenStep, renewal, parity, ST_FORCE, nullptr, nullptr);
+        g.launches = launch_stages<Real>(h, coarsenStep, bioOps, parity, ST_FORCE, nullptr, nullptr);
         CK(cudaStreamEndCapture(h.stream, &graph));
         CK(cudaGraphInstantiate(&g.exec, graph, 0));
         CK(cudaGraphDestroy(graph));
@@ -1019,11 +1105,11 @@ static void run_steps(Handle& h, int n) {
             host_step_bookkeeping(h, it);
             const int parity = (h.cur + b) & 1;
             if (prof || !h.useGraphs)
-                h.launches += launch_stages<Real>(h, it % 10 == 0, renewal_step(h, it), parity, ST_FORCE,
+                h.launches += launch_stages<Real>(h, it % 10 == 0, step_bio_ops(h, it), parity, ST_FORCE,
                                                   prof ? h.kEvents[2 * b] : nullptr,
                                                   prof ? h.kEvents[2 * b + 1] : nullptr);
             else
-                launch_step_graph<Real>(h, parity, it % 10 == 0, renewal_step(h, it));
+                launch_step_graph<Real>(h, parity, it % 10 == 0, step_bio_ops(h, it));
         }
         CK(cudaGetLastError());
         read_status(h);
@@ -1060,7 +1146,7 @@ static void run_steps(Handle& h, int n) {
             const int from = resume_stage(stage);
             if (from < 0) fail(ERR_STATE, "unexpected halt stage");
             reset_status(h, it, h.cellTypesCopied);
-            h.launches += launch_stages<Real>(h, it % 10 == 0, renewal_step(h, it), h.cur, from, nullptr, nullptr);
+            h.launches += launch_stages<Real>(h, it % 10 == 0, step_bio_ops(h, it), h.cur, from, nullptr, nullptr);
             read_status(h);
             if (h.stHost->err) {
                 h.err = h.stHost->err;
@@ -1203,7 +1289,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
             add_force_line(h, line);
         }
     }
-    h.forcesPure = h.forcemap.empty();
+    h.forcesPureAtLoad = h.forcemap.empty();
+    h.forceListIt = h.iteration;
 
     upload_topology(h, hm, false);
     {
