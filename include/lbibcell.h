@@ -193,6 +193,45 @@ int lbib_diff_backward(lbib_handle* h, const double* dLdC, double* gForce, doubl
  * force planes) and frees the run's device memory. */
 int lbib_diff_end(lbib_handle* h);
 
+/* ForceSolver::addForce for n records at once (ForceSolver.cpp:107-139), in
+ * place of one text line each.  Record k has type[k] (0-7, ForceStructs.hpp),
+ * node id1[k], for types 0, 5, 6, 7 the partner node id2[k] (id2 may be NULL
+ * when no record needs one) and four parameters par[4k..4k+3]:
+ *   0, 7  k, l0            1  x, y, k, l0      2  fx, fy
+ *   3, 4  position, k, l0  5, 6  f             (unused ones are ignored)
+ * Each node's new records follow its existing ones in call order, as
+ * forcemap_[id1].push_back does.  An unknown node id fails with
+ * LBIB_ERR_FORCE_NODE (the reference fails when the force is next evaluated,
+ * ForceStructs.hpp "Could not compute and set the forces.").  The records stay
+ * until a deleteForceType of their type or the deleteAllForces of every 10th
+ * iteration (SimulationRunner.cpp:84-87), as in the reference. */
+int lbib_add_forces(lbib_handle* h, const int* type, const unsigned* id1, const unsigned* id2, const double* par,
+                    int n);
+
+/* ForceSolver::deleteForceType (ForceSolver.cpp:183-215): removes every record
+ * of that type, keeping the others in order. */
+int lbib_delete_force_type(lbib_handle* h, int type);
+
+/* ForceSolver::deleteAllForces (ForceSolver.cpp:170-181). */
+int lbib_delete_all_forces(lbib_handle* h);
+
+/* Geometry::getGeometryNodesWithinRadius (Geometry.cpp:306-323), or with
+ * avoidDomain >= 0 getGeometryNodesWithinRadiusWithAvoidance (:325-348): the
+ * ids of the membrane nodes within `radius` of (x, y) (distance <= radius),
+ * leaving out nodes whose adjacent connections carry domain avoidDomain, in
+ * the order of the reference's cell list (1-lu bins by row, then column,
+ * ascending id within a bin; FastNeighborList.hpp:400-444, 494-520).  Writes
+ * up to cap ids; returns the number of hits, or a negated LBIB_ERR_* code. */
+int lbib_nodes_within_radius(lbib_handle* h, double x, double y, double radius, long long avoidDomain,
+                             unsigned* ids, int cap);
+
+/* Geometry::getGeometryNodesWithinRadiusWithAvoidanceClosest
+ * (Geometry.cpp:350-374) for n query points at once: closest[q] = the id of the
+ * first hit of smallest distance in the order above, or -1 when none.
+ * avoidDomain may be NULL (no domain left out) or hold one domain per query. */
+int lbib_closest_nodes(lbib_handle* h, const double* x, const double* y, const long long* avoidDomain, int n,
+                       double radius, long long* closest);
+
 /* Last error: code; message into buf; index of the node/connection involved. */
 int lbib_last_error(lbib_handle* h, char* buf, int len, long long* index);
 

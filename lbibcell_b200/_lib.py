@@ -17,7 +17,8 @@ SYMBOLS = (
     "lbib_download_lattice", "lbib_upload_lattice", "lbib_download_membrane", "lbib_download_connections",
     "lbib_areas", "lbib_areas_static", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
     "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
-    "lbib_write_simulation", "lbib_load_solvers",
+    "lbib_write_simulation", "lbib_load_solvers", "lbib_add_forces", "lbib_delete_force_type",
+    "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes",
 )
 
 _lib = None
@@ -85,5 +86,16 @@ def load() -> ctypes.CDLL:
     L.lbib_write_simulation.argtypes = [vp, cp, cp, cp, cp]
     L.lbib_load_solvers.restype = ip
     L.lbib_load_solvers.argtypes = [vp, cp]
+    L.lbib_add_forces.restype = ip
+    L.lbib_add_forces.argtypes = [vp, vp, vp, vp, vp, ip]
+    L.lbib_delete_force_type.restype = ip
+    L.lbib_delete_force_type.argtypes = [vp, ip]
+    L.lbib_delete_all_forces.restype = ip
+    L.lbib_delete_all_forces.argtypes = [vp]
+    L.lbib_nodes_within_radius.restype = ip
+    L.lbib_nodes_within_radius.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_longlong, vp, ip]
+    L.lbib_closest_nodes.restype = ip
+    L.lbib_closest_nodes.argtypes = [vp, vp, vp, vp, ip, ctypes.c_double, vp]
     _lib = L
     return L

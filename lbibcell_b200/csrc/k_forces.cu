@@ -46,7 +46,9 @@ __global__ void force_snapshot_kernel(MembraneDev m, ForceScratch fs, Status* st
 
 // Records of node i after the edit: the kept ones plus the generated ones.
 __device__ __forceinline__ int gen_count(const ForceScratch& fs, int gen, int i) {
+    if (gen == GEN_NONE) return 0;
     if (gen == GEN_TENSION) return 2;
+    if (gen == GEN_LIST) return fs.listOff[i + 1] - fs.listOff[i];
     return (fs.closest[i] >= 0 ? 1 : 0) + fs.inCnt[i];
 }
 
@@ -101,6 +103,16 @@ __global__ void force_fill_kernel(MembraneDev m, ForceScratch fs, int delType, i
 #pragma unroll
         for (int q = 0; q < 4; ++q) m.fpar[4 * (size_t)o + q] = fs.fparS[4 * (size_t)r + q];
         ++o;
+    }
+    if (gen == GEN_NONE) return;
+    if (gen == GEN_LIST) {
+        for (int r = fs.listOff[i]; r < fs.listOff[i + 1]; ++r, ++o) {
+            m.ftype[o] = fs.listType[r];
+            m.fpartner[o] = fs.listPartner[r];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) m.fpar[4 * (size_t)o + q] = fs.listPar[4 * (size_t)r + q];
+        }
+        return;
     }
     if (gen == GEN_TENSION) {
         const int out = fs.outPos[i], in = fs.inPos[i];
@@ -258,14 +270,70 @@ __global__ void junction_infill_kernel(MembraneDev m, ForceScratch fs, Status* s
     if (c >= 0) fs.inList[fs.inOff[c] + atomicAdd(&fs.inFill[c], 1)] = i;
 }
 
-int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double radius, double K, double L0,
-                     Status* st, cudaStream_t s) {
+int launch_cell_list(MembraneDev& m, ForceScratch& fs, int nx, int ny, cudaStream_t s) {
     if (m.Mcap == 0) return 0;
     const int n = m.Mcap;
     launch_pdl(conn_pos_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, fs);
     launch_pdl(junction_bin_kernel, (n + 255) / 256, 256, 0, s, m, fs, nx, ny);
     cub::DeviceRadixSort::SortPairs(fs.sortTmp, fs.sortTmpBytes, fs.binKey, fs.binKeySorted, fs.binIdx,
                                     fs.binIdxSorted, n, 0, 32, s);
+    return 2;
+}
+
+// Range queries for host plugins, on the cell list of launch_cell_list: hits in
+// the cell list's order (bins by row, then column, id order within a bin);
+// distance > radius drops a node (FastNeighborList.hpp:400-421), and with
+// avoid >= 0 so does a node whose getDomainIdOfAdjacentConnections equals it
+// (:425-444); the closest is the first hit of the smallest distance (:447-465).
+// One thread per query point.
+__global__ void range_query_kernel(MembraneDev m, ForceScratch fs, int nx, int ny, const double* qx,
+                                   const double* qy, const long long* avoid, int nq, double radius, int mode,
+                                   unsigned* ids, int cap, int* count, long long* closest) {
+    pdl_wait();
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const double x = qx[q], y = qy[q];
+    const long long av = avoid != nullptr ? avoid[q] : -1;
+    const int bx0 = bin_index(x - radius, nx), bx1 = bin_index(x + radius, nx);
+    const int by0 = bin_index(y - radius, ny), by1 = bin_index(y + radius, ny);
+    int n = 0, best = -1;
+    double bestD = 0.0;
+    for (int by = by0; by <= by1; ++by)
+        for (int bx = bx0; bx <= bx1; ++bx) {
+            const unsigned key = (unsigned)by * (unsigned)nx + (unsigned)bx;
+            for (int p = lower_bound_key(fs.binKeySorted, m.Mcap, key); p < m.Mcap && fs.binKeySorted[p] == key;
+                 ++p) {
+                const int j = fs.binIdxSorted[p];
+                const double xj = m.x[j], yj = m.y[j];
+                const double d = sqrt((xj - x) * (xj - x) + (yj - y) * (yj - y));
+                if (d > radius) continue;
+                if (av >= 0 && (long long)m.cdom[fs.inPos[j]] == av) continue;
+                if (mode == 0) {
+                    if (n < cap) ids[n] = m.id[j];
+                    ++n;
+                } else if (best < 0 || d < bestD) {
+                    best = j;
+                    bestD = d;
+                }
+            }
+        }
+    if (mode == 0) *count = n;
+    else closest[q] = best < 0 ? -1 : (long long)m.id[best];
+}
+
+void launch_range_query(MembraneDev& m, ForceScratch& fs, int nx, int ny, const double* qx, const double* qy,
+                        const long long* avoid, int nq, double radius, int mode, unsigned* ids, int cap, int* count,
+                        long long* closest, cudaStream_t s) {
+    if (nq <= 0) return;
+    launch_pdl(range_query_kernel, (nq + 127) / 128, 128, 0, s, m, fs, nx, ny, qx, qy, avoid, nq, radius, mode, ids,
+               cap, count, closest);
+}
+
+int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double radius, double K, double L0,
+                     Status* st, cudaStream_t s) {
+    if (m.Mcap == 0) return 0;
+    const int n = m.Mcap;
+    launch_cell_list(m, fs, nx, ny, s);
     launch_pdl(junction_query_kernel, (n + 127) / 128, 128, 0, s, m, fs, nx, ny, radius, st);
     cudaMemsetAsync(fs.inCnt, 0, sizeof(int) * (n + 1), s);
     cudaMemsetAsync(fs.inFill, 0, sizeof(int) * n, s);

@@ -45,7 +45,7 @@ struct MembraneDev {
 };
 
 // Scratch of the device force-list edits and of the cell-junction search.
-enum ForceGen { GEN_TENSION = 1, GEN_JUNCTION = 2 };
+enum ForceGen { GEN_NONE = 0, GEN_TENSION = 1, GEN_JUNCTION = 2, GEN_LIST = 3 };
 // Force-list operations of one bio solver in one step (2 bits per solver).
 enum BioOp { BIO_NONE = 0, BIO_TENSION_FILL = 1, BIO_TENSION_EDIT = 2, BIO_JUNCTIONS = 3 };
 struct ForceScratch {
@@ -62,6 +62,9 @@ struct ForceScratch {
     int* closest;               // Mcap: closest node of another cell within the radius, -1: none
     int* inCnt; int* inOff;     // Mcap+1: nodes that found node i, and their offsets
     int* inList; int* inFill;   // Mcap
+    // records added through the C ABI: CSR by node (Mcap+1 offsets), in call order
+    int* listOff; int* listType; int* listPartner; double* listPar;
+    int listCap;
 };
 
 // Crossing resolution buffers (dense per lattice node and slot E,N,W,S).
@@ -178,6 +181,19 @@ int launch_tension_edit(MembraneDev& m, ForceScratch& fs, double force, Status* 
 int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double radius, double K, double L0,
                      Status* st, cudaStream_t s);
 size_t force_scan_bytes(int n);
+// ForceSolver::deleteForceType(delType) (delType < 0: none) followed by the
+// records of `gen` (GEN_NONE, GEN_LIST) appended per node (launches returned).
+int launch_force_edit(MembraneDev& m, ForceScratch& fs, int delType, int gen, double tensionForce, double K,
+                      double L0, Status* st, cudaStream_t s);
+// The cell list of the nodes (1-lu bins, id order within a bin) and each
+// node's outgoing/incoming connection, for the range queries.
+int launch_cell_list(MembraneDev& m, ForceScratch& fs, int nx, int ny, cudaStream_t s);
+// Geometry::getGeometryNodesWithinRadius[WithAvoidance][Closest] for nq query
+// points (mode 0: the ids of all hits of query 0, up to cap, count in *count;
+// mode 1: the id of the closest hit of each query, or -1, in closest[q]).
+void launch_range_query(MembraneDev& m, ForceScratch& fs, int nx, int ny, const double* qx, const double* qy,
+                        const long long* avoid, int nq, double radius, int mode, unsigned* ids, int cap, int* count,
+                        long long* closest, cudaStream_t s);
 size_t junction_sort_bytes(int n);
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s);
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,

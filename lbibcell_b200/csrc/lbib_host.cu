@@ -155,6 +155,7 @@ struct Handle {
     unsigned forceListIt = 0;
     ForceScratch fs{};
     int fsMcap = 0, fsFcap = 0;  // capacities the scratch was allocated for
+    bool fsQuery = false;        // the scratch holds the cell-list buffers
     int keepRecords = 0;         // force records the host re-uploads after a topology upload
     MembraneDev m{};
     int Mcap = 0, Ccap = 0, Fcap = 0, cellCap = 0;
@@ -548,12 +549,15 @@ static void sync_targets(Handle& h) {
 
 // Scratch of the device force-list edits (membrane tension on a list with other
 // forces, cell junctions), sized for the node and record capacities.
-static void ensure_force_scratch(Handle& h) {
+// `need`: allocate even without a tension or junction solver (the force-list and
+// range-query calls of the C ABI).
+static void ensure_force_scratch(Handle& h, bool need = false) {
     const bool tension = std::find(h.bio.begin(), h.bio.end(), 1) != h.bio.end();
-    const bool junction = has_junctions(h);
+    const bool junction = has_junctions(h) || need || h.fsQuery;
     h.fs.outPos = h.outPos;
     h.fs.inPos = h.inPos;
-    if (!(tension || junction) || (h.fsMcap == h.Mcap && h.fsFcap == h.Fcap)) return;
+    if (!(tension || junction)) return;
+    if (h.fsMcap == h.Mcap && h.fsFcap == h.Fcap && (h.fs.binKey != nullptr) == junction) return;
     auto fr = [](void* p) { if (p) cudaFree(p); };
     ForceScratch& fs = h.fs;
     fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
@@ -582,6 +586,7 @@ static void ensure_force_scratch(Handle& h) {
     }
     h.fsMcap = h.Mcap;
     h.fsFcap = h.Fcap;
+    h.fsQuery = junction;
     h.graphEpoch++;
 }
 
@@ -989,11 +994,20 @@ static void host_step_bookkeeping(Handle& h, unsigned iteration) {
 // own coarsening stage cleared it (iteration % 10 == 0), or when it was
 // cleared at an earlier multiple of 10 and no junction solver added springs,
 // or, before any clearing, when it was loaded empty.
+// The list holds only tension records (or none) at the start of step `it`:
+// after the last clearing since the list was set (a multiple of 10 in
+// [forceListIt, it - 1]) the junction solver, if registered, added springs;
+// before any clearing the list is as set.
+static bool pure_at_start(const Handle& h, unsigned it) {
+    if (it > 0) {
+        const unsigned c = (it - 1) - (it - 1) % 10;
+        if (c >= h.forceListIt) return !has_junctions(h);
+    }
+    return h.forcesPureAtLoad;
+}
+
 static int step_bio_ops(const Handle& h, unsigned it) {
-    bool pure;
-    if (it % 10 == 0) pure = true;
-    else if (it - it % 10 >= h.forceListIt) pure = !has_junctions(h);
-    else pure = h.forcesPureAtLoad;
+    bool pure = it % 10 == 0 ? true : pure_at_start(h, it);
     int ops = 0;
     for (size_t q = 0; q < h.bio.size(); ++q) {
         int op = 0;
@@ -2207,6 +2221,189 @@ int lbib_load_solvers(lbib_handle* hh, const char* solverFile) {
     }
     rc = lbib_upload_lattice(hh, f.data(), h.S ? g.data() : nullptr, nullptr);
     if (rc) return rc;
+    API_END
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The force list and the node range queries for host plugins: the calls a
+// bio solver makes on ForceSolver (addForce, deleteForceType, deleteAllForces;
+// ForceSolver.cpp:107-139,170-215) and Geometry
+// (getGeometryNodesWithinRadius[WithAvoidance][Closest], Geometry.cpp:306-374)
+// between steps, in bulk.
+
+namespace lbib {
+
+// Runs one edit of the force list now (between steps) and checks its status.
+static void run_force_edit(Handle& h, int delType, int gen) {
+    ensure_force_scratch(h, true);
+    reset_status(h, h.iteration, h.cellTypesCopied);
+    launch_force_edit(h.m, h.fs, delType, gen, 0.0, 0.0, 0.0, h.st, h.stream);
+    CK(cudaGetLastError());
+    read_status(h);
+    if (h.stHost->err) fail(h.stHost->err, "force list edit failed", h.stHost->errIndex);
+}
+
+// Makes room for `extra` more records, keeping the list.
+static void reserve_force_records(Handle& h, int extra) {
+    const int M = h.m.M;
+    int R = 0;
+    CK(cudaMemcpyAsync(&R, h.m.foff + M, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    if (R + extra <= h.Fcap) return;
+    std::vector<int> ftype(R), fpart(R);
+    std::vector<double> fpar(4 * (size_t)R);
+    if (R) {
+        CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * fpar.size(), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    }
+    ensure_capacity(h, h.m.M, h.m.C, R + extra + 2 * h.Mcap, h.m.nCells);
+    if (R) {
+        CK(cudaMemcpyAsync(h.m.ftype, ftype.data(), sizeof(int) * R, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.fpartner, fpart.data(), sizeof(int) * R, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.fpar, fpar.data(), sizeof(double) * fpar.size(), cudaMemcpyHostToDevice, h.stream));
+    }
+}
+
+// Index of node `id` in the id-ordered node arrays, -1 if absent.
+static int node_index(const Handle& h, uint32_t id) {
+    auto it = std::lower_bound(h.ids.begin(), h.ids.end(), id);
+    return it != h.ids.end() && *it == id ? (int)(it - h.ids.begin()) : -1;
+}
+
+// The list as it stands between steps, set by a host call: later steps treat
+// it like a list loaded at this iteration.
+static void set_list_state(Handle& h, bool pure) {
+    h.forcesPureAtLoad = pure;
+    h.forceListIt = h.iteration;
+    h.forcemap.clear();
+}
+
+template <typename T>
+static T* upload(Handle& h, const std::vector<T>& v) {
+    T* d = dalloc<T>(std::max<size_t>(v.size(), 1));
+    if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, h.stream));
+    return d;
+}
+
+}  // namespace lbib
+
+extern "C" {
+
+int lbib_add_forces(lbib_handle* hh, const int* type, const unsigned* id1, const unsigned* id2, const double* par,
+                    int n) {
+    if (n < 0 || (n > 0 && (!type || !id1 || !par))) return LBIB_ERR_INPUT;
+    API_BEGIN(hh)
+    if (n == 0) return LBIB_OK;
+    lbib::pull_topology(h);
+    std::vector<int> node(n), partner(n, -1);
+    for (int k = 0; k < n; ++k) {
+        const int t = type[k];
+        if (t < 0 || t > 7) lbib::fail(LBIB_ERR_INPUT, "Invalid force solver type found.", k);
+        node[k] = lbib::node_index(h, id1[k]);
+        if (node[k] < 0) lbib::fail(LBIB_ERR_FORCE_NODE, "Could not compute and set the forces.", (long long)id1[k]);
+        if (t == 0 || t == 5 || t == 6 || t == 7) {
+            if (!id2) lbib::fail(LBIB_ERR_INPUT, "forces of types 0, 5, 6, 7 need a second node", k);
+            partner[k] = lbib::node_index(h, id2[k]);
+            if (partner[k] < 0)
+                lbib::fail(LBIB_ERR_FORCE_NODE, "Could not compute and set the forces.", (long long)id2[k]);
+        }
+    }
+    // per node, in call order (ForceSolver::addForce appends to forcemap_[id1])
+    std::vector<int> off(h.Mcap + 1, 0);
+    for (int k = 0; k < n; ++k) off[node[k] + 1]++;
+    for (int i = 0; i < h.Mcap; ++i) off[i + 1] += off[i];
+    std::vector<int> fill(off.begin(), off.end() - 1), ltype(n), lpart(n);
+    std::vector<double> lpar(4 * (size_t)n);
+    for (int k = 0; k < n; ++k) {
+        const int r = fill[node[k]]++;
+        ltype[r] = type[k];
+        lpart[r] = partner[k];
+        for (int q = 0; q < 4; ++q) lpar[4 * (size_t)r + q] = par[4 * (size_t)k + q];
+    }
+    lbib::reserve_force_records(h, n);
+    lbib::ensure_force_scratch(h, true);
+    h.fs.listOff = lbib::upload(h, off);
+    h.fs.listType = lbib::upload(h, ltype);
+    h.fs.listPartner = lbib::upload(h, lpart);
+    h.fs.listPar = lbib::upload(h, lpar);
+    struct Free {
+        lbib::ForceScratch& fs;
+        ~Free() {
+            cudaFree(fs.listOff); cudaFree(fs.listType); cudaFree(fs.listPartner); cudaFree(fs.listPar);
+            fs.listOff = fs.listType = fs.listPartner = nullptr;
+            fs.listPar = nullptr;
+        }
+    } freeList{h.fs};
+    lbib::run_force_edit(h, -1, lbib::GEN_LIST);
+    lbib::set_list_state(h, false);
+    API_END
+}
+
+int lbib_delete_force_type(lbib_handle* hh, int type) {
+    API_BEGIN(hh)
+    const bool pure = lbib::pure_at_start(h, h.iteration);
+    lbib::run_force_edit(h, type, lbib::GEN_NONE);
+    lbib::set_list_state(h, pure);
+    API_END
+}
+
+int lbib_delete_all_forces(lbib_handle* hh) {
+    API_BEGIN(hh)
+    lbib::launch_clear_forces(h.m, h.stream);
+    CK(cudaStreamSynchronize(h.stream));
+    lbib::set_list_state(h, true);
+    API_END
+}
+
+int lbib_nodes_within_radius(lbib_handle* hh, double x, double y, double radius, long long avoidDomain,
+                             unsigned* ids, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    if (cap < 0 || (cap > 0 && !ids) || !(radius >= 0.0)) return -LBIB_ERR_INPUT;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    try {
+        cudaSetDevice(h.device);
+        lbib::ensure_force_scratch(h, true);
+        lbib::launch_cell_list(h.m, h.fs, h.nx, h.ny, h.stream);
+        const std::vector<double> q = {x, y};
+        const std::vector<long long> av = {avoidDomain};
+        double* dq = lbib::upload(h, q);
+        long long* dav = lbib::upload(h, av);
+        unsigned* dids = lbib::dalloc<unsigned>(std::max(cap, 1));
+        int* dcount = lbib::dalloc<int>(1);
+        lbib::launch_range_query(h.m, h.fs, h.nx, h.ny, dq, dq + 1, dav, 1, radius, 0, dids, cap, dcount, nullptr,
+                                 h.stream);
+        int count = 0;
+        CK(cudaMemcpyAsync(&count, dcount, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+        if (cap > 0) CK(cudaMemcpyAsync(ids, dids, sizeof(unsigned) * cap, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        cudaFree(dq); cudaFree(dav); cudaFree(dids); cudaFree(dcount);
+        return count;
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg;
+        return -e.code;
+    }
+}
+
+int lbib_closest_nodes(lbib_handle* hh, const double* x, const double* y, const long long* avoidDomain, int n,
+                       double radius, long long* closest) {
+    if (n < 0 || (n > 0 && (!x || !y || !closest)) || !(radius >= 0.0)) return LBIB_ERR_INPUT;
+    API_BEGIN(hh)
+    if (n == 0) return LBIB_OK;
+    lbib::ensure_force_scratch(h, true);
+    lbib::launch_cell_list(h.m, h.fs, h.nx, h.ny, h.stream);
+    double* dx = lbib::upload(h, std::vector<double>(x, x + n));
+    double* dy = lbib::upload(h, std::vector<double>(y, y + n));
+    long long* dav = avoidDomain ? lbib::upload(h, std::vector<long long>(avoidDomain, avoidDomain + n)) : nullptr;
+    long long* dout = lbib::dalloc<long long>(n);
+    lbib::launch_range_query(h.m, h.fs, h.nx, h.ny, dx, dy, dav, n, radius, 1, nullptr, 0, nullptr, dout, h.stream);
+    CK(cudaMemcpyAsync(closest, dout, sizeof(long long) * n, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    cudaFree(dx); cudaFree(dy); if (dav) cudaFree(dav); cudaFree(dout);
     API_END
 }
 

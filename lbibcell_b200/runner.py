@@ -150,6 +150,49 @@ class Simulation:
             raise self._error()
         return {int(d[i]): float(a[i]) for i in range(n)}
 
+    # -- force list and range queries (host bio solvers) -----------------------
+    def add_forces(self, types, id1, id2, par) -> None:
+        """ForceSolver::addForce for a batch of records (see lbib_add_forces):
+        types (n,), id1 (n,), id2 (n,) (ignored where the type has no partner),
+        par (n, 4)."""
+        t = np.ascontiguousarray(types, np.int32)
+        a = np.ascontiguousarray(id1, np.uint32)
+        b = np.ascontiguousarray(id2, np.uint32)
+        p = np.ascontiguousarray(par, np.float64).reshape(-1, 4)
+        if not (len(t) == len(a) == len(b) == len(p)):
+            raise ValueError("add_forces: arrays of different lengths")
+        self._check(self._L.lbib_add_forces(self._h, _p(t), _p(a), _p(b), _p(p), len(t)))
+
+    def delete_force_type(self, t: int) -> None:
+        self._check(self._L.lbib_delete_force_type(self._h, int(t)))
+
+    def delete_all_forces(self) -> None:
+        self._check(self._L.lbib_delete_all_forces(self._h))
+
+    def nodes_within_radius(self, x: float, y: float, radius: float, avoid_domain: int = -1) -> np.ndarray:
+        """Geometry::getGeometryNodesWithinRadius[WithAvoidance]: node ids, in the
+        reference's cell-list order."""
+        cap = 64
+        while True:
+            ids = np.zeros(cap, np.uint32)
+            n = self._L.lbib_nodes_within_radius(self._h, float(x), float(y), float(radius), int(avoid_domain),
+                                                 _p(ids), cap)
+            if n < 0:
+                raise self._error()
+            if n <= cap:
+                return ids[:n].copy()
+            cap = n
+
+    def closest_nodes(self, x, y, radius: float, avoid_domain=None) -> np.ndarray:
+        """Geometry::getGeometryNodesWithinRadiusWithAvoidanceClosest for each
+        query point: node id or -1."""
+        qx = np.ascontiguousarray(x, np.float64)
+        qy = np.ascontiguousarray(y, np.float64)
+        av = None if avoid_domain is None else np.ascontiguousarray(avoid_domain, np.int64)
+        out = np.zeros(len(qx), np.int64)
+        self._check(self._L.lbib_closest_nodes(self._h, _p(qx), _p(qy), _p(av), len(qx), float(radius), _p(out)))
+        return out
+
     # -- checkpoint files (the reference's formats) ------------------------------
     def write_simulation(self, prefix: str) -> Dict[str, str]:
         """SimulationRunner::writeSimulation into prefix_{force,geometry,parameters,solver}.txt;
