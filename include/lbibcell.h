@@ -232,6 +232,32 @@ int lbib_nodes_within_radius(lbib_handle* h, double x, double y, double radius, 
 int lbib_closest_nodes(lbib_handle* h, const double* x, const double* y, const long long* avoidDomain, int n,
                        double radius, long long* closest);
 
+/* VTK output without VTK: the block that vtkCellReporter (cells: polygons of
+ * the membrane with domain_identifier, cell_type, boundarydescriptors),
+ * vtkForceReporter (forces: a line per force with a partner, ForceType),
+ * vtkCDEReporter (one concentration array per CDE solver, by name) or
+ * vtkFluidReporter (density, velocity) adds, appended to
+ * <prefix>_<time>.vtm with the block in <prefix>_<time>/<prefix>_<time>_<k>.vt?
+ * (vtkCellReporter.cpp, vtkForceReporter.cpp, vtkCDEReporter.cpp,
+ * vtkFluidReporter.cpp; VTK XML in ASCII mode, as the reference writes it).
+ * `coarsening` is the grid reporters' coarsening factor (1 = every node).
+ * LBIB_VTK_CELL_PNG (vtkCellPNGReporter) needs a graphics stack and writes
+ * nothing.  A geometry file ending in ".vtm" given to lbib_create_from_files
+ * is read like Geometry::loadGeometryVTK (Geometry.cpp:162-306). */
+#define LBIB_VTK_CELLS 1
+#define LBIB_VTK_FORCES 2
+#define LBIB_VTK_CDE 3
+#define LBIB_VTK_FLUID 4
+#define LBIB_VTK_CELL_PNG 5
+int lbib_write_vtk(lbib_handle* h, const char* prefix, unsigned time, int kind, int coarsening);
+
+/* Reads a .vtm geometry as Geometry::loadGeometryVTK does, on the host only
+ * (no GPU, no handle): counts[0] nodes (ids 0..n-1, positions xy[2n] before
+ * GeometryNode's perturbation) and counts[1] connections (id1, id2, domain
+ * per connection).  Up to capNodes / capConns entries are written. */
+int lbib_read_vtm_geometry(const char* path, unsigned* ids, double* xy, int capNodes, unsigned* conns,
+                           int capConns, int* counts);
+
 /* Last error: code; message into buf; index of the node/connection involved. */
 int lbib_last_error(lbib_handle* h, char* buf, int len, long long* index);
 

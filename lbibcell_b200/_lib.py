@@ -18,7 +18,8 @@ SYMBOLS = (
     "lbib_areas", "lbib_areas_static", "lbib_last_error", "lbib_last_timing", "lbib_set_profiling", "lbib_set_species_source",
     "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
     "lbib_write_simulation", "lbib_load_solvers", "lbib_add_forces", "lbib_delete_force_type",
-    "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes",
+    "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes", "lbib_write_vtk",
+    "lbib_read_vtm_geometry",
 )
 
 _lib = None
@@ -95,6 +96,10 @@ def load() -> ctypes.CDLL:
     L.lbib_nodes_within_radius.restype = ip
     L.lbib_nodes_within_radius.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_longlong, vp, ip]
+    L.lbib_write_vtk.restype = ip
+    L.lbib_write_vtk.argtypes = [vp, cp, ctypes.c_uint, ip, ip]
+    L.lbib_read_vtm_geometry.restype = ip
+    L.lbib_read_vtm_geometry.argtypes = [cp, vp, vp, ip, vp, ip, vp]
     L.lbib_closest_nodes.restype = ip
     L.lbib_closest_nodes.argtypes = [vp, vp, vp, vp, ip, ctypes.c_double, vp]
     _lib = L

@@ -26,6 +26,7 @@ UNITS = [
     ("lbib_host.cu", ["--fmad=false"]),
     ("k_lattice32.cu", []),
     ("k_adjoint.cu", []),
+    ("vtk_io.cu", []),
 ]
 
 

@@ -30,6 +30,7 @@
 
 #include "../../include/lbibcell.h"
 #include "kernels.cuh"
+#include "vtk_io.h"
 
 namespace lbib {
 
@@ -1238,17 +1239,40 @@ static void create(Handle& h, const std::string& params, const std::string& geom
 
     h.m.topo = dalloc<Topo>(1);
 
-    // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160); each new
-    // GeometryNode runs perturbatePosition (GeometryNode.cpp:98-117).
-    std::ifstream in(geom);
-    if (!in.is_open()) fail(ERR_INPUT, "Cannot find the geometry.txt file.");
+    // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160), or for a
+    // ".vtm" file loadGeometryVTK (Geometry.cpp:162-306, the choice made at
+    // Geometry.cpp:61-71); each new GeometryNode runs perturbatePosition
+    // (GeometryNode.cpp:98-117), in the order the nodes are created.
     std::map<uint32_t, std::pair<double, double>> nodes;
     std::map<uint32_t, uint32_t> ctypes;
     ctypes[0] = 0;
     std::string line;
     bool readingNodes = true;
     uint32_t maxDom = 0;
-    while (std::getline(in, line)) {
+    const bool vtm = geom.size() >= 4 && geom.compare(geom.size() - 4, 4, ".vtm") == 0;
+    std::ifstream in;
+    if (vtm) {
+        vtk::Geometry vg;
+        try {
+            vtk::read_vtm_geometry(geom, vg);
+        } catch (const std::runtime_error& e) {
+            fail(ERR_INPUT, e.what());
+        }
+        for (size_t k = 0; k < vg.x.size(); ++k) {
+            double x = vg.x[k], y = vg.y[k];
+            perturbate(h, x, y);
+            nodes[(uint32_t)k] = {x, y};
+        }
+        for (const auto& c : vg.conns) {
+            h.conns.push_back(HConn{c.id1, c.id2, c.dom, c.desc});
+            maxDom = std::max(maxDom, c.dom);
+        }
+        for (const auto& kv : vg.cellType) ctypes[kv.first] = kv.second;
+    } else {
+        in.open(geom);
+        if (!in.is_open()) fail(ERR_INPUT, "Cannot find the geometry.txt file.");
+    }
+    while (!vtm && std::getline(in, line)) {
         if (line.empty()) continue;
         if (line.find("#Connection") != std::string::npos) readingNodes = false;
         if (line[0] == '#') continue;
@@ -2404,6 +2428,203 @@ int lbib_closest_nodes(lbib_handle* hh, const double* x, const double* y, const 
     CK(cudaMemcpyAsync(closest, dout, sizeof(long long) * n, cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
     cudaFree(dx); cudaFree(dy); if (dav) cudaFree(dav); cudaFree(dout);
+    API_END
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// VTK reporters without VTK (vtkCellReporter, vtkForceReporter,
+// vtkCDEReporter, vtkFluidReporter): each call appends the functor's block to
+// <prefix>_<time>.vtm.
+
+namespace lbib {
+
+// The reporter's boundary descriptor string: "\t", then "<bsolver>\t<cde>\t"
+// for every pair of the connection's descriptor map (vtkCellReporter.cpp).
+static std::string reporter_descriptor(const std::string& desc) {
+    std::stringstream ls(desc);
+    std::map<std::string, std::vector<std::string>> type;
+    std::string a, b;
+    while (ls >> a >> b) type[a].push_back(b);
+    std::string out = "\t";
+    for (const auto& kv : type)
+        for (const auto& c : kv.second) out += kv.first + "\t" + c + "\t";
+    return out;
+}
+
+static void vtk_cells(lbib_handle* hh, Handle& h, const std::string& vtm) {
+    pull_topology(h);
+    std::vector<unsigned> ids(h.m.M);
+    std::vector<double> st(6 * (size_t)h.m.M);
+    if (int rc = lbib_download_membrane(hh, ids.data(), st.data())) fail(rc, "membrane download failed");
+    std::map<uint32_t, int> index;
+    for (int i = 0; i < h.m.M; ++i) index[ids[i]] = i;
+    std::map<uint32_t, int> outConn;  // node id -> its connection<1> (outgoing)
+    std::map<uint32_t, std::vector<int>> cells;  // domain -> connections in vector order
+    for (size_t c = 0; c < h.conns.size(); ++c) {
+        outConn[h.conns[c].id1] = (int)c;
+        cells[h.conns[c].dom].push_back((int)c);
+    }
+    vtk::PolyData pd;
+    vtk::Array domA{"domain_identifier", 1, "Float64", {}}, typeA{"cell_type", 1, "Float64", {}};
+    std::vector<std::string> descs;
+    for (const auto& kv : cells) {
+        const int start = kv.second[0];
+        int c = start;
+        do {
+            const int n = index.at(h.conns[c].id2);
+            pd.px.push_back(st[6 * (size_t)n]);
+            pd.py.push_back(st[6 * (size_t)n + 1]);
+            pd.connectivity.push_back((int64_t)pd.connectivity.size());
+            domA.values.push_back((double)h.conns[c].dom);
+            const uint32_t d = h.conns[c].dom;
+            if (d >= h.ctypeHost.size()) fail(ERR_STATE, "domainIdentifier not found in the cellTrackerMap.");
+            typeA.values.push_back((double)h.ctypeHost[d]);
+            descs.push_back(reporter_descriptor(h.conns[c].desc));
+            c = outConn.at(h.conns[c].id2);
+        } while (c != start);
+        pd.offsets.push_back((int64_t)pd.connectivity.size());
+    }
+    pd.pointData = {domA, typeA};
+    pd.pointStrings.push_back({"boundarydescriptors", descs});
+    vtk::append_block(vtm, pd);
+}
+
+static void vtk_forces(lbib_handle* hh, Handle& h, const std::string& vtm) {
+    pull_topology(h);
+    const int M = h.m.M;
+    std::vector<unsigned> ids(M);
+    std::vector<double> st(6 * (size_t)M);
+    if (int rc = lbib_download_membrane(hh, ids.data(), st.data())) fail(rc, "membrane download failed");
+    std::vector<int> foff(M + 1);
+    CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (M + 1), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    const int R = foff[M];
+    std::vector<int> ftype(R), fpart(R);
+    if (R) {
+        CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    }
+    vtk::PolyData pd;
+    pd.lines = true;
+    vtk::Array typeA{"ForceType", 1, "UInt32", {}};
+    for (int i = 0; i < M; ++i)
+        for (int r = foff[i]; r < foff[i + 1]; ++r) {
+            const int t = ftype[r];
+            const bool paired = t == 0 || t == 5 || t == 6 || t == 7;
+            // getPartnerGeometryNode() != 0: forces without a partner report 0,
+            // and so does a partner whose id is 0 (vtkForceReporter.cpp)
+            const uint32_t pid = paired && fpart[r] >= 0 && fpart[r] < M ? ids[fpart[r]] : 0u;
+            if (pid == 0) continue;
+            pd.px.push_back(st[6 * (size_t)i]);
+            pd.py.push_back(st[6 * (size_t)i + 1]);
+            pd.px.push_back(st[6 * (size_t)fpart[r]]);
+            pd.py.push_back(st[6 * (size_t)fpart[r] + 1]);
+            pd.connectivity.push_back((int64_t)pd.px.size() - 2);
+            pd.connectivity.push_back((int64_t)pd.px.size() - 1);
+            pd.offsets.push_back((int64_t)pd.connectivity.size());
+            typeA.values.push_back((double)t);
+        }
+    pd.cellData = {typeA};
+    vtk::append_block(vtm, pd);
+}
+
+// vtkCDEReporter / vtkFluidReporter: a uniform grid of nx/f x ny/f points,
+// spacing f, filled by rows y = 0, f, 2f, .. and columns x = 0, f, .. (the
+// functors' loops; when f does not divide the lattice they produce more values
+// than the grid's points, and so does this writer).
+static void vtk_grid(lbib_handle* hh, Handle& h, const std::string& vtm, int f, bool fluid) {
+    const size_t L = h.L;
+    std::vector<double> fd, g, vel;
+    if (fluid) {
+        fd.resize(9 * L);
+        vel.resize(2 * L);
+    } else {
+        g.resize((size_t)std::max(1, h.S) * 5 * L);
+    }
+    if (int rc = lbib_download_lattice(hh, fluid ? fd.data() : nullptr, fluid ? nullptr : g.data(),
+                                       fluid ? vel.data() : nullptr, nullptr, nullptr, nullptr))
+        fail(rc, "lattice download failed");
+    vtk::ImageData im;
+    im.X = h.nx / f;
+    im.Y = h.ny / f;
+    im.spacing = f;
+    if (fluid) {
+        vtk::Array rho{"density", 1, "Float64", {}}, u{"velocity", 3, "Float64", {}};
+        for (int y = 0; y < h.ny; y += f)
+            for (int x = 0; x < h.nx; x += f) {
+                const size_t n = (size_t)y * h.nx + x;
+                double r = 0.0;  // FluidSolver::getRho: accumulate over the slots
+                for (int q = 0; q < 9; ++q) r += fd[9 * n + q];
+                rho.values.push_back(r);
+                u.values.push_back(vel[2 * n]);
+                u.values.push_back(vel[2 * n + 1]);
+                u.values.push_back(0.0);
+            }
+        im.pointData = {rho, u};
+    } else {
+        std::map<std::string, int> byName;  // the functor's map: arrays in name order
+        for (int k = 0; k < h.S; ++k) byName[h.sp[k].name] = k;
+        for (const auto& kv : byName) {
+            vtk::Array c{kv.first, 1, "Float64", {}};
+            for (int y = 0; y < h.ny; y += f)
+                for (int x = 0; x < h.nx; x += f) {
+                    const size_t n = (size_t)y * h.nx + x;
+                    double sum = 0.0;  // CDESolverD2Q5::getC
+                    for (int q = 0; q < 5; ++q) sum += g[((size_t)kv.second * L + n) * 5 + q];
+                    c.values.push_back(sum);
+                }
+            im.pointData.push_back(c);
+        }
+    }
+    vtk::append_block(vtm, im);
+}
+
+}  // namespace lbib
+
+extern "C" {
+
+int lbib_read_vtm_geometry(const char* path, unsigned* ids, double* xy, int capNodes, unsigned* conns,
+                           int capConns, int* counts) {
+    if (!path || !counts || capNodes < 0 || capConns < 0) return LBIB_ERR_INPUT;
+    lbib::vtk::Geometry g;
+    try {
+        lbib::vtk::read_vtm_geometry(path, g);
+    } catch (const std::exception&) {
+        return LBIB_ERR_INPUT;
+    }
+    counts[0] = (int)g.x.size();
+    counts[1] = (int)g.conns.size();
+    for (int k = 0; k < counts[0] && k < capNodes; ++k) {
+        if (ids) ids[k] = (unsigned)k;
+        if (xy) { xy[2 * k] = g.x[k]; xy[2 * k + 1] = g.y[k]; }
+    }
+    for (int c = 0; c < counts[1] && c < capConns; ++c)
+        if (conns) {
+            conns[3 * c] = g.conns[c].id1;
+            conns[3 * c + 1] = g.conns[c].id2;
+            conns[3 * c + 2] = g.conns[c].dom;
+        }
+    return LBIB_OK;
+}
+
+int lbib_write_vtk(lbib_handle* hh, const char* prefix, unsigned time, int kind, int coarsening) {
+    if (!prefix || kind < LBIB_VTK_CELLS || kind > LBIB_VTK_CELL_PNG || coarsening < 1) return LBIB_ERR_INPUT;
+    API_BEGIN(hh)
+    const std::string vtm = std::string(prefix) + "_" + std::to_string(time) + ".vtm";
+    try {
+        switch (kind) {
+            case LBIB_VTK_CELLS: lbib::vtk_cells(hh, h, vtm); break;
+            case LBIB_VTK_FORCES: lbib::vtk_forces(hh, h, vtm); break;
+            case LBIB_VTK_CDE: lbib::vtk_grid(hh, h, vtm, coarsening, false); break;
+            case LBIB_VTK_FLUID: lbib::vtk_grid(hh, h, vtm, coarsening, true); break;
+            default: break;  // vtkCellPNGReporter renders through a graphics stack: nothing is written
+        }
+    } catch (const std::runtime_error& e) {
+        lbib::fail(LBIB_ERR_INPUT, e.what());
+    }
     API_END
 }
 

@@ -193,6 +193,15 @@ class Simulation:
         self._check(self._L.lbib_closest_nodes(self._h, _p(qx), _p(qy), _p(av), len(qx), float(radius), _p(out)))
         return out
 
+    # -- VTK reporters ---------------------------------------------------------------
+    VTK_CELLS, VTK_FORCES, VTK_CDE, VTK_FLUID, VTK_CELL_PNG = 1, 2, 3, 4, 5
+
+    def write_vtk(self, prefix: str, time: int, kind: int, coarsening: int = 1) -> str:
+        """Appends the block of one vtk*Reporter to prefix_time.vtm; returns the
+        .vtm path."""
+        self._check(self._L.lbib_write_vtk(self._h, prefix.encode(), int(time), int(kind), int(coarsening)))
+        return f"{prefix}_{int(time)}.vtm"
+
     # -- checkpoint files (the reference's formats) ------------------------------
     def write_simulation(self, prefix: str) -> Dict[str, str]:
         """SimulationRunner::writeSimulation into prefix_{force,geometry,parameters,solver}.txt;
@@ -241,3 +250,19 @@ class Simulation:
     def concentrations(self) -> np.ndarray:
         """C_k(x) = sum of species k's distributions, shape (S, Nx*Ny)."""
         return self.lattice().g.sum(axis=2)
+
+
+def read_vtm_geometry(path: str):
+    """Geometry::loadGeometryVTK on the host (no GPU): (ids[n], xy[n, 2] before
+    the perturbation of new nodes, connections[c, 3] = id1, id2, domain)."""
+    L = load()
+    counts = np.zeros(2, np.int32)
+    rc = L.lbib_read_vtm_geometry(path.encode(), None, None, 0, None, 0, _p(counts))
+    if rc:
+        raise LbibError(rc, f"cannot read {path}", -1)
+    n, c = int(counts[0]), int(counts[1])
+    ids = np.zeros(n, np.uint32); xy = np.zeros((n, 2)); conns = np.zeros((c, 3), np.uint32)
+    rc = L.lbib_read_vtm_geometry(path.encode(), _p(ids), _p(xy), n, _p(conns), c, _p(counts))
+    if rc:
+        raise LbibError(rc, f"cannot read {path}", -1)
+    return ids, xy, conns
