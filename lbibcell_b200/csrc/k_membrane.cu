@@ -881,44 +881,58 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
                             const SpeciesConst* sp, const double* srcTab, int nDomains, const uint32_t* ctypeTab,
                             int cellTypesCopied, const CrossDev& c, int nx, int ny, size_t L, Status* st,
                             unsigned iteration) {
+    // Every value the update may read is loaded before any is used (the
+    // neighbours' domains and distributions, the node's boundary slots and
+    // velocity), so that the loads overlap instead of forming a chain; the
+    // arithmetic below is the reference's, in its order.
     const uint32_t oldDom = dom[n];
-    dom[n] = newDom;
     const int x = (int)(n % nx), y = (int)(n / nx);
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-    const size_t nb[4] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x};
-    const size_t nNE = (size_t)yp * nx + xp;
+    const size_t nb[5] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x,
+                          (size_t)yp * nx + xp};  // E, N, W, S, then NE
+    uint32_t dnb[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) dnb[s] = dom[nb[s]];
     bool hasBN[4];
+#pragma unroll
     for (int s = 0; s < 4; ++s) hasBN[s] = c.bnDist[n * 4 + s] != kEmpty;
+    const double ux = (double)u[n], uy = (double)u[L + n];
+    dom[n] = newDom;
     // boundaryNodes_[NE] aliases (domainIdentifier_, cellType_): null only if both are 0.
     const uint32_t ctype = cellTypesCopied ? (oldDom < (uint32_t)nDomains ? ctypeTab[oldDom] : 1u) : 0u;
     const bool neNull = newDom == 0 && ctype == 0;
-    const double ux = (double)u[n], uy = (double)u[L + n];
     for (int k = 0; k < nS; ++k) {
-        Real* gk = g + (size_t)k * 5 * L;
+        const Real* gk = g + (size_t)k * 5 * L;
+        // the five slots of the four neighbours and NE, read unconditionally
+        Real gv[5][5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) gv[s][q] = gk[(size_t)q * L + nb[s]];
         double sumC = 0.0;
         int counter = 0;
+#pragma unroll
         for (int s = 0; s < 4; ++s) {
-            const size_t mnode = nb[s];
-            if (!hasBN[s] && newDom == dom[mnode]) {
+            if (!hasBN[s] && newDom == dnb[s]) {
                 // getC() in slot order after localSwap: T, W, S, E, N
                 double C = 0.0;
-                C += (double)gk[0 * L + mnode];
-                C += (double)gk[3 * L + mnode];
-                C += (double)gk[4 * L + mnode];
-                C += (double)gk[1 * L + mnode];
-                C += (double)gk[2 * L + mnode];
+                C += (double)gv[s][0];
+                C += (double)gv[s][3];
+                C += (double)gv[s][4];
+                C += (double)gv[s][1];
+                C += (double)gv[s][2];
                 sumC += C;
                 counter++;
             }
         }
-        if (counter == 0 && neNull && newDom == dom[nNE]) {
+        if (counter == 0 && neNull && newDom == dnb[4]) {
             double C = 0.0;
-            C += (double)gk[0 * L + nNE];
-            C += (double)gk[3 * L + nNE];
-            C += (double)gk[4 * L + nNE];
-            C += (double)gk[1 * L + nNE];
-            C += (double)gk[2 * L + nNE];
+            C += (double)gv[4][0];
+            C += (double)gv[4][3];
+            C += (double)gv[4][4];
+            C += (double)gv[4][1];
+            C += (double)gv[4][2];
             sumC += C;
             counter++;
             atomicAdd(&st->nDiagReinit, 1);
@@ -930,7 +944,8 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
         const double src = (srcTab != nullptr && newDom < (uint32_t)nDomains) ? srcTab[(size_t)k * nDomains + newDom]
                                                                             : 0.0;
         collide_cde64(gi, ux, uy, sp[k].tau, sp[k].kind, src, sp[k].decay, newDom, iteration);
-        for (int q = 0; q < 5; ++q) gk[(size_t)q * L + n] = (Real)gi[q];
+        Real* go = g + (size_t)k * 5 * L;
+        for (int q = 0; q < 5; ++q) go[(size_t)q * L + n] = (Real)gi[q];
     }
 }
 
