@@ -59,9 +59,18 @@ __device__ __forceinline__ double dirac(const double dx, const double dy) {
 
 // ---------------------------------------------------------------------------
 // Force evaluation
-__global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration) {
+// `begin`: also reset the step's counters (the first kernel of a step).
+__global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration, int begin) {
     pdl_wait();
     if (st->halt) return;
+    if (begin && blockIdx.x == 0 && threadIdx.x == 0) {
+        st->nPerturbNode = 0;
+        st->nPerturbConn = 0;
+        st->nChanged = 0;
+        st->nRecords = 0;
+        st->remesh = 0;
+        st->coarsen = 0;
+    }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
     const double x1 = m.x[i], y1 = m.y[i];
@@ -126,12 +135,12 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration)
 }
 
 template <typename Real>
-void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin) {
     if (m.Mcap == 0) return;
-    launch_pdl(force_eval_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st, iteration);
+    launch_pdl(force_eval_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st, iteration, begin ? 1 : 0);
 }
-template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t);
-template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t);
+template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool);
+template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool);
 
 // ---------------------------------------------------------------------------
 // Spreading
@@ -786,7 +795,20 @@ __device__ __forceinline__ void record_noflux(const MembraneDev& m, CrossDev& c,
     if (k < c.nfCap) c.nfKeys[k] = key;
 }
 
-__global__ void cross_win_kernel(CrossDev c, MembraneDev m, const uint32_t* dom, int nx, Status* st) {
+// GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test for a node
+// that left its previous unit cell (GeometryHandler.cpp:610-636,
+// GeometryNode.cpp:256-261, Rectangle.cpp pointWithinBounds).
+__device__ __forceinline__ void edge_check_node(const MembraneDev& m, int i, int nx, int ny, Status* st, int stage) {
+    const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
+    const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
+    if (within) return;
+    if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, stage);
+    else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, stage);
+    else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, stage);
+    else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, stage);
+}
+
+__global__ void cross_win_kernel(CrossDev c, MembraneDev m, const uint32_t* dom, int nx, int ny, Status* st) {
     pdl_wait();
     if (st->halt) return;
     const int n = min(st->pad[2], c.recCap);
@@ -807,11 +829,16 @@ __global__ void cross_win_kernel(CrossDev c, MembraneDev m, const uint32_t* dom,
             if (k < c.changedCap) {
                 c.changedNode[k] = (uint32_t)node;
                 c.changedDom[k] = bdom;
+                c.mark[node] = k + 1;  // the node's position in the list, for the re-initialisation
             } else {
                 raise_error(st, ERR_CAPACITY, (int)node, ST_CROSSINGS);
             }
         }
     }
+    // GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test of the
+    // moved nodes, over the same grid
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.topo->M; i += gridDim.x * blockDim.x)
+        edge_check_node(m, i, nx, ny, st, ST_CROSSINGS);
 }
 
 // Clears the previous step's no-flux boundary nodes (after the stream-collide
@@ -832,13 +859,7 @@ __global__ void edge_check_kernel(MembraneDev m, int nx, int ny, Status* st, int
     if (st->halt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
-    const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
-    const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
-    if (within) return;
-    if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, stage);
-    else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, stage);
-    else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, stage);
-    else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, stage);
+    edge_check_node(m, i, nx, ny, st, stage);
 }
 
 template <typename Real>
@@ -850,8 +871,7 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
     launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
-    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, st);
-    launch_pdl(edge_check_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, nx, ny, st, ST_CROSSINGS);
+    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, ny, st);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
                                        unsigned, cudaStream_t);
@@ -962,17 +982,9 @@ __device__ __forceinline__ void reinit_deps(const CrossDev& c, size_t n, int nx,
     for (int d = 0; d < 6; ++d) deps[d] = nbs[d] < n ? c.mark[nbs[d]] - 1 : -1;
 }
 
-// Re-initialisation, step 1: every changed node marks its position in the list.
-__global__ void reinit_mark_kernel(CrossDev c, Status* st) {
-    pdl_wait();
-    if (st->halt) return;
-    const int cnt = st->nChanged;
-    if (cnt > kReinitMax || cnt > c.changedCap) return;  // reported by the block kernel
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
-        c.mark[c.changedNode[k]] = k + 1;
-}
-
-// Step 2, across the whole GPU: the nodes that wait for no other changed node
+// (Each changed node's position in the list is marked where the crossings
+// append it, in cross_win_kernel; the block kernel clears the marks.)
+// Step 1, across the whole GPU: the nodes that wait for no other changed node
 // (almost all of them) are re-initialised at once.  No two such nodes read
 // each other (a changed neighbour in any of the six directions makes one of
 // the two wait for the other), so the order among them does not matter.
@@ -1019,7 +1031,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[6] = (int(*)[6])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    // Step 3, one block: the nodes that wait for others, in dependency rounds
+    // Step 2, one block: the nodes that wait for others, in dependency rounds
     // (the marks and the free nodes' results come from steps 1 and 2)
     if (threadIdx.x == 0) remaining = 0;
     __syncthreads();
@@ -1066,7 +1078,6 @@ void launch_reinit(CrossDev& c, uint32_t* dom, Real* g, const Real* u, int nS, c
                    size_t L, Status* st, unsigned iteration, cudaStream_t s) {
     if (c.changedCap <= 0) return;
     constexpr size_t smemBytes = kReinitSmem;
-    launch_pdl(reinit_mark_kernel, 148, 256, 0, s, c, st);
     launch_pdl(reinit_free_kernel<Real>, 148, 256, 0, s, c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains,
                ctypeTab, nx, ny, L, st);
     launch_pdl(reinit_kernel<Real>, 1, 1024, smemBytes, s, c, dom, g, u, nS, sp[0], sp[1], sp[2], srcTab, nDomains, ctypeTab,
@@ -1083,8 +1094,17 @@ template void launch_reinit<float>(CrossDev&, uint32_t*, float*, const float*, i
 // Domain fill: one block per row; the row's domain id at x >= 1 is the domain
 // of the last W-slot boundary node at x' in [1, x], else dom(0, y), which must
 // be 0 (GeometryHandler.cpp:68-85).  Reads and clears the W-slot plane.
+// The kernel also resets the (node, slot) entries the step's crossings wrote
+// (every written key has a record), after the re-initialisation that read
+// them; that part runs on a halted step too.
 __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* dom, int nx, int ny, Status* st) {
     pdl_wait();
+    const int nrec = min(st->pad[2], c.recCap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x) {
+        const uint32_t key = c.recKey[k];
+        c.bnDist[key] = kEmpty;
+        c.bnConn[key] = ~0u;
+    }
     if (st->halt) return;
     const int y = blockIdx.x;
     const size_t row = (size_t)y * nx;
@@ -1117,28 +1137,12 @@ __global__ void __launch_bounds__(256) domain_fill_kernel(CrossDev c, uint32_t* 
     }
 }
 
-// Resets the (node, slot) entries this step wrote (grid-stride over the
-// step's count, which lives on the device).
-// Resets the keys written this step (every written key has a record).
-__global__ void cross_clear_kernel(CrossDev c, Status* st) {
-    pdl_wait();
-    const int n = min(st->pad[2], c.recCap);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t key = c.recKey[k];
-        c.bnDist[key] = kEmpty;
-        c.bnConn[key] = ~0u;
-    }
-}
 
 void launch_domain_fill(CrossDev& c, uint32_t* dom, int nx, int ny, size_t L, Status* st, unsigned iteration,
                         cudaStream_t s) {
     launch_pdl(domain_fill_kernel, ny, 256, 0, s, c, dom, nx, ny, st);
 }
 
-void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s) {
-    if (c.recCap <= 0) return;
-    launch_pdl(cross_clear_kernel, 296, 256, 0, s, c, st);
-}
 
 // ---------------------------------------------------------------------------
 // Topology checks

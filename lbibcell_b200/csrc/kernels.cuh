@@ -153,7 +153,7 @@ void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, 
 
 // Membrane pipeline.  `Real` is the lattice precision (velocity / force planes).
 template <typename Real>
-void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin = false);
 template <typename Real>
 void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
                    unsigned iteration, cudaStream_t s);

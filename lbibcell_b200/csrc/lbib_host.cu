@@ -34,7 +34,6 @@
 
 namespace lbib {
 
-void launch_cross_clear(CrossDev& c, Status* st, cudaStream_t s);
 
 struct HostFail {
     int code;
@@ -868,9 +867,10 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
     const unsigned it = 0;  // kernels read the iteration from the status word
     long long nl = 0;
     if (fromStage <= ST_FORCE) {
-        launch_pdl(step_begin_kernel, 1, 1, 0, s, h.st);
-        launch_force_eval<Real>(h.m, h.st, it, s);
-        nl += 1 + hasM;
+        // the step's counters are reset by the force kernel, or alone without a membrane
+        if (hasM) launch_force_eval<Real>(h.m, h.st, it, s, true);
+        else launch_pdl(step_begin_kernel, 1, 1, 0, s, h.st);
+        nl += 1;
     }
     if (fromStage <= ST_SPREAD) {
         launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s);
@@ -898,19 +898,18 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
     }
     if (fromStage <= ST_CROSSINGS) {
         launch_crossings<Real>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
-        nl += hasM ? 4 : 0;
+        nl += hasM ? 3 : 0;
     }
     if (fromStage <= ST_REINIT) {
         SpeciesConst spc[kMaxSpecies] = {};
         for (int k = 0; k < h.S; ++k) spc[k] = h.sp[k].c;
         launch_reinit<Real>(h.cross, h.dom, gcur, (const Real*)h.u, h.S, spc, h.srcTab, h.nDomains, h.ctypeTab, 0,
                             h.nx, h.ny, h.L, h.st, it, s);
-        nl += 3;
+        nl += 2;
     }
     if (fromStage <= ST_DOMAIN) {
         launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
-        launch_cross_clear(h.cross, h.st, s);
-        nl += 2;
+        nl += 1;
     }
     if (fromStage <= ST_REMESH) nl += launch_remesh(h.m, h.td, h.nx, h.ny, h.st, s);
     if (fromStage <= ST_COARSEN && coarsenStep) {
@@ -1410,7 +1409,9 @@ static void cure_lattice(Handle& h, HostMembrane& hm) {
     if (h.precision == LBIB_FP64) launch_crossings<double>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
     else launch_crossings<float>(h.m, h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
     launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, 0, h.stream);
-    launch_cross_clear(h.cross, h.st, h.stream);
+    // the crossings mark the nodes whose domain they change; at set-up no
+    // re-initialisation follows to clear the marks
+    CK(cudaMemsetAsync(h.cross.mark, 0, sizeof(int) * h.L, h.stream));
     read_status(h);
     if (h.stHost->err) fail(h.stHost->err, "lattice set-up failed", h.stHost->errIndex);
     std::memset(h.stHost, 0, sizeof(Status));
