@@ -85,31 +85,23 @@ __global__ void remesh_flag_kernel(MembraneDev m, TopoDev t, Status* st, int* nR
     t.flag[c] = f;
 }
 
-// Decides the pass: K = number of splits; hands over to the host when the
-// pass would overflow a buffer, needs the random generator, or is a third one.
-__global__ void remesh_decide_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng, int lastPass) {
-    pdl_wait();
-    if (st->halt) return;
-    Topo* T = m.topo;
-    const int C = T->C;
-    const int K = t.rank[m.Ccap];  // exclusive scan over Ccap + 1 flags: the total
-    T->K = 0;
-    if (K == 0) return;
-    if (lastPass || *nRng > 0 || T->M + K > m.Mcap || C + K > m.Ccap) {
-        raise_halt(st, ST_REMESH);
-        return;
-    }
-    T->K = K;
-}
-
-__global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
+// Decides the pass (K = number of splits) and applies it.  A pass that would
+// overflow a buffer or needs the random generator goes to the host; so does
+// a third pass (remesh_again_kernel).  Every thread takes the same decision;
+// the first one records it for the copy that follows.
+__global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st, const int* nRng) {
     pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const Topo* T = m.topo;
-    const int K = T->K;
-    if (K == 0 || c >= T->C) return;
+    Topo* T = m.topo;
     const int C = T->C, M = T->M;
+    const int K = t.rank[m.Ccap];  // exclusive scan over Ccap + 1 flags: the total
+    const bool run = K > 0 && *nRng == 0 && M + K <= m.Mcap && C + K <= m.Ccap;
+    if (c == 0) {
+        T->K = run ? K : 0;
+        if (K > 0 && !run) raise_halt(st, ST_REMESH);
+    }
+    if (!run || c >= C) return;
     const int r = t.rank[c];
     if (!t.flag[c]) {
         const int dst = c - r;
@@ -130,56 +122,58 @@ __global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
     t.ca2[base + 1] = j; t.cb2[base + 1] = b; t.cdom2[base + 1] = m.cdom[c]; t.cdesc2[base + 1] = m.cdesc[c];
 }
 
+// Copies the new connection list back; the last block to finish commits the
+// pass (every block has read K and C before any block counts itself done).
 __global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
     pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const Topo* T = m.topo;
-    if (T->K == 0 || c >= T->C + T->K) return;
-    m.ca[c] = t.ca2[c]; m.cb[c] = t.cb2[c]; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
-}
-
-__global__ void remesh_commit_kernel(MembraneDev m, Status* st) {
-    pdl_wait();
-    if (st->halt) return;
     Topo* T = m.topo;
-    const int K = T->K;
+    const int K = T->K, C = T->C;
     if (K == 0) return;
-    T->M += K;
-    T->C += K;
-    T->maxId += K;
-    T->changed = 1;
-    T->K = 0;
-}
-
-// New nodes are bound to the lattice at once (GeometryHandler.cpp:427-428):
-// their old position is 5 lu away, so the edge test of
-// connectGeometryNodesToPhysicalNodes applies (GeometryHandler.cpp:618-636).
-__global__ void new_node_edge_kernel(MembraneDev m, int nx, int ny, Status* st, int from) {
-    pdl_wait();
-    if (st->halt) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.topo->M) return;
-    const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
-    const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
-    if (within) return;
-    if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
-    else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
-    else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
-    else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
+    if (c < C + K) {
+        m.ca[c] = t.ca2[c]; m.cb[c] = t.cb2[c]; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&T->done, 1u) == gridDim.x - 1) {
+            T->M += K;
+            T->C += K;
+            T->maxId += K;
+            T->changed = 1;
+            T->K = 0;
+            T->done = 0;
+        }
+    }
 }
 
 // After the device pass: a connection still longer than MAXLENGTH (a split
 // half of one longer than 2 * MAXLENGTH) needs another pass; that rare case
 // goes to the host, which repeats passes like SimulationRunner.cpp:190-199.
-__global__ void remesh_again_kernel(MembraneDev m, Status* st) {
+// Then the new nodes are bound to the lattice at once
+// (GeometryHandler.cpp:427-428): their old position is 5 lu away, so the edge
+// test of connectGeometryNodesToPhysicalNodes applies (GeometryHandler.cpp:
+// 618-636); the other nodes pass it as they did after the move.
+__global__ void remesh_again_kernel(MembraneDev m, int nx, int ny, Status* st) {
     pdl_wait();
     if (st->halt) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.topo->C) return;
-    const int a = m.ca[c], b = m.cb[c];
-    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-    if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
+    const int stride = gridDim.x * blockDim.x;
+    const int C = m.topo->C, M = m.topo->M;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += stride) {
+        const int a = m.ca[c], b = m.cb[c];
+        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+        if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
+        const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
+        const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
+        if (within || st->halt) continue;
+        if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
+        else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
+        else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
+        else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
+    }
 }
 
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
@@ -189,13 +183,10 @@ int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaSt
     cudaMemsetAsync(nRng, 0, sizeof(int), s);
     launch_pdl(remesh_flag_kernel, cb, 256, 0, s, m, t, st, nRng);
     cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
-    launch_pdl(remesh_decide_kernel, 1, 1, 0, s, m, t, st, nRng, 0);
-    launch_pdl(remesh_apply_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
+    launch_pdl(remesh_apply_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st, (const int*)nRng);
     launch_pdl(remesh_copy_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
-    launch_pdl(remesh_commit_kernel, 1, 1, 0, s, m, st);
-    launch_pdl(remesh_again_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, st);
-    launch_pdl(new_node_edge_kernel, (m.Mcap + 255) / 256, 256, 0, s, m, nx, ny, st, 0);
-    return 9;
+    launch_pdl(remesh_again_kernel, (std::max(m.Ccap, m.Mcap) + 255) / 256, 256, 0, s, m, nx, ny, st);
+    return 6;
 }
 
 // ---------------------------------------------------------------------------

@@ -15,7 +15,7 @@ struct Topo {
     int K;            // connections split by the current remesh pass
     int removed;      // nodes removed by the current coarsening
     int nCand;        // coarsening candidates
-    int pad;
+    unsigned done;    // blocks of the remesh copy that have finished (the last one commits)
 };
 
 // Membrane state on the device (nodes in ascending id order).
