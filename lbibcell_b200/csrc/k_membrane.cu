@@ -59,8 +59,14 @@ __device__ __forceinline__ double dirac(const double dx, const double dy) {
 
 // ---------------------------------------------------------------------------
 // Force evaluation
+__device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid);
+__device__ void tile_slot_node(const MembraneDev& m, TileDev& t, int i, bool ok, int nx, int ny, Status* st);
+
 // `begin`: also reset the step's counters (the first kernel of a step).
-__global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration, int begin) {
+// `slots`: also enter the node in the per-tile lists of the FP32-shifted
+// spread (the tile counts were cleared before the launch).
+__global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration, int begin, TileDev t, int nx,
+                                  int ny, int slots) {
     pdl_wait();
     if (st->halt) return;
     if (begin && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -132,15 +138,25 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration,
     }
     m.fx[i] = Fx;
     m.fy[i] = Fy;
+    if (slots) tile_slot_node(m, t, i, true, nx, ny, st);
 }
 
 template <typename Real>
-void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin) {
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin,
+                       TileDev* tiles, int nx, int ny) {
     if (m.Mcap == 0) return;
-    launch_pdl(force_eval_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st, iteration, begin ? 1 : 0);
+    TileDev t{};
+    if (tiles) {
+        t = *tiles;
+        cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
+    }
+    launch_pdl(force_eval_kernel, (m.Mcap + 127) / 128, 128, 0, s, m, st, iteration, begin ? 1 : 0, t, nx, ny,
+               tiles ? 1 : 0);
 }
-template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool);
-template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool);
+template void launch_force_eval<double>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool, TileDev*, int,
+                                        int);
+template void launch_force_eval<float>(const MembraneDev&, Status*, unsigned, cudaStream_t, bool, TileDev*, int,
+                                       int);
 
 // ---------------------------------------------------------------------------
 // Spreading
@@ -202,6 +218,34 @@ __device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid) {
     return base + __popc(grp & ((1u << lane) - 1u));
 }
 
+// FP32-shifted runs: node i into the fixed-size slot lists of the (up to 2 x 2)
+// tiles its stencil covers.
+__device__ void tile_slot_node(const MembraneDev& m, TileDev& t, int i, bool ok, int nx, int ny, Status* st) {
+    Stencil sc{0, 0, 0, 0};
+    if (ok && !stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
+        raise_error(st, ERR_STENCIL, i, ST_SPREAD);
+        ok = false;
+    }
+    const int tx0 = sc.x0 / kTile, tx1 = sc.x1 / kTile, ty0 = sc.y0 / kTile, ty1 = sc.y1 / kTile;
+    for (int j = 0; j < 4; ++j) {
+        const int tx = tx0 + (j & 1), ty = ty0 + (j >> 1);
+        const bool v = ok && tx <= tx1 && ty <= ty1;
+        const int tile = v ? ty * t.tilesX + tx : -1;
+        const int slot = tile_agg_add(t.count, tile, v);
+        if (v) {
+            if (slot < kTileSlots) t.slots[(size_t)tile * kTileSlots + slot] = i;
+            else raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
+        }
+    }
+}
+
+__global__ void tile_slot_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    tile_slot_node(m, t, i, i < m.topo->M, nx, ny, st);
+}
+
 __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Status* st, int pass) {
     pdl_wait();
     if (st->halt) return;
@@ -220,13 +264,6 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
         const int tile = v ? ty * t.tilesX + tx : -1;
         if (pass == 0) {
             tile_agg_add(t.count, tile, v);
-        } else if (pass == 2) {
-            // FP32-shifted runs: one pass into fixed-size per-tile slots
-            const int slot = tile_agg_add(t.count, tile, v);
-            if (v) {
-                if (slot < kTileSlots) t.slots[(size_t)tile * kTileSlots + slot] = i;
-                else raise_error(st, ERR_CAPACITY, tile, ST_SPREAD);
-            }
         } else {
             const int slot = tile_agg_add(t.fill, tile, v);
             if (v) {
@@ -459,13 +496,14 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
 
 template <typename Real>
 void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
-                   unsigned iteration, cudaStream_t s) {
-    cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
+                   unsigned iteration, cudaStream_t s, bool slotsFilled) {
+    if (!slotsFilled) cudaMemsetAsync(t.count, 0, sizeof(int) * (t.nTiles + 1), s);
     if (m.Mcap == 0) return;
     const int blocks = (m.Mcap + 127) / 128;
     if constexpr (sizeof(Real) == 4) {
-        // one pass into fixed per-tile slots, then the fixed-point scatter
-        launch_pdl(tile_count_kernel, blocks, 128, 0, s, m, t, nx, ny, st, 2);
+        // one pass into fixed per-tile slots (done by the force kernel when
+        // slotsFilled), then the fixed-point scatter
+        if (!slotsFilled) launch_pdl(tile_slot_kernel, blocks, 128, 0, s, m, t, nx, ny, st);
         launch_pdl(spread_fixed_kernel, t.nTiles, 256, 0, s, m, t, (float*)force, nx, ny, L, st);
     } else {
         // exact lists (count, scan, fill), then the ordered gather
@@ -482,9 +520,9 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
     }
 }
 template void launch_spread<double>(const MembraneDev&, TileDev&, double*, int, int, size_t, Status*, unsigned,
-                                    cudaStream_t);
+                                    cudaStream_t, bool);
 template void launch_spread<float>(const MembraneDev&, TileDev&, float*, int, int, size_t, Status*, unsigned,
-                                   cudaStream_t);
+                                   cudaStream_t, bool);
 
 // ---------------------------------------------------------------------------
 // Interpolation and motion

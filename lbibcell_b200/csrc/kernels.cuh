@@ -153,10 +153,13 @@ void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, 
 
 // Membrane pipeline.  `Real` is the lattice precision (velocity / force planes).
 template <typename Real>
-void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin = false);
+// `tiles`: also fill the FP32-shifted spread's per-tile slot lists (then call
+// launch_spread with slotsFilled).
+void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin = false,
+                       TileDev* tiles = nullptr, int nx = 0, int ny = 0);
 template <typename Real>
 void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny, size_t L, Status* st,
-                   unsigned iteration, cudaStream_t s);
+                   unsigned iteration, cudaStream_t s, bool slotsFilled = false);
 template <typename Real>
 void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
                         unsigned iteration, cudaStream_t s);

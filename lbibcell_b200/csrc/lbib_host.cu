@@ -867,14 +867,17 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
     const unsigned it = 0;  // kernels read the iteration from the status word
     long long nl = 0;
     if (fromStage <= ST_FORCE) {
-        // the step's counters are reset by the force kernel, or alone without a membrane
-        if (hasM) launch_force_eval<Real>(h.m, h.st, it, s, true);
+        // the step's counters are reset by the force kernel, or alone without a
+        // membrane; in FP32-shifted runs the force kernel also fills the
+        // spread's per-tile lists
+        if (hasM) launch_force_eval<Real>(h.m, h.st, it, s, true, sizeof(Real) == 4 ? &h.tiles : nullptr, h.nx, h.ny);
         else launch_pdl(step_begin_kernel, 1, 1, 0, s, h.st);
         nl += 1;
     }
     if (fromStage <= ST_SPREAD) {
-        launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s);
-        nl += hasM ? (sizeof(Real) == 8 ? 6 : 2) : 0;
+        const bool filled = sizeof(Real) == 4 && hasM && fromStage <= ST_FORCE;
+        launch_spread<Real>(h.m, h.tiles, (Real*)h.force, h.nx, h.ny, h.L, h.st, it, s, filled);
+        nl += hasM ? (sizeof(Real) == 8 ? 6 : (filled ? 1 : 2)) : 0;
     }
     if (fromStage <= ST_COLLIDE) {
         if (evCollideA) cudaEventRecord(evCollideA, s);
