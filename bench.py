@@ -3,7 +3,7 @@
 
 Workload: the 1024x1024 tissue (400 cells on a hexagonal grid, ~100k membrane
 nodes growing to ~150k after the first remesh, 2 D2Q5 species, tension, area
-regulator, box outlet) in lbibcell_b200/configs.py:config2.  A step is one full
+regulator, cell junctions, box outlet) in lbibcell_b200/configs.py:config2.  A step is one full
 iteration of SimulationRunner::runSimulation's loop body on the GPU.  The metric
 is MLUPS (lattice node updates per second / 1e6, all species included) of the
 FP32-shifted path; the FP64 path's MLUPS and the FP32-vs-FP64 field errors are
@@ -35,7 +35,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS FP32-shifted vs FP64 on 1 B200 @ rel.err≤1e-5; adjoint/forward time"
-WORKLOAD = "tissue_1024: 1024x1024 D2Q9 + 2 D2Q5 species, 400 cells (hex grid, spacing 44, r=20+U(-2,2), 250 nodes/cell), tension, area regulator (hold area), box outlet"
+WORKLOAD = ("tissue_1024: 1024x1024 D2Q9 + 2 D2Q5 species, 400 cells (hex grid, spacing 44, r=20+U(-2,2), "
+            "250 nodes/cell), tension, area regulator (hold area), cell junctions (radius 1 lu, k 0.02, "
+            "rest length 2 lu), box outlet")
 
 
 def parse():

@@ -214,7 +214,9 @@ def hex_tissue(nx: int, ny: int, spacing: float, r0: float, jitter: float, nodes
 def config2(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> Config:
     """1024x1024 tissue: 400 cells (20 x 20) on a hex grid (spacing 44), r=20+U(-2,2),
     250 nodes/cell, 2 species (tau 0.8, 1.2), secretion 1e-3/step from a seeded 10% of
-    the cells."""
+    the cells; membrane tension, area regulator and cell junctions (the
+    reference's tutorial_01 junction solver with a 2 lu rest length: springs
+    between nodes of different cells closer than 1 lu push them apart)."""
     cells = hex_tissue(1024, 1024, 44.0, 20.0, 2.0, 250, seed, cols=20, rows=20)
     rng = np.random.default_rng(seed + 1)
     doms = [d for d, _ in cells]
@@ -228,7 +230,8 @@ def config2(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> 
     # membranes, CDESolverD2Q5.cpp:223).  The area regulator holds each cell's
     # initial area here.
     return Config(name="tissue_1024", nx=1024, ny=1024, tau_fluid=1.0, iterations=iterations,
-                  report_step=report_step, cells=cells, species=species, area=(1.0, 0.01, 0.004))
+                  report_step=report_step, cells=cells, species=species, area=(1.0, 0.01, 0.004),
+                  bio=["LbibCellJunction\tradius\t1.0\tk\t0.02\tl0\t2.0"])
 
 
 def poisson_tissue(nx: int, ny: int, rmin: float, rmax: float, spacing: float, seed: int,

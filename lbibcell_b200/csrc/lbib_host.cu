@@ -56,6 +56,42 @@ struct HConn {
     std::string desc;
 };
 
+// Position of each node id in a node array: a dense table over the ids when
+// they are compact (the usual case: ids 1..n growing by remeshing), else a
+// binary search over the sorted (id, position) pairs.  at() throws
+// std::out_of_range for an absent id, as std::map::at does.
+struct IdIndex {
+    std::vector<int> dense;
+    std::vector<std::pair<uint32_t, int>> sorted;
+    explicit IdIndex(const std::vector<uint32_t>& ids) {
+        uint32_t mx = 0;
+        for (uint32_t id : ids) mx = std::max(mx, id);
+        if ((size_t)mx <= 8 * ids.size() + 1024) {
+            dense.assign((size_t)mx + 1, -1);
+            for (size_t i = 0; i < ids.size(); ++i) dense[ids[i]] = (int)i;
+        } else {
+            sorted.resize(ids.size());
+            for (size_t i = 0; i < ids.size(); ++i) sorted[i] = {ids[i], (int)i};
+            std::sort(sorted.begin(), sorted.end());
+        }
+    }
+    // position of id, or -1
+    int find(uint32_t id) const {
+        if (sorted.empty()) return id < dense.size() ? dense[id] : -1;
+        auto it = std::lower_bound(sorted.begin(), sorted.end(), std::make_pair(id, -1));
+        return it != sorted.end() && it->first == id ? it->second : -1;
+    }
+    int at(uint32_t id) const {
+        if (sorted.empty()) {
+            if (id < dense.size() && dense[id] >= 0) return dense[id];
+        } else {
+            auto it = std::lower_bound(sorted.begin(), sorted.end(), std::make_pair(id, -1));
+            if (it != sorted.end() && it->first == id) return it->second;
+        }
+        throw std::out_of_range("node id");
+    }
+};
+
 struct HForce {
     uint32_t type, id1, id2;
     double p[4];
@@ -308,7 +344,9 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 if (kv.count("frequency")) h.tensionFreq = (unsigned)kv["frequency"];
                 if (h.tensionFreq == 0) fail(ERR_INPUT, "tension frequency must be positive");
             } else if (name == "tutorial_01_BioSolverCellJunction" || name == "tutorial_02_BioSolverCellJunction" ||
-                       name == "BioSolverCellJunction") {
+                       name == "BioSolverCellJunction" || name == "LbibCellJunction") {
+                // the reference's solvers take no parameters; LbibCellJunction is
+                // the same solver with radius, k and l0 from the plugin file
                 h.bio.push_back(3);
                 if (kv.count("radius")) h.junctionRadius = kv["radius"];
                 if (kv.count("k")) h.junctionK = kv["k"];
@@ -388,8 +426,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells);
 static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces) {
     const int M = (int)h.ids.size();
     const int C = (int)h.conns.size();
-    std::map<uint32_t, int> index;
-    for (int i = 0; i < M; ++i) index[h.ids[i]] = i;
+    const IdIndex index(h.ids);
     std::vector<int> ca(C), cb(C), prev(M, -1), next(M, -1), cdesc(C);
     std::vector<uint32_t> cdom(C);
     for (int c = 0; c < C; ++c) {
@@ -439,8 +476,7 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
                 ftype.push_back((int)f.type);
                 int j = -1;
                 if (f.type == 0 || f.type == 7 || f.type == 5 || f.type == 6) {
-                    auto jt = index.find(f.id2);
-                    j = jt == index.end() ? -1 : jt->second;
+                    j = index.find(f.id2);
                 }
                 fpart.push_back(j);
                 for (int q = 0; q < 4; ++q) fpar.push_back(f.p[q]);
@@ -449,7 +485,7 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
         foff[M] = (int)ftype.size();
         // forces on ids that are not membrane nodes fail like nodes.at() would
         for (auto& kv : h.forcemap)
-            if (!kv.second.empty() && !index.count(kv.first)) fail(ERR_FORCE_NODE, "Could not compute and set the forces.", kv.first);
+            if (!kv.second.empty() && index.find(kv.first) < 0) fail(ERR_FORCE_NODE, "Could not compute and set the forces.", kv.first);
     }
     ensure_capacity(h, M, C, 1, cells);
     // room for the loaded records plus the bio solvers' own: two tension records
@@ -725,8 +761,7 @@ static void perturbate(Handle& h, double& x, double& y) {
 // GeometryHandler::perturbConnections + Connection::perturbConnection
 // (GeometryHandler.cpp:326-356, Connection.cpp:332-387) on the host copy.
 static void perturb_connections(Handle& h, HostMembrane& hm) {
-    std::map<uint32_t, int> index;
-    for (size_t i = 0; i < h.ids.size(); ++i) index[h.ids[i]] = (int)i;
+    const IdIndex index(h.ids);
     std::map<uint32_t, int> first;
     for (size_t c = 0; c < h.conns.size(); ++c)
         if (!first.count(h.conns[c].dom)) first[h.conns[c].dom] = (int)c;
@@ -763,8 +798,7 @@ static void perturb_connections(Handle& h, HostMembrane& hm) {
 static bool remesh(Handle& h, HostMembrane& hm) {
     bool any = false;
     for (;;) {
-        std::map<uint32_t, int> index;
-        for (size_t i = 0; i < h.ids.size(); ++i) index[h.ids[i]] = (int)i;
+        const IdIndex index(h.ids);
         std::vector<HConn> kept, added;
         kept.reserve(h.conns.size());
         for (const HConn& c : h.conns) {

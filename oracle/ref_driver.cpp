@@ -105,6 +105,10 @@ PluginList loadPlugins(const std::string& fn) {
                     if (k == "factor") reg.area.factor = v;
                     if (k == "strength") reg.area.strength = v;
                     if (k == "maxsource") reg.area.maxsource = v;
+                } else if (name == "LbibCellJunction") {
+                    if (k == "radius") reg.junction.radius = v;
+                    if (k == "k") reg.junction.k = v;
+                    if (k == "l0") reg.junction.l0 = v;
                 }
             }
         } else if (kind == "CDE") {

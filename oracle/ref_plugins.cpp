@@ -12,6 +12,11 @@
 //                         every `frequency` iterations (as tutorial_01's).
 //   LbibAreaRegulator     per-cell mass source strength*(target-A)/target,
 //                         clamped to +-maxsource, target = factor * first A.
+//   LbibCellJunction      the cell-junction solver of tutorial_01 (every 10th
+//                         iteration: drop type-7 forces, then for each node in
+//                         id order a type-7 spring each way to the closest node
+//                         of another cell within `radius`) with radius, spring
+//                         constant k and rest length l0 from the plugin file.
 //   LbibCDESolverD2Q5_A/B/C  D2Q5 species with R = source[domain] - decay*C,
 //                         added as dt*R/3 (rest) and dt*R/6 (moving) like
 //                         tutorial_01_CDESolverD2Q5_SIGNAL.cpp:102-135.
@@ -99,6 +104,34 @@ class LbibAreaRegulator : public BioBaseSolver<LbibAreaRegulator> {
     std::map<unsigned int, double> target_;
 };
 const std::string LbibAreaRegulator::name = "LbibAreaRegulator";
+
+// ---------------------------------------------------------------------------
+class LbibCellJunction : public BioBaseSolver<LbibCellJunction> {
+ public:
+    LbibCellJunction();
+    virtual void applyBioProcess(geometry::GeometryHandler& gh, solver::ForceSolver& fs) {
+        if (Parameters.getCurrentIteration() % 10 != 0) return;
+        const auto& p = lbibref::registry().junction;
+        fs.deleteForceType(7);
+        const auto nodes = gh.getGeometry().getGeometryNodes();  // id order
+        std::stringstream d;
+        for (const auto& kv : nodes) {
+            const auto& n = kv.second;
+            const std::shared_ptr<nodes::GeometryNode> other =
+                gh.getGeometry().getGeometryNodesWithinRadiusWithAvoidanceClosest(
+                    n->getXPos(), n->getYPos(), p.radius, n->getDomainIdOfAdjacentConnections());
+            if (other == nullptr) continue;
+            d.str(std::string()); d.clear();
+            d << "7\t" << n->getId() << "\t" << other->getId() << "\t" << p.k << "\t" << p.l0;
+            fs.addForce(&d);
+            d.str(std::string()); d.clear();
+            d << "7\t" << other->getId() << "\t" << n->getId() << "\t" << p.k << "\t" << p.l0;
+            fs.addForce(&d);
+        }
+    }
+    static const std::string name;
+};
+const std::string LbibCellJunction::name = "LbibCellJunction";
 
 // ---------------------------------------------------------------------------
 template <class Self>
@@ -252,6 +285,7 @@ LbibCDESolverD2Q5_B::LbibCDESolverD2Q5_B() {}
 LbibCDESolverD2Q5_C::LbibCDESolverD2Q5_C() {}
 LbibMembraneTension::LbibMembraneTension() : BioBaseSolver() {}
 LbibAreaRegulator::LbibAreaRegulator() : BioBaseSolver() {}
+LbibCellJunction::LbibCellJunction() : BioBaseSolver() {}
 
 }  // namespace solver
 }  // namespace LbmLib

@@ -8,10 +8,10 @@ oracle/Makefile, parity flags, OMP_NUM_THREADS=1) and stores:
 * ``config1_digest.json`` -- SHA-256 digests of every state array of the 200x200
   single-cell configuration at t = 0, 500, 1000, 1500, 2000.
 * ``tissue1024_digest.json`` -- the same for the 1024x1024 tissue of 400 cells
-  (2 species) at t = 0, 70, 80.  Between 70 and 80 the reference's species
-  re-initialisation divides 0 by 0 for a node trapped between two touching
-  membranes (CDESolverD2Q5.cpp:156-228); NaN values are hashed as one canonical
-  NaN, since x86 and CUDA give 0/0 different sign bits.
+  (2 species, tension, area regulator, cell junctions) at t = 0, 70, 80.  The
+  reference's species re-initialisation divides 0 by 0 for nodes trapped
+  between touching membranes (CDESolverD2Q5.cpp:156-228); NaN values are
+  hashed as one canonical NaN, since x86 and CUDA give 0/0 different sign bits.
 
 Usage (needs the reference sources, i.e. only in the build container):
     make -C oracle ref && python tests/golden/make_golden.py [toy48 config1 tissue1024]

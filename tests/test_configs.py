@@ -32,6 +32,7 @@ def test_config2_shape():
     cfg = configs.config2()
     assert cfg.nx == 1024 and len(cfg.species) == 2
     assert len(cfg.cells) == 400
+    assert cfg.bio[0].split("\t")[0] == "LbibCellJunction"
     doms = [d for d, _ in cfg.cells]
     assert len(set(doms)) == len(doms)
     for _, v in cfg.cells:

@@ -122,10 +122,11 @@ def test_config1_fp64_matches_reference_digests(lbib, tmp_path):
 
 
 def test_tissue1024_fp64_matches_reference_digests(lbib, tmp_path):
-    """The benchmark workload at full size (1024x1024, 400 cells, 2 species):
-    every array identical to the reference build's at t = 0, 70, 80, including
-    the NaN that the reference's species re-initialisation produces between 70
-    and 80 for a node trapped between two touching membranes."""
+    """The benchmark workload at full size (1024x1024, 400 cells, 2 species,
+    tension, area regulator, cell junctions): every array identical to the
+    reference build's at t = 0, 70, 80, including the NaN values that the
+    reference's species re-initialisation produces for nodes trapped between
+    touching membranes."""
     dig = json.load(open(os.path.join(GOLD, "tissue1024_digest.json")))
     sim = lbib.Simulation(configs.config2(iterations=80, report_step=10).write(str(tmp_path)), lbib.FP64)
     prev = 0
