@@ -153,10 +153,10 @@ size_t force_scan_bytes(int n) {
     return b;
 }
 
-size_t junction_sort_bytes(int n) {
+size_t junction_sort_bytes(int n, int bits) {
     size_t b = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned*)nullptr, (unsigned*)nullptr, (const int*)nullptr,
-                                    (int*)nullptr, n, 0, 32, (cudaStream_t)0);
+                                    (int*)nullptr, n, 0, bits, (cudaStream_t)0);
     return b;
 }
 
@@ -199,22 +199,29 @@ __global__ void junction_bin_kernel(MembraneDev m, ForceScratch fs, int nx, int 
     pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.Mcap) return;
-    unsigned key = 0xffffffffu;  // unused slots sort last
+    unsigned key = (unsigned)nx * (unsigned)ny;  // unused slots sort last
     if (i < m.topo->M) key = (unsigned)bin_index(m.y[i], ny) * (unsigned)nx + (unsigned)bin_index(m.x[i], nx);
     fs.binKey[i] = key;
     fs.binIdx[i] = i;
 }
 
-// First position of `key` in the sorted keys (n entries).
-__device__ __forceinline__ int lower_bound_key(const unsigned* keys, int n, unsigned key) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (keys[mid] < key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
+// binStart[key] = first sorted position of each bin present.  Entries of
+// bins absent now keep old values; a lookup checks the key found there.
+__global__ void bin_start_kernel(MembraneDev m, ForceScratch fs) {
+    pdl_wait();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= m.Mcap) return;
+    const unsigned key = fs.binKeySorted[p];
+    if (key >= fs.binCap) return;
+    if (p == 0 || fs.binKeySorted[p - 1] != key) fs.binStart[key] = p;
 }
+
+// First sorted position of bin `key`, or Mcap when the bin is empty.
+__device__ __forceinline__ int bin_first(const ForceScratch& fs, int mcap, unsigned key) {
+    const int p = fs.binStart[key];
+    return (p >= 0 && p < mcap && fs.binKeySorted[p] == key) ? p : mcap;
+}
+
 
 // The query of node i: candidates in the order the cell list returns them
 // (bins by row, then column, within a bin in id order: the list is rebuilt from
@@ -236,7 +243,7 @@ __global__ void junction_query_kernel(MembraneDev m, ForceScratch fs, int nx, in
     for (int by = by0; by <= by1; ++by)
         for (int bx = bx0; bx <= bx1; ++bx) {
             const unsigned key = (unsigned)by * (unsigned)nx + (unsigned)bx;
-            for (int q = lower_bound_key(fs.binKeySorted, m.Mcap, key); q < m.Mcap && fs.binKeySorted[q] == key;
+            for (int q = bin_first(fs, m.Mcap, key); q < m.Mcap && fs.binKeySorted[q] == key;
                  ++q) {
                 const int j = fs.binIdxSorted[q];
                 const double xj = m.x[j], yj = m.y[j];
@@ -276,8 +283,9 @@ int launch_cell_list(MembraneDev& m, ForceScratch& fs, int nx, int ny, cudaStrea
     launch_pdl(conn_pos_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, fs);
     launch_pdl(junction_bin_kernel, (n + 255) / 256, 256, 0, s, m, fs, nx, ny);
     cub::DeviceRadixSort::SortPairs(fs.sortTmp, fs.sortTmpBytes, fs.binKey, fs.binKeySorted, fs.binIdx,
-                                    fs.binIdxSorted, n, 0, 32, s);
-    return 2;
+                                    fs.binIdxSorted, n, 0, fs.sortBits, s);
+    launch_pdl(bin_start_kernel, (n + 255) / 256, 256, 0, s, m, fs);
+    return 3;
 }
 
 // Range queries for host plugins, on the cell list of launch_cell_list: hits in
@@ -301,7 +309,7 @@ __global__ void range_query_kernel(MembraneDev m, ForceScratch fs, int nx, int n
     for (int by = by0; by <= by1; ++by)
         for (int bx = bx0; bx <= bx1; ++bx) {
             const unsigned key = (unsigned)by * (unsigned)nx + (unsigned)bx;
-            for (int p = lower_bound_key(fs.binKeySorted, m.Mcap, key); p < m.Mcap && fs.binKeySorted[p] == key;
+            for (int p = bin_first(fs, m.Mcap, key); p < m.Mcap && fs.binKeySorted[p] == key;
                  ++p) {
                 const int j = fs.binIdxSorted[p];
                 const double xj = m.x[j], yj = m.y[j];

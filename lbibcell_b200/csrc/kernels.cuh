@@ -59,6 +59,9 @@ struct ForceScratch {
     unsigned* binKey; unsigned* binKeySorted;  // Mcap: cell-list bin of each node
     int* binIdx; int* binIdxSorted;            // Mcap: node index
     void* sortTmp; size_t sortTmpBytes;
+    int sortBits;               // key bits: bins 0..nx*ny-1, nx*ny for unused slots
+    int* binStart;              // nx*ny: first sorted position of each bin (checked on use)
+    unsigned binCap;            // nx*ny
     int* closest;               // Mcap: closest node of another cell within the radius, -1: none
     int* inCnt; int* inOff;     // Mcap+1: nodes that found node i, and their offsets
     int* inList; int* inFill;   // Mcap
@@ -197,7 +200,7 @@ int launch_cell_list(MembraneDev& m, ForceScratch& fs, int nx, int ny, cudaStrea
 void launch_range_query(MembraneDev& m, ForceScratch& fs, int nx, int ny, const double* qx, const double* qy,
                         const long long* avoid, int nq, double radius, int mode, unsigned* ids, int cap, int* count,
                         long long* closest, cudaStream_t s);
-size_t junction_sort_bytes(int n);
+size_t junction_sort_bytes(int n, int bits);
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s);
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const Status* st, cudaStream_t s);

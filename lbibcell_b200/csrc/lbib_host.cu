@@ -276,6 +276,7 @@ Handle::~Handle() {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
     fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
+    fr(fs.binStart);
     fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -598,6 +599,7 @@ static void ensure_force_scratch(Handle& h, bool need = false) {
     ForceScratch& fs = h.fs;
     fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
     fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
+    fr(fs.binStart);
     fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
     fs = ForceScratch{};
     fs.outPos = h.outPos;
@@ -614,8 +616,13 @@ static void ensure_force_scratch(Handle& h, bool need = false) {
     if (junction) {
         fs.binKey = dalloc<unsigned>(n); fs.binKeySorted = dalloc<unsigned>(n);
         fs.binIdx = dalloc<int>(n); fs.binIdxSorted = dalloc<int>(n);
-        fs.sortTmpBytes = junction_sort_bytes(n);
+        fs.sortBits = 1;
+        while ((1ull << fs.sortBits) <= (unsigned long long)h.L && fs.sortBits < 32) ++fs.sortBits;
+        fs.sortTmpBytes = junction_sort_bytes(n, fs.sortBits);
         CK(cudaMalloc(&fs.sortTmp, fs.sortTmpBytes));
+        fs.binCap = (unsigned)h.L;
+        fs.binStart = dalloc<int>(h.L);
+        CK(cudaMemsetAsync(fs.binStart, 0xff, sizeof(int) * h.L, h.stream));
         fs.closest = dalloc<int>(n);
         fs.inCnt = dalloc<int>(n + 1); fs.inOff = dalloc<int>(n + 1);
         fs.inList = dalloc<int>(n); fs.inFill = dalloc<int>(n);
