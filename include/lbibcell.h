@@ -215,6 +215,29 @@ int lbib_delete_force_type(lbib_handle* h, int type);
 /* ForceSolver::deleteAllForces (ForceSolver.cpp:170-181). */
 int lbib_delete_all_forces(lbib_handle* h);
 
+/* The membrane after a host bio solver's topology edits between steps (a cell
+ * division, growth): Geometry::addGeometryNode / removeGeometryNode /
+ * addConnection / eraseConnection (Geometry.cpp:381-452), given as the
+ * resulting lists.  ids[M] ascend; xy[2M] are the positions; conns[3C] hold
+ * (id1, id2, domain) per connection in vector order, each closed ring one
+ * cell.  Nodes that existed keep their velocity, force and old position; new
+ * ones start as a new GeometryNode does (perturbed, GeometryNode.cpp:98-117,
+ * at rest).  Force records of removed nodes, or toward them, are dropped; the
+ * others keep their order.  A connection keeps its boundary descriptor when
+ * one with the same (id1, id2) existed, else has none.  New domain ids get
+ * cell type 1 and no species production (lbib_set_species_source sets it).
+ * Domain ids of the lattice follow at the next step's crossings, or at once
+ * after lbib_cure_lattice, as after the reference plugin's cureLattice. */
+int lbib_upload_membrane(lbib_handle* h, const unsigned* ids, const double* xy, int M, const unsigned* conns,
+                         int C);
+
+/* GeometryHandler::cureLattice (GeometryHandler.cpp:149-170), which a host
+ * plugin calls after its topology edits (tutorial_01_BioSolverCellDivision.cpp
+ * :84): perturbConnections, the edge test of every node, new boundary nodes,
+ * and every lattice node's domain id set at once (no species
+ * re-initialisation, as in the reference). */
+int lbib_cure_lattice(lbib_handle* h);
+
 /* Geometry::getGeometryNodesWithinRadius (Geometry.cpp:306-323), or with
  * avoidDomain >= 0 getGeometryNodesWithinRadiusWithAvoidance (:325-348): the
  * ids of the membrane nodes within `radius` of (x, y) (distance <= radius),

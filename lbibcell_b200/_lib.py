@@ -19,7 +19,7 @@ SYMBOLS = (
     "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
     "lbib_write_simulation", "lbib_load_solvers", "lbib_add_forces", "lbib_delete_force_type",
     "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes", "lbib_write_vtk",
-    "lbib_read_vtm_geometry",
+    "lbib_read_vtm_geometry", "lbib_upload_membrane", "lbib_cure_lattice",
 )
 
 _lib = None
@@ -96,6 +96,10 @@ def load() -> ctypes.CDLL:
     L.lbib_nodes_within_radius.restype = ip
     L.lbib_nodes_within_radius.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_longlong, vp, ip]
+    L.lbib_cure_lattice.restype = ip
+    L.lbib_cure_lattice.argtypes = [vp]
+    L.lbib_upload_membrane.restype = ip
+    L.lbib_upload_membrane.argtypes = [vp, vp, vp, ip, vp, ip]
     L.lbib_write_vtk.restype = ip
     L.lbib_write_vtk.argtypes = [vp, cp, ctypes.c_uint, ip, ip]
     L.lbib_read_vtm_geometry.restype = ip

@@ -2674,3 +2674,173 @@ int lbib_write_vtk(lbib_handle* hh, const char* prefix, unsigned time, int kind,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Topology edits by a host bio solver (a cell division, a growth step):
+// the Geometry calls addGeometryNode / removeGeometryNode / addConnection /
+// eraseConnection (Geometry.cpp:381-452) made between steps, given as the
+// resulting node and connection lists.
+
+namespace lbib {
+
+// Widens the per-domain tables to nd domains (new domains: no mass source, no
+// species production, cell type 1 as the text geometry loader gives).
+static void grow_domains(Handle& h, int nd) {
+    if (nd <= h.nDomains) return;
+    const int old = h.nDomains;
+    double* mt = dalloc<double>(nd);
+    CK(cudaMemsetAsync(mt, 0, sizeof(double) * nd, h.stream));
+    CK(cudaMemcpyAsync(mt, h.massTab, sizeof(double) * old, cudaMemcpyDeviceToDevice, h.stream));
+    const int S = std::max(1, h.S);
+    double* st = dalloc<double>((size_t)S * nd);
+    CK(cudaMemsetAsync(st, 0, sizeof(double) * S * nd, h.stream));
+    for (int k = 0; k < S; ++k)
+        CK(cudaMemcpyAsync(st + (size_t)k * nd, h.srcTab + (size_t)k * old, sizeof(double) * old,
+                           cudaMemcpyDeviceToDevice, h.stream));
+    h.ctypeHost.resize(nd, 1u);
+    uint32_t* ct = dalloc<uint32_t>(nd);
+    CK(cudaMemcpyAsync(ct, h.ctypeHost.data(), sizeof(uint32_t) * nd, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    cudaFree(h.massTab); cudaFree(h.srcTab); cudaFree(h.ctypeTab);
+    h.massTab = mt; h.srcTab = st; h.ctypeTab = ct;
+    cudaFree(h.td.cellOfDom); cudaFree(h.td.firstConn);  // re-made for nd by upload_topology
+    h.td.cellOfDom = nullptr; h.td.firstConn = nullptr;
+    h.nDomains = nd;
+    h.graphEpoch++;
+}
+
+// The device table of boundary solvers has one entry per descriptor string; a
+// string first seen now gets an entry with no solvers.
+static void ensure_descriptor(Handle& h, const std::string& desc) {
+    if (std::find(h.descTable.begin(), h.descTable.end(), desc) != h.descTable.end()) return;
+    h.descTable.push_back(desc);
+    if (!h.nfTabDev) return;
+    const size_t n = h.descTable.size();
+    NfSpec* t = dalloc<NfSpec>(n);
+    CK(cudaMemsetAsync(t, 0, sizeof(NfSpec) * n, h.stream));
+    CK(cudaMemcpyAsync(t, h.nfTabDev, sizeof(NfSpec) * (n - 1), cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    cudaFree(h.nfTabDev);
+    h.nfTabDev = t;
+    h.cross.nfTab = t;
+    h.graphEpoch++;
+}
+
+}  // namespace lbib
+
+extern "C" {
+
+int lbib_upload_membrane(lbib_handle* hh, const unsigned* ids, const double* xy, int M, const unsigned* conns,
+                         int C) {
+    if (M < 0 || C < 0 || (M > 0 && (!ids || !xy)) || (C > 0 && !conns)) return LBIB_ERR_INPUT;
+    API_BEGIN(hh)
+    if (h.diff) lbib::fail(LBIB_ERR_STATE, "topology edits are not possible during a differentiated run");
+    for (int k = 1; k < M; ++k)
+        if (ids[k] <= ids[k - 1]) lbib::fail(LBIB_ERR_INPUT, "node ids must ascend", k);
+    lbib::pull_topology(h);
+    lbib::HostMembrane old;
+    lbib::download_membrane(h, old);
+    lbib::sync_targets(h);
+    const lbib::IdIndex oldIdx(h.ids);
+    const std::vector<uint32_t> oldIds = h.ids;
+    // the force list, remapped by node id; records of removed nodes go
+    std::vector<int> foff(h.m.M + 1);
+    CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (h.m.M + 1), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    const int R = foff[h.m.M];
+    std::vector<int> ftype(R), fpart(R);
+    std::vector<double> fpar(4 * (size_t)R);
+    if (R) {
+        CK(cudaMemcpyAsync(ftype.data(), h.m.ftype, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(fpart.data(), h.m.fpartner, sizeof(int) * R, cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaMemcpyAsync(fpar.data(), h.m.fpar, sizeof(double) * fpar.size(), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+    }
+    // the new node arrays: kept nodes keep their state, new ones start like a
+    // GeometryNode created at (x, y) (perturbed, old position 5 lu away, at rest)
+    std::vector<uint32_t> newIds(ids, ids + M);
+    lbib::HostMembrane hm;
+    for (int k = 0; k < M; ++k) {
+        double x = xy[2 * k], y = xy[2 * k + 1];
+        const int o = oldIdx.find(newIds[k]);
+        if (o >= 0) {
+            hm.ox.push_back(old.ox[o]); hm.oy.push_back(old.oy[o]);
+            hm.vx.push_back(old.vx[o]); hm.vy.push_back(old.vy[o]);
+            hm.fx.push_back(old.fx[o]); hm.fy.push_back(old.fy[o]);
+        } else {
+            lbib::perturbate(h, x, y);
+            hm.ox.push_back(x - 5.0); hm.oy.push_back(y - 5.0);
+            hm.vx.push_back(0.0); hm.vy.push_back(0.0); hm.fx.push_back(0.0); hm.fy.push_back(0.0);
+        }
+        hm.x.push_back(x);
+        hm.y.push_back(y);
+    }
+    const lbib::IdIndex newIdx(newIds);
+    std::vector<int> nfoff(M + 1, 0), nftype, nfpart;
+    std::vector<double> nfpar;
+    for (int k = 0; k < M; ++k) {
+        const int o = oldIdx.find(newIds[k]);
+        if (o >= 0)
+            for (int r = foff[o]; r < foff[o + 1]; ++r) {
+                int p = fpart[r];
+                if (p >= 0) {
+                    p = p < (int)oldIds.size() ? newIdx.find(oldIds[p]) : -1;
+                    if (p < 0) continue;  // its partner was removed
+                }
+                nftype.push_back(ftype[r]);
+                nfpart.push_back(p);
+                for (int q = 0; q < 4; ++q) nfpar.push_back(fpar[4 * (size_t)r + q]);
+            }
+        nfoff[k + 1] = (int)nftype.size();
+    }
+    // connections keep their boundary descriptor; new ones have none
+    std::map<std::pair<uint32_t, uint32_t>, std::string> oldDesc;
+    for (const auto& c : h.conns) oldDesc[{c.id1, c.id2}] = c.desc;
+    std::vector<lbib::HConn> nc(C);
+    uint32_t maxDom = 0;
+    for (int c = 0; c < C; ++c) {
+        nc[c].id1 = conns[3 * c];
+        nc[c].id2 = conns[3 * c + 1];
+        nc[c].dom = conns[3 * c + 2];
+        if (newIdx.find(nc[c].id1) < 0 || newIdx.find(nc[c].id2) < 0)
+            lbib::fail(LBIB_ERR_INPUT, "a connection names a node that is not in the list", c);
+        auto it = oldDesc.find({nc[c].id1, nc[c].id2});
+        nc[c].desc = it == oldDesc.end() ? std::string() : it->second;
+        lbib::ensure_descriptor(h, nc[c].desc);
+        maxDom = std::max(maxDom, nc[c].dom);
+    }
+    lbib::grow_domains(h, (int)maxDom + 1);
+    h.ids = newIds;
+    h.conns = nc;
+    h.keepRecords = (int)nftype.size();
+    lbib::upload_topology(h, hm, false);
+    h.keepRecords = 0;
+    CK(cudaMemcpyAsync(h.m.foff, nfoff.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice, h.stream));
+    if (!nftype.empty()) {
+        CK(cudaMemcpyAsync(h.m.ftype, nftype.data(), sizeof(int) * nftype.size(), cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.fpartner, nfpart.data(), sizeof(int) * nfpart.size(), cudaMemcpyHostToDevice,
+                           h.stream));
+        CK(cudaMemcpyAsync(h.m.fpar, nfpar.data(), sizeof(double) * nfpar.size(), cudaMemcpyHostToDevice,
+                           h.stream));
+    }
+    // new nodes are bound to the lattice at once: the edge test of
+    // connectGeometryNodesToPhysicalNodes (GeometryHandler.cpp:618-636)
+    lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+    lbib::launch_edge_check(h.m, h.nx, h.ny, h.st, 0, h.stream);
+    lbib::read_status(h);
+    if (h.stHost->err) lbib::fail(h.stHost->err, "geometry point moved too close to the boundary", h.stHost->errIndex);
+    h.graphEpoch++;
+    API_END
+}
+
+int lbib_cure_lattice(lbib_handle* hh) {
+    API_BEGIN(hh)
+    if (h.diff) lbib::fail(LBIB_ERR_STATE, "topology edits are not possible during a differentiated run");
+    lbib::pull_topology(h);
+    lbib::HostMembrane hm;
+    lbib::download_membrane(h, hm);
+    lbib::cure_lattice(h, hm);
+    API_END
+}
+
+}  // extern "C"

@@ -150,6 +150,21 @@ class Simulation:
             raise self._error()
         return {int(d[i]): float(a[i]) for i in range(n)}
 
+    # -- topology edits by host bio solvers -----------------------------------------
+    def upload_membrane(self, ids, xy, conns) -> None:
+        """The membrane after a host plugin's edits (see lbib_upload_membrane):
+        ids (M,) ascending, xy (M, 2), conns (C, 3) = id1, id2, domain."""
+        i = np.ascontiguousarray(ids, np.uint32)
+        p = np.ascontiguousarray(xy, np.float64).reshape(-1, 2)
+        c = np.ascontiguousarray(conns, np.uint32).reshape(-1, 3)
+        if len(i) != len(p):
+            raise ValueError("upload_membrane: ids and xy of different lengths")
+        self._check(self._L.lbib_upload_membrane(self._h, _p(i), _p(p), len(i), _p(c), len(c)))
+
+    def cure_lattice(self) -> None:
+        """GeometryHandler::cureLattice after topology edits (see lbib_cure_lattice)."""
+        self._check(self._L.lbib_cure_lattice(self._h))
+
     # -- force list and range queries (host bio solvers) -----------------------
     def add_forces(self, types, id1, id2, par) -> None:
         """ForceSolver::addForce for a batch of records (see lbib_add_forces):

@@ -9,13 +9,15 @@
 // AbstractReportFunctor.hpp) dumps the state every ReportStep iterations.
 //
 // usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir
-//                   [timing W K] [restart SOLVERFILE] [write PREFIX]
+//                   [timing W K] [restart SOLVERFILE] [write PREFIX] [edit ITER FILE]
 //   With "timing W K" no reporter is registered: runSimulation() runs W
 //   untimed iterations, then K iterations whose wall time is printed as JSON
 //   (the CPU baseline).  "restart SOLVERFILE" loads the distributions with
 //   SimulationRunner::initSolvers(file) after initSolvers(); "write PREFIX"
 //   calls SimulationRunner::writeSimulation at the end, into PREFIX_force.txt,
-//   PREFIX_geometry.txt, PREFIX_parameters.txt and PREFIX_solver.txt.  The log
+//   PREFIX_geometry.txt, PREFIX_parameters.txt and PREFIX_solver.txt.  "edit
+//   ITER FILE" stops at iteration ITER, applies the topology edit in FILE
+//   through GeometryHandler (applyEdit), cures the lattice and runs on.  The log
 //   goes to outdir/log.txt as in apps/tutorial_01.cpp:47-57.
 //
 // Dump file outdir/dump_<t>.bin (little endian):
@@ -205,6 +207,39 @@ class DumpReporter : public LbmLib::reportHandler::AbstractReportFunctor {
 
 }  // namespace
 
+// A topology edit between steps, as a host bio solver (a cell division) makes
+// it through GeometryHandler: lines "erase id1 id2" (eraseConnection), "node x
+// y" (createGeometryNode, ids in order), "conn id1 id2 domain"
+// (createConnection with no boundary descriptor), applied in file order.
+void applyEdit(LbmLib::geometry::GeometryHandler& gh, const std::string& file) {
+    std::ifstream in(file);
+    if (!in.is_open()) throw std::runtime_error("cannot open edit file " + file);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::stringstream ls(line);
+        std::string k;
+        ls >> k;
+        if (k == "erase") {
+            unsigned a, b;
+            ls >> a >> b;
+            std::shared_ptr<LbmLib::geometry::Connection> hit;
+            for (const auto& c : gh.getGeometry().getConnections())
+                if (c->getGeometryNodes().first->getId() == a && c->getGeometryNodes().second->getId() == b) hit = c;
+            if (!hit) throw std::runtime_error("edit: no connection to erase");
+            gh.eraseConnection(hit);
+        } else if (k == "node") {
+            double x, y;
+            ls >> x >> y;
+            gh.createGeometryNode(x, y);
+        } else if (k == "conn") {
+            unsigned a, b, d;
+            ls >> a >> b >> d;
+            gh.createConnection(gh.returnGeometryNode(a), gh.returnGeometryNode(b),
+                                std::map<std::string, std::vector<std::string>>(), d);
+        }
+    }
+}
+
 int main(int argc, char** argv) {
     if (argc < 6) {
         std::cerr << "usage: ref_driver params geometry force plugins outdir [timing]\n";
@@ -212,7 +247,8 @@ int main(int argc, char** argv) {
     }
     bool timing = false;
     unsigned warm = 0, steps = 0;
-    std::string restartFile, writePrefix;
+    std::string restartFile, writePrefix, editFile;
+    unsigned editIter = 0;
     for (int a = 6; a < argc; ++a) {
         const std::string k = argv[a];
         if (k == "timing" && a + 2 < argc) {
@@ -224,6 +260,10 @@ int main(int argc, char** argv) {
             restartFile = argv[++a];
         } else if (k == "write" && a + 1 < argc) {
             writePrefix = argv[++a];
+        } else if (k == "edit" && a + 2 < argc) {
+            editIter = (unsigned)std::stoul(argv[a + 1]);
+            editFile = argv[a + 2];
+            a += 2;
         } else {
             std::cerr << "unknown argument " << k << "\n";
             return 2;
@@ -246,7 +286,20 @@ int main(int argc, char** argv) {
         simRunner.initForceSolver(argv[3]);
         if (pl.outlet) simRunner.addMassSolver("MassSolverBoxOutlet");
         for (const auto& b : pl.bio) simRunner.addBioSolver(b);
-        if (!timing) {
+        if (!timing && !editFile.empty()) {
+            // run to the edit's iteration, edit, run the rest
+            const unsigned total = LbmLib::Parameters.iterations_;
+            const unsigned first = editIter - LbmLib::Parameters.getCurrentIteration();
+            LbmLib::Parameters.iterations_ = first;
+            simRunner.runSimulation();
+            applyEdit(geohandler, editFile);
+            // then what a division plugin does after its edits
+            // (tutorial_01_BioSolverCellDivision.cpp:84-91)
+            geohandler.cureLattice();
+            geohandler.copyCellTypeToPhysicalNodes(geohandler.getCellTypeTrackerMap());
+            LbmLib::Parameters.iterations_ = total - first;
+            simRunner.runSimulation();
+        } else if (!timing) {
             simRunner.runSimulation();
             if (!writePrefix.empty())
                 simRunner.writeSimulation(writePrefix + "_force.txt", writePrefix + "_geometry.txt",
