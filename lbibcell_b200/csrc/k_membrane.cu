@@ -669,8 +669,10 @@ __device__ __forceinline__ int slot_code(int d) {  // E,N,W,S -> 0..3
 // boundary node for one (node, slot) key.  The closest distance per key is
 // found by atomicMin on the distance's bits; each candidate is recorded for
 // passes 1 and 2 and for the reset of its key at the end of the step.  A warp
-// reserves its records with one atomic.
-constexpr int kRecPerConn = 16;
+// reserves its records with one atomic.  A connection may be long (the
+// cut across a cell that a division adds, until remeshing splits it): the
+// loops run over the lattice lines between its end points, which the bounds
+// test below keeps on the lattice.
 
 struct CrossRec {
     uint32_t key;
@@ -737,7 +739,6 @@ __device__ __forceinline__ int for_each_record(const MembraneDev& m, int cn, int
     for (int i = (int)ceil(minX); i <= (int)floor(maxX); i++) {
         const double yc = mm * i + nn;
         // fluidS gets its N slot, fluidN its S slot (Connection.cpp:273-279)
-        if (k + 2 > kRecPerConn) break;
         if (!make_record(nx, ny, i, (int)floor(yc), N, (double)i, yc, eastward ? 0u : D, r)) break;
         fn(k++, r);
         if (!make_record(nx, ny, i, (int)ceil(yc), S, (double)i, yc, eastward ? D : 0u, r)) break;
@@ -746,7 +747,6 @@ __device__ __forceinline__ int for_each_record(const MembraneDev& m, int cn, int
     for (int i = (int)ceil(minY); i <= (int)floor(maxY); i++) {
         const double xc = (i - nn) / mm;
         // fluidW gets its E slot, fluidE its W slot (Connection.cpp:307-313)
-        if (k + 2 > kRecPerConn) break;
         if (!make_record(nx, ny, (int)floor(xc), i, E, xc, (double)i, southward ? 0u : D, r)) break;
         fn(k++, r);
         if (!make_record(nx, ny, (int)ceil(xc), i, W, xc, (double)i, southward ? D : 0u, r)) break;

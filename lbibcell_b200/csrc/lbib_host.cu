@@ -159,7 +159,7 @@ struct Handle {
     unsigned iteration = 0, iterations = 0, reportStep = 1;
     std::vector<Species> sp;
     bool outlet = false;
-    std::vector<int> bio;  // 1 tension, 2 area regulator, 3 cell junctions
+    std::vector<int> bio;  // 1 tension, 2 area regulator, 3 cell junctions, 4 cell division
     double tensionForce = 0.01;
     unsigned tensionFreq = 10;
     // tutorial_01_BioSolverCellJunction.cpp:37-41
@@ -215,6 +215,13 @@ struct Handle {
     std::mt19937 genNode{1};
     std::mt19937 genConn{1};
     std::uniform_real_distribution<> dis{-kPERTURBATION, kPERTURBATION};
+    // cell division (bio kind 4, the last bio solver): every divisionFreq-th
+    // iteration, cells larger than divisionMax split; policy 0 = across the
+    // longest axis, 1 = along a random direction (generator seeded 1)
+    int divisionPolicy = 0;
+    unsigned divisionFreq = 100;
+    double divisionMax = 380.0;
+    std::mt19937 genDiv{1};
 
     long long hostEvents = 0;
     long long launches = 0;
@@ -352,6 +359,12 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 if (kv.count("radius")) h.junctionRadius = kv["radius"];
                 if (kv.count("k")) h.junctionK = kv["k"];
                 if (kv.count("l0")) h.junctionL0 = kv["l0"];
+            } else if (name == "tutorial_01_BioSolverCellDivision" || name == "tutorial_02_BioSolverCellDivision" ||
+                       name == "BioSolverCellDivision") {
+                // tutorial_01_BioSolverCellDivision.cpp:33-36 (the plain one
+                // divides along a random direction, BioSolverCellDivision.cpp:100-101)
+                h.bio.push_back(4);
+                h.divisionPolicy = name == "BioSolverCellDivision" ? 1 : 0;
             } else if (name == "LbibAreaRegulator") {
                 h.bio.push_back(2);
                 if (kv.count("factor")) h.areaFactor = kv["factor"];
@@ -359,6 +372,8 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 if (kv.count("maxsource")) h.areaMax = kv["maxsource"];
             } else fail(ERR_INPUT, "unknown bio solver " + name);
             if (h.bio.size() > 8) fail(ERR_INPUT, "more than 8 bio solvers");
+            for (size_t q = 0; q + 1 < h.bio.size(); ++q)
+                if (h.bio[q] == 4) fail(ERR_INPUT, "the cell-division solver must be the last bio solver");
         } else if (kind == "CDE") {
             std::string k; double v;
             while (ls >> k >> v) kv[k] = v;
@@ -1146,11 +1161,25 @@ static void launch_step_graph(Handle& h, int parity, bool coarsenStep, int bioOp
     h.launches += g.launches;
 }
 
+static bool has_division(const Handle& h) {
+    return std::find(h.bio.begin(), h.bio.end(), 4) != h.bio.end();
+}
+static void run_division(Handle& h);
+
 template <typename Real>
 static void run_steps(Handle& h, int n) {
     const int kBatch = 64;
+    const bool division = has_division(h);
     while (n > 0) {
-        const int B = std::min(n, kBatch);
+        int B = std::min(n, kBatch);
+        if (division) {
+            // the batch ends with the next division step; the division follows it
+            for (int b = 0; b < B; ++b)
+                if ((h.iteration + b) % h.divisionFreq == 0) {
+                    B = b + 1;
+                    break;
+                }
+        }
         reset_status(h, h.iteration, h.cellTypesCopied);
         const bool prof = h.profiling;
         while ((int)h.kEvents.size() < 2 * B) {
@@ -1187,6 +1216,7 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += done;
         if (done > 0) h.cellTypesCopied = true;
         n -= done;
+        if (division && done > 0 && (h.iteration - 1) % h.divisionFreq == 0) run_division(h);
         if (!st.halt) continue;
         if (st.err) {
             h.err = st.err;
@@ -1219,6 +1249,7 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += 1;
         h.cellTypesCopied = true;
         n -= 1;
+        if (division && (h.iteration - 1) % h.divisionFreq == 0) run_division(h);
     }
 }
 
@@ -2844,3 +2875,151 @@ int lbib_cure_lattice(lbib_handle* hh) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The cell-division bio solver (tutorial_01_BioSolverCellDivision.cpp:42-140,
+// the same in tutorial_02; BioSolverCellDivision.cpp with a random direction),
+// run on the host after the step of every FREQUENCY-th iteration: it is the
+// last bio solver of its run, so nothing on the device follows it in the step.
+
+namespace lbib {
+
+// The two connections of a cell that a division line crosses
+// (getTwoConnectionsLongestAxis / getTwoConnectionsRandomDirection,
+// tutorial_01_BioSolverCellDivision.cpp:151-248): connection (p, q) is cut
+// when p lies above the line and q below it, or p on or below and q on or
+// above.
+static std::vector<int> cut_connections(const Handle& h, const HostMembrane& hm, const IdIndex& idx,
+                                        const std::vector<int>& cell, double slope, double intercept) {
+    std::vector<int> cut;
+    for (int c : cell) {
+        const int p = idx.at(h.conns[c].id1), q = idx.at(h.conns[c].id2);
+        const bool c1 = hm.y[p] > slope * hm.x[p] + intercept;
+        const bool c2 = hm.y[q] < slope * hm.x[q] + intercept;
+        if ((c1 && c2) || (!c1 && !c2)) cut.push_back(c);
+    }
+    return cut;
+}
+
+static std::map<std::string, std::vector<std::string>> descriptor_map(const std::string& desc) {
+    std::stringstream ls(desc);
+    std::map<std::string, std::vector<std::string>> m;
+    std::string a, b;
+    while (ls >> a >> b) m[a].push_back(b);
+    return m;
+}
+
+// divideCell (tutorial_01_BioSolverCellDivision.cpp:94-149) on the host
+// mirror; returns the new cell's domain id.
+static uint32_t divide_cell(Handle& h, const HostMembrane& hm, uint32_t dom,
+                            const std::map<uint32_t, std::vector<int>>& cells) {
+    const uint32_t newId = cells.rbegin()->first + 1;
+    const IdIndex idx(h.ids);
+    const std::vector<int>& cell = cells.at(dom);
+    std::vector<int> cut;
+    if (h.divisionPolicy == 0) {
+        // the furthest pair of the connections' first nodes (the first found
+        // of equal distance), then the perpendicular bisector
+        double dist = 0.0;
+        int n1 = -1, n2 = -1;
+        for (int c1 : cell)
+            for (int c2 : cell) {
+                const int a = idx.at(h.conns[c1].id1), b = idx.at(h.conns[c2].id1);
+                const double dx = hm.x[a] - hm.x[b], dy = hm.y[a] - hm.y[b];
+                const double d = std::sqrt(dx * dx + dy * dy);
+                if (d > dist) {
+                    dist = d;
+                    n1 = a;
+                    n2 = b;
+                }
+            }
+        if (n1 < 0) fail(ERR_STATE, "cell division: degenerate cell", dom);
+        const double mx = 0.5 * (hm.x[n1] + hm.x[n2]), my = 0.5 * (hm.y[n1] + hm.y[n2]);
+        const double slope = -(hm.x[n2] - hm.x[n1]) / (hm.y[n2] - hm.y[n1]);
+        const double intercept = my - slope * mx;
+        cut = cut_connections(h, hm, idx, cell, slope, intercept);
+    } else {
+        // a random direction through the centre of the first nodes
+        double cx = 0.0, cy = 0.0;
+        for (int c : cell) {
+            const int a = idx.at(h.conns[c].id1);
+            cx += hm.x[a];
+            cy += hm.y[a];
+        }
+        cx /= (double)cell.size();
+        cy /= (double)cell.size();
+        std::uniform_real_distribution<> angle(0.0, 2.0 * M_PI);
+        for (int tries = 1;; ++tries) {
+            const double slope = std::tan(angle(h.genDiv));
+            const double intercept = cy - slope * cx;
+            cut = cut_connections(h, hm, idx, cell, slope, intercept);
+            if (cut.size() == 2) break;
+            if (tries > 10) fail(ERR_STATE, "could not find cell division plane", dom);
+        }
+    }
+    if (cut.size() != 2) fail(ERR_STATE, "More or less than 2 connections found in the cell division", dom);
+    const HConn c0 = h.conns[cut[0]], c1 = h.conns[cut[1]];
+    if (descriptor_map(c0.desc) != descriptor_map(c1.desc))
+        fail(ERR_STATE, "The method cannot handle cell division cases with heterogeneous boundary conditions.", dom);
+    // the two new connections are appended, the two cut ones erased
+    std::vector<HConn> next;
+    next.reserve(h.conns.size());
+    for (size_t c = 0; c < h.conns.size(); ++c)
+        if ((int)c != cut[0] && (int)c != cut[1]) next.push_back(h.conns[c]);
+    next.push_back(HConn{c0.id1, c1.id2, dom, c0.desc});
+    next.push_back(HConn{c1.id1, c0.id2, dom, c0.desc});
+    h.conns.swap(next);
+    // the ring through c1's second node becomes the new cell
+    std::map<uint32_t, int> out;
+    for (size_t c = 0; c < h.conns.size(); ++c) out[h.conns[c].id1] = (int)c;
+    const int start = out.at(c1.id2);
+    int c = start;
+    do {
+        h.conns[c].dom = newId;
+        c = out.at(h.conns[c].id2);
+    } while (c != start);
+    return newId;
+}
+
+static void run_division(Handle& h) {
+    pull_topology(h);
+    HostMembrane hm;
+    download_membrane(h, hm);
+    sync_targets(h);
+    // GeometryHandler::computeAreas, in ring order
+    launch_rings(h.m, h.td, h.st, h.stream);
+    launch_areas(h.m, h.area, h.stream);
+    std::vector<double> a(h.m.nCells);
+    if (h.m.nCells) CK(cudaMemcpyAsync(a.data(), h.area, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    std::map<uint32_t, double> areas;
+    for (int c = 0; c < h.m.nCells; ++c) areas[h.ringDomHost[c]] = a[c];
+    areas[0] = 0.0;
+    auto cellsOf = [&]() {
+        std::map<uint32_t, std::vector<int>> cells;
+        for (size_t c = 0; c < h.conns.size(); ++c) cells[h.conns[c].dom].push_back((int)c);
+        return cells;
+    };
+    for (auto it = std::next(areas.begin()); it != areas.end(); ++it) {
+        if (!(it->second > h.divisionMax)) continue;
+        const uint32_t newId = divide_cell(h, hm, it->first, cellsOf());
+        grow_domains(h, (int)newId + 1);
+        h.ctypeHost[newId] = it->first < h.ctypeHost.size() ? h.ctypeHost[it->first] : 1u;
+        // the edited topology on the device (the force list stays: no node
+        // changed), then GeometryHandler::cureLattice
+        std::vector<int> foff(h.m.M + 1);
+        CK(cudaMemcpyAsync(foff.data(), h.m.foff, sizeof(int) * (h.m.M + 1), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        h.keepRecords = foff[h.m.M];
+        upload_topology(h, hm, false);
+        h.keepRecords = 0;
+        cure_lattice(h, hm);
+        h.graphEpoch++;
+    }
+    // copyCellTypeToPhysicalNodes: the cell-type table
+    CK(cudaMemcpyAsync(h.ctypeTab, h.ctypeHost.data(), sizeof(uint32_t) * h.nDomains, cudaMemcpyHostToDevice,
+                       h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+}  // namespace lbib

@@ -13,7 +13,28 @@
 #include <sstream>
 #include <vector>
 
-#define BOOST_GEOMETRY_REGISTER_POINT_2D_GET_SET(Point, Coord, Cs, Get0, Get1, Set0, Set1)
+// Point registration: records the two getters, so that distance() works on a
+// registered type (the cell-division plugins measure GeometryNode distances).
+namespace boost {
+namespace geometry {
+namespace lbib_traits {
+template <typename P>
+struct access {};
+}  // namespace lbib_traits
+}  // namespace geometry
+}  // namespace boost
+#define BOOST_GEOMETRY_REGISTER_POINT_2D_GET_SET(Point, Coord, Cs, Get0, Get1, Set0, Set1)   \
+    namespace boost {                                                                    \
+    namespace geometry {                                                                 \
+    namespace lbib_traits {                                                              \
+    template <>                                                                          \
+    struct access<Point> {                                                               \
+        static Coord x(const Point& p) { return p.Get0(); }                             \
+        static Coord y(const Point& p) { return p.Get1(); }                             \
+    };                                                                                   \
+    }                                                                                    \
+    }                                                                                    \
+    }
 
 namespace boost {
 namespace geometry {
@@ -35,6 +56,10 @@ struct point_xy {
 template <typename T, std::size_t D, typename CS>
 struct point {
     T v[D];
+    template <std::size_t I>
+    T get() const { return v[I]; }
+    template <std::size_t I>
+    void set(T a) { v[I] = a; }
 };
 template <typename P, bool ClockWise = true, bool Closed = true>
 struct polygon {
@@ -62,9 +87,23 @@ double area(const model::polygon<P, CW, CL>& poly) {
     return sum / 2.0;
 }
 
+// Coordinates of a point: a registered type through its getters, point_xy
+// through x() / y().
+template <typename P>
+auto coord_x(const P& p, int) -> decltype(lbib_traits::access<P>::x(p)) { return lbib_traits::access<P>::x(p); }
+template <typename P>
+auto coord_x(const P& p, long) -> decltype(p.x()) { return p.x(); }
+template <typename P>
+auto coord_y(const P& p, int) -> decltype(lbib_traits::access<P>::y(p)) { return lbib_traits::access<P>::y(p); }
+template <typename P>
+auto coord_y(const P& p, long) -> decltype(p.y()) { return p.y(); }
+
+// Cartesian (Pythagoras) distance: the squared differences summed by
+// dimension, then the root.
 template <typename A, typename B>
 double distance(const A& a, const B& b) {
-    return std::sqrt((a.x() - b.x()) * (a.x() - b.x()) + (a.y() - b.y()) * (a.y() - b.y()));
+    const double dx = coord_x(a, 0) - coord_x(b, 0), dy = coord_y(a, 0) - coord_y(b, 0);
+    return std::sqrt(dx * dx + dy * dy);
 }
 }  // namespace geometry
 }  // namespace boost

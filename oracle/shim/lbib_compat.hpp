@@ -1,6 +1,6 @@
 // Force-included into every reference translation unit of the oracle/_ref
 // build.  It supplies what older standard libraries pulled in transitively
-// (<cstring>, <algorithm>) and the stream-to-stream insertion that pre-C++11
+// (<cstring>, <algorithm>, <random>) and the stream-to-stream insertion that pre-C++11
 // libraries accepted through the void* conversion; the message text is
 // written instead of a pointer value.
 #ifndef LBIB_COMPAT_HPP
@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 #include <ostream>
+#include <random>
 #include <sstream>
 // Declared in namespace std so that argument-dependent lookup finds it from
 // inside the reference's namespaces, which declare operator<< of their own.

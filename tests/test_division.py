@@ -1,0 +1,71 @@
+"""The cell-division bio solver (tutorial_01_BioSolverCellDivision.cpp:42-149;
+the same in tutorial_02; BioSolverCellDivision.cpp divides along a random
+direction): every 100th iteration a cell larger than 380 lu^2 splits in two,
+then the lattice is cured.  Here it runs on the host after the step, against
+the reference build's own plugins (FP64, exact)."""
+import os
+
+import numpy as np
+import pytest
+
+from lbibcell_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lbib():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from lbibcell_b200 import build, runner
+    build.build()
+    return runner
+
+
+def _cfg(name, iterations=30):
+    # radius 12: area ~450 > 380, so the cell divides at iteration 0
+    cfg = configs.toy(n=64, r=12.0, nodes=120, iterations=iterations, report_step=10, species=2)
+    cfg.area = None
+    cfg.bio = [name]
+    return cfg
+
+
+@pytest.mark.parametrize("name", ["tutorial_01_BioSolverCellDivision", "BioSolverCellDivision"])
+def test_division_matches_reference(lbib, oracle_mod, tmp_path, name):
+    if not os.path.exists(oracle_mod.REF_DRIVER):
+        pytest.skip("reference build not available")
+    paths = _cfg(name).write(str(tmp_path / "cfg"))
+    dumps = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    done = 0
+    for t in (10, 20, 30):
+        sim.step(t - done)
+        done = t
+        ref = dumps[t]
+        lat = sim.lattice()
+        for field in ("f", "g", "vel", "dom", "ctype"):
+            a, b = getattr(lat, field), getattr(ref, field)
+            assert np.array_equal(a, b), f"t={t} {field}: max |diff| {np.abs(a.astype(float) - b.astype(float)).max()}"
+        ids, node = sim.membrane()
+        assert np.array_equal(ids, ref.ids) and np.array_equal(node, ref.node), f"t={t}: membrane differs"
+        assert np.array_equal(sim.connections(), ref.conn), f"t={t}: connections differ"
+    assert set(np.unique(sim.lattice().dom).tolist()) == {0, 1, 2}
+
+
+def test_division_fp32_shifted(lbib, tmp_path):
+    paths = _cfg("tutorial_01_BioSolverCellDivision", 20).write(str(tmp_path))
+    a = lbib.Simulation(paths, lbib.FP64)
+    b = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    a.step(20)
+    b.step(20)
+    assert np.array_equal(a.connections(), b.connections())
+    assert len(b.areas()) == 2
+
+
+def test_division_must_be_last(lbib, tmp_path):
+    cfg = _cfg("tutorial_01_BioSolverCellDivision")
+    cfg.bio = ["tutorial_01_BioSolverCellDivision", "tutorial_01_BioSolverCellJunction"]
+    with pytest.raises(lbib.LbibError) as e:
+        lbib.Simulation(cfg.write(str(tmp_path)), lbib.FP64)
+    assert e.value.code == 90
