@@ -120,6 +120,26 @@ int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
  * as lbib_areas. */
 int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
 
+/* GeometryHandler::computeAccumulatedDomainConcentrations(species)
+ * (libs/LbmLib/src/geometry/GeometryHandler.cpp:136-147): per domain id
+ * (ascending), the sum of the named CDE solver's concentration over the
+ * lattice nodes of that domain, rows in order and columns from x = 1 (the
+ * reference leaves column 0 out).  Returns the number of domains, or the
+ * negated error code (LBIB_ERR_INPUT for an unknown species,
+ * LBIB_ERR_CAPACITY when cap is too small). */
+int lbib_accumulated_concentrations(lbib_handle* h, const char* species, unsigned* dom, double* acc, int cap);
+
+/* GeometryHandler::getCellTypeTrackerMap()[dom[i]] = type[i] for n entries,
+ * then copyCellTypeToPhysicalNodes (GeometryHandler.cpp:267-314): the
+ * lattice nodes of those domains take the new types from the next step on
+ * (a bio solver that reads them in the same step sees them at once). */
+int lbib_set_cell_types(lbib_handle* h, const unsigned* dom, const unsigned* type, int n);
+
+/* GeometryHandler::getCellTypeTrackerMap (GeometryHandler.cpp:316-319): the
+ * cell type of every domain id below the handle's domain count.  Returns the
+ * count, or the negated error code. */
+int lbib_get_cell_types(lbib_handle* h, unsigned* dom, unsigned* type, int cap);
+
 /* Sets species k's production rate per domain id (rates[0..n), n <= number of
  * domain ids), taking effect at the next step.  This is the per-domain table
  * that a host BioSolver plugin would otherwise write node by node through

@@ -19,7 +19,8 @@ SYMBOLS = (
     "lbib_get_domain_count", "lbib_diff_begin", "lbib_diff_forward", "lbib_diff_backward", "lbib_diff_end",
     "lbib_write_simulation", "lbib_load_solvers", "lbib_add_forces", "lbib_delete_force_type",
     "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes", "lbib_write_vtk",
-    "lbib_read_vtm_geometry", "lbib_upload_membrane", "lbib_cure_lattice",
+    "lbib_read_vtm_geometry", "lbib_upload_membrane", "lbib_cure_lattice", "lbib_accumulated_concentrations",
+    "lbib_set_cell_types", "lbib_get_cell_types",
 )
 
 _lib = None
@@ -65,6 +66,12 @@ def load() -> ctypes.CDLL:
     L.lbib_areas.argtypes = [vp, vp, vp, ip]
     L.lbib_areas_static.restype = ip
     L.lbib_areas_static.argtypes = [vp, vp, vp, ip]
+    L.lbib_accumulated_concentrations.restype = ip
+    L.lbib_accumulated_concentrations.argtypes = [vp, ctypes.c_char_p, vp, vp, ip]
+    L.lbib_set_cell_types.restype = ip
+    L.lbib_set_cell_types.argtypes = [vp, vp, vp, ip]
+    L.lbib_get_cell_types.restype = ip
+    L.lbib_get_cell_types.argtypes = [vp, vp, vp, ip]
     L.lbib_last_error.restype = ip
     L.lbib_last_error.argtypes = [vp, cp, ip, ctypes.POINTER(ctypes.c_longlong)]
     L.lbib_last_timing.restype = ip

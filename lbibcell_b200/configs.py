@@ -64,6 +64,7 @@ class Config:
     cells: List[Tuple[int, np.ndarray]]  # (domainId, (n, 2) CCW vertices)
     species: List[Species]
     outlet: bool = True
+    current_iteration: int = 0
     tension: Optional[Tuple[float, int]] = (0.1, 10)  # (force, frequency)
     area: Optional[Tuple[float, float, float]] = (1.2, 0.01, 0.004)  # factor, strength, maxsource
     forces: List[str] = field(default_factory=list)
@@ -89,7 +90,7 @@ class Config:
         paths = {k: os.path.join(directory, k + ".txt") for k in ("parameters", "geometry", "force", "plugins")}
         with open(paths["parameters"], "w") as f:
             f.write("#Global Parameter file\n")
-            f.write("CurrentIterations:\t0\n")
+            f.write(f"CurrentIterations:\t{self.current_iteration}\n")
             f.write(f"Iterations:\t{self.iterations}\n")
             f.write(f"ReportStep:\t{self.report_step}\n")
             f.write(f"SizeX:\t{self.nx}\n")

@@ -23,10 +23,49 @@ __device__ __forceinline__ float reaction32(int kind, float src, float decay, ui
     return 0.0f;
 }
 
+// The reaction terms for slot T (r0) and E, N, W, S (r1): the FP64 solvers'
+// terms (reaction_terms64) in FP32.  COUPLED = false compiles only the
+// RX_LINEAR / RX_SIGNAL terms.
+template <bool COUPLED>
+__device__ __forceinline__ void reaction_terms32(const SpeciesConst& sp, float src, float C, float Cp, uint32_t dom,
+                                                 uint32_t ctype, unsigned iteration, float& r0, float& r1) {
+    if (COUPLED && coupled_kind(sp.kind)) {
+        float R, dt = (float)sp.dt;  // the rate the solver multiplies by its deltaT
+        switch (sp.kind) {
+            case RX_T2_R: R = dom != 0 ? 100.0f * (0.1f - C + C * C * Cp) : 0.0f; dt = 1.0e-4f; break;
+            case RX_T2_L: R = dom != 0 ? 100.0f * (0.9f - Cp * Cp * C) : 0.0f; dt = 1.0e-4f; break;
+            case RX_SCHNAK_U: R = dom != 0 ? 800.0f * (0.1f - C + C * C * Cp) : 0.0f; break;
+            case RX_SCHNAK_V: R = dom != 0 ? 800.0f * (0.9f - Cp * Cp * C) : 0.0f; break;
+            default:  // RX_BMP
+                if (ctype == 2) {
+                    const float h2 = Cp * Cp, h4 = h2 * h2;
+                    R = 0.00001f * h4 / ((float)sp.hill + h4);
+                } else {
+                    R = -0.001f * C;
+                }
+                break;
+        }
+        const float x = dt * R;
+        r0 = x * (1.0f / 3.0f);
+        r1 = x * (1.0f / 6.0f);
+        return;
+    }
+    const float R = reaction32(sp.kind, src, (float)sp.decay, dom, iteration, C);
+    r0 = R * (1.0f / 3.0f);
+    r1 = R * (1.0f / 6.0f);
+}
+
 // NS = number of species, a compile-time constant so that every input of a
 // node (9 + 5 NS values) is loaded before any arithmetic.  Grid (nx/256, ny).
-template <int NS>
+// MODE bit 0 (COUPLED): a species' reaction reads a partner species (its
+// pre-collide sum until it has collided at this node, its post-collide sum
+// after) or the node's cell type.  MODE bit 1 (MASSNODE): the mass source is
+// per node (massNode) instead of per domain.  Each combination is its own
+// instantiation, so that the plain case carries no code for the others.
+template <int NS, int MODE>
 __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
+    constexpr bool COUPLED = (MODE & 1) != 0;   // coupled species reactions
+    constexpr bool MASSNODE = (MODE & 2) != 0;  // per-node mass source
     pdl_wait();
     if (a.status->halt) return;
     const int nx = a.nx, ny = a.ny;
@@ -60,7 +99,8 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     }
     const uint32_t dom = a.dom[n];
     float rta = 0.0f;
-    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = (float)a.massTab[dom];
+    if (MASSNODE) rta = (float)a.massNode[n];
+    else if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = (float)a.massTab[dom];
     float Fx = 0.0f, Fy = 0.0f;
     if (a.tileCount[(y / kTile) * a.tilesX + (x / kTile)] > 0) {
         Fx = a.force[n];
@@ -121,6 +161,13 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     // exactly up to one rounding: with C/3 and C/6 each rounded in FP32 the
     // relaxation adds a systematic 3e-8 C / tau per step.
     const unsigned iteration = NS > 0 ? a.status->iteration : 0u;
+    float Cs[NS > 0 ? NS : 1];
+    uint32_t ctype = 0;
+    if (COUPLED) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Cs[k] = ((gi[k][0] + gi[k][1]) + (gi[k][2] + gi[k][3])) + gi[k][4];
+        if (a.status->cellTypesCopied) ctype = dom < (uint32_t)a.nDomains ? a.ctypeTab[dom] : 1u;
+    }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const float gT = gi[k][0], gE = gi[k][1], gN = gi[k][2], gW = gi[k][3], gS = gi[k][4];
@@ -128,8 +175,14 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         const float tI = (float)(1.0 / a.sp[k].tau);
         float src = 0.0f;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = (float)a.srcTab[(size_t)k * a.nDomains + dom];
-        const float R = reaction32(a.sp[k].kind, src, (float)a.sp[k].decay, dom, iteration, C);
-        const float r0 = R * (1.0f / 3.0f), r1 = R * (1.0f / 6.0f);
+        float Cp = 0.0f;
+        if (COUPLED) {
+#pragma unroll
+            for (int j = 0; j < NS; ++j)
+                if (a.sp[k].partner == j) Cp = Cs[j];
+        }
+        float r0, r1;
+        reaction_terms32<COUPLED>(a.sp[k], src, C, Cp, dom, ctype, iteration, r0, r1);
         const float e1 = C * (1.0f / 6.0f), e0 = C - 4.0f * e1;
         float go[5];
         go[0] = gT + (e0 - gT) * tI + r0;
@@ -137,6 +190,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
         go[2] = gN + (e1 * (1.0f + 3.0f * uyo) - gN) * tI + r1;
         go[3] = gW + (e1 * (1.0f - 3.0f * uxo) - gW) * tI + r1;
         go[4] = gS + (e1 * (1.0f - 3.0f * uyo) - gS) * tI + r1;
+        if (COUPLED) Cs[k] = ((go[0] + go[1]) + (go[2] + go[3])) + go[4];
         for (int p = 0; p < passes; ++p)
 #pragma unroll
             for (int q = 0; q < 5; ++q) go[q] *= rs[p];
@@ -215,11 +269,16 @@ __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double ta
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     if (a.nfTab != nullptr) launch_noflux<float>(a, s);
-    switch (a.S) {
-        case 0: launch_pdl(stream_collide32<0>, grid, 256, 0, s, a); break;
-        case 1: launch_pdl(stream_collide32<1>, grid, 256, 0, s, a); break;
-        case 2: launch_pdl(stream_collide32<2>, grid, 256, 0, s, a); break;
-        default: launch_pdl(stream_collide32<3>, grid, 256, 0, s, a); break;
+    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0);
+    switch (mode * 4 + (a.S < 3 ? a.S : 3)) {
+#define LBIB_SC_CASE(M, N) \
+    case M * 4 + N: launch_pdl(stream_collide32<N, M>, grid, 256, 0, s, a); break;
+        LBIB_SC_CASE(0, 0) LBIB_SC_CASE(0, 1) LBIB_SC_CASE(0, 2) LBIB_SC_CASE(0, 3)
+        LBIB_SC_CASE(2, 0) LBIB_SC_CASE(2, 1) LBIB_SC_CASE(2, 2) LBIB_SC_CASE(2, 3)
+        // coupled reactions need a partner species: two or three species
+        LBIB_SC_CASE(1, 2) LBIB_SC_CASE(1, 3) LBIB_SC_CASE(3, 2) LBIB_SC_CASE(3, 3)
+#undef LBIB_SC_CASE
+        default: break;
     }
 }
 

@@ -16,9 +16,14 @@
 namespace lbib {
 
 // NS = number of species (a.S), a compile-time constant so that the pulled
-// species values stay in registers.
-template <int NS>
+// species values stay in registers.  MODE bit 0 (COUPLED): some species'
+// reaction reads a partner species or the cell type (the partner's getC() is
+// its pre-collide sum while it has not collided at this node, its
+// post-collide sum after).  MODE bit 1 (MASSNODE): per-node mass source.
+template <int NS, int MODE>
 __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
+    constexpr bool COUPLED = (MODE & 1) != 0;   // coupled species reactions
+    constexpr bool MASSNODE = (MODE & 2) != 0;  // per-node mass source
     pdl_wait();
     if (a.status->halt) return;
     // grid (nx/256, ny): one lattice node per thread
@@ -45,7 +50,8 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
 
     const uint32_t dom = a.dom[n];
     double rta = 0.0;
-    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
+    if (MASSNODE) rta = a.massNode[n];
+    else if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
     double fx = 0.0, fy = 0.0;
     if (a.tileCount[(y / kTile) * a.tilesX + (x / kTile)] > 0) {
         fx = a.force[n];
@@ -83,12 +89,28 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         gAll[k][W] = gin[3 * L + rC + xp];
         gAll[k][S] = gin[4 * L + rP + x];
     }
+    // the species' getC() as a coupled reaction reads it, and the node's cell
+    // type (copied from the per-domain table after every step's move)
+    double Cs[NS > 0 ? NS : 1];
+    uint32_t ctype = 0;
+    if (COUPLED) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Cs[k] = sum5(gAll[k]);
+        if (a.status->cellTypesCopied) ctype = dom < (uint32_t)a.nDomains ? a.ctypeTab[dom] : 1u;
+    }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         double* g = gAll[k];
         double src = 0.0;
         if (a.srcTab != nullptr && dom < (uint32_t)a.nDomains) src = a.srcTab[(size_t)k * a.nDomains + dom];
-        collide_cde64(g, ux, uy, a.sp[k].tau, a.sp[k].kind, src, a.sp[k].decay, dom, a.status->iteration);
+        double Cp = 0.0;
+        if (COUPLED) {
+#pragma unroll
+            for (int j = 0; j < NS; ++j)
+                if (a.sp[k].partner == j) Cp = Cs[j];
+        }
+        collide_cde64<COUPLED>(g, ux, uy, a.sp[k], src, Cp, dom, ctype, a.status->iteration);
+        if (COUPLED) Cs[k] = sum5_swapped(g);
         for (int p = 0; p < passes; ++p)
 #pragma unroll
             for (int q = 0; q < 5; ++q) g[q] *= sc[p];
@@ -150,7 +172,7 @@ __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double
         if (sp[k].kind == RX_NONE) {
             // CDESolverD2Q5::initSolver — CDESolverD2Q5.cpp:37-40
             gi[0] = 1.0; gi[1] = gi[2] = gi[3] = gi[4] = 0.0;
-            collide_cde64(gi, ux, uy, sp[k].tau, RX_NONE, 0.0, 0.0, dom[n], 0);
+            collide_cde64(gi, ux, uy, sp[k], 0.0, 0.0, dom[n], 0u, 0u);
         } else if (sp[k].kind == RX_SIGNAL) {
             // tutorial_01_CDESolverD2Q5_SIGNAL::initSolver — :46-57
             const double v = dom[n] == 0 ? 0.0 : 1.0 / 5.0;
@@ -270,11 +292,16 @@ template void launch_noflux<float>(const LatticeArgs<float>&, cudaStream_t);
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     if (a.nfTab != nullptr) launch_noflux<double>(a, s);
-    switch (a.S) {
-        case 0: launch_pdl(stream_collide64<0>, grid, 256, 0, s, a); break;
-        case 1: launch_pdl(stream_collide64<1>, grid, 256, 0, s, a); break;
-        case 2: launch_pdl(stream_collide64<2>, grid, 256, 0, s, a); break;
-        default: launch_pdl(stream_collide64<3>, grid, 256, 0, s, a); break;
+    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0);
+    switch (mode * 4 + (a.S < 3 ? a.S : 3)) {
+#define LBIB_SC_CASE(M, N) \
+    case M * 4 + N: launch_pdl(stream_collide64<N, M>, grid, 256, 0, s, a); break;
+        LBIB_SC_CASE(0, 0) LBIB_SC_CASE(0, 1) LBIB_SC_CASE(0, 2) LBIB_SC_CASE(0, 3)
+        LBIB_SC_CASE(2, 0) LBIB_SC_CASE(2, 1) LBIB_SC_CASE(2, 2) LBIB_SC_CASE(2, 3)
+        // coupled reactions need a partner species: two or three species
+        LBIB_SC_CASE(1, 2) LBIB_SC_CASE(1, 3) LBIB_SC_CASE(3, 2) LBIB_SC_CASE(3, 3)
+#undef LBIB_SC_CASE
+        default: break;
     }
 }
 

@@ -932,7 +932,7 @@ void launch_edge_check(const MembraneDev& m, int nx, int ny, Status* st, unsigne
 // changed nodes among its E,N,W,S,NE (read after write) and SW (write after
 // read) neighbours, and processes nodes in rounds once those are done.
 constexpr int kReinitMax = 4096;  // changed nodes per step (dynamic shared memory)
-constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 6 * sizeof(int) + 1) + 16;
+constexpr size_t kReinitSmem = (size_t)kReinitMax * (sizeof(unsigned long long) + 8 * sizeof(int) + 1) + 16;
 
 template <typename Real>
 __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, const Real* u, int nS,
@@ -960,6 +960,7 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     // boundaryNodes_[NE] aliases (domainIdentifier_, cellType_): null only if both are 0.
     const uint32_t ctype = cellTypesCopied ? (oldDom < (uint32_t)nDomains ? ctypeTab[oldDom] : 1u) : 0u;
     const bool neNull = newDom == 0 && ctype == 0;
+    double Cnew[kMaxSpecies] = {0.0, 0.0, 0.0};  // getC() of the species already re-initialised here
     for (int k = 0; k < nS; ++k) {
         const Real* gk = g + (size_t)k * 5 * L;
         // the five slots of the four neighbours and NE, read unconditionally
@@ -968,40 +969,72 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
         for (int s = 0; s < 5; ++s)
 #pragma unroll
             for (int q = 0; q < 5; ++q) gv[s][q] = gk[(size_t)q * L + nb[s]];
+        // getC() in slot order after localSwap: T, W, S, E, N
+        auto cOf = [](const Real* v) {
+            double C = 0.0;
+            C += (double)v[0];
+            C += (double)v[3];
+            C += (double)v[4];
+            C += (double)v[1];
+            C += (double)v[2];
+            return C;
+        };
+        const int style = sp[k].reinit;
         double sumC = 0.0;
         int counter = 0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             if (!hasBN[s] && newDom == dnb[s]) {
-                // getC() in slot order after localSwap: T, W, S, E, N
-                double C = 0.0;
-                C += (double)gv[s][0];
-                C += (double)gv[s][3];
-                C += (double)gv[s][4];
-                C += (double)gv[s][1];
-                C += (double)gv[s][2];
-                sumC += C;
+                sumC += cOf(gv[s]);
                 counter++;
             }
         }
-        if (counter == 0 && neNull && newDom == dnb[4]) {
-            double C = 0.0;
-            C += (double)gv[4][0];
-            C += (double)gv[4][3];
-            C += (double)gv[4][4];
-            C += (double)gv[4][1];
-            C += (double)gv[4][2];
-            sumC += C;
+        if (counter == 0 && style != RI_DIAG && neNull && newDom == dnb[4]) {
+            sumC += cOf(gv[4]);
             counter++;
             atomicAdd(&st->nDiagReinit, 1);
+        }
+        if (counter == 0 && style == RI_DIAG) {
+            // NE, NW, SW, SE of the same domain, no boundary-node test
+            const size_t dg[4] = {nb[4], (size_t)yp * nx + xm, (size_t)ym * nx + xm, (size_t)ym * nx + xp};
+            for (int s = 0; s < 4; ++s) {
+                if (dom[dg[s]] != newDom) continue;
+                Real v[5];
+                for (int q = 0; q < 5; ++q) v[q] = gk[(size_t)q * L + dg[s]];
+                sumC += cOf(v);
+                counter++;
+            }
+            if (counter != 0) atomicAdd(&st->nDiagReinit, 1);
+        }
+        if (counter == 0 && style == RI_ALL4) {
+            // all of E, N, W, S whatever their domain
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                sumC += cOf(gv[s]);
+                counter++;
+            }
         }
         if (counter == 0) atomicAdd(&st->nFailedReinit, 1);
         sumC /= static_cast<double>(counter);
         double gi[5];
-        for (int q = 0; q < 5; ++q) gi[q] = sumC / 5.0;
+        for (int q = 0; q < 5; ++q) gi[q] = style == RI_DIAG ? sumC / 4.0 : sumC / 5.0;
         const double src = (srcTab != nullptr && newDom < (uint32_t)nDomains) ? srcTab[(size_t)k * nDomains + newDom]
                                                                             : 0.0;
-        collide_cde64(gi, ux, uy, sp[k].tau, sp[k].kind, src, sp[k].decay, newDom, iteration);
+        // a coupled reaction reads the partner's getC(): re-initialised
+        // already (an earlier species), else its state from this step's collide
+        double Cp = 0.0;
+        const int pj = sp[k].partner;
+        if (pj >= 0 && pj < nS) {
+            if (pj < k) {
+                Cp = Cnew[pj];
+            } else {
+                Real v[5];
+                for (int q = 0; q < 5; ++q) v[q] = g[((size_t)pj * 5 + q) * L + n];
+                Cp = cOf(v);
+            }
+        }
+        collide_cde64(gi, ux, uy, sp[k], src, Cp, newDom, ctype, iteration);
+        Cnew[k] = sum5_swapped(gi);
         Real* go = g + (size_t)k * 5 * L;
         for (int q = 0; q < 5; ++q) go[(size_t)q * L + n] = (Real)gi[q];
     }
@@ -1009,15 +1042,17 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
 
 // The earlier changed nodes a changed node n waits for: its E,N,W,S (read
 // after write: n reads their new state) and NE / SW neighbours (SW reads n's
-// old state through its NE fallback) with a smaller row-major index; -1 none.
+// old state through its NE fallback) with a smaller row-major index; with a
+// species that falls back on all four diagonals (RI_DIAG) also NW / SE; -1 none.
+constexpr int kReinitDeps = 8;
 __device__ __forceinline__ void reinit_deps(const CrossDev& c, size_t n, int nx, int ny, int* deps) {
     const int x = (int)(n % nx), y = (int)(n / nx);
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-    const size_t nbs[6] = {(size_t)y * nx + xp, (size_t)yp * nx + x, (size_t)y * nx + xm, (size_t)ym * nx + x,
-                           (size_t)yp * nx + xp, (size_t)ym * nx + xm};
+    const size_t nbs[8] = {(size_t)y * nx + xp,  (size_t)yp * nx + x,  (size_t)y * nx + xm,  (size_t)ym * nx + x,
+                           (size_t)yp * nx + xp, (size_t)ym * nx + xm, (size_t)yp * nx + xm, (size_t)ym * nx + xp};
 #pragma unroll
-    for (int d = 0; d < 6; ++d) deps[d] = nbs[d] < n ? c.mark[nbs[d]] - 1 : -1;
+    for (int d = 0; d < 8; ++d) deps[d] = (d < 6 || c.diag8) && nbs[d] < n ? c.mark[nbs[d]] - 1 : -1;
 }
 
 // (Each changed node's position in the list is marked where the crossings
@@ -1037,11 +1072,11 @@ __global__ void reinit_free_kernel(CrossDev c, uint32_t* dom, Real* g, const Rea
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
         const size_t n = c.changedNode[k];
-        int deps[6];
+        int deps[kReinitDeps];
         reinit_deps(c, n, nx, ny, deps);
         bool free = true;
 #pragma unroll
-        for (int d = 0; d < 6; ++d) free &= deps[d] < 0;
+        for (int d = 0; d < kReinitDeps; ++d) free &= deps[d] < 0;
         c.reinitDone[k] = free ? 1 : 0;
         if (free)
             reinit_node<Real>(n, c.changedDom[k], dom, g, u, nS, sp, srcTab, nDomains, ctypeTab, st->cellTypesCopied,
@@ -1066,7 +1101,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* key = (unsigned long long*)smem;  // node << 32 | newDom
-    int(*deps)[6] = (int(*)[6])(key + kReinitMax);
+    int(*deps)[kReinitDeps] = (int(*)[kReinitDeps])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
     // Step 2, one block: the nodes that wait for others, in dependency rounds
@@ -1088,7 +1123,7 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
             if (done[k]) continue;
             bool ready = true;
-            for (int d = 0; d < 6; ++d)
+            for (int d = 0; d < kReinitDeps; ++d)
                 if (deps[k][d] >= 0 && done[deps[k][d]] != 1) ready = false;
             if (ready) done[k] = 2;  // processing this round
         }
@@ -1291,22 +1326,98 @@ __global__ void __launch_bounds__(256) areas_kernel(MembraneDev m, double* area,
     }
 }
 
+// ctypeTab == nullptr: LbibAreaRegulator, target = factor x the first area,
+// rate strength (target - A) / target.  Otherwise
+// tutorial_01_BioSolverAreaRegulator (tutorial_01_BioSolverAreaRegulator.cpp:
+// 44-97): target = factor (TARGETAREA), rate strength (target - A) (KP), and
+// cells of type 1 get maxsource whatever their area.
 __global__ void area_regulator_kernel(MembraneDev m, const double* area, double* target, double* massTab,
                                       int nDomains, double factor, double strength, double maxsource,
-                                      const Status* st) {
+                                      const uint32_t* ctypeTab, const Status* st) {
     pdl_wait();
     if (st->halt) return;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= m.nCells) return;
     const double A = area[cell];
-    if (isnan(target[cell])) target[cell] = factor * A;
-    const double tgt = target[cell];
-    double r = strength * (tgt - A) / tgt;
+    double r;
+    if (ctypeTab == nullptr) {
+        if (isnan(target[cell])) target[cell] = factor * A;
+        const double tgt = target[cell];
+        r = strength * (tgt - A) / tgt;
+    } else {
+        if (isnan(target[cell])) target[cell] = factor;
+        r = strength * (target[cell] - A);
+    }
     if (r > maxsource) r = maxsource;
     else if (r < -maxsource) r = -maxsource;
     const uint32_t d = m.ringDom[cell];
-    if (d < (uint32_t)nDomains && d != 0) massTab[d] = r;
+    if (d < (uint32_t)nDomains && d != 0) {
+        if (ctypeTab != nullptr && ctypeTab[d] == 1) r = maxsource;
+        massTab[d] = r;
+    }
 }
+
+// tutorial_02_BioSolverGrowth::applyBioProcess (tutorial_02_BioSolverGrowth.cpp:
+// 44-80): every node inside a cell gets the mass source MAXSOURCE = 0.001 where
+// R^2 L > 1 (THRESHOLD) and MAXSOURCE / 10 elsewhere; R and L are the species'
+// getC() after the step (post-collide slot order T, W, S, E, N).  The source is
+// per node: FluidSolver::addMass sets the next collide's rhoToAdd.
+template <typename Real>
+__global__ void growth_kernel(const Real* g, const uint32_t* dom, size_t L, int iR, int iL, double* massNode,
+                              const Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L) return;
+    const uint32_t d = dom[n];
+    double src = 0.0;
+    if (d != 0) {
+        auto cOf = [&](int k) {
+            const Real* gk = g + (size_t)k * 5 * L;
+            double C = 0.0;
+            C += (double)gk[0 * L + n];
+            C += (double)gk[3 * L + n];
+            C += (double)gk[4 * L + n];
+            C += (double)gk[1 * L + n];
+            C += (double)gk[2 * L + n];
+            return C;
+        };
+        const double R = cOf(iR), Lc = cOf(iL);
+        const double maxsource = 0.001;
+        src = R * R * Lc > 1.0 ? maxsource : maxsource / 10.0;
+    }
+    massNode[n] = src;
+}
+
+// The per-domain rates of an area regulator as per-node sources, for runs
+// whose host bio solvers change domains after the bio step (a division's
+// cureLattice): FluidSolver::addMass gave each node its rate by the domain it
+// had at bio time, which the next collide applies whatever the node's domain
+// is by then.
+__global__ void mass_expand_kernel(const uint32_t* dom, size_t L, const double* massTab, int nDomains,
+                                   double* massNode, const Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L) return;
+    const uint32_t d = dom[n];
+    massNode[n] = (d != 0 && d < (uint32_t)nDomains) ? massTab[d] : 0.0;
+}
+
+void launch_mass_expand(const uint32_t* dom, size_t L, const double* massTab, int nDomains, double* massNode,
+                        const Status* st, cudaStream_t s) {
+    launch_pdl(mass_expand_kernel, (unsigned)((L + 255) / 256), 256, 0, s, dom, L, massTab, nDomains, massNode, st);
+}
+
+template <typename Real>
+void launch_growth(const Real* g, const uint32_t* dom, size_t L, int iR, int iL, double* massNode, const Status* st,
+                   cudaStream_t s) {
+    launch_pdl(growth_kernel<Real>, (unsigned)((L + 255) / 256), 256, 0, s, g, dom, L, iR, iL, massNode, st);
+}
+template void launch_growth<double>(const double*, const uint32_t*, size_t, int, int, double*, const Status*,
+                                    cudaStream_t);
+template void launch_growth<float>(const float*, const uint32_t*, size_t, int, int, double*, const Status*,
+                                   cudaStream_t);
 
 // FP32-shifted runs: the per-cell shoelace sums over the connections in any
 // order, each term x_a y_b - x_b y_a (a -> b along the ring) rounded to 64-bit
@@ -1357,21 +1468,22 @@ cudaError_t static_area_scratch(double** ptr) {
 }
 
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
-                           double factor, double strength, double maxsource, const Status* st, cudaStream_t s) {
+                           double factor, double strength, double maxsource, const uint32_t* ctypeTab,
+                           const Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
     launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, (Status*)st);
     launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
-                                                                 strength, maxsource, st);
+                                                                 strength, maxsource, ctypeTab, st);
 }
 
 void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
                                  double* target, double* massTab, int nDomains, double factor, double strength,
-                                 double maxsource, const Status* st, cudaStream_t s) {
+                                 double maxsource, const uint32_t* ctypeTab, const Status* st, cudaStream_t s) {
     if (m.nCells == 0 || m.Ccap == 0) return;
     launch_pdl(areas_fixed_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, cellOfDom, nDomains, acc);
     launch_pdl(areas_fixed_finish, (m.nCells + 127) / 128, 128, 0, s, acc, m.nCells, area);
     launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
-                                                                 strength, maxsource, st);
+                                                                 strength, maxsource, ctypeTab, st);
 }
 
 }  // namespace lbib

@@ -81,6 +81,7 @@ struct CrossDev {
     uint32_t* changedNode;       // capacity: nodes whose domain changes
     uint32_t* changedDom;
     int changedCap;
+    int diag8;                   // a species re-initialises from all four diagonals (RI_DIAG)
     int* perturbList;            // membrane node indices flagged for the host RNG
     int perturbCap;
     // crossing records of this step (one per candidate node-slot pair)
@@ -202,14 +203,24 @@ void launch_range_query(MembraneDev& m, ForceScratch& fs, int nx, int ny, const 
                         long long* closest, cudaStream_t s);
 size_t junction_sort_bytes(int n, int bits);
 void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double force, cudaStream_t s);
+// ctypeTab != nullptr selects tutorial_01_BioSolverAreaRegulator's rule (fixed
+// target, cell type 1 at maxsource); nullptr the LbibAreaRegulator rule.
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
-                           double factor, double strength, double maxsource, const Status* st, cudaStream_t s);
+                           double factor, double strength, double maxsource, const uint32_t* ctypeTab,
+                           const Status* st, cudaStream_t s);
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
 // FP32-shifted runs: areas from the connections in fixed point (no ring order
 // needed), then the regulator.  acc (nCells) must start at zero; it is left zero.
 void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
                                  double* target, double* massTab, int nDomains, double factor, double strength,
-                                 double maxsource, const Status* st, cudaStream_t s);
+                                 double maxsource, const uint32_t* ctypeTab, const Status* st, cudaStream_t s);
+// massNode[n] = massTab[dom[n]] (0 outside cells).
+void launch_mass_expand(const uint32_t* dom, size_t L, const double* massTab, int nDomains, double* massNode,
+                        const Status* st, cudaStream_t s);
+// tutorial_02_BioSolverGrowth: the per-node mass source from species iR, iL.
+template <typename Real>
+void launch_growth(const Real* g, const uint32_t* dom, size_t L, int iR, int iL, double* massNode, const Status* st,
+                   cudaStream_t s);
 
 // Cells that fit the fixed device array of lbib_areas_static (16384 doubles,
 // 128 KB), and the address of that array on the current device.

@@ -82,34 +82,112 @@ __host__ __device__ __forceinline__ double reaction64(int kind, double src, doub
     return -0.00001 * C;
 }
 
+// x^4 rounded once: x*x and (x*x)^2 split into exact head and tail with fma
+// (Dekker's exact product), the tails summed, one final rounding.  The result
+// is the correctly rounded x^4 except within about 2^-100 of a rounding
+// boundary.
+__host__ __device__ __forceinline__ double pow4_rn(double x) {
+    const double p = x * x;
+    const double pe = fma(x, x, -p);
+    const double q = p * p;
+    const double qe = fma(p, p, -q);
+    return q + (qe + 2.0 * p * pe);
+}
+
+// The two reaction terms a species' collide adds to slot T (r0) and to E, N,
+// W, S (r1), each in its solver's own expression order.  C is the species'
+// concentration, Cp that of the partner species the reaction reads (as the
+// partner's getC() returns it at that moment), ctype the node's cell type.
+// COUPLED = false compiles only the RX_LINEAR / RX_SIGNAL terms (the
+// lattice kernels instantiate it when no species has a coupled kind).
+template <bool COUPLED = true>
+__host__ __device__ __forceinline__ void reaction_terms64(const SpeciesConst& sp, double src, double C, double Cp,
+                                                          uint32_t dom, uint32_t ctype, unsigned iteration,
+                                                          double& r0, double& r1) {
+    switch (COUPLED ? sp.kind : RX_LINEAR) {
+        case RX_T2_R: {  // tutorial_02_CDESolverD2Q5_R.cpp:94-105,130-132 (gamma 100, a 0.1, deltaT 1e-4)
+            const double R = dom != 0 ? 100.0 * (0.1 - C + C * C * Cp) : 0.0;
+            r0 = 1.0e-4 * R / 3.0;
+            r1 = 1.0e-4 * R / 6.0;
+            return;
+        }
+        case RX_T2_L: {  // tutorial_02_CDESolverD2Q5_L.cpp:94-106 (b 0.9; R is the partner)
+            const double R = dom != 0 ? 100.0 * (0.9 - Cp * Cp * C) : 0.0;
+            r0 = 1.0e-4 * R / 3.0;
+            r1 = 1.0e-4 * R / 6.0;
+            return;
+        }
+        case RX_SCHNAK_U:  // SchnakenbergD2Q5u.cpp:114-121 (gamma 800, a 0.1)
+            r0 = sp.dt * 800.0 * (0.1 - C + C * C * Cp) / 3.0;
+            r1 = sp.dt * 800.0 * (0.1 - C + C * C * Cp) / 6.0;
+            if (dom == 0) r0 = r1 = 0.0;
+            return;
+        case RX_SCHNAK_V:  // SchnakenbergD2Q5v.cpp:110-117 (b 0.9; u is the partner)
+            r0 = sp.dt * 800.0 * (0.9 - Cp * Cp * C) / 3.0;
+            r1 = sp.dt * 800.0 * (0.9 - Cp * Cp * C) / 6.0;
+            if (dom == 0) r0 = r1 = 0.0;
+            return;
+        case RX_BMP: {  // CDESolverD2Q5BMP.cpp:107-120: decay 0.001, Hill production 1e-5 on cell type 2
+            if (ctype == 2) {
+                const double h4 = pow4_rn(Cp);
+                r0 = sp.dt * 0.00001 / 3.0 * h4 / (sp.hill + h4);
+                r1 = sp.dt * 0.00001 / 6.0 * h4 / (sp.hill + h4);
+            } else {
+                r0 = sp.dt * (-0.001 * C) / 3.0;
+                r1 = sp.dt * (-0.001 * C) / 6.0;
+            }
+            return;
+        }
+        default: {  // RX_LINEAR, RX_SIGNAL
+            const double R = reaction64(sp.kind, src, sp.decay, dom, iteration, C);
+            const double deltaT = 1.0;
+            r0 = deltaT * R / 3.0;
+            r1 = deltaT * R / 6.0;
+            return;
+        }
+    }
+}
+
 // CDESolverD2Q5::collide (kind RX_NONE) or the reaction variant, in place on gi[5].
-__host__ __device__ __forceinline__ void collide_cde64(double* gi, double ux, double uy, double tau, int kind,
-                                                      double src, double decay, uint32_t dom, unsigned iteration) {
+template <bool COUPLED = true>
+__host__ __device__ __forceinline__ void collide_cde64(double* gi, double ux, double uy, const SpeciesConst& sp,
+                                                      double src, double Cp, uint32_t dom, uint32_t ctype,
+                                                      unsigned iteration) {
     const double C = sum5(gi);
     const double w0 = C / 3.0;
     const double w1 = C / 6.0;
-    const double tauI = 1.0 / tau;
+    const double tauI = 1.0 / sp.tau;
     double temp[5];
     temp[T] = w0;
     temp[E] = w1 * (1.0 + ux * 3.0);
     temp[N] = w1 * (1.0 + uy * 3.0);
     temp[W] = w1 * (1.0 + (-ux) * 3.0);
     temp[S] = w1 * (1.0 + (-uy) * 3.0);
-    if (kind == RX_NONE) {
+    if (sp.kind == RX_NONE) {
 #pragma unroll
         for (int d = 0; d < 5; ++d) {
             const double tempD = gi[d];
             gi[d] = tempD - tempD * tauI + temp[d] * tauI;
         }
     } else {
-        const double R = reaction64(kind, src, decay, dom, iteration, C);
-        const double deltaT = 1.0;
-        const double r0 = deltaT * R / 3.0;
-        const double r1 = deltaT * R / 6.0;
+        double r0, r1;
+        reaction_terms64<COUPLED>(sp, src, C, Cp, dom, ctype, iteration, r0, r1);
         gi[T] = gi[T] - gi[T] * tauI + temp[T] * tauI + r0;
 #pragma unroll
         for (int d = 1; d < 5; ++d) gi[d] = gi[d] - gi[d] * tauI + temp[d] * tauI + r1;
     }
+}
+
+// getC() of a species whose array is in post-collide order (after
+// localSwap): the sum runs T, W, S, E, N over the direction-indexed slots.
+__host__ __device__ __forceinline__ double sum5_swapped(const double* gi) {
+    double C = 0.0;
+    C += gi[T];
+    C += gi[W];
+    C += gi[S];
+    C += gi[E];
+    C += gi[N];
+    return C;
 }
 
 }  // namespace lbib

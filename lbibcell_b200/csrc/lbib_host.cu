@@ -30,6 +30,7 @@
 
 #include "../../include/lbibcell.h"
 #include "kernels.cuh"
+#include "lattice_math.cuh"
 #include "vtk_io.h"
 
 namespace lbib {
@@ -97,11 +98,21 @@ struct HForce {
     double p[4];
 };
 
+// Initial conditions set on the host (the rest by the init kernels).
+enum InitStyle {
+    INIT_KERNEL = 0,  // init64 / init32
+    INIT_ZERO,        // CDESolverD2Q5BMP.cpp:45-50
+    INIT_T2,          // tutorial_02_CDESolverD2Q5_R.cpp:44-59: (1 + U(-0.01, 0.01)) / 5 per slot, 0 outside cells
+    INIT_SCHNAK       // SchnakenbergD2Q5u.cpp:43-58: 0.2 (1 + U(-0.01, 0.01)) per node, 0 outside cells
+};
+
 struct Species {
     std::string name;
     SpeciesConst c;
     double init = 0.0;
     std::map<uint32_t, double> source;
+    std::string partnerName;
+    int initStyle = INIT_KERNEL;
 };
 
 template <typename T>
@@ -159,12 +170,19 @@ struct Handle {
     unsigned iteration = 0, iterations = 0, reportStep = 1;
     std::vector<Species> sp;
     bool outlet = false;
-    std::vector<int> bio;  // 1 tension, 2 area regulator, 3 cell junctions, 4 cell division
+    // 1 tension, 2 area regulator, 3 cell junctions, 4 cell division (host),
+    // 5 differentiation (host), 6 growth
+    std::vector<int> bio;
     double tensionForce = 0.01;
     unsigned tensionFreq = 10;
     // tutorial_01_BioSolverCellJunction.cpp:37-41
     double junctionRadius = 1.0, junctionK = 0.02, junctionL0 = 0.5;
     double areaFactor = 1.2, areaStrength = 0.01, areaMax = 0.004;
+    bool areaTutorial = false;   // tutorial_01_BioSolverAreaRegulator's rule
+    int diffSpecies = -1;        // the species differentiation reads
+    bool diffInit = false;       // its one-time reset of the cell-type map done
+    int growthR = -1, growthL = -1;
+    double* massNode = nullptr;  // per-node mass source (growth)
 
     // lattice buffers
     void* f[2] = {nullptr, nullptr};
@@ -258,7 +276,7 @@ Handle::~Handle() {
     delete diff;
     auto fr = [](void* p) { if (p) cudaFree(p); };
     for (int i = 0; i < 2; ++i) { fr(f[i]); fr(g[i]); }
-    fr(u); fr(force); fr(dom); fr(massTab); fr(srcTab); fr(ctypeTab);
+    fr(u); fr(force); fr(dom); fr(massTab); fr(massNode); fr(srcTab); fr(ctypeTab);
     fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id);
     fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
@@ -314,18 +332,59 @@ static void load_parameters(Handle& h, const std::string& fn) {
             while (ls >> nm >> tau) cdes[nm] = tau;
         } else fail(ERR_INPUT, "An unknown parameter was passed in the global Parameter file");
     }
+    // The reference's CDE solvers by name (libs/LbmLib/src/solver/CDESolver),
+    // and the Lbib species plugins (any other name): reaction kind, partner
+    // species, reinitialise() variant, deltaT and initial condition.
     for (auto& kv : cdes) {
         Species s;
         s.name = kv.first;
         s.c.tau = kv.second;
         s.c.decay = 0.0;
-        if (kv.first == "CDESolverD2Q5") s.c.kind = RX_NONE;
-        else if (kv.first == "tutorial_01_CDESolverD2Q5_SIGNAL") s.c.kind = RX_SIGNAL;
-        else s.c.kind = RX_LINEAR;
+        s.c.partner = -1;
+        s.c.reinit = RI_BASE;
+        s.c.dt = 1.0;
+        s.c.hill = 0.0;
+        const std::string& nm = kv.first;
+        if (nm == "CDESolverD2Q5") {
+            s.c.kind = RX_NONE;
+        } else if (nm == "tutorial_01_CDESolverD2Q5_SIGNAL" || nm == "CDESolverD2Q5HH") {
+            s.c.kind = RX_SIGNAL;
+            s.c.reinit = RI_ALL4;
+        } else if (nm == "tutorial_02_CDESolverD2Q5_R" || nm == "tutorial_02_CDESolverD2Q5_L") {
+            s.c.kind = nm.back() == 'R' ? RX_T2_R : RX_T2_L;
+            s.c.reinit = RI_ALL4;
+            s.partnerName = nm.back() == 'R' ? "tutorial_02_CDESolverD2Q5_L" : "tutorial_02_CDESolverD2Q5_R";
+            s.initStyle = INIT_T2;
+        } else if (nm == "SchnakenbergD2Q5u" || nm == "SchnakenbergD2Q5v") {
+            s.c.kind = nm.back() == 'u' ? RX_SCHNAK_U : RX_SCHNAK_V;
+            s.c.reinit = RI_DIAG;
+            s.c.dt = 20.0 / (double)h.iterations;  // SchnakenbergD2Q5u.cpp:57
+            s.partnerName = nm.back() == 'u' ? "SchnakenbergD2Q5v" : "SchnakenbergD2Q5u";
+            s.initStyle = INIT_SCHNAK;
+        } else if (nm == "CDESolverD2Q5BMP") {
+            s.c.kind = RX_BMP;
+            s.c.reinit = RI_ALL4;
+            s.c.hill = std::pow(0.01, 4.0);  // pow(k_hill, n_hill), CDESolverD2Q5BMP.cpp:113-117
+            s.partnerName = "CDESolverD2Q5HH";
+            s.initStyle = INIT_ZERO;
+        } else if (nm.compare(0, 4, "Lbib") == 0) {
+            s.c.kind = RX_LINEAR;
+        } else {
+            // DiracD2Q5 (whose advect keeps the populations of boundary links,
+            // DiracD2Q5.cpp:166-180) and the D2Q4 solvers are not built
+            fail(ERR_INPUT, "unknown or unsupported CDE solver " + nm);
+        }
         h.sp.push_back(s);
     }
     h.S = (int)h.sp.size();
     if (h.S > kMaxSpecies) fail(ERR_INPUT, "at most 3 CDE species are supported");
+    for (auto& s : h.sp) {
+        if (s.partnerName.empty()) continue;
+        for (int j = 0; j < h.S; ++j)
+            if (h.sp[j].name == s.partnerName) s.c.partner = j;
+        // PhysicalNode::getCDESolverSlow throws for a solver the node lacks
+        if (s.c.partner < 0) fail(ERR_INPUT, s.name + " needs the CDE solver " + s.partnerName);
+    }
     if (h.nx < 8 || h.ny < 8) fail(ERR_INPUT, "lattice too small");
 }
 
@@ -351,6 +410,28 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 if (kv.count("force")) h.tensionForce = kv["force"];
                 if (kv.count("frequency")) h.tensionFreq = (unsigned)kv["frequency"];
                 if (h.tensionFreq == 0) fail(ERR_INPUT, "tension frequency must be positive");
+            } else if (name == "tutorial_01_BioSolverMembraneTension" ||
+                       name == "tutorial_02_BioSolverMembraneTension" || name == "BioSolverMembraneTension") {
+                // the same renewal with the constants of each file (FREQUENCY 10; FORCE
+                // 0.01, 0.005, 0.02: tutorial_01_BioSolverMembraneTension.cpp:34-35,
+                // tutorial_02_...:34-35, BioSolverMembraneTension.cpp:34-35)
+                h.bio.push_back(1);
+                h.tensionFreq = 10;
+                h.tensionForce = name == "tutorial_01_BioSolverMembraneTension"   ? 0.01
+                                 : name == "tutorial_02_BioSolverMembraneTension" ? 0.005
+                                                                                  : 0.02;
+            } else if (name == "tutorial_01_BioSolverAreaRegulator") {
+                // tutorial_01_BioSolverAreaRegulator.cpp:34-37: TARGETAREA 200, KP 1e-5, MAXSOURCE 0.004
+                h.bio.push_back(2);
+                h.areaTutorial = true;
+                h.areaFactor = 200.0;
+                h.areaStrength = 0.00001;
+                h.areaMax = 0.004;
+            } else if (name == "tutorial_01_BioSolverDifferentiation" || name == "BioSolverDifferentiation") {
+                // tutorial_01_BioSolverDifferentiation.cpp:33-84 (host, every 100th iteration)
+                h.bio.push_back(5);
+            } else if (name == "tutorial_02_BioSolverGrowth") {
+                h.bio.push_back(6);
             } else if (name == "tutorial_01_BioSolverCellJunction" || name == "tutorial_02_BioSolverCellJunction" ||
                        name == "BioSolverCellJunction" || name == "LbibCellJunction") {
                 // the reference's solvers take no parameters; LbibCellJunction is
@@ -367,6 +448,7 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 h.divisionPolicy = name == "BioSolverCellDivision" ? 1 : 0;
             } else if (name == "LbibAreaRegulator") {
                 h.bio.push_back(2);
+                h.areaTutorial = false;
                 if (kv.count("factor")) h.areaFactor = kv["factor"];
                 if (kv.count("strength")) h.areaStrength = kv["strength"];
                 if (kv.count("maxsource")) h.areaMax = kv["maxsource"];
@@ -374,6 +456,12 @@ static void load_plugins(Handle& h, const std::string& fn) {
             if (h.bio.size() > 8) fail(ERR_INPUT, "more than 8 bio solvers");
             for (size_t q = 0; q + 1 < h.bio.size(); ++q)
                 if (h.bio[q] == 4) fail(ERR_INPUT, "the cell-division solver must be the last bio solver");
+            // the host bio solvers run after the device's step: none may precede a device one
+            bool host = false;
+            for (int b : h.bio) {
+                if (b == 4 || b == 5) host = true;
+                else if (host) fail(ERR_INPUT, "differentiation and cell division must follow the other bio solvers");
+            }
         } else if (kind == "CDE") {
             std::string k; double v;
             while (ls >> k >> v) kv[k] = v;
@@ -388,6 +476,29 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 for (auto& s : h.sp)
                     if (s.name == name) s.source[d] = r;
         } else fail(ERR_INPUT, "unknown plugin line " + kind);
+    }
+}
+
+// Checks of the bio solvers that read species or share state, once the
+// parameter and plugin files are both read.
+static void check_bio(Handle& h) {
+    auto species = [&](const char* nm) {
+        for (int k = 0; k < h.S; ++k)
+            if (h.sp[k].name == nm) return k;
+        // PhysicalNode::getCDESolverSlow throws for a solver the node lacks
+        fail(ERR_INPUT, std::string("a bio solver needs the CDE solver ") + nm);
+        return -1;
+    };
+    int count[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int b : h.bio) count[b]++;
+    if (count[1] > 1 || count[2] > 1)
+        fail(ERR_INPUT, "one membrane-tension and one area-regulator solver at most");
+    if (count[5]) h.diffSpecies = species("tutorial_01_CDESolverD2Q5_SIGNAL");
+    if (count[6]) {
+        h.growthR = species("tutorial_02_CDESolverD2Q5_R");
+        h.growthL = species("tutorial_02_CDESolverD2Q5_L");
+        // FluidSolver::addMass overwrites: the two would depend on their order
+        if (count[2]) fail(ERR_INPUT, "tutorial_02_BioSolverGrowth and an area regulator both set the mass source");
     }
 }
 
@@ -870,10 +981,15 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     bool area = false;
     for (int b : h.bio) area |= (b == 2);
     a.massTab = area ? h.massTab : nullptr;
+    a.massNode = h.massNode;
     a.nDomains = h.nDomains;
     a.srcTab = h.srcTab;
+    a.ctypeTab = h.ctypeTab;
     a.tauF = h.tauF;
-    for (int k = 0; k < h.S; ++k) a.sp[k] = h.sp[k].c;
+    for (int k = 0; k < h.S; ++k) {
+        a.sp[k] = h.sp[k].c;
+        a.coupled |= coupled_kind(h.sp[k].c.kind) ? 1 : 0;
+    }
     a.status = h.st;
     a.outlet = h.outlet ? 1 : 0;
     if (h.cross.nfTab != nullptr) {
@@ -985,15 +1101,23 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
         for (size_t q = 0; q < h.bio.size(); ++q) {
             const int b = h.bio[q], op = (bioOps >> (2 * q)) & 3;
             if (b == 2) {
+                const uint32_t* ct = h.areaTutorial ? h.ctypeTab : nullptr;
                 if (sizeof(Real) == 8) {
                     launch_area_regulator(h.m, h.area, h.target, h.massTab, h.nDomains, h.areaFactor,
-                                          h.areaStrength, h.areaMax, h.st, s);
+                                          h.areaStrength, h.areaMax, ct, h.st, s);
                     nl += h.m.nCells > 0 ? 2 : 0;
                 } else {
                     launch_area_regulator_fixed(h.m, h.td.cellOfDom, h.areaAcc, h.area, h.target, h.massTab,
-                                                h.nDomains, h.areaFactor, h.areaStrength, h.areaMax, h.st, s);
+                                                h.nDomains, h.areaFactor, h.areaStrength, h.areaMax, ct, h.st, s);
                     nl += h.m.nCells > 0 ? 3 : 0;
                 }
+                if (h.massNode != nullptr) {
+                    launch_mass_expand(h.dom, h.L, h.massTab, h.nDomains, h.massNode, h.st, s);
+                    nl += 1;
+                }
+            } else if (b == 6) {
+                launch_growth<Real>(gcur, h.dom, h.L, h.growthR, h.growthL, h.massNode, h.st, s);
+                nl += 1;
             } else if (b == 1 && op == BIO_TENSION_FILL) {
                 launch_tension_renewal(h.m, h.outPos, h.inPos, h.tensionForce, s);
                 nl += hasM ? 2 : 0;
@@ -1161,21 +1285,38 @@ static void launch_step_graph(Handle& h, int parity, bool coarsenStep, int bioOp
     h.launches += g.launches;
 }
 
-static bool has_division(const Handle& h) {
-    return std::find(h.bio.begin(), h.bio.end(), 4) != h.bio.end();
+// Bio solvers that run on the host after the device's step: cell division
+// (kind 4) and differentiation (kind 5), each every 100th iteration.
+static bool host_bio_at(const Handle& h, unsigned it) {
+    for (int b : h.bio) {
+        if (b == 4 && it % h.divisionFreq == 0) return true;
+        if (b == 5 && it % 100u == 0) return true;
+    }
+    return false;
 }
 static void run_division(Handle& h);
+static void run_differentiation(Handle& h);
+static std::map<uint32_t, double> accumulated_concentrations(Handle& h, int k);
+static void grow_domains(Handle& h, int nd);
+// The host bio solvers of iteration `it` (the step just run), in list order.
+static void run_host_bio(Handle& h, unsigned it) {
+    for (int b : h.bio) {
+        if (b == 5 && it % 100u == 0) run_differentiation(h);
+        if (b == 4 && it % h.divisionFreq == 0) run_division(h);
+    }
+}
 
 template <typename Real>
 static void run_steps(Handle& h, int n) {
     const int kBatch = 64;
-    const bool division = has_division(h);
+    const bool hostBio = std::find_if(h.bio.begin(), h.bio.end(), [](int b) { return b == 4 || b == 5; }) !=
+                         h.bio.end();
     while (n > 0) {
         int B = std::min(n, kBatch);
-        if (division) {
-            // the batch ends with the next division step; the division follows it
+        if (hostBio) {
+            // the batch ends with the next step that has host bio solvers; they follow it
             for (int b = 0; b < B; ++b)
-                if ((h.iteration + b) % h.divisionFreq == 0) {
+                if (host_bio_at(h, h.iteration + b)) {
                     B = b + 1;
                     break;
                 }
@@ -1216,7 +1357,7 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += done;
         if (done > 0) h.cellTypesCopied = true;
         n -= done;
-        if (division && done > 0 && (h.iteration - 1) % h.divisionFreq == 0) run_division(h);
+        if (hostBio && done > 0) run_host_bio(h, h.iteration - 1);
         if (!st.halt) continue;
         if (st.err) {
             h.err = st.err;
@@ -1249,7 +1390,7 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += 1;
         h.cellTypesCopied = true;
         n -= 1;
-        if (division && (h.iteration - 1) % h.divisionFreq == 0) run_division(h);
+        if (hostBio) run_host_bio(h, h.iteration - 1);
     }
 }
 
@@ -1259,6 +1400,54 @@ static void run_steps(Handle& h, int n) {
 static void cure_lattice(Handle& h, HostMembrane& hm);
 static void setup_boundary_solvers(Handle& h);
 
+// The initial conditions of the species whose initSolver the init kernels do
+// not cover, set on the host in SimulationRunner::initSolvers' node order
+// (rows, then columns; SimulationRunner.cpp:290-306).  The reference seeds its
+// generators from std::random_device, so no two of its runs agree; here each
+// solver type has one std::mt19937 with the default seed, drawn in that order.
+static void init_species_host(Handle& h) {
+    bool any = false;
+    for (const auto& s : h.sp) any |= s.initStyle != INIT_KERNEL;
+    if (!any) return;
+    const size_t L = h.L;
+    std::vector<uint32_t> dom(L);
+    CK(cudaMemcpyAsync(dom.data(), h.dom, sizeof(uint32_t) * L, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    std::map<int, std::mt19937> gens;  // one generator per solver type
+    for (int k = 0; k < h.S; ++k) {
+        const Species& s = h.sp[k];
+        if (s.initStyle == INIT_KERNEL) continue;
+        std::mt19937& gen = gens[s.c.kind];
+        std::uniform_real_distribution<> dis(-0.01, 0.01);
+        std::vector<double> g(5 * L);
+        for (size_t n = 0; n < L; ++n) {
+            double gi[5];
+            switch (s.initStyle) {
+                case INIT_T2:
+                    for (int q = 0; q < 5; ++q) gi[q] = dom[n] == 0 ? 0.0 : (1.0 + dis(gen)) / 5.0;
+                    break;
+                case INIT_SCHNAK: {
+                    const double temp = 0.2 * (1.0 + dis(gen));
+                    for (int q = 0; q < 5; ++q) gi[q] = dom[n] == 0 ? 0.0 : temp;
+                    break;
+                }
+                default:
+                    for (int q = 0; q < 5; ++q) gi[q] = 0.0;
+            }
+            for (int q = 0; q < 5; ++q) g[(size_t)q * L + n] = gi[q];
+        }
+        if (h.precision == LBIB_FP64) {
+            CK(cudaMemcpyAsync((double*)h.g[0] + (size_t)k * 5 * L, g.data(), sizeof(double) * 5 * L,
+                               cudaMemcpyHostToDevice, h.stream));
+        } else {
+            std::vector<float> gf(g.begin(), g.end());
+            CK(cudaMemcpyAsync((float*)h.g[0] + (size_t)k * 5 * L, gf.data(), sizeof(float) * 5 * L,
+                               cudaMemcpyHostToDevice, h.stream));
+        }
+        CK(cudaStreamSynchronize(h.stream));
+    }
+}
+
 static void create(Handle& h, const std::string& params, const std::string& geom, const std::string& forceFile,
                    const std::string& plugins) {
     CK(cudaSetDevice(h.device));
@@ -1267,6 +1456,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaEventCreate(&h.evB));
     load_parameters(h, params);
     load_plugins(h, plugins);
+    check_bio(h);
+    for (const auto& sp : h.sp) h.cross.diag8 |= sp.c.reinit == RI_DIAG ? 1 : 0;
     h.L = (size_t)h.nx * h.ny;
     const size_t rs = h.precision == LBIB_FP64 ? sizeof(double) : sizeof(float);
     for (int i = 0; i < 2; ++i) {
@@ -1381,6 +1572,13 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     h.nDomains = (int)maxDom + 1;
     h.massTab = dalloc<double>(h.nDomains);
     CK(cudaMemsetAsync(h.massTab, 0, sizeof(double) * h.nDomains, h.stream));
+    // per-node sources: growth, or an area regulator in a run whose cell
+    // division changes domains after the bio step
+    const bool areaDiv = std::count(h.bio.begin(), h.bio.end(), 2) && std::count(h.bio.begin(), h.bio.end(), 4);
+    if (h.growthR >= 0 || areaDiv) {
+        h.massNode = dalloc<double>(h.L);
+        CK(cudaMemsetAsync(h.massNode, 0, sizeof(double) * h.L, h.stream));
+    }
     std::vector<double> src((size_t)std::max(1, h.S) * h.nDomains, 0.0);
     for (int k = 0; k < h.S; ++k)
         for (auto& kv : h.sp[k].source) src[(size_t)k * h.nDomains + kv.first] = kv.second;
@@ -1420,6 +1618,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
         launch_init64((double*)h.f[0], (double*)h.g[0], (double*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
     else
         launch_init32((float*)h.f[0], (float*)h.g[0], (float*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
+    init_species_host(h);
     h.cur = 0;
     // SimulationRunner::initForceSolver: the force list
     if (!h.forcemap.empty()) upload_topology(h, hm, true);
@@ -2015,6 +2214,79 @@ int lbib_areas_static(lbib_handle* hh, unsigned* dom, double* area, int cap) {
     }
 }
 
+// GeometryHandler::computeAccumulatedDomainConcentrations(name)
+// (GeometryHandler.cpp:136-147).
+int lbib_accumulated_concentrations(lbib_handle* hh, const char* species, unsigned* dom, double* acc, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    int count = 0;
+    try {
+        cudaSetDevice(h.device);
+        if (species == nullptr || dom == nullptr || acc == nullptr) lbib::fail(LBIB_ERR_INPUT, "null argument");
+        int k = -1;
+        for (int j = 0; j < h.S; ++j)
+            if (h.sp[j].name == species) k = j;
+        if (k < 0) lbib::fail(LBIB_ERR_INPUT, std::string("no CDE solver ") + species);
+        const auto m = lbib::accumulated_concentrations(h, k);
+        if ((int)m.size() > cap) lbib::fail(LBIB_ERR_CAPACITY, "accumulated concentrations: buffer too small");
+        for (const auto& kv : m) {
+            dom[count] = kv.first;
+            acc[count] = kv.second;
+            ++count;
+        }
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index;
+        return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
+    }
+    return count;
+}
+
+// GeometryHandler::getCellTypeTrackerMap()[dom] = type, then
+// copyCellTypeToPhysicalNodes (GeometryHandler.cpp:267-314).
+int lbib_set_cell_types(lbib_handle* hh, const unsigned* dom, const unsigned* type, int n) {
+    API_BEGIN(hh)
+    if (n < 0 || (n > 0 && (dom == nullptr || type == nullptr))) lbib::fail(LBIB_ERR_INPUT, "bad cell-type list");
+    unsigned top = 0;
+    for (int i = 0; i < n; ++i) top = std::max(top, dom[i]);
+    if (n > 0) lbib::grow_domains(h, (int)top + 1);
+    for (int i = 0; i < n; ++i) h.ctypeHost[dom[i]] = type[i];
+    CK(cudaMemcpyAsync(h.ctypeTab, h.ctypeHost.data(), sizeof(uint32_t) * h.nDomains, cudaMemcpyHostToDevice,
+                       h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    h.cellTypesCopied = true;
+    API_END
+}
+
+// GeometryHandler::getCellTypeTrackerMap (GeometryHandler.cpp:316-319): the
+// type of every domain id below the handle's domain count.
+int lbib_get_cell_types(lbib_handle* hh, unsigned* dom, unsigned* type, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    int count = 0;
+    try {
+        cudaSetDevice(h.device);
+        if (dom == nullptr || type == nullptr) lbib::fail(LBIB_ERR_INPUT, "null argument");
+        if ((int)h.ctypeHost.size() > cap) lbib::fail(LBIB_ERR_CAPACITY, "cell types: buffer too small");
+        for (size_t d = 0; d < h.ctypeHost.size(); ++d) {
+            dom[count] = (unsigned)d;
+            type[count] = h.ctypeHost[d];
+            ++count;
+        }
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index;
+        return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
+    }
+    return count;
+}
+
 int lbib_set_species_source(lbib_handle* hh, int k, const double* rates, int n) {
     API_BEGIN(hh)
     if (k < 0 || k >= h.S || n < 0 || n > h.nDomains || (n > 0 && !rates))
@@ -2067,6 +2339,10 @@ int lbib_diff_begin(lbib_handle* hh, int T, int K) {
     if (h.precision != LBIB_FP64) lbib::fail(LBIB_ERR_STATE, "differentiated runs need an FP64 handle");
     if (h.cross.nfTab != nullptr)
         lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover boundary solvers on connections");
+    if (h.massNode != nullptr) lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover per-node mass sources");
+    for (int k = 0; k < h.S; ++k)
+        if (lbib::coupled_kind(h.sp[k].c.kind))
+            lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover the coupled reaction of " + h.sp[k].name);
     if (T < 1) lbib::fail(LBIB_ERR_INPUT, "differentiated run: T must be at least 1");
     if (K <= 0) K = (int)std::ceil(std::sqrt((double)T));
     if (K > T) K = T;
@@ -3005,6 +3281,11 @@ static void run_division(Handle& h) {
         const uint32_t newId = divide_cell(h, hm, it->first, cellsOf());
         grow_domains(h, (int)newId + 1);
         h.ctypeHost[newId] = it->first < h.ctypeHost.size() ? h.ctypeHost[it->first] : 1u;
+        // the daughter's nodes keep the mass source the step's area regulator
+        // gave them (FluidSolver::addMass ran before the division)
+        if (it->first < (uint32_t)h.nDomains)
+            CK(cudaMemcpyAsync(h.massTab + newId, h.massTab + it->first, sizeof(double), cudaMemcpyDeviceToDevice,
+                               h.stream));
         // the edited topology on the device (the force list stays: no node
         // changed), then GeometryHandler::cureLattice
         std::vector<int> foff(h.m.M + 1);
@@ -3020,6 +3301,58 @@ static void run_division(Handle& h) {
     CK(cudaMemcpyAsync(h.ctypeTab, h.ctypeHost.data(), sizeof(uint32_t) * h.nDomains, cudaMemcpyHostToDevice,
                        h.stream));
     CK(cudaStreamSynchronize(h.stream));
+}
+
+// GeometryHandler::computeAccumulatedDomainConcentrations (GeometryHandler.cpp:
+// 136-147): per domain, the sum of species k's getC() over the lattice, rows
+// in order and columns from x = 1 (column 0 is left out, as there).
+static std::map<uint32_t, double> accumulated_concentrations(Handle& h, int k) {
+    const size_t L = h.L;
+    std::vector<uint32_t> dom(L);
+    const size_t rs = h.precision == LBIB_FP64 ? sizeof(double) : sizeof(float);
+    std::vector<unsigned char> raw(5 * L * rs);
+    CK(cudaMemcpyAsync(dom.data(), h.dom, sizeof(uint32_t) * L, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(raw.data(), (const unsigned char*)h.g[h.cur] + (size_t)k * 5 * L * rs, 5 * L * rs,
+                       cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    auto val = [&](int q, size_t n) {
+        return rs == 8 ? ((const double*)raw.data())[(size_t)q * L + n] : (double)((const float*)raw.data())[(size_t)q * L + n];
+    };
+    std::map<uint32_t, double> acc;
+    for (int y = 0; y < h.ny; ++y)
+        for (int x = 1; x < h.nx; ++x) {
+            const size_t n = (size_t)y * h.nx + x;
+            double C = 0.0;  // getC(): slots T, W, S, E, N after localSwap
+            C += val(0, n);
+            C += val(3, n);
+            C += val(4, n);
+            C += val(1, n);
+            C += val(2, n);
+            acc[dom[n]] += C;
+        }
+    return acc;
+}
+
+// tutorial_01_BioSolverDifferentiation::applyBioProcess
+// (tutorial_01_BioSolverDifferentiation.cpp:42-84): the first call resets the
+// cell-type map (domain 0 type 0, every cell type 1); each call marks the
+// cells whose accumulated signal is below THRESHOLD 1.6 as type 2 (the map's
+// first domain, the extracellular one, is skipped) and copies the map to the
+// lattice.  The reference's reset runs once per process (a std::once_flag);
+// here it runs once per handle.
+static void run_differentiation(Handle& h) {
+    const std::map<uint32_t, double> acc = accumulated_concentrations(h, h.diffSpecies);
+    if (!h.diffInit) {
+        h.diffInit = true;
+        std::fill(h.ctypeHost.begin(), h.ctypeHost.end(), 1u);
+        if (!h.ctypeHost.empty()) h.ctypeHost[0] = 0;
+    }
+    for (auto it = std::next(acc.begin()); it != acc.end(); ++it)
+        if (it->second < 1.6 && it->first < h.ctypeHost.size()) h.ctypeHost[it->first] = 2;
+    CK(cudaMemcpyAsync(h.ctypeTab, h.ctypeHost.data(), sizeof(uint32_t) * h.nDomains, cudaMemcpyHostToDevice,
+                       h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    h.cellTypesCopied = true;
 }
 
 }  // namespace lbib

@@ -132,8 +132,28 @@ __device__ __forceinline__ void raise_halt(Status* st, int stage) {
     atomicCAS(&st->haltStage, 0, stage);
 }
 
-// Reaction kinds of the CDE species.
-enum Reaction { RX_NONE = 0, RX_LINEAR = 1, RX_SIGNAL = 2 };
+// Reaction kinds of the CDE species (the reaction term of each solver's collide):
+//   RX_NONE      CDESolverD2Q5
+//   RX_LINEAR    source[domain] - decay*C (the Lbib species plugins)
+//   RX_SIGNAL    tutorial_01_CDESolverD2Q5_SIGNAL.cpp:92-100; CDESolverD2Q5HH.cpp:113-129
+//                computes the same terms with the same constants
+//   RX_T2_R/L    tutorial_02_CDESolverD2Q5_R.cpp:94-105 / _L.cpp:94-106 (partner L / R)
+//   RX_SCHNAK_U/V SchnakenbergD2Q5u.cpp:114-121 / v.cpp:110-117 (partner v / u)
+//   RX_BMP       CDESolverD2Q5BMP.cpp:107-120 (partner CDESolverD2Q5HH, cell type 2)
+enum Reaction {
+    RX_NONE = 0, RX_LINEAR = 1, RX_SIGNAL = 2, RX_T2_R = 3, RX_T2_L = 4, RX_SCHNAK_U = 5, RX_SCHNAK_V = 6,
+    RX_BMP = 7
+};
+// The kinds whose reaction reads another species or the cell type.
+__host__ __device__ __forceinline__ bool coupled_kind(int kind) { return kind >= RX_T2_R; }
+
+// reinitialise() variants (domain change of a lattice node):
+//   RI_BASE  CDESolverD2Q5.cpp:156-228: E,N,W,S, then the diagonals, else 0/0
+//   RI_ALL4  tutorial_01_CDESolverD2Q5_SIGNAL.cpp:184-250 (and tutorial_02 R/L,
+//            BMP, HH): as RI_BASE, then all of E,N,W,S whatever their domain
+//   RI_DIAG  SchnakenbergD2Q5u.cpp:190-231 and v: the four diagonals
+//            of the same domain without the boundary-node test, C/4 per slot
+enum Reinit { RI_BASE = 0, RI_ALL4 = 1, RI_DIAG = 2 };
 
 constexpr int kMaxSpecies = 3;
 
@@ -142,6 +162,10 @@ struct SpeciesConst {
     int kind;
     double tau;
     double decay;
+    int partner;    // species index the reaction reads (-1: none)
+    int reinit;     // Reinit
+    double dt;      // the solver's deltaT (SchnakenbergD2Q5u/v: 20 / Iterations; BMP: 1)
+    double hill;    // RX_BMP: pow(k_hill, n_hill) as the host's pow gives it
 };
 
 // Boundary solvers on connections (the "bsolver cdesolver" pairs of a
@@ -175,10 +199,13 @@ struct LatticeArgs {
     int tilesX;
     const uint32_t* dom;  // L
     const double* massTab;     // per-domain rhoToAdd (nullptr: none)
+    const double* massNode;    // per-node rhoToAdd (nullptr: none; replaces massTab)
     int nDomains;              // entries in massTab / srcTab rows
     const double* srcTab;      // [S][nDomains] production per step
+    const uint32_t* ctypeTab;  // per-domain cell type (read by RX_BMP)
     double tauF;
     SpeciesConst sp[kMaxSpecies];
+    int coupled;               // some species has a coupled_kind reaction
     const Status* status;
     int outlet;                // MassSolverBoxOutlet registered: rescale x=0 / y=0 nodes
     // no-flux boundary nodes of the previous step's crossings (nullptr: none)

@@ -150,6 +150,30 @@ class Simulation:
             raise self._error()
         return {int(d[i]): float(a[i]) for i in range(n)}
 
+    def accumulated_concentrations(self, species: str) -> Dict[int, float]:
+        """GeometryHandler::computeAccumulatedDomainConcentrations(species)."""
+        cap = max(1, self.domain_count())
+        d = np.zeros(cap, np.uint32); a = np.zeros(cap)
+        n = self._L.lbib_accumulated_concentrations(self._h, species.encode(), _p(d), _p(a), cap)
+        if n < 0:
+            raise self._error()
+        return {int(d[i]): float(a[i]) for i in range(n)}
+
+    def set_cell_types(self, types: Dict[int, int]) -> None:
+        """getCellTypeTrackerMap()[d] = t for each entry, then copyCellTypeToPhysicalNodes."""
+        d = np.array(sorted(types), np.uint32)
+        t = np.array([types[int(k)] for k in d], np.uint32)
+        self._check(self._L.lbib_set_cell_types(self._h, _p(d), _p(t), len(d)))
+
+    def cell_types(self) -> Dict[int, int]:
+        """GeometryHandler::getCellTypeTrackerMap."""
+        cap = max(1, self.domain_count())
+        d = np.zeros(cap, np.uint32); t = np.zeros(cap, np.uint32)
+        n = self._L.lbib_get_cell_types(self._h, _p(d), _p(t), cap)
+        if n < 0:
+            raise self._error()
+        return {int(d[i]): int(t[i]) for i in range(n)}
+
     # -- topology edits by host bio solvers -----------------------------------------
     def upload_membrane(self, ids, xy, conns) -> None:
         """The membrane after a host plugin's edits (see lbib_upload_membrane):

@@ -9,7 +9,8 @@
 // AbstractReportFunctor.hpp) dumps the state every ReportStep iterations.
 //
 // usage: ref_driver params.txt geometry.txt force.txt plugins.txt outdir
-//                   [timing W K] [restart SOLVERFILE] [write PREFIX] [edit ITER FILE]
+//                   [timing W K] [restart SOLVERFILE] [write PREFIX] [edit ITER FILE] [run N]
+//                   [celltype DOMAIN TYPE]...
 //   With "timing W K" no reporter is registered: runSimulation() runs W
 //   untimed iterations, then K iterations whose wall time is printed as JSON
 //   (the CPU baseline).  "restart SOLVERFILE" loads the distributions with
@@ -17,7 +18,12 @@
 //   calls SimulationRunner::writeSimulation at the end, into PREFIX_force.txt,
 //   PREFIX_geometry.txt, PREFIX_parameters.txt and PREFIX_solver.txt.  "edit
 //   ITER FILE" stops at iteration ITER, applies the topology edit in FILE
-//   through GeometryHandler (applyEdit), cures the lattice and runs on.  The log
+//   through GeometryHandler (applyEdit), cures the lattice and runs on.  "run N"
+//   runs N iterations where the parameter file's Iterations count is larger
+//   (the solvers' initSolver still sees the file's count).  "celltype D T"
+//   sets the cell type of domain D in GeometryHandler's cell-type tracker map
+//   and copies the map to the lattice (copyCellTypeToPhysicalNodes) after
+//   initSolvers, as a host bio solver does.  The log
 //   goes to outdir/log.txt as in apps/tutorial_01.cpp:47-57.
 //
 // Dump file outdir/dump_<t>.bin (little endian):
@@ -248,7 +254,8 @@ int main(int argc, char** argv) {
     bool timing = false;
     unsigned warm = 0, steps = 0;
     std::string restartFile, writePrefix, editFile;
-    unsigned editIter = 0;
+    unsigned editIter = 0, runIters = 0;
+    std::vector<std::pair<unsigned, unsigned>> cellTypes;
     for (int a = 6; a < argc; ++a) {
         const std::string k = argv[a];
         if (k == "timing" && a + 2 < argc) {
@@ -260,6 +267,11 @@ int main(int argc, char** argv) {
             restartFile = argv[++a];
         } else if (k == "write" && a + 1 < argc) {
             writePrefix = argv[++a];
+        } else if (k == "run" && a + 1 < argc) {
+            runIters = (unsigned)std::stoul(argv[++a]);
+        } else if (k == "celltype" && a + 2 < argc) {
+            cellTypes.emplace_back((unsigned)std::stoul(argv[a + 1]), (unsigned)std::stoul(argv[a + 2]));
+            a += 2;
         } else if (k == "edit" && a + 2 < argc) {
             editIter = (unsigned)std::stoul(argv[a + 1]);
             editFile = argv[a + 2];
@@ -283,9 +295,14 @@ int main(int argc, char** argv) {
                 new DumpReporter(geohandler, argv[5])));
         simRunner.initSolvers();
         if (!restartFile.empty()) simRunner.initSolvers(restartFile);
+        if (!cellTypes.empty()) {
+            for (const auto& ct : cellTypes) geohandler.getCellTypeTrackerMap()[ct.first] = ct.second;
+            geohandler.copyCellTypeToPhysicalNodes(geohandler.getCellTypeTrackerMap());
+        }
         simRunner.initForceSolver(argv[3]);
         if (pl.outlet) simRunner.addMassSolver("MassSolverBoxOutlet");
         for (const auto& b : pl.bio) simRunner.addBioSolver(b);
+        if (runIters) LbmLib::Parameters.iterations_ = runIters;
         if (!timing && !editFile.empty()) {
             // run to the edit's iteration, edit, run the rest
             const unsigned total = LbmLib::Parameters.iterations_;
