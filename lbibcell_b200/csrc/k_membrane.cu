@@ -1331,13 +1331,20 @@ __global__ void __launch_bounds__(256) areas_kernel(MembraneDev m, double* area,
 // tutorial_01_BioSolverAreaRegulator (tutorial_01_BioSolverAreaRegulator.cpp:
 // 44-97): target = factor (TARGETAREA), rate strength (target - A) (KP), and
 // cells of type 1 get maxsource whatever their area.
-__global__ void area_regulator_kernel(MembraneDev m, const double* area, double* target, double* massTab,
+// acc != nullptr (FP32-shifted runs): the cell's area is first formed from
+// its fixed-point sum, which is reset for the next step (on a halted step too).
+constexpr double kAreaFix = 16777216.0;  // 2^24: the fixed-point scale of the shoelace terms
+__global__ void area_regulator_kernel(MembraneDev m, double* area, double* target, double* massTab,
                                       int nDomains, double factor, double strength, double maxsource,
-                                      const uint32_t* ctypeTab, const Status* st) {
+                                      const uint32_t* ctypeTab, unsigned long long* acc, const Status* st) {
     pdl_wait();
-    if (st->halt) return;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= m.nCells) return;
+    if (acc != nullptr) {
+        area[cell] = (double)(long long)acc[cell] * (1.0 / kAreaFix) / 2.0;
+        acc[cell] = 0ull;
+    }
+    if (st->halt) return;
     const double A = area[cell];
     double r;
     if (ctypeTab == nullptr) {
@@ -1423,7 +1430,6 @@ template void launch_growth<float>(const float*, const uint32_t*, size_t, int, i
 // order, each term x_a y_b - x_b y_a (a -> b along the ring) rounded to 64-bit
 // fixed point (2^-24), so that the integer sums are exact and independent of
 // the order; no ring ranking is needed.  FP64 runs keep the ring-ordered sum.
-constexpr double kAreaFix = 16777216.0;  // 2^24
 __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDomains, unsigned long long* acc) {
     pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1446,14 +1452,6 @@ __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDom
         atomicAdd(acc + cell, (unsigned long long)sum);
 }
 
-__global__ void areas_fixed_finish(unsigned long long* acc, int nCells, double* area) {
-    pdl_wait();
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nCells) return;
-    area[c] = (double)(long long)acc[c] * (1.0 / kAreaFix) / 2.0;
-    acc[c] = 0ull;
-}
-
 void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
     if (m.nCells == 0) return;
     launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, nullptr);
@@ -1473,7 +1471,7 @@ void launch_area_regulator(const MembraneDev& m, double* area, double* target, d
     if (m.nCells == 0) return;
     launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, (Status*)st);
     launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
-                                                                 strength, maxsource, ctypeTab, st);
+               strength, maxsource, ctypeTab, (unsigned long long*)nullptr, st);
 }
 
 void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
@@ -1481,9 +1479,8 @@ void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, uns
                                  double maxsource, const uint32_t* ctypeTab, const Status* st, cudaStream_t s) {
     if (m.nCells == 0 || m.Ccap == 0) return;
     launch_pdl(areas_fixed_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, cellOfDom, nDomains, acc);
-    launch_pdl(areas_fixed_finish, (m.nCells + 127) / 128, 128, 0, s, acc, m.nCells, area);
     launch_pdl(area_regulator_kernel, (m.nCells + 127) / 128, 128, 0, s, m, area, target, massTab, nDomains, factor,
-                                                                 strength, maxsource, ctypeTab, st);
+               strength, maxsource, ctypeTab, acc, st);
 }
 
 }  // namespace lbib

@@ -1109,7 +1109,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
                 } else {
                     launch_area_regulator_fixed(h.m, h.td.cellOfDom, h.areaAcc, h.area, h.target, h.massTab,
                                                 h.nDomains, h.areaFactor, h.areaStrength, h.areaMax, ct, h.st, s);
-                    nl += h.m.nCells > 0 ? 3 : 0;
+                    nl += h.m.nCells > 0 ? 2 : 0;
                 }
                 if (h.massNode != nullptr) {
                     launch_mass_expand(h.dom, h.L, h.massTab, h.nDomains, h.massNode, h.st, s);
