@@ -961,6 +961,8 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
     const uint32_t ctype = cellTypesCopied ? (oldDom < (uint32_t)nDomains ? ctypeTab[oldDom] : 1u) : 0u;
     const bool neNull = newDom == 0 && ctype == 0;
     double Cnew[kMaxSpecies] = {0.0, 0.0, 0.0};  // getC() of the species already re-initialised here
+    bool coupled = false;
+    for (int k = 0; k < nS; ++k) coupled |= sp[k].partner >= 0;
     for (int k = 0; k < nS; ++k) {
         const Real* gk = g + (size_t)k * 5 * L;
         // the five slots of the four neighbours and NE, read unconditionally
@@ -1034,7 +1036,7 @@ __device__ void reinit_node(size_t n, uint32_t newDom, uint32_t* dom, Real* g, c
             }
         }
         collide_cde64(gi, ux, uy, sp[k], src, Cp, newDom, ctype, iteration);
-        Cnew[k] = sum5_swapped(gi);
+        if (coupled) Cnew[k] = sum5_swapped(gi);
         Real* go = g + (size_t)k * 5 * L;
         for (int q = 0; q < 5; ++q) go[(size_t)q * L + n] = (Real)gi[q];
     }
