@@ -1370,7 +1370,8 @@ __global__ void area_regulator_kernel(MembraneDev m, double* area, double* targe
 // 44-80): every node inside a cell gets the mass source MAXSOURCE = 0.001 where
 // R^2 L > 1 (THRESHOLD) and MAXSOURCE / 10 elsewhere; R and L are the species'
 // getC() after the step (post-collide slot order T, W, S, E, N).  The source is
-// per node: FluidSolver::addMass sets the next collide's rhoToAdd.
+// per node: FluidSolver::addMass sets the next collide's rhoToAdd.  iR < 0:
+// BioSolverGrowth (BioSolverGrowth.cpp:41-62), 0.0025 at every node inside a cell.
 template <typename Real>
 __global__ void growth_kernel(const Real* g, const uint32_t* dom, size_t L, int iR, int iL, double* massNode,
                               const Status* st) {
@@ -1391,9 +1392,13 @@ __global__ void growth_kernel(const Real* g, const uint32_t* dom, size_t L, int 
             C += (double)gk[2 * L + n];
             return C;
         };
-        const double R = cOf(iR), Lc = cOf(iL);
-        const double maxsource = 0.001;
-        src = R * R * Lc > 1.0 ? maxsource : maxsource / 10.0;
+        if (iR < 0) {
+            src = 0.0025;  // BioSolverGrowth: the same source everywhere inside cells
+        } else {
+            const double R = cOf(iR), Lc = cOf(iL);
+            const double maxsource = 0.001;
+            src = R * R * Lc > 1.0 ? maxsource : maxsource / 10.0;
+        }
     }
     massNode[n] = src;
 }

@@ -182,6 +182,7 @@ struct Handle {
     int diffSpecies = -1;        // the species differentiation reads
     bool diffInit = false;       // its one-time reset of the cell-type map done
     int growthR = -1, growthL = -1;
+    bool growthConst = false;    // BioSolverGrowth (constant source) rather than tutorial_02's
     double* massNode = nullptr;  // per-node mass source (growth)
 
     // lattice buffers
@@ -430,8 +431,12 @@ static void load_plugins(Handle& h, const std::string& fn) {
             } else if (name == "tutorial_01_BioSolverDifferentiation" || name == "BioSolverDifferentiation") {
                 // tutorial_01_BioSolverDifferentiation.cpp:33-84 (host, every 100th iteration)
                 h.bio.push_back(5);
-            } else if (name == "tutorial_02_BioSolverGrowth") {
+            } else if (name == "tutorial_02_BioSolverGrowth" || name == "BioSolverGrowth") {
+                // BioSolverGrowth.cpp:33-64: every node inside a cell gets 0.0025
                 h.bio.push_back(6);
+                h.growthConst = name == "BioSolverGrowth";
+            } else if (name == "BioSolverEmpty") {
+                // BioSolverEmpty.cpp:36-45 does nothing
             } else if (name == "tutorial_01_BioSolverCellJunction" || name == "tutorial_02_BioSolverCellJunction" ||
                        name == "BioSolverCellJunction" || name == "LbibCellJunction") {
                 // the reference's solvers take no parameters; LbibCellJunction is
@@ -495,10 +500,12 @@ static void check_bio(Handle& h) {
         fail(ERR_INPUT, "one membrane-tension and one area-regulator solver at most");
     if (count[5]) h.diffSpecies = species("tutorial_01_CDESolverD2Q5_SIGNAL");
     if (count[6]) {
-        h.growthR = species("tutorial_02_CDESolverD2Q5_R");
-        h.growthL = species("tutorial_02_CDESolverD2Q5_L");
-        // FluidSolver::addMass overwrites: the two would depend on their order
-        if (count[2]) fail(ERR_INPUT, "tutorial_02_BioSolverGrowth and an area regulator both set the mass source");
+        if (!h.growthConst) {
+            h.growthR = species("tutorial_02_CDESolverD2Q5_R");
+            h.growthL = species("tutorial_02_CDESolverD2Q5_L");
+        }
+        // FluidSolver::addMass overwrites: two mass sources would depend on their order
+        if (count[2] || count[6] > 1) fail(ERR_INPUT, "two bio solvers set the mass source (growth, area regulator)");
     }
 }
 
@@ -1575,7 +1582,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     // per-node sources: growth, or an area regulator in a run whose cell
     // division changes domains after the bio step
     const bool areaDiv = std::count(h.bio.begin(), h.bio.end(), 2) && std::count(h.bio.begin(), h.bio.end(), 4);
-    if (h.growthR >= 0 || areaDiv) {
+    const bool growth = std::count(h.bio.begin(), h.bio.end(), 6) > 0;
+    if (growth || areaDiv) {
         h.massNode = dalloc<double>(h.L);
         CK(cudaMemsetAsync(h.massNode, 0, sizeof(double) * h.L, h.stream));
     }

@@ -180,3 +180,13 @@ def test_tutorial_plugins_fp32_shifted(lbib, tmp_path, which):
     ib, _ = b.membrane()
     assert len(np.setxor1d(ia, ib)) <= 0.05 * len(ia)
     assert np.isfinite(b.lattice().g).all()
+
+
+def test_plain_plugins(lbib, oracle_mod, tmp_path):
+    """The reference's non-tutorial bio solvers of the same families:
+    BioSolverGrowth (0.0025 at every node inside a cell), BioSolverEmpty,
+    BioSolverMembraneTension (FORCE 0.02) and BioSolverCellJunction
+    (BioSolverCellDivision is covered by test_division.py)."""
+    bio = ["BioSolverGrowth", "BioSolverEmpty", "BioSolverMembraneTension", "BioSolverCellJunction"]
+    sim = _run_both(lbib, oracle_mod, tmp_path, _cfg([(SIGNAL, 1.0)], bio, start=0))
+    assert len(sim.areas()) == 1
