@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import statistics
@@ -50,7 +51,30 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiated-run timing")
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="T of the differentiated run")
+    ap.add_argument("--no-large", action="store_true", help="skip the tissue_4096 block")
+    ap.add_argument("--large-steps", type=int, default=30, help="timed steps of the tissue_4096 block")
+    ap.add_argument("--no-adjoint-large", action="store_true", help="skip the adjoint_2048 block")
+    ap.add_argument("--large-cpu", action="store_true",
+                    help="time the reference CPU build on tissue_4096 too (its set-up alone takes minutes)")
+    ap.add_argument("--adjoint-large-steps", type=int, default=10000, help="T of the adjoint_2048 block")
     return ap.parse_args()
+
+
+def workload_config(cfg):
+    """The workload both arms run (the same dict in both JSON lines)."""
+    return {"workload": WORKLOAD, "lattice": [cfg.nx, cfg.ny], "species": len(cfg.species), "cells": len(cfg.cells),
+            "membrane_nodes_initial": cfg.membrane_nodes,
+            "l2": "inputs larger than L2 (lattice state ~170 MB per copy set)"}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def measured_peaks():
@@ -197,9 +221,10 @@ def reference_arm(args, cfg, paths):
         "impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / res["iterations"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": [cfg.nx, cfg.ny], "species": len(cfg.species),
-                   "cells": len(cfg.cells), "precision": "FP64 (reference CPU build, -O3 -march=x86-64-v3 -fopenmp)"},
-        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind, "sample": sample},
+        "config": workload_config(cfg),
+        "precision": "FP64 (reference CPU build, -O3 -march=x86-64-v3 -fopenmp)",
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind, "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -225,6 +250,168 @@ def rel_errors(a, b):
     out["nonfinite"] = int((~np.isfinite(a.g)).sum() + (~np.isfinite(b.g)).sum())
     out["domain_mismatch"] = int(np.count_nonzero(a.dom != b.dom))
     return out
+
+
+def fp32_error_at(paths, horizons, local):
+    """FP32-shifted vs FP64 errors (rel_errors) after each horizon of full steps,
+    with the non-finite counts: the reference's re-initialisation writes NaN
+    for nodes trapped between touching membranes (CDESolverD2Q5.cpp:223)."""
+    from lbibcell_b200 import runner
+    a = runner.Simulation(paths, runner.FP64, device=local)
+    b = runner.Simulation(paths, runner.FP32_SHIFTED, device=local)
+    out, done = {}, 0
+    for h in horizons:
+        a.step(h - done)
+        b.step(h - done)
+        done = h
+        la, lb = a.lattice(), b.lattice()
+        e = rel_errors(la, lb)
+        e["nonfinite_fp64_g"] = int((~np.isfinite(la.g)).sum())
+        e["finite_fraction_g"] = float(np.isfinite(la.g).mean())
+        out[str(h)] = e
+    a.close()
+    b.close()
+    return out
+
+
+def large_block(args, tmp, rank, world, local):
+    """tissue_4096 (configs.config3: 4096x4096, 6000 cells, ~1M membrane nodes,
+    3 species, tension, junctions, growth and division): FP32-shifted and FP64
+    step rates, the whole-step and stream-collide roofline fractions, the
+    FP32-vs-FP64 error after the same steps, and a truncated CPU baseline."""
+    from lbibcell_b200 import configs, runner
+    cfg = configs.config3(iterations=10 ** 6)
+    paths = cfg.write(os.path.join(tmp, f"large_rank{rank}"))
+    L, S = cfg.nx * cfg.ny, len(cfg.species)
+    warm, K, prof = 5, args.large_steps, 10
+    peak, _ = measured_peaks()
+    out = {"workload": f"{cfg.name}: {cfg.nx}x{cfg.ny}, {len(cfg.cells)} cells (Poisson-disk, r U(10,16)), "
+                       f"{cfg.membrane_nodes} membrane nodes at t=0, 3 species, tension, junctions, "
+                       "growth to 2.5x area, division at 2x", "steps_timed": K}
+    runs = {}
+    for name, prec in (("fp32", runner.FP32_SHIFTED), ("fp64", runner.FP64)):
+        sim = runner.Simulation(paths, prec, device=local)
+        sim.step(warm)
+        barrier(world)
+        sim.step(K)
+        ms = dist_max(sim.last_timing()["total_ms"], world)
+        sim.set_profiling(True)
+        sim.step(prof)
+        sim.set_profiling(False)
+        tp = sim.last_timing()
+        avg = tp["collide_ms"] / max(1, tp["collide_launches"])
+        bpn = (80 + 48 * S) * (2 if prec == runner.FP64 else 1)
+        mlups = world * L * K / (ms / 1e3) / 1e6
+        runs[name] = sim
+        out[name] = {"mlups": mlups, "ms_per_step": ms / K,
+                     "whole_step_roofline_frac": mlups * 1e6 * bpn / (peak * 1e9),
+                     "stream_collide_avg_ms": avg,
+                     "stream_collide_roofline_frac": bpn * L / (avg / 1e3) / 1e9 / peak,
+                     "algorithmic_bytes_per_node": bpn, "membrane_nodes": sim.sizes()["M"],
+                     "host_events": sim.sizes()["host_events"]}
+    out["fp32_over_fp64"] = out["fp32"]["mlups"] / out["fp64"]["mlups"]
+    a, b = runs["fp64"].lattice(), runs["fp32"].lattice()
+    out["fp32_vs_fp64_rel_err"] = rel_errors(a, b)
+    out["steps_compared"] = warm + K + prof
+    del a, b
+    for sim in runs.values():
+        sim.close()
+    if rank == 0 and args.large_cpu and world == 1:
+        try:
+            res = ref_cpu_time(paths, 1, 20, os.cpu_count() or 1)
+            if res is not None:
+                out["cpu_baseline_truncated"] = {
+                    "value": L * res["iterations"] / res["seconds"] / 1e6, "unit": "MLUPS",
+                    "cores": res.get("threads", 1), "cpu_model": cpu_model(),
+                    "sample": f"truncated: {res['iterations']} steps after 1 warm-up step of {cfg.name} "
+                              "(set-up excluded), reference CPU build"}
+        except Exception as e:
+            out["cpu_baseline_truncated"] = {"value": None, "sample": f"failed: {e}"[:300]}
+    return out
+
+
+def adjoint_large_block(args, tmp, rank, world, local):
+    """adjoint_2048 (configs.config5): 2048x2048, 1000 cells, fluid + 2 species,
+    frozen geometry after 3 full steps.  Parameters: the 1000 per-cell
+    area-regulator strengths s_d, entering as the mass source
+    m_d = s_d (target_d - A_d) / target_d (LbibAreaRegulator below its clamp,
+    areas frozen).  Loss: the kinetic energy of the final distributions in the
+    central 256x256 window plus sum (C_k - c_target_k)^2, c_target from a
+    forward run with the strengths perturbed by N(0, 0.1) relative.  sqrt(T)
+    checkpoints with segment recompute.  Reports adjoint/forward time, the
+    device memory in use during the run and one central-difference check."""
+    import torch
+    from lbibcell_b200 import configs, runner
+    cfg = configs.config5()
+    paths = cfg.write(os.path.join(tmp, f"adj2048_rank{rank}"))
+    T = args.adjoint_large_steps
+    sim = runner.Simulation(paths, runner.FP64, device=local)
+    first = sim.areas()          # the regulator's targets: 1.2 x these
+    sim.step(3)
+    areas = sim.areas()
+    nD = sim.domain_count()
+    factor, strength0, maxsource = cfg.area
+    coef = np.zeros(nD)
+    for d, a in areas.items():
+        tgt = factor * first[d]
+        coef[d] = (tgt - a) / tgt
+    strengths = np.full(nD, strength0)
+    strengths[0] = 0.0
+
+    def mass_of(s):
+        return np.clip(s * coef, -maxsource, maxsource)
+
+    free0, total = torch.cuda.mem_get_info(local)
+    sim.diff_begin(T, 0)
+    free1, _ = torch.cuda.mem_get_info(local)
+    n = cfg.nx
+    yy, xx = np.divmod(np.arange(n * n), n)
+    window = (abs(xx - n // 2) < 128) & (abs(yy - n // 2) < 128)
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1])[[0, 3, 4, 1, 2, 7, 8, 5, 6]]
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1])[[0, 3, 4, 1, 2, 7, 8, 5, 6]]
+    target = strengths * (1.0 + np.random.default_rng(6).normal(0.0, 0.1, nD))
+    sim.diff_mass(mass_of(target))
+    sim.diff_forward()
+    c_target = sim.concentrations().copy()
+
+    def loss(s):
+        sim.diff_mass(mass_of(s))
+        sim.diff_forward()
+        f = sim.lattice().f
+        rho = f.sum(1)
+        jx, jy = f @ ex, f @ ey
+        e = 0.5 * (jx * jx + jy * jy) / rho
+        C = sim.concentrations()
+        dke = ((np.outer(jx, ex) + np.outer(jy, ey)) / rho[:, None] - (e / rho)[:, None]) * window[:, None]
+        return float(e[window].sum() + ((C - c_target) ** 2).sum()), dke, 2.0 * (C - c_target)
+
+    torch.cuda.synchronize()
+    L0, dke, dC = loss(strengths)
+    fwd_ms = sim.last_timing()["total_ms"]
+    sim.diff_fluid_seed(dke)
+    g = sim.diff_backward(dC)
+    bwd_ms = sim.last_timing()["total_ms"]
+    free2, _ = torch.cuda.mem_get_info(local)
+    gS = sim.diff_mass() * coef
+    d = int(np.argmax(np.abs(gS[1:]))) + 1
+    h = 1e-6
+    sp, sm = strengths.copy(), strengths.copy()
+    sp[d] += h
+    sm[d] -= h
+    fd = (loss(sp)[0] - loss(sm)[0]) / (2 * h)
+    sim.diff_end()
+    sim.close()
+    return {"workload": f"{cfg.name}: {cfg.nx}x{cfg.ny}, {len(cfg.cells)} cells, fluid + {len(cfg.species)} species, "
+                        "frozen geometry, FP64 forward and adjoint",
+            "T": T, "K": int(math.ceil(math.sqrt(T))), "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "adjoint_over_forward": bwd_ms / fwd_ms,
+            "device_memory_gb": {"before_run": (total - free0) / 1e9, "run_allocated": (total - free1) / 1e9,
+                                 "after_backward": (total - free2) / 1e9, "total": total / 1e9},
+            "parameters": f"{nD - 1} per-cell area-regulator strengths", "loss": L0,
+            "grad_strength_max": float(np.abs(gS).max()),
+            "fd_check": {"domain": d, "adjoint": float(gS[d]), "central_difference": fd, "h": h,
+                         "rel_err": abs(gS[d] - fd) / max(abs(fd), 1e-300)},
+            "grad_finite": bool(np.isfinite(gS).all() and np.isfinite(g["tau"]).all())}
 
 
 def main():
@@ -367,6 +554,22 @@ def main():
                    "backward_note": "segment recompute from checkpoints + adjoint steps",
                    "grad_finite": bool(np.isfinite(g["force"]).all() and np.isfinite(g["tau"]).all())}
 
+    # ---- FP32-shifted error at fixed horizons (independent of --steps) -------
+    horizons = None
+    if not args.no_fp64:
+        horizons = fp32_error_at(configs.config2(iterations=1000).write(os.path.join(tmp, f"hz_rank{rank}")),
+                                 (500, 1000), local)
+
+    # ---- adjoint_2048: the large differentiated run -------------------------
+    adjoint_large = None
+    if not args.no_adjoint_large:
+        adjoint_large = adjoint_large_block(args, tmp, rank, world, local)
+
+    # ---- tissue_4096: the large configuration ------------------------------
+    large = None
+    if not args.no_large:
+        large = large_block(args, tmp, rank, world, local)
+
     if rank != 0:
         return
     cpu = None
@@ -378,8 +581,13 @@ def main():
                 res = port_cpu_time(paths, 2)
                 kind = "port"
             cpu = {"value": L * res["iterations"] / res["seconds"] / 1e6, "unit": "MLUPS",
-                   "cores": res.get("threads", 1), "kind": kind,
+                   "cores": res.get("threads", 1), "kind": kind, "cpu_model": cpu_model(),
                    "sample": f"{res['iterations']} steps of {cfg.name} after {res.get('warmup', 1)} warm-up steps"}
+            if kind == "reference":
+                one = ref_cpu_time(paths, 1, 3, 1)
+                cpu["single_thread"] = {"value": L * one["iterations"] / one["seconds"] / 1e6, "unit": "MLUPS",
+                                        "cores": 1, "sample": f"{one['iterations']} steps after 1 warm-up step, "
+                                                              "OMP_NUM_THREADS=1"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"[:300]}
@@ -388,19 +596,21 @@ def main():
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": [cfg.nx, cfg.ny], "species": S, "cells": len(cfg.cells),
-                   "membrane_nodes": M, "precision": "FP32-shifted distributions, FP64 membrane",
-                   "l2": "inputs larger than L2 (lattice state ~170 MB per copy set)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "host_events": host_events},
+        "config": workload_config(cfg),
+        "precision": "FP32-shifted distributions, FP64 membrane",
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "membrane_nodes": M, "host_events": host_events,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "stream_collide32",
                      "algorithmic_bytes_per_node": bytes_per_node, "avg_launch_ms": avg_ms,
                      "launches_timed": tp_["collide_launches"], "peak_source": peak_kind},
         "fp64": fp64,
         "fp32_over_fp64": (value / fp64["mlups"]) if fp64 else None,
+        "fp32_error_at_horizons": horizons,
+        "tissue_4096": large,
         "adjoint_over_forward": (adjoint["backward_ms"] / adjoint["forward_ms"]) if adjoint else None,
         "adjoint": adjoint,
+        "adjoint_2048": adjoint_large,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(tm["launches"]),

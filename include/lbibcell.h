@@ -92,6 +92,14 @@ int lbib_download_lattice(lbib_handle* h, double* f, double* g, double* vel, dou
  * (SimulationRunner.cpp:151-182) for restarts and stage-level tests. */
 int lbib_upload_lattice(lbib_handle* h, const double* f, const double* g, const double* force);
 
+/* SimulationRunner::initSolvers(Field<double>) (SimulationRunner.cpp:308-320):
+ * every node's fluid at the equilibrium of density 1 and the uniform
+ * velocity (ux, uy) (FluidSolver::setVelocity + initWithVelocity,
+ * FluidSolver.cpp:62-101, 233-240), its stored velocity set to (ux, uy),
+ * then each CDE solver's initSolver (which collides at that velocity).
+ * Replaces the lattice state; the membrane and force list are unchanged. */
+int lbib_init_velocity(lbib_handle* h, double ux, double uy);
+
 /* Membrane nodes in ascending id order (Geometry::getGeometryNodes):
  * ids[M], state[M][6] = x, y, vx, vy, fx, fy. */
 int lbib_download_membrane(lbib_handle* h, unsigned* ids, double* state);
@@ -100,7 +108,9 @@ int lbib_download_membrane(lbib_handle* h, unsigned* ids, double* state);
 int lbib_download_connections(lbib_handle* h, unsigned* conn);
 
 /* Cell areas (GeometryHandler::computeAreas, GeometryHandler.cpp:101-134):
- * dom[k], area[k] for k < return value (capped at cap). Negative on error. */
+ * dom[k], area[k] for k < return value (capped at cap). Negative on error:
+ * -LBIB_ERR_CAPACITY (the handle stays usable) when a cell's ring holds more
+ * than 4096 membrane nodes, the most one ring sum takes. */
 int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
 
 /* The same cell areas as lbib_areas, computed without any allocation: no
@@ -112,12 +122,14 @@ int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
  * (128 KB); a simulation with more cells is rejected with
  * -LBIB_ERR_CAPACITY, its message readable by lbib_last_error, and the
  * handle stays usable.  Every call on a device, from any handle, shares
- * that one array: each call writes every entry it reads, so nothing in it
- * needs to start at zero, but calls that overlap in time (two threads, or
- * two handles on different streams) race on it and must be serialised by
- * the caller.  The first call on a device looks up the array's address;
- * make that call before any stream capture.  Returns the number of cells,
- * as lbib_areas. */
+ * that one array: each call first sets the entries it will read to NaN, so
+ * no value of an earlier call can come back, but calls that overlap in time
+ * (two threads, or two handles on different streams) race on it and must be
+ * serialised by the caller.  A cell whose ring holds more than 4096 nodes
+ * gives -LBIB_ERR_CAPACITY with the cell's index in lbib_last_error (the
+ * handle stays usable; area[] may then hold NaN).  The first call on a
+ * device looks up the array's address; make that call before any stream
+ * capture.  Returns the number of cells, as lbib_areas. */
 int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
 
 /* GeometryHandler::computeAccumulatedDomainConcentrations(species)
@@ -208,6 +220,24 @@ int lbib_diff_forward(lbib_handle* h, const double* memForce, const double* tau,
  * Per-domain and relaxation-time gradients are sums of atomic adds: their
  * last bits can differ between calls. */
 int lbib_diff_backward(lbib_handle* h, const double* dLdC, double* gForce, double* gTau, double* gRates);
+
+/* The per-domain mass source as a parameter of a differentiated run: the
+ * rhoToAdd that FluidSolver::addMass sets (FluidSolver.cpp:141-145, 196-257)
+ * and the collide adds to the density, frozen for the run (the area
+ * regulator's rates of the last step, or none).  mass[n], when non-NULL,
+ * replaces that table for the following lbib_diff_forward calls (a run
+ * without an area regulator then gets one); gMass[n], when non-NULL,
+ * receives dL/d mass[d] of the last lbib_diff_backward (zeros when the run
+ * has no mass table).  n must be the domain count (lbib_get_domain_count).
+ * With frozen cell areas an area regulator's rate is linear in its strength
+ * below the clamp, so dL/d strength = dL/d mass times the rate's factor. */
+int lbib_diff_mass(lbib_handle* h, const double* mass, double* gMass, int n);
+
+/* dL/d of the final fluid distributions, dLdf[L][9] in lbib_download_lattice's
+ * layout, joined to the species' seed of the following lbib_diff_backward
+ * calls (for a loss of the flow, such as its kinetic energy); NULL removes
+ * it.  Must be called after lbib_diff_begin. */
+int lbib_diff_fluid_seed(lbib_handle* h, const double* dLdf);
 
 /* Restores the snapshot taken by lbib_diff_begin (distributions, velocity and
  * force planes) and frees the run's device memory. */

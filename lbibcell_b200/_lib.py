@@ -20,7 +20,7 @@ SYMBOLS = (
     "lbib_write_simulation", "lbib_load_solvers", "lbib_add_forces", "lbib_delete_force_type",
     "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes", "lbib_write_vtk",
     "lbib_read_vtm_geometry", "lbib_upload_membrane", "lbib_cure_lattice", "lbib_accumulated_concentrations",
-    "lbib_set_cell_types", "lbib_get_cell_types",
+    "lbib_set_cell_types", "lbib_get_cell_types", "lbib_init_velocity", "lbib_diff_mass", "lbib_diff_fluid_seed",
 )
 
 _lib = None
@@ -58,6 +58,8 @@ def load() -> ctypes.CDLL:
     L.lbib_download_lattice.argtypes = [vp] + [vp] * 6
     L.lbib_upload_lattice.restype = ip
     L.lbib_upload_lattice.argtypes = [vp, vp, vp, vp]
+    L.lbib_init_velocity.restype = ip
+    L.lbib_init_velocity.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     L.lbib_download_membrane.restype = ip
     L.lbib_download_membrane.argtypes = [vp, vp, vp]
     L.lbib_download_connections.restype = ip
@@ -90,6 +92,10 @@ def load() -> ctypes.CDLL:
     L.lbib_diff_backward.argtypes = [vp, vp, vp, vp, vp]
     L.lbib_diff_end.restype = ip
     L.lbib_diff_end.argtypes = [vp]
+    L.lbib_diff_mass.restype = ip
+    L.lbib_diff_mass.argtypes = [vp, vp, vp, ip]
+    L.lbib_diff_fluid_seed.restype = ip
+    L.lbib_diff_fluid_seed.argtypes = [vp, vp]
     L.lbib_write_simulation.restype = ip
     L.lbib_write_simulation.argtypes = [vp, cp, cp, cp, cp]
     L.lbib_load_solvers.restype = ip

@@ -20,6 +20,8 @@ Each configuration is four files:
       MassSolver  MassSolverBoxOutlet
       BioSolver   LbibAreaRegulator    factor F strength K maxsource M
       BioSolver   LbibMembraneTension  force F frequency N
+      BioSolver   LbibCellDivision     factor F frequency N
+      ForceModel  GuoZhengShi2002ForceModel  (or ...Corrected; default Luo1993ForceModel)
       CDE         <species name>       init C0 decay D
       CDESource   <species name>       <domainId> <rate> [<domainId> <rate> ...]
 
@@ -75,6 +77,9 @@ class Config:
     # registered before (bio_first) or after the area regulator and tension
     bio: List[str] = field(default_factory=list)
     bio_first: bool = False
+    # FluidSolver's force model: None (Luo1993ForceModel, the reference's),
+    # "GuoZhengShi2002ForceModel" or "GuoZhengShi2002ForceModelCorrected"
+    force_model: Optional[str] = None
 
     @property
     def lattice_nodes(self) -> int:
@@ -122,6 +127,8 @@ class Config:
                 f.write(line.rstrip("\n") + "\n")
         with open(paths["plugins"], "w") as f:
             f.write("#lbibcell_b200 plugin file\n")
+            if self.force_model:
+                f.write(f"ForceModel\t{self.force_model}\n")
             if self.outlet:
                 f.write("MassSolver\tMassSolverBoxOutlet\n")
             if self.bio_first:
@@ -277,14 +284,22 @@ def poisson_tissue(nx: int, ny: int, rmin: float, rmax: float, spacing: float, s
     return cells
 
 
-def config3(iterations: int = 5000, report_step: int = 1000, seed: int = 0) -> Config:
-    """4096x4096 tissue: Poisson-disk cells r~U(10,16), node spacing 0.5, 3 species
-    (tau 0.55/1.0/1.5) with linear decay 1e-4."""
-    cells = poisson_tissue(4096, 4096, 10.0, 16.0, 0.5, seed)
-    species = [Species(SPECIES_NAMES[k], t, decay=1e-4, source={d: 1e-3 for d, _ in cells[::10]})
+def config3(iterations: int = 5000, report_step: int = 1000, seed: int = 0, cells: int = 6000) -> Config:
+    """4096x4096 tissue: ``cells`` cells placed by seeded Poisson-disk sampling
+    (dart throwing, gap 3 lu) with radii U(10,16) and membrane node spacing
+    0.5 lu (~1.1M nodes for 6000 cells); membrane tension, cell junctions
+    (radius 1 lu, k 0.02, rest length 2 lu), area growth toward 2.5x the
+    initial area (LbibAreaRegulator: strength 0.01, at most 2e-4 per node and
+    step) with division at 2x the initial area (LbibCellDivision, checked every
+    100 iterations); 3 D2Q5 species (tau 0.55, 1.0, 1.5) with linear decay
+    1e-4, secreted at 1e-3 per step by every tenth cell."""
+    placed = poisson_tissue(4096, 4096, 10.0, 16.0, 0.5, seed, max_cells=cells)
+    species = [Species(SPECIES_NAMES[k], t, decay=1e-4, source={d: 1e-3 for d, _ in placed[::10]})
                for k, t in enumerate((0.55, 1.0, 1.5))]
     return Config(name="tissue_4096", nx=4096, ny=4096, tau_fluid=1.0, iterations=iterations,
-                  report_step=report_step, cells=cells, species=species)
+                  report_step=report_step, cells=placed, species=species, area=(2.5, 0.01, 2e-4),
+                  bio=["LbibCellJunction\tradius\t1.0\tk\t0.02\tl0\t2.0",
+                       "LbibCellDivision\tfactor\t2.0\tfrequency\t100"])
 
 
 def config4(iterations: int = 2000, report_step: int = 1000, seed: int = 0) -> Config:
@@ -302,14 +317,16 @@ def config4(iterations: int = 2000, report_step: int = 1000, seed: int = 0) -> C
 
 def config5(iterations: int = 10000, report_step: int = 1000, seed: int = 0) -> Config:
     """Adjoint workload, 2048x2048: 1000 Poisson-disk cells r~U(10,16), two
-    species (tau 0.8, 1.2) with seeded per-cell rates.  Differentiated over
+    species (tau 0.8, 1.2) with seeded per-cell rates, and the area regulator
+    (target 1.2x the first area, strength 0.01 per cell) whose per-cell
+    strengths are the differentiated parameters.  Differentiated over
     T=10000 steps with sqrt(T) checkpoints."""
     cells = poisson_tissue(2048, 2048, 10.0, 16.0, 0.5, seed, max_cells=1000)
     rng = np.random.default_rng(seed + 5)
     species = [Species(SPECIES_NAMES[k], t, source={d: float(1e-3 * rng.uniform(0.5, 1.5)) for d, _ in cells})
                for k, t in enumerate((0.8, 1.2))]
     return Config(name="adjoint_2048", nx=2048, ny=2048, tau_fluid=1.0, iterations=iterations,
-                  report_step=report_step, cells=cells, species=species, area=None)
+                  report_step=report_step, cells=cells, species=species, area=(1.2, 0.01, 0.004), tension=None)
 
 
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "config4": config4, "config5": config5,

@@ -25,9 +25,14 @@
 //                               block b (each block owns its slots; the same
 //                               blocks cover the same nodes every step),
 //   racc[k][x]                  dL/d source_k at node x (RX_LINEAR species),
+//   macc[x]                     dL/d rhoToAdd at node x (FluidSolver::addMass's
+//                               per-domain mass source, when the run has one),
 //   G[x]                        dL/dF(x) of the force field,
-// all summed over the steps; launch_adjoint_finish reduces part and racc into
-// grad[0..S] and grad[1 + S + k*nDomains + domain].
+// all summed over the steps; launch_adjoint_finish reduces part, racc and macc
+// into grad[0..S], grad[1 + S + k*nDomains + domain] and
+// grad[1 + S + S*nDomains + domain].  A seed for the fluid (seedF, the
+// gradient of the loss with respect to the final stored distributions) joins
+// the species' seed at the final step.
 #include "kernels.cuh"
 
 namespace lbib {
@@ -68,9 +73,15 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 }  // namespace
 
 // NS = number of species (compile-time, so that every input of a node is
-// loaded before any arithmetic).  Grid (ceil(nx / 256), ny).
+// loaded before any arithmetic).  Grid (ceil(nx / 256), ny).  The kernel
+// holds a node's whole forward and reverse state; LBIB_ADJOINT_MIN_BLOCKS
+// (blocks per SM the register budget is sized for) trades occupancy against
+// register spills.
+#ifndef LBIB_ADJOINT_MIN_BLOCKS
+#define LBIB_ADJOINT_MIN_BLOCKS 2
+#endif
 template <int NS>
-__global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
+__global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
     pdl_wait();
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
@@ -91,7 +102,8 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) f[q] = fprev[(size_t)q * L + pull[q]];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) lf[q] = a.seed ? 0.0 : (double)a.pf[(size_t)q * L + push[q]];
+    for (int q = 0; q < 9; ++q)
+        lf[q] = a.seed ? (a.seedF ? a.seedF[(size_t)q * L + n] : 0.0) : (double)a.pf[(size_t)q * L + push[q]];
     double gA[NS > 0 ? NS : 1][5], muA[NS > 0 ? NS : 1][5];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -119,7 +131,9 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
     double gTauK[NS > 0 ? NS : 1];
     double rta = 0.0;
     if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
+    const bool hasMass = a.macc != nullptr && a.massTab != nullptr && dom < (uint32_t)a.nDomains && isfinite(rta);
     if (!isfinite(rta)) rta = 0.0;
+    const double maccA = hasMass ? a.macc[n] : 0.0;
 
     // ---- forward recomputation of the fluid collision --------------------
     const double tauI = a.tauIF;
@@ -280,6 +294,8 @@ __global__ void __launch_bounds__(256, 2) adjoint_step64(AdjointArgs a) {
     const double mjx = mux * rhoI, mjy = muy * rhoI;
     mrho -= (ux * mux + uy * muy) * rhoI;
     mrhoF += mrho;
+    // rho = sum f + rhoToAdd: dL/d rhoToAdd = dL/d rho
+    if (valid && hasMass) a.macc[n] = maccA + mrho;
     if (valid) {
 #pragma unroll
         for (int q = 0; q < 9; ++q)
@@ -354,11 +370,25 @@ void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
     }
 }
 
+// Sums the per-node mass-source partials into grad[base + dom].
+__global__ void adjoint_mass_reduce(const double* macc, const uint32_t* dom, size_t L, int nDomains, int base,
+                                    double* grad) {
+    pdl_wait();
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = n < L;
+    const uint32_t d = valid ? dom[n] : 0u;
+    const int key = (valid && d < (uint32_t)nDomains) ? base + (int)d : -1;
+    warp_keyed_add(grad, key, valid ? macc[n] : 0.0);
+}
+
 void launch_adjoint_finish(const AdjointArgs& a, cudaStream_t s) {
     launch_pdl(adjoint_part_reduce, 1, 256, 0, s, a.part, adjoint_blocks(a.nx, a.ny), 1 + a.S, a.grad);
     if (a.S > 0 && a.srcTab != nullptr)
         launch_pdl(adjoint_rate_reduce, (unsigned)((a.L + 255) / 256), 256, 0, s, a.racc, a.dom, a.L, a.S, a.nDomains,
                                                                           a.grad);
+    if (a.macc != nullptr && a.massTab != nullptr)
+        launch_pdl(adjoint_mass_reduce, (unsigned)((a.L + 255) / 256), 256, 0, s, a.macc, a.dom, a.L, a.nDomains,
+                   1 + a.S + a.S * a.nDomains, a.grad);
 }
 
 void launch_set_iteration(Status* st, unsigned it, cudaStream_t s) { launch_pdl(set_iteration_kernel, 1, 1, 0, s, st, it); }

@@ -60,12 +60,24 @@ __device__ __forceinline__ void reaction_terms32(const SpeciesConst& sp, float s
 // MODE bit 0 (COUPLED): a species' reaction reads a partner species (its
 // pre-collide sum until it has collided at this node, its post-collide sum
 // after) or the node's cell type.  MODE bit 1 (MASSNODE): the mass source is
-// per node (massNode) instead of per domain.  Each combination is its own
-// instantiation, so that the plain case carries no code for the others.
+// per node (massNode) instead of per domain.  MODE bit 2 (GUO): the Guo
+// force model (below).  MODE bit 3 (BOUNCE): DiracD2Q5 species keep the
+// populations of links with a boundary node (as in stream_collide64).  Each combination is its own instantiation, so that
+// the plain case carries no code for the others.
+//
+// Guo force model (GuoZhengShi2002ForceModel.cpp:29-78) in shifted form:
+//   u     = (sum c_q h_q + F/2) / rho
+//   h_q' = h_q + (heq_q - h_q)/tau + G_q [3 (c_q - v) . F + 9 (c_q . v)(c_q . F)]
+//   G_q   = (1 - 1/2tau) w_q,  v = the node's stored velocity (last collide)
+//   u'    = (sum c_q h_q' + F/2) / rho
+// with the reference's NE coefficient (-3 v_y in place of +6 v_y in the F_y
+// factor) for FM_GUO: G_NE * 9 v_y F_y less on NE.
 template <int NS, int MODE>
 __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     constexpr bool COUPLED = (MODE & 1) != 0;   // coupled species reactions
     constexpr bool MASSNODE = (MODE & 2) != 0;  // per-node mass source
+    constexpr bool GUO = (MODE & 4) != 0;       // Guo force model
+    constexpr bool BOUNCE = (MODE & 8) != 0;    // a DiracD2Q5 species (bounce-back at boundary links)
     pdl_wait();
     if (a.status->halt) return;
     const int nx = a.nx, ny = a.ny;
@@ -88,14 +100,28 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const float hSW = fin[7 * L + rP + xp];
     const float hSE = fin[8 * L + rP + xm];
     float gi[NS > 0 ? NS : 1][5];
+    uint8_t bW = 0, bWe = 0, bS = 0, bSn = 0;
+    if (BOUNCE) {
+        bW = a.bounceW[n];
+        bWe = a.bounceW[rC + xp];
+        bS = a.bounceS[n];
+        bSn = a.bounceS[rP + x];
+    }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const float* __restrict__ gin = a.gin + (size_t)k * 5 * L;
         gi[k][0] = gin[0 * L + rC + x];
-        gi[k][1] = gin[1 * L + rC + xm];
-        gi[k][2] = gin[2 * L + rM + x];
-        gi[k][3] = gin[3 * L + rC + xp];
-        gi[k][4] = gin[4 * L + rP + x];
+        if (BOUNCE && a.sp[k].bounce) {
+            gi[k][1] = bW ? gin[3 * L + n] : gin[1 * L + rC + xm];
+            gi[k][2] = bS ? gin[4 * L + n] : gin[2 * L + rM + x];
+            gi[k][3] = bWe ? gin[1 * L + n] : gin[3 * L + rC + xp];
+            gi[k][4] = bSn ? gin[2 * L + n] : gin[4 * L + rP + x];
+        } else {
+            gi[k][1] = gin[1 * L + rC + xm];
+            gi[k][2] = gin[2 * L + rM + x];
+            gi[k][3] = gin[3 * L + rC + xp];
+            gi[k][4] = gin[4 * L + rP + x];
+        }
     }
     const uint32_t dom = a.dom[n];
     float rta = 0.0f;
@@ -110,33 +136,69 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const float dr = drho + rta;          // rho - 1
     const float rhoF = 1.0f + drho;
     const float rho = rhoF + rta;
-    const float jx = (hE - hW) + (hNE - hNW) + (hSE - hSW);
-    const float jy = (hN - hS) + (hNE - hSE) + (hNW - hSW);
+    float jx = (hE - hW) + (hNE - hNW) + (hSE - hSW);
+    float jy = (hN - hS) + (hNE - hSE) + (hNW - hSW);
+    if (GUO) {
+        jx += 0.5f * Fx;
+        jy += 0.5f * Fy;
+    }
     const float rinv = 1.0f / rho;
     const float ux = jx * rinv, uy = jy * rinv;
     const float tauI = (float)(1.0 / a.tauF);
     const float usq = 1.5f * (ux * ux + uy * uy);
     const float w0 = 4.0f / 9.0f, w1 = 1.0f / 9.0f, w2 = 1.0f / 36.0f;
-    const float f3 = 3.0f * rhoF;
     float ho[9];
-    ho[0] = hT + (w0 * dr + w0 * rho * (-usq) - hT) * tauI;
+    if (!GUO) {
+        const float f3 = 3.0f * rhoF;
+        ho[0] = hT + (w0 * dr + w0 * rho * (-usq) - hT) * tauI;
 #define LBIB_Q(idx, h, w, cu, cf)                                                 \
     {                                                                             \
         const float c_u = (cu);                                                   \
         const float heq = (w) * dr + (w) * rho * (3.0f * c_u + 4.5f * c_u * c_u - usq); \
         ho[idx] = (h) + (heq - (h)) * tauI + (w) * f3 * (cf);                     \
     }
-    LBIB_Q(1, hE, w1, ux, Fx)
-    LBIB_Q(2, hN, w1, uy, Fy)
-    LBIB_Q(3, hW, w1, -ux, -Fx)
-    LBIB_Q(4, hS, w1, -uy, -Fy)
-    LBIB_Q(5, hNE, w2, ux + uy, Fx + Fy)
-    LBIB_Q(6, hNW, w2, -ux + uy, -Fx + Fy)
-    LBIB_Q(7, hSW, w2, -ux - uy, -Fx - Fy)
-    LBIB_Q(8, hSE, w2, ux - uy, Fx - Fy)
+        LBIB_Q(1, hE, w1, ux, Fx)
+        LBIB_Q(2, hN, w1, uy, Fy)
+        LBIB_Q(3, hW, w1, -ux, -Fx)
+        LBIB_Q(4, hS, w1, -uy, -Fy)
+        LBIB_Q(5, hNE, w2, ux + uy, Fx + Fy)
+        LBIB_Q(6, hNW, w2, -ux + uy, -Fx + Fy)
+        LBIB_Q(7, hSW, w2, -ux - uy, -Fx - Fy)
+        LBIB_Q(8, hSE, w2, ux - uy, Fx - Fy)
 #undef LBIB_Q
-    const float s = rhoF * rinv;
-    const float uxo = ux + s * Fx, uyo = uy + s * Fy;
+    } else {
+        const float vx = a.u[n], vy = a.u[L + n];  // the stored velocity, before it is overwritten
+        const float gf = (float)(1.0 - 0.5 / a.tauF);
+        const float vF = vx * Fx + vy * Fy;
+        ho[0] = hT + (w0 * dr + w0 * rho * (-usq) - hT) * tauI + w0 * gf * (-3.0f * vF);
+#define LBIB_G(idx, h, w, cu, cv, cF)                                             \
+    {                                                                             \
+        const float c_u = (cu);                                                   \
+        const float heq = (w) * dr + (w) * rho * (3.0f * c_u + 4.5f * c_u * c_u - usq); \
+        ho[idx] = (h) + (heq - (h)) * tauI + (w) * gf * (3.0f * ((cF) - vF) + 9.0f * (cv) * (cF)); \
+    }
+        LBIB_G(1, hE, w1, ux, vx, Fx)
+        LBIB_G(2, hN, w1, uy, vy, Fy)
+        LBIB_G(3, hW, w1, -ux, -vx, -Fx)
+        LBIB_G(4, hS, w1, -uy, -vy, -Fy)
+        LBIB_G(5, hNE, w2, ux + uy, vx + vy, Fx + Fy)
+        LBIB_G(6, hNW, w2, -ux + uy, -vx + vy, -Fx + Fy)
+        LBIB_G(7, hSW, w2, -ux - uy, -vx - vy, -Fx - Fy)
+        LBIB_G(8, hSE, w2, ux - uy, vx - vy, Fx - Fy)
+#undef LBIB_G
+        if (a.forceModel == FM_GUO) ho[5] -= w2 * gf * 9.0f * vy * Fy;
+    }
+    float uxo, uyo;
+    if (!GUO) {
+        const float s = rhoF * rinv;
+        uxo = ux + s * Fx;
+        uyo = uy + s * Fy;
+    } else {
+        const float jxo = (ho[1] - ho[3]) + (ho[5] - ho[6]) + (ho[8] - ho[7]);
+        const float jyo = (ho[2] - ho[4]) + (ho[5] - ho[8]) + (ho[6] - ho[7]);
+        uxo = (jxo + 0.5f * Fx) * rinv;
+        uyo = (jyo + 0.5f * Fy) * rinv;
+    }
     a.u[n] = uxo;
     a.u[L + n] = uyo;
     // MassSolverBoxOutlet on the x=0 column and the y=0 row (the corner twice),
@@ -232,28 +294,42 @@ __global__ void outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, c
 }
 
 // Initial state: the FP64 initial collision (f_T = 1, zero force and mass)
-// converted to deviations, and the species' initial conditions.
+// converted to deviations, and the species' initial conditions.  withVel:
+// FluidSolver::initWithVelocity at the uniform velocity (vx, vy) instead
+// (equilibrium at rho = 1, FluidSolver.cpp:62-101), and the species'
+// initSolver collides at that velocity.
 __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
                        SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1,
-                       double init2) {
+                       double init2, int withVel, double vx, double vy) {
     pdl_wait();
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L) return;
     const double wq[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
                           1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
     const double tauI = 1.0 / tauF;
-    // f_q' = f_q - f_q/tau + w_q/tau with f = (1, 0, ..., 0), so h_q = (f_q - w_q)(1 - 1/tau).
-    for (int q = 0; q < 9; ++q) {
-        const double f0 = q == 0 ? 1.0 : 0.0;
-        f[(size_t)q * L + n] = (float)((f0 - wq[q]) * (1.0 - tauI));
+    if (withVel) {
+        double fi[9];
+        equilibrium_at_velocity64(vx, vy, fi);
+        for (int q = 0; q < 9; ++q) f[(size_t)q * L + n] = (float)(fi[q] - wq[q]);
+        u[n] = (float)vx;
+        u[L + n] = (float)vy;
+    } else {
+        // f_q' = f_q - f_q/tau + w_q/tau with f = (1, 0, ..., 0), so h_q = (f_q - w_q)(1 - 1/tau).
+        for (int q = 0; q < 9; ++q) {
+            const double f0 = q == 0 ? 1.0 : 0.0;
+            f[(size_t)q * L + n] = (float)((f0 - wq[q]) * (1.0 - tauI));
+        }
+        u[n] = 0.0f;
+        u[L + n] = 0.0f;
     }
-    u[n] = 0.0f;
-    u[L + n] = 0.0f;
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
     const double init[3] = {init0, init1, init2};
     for (int k = 0; k < nS; ++k) {
         double gi[5];
-        if (sp[k].kind == RX_NONE) {
+        if (sp[k].kind == RX_NONE && withVel) {
+            gi[0] = 1.0; gi[1] = gi[2] = gi[3] = gi[4] = 0.0;
+            collide_cde64(gi, vx, vy, sp[k], 0.0, 0.0, dom[n], 0u, 0u);
+        } else if (sp[k].kind == RX_NONE) {
             const double tI = 1.0 / sp[k].tau;
             gi[0] = 1.0 - tI + (1.0 / 3.0) * tI;
             for (int q = 1; q < 5; ++q) gi[q] = (1.0 / 6.0) * tI;
@@ -269,7 +345,8 @@ __global__ void init32(float* f, float* g, float* u, int nS, size_t L, double ta
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     if (a.nfTab != nullptr) launch_noflux<float>(a, s);
-    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0);
+    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0) | (a.forceModel != FM_LUO ? 4 : 0) |
+                     (a.bounceW != nullptr ? 8 : 0);
     switch (mode * 4 + (a.S < 3 ? a.S : 3)) {
 #define LBIB_SC_CASE(M, N) \
     case M * 4 + N: launch_pdl(stream_collide32<N, M>, grid, 256, 0, s, a); break;
@@ -277,6 +354,11 @@ void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s) {
         LBIB_SC_CASE(2, 0) LBIB_SC_CASE(2, 1) LBIB_SC_CASE(2, 2) LBIB_SC_CASE(2, 3)
         // coupled reactions need a partner species: two or three species
         LBIB_SC_CASE(1, 2) LBIB_SC_CASE(1, 3) LBIB_SC_CASE(3, 2) LBIB_SC_CASE(3, 3)
+        // the same with the Guo force model
+        LBIB_SC_CASE(4, 0) LBIB_SC_CASE(4, 1) LBIB_SC_CASE(4, 2) LBIB_SC_CASE(4, 3)
+        LBIB_SC_CASE(6, 0) LBIB_SC_CASE(6, 1) LBIB_SC_CASE(6, 2) LBIB_SC_CASE(6, 3)
+        LBIB_SC_CASE(5, 2) LBIB_SC_CASE(5, 3) LBIB_SC_CASE(7, 2) LBIB_SC_CASE(7, 3)
+        LBIB_SC_CASE(8, 1) LBIB_SC_CASE(8, 2) LBIB_SC_CASE(8, 3)
 #undef LBIB_SC_CASE
         default: break;
     }
@@ -287,10 +369,10 @@ void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const
     launch_pdl(outlet32, (n + 255) / 256, 256, 0, s, f, g, nS, nx, ny, L, st);
 }
 
-void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
+void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom, const double* vel,
                    const SpeciesConst* sp, const double* init, cudaStream_t s) {
     launch_pdl(init32, (unsigned)((L + 255) / 256), 256, 0, s, f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
-                                                       init[1], init[2]);
+               init[1], init[2], vel != nullptr ? 1 : 0, vel != nullptr ? vel[0] : 0.0, vel != nullptr ? vel[1] : 0.0);
 }
 
 }  // namespace lbib

@@ -20,10 +20,18 @@ namespace lbib {
 // reaction reads a partner species or the cell type (the partner's getC() is
 // its pre-collide sum while it has not collided at this node, its
 // post-collide sum after).  MODE bit 1 (MASSNODE): per-node mass source.
+// MODE bit 2 (GUO): GuoZhengShi2002ForceModel in place of Luo1993ForceModel
+// (it reads the node's stored velocity before overwriting it).  MODE bit 3
+// (BOUNCE): species whose advect keeps the populations of links with a
+// boundary node (DiracD2Q5::advect, DiracD2Q5.cpp:166-180): the swap with the
+// W (S) neighbour is skipped when the node has a W (S) boundary node, so the
+// node's own opposite population stays.
 template <int NS, int MODE>
 __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
     constexpr bool COUPLED = (MODE & 1) != 0;   // coupled species reactions
     constexpr bool MASSNODE = (MODE & 2) != 0;  // per-node mass source
+    constexpr bool GUO = (MODE & 4) != 0;       // Guo force model
+    constexpr bool BOUNCE = (MODE & 8) != 0;    // a DiracD2Q5 species (bounce-back at boundary links)
     pdl_wait();
     if (a.status->halt) return;
     // grid (nx/256, ny): one lattice node per thread
@@ -58,7 +66,8 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
         fy = a.force[L + n];
     }
     double ux, uy;
-    collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
+    if (GUO) collide_fluid64_guo(f, rta, fx, fy, a.tauF, a.u[n], a.u[L + n], guo_ne_y(a.forceModel), ux, uy);
+    else collide_fluid64(f, rta, fx, fy, a.tauF, ux, uy);
     a.u[n] = ux;
     a.u[L + n] = uy;
     // MassSolverBoxOutlet (MassSolverBoxOutlet.cpp:42-72) on the x=0 column and
@@ -80,14 +89,28 @@ __global__ void __launch_bounds__(256) stream_collide64(LatticeArgs<double> a) {
     for (int q = 0; q < 9; ++q) a.fout[q * L + n] = f[q];
 
     double gAll[NS > 0 ? NS : 1][5];
+    uint8_t bW = 0, bWe = 0, bS = 0, bSn = 0;  // W / S boundary nodes here, at the E and N neighbours
+    if (BOUNCE) {
+        bW = a.bounceW[n];
+        bWe = a.bounceW[rC + xp];
+        bS = a.bounceS[n];
+        bSn = a.bounceS[rP + x];
+    }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const double* gin = a.gin + (size_t)k * 5 * L;
         gAll[k][T] = gin[0 * L + rC + x];
-        gAll[k][E] = gin[1 * L + rC + xm];
-        gAll[k][N] = gin[2 * L + rM + x];
-        gAll[k][W] = gin[3 * L + rC + xp];
-        gAll[k][S] = gin[4 * L + rP + x];
+        if (BOUNCE && a.sp[k].bounce) {
+            gAll[k][E] = bW ? gin[3 * L + n] : gin[1 * L + rC + xm];
+            gAll[k][N] = bS ? gin[4 * L + n] : gin[2 * L + rM + x];
+            gAll[k][W] = bWe ? gin[1 * L + n] : gin[3 * L + rC + xp];
+            gAll[k][S] = bSn ? gin[2 * L + n] : gin[4 * L + rP + x];
+        } else {
+            gAll[k][E] = gin[1 * L + rC + xm];
+            gAll[k][N] = gin[2 * L + rM + x];
+            gAll[k][W] = gin[3 * L + rC + xp];
+            gAll[k][S] = gin[4 * L + rP + x];
+        }
     }
     // the species' getC() as a coupled reaction reads it, and the node's cell
     // type (copied from the per-domain table after every step's move)
@@ -152,15 +175,26 @@ __global__ void outlet64(double* f, double* g, int nS, int nx, int ny, size_t L,
 }
 
 // FluidSolver::initSolver (f_T = 1, then collide with zero force and mass)
-// and the species' initial conditions.
+// and the species' initial conditions.  withVel: FluidSolver::initWithVelocity
+// at the uniform velocity (vx, vy) (SimulationRunner::initSolvers(Field<double>),
+// SimulationRunner.cpp:308-320): the distributions are the equilibrium at
+// rho = 1, the stored velocity is (vx, vy), and the species' initSolver
+// collides at that velocity.
 __global__ void init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
-                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1, double init2) {
+                       SpeciesConst sp0, SpeciesConst sp1, SpeciesConst sp2, double init0, double init1, double init2,
+                       int withVel, double vx, double vy) {
     pdl_wait();
     const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L) return;
     double fi[9] = {1.0, 0, 0, 0, 0, 0, 0, 0, 0};
     double ux, uy;
-    collide_fluid64(fi, 0.0, 0.0, 0.0, tauF, ux, uy);
+    if (withVel) {
+        equilibrium_at_velocity64(vx, vy, fi);
+        ux = vx;
+        uy = vy;
+    } else {
+        collide_fluid64(fi, 0.0, 0.0, 0.0, tauF, ux, uy);
+    }
 #pragma unroll
     for (int q = 0; q < 9; ++q) f[(size_t)q * L + n] = fi[q];
     u[n] = ux;
@@ -292,7 +326,8 @@ template void launch_noflux<float>(const LatticeArgs<float>&, cudaStream_t);
 void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
     if (a.nfTab != nullptr) launch_noflux<double>(a, s);
-    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0);
+    const int mode = (a.coupled ? 1 : 0) | (a.massNode != nullptr ? 2 : 0) | (a.forceModel != FM_LUO ? 4 : 0) |
+                     (a.bounceW != nullptr ? 8 : 0);
     switch (mode * 4 + (a.S < 3 ? a.S : 3)) {
 #define LBIB_SC_CASE(M, N) \
     case M * 4 + N: launch_pdl(stream_collide64<N, M>, grid, 256, 0, s, a); break;
@@ -300,6 +335,12 @@ void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s) {
         LBIB_SC_CASE(2, 0) LBIB_SC_CASE(2, 1) LBIB_SC_CASE(2, 2) LBIB_SC_CASE(2, 3)
         // coupled reactions need a partner species: two or three species
         LBIB_SC_CASE(1, 2) LBIB_SC_CASE(1, 3) LBIB_SC_CASE(3, 2) LBIB_SC_CASE(3, 3)
+        // the same with the Guo force model
+        LBIB_SC_CASE(4, 0) LBIB_SC_CASE(4, 1) LBIB_SC_CASE(4, 2) LBIB_SC_CASE(4, 3)
+        LBIB_SC_CASE(6, 0) LBIB_SC_CASE(6, 1) LBIB_SC_CASE(6, 2) LBIB_SC_CASE(6, 3)
+        LBIB_SC_CASE(5, 2) LBIB_SC_CASE(5, 3) LBIB_SC_CASE(7, 2) LBIB_SC_CASE(7, 3)
+        // DiracD2Q5 species with the plain fluid (the combination create accepts)
+        LBIB_SC_CASE(8, 1) LBIB_SC_CASE(8, 2) LBIB_SC_CASE(8, 3)
 #undef LBIB_SC_CASE
         default: break;
     }
@@ -311,9 +352,9 @@ void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, con
 }
 
 void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
-                   const SpeciesConst* sp, const double* init, cudaStream_t s) {
+                   const double* vel, const SpeciesConst* sp, const double* init, cudaStream_t s) {
     launch_pdl(init64, (unsigned)((L + 255) / 256), 256, 0, s, f, g, u, nS, L, tauF, dom, sp[0], sp[1], sp[2], init[0],
-                                                       init[1], init[2]);
+               init[1], init[2], vel != nullptr ? 1 : 0, vel != nullptr ? vel[0] : 0.0, vel != nullptr ? vel[1] : 0.0);
 }
 
 }  // namespace lbib

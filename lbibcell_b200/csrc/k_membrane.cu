@@ -222,7 +222,7 @@ __device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid) {
 // tiles its stencil covers.
 __device__ void tile_slot_node(const MembraneDev& m, TileDev& t, int i, bool ok, int nx, int ny, Status* st) {
     Stencil sc{0, 0, 0, 0};
-    if (ok && !stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
+    if (ok && !stencil_range(m.bx[i], m.by[i], nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_SPREAD);
         ok = false;
     }
@@ -252,7 +252,7 @@ __global__ void tile_count_kernel(MembraneDev m, TileDev t, int nx, int ny, Stat
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool ok = i < m.topo->M;
     Stencil sc{0, 0, 0, 0};
-    if (ok && !stencil_range(m.x[i], m.y[i], nx, ny, sc)) {
+    if (ok && !stencil_range(m.bx[i], m.by[i], nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_SPREAD);
         ok = false;
     }
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(256) spread_kernel(MembraneDev m, TileDev t, R
         sfx[k] = m.fx[i];
         sfy[k] = m.fy[i];
         Stencil sc;
-        stencil_range(X, Y, nx, ny, sc);
+        stencil_range(m.bx[i], m.by[i], nx, ny, sc);
         code[k] = pack_stencil(sc, tileX0, tileY0);
         double* f = fac + 10 * k;
 #pragma unroll
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
             const int i = list[c0 + e];
             const double X = m.x[i], Y = m.y[i];
             Stencil sc;
-            stencil_range(X, Y, nx, ny, sc);
+            stencil_range(m.bx[i], m.by[i], nx, ny, sc);
             org[e] = pack_stencil(sc, tileX0, tileY0);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
@@ -545,7 +545,7 @@ __global__ void interp_move_kernel(MembraneDev m, const Real* u, int nx, int ny,
     if (i >= m.topo->M) return;
     const double X = m.x[i], Y = m.y[i];
     Stencil sc;
-    if (!stencil_range(X, Y, nx, ny, sc)) {
+    if (!stencil_range(m.bx[i], m.by[i], nx, ny, sc)) {
         raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
         return;
     }
@@ -613,7 +613,7 @@ __global__ void force_adjoint_kernel(MembraneDev m, const double* G, int nx, int
     const double X = m.x[i], Y = m.y[i];
     Stencil sc;
     double gx = 0.0, gy = 0.0;
-    if (stencil_range(X, Y, nx, ny, sc)) {
+    if (stencil_range(m.bx[i], m.by[i], nx, ny, sc)) {
         for (int k = 0; k < 16; ++k) {
             int xk, yk;
             stencil_slot(sc, k, xk, yk);
@@ -833,13 +833,17 @@ __device__ __forceinline__ void record_noflux(const MembraneDev& m, CrossDev& c,
     if (k < c.nfCap) c.nfKeys[k] = key;
 }
 
-// GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test for a node
-// that left its previous unit cell (GeometryHandler.cpp:610-636,
-// GeometryNode.cpp:256-261, Rectangle.cpp pointWithinBounds).
+// GeometryHandler::connectGeometryNodesToPhysicalNodes for one node
+// (GeometryHandler.cpp:608-644): a node that left its previous unit cell
+// (GeometryNode::isUpdateNeeded, GeometryNode.cpp:256-261, Rectangle.cpp
+// pointWithinBounds) is bound again from its current position, after the
+// edge test; the others keep their binding.
 __device__ __forceinline__ void edge_check_node(const MembraneDev& m, int i, int nx, int ny, Status* st, int stage) {
     const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
     const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
     if (within) return;
+    m.bx[i] = X;
+    m.by[i] = Y;
     if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, stage);
     else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, stage);
     else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, stage);
@@ -858,6 +862,14 @@ __global__ void cross_win_kernel(CrossDev c, MembraneDev m, const uint32_t* dom,
         const int s = (int)(key & 3u);
         c.bnDom[key] = bdom;
         if (c.nfTab != nullptr) record_noflux(m, c, (int)c.recConn[r], key, nx);
+        if (c.bounceW != nullptr && s >= 2) {
+            // DiracD2Q5's advect skips the swap with the W / S neighbour when
+            // this node has a boundary node there (DiracD2Q5.cpp:166-180)
+            (s == 2 ? c.bounceW : c.bounceS)[node] = 1;
+            const int k = atomicAdd(c.bounceN, 1);
+            if (k < c.bounceCap) c.bounceKeys[k] = key;
+            else raise_error(st, ERR_CAPACITY, (int)node, ST_CROSSINGS);
+        }
         if (s == 2) c.wDom[node] = bdom + 1;
         bool last = true;
         for (int s2 = s + 1; s2 < 4; ++s2)
@@ -889,6 +901,19 @@ __global__ void noflux_reset_kernel(CrossDev c) {
     if (threadIdx.x == 0) *c.nfN = 0;
 }
 
+// Clears the previous step's W / S boundary-node marks (after the
+// stream-collide that used them, before this step's crossings set new ones).
+__global__ void bounce_reset_kernel(CrossDev c) {
+    pdl_wait();
+    const int n = min(*c.bounceN, c.bounceCap);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const uint32_t key = c.bounceKeys[k];
+        ((key & 3u) == 2u ? c.bounceW : c.bounceS)[key >> 2] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *c.bounceN = 0;
+}
+
 // GeometryHandler::connectGeometryNodesToPhysicalNodes' edge test for nodes
 // that left their previous unit cell (GeometryHandler.cpp:610-636,
 // GeometryNode.cpp:256-261, Rectangle.cpp pointWithinBounds).
@@ -906,6 +931,7 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     if (m.Ccap == 0) return;
     const int blocks = (m.Ccap + 127) / 128;
     if (c.nfTab != nullptr) launch_pdl(noflux_reset_kernel, 1, 1024, 0, s, c);
+    if (c.bounceW != nullptr) launch_pdl(bounce_reset_kernel, 1, 1024, 0, s, c);
     cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
     launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
@@ -1459,9 +1485,9 @@ __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDom
         atomicAdd(acc + cell, (unsigned long long)sum);
 }
 
-void launch_areas(const MembraneDev& m, double* area, cudaStream_t s) {
+void launch_areas(const MembraneDev& m, double* area, Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
-    launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, nullptr);
+    launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, st);
 }
 
 // The fixed device array of lbib_areas_static: the per-cell sums of one call.

@@ -113,6 +113,7 @@ __global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st, const 
     const double x = (m.x[a] + m.x[b]) / 2, y = (m.y[a] + m.y[b]) / 2;
     m.x[j] = x; m.y[j] = y;
     m.ox[j] = x - 5.0; m.oy[j] = y - 5.0;   // GeometryNode.cpp:98-103
+    m.bx[j] = x; m.by[j] = y;               // bound by remesh_again_kernel
     m.vx[j] = 0.0; m.vy[j] = 0.0; m.fx[j] = 0.0; m.fy[j] = 0.0;
     m.id[j] = T->maxId + 1 + (unsigned)r;
     m.next[a] = j; m.prev[j] = a; m.next[j] = b; m.prev[b] = j;
@@ -169,6 +170,8 @@ __global__ void remesh_again_kernel(MembraneDev m, int nx, int ny, Status* st) {
         const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
         const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
         if (within || st->halt) continue;
+        m.bx[i] = X;  // bound from the current position (GeometryHandler.cpp:637-643)
+        m.by[i] = Y;
         if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
         else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
         else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
@@ -353,6 +356,7 @@ __global__ void coarsen_gather_kernel(MembraneDev m, TopoDev t, Status* st) {
         const size_t cap = (size_t)m.Mcap;
         a[0 * cap + d] = m.x[i]; a[1 * cap + d] = m.y[i]; a[2 * cap + d] = m.ox[i]; a[3 * cap + d] = m.oy[i];
         a[4 * cap + d] = m.vx[i]; a[5 * cap + d] = m.vy[i]; a[6 * cap + d] = m.fx[i]; a[7 * cap + d] = m.fy[i];
+        a[8 * cap + d] = m.bx[i]; a[9 * cap + d] = m.by[i];
         t.id2[d] = m.id[i];
         t.prev2[d] = t.nrank[m.prev[i]];
         t.next2[d] = t.nrank[m.next[i]];
@@ -380,6 +384,7 @@ __global__ void coarsen_scatter_back_kernel(MembraneDev m, TopoDev t, Status* st
         const size_t cap = (size_t)m.Mcap;
         m.x[i] = a[0 * cap + i]; m.y[i] = a[1 * cap + i]; m.ox[i] = a[2 * cap + i]; m.oy[i] = a[3 * cap + i];
         m.vx[i] = a[4 * cap + i]; m.vy[i] = a[5 * cap + i]; m.fx[i] = a[6 * cap + i]; m.fy[i] = a[7 * cap + i];
+        m.bx[i] = a[8 * cap + i]; m.by[i] = a[9 * cap + i];
         m.id[i] = t.id2[i]; m.prev[i] = t.prev2[i]; m.next[i] = t.next2[i];
     }
     if (i <= Mn) m.foff[i] = 0;  // the force list is empty at a coarsening step

@@ -26,6 +26,11 @@ struct MembraneDev {
     int C;          // host view of the connection count
     double* x; double* y;       // LagrangianPoint::position_
     double* ox; double* oy;     // GeometryNode::oldPosition_
+    // position at the node's last stencil binding: GeometryNode::
+    // neighbourPhysicalNodes_ is rebound only when isUpdateNeeded fires
+    // (GeometryNode.cpp:256-261), from the position of that moment
+    // (GeometryHandler.cpp:608-644); the stencil ranges derive from it
+    double* bx; double* by;
     double* vx; double* vy;     // LagrangianPoint::velocity_
     double* fx; double* fy;     // GeometryNode::force_
     uint32_t* id;
@@ -96,6 +101,13 @@ struct CrossDev {
     double* nfD;                 // 2 per key, scratch of the boundary solvers
     int* nfN;                    // number of nfKeys
     int nfCap;
+    // the W- and S-slot boundary nodes of this step's crossings, for the next
+    // step's advect of DiracD2Q5 species (nullptr when none is registered)
+    uint8_t* bounceW;            // L
+    uint8_t* bounceS;            // L
+    uint32_t* bounceKeys;        // keys set, for the reset
+    int* bounceN;
+    int bounceCap;
 };
 
 // Tiles for force spreading.
@@ -122,7 +134,7 @@ struct TopoDev {
     int* nflag;         // Mcap + 1
     int* nrank;         // Mcap + 1
     int* ca2; int* cb2; uint32_t* cdom2; int* cdesc2;    // Ccap
-    double* dalt;       // 8 * Mcap node doubles
+    double* dalt;       // 10 * Mcap node doubles
     uint32_t* id2; int* prev2; int* next2;                // Mcap
     int* inConn; int* outConn;                            // Mcap
     unsigned char* removed;                               // Mcap
@@ -147,13 +159,15 @@ void launch_stream_collide64(const LatticeArgs<double>& a, cudaStream_t s);
 template <typename Real>
 void launch_noflux(const LatticeArgs<Real>& a, cudaStream_t s);
 void launch_outlet64(double* f, double* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
+// vel == nullptr: FluidSolver::initSolver (f_T = 1, then collide); else
+// FluidSolver::initWithVelocity at the uniform velocity vel[0], vel[1].
 void launch_init64(double* f, double* g, double* u, int nS, size_t L, double tauF, const uint32_t* dom,
-                   const SpeciesConst* sp, const double* init, cudaStream_t s);
+                   const double* vel, const SpeciesConst* sp, const double* init, cudaStream_t s);
 
 void launch_stream_collide32(const LatticeArgs<float>& a, cudaStream_t s);
 void launch_outlet32(float* f, float* g, int nS, int nx, int ny, size_t L, const Status* st, cudaStream_t s);
 void launch_init32(float* f, float* g, float* u, int nS, size_t L, double tauF, const uint32_t* dom,
-                   const SpeciesConst* sp, const double* init, cudaStream_t s);
+                   const double* vel, const SpeciesConst* sp, const double* init, cudaStream_t s);
 
 // Membrane pipeline.  `Real` is the lattice precision (velocity / force planes).
 template <typename Real>
@@ -208,7 +222,8 @@ void launch_tension_renewal(MembraneDev& m, int* outPos, int* inPos, double forc
 void launch_area_regulator(const MembraneDev& m, double* area, double* target, double* massTab, int nDomains,
                            double factor, double strength, double maxsource, const uint32_t* ctypeTab,
                            const Status* st, cudaStream_t s);
-void launch_areas(const MembraneDev& m, double* area, cudaStream_t s);
+// st != nullptr: a ring longer than the kernel's limit raises ERR_CAPACITY there.
+void launch_areas(const MembraneDev& m, double* area, Status* st, cudaStream_t s);
 // FP32-shifted runs: areas from the connections in fixed point (no ring order
 // needed), then the regulator.  acc (nCells) must start at zero; it is left zero.
 void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,
@@ -244,6 +259,7 @@ struct AdjointArgs {
     const float* pf;       // 9*L      adjoint planes of step t+1 (unused with seed), FP32
     const float* pg;       // S*5*L
     const double* seed;    // S*L      dL/dC_k at the final step, or nullptr
+    const double* seedF;   // 9*L      dL/d(stored fluid state) at the final step (natural order), or nullptr
     float* qf;             // 9*L      adjoint planes of step t (output), FP32
     float* qg;             // S*5*L
     const double* force;   // 2*L      spread force field (zero outside the force tiles)
@@ -258,8 +274,9 @@ struct AdjointArgs {
     int outlet;
     double* G;             // 2*L      dL/dF(x), summed over steps
     double* racc;          // S*L      dL/d source at each node, summed over steps
+    double* macc;          // L        dL/d rhoToAdd at each node, summed over steps (with massTab)
     double* part;          // adjoint_blocks * (1 + S): per-block relaxation-time partials
-    double* grad;          // 1 + S + S*nDomains (written by launch_adjoint_finish)
+    double* grad;          // 1 + S + S*nDomains + nDomains (written by launch_adjoint_finish)
 };
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s);
 // Thread blocks of one adjoint launch (the rows of AdjointArgs::part).

@@ -72,6 +72,91 @@ __host__ __device__ __forceinline__ void collide_fluid64(double* fi, double rhoT
     luo_velocity(rho, fi, uxo, uyo);
 }
 
+// FluidSolver::initWithVelocity (FluidSolver.cpp:62-101): the equilibrium at
+// rho = 1 and velocity (u, v), natural direction order.
+__host__ __device__ __forceinline__ void equilibrium_at_velocity64(double u, double v, double* fi) {
+    const double W0 = 4.0 / 9.0, W1 = 1.0 / 9.0, W2 = 1.0 / 36.0;
+    const double rho = 1.0;
+    const double u2 = u * u;
+    const double v2 = v * v;
+    const double W1rho = W1 * rho;
+    const double W2rho = W2 * rho;
+    const double W3 = 9.0 / 2.0;
+    const double lastTerm = 3.0 / 2.0 * (u2 + v2);
+    fi[T] = W0 * rho * (1.0 - lastTerm);
+    fi[E] = W1rho * (1.0 + 3.0 * u + W3 * u2 - lastTerm);
+    fi[NE] = W2rho * (1.0 + 3.0 * (u + v) + W3 * (u + v) * (u + v) - lastTerm);
+    fi[N] = W1rho * (1.0 + 3.0 * v + W3 * v2 - lastTerm);
+    fi[NW] = W2rho * (1.0 + 3.0 * (-u + v) + W3 * (-u + v) * (-u + v) - lastTerm);
+    fi[W] = W1rho * (1.0 + 3.0 * (-u) + W3 * u2 - lastTerm);
+    fi[SW] = W2rho * (1.0 + 3.0 * (-u - v) + W3 * (-u - v) * (-u - v) - lastTerm);
+    fi[S] = W1rho * (1.0 + 3.0 * (-v) + W3 * v2 - lastTerm);
+    fi[SE] = W2rho * (1.0 + 3.0 * (u - v) + W3 * (u - v) * (u - v) - lastTerm);
+}
+
+// GuoZhengShi2002ForceModel::computeVelocity (GuoZhengShi2002ForceModel.cpp:60-78):
+// the momentum includes half the force.
+__host__ __device__ __forceinline__ void guo_velocity(double rho, const double* fi, double fx, double fy, double& ux,
+                                                      double& uy) {
+    const double rhoI = 1.0 / rho;
+    ux = (fi[E] + fi[NE] + fi[SE] - (fi[NW] + fi[W] + fi[SW]) + 0.5 * fx) * rhoI;
+    uy = (fi[NE] + fi[N] + fi[NW] - (fi[SW] + fi[S] + fi[SE]) + 0.5 * fy) * rhoI;
+}
+
+// FluidSolver::collide with GuoZhengShi2002ForceModel as the force model
+// (the base class FluidSolver.hpp:41 names in a comment).  The equilibrium
+// uses u of guo_velocity; the force term (GuoZhengShi2002ForceModel.cpp:29-58)
+// is (1 - 1/2tau) w_i [3 (e_i - v) + 9 (e_i . v) e_i] . F with v the node's
+// stored velocity (FluidSolver::getVelocity, the last collide's result: vx,
+// vy).  neY is the coefficient of v_y in the NE term's F_y factor: the
+// reference writes -3 (`9.0*u.x - 3.0*u.y + 3.0`, :51); the expansion above
+// gives +6.  The expressions keep the reference's evaluation order.
+__host__ __device__ __forceinline__ void collide_fluid64_guo(double* fi, double rhoToAdd, double fx, double fy,
+                                                            double tauF, double vx, double vy, double neY,
+                                                            double& uxo, double& uyo) {
+    const double W0 = 4.0 / 9.0, W1 = 1.0 / 9.0, W2 = 1.0 / 36.0;
+    double rho = sum9(fi);
+    if (isfinite(rhoToAdd)) rho += rhoToAdd;
+    double ux, uy;
+    guo_velocity(rho, fi, fx, fy, ux, uy);
+    const double ux2 = ux * ux;
+    const double uy2 = uy * uy;
+    const double lastTerm = 3.0 / 2.0 * (ux2 + uy2);
+    const double tauI = 1.0 / tauF;
+    const double W3 = 9.0 / 2.0;
+    const double W1rho = W1 * rho;
+    const double W2rho = W2 * rho;
+    const double G0 = (1.0 - 0.5 / tauF) * 4.0 / 9.0;
+    const double G1 = (1.0 - 0.5 / tauF) / 9.0;
+    const double G2 = (1.0 - 0.5 / tauF) / 36.0;
+    double fc[9];
+    fc[T] = G0 * (-3.0 * vx * fx - 3.0 * vy * fy);
+    fc[E] = G1 * ((6.0 * vx + 3.0) * fx - 3.0 * vy * fy);
+    fc[N] = G1 * (-3.0 * vx * fx + (6.0 * vy + 3.0) * fy);
+    fc[W] = G1 * ((6.0 * vx - 3.0) * fx - 3.0 * vy * fy);
+    fc[S] = G1 * (-3.0 * vx * fx + (6.0 * vy - 3.0) * fy);
+    fc[NE] = G2 * ((6.0 * vx + 9.0 * vy + 3.0) * fx + (9.0 * vx + neY * vy + 3.0) * fy);
+    fc[NW] = G2 * ((6.0 * vx - 9.0 * vy - 3.0) * fx + (-9.0 * vx + 6.0 * vy + 3.0) * fy);
+    fc[SW] = G2 * ((6.0 * vx + 9.0 * vy - 3.0) * fx + (9.0 * vx + 6.0 * vy - 3.0) * fy);
+    fc[SE] = G2 * ((6.0 * vx - 9.0 * vy + 3.0) * fx + (-9.0 * vx + 6.0 * vy - 3.0) * fy);
+    double temp[9];
+    temp[T] = W0 * rho * (1.0 - lastTerm) * tauI + fc[T];
+    temp[E] = W1rho * (1.0 + 3.0 * ux + W3 * ux2 - lastTerm) * tauI + fc[E];
+    temp[NE] = W2rho * (1.0 + 3.0 * (ux + uy) + W3 * (ux + uy) * (ux + uy) - lastTerm) * tauI + fc[NE];
+    temp[N] = W1rho * (1.0 + 3.0 * uy + W3 * uy2 - lastTerm) * tauI + fc[N];
+    temp[NW] = W2rho * (1.0 + 3.0 * (-ux + uy) + W3 * (-ux + uy) * (-ux + uy) - lastTerm) * tauI + fc[NW];
+    temp[W] = W1rho * (1.0 + 3.0 * (-ux) + W3 * ux2 - lastTerm) * tauI + fc[W];
+    temp[SW] = W2rho * (1.0 + 3.0 * (-ux - uy) + W3 * (-ux - uy) * (-ux - uy) - lastTerm) * tauI + fc[SW];
+    temp[S] = W1rho * (1.0 + 3.0 * (-uy) + W3 * uy2 - lastTerm) * tauI + fc[S];
+    temp[SE] = W2rho * (1.0 + 3.0 * (ux - uy) + W3 * (ux - uy) * (ux - uy) - lastTerm) * tauI + fc[SE];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) {
+        const double tempD = fi[d];
+        fi[d] = tempD - tempD * tauI + temp[d];
+    }
+    guo_velocity(rho, fi, fx, fy, uxo, uyo);
+}
+
 // Reaction term R for one species at one node.
 //   RX_LINEAR: R = source[domain] - decay*C (the Lbib species plugins)
 //   RX_SIGNAL: tutorial_01_CDESolverD2Q5_SIGNAL.cpp:92-100

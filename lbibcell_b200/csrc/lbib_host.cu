@@ -103,7 +103,8 @@ enum InitStyle {
     INIT_KERNEL = 0,  // init64 / init32
     INIT_ZERO,        // CDESolverD2Q5BMP.cpp:45-50
     INIT_T2,          // tutorial_02_CDESolverD2Q5_R.cpp:44-59: (1 + U(-0.01, 0.01)) / 5 per slot, 0 outside cells
-    INIT_SCHNAK       // SchnakenbergD2Q5u.cpp:43-58: 0.2 (1 + U(-0.01, 0.01)) per node, 0 outside cells
+    INIT_SCHNAK,      // SchnakenbergD2Q5u.cpp:43-58: 0.2 (1 + U(-0.01, 0.01)) per node, 0 outside cells
+    INIT_DIRAC        // DiracD2Q5.cpp:39-66: the 2D heat kernel at t = 50, D = 0.04, centred at (32, 32)
 };
 
 struct Species {
@@ -146,6 +147,12 @@ struct DiffCtx {
     double* grad = nullptr;   // 1 + S + S*nDomains
     double* racc = nullptr;   // S*L
     double* part = nullptr;   // adjoint blocks * (1 + S)
+    double* massTab = nullptr;  // nDomains: the run's per-domain mass source (rhoToAdd)
+    double* macc = nullptr;     // L: dL/d rhoToAdd per node
+    double* seedF = nullptr;    // 9*L: dL/d(final fluid state), natural direction order
+    bool massUsed = false;      // the run applies massTab (an area regulator, or lbib_diff_mass)
+    bool haveSeedF = false;
+    std::vector<double> gmass;  // dL/d massTab of the last backward pass
     Status* st = nullptr;
     double tauF = 1.0;
     double tau[kMaxSpecies] = {1.0, 1.0, 1.0};
@@ -156,7 +163,7 @@ struct DiffCtx {
     ~DiffCtx() {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(x0); fr(u0); fr(ck); fr(seg); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(fxp); fr(fyp); fr(gfx); fr(gfy);
-        fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st);
+        fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st); fr(massTab); fr(macc); fr(seedF);
     }
 };
 
@@ -167,6 +174,7 @@ struct Handle {
     int precision = 0;
     int device = 0;
     double tauF = 1.0;
+    int forceModel = FM_LUO;  // the fluid's force model (plugin file line "ForceModel <name>")
     unsigned iteration = 0, iterations = 0, reportStep = 1;
     std::vector<Species> sp;
     bool outlet = false;
@@ -229,6 +237,9 @@ struct Handle {
     NfSpec* nfTabDev = nullptr;          // boundary solvers per descriptor (device), nullptr: none
     Status* st = nullptr;
     Status* stHost = nullptr;
+    Topo* topoHost = nullptr;   // pinned copy of the device counts, read with the status word
+    bool ringsCurrent = false;  // the device's ring order matches the topology (no rebuild needed)
+    std::vector<double> areaHost;  // staging of lbib_areas' read-back
     cudaStream_t stream = nullptr;
 
     std::mt19937 genNode{1};
@@ -240,6 +251,11 @@ struct Handle {
     int divisionPolicy = 0;
     unsigned divisionFreq = 100;
     double divisionMax = 380.0;
+    // LbibCellDivision: threshold divisionFactor x the cell's reference area
+    // (its area at the solver's first look; daughters inherit it); 0 = the
+    // fixed divisionMax of the reference's plugins
+    double divisionFactor = 0.0;
+    std::map<uint32_t, double> divisionRef;
     std::mt19937 genDiv{1};
 
     long long hostEvents = 0;
@@ -278,7 +294,7 @@ Handle::~Handle() {
     auto fr = [](void* p) { if (p) cudaFree(p); };
     for (int i = 0; i < 2; ++i) { fr(f[i]); fr(g[i]); }
     fr(u); fr(force); fr(dom); fr(massTab); fr(massNode); fr(srcTab); fr(ctypeTab);
-    fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id);
+    fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id); fr(m.bx); fr(m.by);
     fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
     fr(outPos); fr(inPos); fr(area); fr(target); fr(areaAcc);
@@ -287,6 +303,7 @@ Handle::~Handle() {
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
     fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys); fr(cross.nfD);
     fr(cross.nfSpec); fr(cross.nfU); fr(cross.nfN); fr(nfTabDev);
+    fr(cross.bounceW); fr(cross.bounceS); fr(cross.bounceKeys); fr(cross.bounceN);
     fr(m.topo); fr(m.cdesc);
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
     fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
@@ -295,6 +312,7 @@ Handle::~Handle() {
     fr(td.dist); fr(td.startNode); fr(td.scanTmp);
     fr(st);
     if (stHost) cudaFreeHost(stHost);
+    if (topoHost) cudaFreeHost(topoHost);
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
     for (auto e : kEvents) cudaEventDestroy(e);
@@ -345,6 +363,7 @@ static void load_parameters(Handle& h, const std::string& fn) {
         s.c.reinit = RI_BASE;
         s.c.dt = 1.0;
         s.c.hill = 0.0;
+        s.c.bounce = 0;
         const std::string& nm = kv.first;
         if (nm == "CDESolverD2Q5") {
             s.c.kind = RX_NONE;
@@ -368,11 +387,19 @@ static void load_parameters(Handle& h, const std::string& fn) {
             s.c.hill = std::pow(0.01, 4.0);  // pow(k_hill, n_hill), CDESolverD2Q5BMP.cpp:113-117
             s.partnerName = "CDESolverD2Q5HH";
             s.initStyle = INIT_ZERO;
+        } else if (nm == "DiracD2Q5") {
+            // DiracD2Q5.cpp: CDESolverD2Q5's collide without reaction; advect
+            // keeps the populations of links with a boundary node (:166-180);
+            // reinitialise from E,N,W,S without a boundary node, else the four
+            // diagonals, C/4 per slot (:182-228)
+            s.c.kind = RX_NONE;
+            s.c.reinit = RI_DIAG;
+            s.c.bounce = 1;
+            s.initStyle = INIT_DIRAC;
         } else if (nm.compare(0, 4, "Lbib") == 0) {
             s.c.kind = RX_LINEAR;
         } else {
-            // DiracD2Q5 (whose advect keeps the populations of boundary links,
-            // DiracD2Q5.cpp:166-180) and the D2Q4 solvers are not built
+            // the D2Q4 solvers are not built
             fail(ERR_INPUT, "unknown or unsupported CDE solver " + nm);
         }
         h.sp.push_back(s);
@@ -403,6 +430,13 @@ static void load_plugins(Handle& h, const std::string& fn) {
         if (kind == "MassSolver") {
             if (name == "MassSolverBoxOutlet") h.outlet = true;
             else fail(ERR_INPUT, "unknown mass solver " + name);
+        } else if (kind == "ForceModel") {
+            // FluidSolver's force model, a base class chosen when the
+            // reference is compiled (FluidSolver.hpp:41); here per handle
+            if (name == "Luo1993ForceModel") h.forceModel = FM_LUO;
+            else if (name == "GuoZhengShi2002ForceModel") h.forceModel = FM_GUO;
+            else if (name == "GuoZhengShi2002ForceModelCorrected") h.forceModel = FM_GUO_CORRECTED;
+            else fail(ERR_INPUT, "unknown force model " + name);
         } else if (kind == "BioSolver") {
             std::string k; double v;
             while (ls >> k >> v) kv[k] = v;
@@ -451,6 +485,16 @@ static void load_plugins(Handle& h, const std::string& fn) {
                 // divides along a random direction, BioSolverCellDivision.cpp:100-101)
                 h.bio.push_back(4);
                 h.divisionPolicy = name == "BioSolverCellDivision" ? 1 : 0;
+            } else if (name == "LbibCellDivision") {
+                // the tutorial_01 division (longest axis) with a per-cell
+                // threshold: factor x the cell's reference area, every
+                // `frequency` iterations
+                h.bio.push_back(4);
+                h.divisionPolicy = 0;
+                h.divisionFactor = kv.count("factor") ? kv["factor"] : 2.0;
+                h.divisionFreq = kv.count("frequency") ? (unsigned)kv["frequency"] : 100u;
+                if (h.divisionFreq == 0 || !(h.divisionFactor > 0.0))
+                    fail(ERR_INPUT, "LbibCellDivision needs a positive factor and frequency");
             } else if (name == "LbibAreaRegulator") {
                 h.bio.push_back(2);
                 h.areaTutorial = false;
@@ -534,12 +578,14 @@ static void add_force_line(Handle& h, const std::string& line) {
 
 struct HostMembrane {
     std::vector<double> x, y, ox, oy, vx, vy, fx, fy;
+    std::vector<double> bx, by;  // position at the last stencil binding
 };
 
 static void download_membrane(Handle& h, HostMembrane& hm) {
     const int M = h.m.M;
     hm.x.resize(M); hm.y.resize(M); hm.ox.resize(M); hm.oy.resize(M);
     hm.vx.resize(M); hm.vy.resize(M); hm.fx.resize(M); hm.fy.resize(M);
+    hm.bx.resize(M); hm.by.resize(M);
     if (M == 0) return;
     const size_t b = sizeof(double) * M;
     CK(cudaMemcpyAsync(hm.x.data(), h.m.x, b, cudaMemcpyDeviceToHost, h.stream));
@@ -550,6 +596,8 @@ static void download_membrane(Handle& h, HostMembrane& hm) {
     CK(cudaMemcpyAsync(hm.vy.data(), h.m.vy, b, cudaMemcpyDeviceToHost, h.stream));
     CK(cudaMemcpyAsync(hm.fx.data(), h.m.fx, b, cudaMemcpyDeviceToHost, h.stream));
     CK(cudaMemcpyAsync(hm.fy.data(), h.m.fy, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.bx.data(), h.m.bx, b, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(hm.by.data(), h.m.by, b, cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
 }
 
@@ -637,6 +685,7 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
     up(h.m.ox, hm.ox.data(), bd); up(h.m.oy, hm.oy.data(), bd);
     up(h.m.vx, hm.vx.data(), bd); up(h.m.vy, hm.vy.data(), bd);
     up(h.m.fx, hm.fx.data(), bd); up(h.m.fy, hm.fy.data(), bd);
+    up(h.m.bx, hm.bx.data(), bd); up(h.m.by, hm.by.data(), bd);
     up(h.m.id, h.ids.data(), sizeof(uint32_t) * M);
     up(h.m.prev, prev.data(), sizeof(int) * M);
     up(h.m.next, next.data(), sizeof(int) * M);
@@ -680,6 +729,7 @@ static void upload_topology(Handle& h, const HostMembrane& hm, bool uploadForces
     h.targetHost = tnew;
     up(h.target, tnew.data(), sizeof(double) * cells);
     CK(cudaStreamSynchronize(h.stream));
+    h.ringsCurrent = true;  // the rings were uploaded with the topology
 }
 
 // Refreshes the host mirror of the topology (node ids, connection vector)
@@ -778,7 +828,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     if (grow(M, h.Mcap)) {
         // membrane arrays are rewritten by every upload_topology; no copy needed
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.x); fr(h.m.y); fr(h.m.ox); fr(h.m.oy); fr(h.m.vx); fr(h.m.vy); fr(h.m.fx); fr(h.m.fy);
+        fr(h.m.x); fr(h.m.y); fr(h.m.ox); fr(h.m.oy); fr(h.m.vx); fr(h.m.vy); fr(h.m.fx); fr(h.m.fy); fr(h.m.bx); fr(h.m.by);
         fr(h.m.id); fr(h.m.prev); fr(h.m.next); fr(h.outPos); fr(h.inPos); fr(h.cross.perturbList);
         fr(h.m.foff); fr(h.m.ringNode); fr(h.tiles.list);
         fr(h.td.nflag); fr(h.td.nrank); fr(h.td.dalt); fr(h.td.id2); fr(h.td.prev2); fr(h.td.next2);
@@ -786,7 +836,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         fr(h.td.ncDesc); fr(h.td.ncAlive); fr(h.td.members); fr(h.td.succ); fr(h.td.dist);
         const int n = h.Mcap;
         h.td.nflag = dalloc<int>(n + 1); h.td.nrank = dalloc<int>(n + 1);
-        h.td.dalt = dalloc<double>(8 * (size_t)n);
+        h.td.dalt = dalloc<double>(10 * (size_t)n);
         h.td.id2 = dalloc<uint32_t>(n); h.td.prev2 = dalloc<int>(n); h.td.next2 = dalloc<int>(n);
         h.td.inConn = dalloc<int>(n); h.td.outConn = dalloc<int>(n);
         h.td.removed = dalloc<unsigned char>(n);
@@ -796,6 +846,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         CK(cudaMemsetAsync(h.td.ncAlive, 0, sizeof(int) * (n + 1), h.stream));
         h.td.members = dalloc<int>(n); h.td.succ = dalloc<int>(n + 1); h.td.dist = dalloc<int>(n + 1);
         h.m.x = dalloc<double>(n); h.m.y = dalloc<double>(n); h.m.ox = dalloc<double>(n); h.m.oy = dalloc<double>(n);
+        h.m.bx = dalloc<double>(n); h.m.by = dalloc<double>(n);
         h.m.vx = dalloc<double>(n); h.m.vy = dalloc<double>(n); h.m.fx = dalloc<double>(n); h.m.fy = dalloc<double>(n);
         h.m.id = dalloc<uint32_t>(n); h.m.prev = dalloc<int>(n); h.m.next = dalloc<int>(n);
         h.outPos = dalloc<int>(n); h.inPos = dalloc<int>(n);
@@ -953,6 +1004,7 @@ static bool remesh(Handle& h, HostMembrane& hm) {
                 h.ids.push_back(nid);
                 hm.x.push_back(nx); hm.y.push_back(ny);
                 hm.ox.push_back(ox); hm.oy.push_back(oy);
+                hm.bx.push_back(nx); hm.by.push_back(ny);  // bound by the edge check after the upload
                 hm.vx.push_back(0.0); hm.vy.push_back(0.0);
                 hm.fx.push_back(0.0); hm.fy.push_back(0.0);
                 added.push_back(HConn{c.id1, nid, c.dom, c.desc});
@@ -993,12 +1045,15 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     a.srcTab = h.srcTab;
     a.ctypeTab = h.ctypeTab;
     a.tauF = h.tauF;
+    a.forceModel = h.forceModel;
     for (int k = 0; k < h.S; ++k) {
         a.sp[k] = h.sp[k].c;
         a.coupled |= coupled_kind(h.sp[k].c.kind) ? 1 : 0;
     }
     a.status = h.st;
     a.outlet = h.outlet ? 1 : 0;
+    a.bounceW = h.cross.bounceW;
+    a.bounceS = h.cross.bounceS;
     if (h.cross.nfTab != nullptr) {
         a.nfSpec = h.cross.nfSpec;
         a.nfU = h.cross.nfU;
@@ -1150,9 +1205,14 @@ static int resume_stage(int stage) {
     }
 }
 
+// Reads the status word and, in the same synchronisation, the device counts:
+// their `changed` flag says whether the ring order of the cell areas is stale
+// (remeshing or coarsening on the device set it; a ring rebuild clears it).
 static void read_status(Handle& h) {
     CK(cudaMemcpyAsync(h.stHost, h.st, sizeof(Status), cudaMemcpyDeviceToHost, h.stream));
+    if (h.m.topo) CK(cudaMemcpyAsync(h.topoHost, h.m.topo, sizeof(Topo), cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
+    if (h.m.topo) h.ringsCurrent = h.topoHost->changed == 0;
 }
 
 static void write_status(Handle& h) {
@@ -1412,7 +1472,7 @@ static void setup_boundary_solvers(Handle& h);
 // (rows, then columns; SimulationRunner.cpp:290-306).  The reference seeds its
 // generators from std::random_device, so no two of its runs agree; here each
 // solver type has one std::mt19937 with the default seed, drawn in that order.
-static void init_species_host(Handle& h) {
+static void init_species_host(Handle& h, const double* vel) {
     bool any = false;
     for (const auto& s : h.sp) any |= s.initStyle != INIT_KERNEL;
     if (!any) return;
@@ -1438,6 +1498,20 @@ static void init_species_host(Handle& h) {
                     for (int q = 0; q < 5; ++q) gi[q] = dom[n] == 0 ? 0.0 : temp;
                     break;
                 }
+                case INIT_DIRAC: {
+                    // DiracD2Q5::initSolver (DiracD2Q5.cpp:39-66) on the host, with
+                    // the host's exp: every slot 0.2 x the heat kernel at the
+                    // node's distance from (32, 32), then collide at the
+                    // fluid's velocity (zero after FluidSolver::initSolver)
+                    const double pos = 32, D = 0.04, t = 50;
+                    const double PI = std::atan(1) * 4;
+                    const double px = (double)(n % (size_t)h.nx), py = (double)(n / (size_t)h.nx);
+                    const double dist = std::sqrt((pos - px) * (pos - px) + (pos - py) * (pos - py));
+                    const double kernel = std::exp(-dist * dist / (4.0 * D * t)) / (4.0 * PI * D * t);
+                    for (int q = 0; q < 5; ++q) gi[q] = kernel * 0.2;
+                    collide_cde64(gi, vel ? vel[0] : 0.0, vel ? vel[1] : 0.0, s.c, 0.0, 0.0, dom[n], 0u, 0u);
+                    break;
+                }
                 default:
                     for (int q = 0; q < 5; ++q) gi[q] = 0.0;
             }
@@ -1453,6 +1527,23 @@ static void init_species_host(Handle& h) {
         }
         CK(cudaStreamSynchronize(h.stream));
     }
+}
+
+// SimulationRunner::initSolvers (SimulationRunner.cpp:290-306), or with a
+// velocity initSolvers(Field<double>) (:308-320): every node's FluidSolver
+// initSolver (FluidSolver.cpp:50-101) and then its CDE solvers' initSolver.
+static void init_lattice(Handle& h, const double* vel) {
+    SpeciesConst spc[kMaxSpecies] = {};
+    double init[kMaxSpecies] = {0, 0, 0};
+    for (int k = 0; k < h.S; ++k) { spc[k] = h.sp[k].c; init[k] = h.sp[k].init; }
+    if (h.precision == LBIB_FP64)
+        launch_init64((double*)h.f[0], (double*)h.g[0], (double*)h.u, h.S, h.L, h.tauF, h.dom, vel, spc, init,
+                      h.stream);
+    else
+        launch_init32((float*)h.f[0], (float*)h.g[0], (float*)h.u, h.S, h.L, h.tauF, h.dom, vel, spc, init,
+                      h.stream);
+    init_species_host(h, vel);
+    h.cur = 0;
 }
 
 static void create(Handle& h, const std::string& params, const std::string& geom, const std::string& forceFile,
@@ -1478,6 +1569,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.dom, 0, sizeof(uint32_t) * h.L, h.stream));
     CK(cudaMalloc(&h.st, sizeof(Status)));
     CK(cudaMallocHost(&h.stHost, sizeof(Status)));
+    CK(cudaMallocHost(&h.topoHost, sizeof(Topo)));
+    std::memset(h.topoHost, 0, sizeof(Topo));
     init_kernel_attributes();
     // LBIB_NO_GRAPHS=1 launches every stage kernel directly (no CUDA graphs)
     if (const char* e = std::getenv("LBIB_NO_GRAPHS")) h.useGraphs = !(e[0] == '1');
@@ -1508,6 +1601,19 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.cross.bnDist, 0xff, sizeof(unsigned long long) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.bnConn, 0xff, sizeof(uint32_t) * 4 * h.L, h.stream));
     CK(cudaMemsetAsync(h.cross.wDom, 0, sizeof(uint32_t) * h.L, h.stream));
+    bool bounce = false;
+    for (const auto& s : h.sp) bounce |= s.c.bounce != 0;
+    if (bounce) {
+        // DiracD2Q5: the W / S boundary-node marks its advect reads
+        h.cross.bounceW = dalloc<uint8_t>(h.L);
+        h.cross.bounceS = dalloc<uint8_t>(h.L);
+        CK(cudaMemsetAsync(h.cross.bounceW, 0, h.L, h.stream));
+        CK(cudaMemsetAsync(h.cross.bounceS, 0, h.L, h.stream));
+        h.cross.bounceCap = (int)std::min<size_t>(2 * h.L, 0x7fffffff);
+        h.cross.bounceKeys = dalloc<uint32_t>(h.cross.bounceCap);
+        h.cross.bounceN = dalloc<int>(1);
+        CK(cudaMemsetAsync(h.cross.bounceN, 0, sizeof(int), h.stream));
+    }
 
     h.m.topo = dalloc<Topo>(1);
 
@@ -1571,6 +1677,8 @@ static void create(Handle& h, const std::string& params, const std::string& geom
         hm.y.push_back(kv.second.second);
         hm.ox.push_back(kv.second.first - 5.0);
         hm.oy.push_back(kv.second.second - 5.0);
+        hm.bx.push_back(kv.second.first);   // bound by cureLattice's edge check
+        hm.by.push_back(kv.second.second);
         hm.vx.push_back(0.0); hm.vy.push_back(0.0); hm.fx.push_back(0.0); hm.fy.push_back(0.0);
     }
     // tables indexed by domain id
@@ -1618,16 +1726,16 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     setup_boundary_solvers(h);
     cure_lattice(h, hm);
 
+    if (h.cross.bounceW != nullptr) {
+        // the lattice kernels carry DiracD2Q5's advect for the plain fluid only
+        if (h.forceModel != FM_LUO || h.massNode != nullptr || h.cross.nfTab != nullptr)
+            fail(ERR_INPUT, "DiracD2Q5 runs with the Luo force model, without per-node mass sources and "
+                            "without boundary solvers on connections");
+        for (const auto& s : h.sp)
+            if (coupled_kind(s.c.kind)) fail(ERR_INPUT, "DiracD2Q5 runs without coupled reactions");
+    }
     // SimulationRunner::initSolvers (SimulationRunner.cpp:290-306)
-    SpeciesConst spc[kMaxSpecies] = {};
-    double init[kMaxSpecies] = {0, 0, 0};
-    for (int k = 0; k < h.S; ++k) { spc[k] = h.sp[k].c; init[k] = h.sp[k].init; }
-    if (h.precision == LBIB_FP64)
-        launch_init64((double*)h.f[0], (double*)h.g[0], (double*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
-    else
-        launch_init32((float*)h.f[0], (float*)h.g[0], (float*)h.u, h.S, h.L, h.tauF, h.dom, spc, init, h.stream);
-    init_species_host(h);
-    h.cur = 0;
+    init_lattice(h, nullptr);
     // SimulationRunner::initForceSolver: the force list
     if (!h.forcemap.empty()) upload_topology(h, hm, true);
     CK(cudaStreamSynchronize(h.stream));
@@ -1714,8 +1822,8 @@ static void diff_begin(Handle& h, int T, int K) {
     const size_t stateDoubles = (size_t)(9 + 5 * S) * L;
     const size_t states = 1 + (size_t)(nSeg - 1) + (size_t)(K - 1) + 2;
     const size_t nPart = (size_t)adjoint_blocks(h.nx, h.ny) * (1 + S);
-    const size_t bytes = sizeof(double) * (states * stateDoubles + 10 * L + 2 * (size_t)S * L + nPart + 4 * (size_t)h.Mcap +
-                                           2 * (size_t)S * h.nDomains + 1 + S);
+    const size_t bytes = sizeof(double) * (states * stateDoubles + 20 * L + 2 * (size_t)S * L + nPart + 4 * (size_t)h.Mcap +
+                                           2 * (size_t)S * h.nDomains + 2 * (size_t)h.nDomains + 1 + S);
     size_t freeB = 0, totalB = 0;
     CK(cudaMemGetInfo(&freeB, &totalB));
     if (bytes + (256u << 20) > freeB)
@@ -1735,8 +1843,20 @@ static void diff_begin(Handle& h, int T, int K) {
     d->gfx = dalloc<double>(h.Mcap); d->gfy = dalloc<double>(h.Mcap);
     d->srcTab = dalloc<double>((size_t)S * h.nDomains);
     d->seed = dalloc<double>((size_t)S * L);
-    d->grad = dalloc<double>(1 + S + (size_t)S * h.nDomains);
+    d->grad = dalloc<double>(1 + S + (size_t)(S + 1) * h.nDomains);
     d->racc = dalloc<double>((size_t)S * L);
+    d->massTab = dalloc<double>(h.nDomains);
+    d->macc = dalloc<double>(L);
+    d->seedF = dalloc<double>(9 * L);
+    {
+        // the frozen mass table: the area regulator's last rates, or none
+        bool area = false;
+        for (int b : h.bio) area |= (b == 2);
+        d->massUsed = area;
+        if (area) CK(cudaMemcpyAsync(d->massTab, h.massTab, sizeof(double) * h.nDomains, cudaMemcpyDeviceToDevice,
+                                     h.stream));
+        else CK(cudaMemsetAsync(d->massTab, 0, sizeof(double) * h.nDomains, h.stream));
+    }
     d->part = dalloc<double>(nPart);
     d->st = dalloc<Status>(1);
     CK(cudaMemsetAsync(d->st, 0, sizeof(Status), h.stream));
@@ -1774,6 +1894,7 @@ static void diff_forward_step(Handle& h, DiffCtx& d, const double* in, double* o
     a.gin = in + 9 * h.L; a.gout = out + 9 * h.L;
     a.force = d.force;
     a.srcTab = d.srcTab;
+    a.massTab = d.massUsed ? d.massTab : nullptr;
     a.tauF = d.tauF;
     for (int k = 0; k < h.S; ++k) a.sp[k].tau = d.tau[k];
     a.status = d.st;
@@ -1817,16 +1938,16 @@ static void diff_backward(Handle& h, DiffCtx& d) {
     const size_t L = h.L;
     const int S = h.S;
     CK(cudaMemsetAsync(d.G, 0, sizeof(double) * 2 * L, h.stream));
-    CK(cudaMemsetAsync(d.grad, 0, sizeof(double) * (1 + S + (size_t)S * h.nDomains), h.stream));
+    CK(cudaMemsetAsync(d.grad, 0, sizeof(double) * (1 + S + (size_t)(S + 1) * h.nDomains), h.stream));
     if (S) CK(cudaMemsetAsync(d.racc, 0, sizeof(double) * S * L, h.stream));
+    CK(cudaMemsetAsync(d.macc, 0, sizeof(double) * L, h.stream));
     CK(cudaMemsetAsync(d.part, 0, sizeof(double) * adjoint_blocks(h.nx, h.ny) * (1 + S), h.stream));
-    bool area = false;
-    for (int b : h.bio) area |= (b == 2);
     AdjointArgs a{};
     a.nx = h.nx; a.ny = h.ny; a.L = L; a.S = S;
     a.force = d.force;
     a.dom = h.dom;
-    a.massTab = area ? h.massTab : nullptr;
+    a.massTab = d.massUsed ? d.massTab : nullptr;
+    a.macc = d.massUsed ? d.macc : nullptr;
     a.nDomains = h.nDomains;
     a.srcTab = d.srcTab;
     a.tauIF = 1.0 / d.tauF;
@@ -1858,6 +1979,7 @@ static void diff_backward(Handle& h, DiffCtx& d) {
             a.pf = seedStep ? nullptr : pin;
             a.pg = seedStep ? nullptr : pin + 9 * L;
             a.seed = seedStep ? d.seed : nullptr;
+            a.seedF = seedStep && d.haveSeedF ? d.seedF : nullptr;
             a.qf = (float*)d.P[t & 1];
             a.qg = (float*)d.P[t & 1] + 9 * L;
             a.iteration = d.it0 + (unsigned)(t - 1);
@@ -2117,6 +2239,16 @@ int lbib_upload_lattice(lbib_handle* hh, const double* f, const double* g, const
     API_END
 }
 
+int lbib_init_velocity(lbib_handle* hh, double ux, double uy) {
+    API_BEGIN(hh)
+    if (!std::isfinite(ux) || !std::isfinite(uy)) lbib::fail(LBIB_ERR_INPUT, "lbib_init_velocity: non-finite velocity");
+    const double vel[2] = {ux, uy};
+    lbib::init_lattice(h, vel);
+    CK(cudaStreamSynchronize(h.stream));
+    CK(cudaGetLastError());
+    API_END
+}
+
 int lbib_download_membrane(lbib_handle* hh, unsigned* ids, double* state) {
     API_BEGIN(hh)
     lbib::pull_topology(h);
@@ -2145,22 +2277,41 @@ int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
     if (!hh) return -LBIB_ERR_STATE;
     Handle& h = hh->h;
     if (h.err) return -h.err;
+    if (cap < 0 || (cap > 0 && (!dom || !area))) {
+        h.msg = "lbib_areas: bad output buffers";
+        return -LBIB_ERR_INPUT;
+    }
     try {
-        cudaSetDevice(h.device);
-        lbib::launch_rings(h.m, h.td, h.st, h.stream);  // FP32-shifted steps leave the ring order stale
-        lbib::launch_areas(h.m, h.area, h.stream);
-        std::vector<double> a(h.m.nCells);
+        CK(cudaSetDevice(h.device));
+        lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+        // the ring order is rebuilt only when the topology changed since it was
+        // last built (FP32-shifted steps and remeshing leave it stale)
+        if (!h.ringsCurrent) lbib::launch_rings(h.m, h.td, h.st, h.stream);
+        lbib::launch_areas(h.m, h.area, h.st, h.stream);
+        CK(cudaGetLastError());
+        h.areaHost.resize(h.m.nCells);
         if (h.m.nCells)
-            CK(cudaMemcpyAsync(a.data(), h.area, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, h.stream));
-        CK(cudaStreamSynchronize(h.stream));
+            CK(cudaMemcpyAsync(h.areaHost.data(), h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost,
+                               h.stream));
+        lbib::read_status(h);
+        if (h.stHost->err) {
+            const long long idx = h.stHost->errIndex;
+            lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+            h.msg = "lbib_areas: cell " + std::to_string(idx) + " has more membrane nodes than one ring may hold";
+            h.errIndex = idx;
+            return -LBIB_ERR_CAPACITY;
+        }
         for (int c = 0; c < h.m.nCells && c < cap; ++c) {
             dom[c] = h.ringDomHost[c];
-            area[c] = a[c];
+            area[c] = h.areaHost[c];
         }
         return h.m.nCells;
     } catch (const HostFail& e) {
         h.err = e.code; h.msg = e.msg;
         return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
     }
 }
 
@@ -2208,17 +2359,31 @@ int lbib_areas_static(lbib_handle* hh, unsigned* dom, double* area, int cap) {
         CK(cudaSetDevice(h.device));
         double* scratch = nullptr;
         CK(static_area_address(h.device, &scratch));
-        lbib::launch_rings(h.m, h.td, h.st, h.stream);  // FP32-shifted steps leave the ring order stale
-        lbib::launch_areas(h.m, scratch, h.stream);
+        lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+        // all-ones bytes read back as NaN: a cell the kernel leaves out shows
+        // no value of an earlier call (or of another handle sharing the array)
+        if (h.m.nCells > 0) CK(cudaMemsetAsync(scratch, 0xFF, sizeof(double) * h.m.nCells, h.stream));
+        if (!h.ringsCurrent) lbib::launch_rings(h.m, h.td, h.st, h.stream);
+        lbib::launch_areas(h.m, scratch, h.st, h.stream);
         CK(cudaGetLastError());
         const int n = std::min(h.m.nCells, cap);
         if (n > 0) CK(cudaMemcpyAsync(area, scratch, sizeof(double) * n, cudaMemcpyDeviceToHost, h.stream));
-        CK(cudaStreamSynchronize(h.stream));
+        lbib::read_status(h);
+        if (h.stHost->err) {
+            const long long idx = h.stHost->errIndex;
+            lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+            h.msg = "lbib_areas_static: a cell has more membrane nodes than one ring may hold";
+            h.errIndex = idx;
+            return -LBIB_ERR_CAPACITY;
+        }
         for (int c = 0; c < n; ++c) dom[c] = h.ringDomHost[c];
         return h.m.nCells;
     } catch (const HostFail& e) {
         h.err = e.code; h.msg = e.msg;
         return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
     }
 }
 
@@ -2348,6 +2513,8 @@ int lbib_diff_begin(lbib_handle* hh, int T, int K) {
     if (h.cross.nfTab != nullptr)
         lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover boundary solvers on connections");
     if (h.massNode != nullptr) lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover per-node mass sources");
+    if (h.forceModel != lbib::FM_LUO) lbib::fail(LBIB_ERR_STATE, "differentiated runs cover the Luo force model only");
+    if (h.cross.bounceW != nullptr) lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover DiracD2Q5");
     for (int k = 0; k < h.S; ++k)
         if (lbib::coupled_kind(h.sp[k].c.kind))
             lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover the coupled reaction of " + h.sp[k].name);
@@ -2404,9 +2571,10 @@ int lbib_diff_backward(lbib_handle* hh, const double* dLdC, double* gForce, doub
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
     h.lastTotalMs = ms;
-    const size_t nG = 1 + h.S + (size_t)h.S * h.nDomains;
+    const size_t nG = 1 + h.S + (size_t)(h.S + 1) * h.nDomains;
     std::vector<double> grad(nG);
     CK(cudaMemcpy(grad.data(), d.grad, sizeof(double) * nG, cudaMemcpyDeviceToHost));
+    d.gmass.assign(grad.begin() + 1 + h.S + (size_t)h.S * h.nDomains, grad.end());
     if (gTau) {
         gTau[0] = -grad[0] / (d.tauF * d.tauF);
         for (int k = 0; k < h.S; ++k) gTau[1 + k] = -grad[1 + k] / (d.tau[k] * d.tau[k]);
@@ -2419,6 +2587,40 @@ int lbib_diff_backward(lbib_handle* hh, const double* dLdC, double* gForce, doub
         CK(cudaMemcpy(gx.data(), d.gfx, sizeof(double) * M, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(gy.data(), d.gfy, sizeof(double) * M, cudaMemcpyDeviceToHost));
         for (int i = 0; i < M; ++i) { gForce[2 * i] = gx[i]; gForce[2 * i + 1] = gy[i]; }
+    }
+    API_END
+}
+
+int lbib_diff_mass(lbib_handle* hh, const double* mass, double* gMass, int n) {
+    API_BEGIN(hh)
+    if (!h.diff) lbib::fail(LBIB_ERR_STATE, "lbib_diff_mass outside a differentiated run");
+    if (n != h.nDomains) lbib::fail(LBIB_ERR_INPUT, "lbib_diff_mass: n must be the domain count");
+    lbib::DiffCtx& d = *h.diff;
+    if (mass) {
+        CK(cudaMemcpyAsync(d.massTab, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        d.massUsed = true;
+        d.forwardDone = false;
+    }
+    if (gMass)
+        for (int i = 0; i < n; ++i) gMass[i] = d.massUsed && i < (int)d.gmass.size() ? d.gmass[i] : 0.0;
+    API_END
+}
+
+int lbib_diff_fluid_seed(lbib_handle* hh, const double* dLdf) {
+    API_BEGIN(hh)
+    if (!h.diff) lbib::fail(LBIB_ERR_STATE, "lbib_diff_fluid_seed outside a differentiated run");
+    lbib::DiffCtx& d = *h.diff;
+    d.haveSeedF = dLdf != nullptr;
+    if (dLdf) {
+        // lbib_download_lattice's slot layout [L][9] to the device's direction planes
+        static const int INV9[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+        const size_t L = h.L;
+        std::vector<double> nat(9 * L);
+        for (size_t n = 0; n < L; ++n)
+            for (int q = 0; q < 9; ++q) nat[(size_t)q * L + n] = dLdf[n * 9 + INV9[q]];
+        CK(cudaMemcpyAsync(d.seedF, nat.data(), sizeof(double) * 9 * L, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
     }
     API_END
 }
@@ -3080,11 +3282,13 @@ int lbib_upload_membrane(lbib_handle* hh, const unsigned* ids, const double* xy,
         const int o = oldIdx.find(newIds[k]);
         if (o >= 0) {
             hm.ox.push_back(old.ox[o]); hm.oy.push_back(old.oy[o]);
+            hm.bx.push_back(old.bx[o]); hm.by.push_back(old.by[o]);
             hm.vx.push_back(old.vx[o]); hm.vy.push_back(old.vy[o]);
             hm.fx.push_back(old.fx[o]); hm.fy.push_back(old.fy[o]);
         } else {
             lbib::perturbate(h, x, y);
             hm.ox.push_back(x - 5.0); hm.oy.push_back(y - 5.0);
+            hm.bx.push_back(x); hm.by.push_back(y);
             hm.vx.push_back(0.0); hm.vy.push_back(0.0); hm.fx.push_back(0.0); hm.fy.push_back(0.0);
         }
         hm.x.push_back(x);
@@ -3266,27 +3470,42 @@ static uint32_t divide_cell(Handle& h, const HostMembrane& hm, uint32_t dom,
 }
 
 static void run_division(Handle& h) {
-    pull_topology(h);
-    HostMembrane hm;
-    download_membrane(h, hm);
-    sync_targets(h);
     // GeometryHandler::computeAreas, in ring order
     launch_rings(h.m, h.td, h.st, h.stream);
-    launch_areas(h.m, h.area, h.stream);
+    launch_areas(h.m, h.area, nullptr, h.stream);
     std::vector<double> a(h.m.nCells);
     if (h.m.nCells) CK(cudaMemcpyAsync(a.data(), h.area, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
+    h.ringsCurrent = true;
     std::map<uint32_t, double> areas;
     for (int c = 0; c < h.m.nCells; ++c) areas[h.ringDomHost[c]] = a[c];
     areas[0] = 0.0;
+    // LbibCellDivision: a cell's threshold is divisionFactor times its
+    // reference area, the area at the solver's first look at it
+    if (h.divisionFactor > 0.0)
+        for (const auto& kv : areas)
+            if (kv.first != 0 && !h.divisionRef.count(kv.first)) h.divisionRef[kv.first] = kv.second;
+    auto divides = [&](uint32_t dom, double area) {
+        return h.divisionFactor > 0.0 ? area > h.divisionFactor * h.divisionRef[dom] : area > h.divisionMax;
+    };
+    bool any = false;
+    for (auto it = std::next(areas.begin()); it != areas.end(); ++it) any |= divides(it->first, it->second);
+    HostMembrane hm;
+    if (any) {
+        // the host mirror of the membrane, only when a cell divides
+        pull_topology(h);
+        download_membrane(h, hm);
+        sync_targets(h);
+    }
     auto cellsOf = [&]() {
         std::map<uint32_t, std::vector<int>> cells;
         for (size_t c = 0; c < h.conns.size(); ++c) cells[h.conns[c].dom].push_back((int)c);
         return cells;
     };
     for (auto it = std::next(areas.begin()); it != areas.end(); ++it) {
-        if (!(it->second > h.divisionMax)) continue;
+        if (!divides(it->first, it->second)) continue;
         const uint32_t newId = divide_cell(h, hm, it->first, cellsOf());
+        if (h.divisionFactor > 0.0) h.divisionRef[newId] = h.divisionRef[it->first];
         grow_domains(h, (int)newId + 1);
         h.ctypeHost[newId] = it->first < h.ctypeHost.size() ? h.ctypeHost[it->first] : 1u;
         // the daughter's nodes keep the mass source the step's area regulator

@@ -166,6 +166,7 @@ struct SpeciesConst {
     int reinit;     // Reinit
     double dt;      // the solver's deltaT (SchnakenbergD2Q5u/v: 20 / Iterations; BMP: 1)
     double hill;    // RX_BMP: pow(k_hill, n_hill) as the host's pow gives it
+    int bounce;     // DiracD2Q5: advect keeps the populations of links with a boundary node
 };
 
 // Boundary solvers on connections (the "bsolver cdesolver" pairs of a
@@ -204,6 +205,7 @@ struct LatticeArgs {
     const double* srcTab;      // [S][nDomains] production per step
     const uint32_t* ctypeTab;  // per-domain cell type (read by RX_BMP)
     double tauF;
+    int forceModel;            // FM_LUO, FM_GUO (as the reference writes it), FM_GUO_CORRECTED
     SpeciesConst sp[kMaxSpecies];
     int coupled;               // some species has a coupled_kind reaction
     const Status* status;
@@ -216,8 +218,20 @@ struct LatticeArgs {
     const int* nfN;            // number of nfKeys
     int nfCap;
     double* nfD;               // 2 per key: preAdvect's value of each solver
+    // links with a boundary node, for species whose advect keeps their
+    // populations (DiracD2Q5): per node, a boundary node in the W / S slot
+    // (nullptr: no such species)
+    const uint8_t* bounceW;
+    const uint8_t* bounceS;
 };
 
 constexpr int kTile = 16;  // force tiles are 16x16 lattice nodes
+
+// Force models of FluidSolver (its base class, FluidSolver.hpp:41):
+// Luo1993ForceModel (compiled in by the reference), GuoZhengShi2002ForceModel
+// as the reference writes it (NE term with -3 u_y, GuoZhengShi2002ForceModel.cpp:51)
+// and with the coefficient of the model's expansion (+6 u_y).
+enum ForceModel { FM_LUO = 0, FM_GUO = 1, FM_GUO_CORRECTED = 2 };
+__host__ __device__ __forceinline__ double guo_ne_y(int forceModel) { return forceModel == FM_GUO ? -3.0 : 6.0; }
 
 }  // namespace lbib

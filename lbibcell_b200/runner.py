@@ -129,6 +129,11 @@ class Simulation:
         args = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (f, g, force)]
         self._check(self._L.lbib_upload_lattice(self._h, *[_p(a) for a in args]))
 
+    def init_velocity(self, ux: float, uy: float) -> None:
+        """SimulationRunner::initSolvers(Field<double>): the lattice at the
+        equilibrium of the uniform velocity (ux, uy)."""
+        self._check(self._L.lbib_init_velocity(self._h, float(ux), float(uy)))
+
     def membrane(self):
         """(ids[M], state[M, 6]) with state = x, y, vx, vy, fx, fy, in id order."""
         M = self.sizes()["M"]
@@ -281,6 +286,21 @@ class Simulation:
         gF = np.zeros((M, 2)); gT = np.zeros(1 + S); gR = np.zeros((S, self.domain_count()))
         self._check(self._L.lbib_diff_backward(self._h, _p(seed), _p(gF), _p(gT), _p(gR)))
         return {"force": gF, "tau": gT, "rates": gR}
+
+    def diff_mass(self, mass=None) -> np.ndarray:
+        """Sets the run's per-domain mass source (when given) and returns dL/d
+        mass of the last backward pass."""
+        n = self.domain_count()
+        m = None if mass is None else np.ascontiguousarray(mass, np.float64)
+        g = np.zeros(n)
+        self._check(self._L.lbib_diff_mass(self._h, _p(m), _p(g), n))
+        return g
+
+    def diff_fluid_seed(self, dLdf=None) -> None:
+        """dL/d of the final fluid distributions ((L, 9), lattice() layout) for
+        the next backward passes; None removes it."""
+        a = None if dLdf is None else np.ascontiguousarray(dLdf, np.float64)
+        self._check(self._L.lbib_diff_fluid_seed(self._h, _p(a)))
 
     def diff_end(self) -> None:
         """Restore the snapshot and free the run's checkpoints."""

@@ -175,6 +175,10 @@ struct Sim {
 
     // Solvers
     bool outlet = false;
+    // FluidSolver's force model (its base class, FluidSolver.hpp:41): 0 Luo 1993,
+    // 1 Guo, Zheng & Shi 2002 as GuoZhengShi2002ForceModel.cpp writes it,
+    // 2 the same with the NE coefficient of the model's expansion (+6 u_y, :51)
+    int forceModel = 0;
     std::vector<int> bioOrder;      // 1 tension, 2 area regulator, in registration order
     TensionSpec tension;
     AreaSpec area;
@@ -251,6 +255,11 @@ static void loadPlugins(Sim& s, const std::string& fn) {
         if (kind == "MassSolver") {
             if (name == "MassSolverBoxOutlet") s.outlet = true;
             else fail(ERR_INPUT, "unknown mass solver " + name);
+        } else if (kind == "ForceModel") {
+            if (name == "Luo1993ForceModel") s.forceModel = 0;
+            else if (name == "GuoZhengShi2002ForceModel") s.forceModel = 1;
+            else if (name == "GuoZhengShi2002ForceModelCorrected") s.forceModel = 2;
+            else fail(ERR_INPUT, "unknown force model " + name);
         } else if (kind == "BioSolver") {
             std::string k; double v;
             while (ls >> k >> v) kv[k] = v;
@@ -400,14 +409,63 @@ static inline void computeVelocity(double rho, const double* fi, double& uxo, do
     uyo = (fi[NE] + fi[N] + fi[NW] - (fi[SW] + fi[S] + fi[SE])) * rhoI;
 }
 
-// FluidSolver::collide — FluidSolver.cpp:103-183, with the Luo force
-// contribution (Luo1993ForceModel.cpp:29-49) and localSwap (:259-264).
+// GuoZhengShi2002ForceModel::computeVelocity — GuoZhengShi2002ForceModel.cpp:60-78
+static inline void computeVelocityGuo(double rho, const double* fi, double fx, double fy, double& uxo, double& uyo) {
+    const double rhoI = 1.0 / rho;
+    uxo = (fi[E] + fi[NE] + fi[SE] - (fi[NW] + fi[W] + fi[SW]) + 0.5 * fx) * rhoI;
+    uyo = (fi[NE] + fi[N] + fi[NW] - (fi[SW] + fi[S] + fi[SE]) + 0.5 * fy) * rhoI;
+}
+
+// The force contribution of FluidSolver::collide (FluidSolver.cpp:140-145):
+// Luo1993ForceModel::computeForce (Luo1993ForceModel.cpp:29-49) from getRho()
+// without rhoToAdd, or GuoZhengShi2002ForceModel::computeForce
+// (GuoZhengShi2002ForceModel.cpp:29-58) from tau and the stored velocity
+// getVelocity() (velocity_ of the previous collide).
+static void forceContribution(const Sim& s, size_t n, const double* fi, double* fc) {
+    const double fx = s.frx[n], fy = s.fry[n];
+    if (s.forceModel == 0) {
+        const double rhoF = sumSlots9(fi);
+        const double W1rho3 = rhoF * 3.0 / 9.0;
+        const double W2rho3 = rhoF * 3.0 / 36.0;
+        fc[T] = 0.0;
+        fc[E] = W1rho3 * fx;
+        fc[N] = W1rho3 * fy;
+        fc[W] = -W1rho3 * fx;
+        fc[S] = -W1rho3 * fy;
+        fc[NE] = W2rho3 * (fx + fy);
+        fc[NW] = W2rho3 * (-fx + fy);
+        fc[SW] = W2rho3 * (-fx - fy);
+        fc[SE] = W2rho3 * (fx - fy);
+        return;
+    }
+    const double vx = s.ux[n], vy = s.uy[n];
+    const double tau = s.tauF;
+    const double G0 = (1.0 - 0.5 / tau) * 4.0 / 9.0;
+    const double G1 = (1.0 - 0.5 / tau) / 9.0;
+    const double G2 = (1.0 - 0.5 / tau) / 36.0;
+    // the NE term's F_y factor: 9 v_x - 3 v_y + 3 as written at :51; 9 v_x + 6 v_y + 3 corrected
+    const double neY = s.forceModel == 1 ? -3.0 : 6.0;
+    fc[T] = G0 * (-3.0 * vx * fx - 3.0 * vy * fy);
+    fc[E] = G1 * ((6.0 * vx + 3.0) * fx - 3.0 * vy * fy);
+    fc[N] = G1 * (-3.0 * vx * fx + (6.0 * vy + 3.0) * fy);
+    fc[W] = G1 * ((6.0 * vx - 3.0) * fx - 3.0 * vy * fy);
+    fc[S] = G1 * (-3.0 * vx * fx + (6.0 * vy - 3.0) * fy);
+    fc[NE] = G2 * ((6.0 * vx + 9.0 * vy + 3.0) * fx + (9.0 * vx + neY * vy + 3.0) * fy);
+    fc[NW] = G2 * ((6.0 * vx - 9.0 * vy - 3.0) * fx + (-9.0 * vx + 6.0 * vy + 3.0) * fy);
+    fc[SW] = G2 * ((6.0 * vx + 9.0 * vy - 3.0) * fx + (9.0 * vx + 6.0 * vy - 3.0) * fy);
+    fc[SE] = G2 * ((6.0 * vx - 9.0 * vy + 3.0) * fx + (-9.0 * vx + 6.0 * vy - 3.0) * fy);
+}
+
+// FluidSolver::collide — FluidSolver.cpp:103-183, with the force model's
+// velocity and force contribution, and localSwap (:259-264).
 static void fluidCollide(Sim& s, size_t n) {
     double* fi = &s.f[n * 9];
     double rho = sumSlots9(fi);
     if (std::isfinite(s.rhoToAdd[n])) rho += s.rhoToAdd[n];
+    const double fx = s.frx[n], fy = s.fry[n];
     double ux, uy;
-    computeVelocity(rho, fi, ux, uy);
+    if (s.forceModel == 0) computeVelocity(rho, fi, ux, uy);
+    else computeVelocityGuo(rho, fi, fx, fy, ux, uy);
     const double ux2 = ux * ux;
     const double uy2 = uy * uy;
     const double lastTerm = 3.0 / 2.0 * (ux2 + uy2);
@@ -415,21 +473,8 @@ static void fluidCollide(Sim& s, size_t n) {
     const double W3 = 9.0 / 2.0;
     const double W1rho = W1 * rho;
     const double W2rho = W2 * rho;
-    // forcecontribution uses getRho() without rhoToAdd (FluidSolver.cpp:141-145)
-    const double rhoF = sumSlots9(fi);
-    const double fx = s.frx[n], fy = s.fry[n];
-    const double W1rho3 = rhoF * 3.0 / 9.0;
-    const double W2rho3 = rhoF * 3.0 / 36.0;
     double fc[9];
-    fc[T] = 0.0;
-    fc[E] = W1rho3 * fx;
-    fc[N] = W1rho3 * fy;
-    fc[W] = -W1rho3 * fx;
-    fc[S] = -W1rho3 * fy;
-    fc[NE] = W2rho3 * (fx + fy);
-    fc[NW] = W2rho3 * (-fx + fy);
-    fc[SW] = W2rho3 * (-fx - fy);
-    fc[SE] = W2rho3 * (fx - fy);
+    forceContribution(s, n, fi, fc);
     double temp[9];
     temp[T] = W0 * rho * (1.0 - lastTerm) * tauI + fc[T];
     temp[E] = W1rho * (1.0 + 3.0 * ux + W3 * ux2 - lastTerm) * tauI + fc[E];
@@ -444,7 +489,8 @@ static void fluidCollide(Sim& s, size_t n) {
         const double tempD = fi[d];
         fi[d] = tempD - tempD * tauI + temp[d];
     }
-    computeVelocity(rho, fi, ux, uy);
+    if (s.forceModel == 0) computeVelocity(rho, fi, ux, uy);
+    else computeVelocityGuo(rho, fi, fx, fy, ux, uy);
     s.ux[n] = ux; s.uy[n] = uy;
     s.rhoToAdd[n] = 0.0;
     std::swap(fi[E], fi[W]); std::swap(fi[NE], fi[SW]);

@@ -18,14 +18,27 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
 REF_DRIVER_FAST = os.path.join(HERE, "_ref", "ref_driver_fast")
+# the reference built with GuoZhengShi2002ForceModel as FluidSolver's base class
+REF_DRIVER_GUO = os.path.join(HERE, "_ref", "ref_driver_guo")
+# apps/tutorial_01.cpp and tutorial_02.cpp of the reference, unmodified, built
+# against lbibcell_b200's drop-in libLbmLib
+REF_APPS = os.path.join(HERE, "_ref", "apps")
+# Root of the reference's source tree (read only by the build recipe and by
+# tests that use its files where they are present): one environment variable.
+REFERENCE = os.environ.get("LBIB_REFERENCE", "/root/reference")
+
+
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE, "libs"))
 
 _lib = None
 
 
 def build(ref: bool = False) -> None:
-    """Compile the oracle (and, with ``ref``, the reference build) via oracle/Makefile."""
-    targets = ["oracle"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+    """Compile the oracle (and, with ``ref``, the reference build and the
+    reference's applications against the drop-in library) via oracle/Makefile."""
+    targets = ["oracle"] + (["ref", "apps"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", "REF=" + REFERENCE] + targets, check=True)
 
 
 def lib() -> ctypes.CDLL:

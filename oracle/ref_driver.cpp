@@ -117,6 +117,9 @@ PluginList loadPlugins(const std::string& fn) {
                     if (k == "radius") reg.junction.radius = v;
                     if (k == "k") reg.junction.k = v;
                     if (k == "l0") reg.junction.l0 = v;
+                } else if (name == "LbibCellDivision") {
+                    if (k == "factor") reg.division.factor = v;
+                    if (k == "frequency") reg.division.frequency = (unsigned)v;
                 }
             }
         } else if (kind == "CDE") {
@@ -255,6 +258,8 @@ int main(int argc, char** argv) {
     unsigned warm = 0, steps = 0;
     std::string restartFile, writePrefix, editFile;
     unsigned editIter = 0, runIters = 0;
+    bool withVelocity = false;
+    double velX = 0.0, velY = 0.0;
     std::vector<std::pair<unsigned, unsigned>> cellTypes;
     for (int a = 6; a < argc; ++a) {
         const std::string k = argv[a];
@@ -271,6 +276,11 @@ int main(int argc, char** argv) {
             runIters = (unsigned)std::stoul(argv[++a]);
         } else if (k == "celltype" && a + 2 < argc) {
             cellTypes.emplace_back((unsigned)std::stoul(argv[a + 1]), (unsigned)std::stoul(argv[a + 2]));
+            a += 2;
+        } else if (k == "velocity" && a + 2 < argc) {
+            withVelocity = true;
+            velX = std::stod(argv[a + 1]);
+            velY = std::stod(argv[a + 2]);
             a += 2;
         } else if (k == "edit" && a + 2 < argc) {
             editIter = (unsigned)std::stoul(argv[a + 1]);
@@ -294,6 +304,8 @@ int main(int argc, char** argv) {
             reporter.registerReporter(std::unique_ptr<LbmLib::reportHandler::AbstractReportFunctor>(
                 new DumpReporter(geohandler, argv[5])));
         simRunner.initSolvers();
+        // SimulationRunner::initSolvers(Field<double>): the lattice again, at a uniform velocity
+        if (withVelocity) simRunner.initSolvers(LbmLib::Field<double>(velX, velY));
         if (!restartFile.empty()) simRunner.initSolvers(restartFile);
         if (!cellTypes.empty()) {
             for (const auto& ct : cellTypes) geohandler.getCellTypeTrackerMap()[ct.first] = ct.second;

@@ -17,6 +17,12 @@
 //                         id order a type-7 spring each way to the closest node
 //                         of another cell within `radius`) with radius, spring
 //                         constant k and rest length l0 from the plugin file.
+//   LbibCellDivision      every `frequency` iterations, a cell whose area
+//                         exceeds `factor` times its reference area (its area
+//                         when this solver first saw it; a daughter inherits
+//                         its mother's) splits across the perpendicular
+//                         bisector of its longest axis, as tutorial_01's
+//                         division does; then the lattice is cured.
 //   LbibCDESolverD2Q5_A/B/C  D2Q5 species with R = source[domain] - decay*C,
 //                         added as dt*R/3 (rest) and dt*R/6 (moving) like
 //                         tutorial_01_CDESolverD2Q5_SIGNAL.cpp:102-135.
@@ -33,6 +39,8 @@
 #include <LbmLib/include/geometry/Connection.hpp>
 
 #include <array>
+#include <cmath>
+#include <iterator>
 #include <map>
 #include <numeric>
 #include <sstream>
@@ -132,6 +140,96 @@ class LbibCellJunction : public BioBaseSolver<LbibCellJunction> {
     static const std::string name;
 };
 const std::string LbibCellJunction::name = "LbibCellJunction";
+
+// ---------------------------------------------------------------------------
+class LbibCellDivision : public BioBaseSolver<LbibCellDivision> {
+ public:
+    LbibCellDivision();
+    virtual void applyBioProcess(geometry::GeometryHandler& gh, solver::ForceSolver&) {
+        const auto& p = lbibref::registry().division;
+        if (Parameters.getCurrentIteration() % p.frequency != 0) return;
+        auto& types = gh.getCellTypeTrackerMap();
+        if (types.empty()) {
+            types[0] = 0;
+            for (const auto& kv : cellsOf(gh)) types[kv.first] = 1;
+        }
+        std::map<unsigned int, double> areas = gh.computeAreas();
+        areas[0] = 0.0;
+        for (const auto& a : areas)
+            if (a.first != 0 && refArea_.find(a.first) == refArea_.end()) refArea_[a.first] = a.second;
+        for (auto it = std::next(areas.begin()); it != areas.end(); ++it) {
+            if (!(it->second > p.factor * refArea_[it->first])) continue;
+            const unsigned int born = divide(gh, it->first);
+            refArea_[born] = refArea_[it->first];
+            types[born] = types[it->first];
+            gh.cureLattice();
+        }
+        gh.copyCellTypeToPhysicalNodes(types);
+    }
+    static const std::string name;
+
+ private:
+    typedef std::shared_ptr<geometry::Connection> ConnPtr;
+
+    // the connections of each cell, in the geometry's connection order
+    static std::map<unsigned int, std::vector<ConnPtr>> cellsOf(geometry::GeometryHandler& gh) {
+        std::map<unsigned int, std::vector<ConnPtr>> cells;
+        for (const auto& c : gh.getGeometry().getConnections()) cells[c->getDomainIdentifier()].push_back(c);
+        return cells;
+    }
+
+    // Splits cell `dom`; returns the new cell's domain id (one above the largest).
+    static unsigned int divide(geometry::GeometryHandler& gh, unsigned int dom) {
+        auto cells = cellsOf(gh);
+        const unsigned int born = cells.rbegin()->first + 1;
+        const std::vector<ConnPtr>& cell = cells[dom];
+        // the two first nodes furthest apart (the first pair found of the largest distance)
+        double far = 0.0;
+        std::shared_ptr<nodes::GeometryNode> a, b;
+        for (const auto& c1 : cell)
+            for (const auto& c2 : cell) {
+                const auto& p = c1->getGeometryNodes().first;
+                const auto& q = c2->getGeometryNodes().first;
+                const double dx = p->getXPos() - q->getXPos(), dy = p->getYPos() - q->getYPos();
+                const double d = std::sqrt(dx * dx + dy * dy);
+                if (d > far) { far = d; a = p; b = q; }
+            }
+        // the perpendicular bisector y = slope x + icpt, and the two connections it cuts
+        const double mx = 0.5 * (a->getXPos() + b->getXPos()), my = 0.5 * (a->getYPos() + b->getYPos());
+        const double slope = -(b->getXPos() - a->getXPos()) / (b->getYPos() - a->getYPos());
+        const double icpt = my - slope * mx;
+        std::vector<ConnPtr> cut;
+        for (const auto& c : cell) {
+            const auto& p = c->getGeometryNodes().first;
+            const auto& q = c->getGeometryNodes().second;
+            const bool above = p->getYPos() > slope * p->getXPos() + icpt;
+            const bool below = q->getYPos() < slope * q->getXPos() + icpt;
+            if (above == below) cut.push_back(c);
+        }
+        if (cut.size() != 2) lbm_fail("LbibCellDivision: the bisector does not cut exactly two connections");
+        const auto desc = cut[0]->getBoundaryConditionDescriptor();
+        if (desc != cut[1]->getBoundaryConditionDescriptor())
+            lbm_fail("LbibCellDivision: the two cut connections carry different boundary solvers");
+        cut[0]->getGeometryNodes().first->setConnection<1>(nullptr);
+        cut[0]->getGeometryNodes().second->setConnection<0>(nullptr);
+        cut[1]->getGeometryNodes().first->setConnection<1>(nullptr);
+        cut[1]->getGeometryNodes().second->setConnection<0>(nullptr);
+        gh.createConnection(cut[0]->getGeometryNodes().first, cut[1]->getGeometryNodes().second, desc, dom);
+        gh.createConnection(cut[1]->getGeometryNodes().first, cut[0]->getGeometryNodes().second, desc, dom);
+        for (const auto& c : cut) gh.eraseConnection(c);
+        // the ring through the second cut's end node becomes the new cell
+        const ConnPtr start = cut[1]->getGeometryNodes().second->getConnection<1>();
+        ConnPtr c = start;
+        do {
+            c->setDomainIdentifier(born);
+            c = c->getGeometryNodes().second->getConnection<1>();
+        } while (c != start);
+        return born;
+    }
+
+    std::map<unsigned int, double> refArea_;
+};
+const std::string LbibCellDivision::name = "LbibCellDivision";
 
 // ---------------------------------------------------------------------------
 template <class Self>
@@ -286,6 +384,7 @@ LbibCDESolverD2Q5_C::LbibCDESolverD2Q5_C() {}
 LbibMembraneTension::LbibMembraneTension() : BioBaseSolver() {}
 LbibAreaRegulator::LbibAreaRegulator() : BioBaseSolver() {}
 LbibCellJunction::LbibCellJunction() : BioBaseSolver() {}
+LbibCellDivision::LbibCellDivision() : BioBaseSolver() {}
 
 }  // namespace solver
 }  // namespace LbmLib

@@ -5,8 +5,13 @@ oracle/Makefile, parity flags, OMP_NUM_THREADS=1) and stores:
 
 * ``toy48.npz`` -- full state arrays of a 48x48 single-cell run at t = 0, 30, 60
   (1 species; remeshing happens at step 1).
+* ``guo48.npz`` -- the toy48 run with the reference compiled with
+  GuoZhengShi2002ForceModel as FluidSolver's base class (ref_driver_guo).
 * ``config1_digest.json`` -- SHA-256 digests of every state array of the 200x200
   single-cell configuration at t = 0, 500, 1000, 1500, 2000.
+* ``tissue4096_digest.json`` -- the same for the 4096x4096 tissue of 6000
+  cells (3 species, tension, junctions, growth, division at 2x area) at
+  t = 0, 10, 20.
 * ``tissue1024_digest.json`` -- the same for the 1024x1024 tissue of 400 cells
   (2 species, tension, area regulator, cell junctions) at t = 0, 70, 80.  The
   reference's species re-initialisation divides 0 by 0 for nodes trapped
@@ -51,6 +56,16 @@ def tissue1024() -> configs.Config:
     return configs.config2(iterations=80, report_step=10)
 
 
+def guo48() -> configs.Config:
+    cfg = toy48()
+    cfg.force_model = "GuoZhengShi2002ForceModel"
+    return cfg
+
+
+def tissue4096() -> configs.Config:
+    return configs.config3(iterations=20, report_step=10)
+
+
 def _digests(ref, times):
     dig = {}
     for t in times:
@@ -63,6 +78,12 @@ def _digests(ref, times):
 
 
 def main(cases) -> None:
+    if "tissue4096" in cases:
+        with tempfile.TemporaryDirectory() as tmp:
+            paths = tissue4096().write(os.path.join(tmp, "t4096"))
+            ref = O.run_reference(paths, os.path.join(tmp, "t4096", "ref"), timeout=6 * 3600)
+            with open(os.path.join(HERE, "tissue4096_digest.json"), "w") as f:
+                json.dump(_digests(ref, (0, 10, 20)), f, indent=1, sort_keys=True)
     if "tissue1024" in cases:
         with tempfile.TemporaryDirectory() as tmp:
             paths = tissue1024().write(os.path.join(tmp, "t1024"))
@@ -82,6 +103,19 @@ def main(cases) -> None:
                 out[f"iter_{t}"] = np.array(st.current_iteration)
             np.savez_compressed(os.path.join(HERE, "toy48.npz"), **out)
 
+    if "guo48" in cases:
+        # the reference built with the Guo force model (oracle/Makefile, ref_driver_guo)
+        with tempfile.TemporaryDirectory() as tmp:
+            paths = guo48().write(os.path.join(tmp, "guo"))
+            ref = O.run_reference(paths, os.path.join(tmp, "guo", "ref"), driver=O.REF_DRIVER_GUO)
+            out = {}
+            for t in (0, 30, 60):
+                st = ref[t]
+                for k in FIELDS:
+                    out[f"{k}_{t}"] = getattr(st, k)
+                out[f"iter_{t}"] = np.array(st.current_iteration)
+            np.savez_compressed(os.path.join(HERE, "guo48.npz"), **out)
+
     if "config1" in cases:
         with tempfile.TemporaryDirectory() as tmp:
             paths = configs.config1().write(os.path.join(tmp, "c1"))
@@ -94,4 +128,4 @@ def main(cases) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["toy48", "config1", "tissue1024"])
+    main(sys.argv[1:] or ["toy48", "guo48", "config1", "tissue1024", "tissue4096"])

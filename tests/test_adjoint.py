@@ -259,3 +259,140 @@ def test_adjoint_row_blocks(lbib, tmp_path, nx):
     fd = (P.loss(F=P.F + h * v) - P.loss(F=P.F - h * v)) / (2 * h)
     _close(float((g["force"] * v).sum()), fd, np.abs(g["force"] * v).sum(), "dL/dF . v")
     P.sim.diff_end()
+
+
+def test_config4_adjoint_vs_central_differences(lbib, tmp_path):
+    """The adjoint workload as specified: 512x512, 50 cells, one species
+    (tau 0.8), T = 2000 with a checkpoint every 100 steps; loss
+    L = sum_x (C(T) - c_target)^2 with c_target from a forward run whose 50
+    per-cell source rates are perturbed by N(0, 0.1) relative; central
+    differences of the FP64 forward with step h = 1e-6.  Every gradient entry
+    of magnitude >= 1e-3 of the largest entry of its kind must match to 1e-4
+    relative, with no floor; smaller entries to 1e-4 of that magnitude."""
+    cfg = configs.config4()
+    paths = cfg.write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    sim.step(3)
+    nD = sim.domain_count()
+    T, K, h = 2000, 100, 1e-6
+    rates = np.zeros((1, nD))
+    for d, r in cfg.species[0].source.items():
+        rates[0, d] = r
+    tau = np.array([cfg.tau_fluid, cfg.species[0].tau])
+    # the membrane forces of the last force evaluation (the run's default)
+    forces = np.ascontiguousarray(sim.membrane()[1][:, 4:6])
+    sim.diff_begin(T, K)
+    target_rates = rates * (1.0 + np.random.default_rng(4).normal(0.0, 0.1, rates.shape))
+    sim.diff_forward(forces, tau, target_rates)
+    c_target = sim.concentrations().copy()
+
+    def loss(F=None, tau_=None, rates_=None):
+        # every parameter passed: a call's parameters stay in effect for the next
+        sim.diff_forward(forces if F is None else F, tau if tau_ is None else tau_,
+                         rates if rates_ is None else rates_)
+        C = sim.concentrations()
+        return float(((C - c_target) ** 2).sum()), C
+
+    L0, C0 = loss()
+    g = sim.diff_backward(2.0 * (C0 - c_target))
+
+    def check(adj, fd, mag, what):
+        if abs(fd) >= mag:
+            assert abs(adj - fd) <= RTOL * abs(fd), f"{what}: adjoint {adj:.10e} vs central difference {fd:.10e}"
+        else:
+            assert abs(adj - fd) <= RTOL * mag, f"{what}: adjoint {adj:.10e} vs central difference {fd:.10e}"
+
+    # all 50 per-cell source rates (domains 1..50)
+    magR = 1e-3 * np.abs(g["rates"][0, 1:]).max()
+    assert magR > 0
+    for d in range(1, nD):
+        rp, rm = rates.copy(), rates.copy()
+        rp[0, d] += h
+        rm[0, d] -= h
+        fd = (loss(rates_=rp)[0] - loss(rates_=rm)[0]) / (2 * h)
+        check(g["rates"][0, d], fd, magR, f"dL/drate[{d}]")
+    # the species' and the fluid's relaxation times
+    for i in range(2):
+        tp, tm = tau.copy(), tau.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (loss(tau_=tp)[0] - loss(tau_=tm)[0]) / (2 * h)
+        check(g["tau"][i], fd, 1e-3 * np.abs(g["tau"]).max(), f"dL/dtau[{i}]")
+    # membrane node forces (the tension of the last force evaluation): the
+    # largest entries and a random direction in force space
+    magF = 1e-3 * np.abs(g["force"]).max()
+    assert magF > 0
+    order = np.argsort(-np.abs(g["force"]).ravel())[:4]
+    for flat in order:
+        i, c = divmod(int(flat), 2)
+        Fp, Fm = forces.copy(), forces.copy()
+        Fp[i, c] += h
+        Fm[i, c] -= h
+        fd = (loss(F=Fp)[0] - loss(F=Fm)[0]) / (2 * h)
+        check(g["force"][i, c], fd, magF, f"dL/dF[{i},{c}]")
+    v = np.random.default_rng(9).normal(size=forces.shape)
+    fd = (loss(F=forces + h * v)[0] - loss(F=forces - h * v)[0]) / (2 * h)
+    check(float((g["force"] * v).sum()), fd, 0.0, "dL/dF . v")
+    sim.diff_end()
+
+
+# lattice() slot d holds the population of direction INV9[d] (after localSwap)
+_INV9 = np.array([0, 3, 4, 1, 2, 7, 8, 5, 6])
+_CX = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1])[_INV9]
+_CY = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1])[_INV9]
+
+
+def _kinetic(f, window):
+    """Kinetic energy 1/2 |j|^2 / rho of the stored distributions over the
+    nodes in `window`, and its gradient with respect to f (lattice() layout)."""
+    rho = f.sum(1)
+    jx, jy = f @ _CX, f @ _CY
+    e = 0.5 * (jx * jx + jy * jy) / rho
+    grad = (np.outer(jx, _CX) + np.outer(jy, _CY)) / rho[:, None] - (e / rho)[:, None]
+    return float(e[window].sum()), grad * window[:, None]
+
+
+def test_mass_source_and_flow_loss_gradients(lbib, tmp_path):
+    """The per-domain mass source (rhoToAdd, lbib_diff_mass) and a loss of the
+    flow (the kinetic energy in a central window, seeded through
+    lbib_diff_fluid_seed) plus a concentration term: the adjoint against
+    central differences of the FP64 forward, 1e-4 relative."""
+    paths = _cfg(n=64).write(str(tmp_path))
+    P = _Problem(lbib, paths, T=24, K=5, steps_before=3)
+    n = 64
+    yy, xx = np.divmod(np.arange(n * n), n)
+    window = (abs(xx - 32) < 12) & (abs(yy - 32) < 12)
+    mass = np.zeros(P.nD)
+    mass[1] = 2e-3
+    P.sim.diff_mass(mass)
+
+    def loss(F=None, tau=None, rates=None, m=None):
+        P.sim.diff_mass(mass if m is None else m)
+        P.sim.diff_forward(P.F if F is None else F, P.tau if tau is None else tau,
+                           P.rates if rates is None else rates)
+        lat = P.sim.lattice()
+        ke, dke = _kinetic(lat.f, window)
+        return ke + float((P.sim.concentrations() * P.w).sum()), dke
+
+    L0, dke = loss()
+    P.sim.diff_fluid_seed(dke)
+    g = P.sim.diff_backward(P.w)
+    gm = P.sim.diff_mass()
+    h = 1e-6
+    for d in (0, 1):
+        mp, mm = mass.copy(), mass.copy()
+        mp[d] += h
+        mm[d] -= h
+        fd = (loss(m=mp)[0] - loss(m=mm)[0]) / (2 * h)
+        _close(gm[d], fd, np.abs(gm).max(), f"dL/dmass[{d}]")
+    for i in range(1 + P.S):
+        tp, tm = P.tau.copy(), P.tau.copy()
+        tp[i] += 1e-5
+        tm[i] -= 1e-5
+        fd = (loss(tau=tp)[0] - loss(tau=tm)[0]) / 2e-5
+        _close(g["tau"][i], fd, np.abs(g["tau"]).max(), f"dL/dtau[{i}]")
+    v = np.random.default_rng(3).normal(size=P.F.shape)
+    fd = (loss(F=P.F + 1e-5 * v)[0] - loss(F=P.F - 1e-5 * v)[0]) / 2e-5
+    _close(float((g["force"] * v).sum()), fd, np.abs(g["force"] * v).sum(), "dL/dF . v")
+    P.sim.diff_fluid_seed(None)
+    P.sim.diff_end()

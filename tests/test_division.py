@@ -69,3 +69,45 @@ def test_division_must_be_last(lbib, tmp_path):
     with pytest.raises(lbib.LbibError) as e:
         lbib.Simulation(cfg.write(str(tmp_path)), lbib.FP64)
     assert e.value.code == 90
+
+
+def _grow_cfg(iterations=50):
+    """Two growing cells (area regulator toward 1.5x) and LbibCellDivision with
+    threshold 1.01x the reference area, checked every 10 iterations: the
+    membrane tension first shrinks the cells, then both grow past the
+    threshold and divide in one check, one after the other; the daughters
+    (reference area inherited from their mothers) do not divide again."""
+    cells = [(1, configs.circle(30.0, 40.0, 12.0, 120, phase=0.1)),
+             (2, configs.circle(62.0, 40.0, 11.0, 110, phase=0.2))]
+    return configs.Config(name="grow2", nx=96, ny=80, tau_fluid=1.0, iterations=iterations, report_step=10,
+                          cells=cells, species=[configs.Species(configs.SPECIES_NAMES[0], 0.8, source={1: 1e-3})],
+                          area=(1.5, 0.01, 0.004), bio=["LbibCellDivision\tfactor\t1.01\tfrequency\t10"])
+
+
+def test_lbib_division_per_cell_threshold_matches_reference(lbib, oracle_mod, tmp_path):
+    if not os.path.exists(oracle_mod.REF_DRIVER):
+        pytest.skip("reference build not available")
+    paths = _grow_cfg().write(str(tmp_path / "cfg"))
+    dumps = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    done = 0
+    for t in (10, 20, 30, 40, 50):
+        sim.step(t - done)
+        done = t
+        ref = dumps[t]
+        lat = sim.lattice()
+        for field in ("f", "g", "vel", "force", "dom", "ctype"):
+            a, b = getattr(lat, field), getattr(ref, field)
+            assert np.array_equal(a, b), f"t={t} {field}: max |diff| {np.abs(a.astype(float) - b.astype(float)).max()}"
+        ids, node = sim.membrane()
+        assert np.array_equal(ids, ref.ids) and np.array_equal(node, ref.node), f"t={t}: membrane differs"
+        assert np.array_equal(sim.connections(), ref.conn), f"t={t}: connections differ"
+    assert set(np.unique(sim.lattice().dom).tolist()) == {0, 1, 2, 3, 4}
+
+
+def test_lbib_division_refusals(lbib, tmp_path):
+    cfg = _grow_cfg()
+    cfg.bio = ["LbibCellDivision\tfactor\t0\tfrequency\t10"]
+    with pytest.raises(lbib.LbibError) as e:
+        lbib.Simulation(cfg.write(str(tmp_path)), lbib.FP64)
+    assert e.value.code == 90

@@ -87,6 +87,39 @@ def test_toy48_full_steps_fp64(lbib, oracle_mod, tmp_path):
         _compare_state(sim, o.state())
 
 
+def _centred_circle(tmp_path):
+    # 120 nodes of a circle centred on lattice node (32, 32): the bottom node
+    # is at x = 32 - 4e-15, so x + 2 rounds to 34 and the reference binds a
+    # 5-column stencil (GeometryHandler.cpp:637-643; the fifth column
+    # overwrites the first's slots), which it keeps while the node stays in
+    # its unit cell (GeometryNode::isUpdateNeeded, GeometryNode.cpp:256-261)
+    cfg = configs.toy(n=64, r=12.0, nodes=120, iterations=60, report_step=20, species=1)
+    cfg.cells = [(1, configs.circle(32.0, 32.0, 12.0, 120))]
+    x = cfg.cells[0][1][90][0]
+    assert x < 32.0 and x + 2.0 == 34.0
+    return cfg.write(str(tmp_path))
+
+
+def test_stencil_binding_kept_in_unit_cell_fp64(lbib, oracle_mod, tmp_path):
+    """The persistent stencil binding: identical to the oracle (whose
+    per-node slot table follows the reference's rebinding rule) after each
+    step of the first 20, and to the reference build at t = 20, 40, 60."""
+    paths = _centred_circle(tmp_path / "cfg")
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    for _ in range(20):
+        sim.step(1)
+        o.step(1)
+        _compare_state(sim, o.state())
+    if os.path.exists(oracle_mod.REF_DRIVER):
+        dumps = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
+        done = 20
+        for t in (20, 40, 60):
+            sim.step(t - done)
+            done = t
+            _compare_state(sim, dumps[t])
+
+
 def test_toy_two_species_fp64(lbib, oracle_mod, tmp_path):
     paths = configs.toy(n=64, r=12.0, nodes=120, iterations=200, species=2).write(str(tmp_path))
     sim = lbib.Simulation(paths, lbib.FP64)
@@ -185,3 +218,39 @@ def test_hex25_tissue_fp64(lbib, oracle_mod, tmp_path):
         sim.step(n)
         o.step(n)
         _compare_state(sim, o.state())
+
+
+def test_tissue4096_fp64_matches_reference_digests(lbib, tmp_path):
+    """The large configuration (4096x4096, 6000 cells placed by Poisson-disk
+    sampling, ~1M membrane nodes, 3 species with decay, tension, cell
+    junctions, growth and division at 2x area): every array identical to the
+    reference build's at t = 0, 10, 20 (golden digests from oracle/_ref)."""
+    path = os.path.join(GOLD, "tissue4096_digest.json")
+    if not os.path.exists(path):
+        pytest.skip("tissue4096 digests not generated")
+    dig = json.load(open(path))
+    sim = lbib.Simulation(configs.config3(iterations=20, report_step=10).write(str(tmp_path)), lbib.FP64)
+    prev = 0
+    for t in (0, 10, 20):
+        sim.step(t - prev)
+        prev = t
+        lat = sim.lattice()
+        ids, node = sim.membrane()
+        assert ids.shape[0] == dig[str(t)]["M"], t
+        got = {"f": lat.f, "g": lat.g, "vel": lat.vel, "force": lat.force, "dom": lat.dom, "ctype": lat.ctype,
+               "ids": ids, "node": node, "conn": sim.connections()}
+        for k, v in got.items():
+            assert _digest(v) == dig[str(t)][k], (t, k)
+        del lat, got
+
+
+def test_tissue4096_fp32_shifted_runs(lbib, tmp_path):
+    """The same configuration in FP32-shifted storage: 20 steps without a
+    device error, the same membrane size as FP64 and finite fields."""
+    paths = configs.config3(iterations=20, report_step=10).write(str(tmp_path))
+    sim = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    sim.step(20)
+    s = sim.sizes()
+    assert s["M"] > 900000 and s["cells"] == 6000
+    lat = sim.lattice()
+    assert np.isfinite(lat.f).all() and np.isfinite(lat.g).all()

@@ -45,13 +45,12 @@ def lbib():
 
 
 def _cfg(species, bio, iterations=30, start=95):
-    # one cell of radius 12 (area ~450, above the division threshold 380).
-    # Its nodes are turned by a phase of 0.1 rad: with none, a node sits at
-    # x = 32 - 4e-15, where the reference binds a 5-column stencil (x + 2
-    # rounds to an integer) and keeps it after the node has moved within its
-    # cell, while the device derives the stencil from the current position.
+    # one cell of radius 12 (area ~450, above the division threshold 380),
+    # centred on a lattice node: its bottom node sits at x = 32 - 4e-15,
+    # where the reference binds a 5-column stencil (x + 2 rounds to an
+    # integer) and keeps it while the node stays in its unit cell
     cfg = configs.toy(n=64, r=12.0, nodes=120, iterations=iterations, report_step=10, species=1)
-    cfg.cells = [(1, configs.circle(32.0, 32.0, 12.0, 120, phase=0.1))]
+    cfg.cells = [(1, configs.circle(32.0, 32.0, 12.0, 120))]
     cfg.area = None
     cfg.tension = None
     cfg.bio = list(bio)

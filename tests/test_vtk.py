@@ -129,7 +129,8 @@ def _etree_polygon_block(vtm):
 def test_reference_vtm_geometry():
     """The geometry file that the reference's tutorial_01 loads
     (apps/config/vtk/Cells_0.vtm), where the reference sources are present."""
-    path = "/root/reference/apps/config/vtk/Cells_0.vtm"
+    from oracle import oracle as O
+    path = os.path.join(O.REFERENCE, "apps", "config", "vtk", "Cells_0.vtm")
     if not os.path.exists(path):
         pytest.skip("reference sources not present")
     from lbibcell_b200 import runner

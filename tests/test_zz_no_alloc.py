@@ -99,3 +99,48 @@ def test_areas_static_two_handles_in_turn(lib, tmp_path):
     finally:
         assert lib.lbib_destroy(a) == 0
         assert lib.lbib_destroy(b) == 0
+
+
+def test_areas_static_rejections_keep_the_handle(lib, tmp_path):
+    """Missing output buffers are refused with LBIB_ERR_INPUT, and the same
+    handle still gives lbib_areas' values afterwards."""
+    h = _create(lib, _tissue(tmp_path), 0)
+    try:
+        assert lib.lbib_step(h, 3) == 0
+        assert lib.lbib_areas_static(h, None, None, 5) == -90  # LBIB_ERR_INPUT
+        ref = _areas(lib.lbib_areas, h, 64)
+        got = _areas(lib.lbib_areas_static, h, 64)
+        assert got[0] == ref[0] == 25
+        np.testing.assert_array_equal(got[1], ref[1])
+        np.testing.assert_array_equal(got[2], ref[2])
+        assert lib.lbib_step(h, 2) == 0
+    finally:
+        assert lib.lbib_destroy(h) == 0
+
+
+def test_areas_static_ring_too_long(lib, tmp_path):
+    """A cell whose ring holds more nodes than the area kernel sums in one
+    block (4096) is reported as a capacity error, with the index of the cell,
+    and the caller's buffer holds no value of an earlier call."""
+    cfg = configs.Config(name="big_ring", nx=720, ny=720, tau_fluid=1.0, iterations=10, report_step=10,
+                         cells=[(1, configs.circle(360.0, 360.0, 330.0, 4200, phase=0.1))],
+                         species=[], area=None, tension=None)
+    small = _create(lib, _tissue(str(tmp_path / "small")), 0)
+    big = _create(lib, cfg.write(str(tmp_path / "big")), 0)
+    try:
+        _areas(lib.lbib_areas_static, small, 64)  # leaves 25 areas in the shared array
+        dom = np.zeros(4, np.uint32)
+        area = np.full(4, 7.0)
+        assert lib.lbib_areas_static(big, _p(dom), _p(area), 4) == -70  # LBIB_ERR_CAPACITY
+        assert not np.any(area[:1] > 100.0)  # no stale area of the other handle
+        buf = ctypes.create_string_buffer(256)
+        idx = ctypes.c_longlong(-1)
+        lib.lbib_last_error(big, buf, 256, ctypes.byref(idx))
+        assert b"ring" in buf.value and idx.value == 0
+        assert lib.lbib_areas(big, _p(dom), _p(area), 4) == -70
+        # the other handle is unaffected
+        n, _, a = _areas(lib.lbib_areas_static, small, 64)
+        assert n == 25 and np.all(a > 100.0)
+    finally:
+        assert lib.lbib_destroy(big) == 0
+        assert lib.lbib_destroy(small) == 0
