@@ -338,14 +338,17 @@ def adjoint_large_block(args, tmp, rank, world, local):
     areas frozen).  Loss: the kinetic energy of the final distributions in the
     central 256x256 window plus sum (C_k - c_target_k)^2, c_target from a
     forward run with the strengths perturbed by N(0, 0.1) relative.  sqrt(T)
-    checkpoints with segment recompute.  Reports adjoint/forward time, the
-    device memory in use during the run and one central-difference check."""
+    checkpoints with segment recompute.  FP32-shifted forward and FP32
+    checkpoints; the reverse step computes in FP64 and the parameter gradients
+    accumulate in FP64.  Reports adjoint/forward time, the device memory in
+    use during the run and one central-difference check (step 1e-4 on a
+    strength of 0.01: the FP32 forward's rounding rules out smaller steps)."""
     import torch
     from lbibcell_b200 import configs, runner
     cfg = configs.config5()
     paths = cfg.write(os.path.join(tmp, f"adj2048_rank{rank}"))
     T = args.adjoint_large_steps
-    sim = runner.Simulation(paths, runner.FP64, device=local)
+    sim = runner.Simulation(paths, runner.FP32_SHIFTED, device=local)
     first = sim.areas()          # the regulator's targets: 1.2 x these
     sim.step(3)
     areas = sim.areas()
@@ -394,7 +397,7 @@ def adjoint_large_block(args, tmp, rank, world, local):
     free2, _ = torch.cuda.mem_get_info(local)
     gS = sim.diff_mass() * coef
     d = int(np.argmax(np.abs(gS[1:]))) + 1
-    h = 1e-6
+    h = 1e-4
     sp, sm = strengths.copy(), strengths.copy()
     sp[d] += h
     sm[d] -= h
@@ -402,7 +405,7 @@ def adjoint_large_block(args, tmp, rank, world, local):
     sim.diff_end()
     sim.close()
     return {"workload": f"{cfg.name}: {cfg.nx}x{cfg.ny}, {len(cfg.cells)} cells, fluid + {len(cfg.species)} species, "
-                        "frozen geometry, FP64 forward and adjoint",
+                        "frozen geometry, FP32-shifted forward and checkpoints, FP64 reverse arithmetic",
             "T": T, "K": int(math.ceil(math.sqrt(T))), "forward_ms": fwd_ms, "backward_ms": bwd_ms,
             "adjoint_over_forward": bwd_ms / fwd_ms,
             "device_memory_gb": {"before_run": (total - free0) / 1e9, "run_allocated": (total - free1) / 1e9,
@@ -546,13 +549,31 @@ def main():
         bwd_ms = dist_max(d.last_timing()["total_ms"], world)
         d.diff_end()
         d.close()
+        # the same run on an FP32-shifted handle (FP32 forward and states)
+        d32 = runner.Simulation(apaths, runner.FP32_SHIFTED, device=local)
+        d32.step(3)
+        d32.diff_begin(T, K)
+        d32.diff_forward()
+        d32.diff_backward(seed)
+        torch.cuda.synchronize()
+        d32.diff_forward()
+        fwd32 = dist_max(d32.last_timing()["total_ms"], world)
+        g32 = d32.diff_backward(seed)
+        bwd32 = dist_max(d32.last_timing()["total_ms"], world)
+        d32.diff_end()
+        d32.close()
         AL = acfg.nx * acfg.ny
+        adjoint_fp32 = {"forward_ms": fwd32, "backward_ms": bwd32, "adjoint_over_forward": bwd32 / fwd32,
+                        "grad_rel_diff_vs_fp64": {
+                            k: float(np.abs(g32[k] - g[k]).max() / max(np.abs(g[k]).max(), 1e-300))
+                            for k in ("force", "tau", "rates")}}
         adjoint = {"workload": f"{acfg.name}: {acfg.nx}x{acfg.ny}, {len(acfg.cells)} cells, "
                                f"{len(acfg.species)} species, frozen geometry, FP64",
                    "T": T, "K": K, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "forward_mlups": world * AL * T / (fwd_ms / 1e3) / 1e6,
                    "backward_note": "segment recompute from checkpoints + adjoint steps",
-                   "grad_finite": bool(np.isfinite(g["force"]).all() and np.isfinite(g["tau"]).all())}
+                   "grad_finite": bool(np.isfinite(g["force"]).all() and np.isfinite(g["tau"]).all()),
+                   "fp32": adjoint_fp32}
 
     # ---- FP32-shifted error at fixed horizons (independent of --steps) -------
     horizons = None

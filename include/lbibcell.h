@@ -181,7 +181,11 @@ int lbib_load_solvers(lbib_handle* h, const char* solverFile);
 /* Number of domain ids (rows of the per-domain source and mass tables). */
 int lbib_get_domain_count(lbib_handle* h, int* n);
 
-/* Differentiated runs (no counterpart in the reference).  FP64 handles only.
+/* Differentiated runs (no counterpart in the reference).  An FP64 handle
+ * runs them in FP64; an FP32-shifted handle runs the forward steps in its
+ * FP32 kernel and stores the checkpoints in FP32 (half the memory), while the
+ * reverse step computes in FP64 from those states and the parameter
+ * gradients accumulate in FP64.
  *
  * A differentiated run advances the lattice T steps with the geometry frozen
  * at its state when lbib_diff_begin is called: the membrane positions (so the
@@ -198,7 +202,7 @@ int lbib_get_domain_count(lbib_handle* h, int* n);
  * lbib_diff_begin snapshots the current lattice as the run's initial state
  * and allocates the checkpoints: one state every K steps (K <= 0 picks
  * ceil(sqrt(T))) plus K-1 states of the segment being reversed; each state is
- * (9 + 5 S) * Nx * Ny doubles.  The defaults of the parameters are the
+ * (9 + 5 S) * Nx * Ny values of the lattice precision.  The defaults of the parameters are the
  * handle's: the membrane forces of the last force evaluation, the relaxation
  * times and source rates of the files. */
 int lbib_diff_begin(lbib_handle* h, int T, int K);

@@ -80,7 +80,10 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 #ifndef LBIB_ADJOINT_MIN_BLOCKS
 #define LBIB_ADJOINT_MIN_BLOCKS 2
 #endif
-template <int NS>
+// Real: the precision the states are stored in.  An FP32-shifted run stores
+// f_q - w_q in FP32 (and its species as they are); the reverse step reads
+// them back as f and runs its arithmetic in FP64 all the same.
+template <int NS, typename Real>
 __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
     pdl_wait();
     const int nx = a.nx, ny = a.ny;
@@ -97,17 +100,19 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
     const unsigned push[9] = {rC + x, rC + xp, rP + x, rC + xm, rM + x, rP + xp, rP + xm, rM + xm, rM + xp};
 
     // ---- every input of the node, loaded before any arithmetic -----------
-    const double* __restrict__ fprev = a.fprev;
+    const Real* __restrict__ fprev = (const Real*)a.fprev;
     double f[9], lf[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = fprev[(size_t)q * L + pull[q]];
+    for (int q = 0; q < 9; ++q)
+        f[q] = sizeof(Real) == 8 ? (double)fprev[(size_t)q * L + pull[q]]
+                                 : (double)fprev[(size_t)q * L + pull[q]] + weight9(q);
 #pragma unroll
     for (int q = 0; q < 9; ++q)
         lf[q] = a.seed ? (a.seedF ? a.seedF[(size_t)q * L + n] : 0.0) : (double)a.pf[(size_t)q * L + push[q]];
     double gA[NS > 0 ? NS : 1][5], muA[NS > 0 ? NS : 1][5];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-        const double* gp = a.gprev + (size_t)k * 5 * L;
+        const Real* gp = (const Real*)a.gprev + (size_t)k * 5 * L;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gA[k][q] = gp[(size_t)q * L + pull[q]];
         if (a.seed) {
@@ -362,12 +367,26 @@ int adjoint_blocks(int nx, int ny) { return ((nx + 255) / 256) * ny; }
 
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
-    switch (a.S) {
-        case 0: launch_pdl(adjoint_step64<0>, grid, 256, 0, s, a); break;
-        case 1: launch_pdl(adjoint_step64<1>, grid, 256, 0, s, a); break;
-        case 2: launch_pdl(adjoint_step64<2>, grid, 256, 0, s, a); break;
-        default: launch_pdl(adjoint_step64<3>, grid, 256, 0, s, a); break;
+    switch (a.S + (a.fp32 ? 4 : 0)) {
+        case 0: launch_pdl(adjoint_step64<0, double>, grid, 256, 0, s, a); break;
+        case 1: launch_pdl(adjoint_step64<1, double>, grid, 256, 0, s, a); break;
+        case 2: launch_pdl(adjoint_step64<2, double>, grid, 256, 0, s, a); break;
+        case 3: launch_pdl(adjoint_step64<3, double>, grid, 256, 0, s, a); break;
+        case 4: launch_pdl(adjoint_step64<0, float>, grid, 256, 0, s, a); break;
+        case 5: launch_pdl(adjoint_step64<1, float>, grid, 256, 0, s, a); break;
+        case 6: launch_pdl(adjoint_step64<2, float>, grid, 256, 0, s, a); break;
+        default: launch_pdl(adjoint_step64<3, float>, grid, 256, 0, s, a); break;
     }
+}
+
+__global__ void to_float_kernel(const double* in, float* out, size_t n) {
+    pdl_wait();
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+void launch_to_float(const double* in, float* out, size_t n, cudaStream_t s) {
+    launch_pdl(to_float_kernel, (unsigned)((n + 255) / 256), 256, 0, s, in, out, n);
 }
 
 // Sums the per-node mass-source partials into grad[base + dom].

@@ -254,8 +254,9 @@ struct AdjointArgs {
     int nx, ny;
     size_t L;
     int S;
-    const double* fprev;   // 9*L      state after step t-1
-    const double* gprev;   // S*5*L
+    const void* fprev;     // 9*L      state after step t-1 (FP64, or FP32 deviations from rest with fp32)
+    const void* gprev;     // S*5*L
+    int fp32;              // the states are FP32-shifted (f = stored value + w_q)
     const float* pf;       // 9*L      adjoint planes of step t+1 (unused with seed), FP32
     const float* pg;       // S*5*L
     const double* seed;    // S*L      dL/dC_k at the final step, or nullptr
@@ -279,6 +280,8 @@ struct AdjointArgs {
     double* grad;          // 1 + S + S*nDomains + nDomains (written by launch_adjoint_finish)
 };
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s);
+// Converts n doubles to floats (the force field of an FP32-shifted run).
+void launch_to_float(const double* in, float* out, size_t n, cudaStream_t s);
 // Thread blocks of one adjoint launch (the rows of AdjointArgs::part).
 int adjoint_blocks(int nx, int ny);
 // Reduces the per-block and per-node partials into grad.

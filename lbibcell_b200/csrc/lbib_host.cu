@@ -130,14 +130,17 @@ static T* dalloc(size_t n) {
 // planes (9*L) followed by the species planes (S*5*L), FP64.
 struct DiffCtx {
     int T = 0, K = 0, nSeg = 0;
-    size_t stateDoubles = 0;
-    double* x0 = nullptr;     // state at step 0
-    double* u0 = nullptr;     // velocity and force planes at step 0 (restored by lbib_diff_end), 4*L
-    double* ck = nullptr;     // states at steps K, 2K, ... (nSeg - 1 of them)
-    double* seg = nullptr;    // states base+1 .. base+K-1 of the segment being reversed
-    double* P[2] = {nullptr, nullptr};
+    size_t stateBytes = 0;    // (9 + 5 S) L values of the lattice precision
+    int rs = 8;               // bytes of a stored value: 8 (FP64) or 4 (FP32-shifted)
+    char* x0 = nullptr;       // state at step 0
+    char* u0 = nullptr;       // velocity and force planes at step 0 (restored by lbib_diff_end), 4*L values
+    char* ck = nullptr;       // states at steps K, 2K, ... (nSeg - 1 of them)
+    char* seg = nullptr;      // states base+1 .. base+K-1 of the segment being reversed
+    char* fin = nullptr;      // the final state of the forward pass
+    float* P[2] = {nullptr, nullptr};  // adjoint planes, (9 + 5 S) L each
     double* G = nullptr;      // 2*L
     double* force = nullptr;  // 2*L spread of the parameter forces
+    float* force32 = nullptr; // 2*L the same for the FP32-shifted forward
     double* fxp = nullptr;    // membrane forces (parameters), Mcap each
     double* fyp = nullptr;
     double* gfx = nullptr;
@@ -159,10 +162,11 @@ struct DiffCtx {
     int outlet = 0;
     unsigned it0 = 0;
     bool forwardDone = false;
-    double* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateDoubles; }
+    char* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateBytes; }
     ~DiffCtx() {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(x0); fr(u0); fr(ck); fr(seg); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(fxp); fr(fyp); fr(gfx); fr(gfy);
+        fr(x0); fr(u0); fr(ck); fr(seg); fr(fin); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(force32); fr(fxp);
+        fr(fyp); fr(gfx); fr(gfy);
         fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st); fr(massTab); fr(macc); fr(seedF);
     }
 };
@@ -1819,10 +1823,13 @@ static void diff_begin(Handle& h, int T, int K) {
     const size_t L = h.L;
     const int S = h.S;
     const int nSeg = (T + K - 1) / K;
-    const size_t stateDoubles = (size_t)(9 + 5 * S) * L;
-    const size_t states = 1 + (size_t)(nSeg - 1) + (size_t)(K - 1) + 2;
+    const int rs = h.precision == LBIB_FP64 ? 8 : 4;
+    const size_t stateElems = (size_t)(9 + 5 * S) * L;
+    const size_t stateBytes = stateElems * rs;
+    const size_t states = 1 + (size_t)(nSeg - 1) + (size_t)(K - 1) + 1;
     const size_t nPart = (size_t)adjoint_blocks(h.nx, h.ny) * (1 + S);
-    const size_t bytes = sizeof(double) * (states * stateDoubles + 20 * L + 2 * (size_t)S * L + nPart + 4 * (size_t)h.Mcap +
+    const size_t bytes = states * stateBytes + 2 * stateElems * sizeof(float) +
+                         sizeof(double) * (22 * L + 2 * (size_t)S * L + nPart + 4 * (size_t)h.Mcap +
                                            2 * (size_t)S * h.nDomains + 2 * (size_t)h.nDomains + 1 + S);
     size_t freeB = 0, totalB = 0;
     CK(cudaMemGetInfo(&freeB, &totalB));
@@ -1830,15 +1837,17 @@ static void diff_begin(Handle& h, int T, int K) {
         fail(ERR_CAPACITY, "differentiated run needs " + std::to_string(bytes >> 20) + " MiB of device memory, " +
                                std::to_string(freeB >> 20) + " MiB free (raise K or lower T)");
     std::unique_ptr<DiffCtx> d(new DiffCtx());
-    d->T = T; d->K = K; d->nSeg = nSeg; d->stateDoubles = stateDoubles;
-    d->x0 = dalloc<double>(stateDoubles);
-    d->u0 = dalloc<double>(4 * L);
-    d->ck = dalloc<double>((size_t)(nSeg - 1) * stateDoubles);
-    d->seg = dalloc<double>((size_t)(K - 1) * stateDoubles);
-    d->P[0] = dalloc<double>(stateDoubles);
-    d->P[1] = dalloc<double>(stateDoubles);
+    d->T = T; d->K = K; d->nSeg = nSeg; d->stateBytes = stateBytes; d->rs = rs;
+    d->x0 = dalloc<char>(stateBytes);
+    d->u0 = dalloc<char>(4 * L * rs);
+    d->ck = dalloc<char>((size_t)(nSeg - 1) * stateBytes);
+    d->seg = dalloc<char>((size_t)(K - 1) * stateBytes);
+    d->fin = dalloc<char>(stateBytes);
+    d->P[0] = dalloc<float>(stateElems);
+    d->P[1] = dalloc<float>(stateElems);
     d->G = dalloc<double>(2 * L);
     d->force = dalloc<double>(2 * L);
+    if (rs == 4) d->force32 = dalloc<float>(2 * L);
     d->fxp = dalloc<double>(h.Mcap); d->fyp = dalloc<double>(h.Mcap);
     d->gfx = dalloc<double>(h.Mcap); d->gfy = dalloc<double>(h.Mcap);
     d->srcTab = dalloc<double>((size_t)S * h.nDomains);
@@ -1862,10 +1871,10 @@ static void diff_begin(Handle& h, int T, int K) {
     CK(cudaMemsetAsync(d->st, 0, sizeof(Status), h.stream));
     CK(cudaMemsetAsync(d->force, 0, sizeof(double) * 2 * L, h.stream));
     // snapshot of the lattice and the run's default parameters
-    CK(cudaMemcpyAsync(d->x0, h.f[h.cur], sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
-    if (S) CK(cudaMemcpyAsync(d->x0 + 9 * L, h.g[h.cur], sizeof(double) * 5 * S * L, cudaMemcpyDeviceToDevice, h.stream));
-    CK(cudaMemcpyAsync(d->u0, h.u, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
-    CK(cudaMemcpyAsync(d->u0 + 2 * L, h.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(d->x0, h.f[h.cur], 9 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
+    if (S) CK(cudaMemcpyAsync(d->x0 + 9 * L * rs, h.g[h.cur], 5 * S * L * rs, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(d->u0, h.u, 2 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(d->u0 + 2 * L * rs, h.force, 2 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
     if (S) CK(cudaMemcpyAsync(d->srcTab, h.srcTab, sizeof(double) * S * h.nDomains, cudaMemcpyDeviceToDevice, h.stream));
     if (h.m.M) {
         CK(cudaMemcpyAsync(d->fxp, h.m.fx, sizeof(double) * h.m.M, cudaMemcpyDeviceToDevice, h.stream));
@@ -1885,21 +1894,29 @@ static bool diff_needs_iteration(const Handle& h) {
     return false;
 }
 
-// Forward step t of the differentiated run: state `in` (after step t-1) to `out`.
-static void diff_forward_step(Handle& h, DiffCtx& d, const double* in, double* out, int t) {
+// Forward step t of the differentiated run: state `in` (after step t-1) to
+// `out`, in the handle's lattice precision.
+template <typename Real>
+static void diff_forward_step_t(Handle& h, DiffCtx& d, const char* in, char* out, int t) {
     const unsigned it = d.it0 + (unsigned)(t - 1);
     if (diff_needs_iteration(h)) launch_set_iteration(d.st, it, h.stream);
-    LatticeArgs<double> a = lattice_args<double>(h, it, h.cur);
-    a.fin = in; a.fout = out;
-    a.gin = in + 9 * h.L; a.gout = out + 9 * h.L;
-    a.force = d.force;
+    LatticeArgs<Real> a = lattice_args<Real>(h, it, h.cur);
+    a.fin = (const Real*)in; a.fout = (Real*)out;
+    a.gin = (const Real*)in + 9 * h.L; a.gout = (Real*)out + 9 * h.L;
+    a.force = sizeof(Real) == 8 ? (const Real*)d.force : (const Real*)d.force32;
     a.srcTab = d.srcTab;
     a.massTab = d.massUsed ? d.massTab : nullptr;
     a.tauF = d.tauF;
     for (int k = 0; k < h.S; ++k) a.sp[k].tau = d.tau[k];
     a.status = d.st;
     a.outlet = d.outlet;
-    launch_stream_collide64(a, h.stream);
+    if (sizeof(Real) == 8) launch_stream_collide64(*(const LatticeArgs<double>*)&a, h.stream);
+    else launch_stream_collide32(*(const LatticeArgs<float>*)&a, h.stream);
+}
+
+static void diff_forward_step(Handle& h, DiffCtx& d, const char* in, char* out, int t) {
+    if (d.rs == 8) diff_forward_step_t<double>(h, d, in, out, t);
+    else diff_forward_step_t<float>(h, d, in, out, t);
 }
 
 static void diff_check_status(Handle& h, DiffCtx& d) {
@@ -1915,20 +1932,25 @@ static void diff_forward(Handle& h, DiffCtx& d) {
     mp.fx = d.fxp;
     mp.fy = d.fyp;
     launch_spread<double>(mp, h.tiles, d.force, h.nx, h.ny, L, d.st, d.it0, h.stream);
-    const double* in = d.x0;
-    double* out = nullptr;
+    if (d.rs == 4) launch_to_float(d.force, d.force32, 2 * L, h.stream);
+    // two scratch states for the steps between checkpoints (the segment
+    // buffer, free during the forward pass; with K = 2 one is enough, with
+    // K = 1 every state but the last is a checkpoint)
+    char* scratch[2] = {d.seg, d.K > 2 ? d.seg + d.stateBytes : d.seg};
+    const char* in = d.x0;
+    char* out = nullptr;
     for (int t = 1; t <= d.T; ++t) {
-        out = (t % d.K == 0 && t < d.T) ? d.state(t / d.K) : d.P[t & 1];
+        out = (t % d.K == 0 && t < d.T) ? d.state(t / d.K) : (t == d.T ? d.fin : scratch[t & 1]);
         diff_forward_step(h, d, in, out, t);
         in = out;
     }
     // the final state and the force field become the handle's lattice, for
     // lbib_download_lattice
-    CK(cudaMemcpyAsync(h.force, d.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
-    CK(cudaMemcpyAsync(h.f[h.cur], in, sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
+    if (d.rs == 8) CK(cudaMemcpyAsync(h.force, d.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    else CK(cudaMemcpyAsync(h.force, d.force32, sizeof(float) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.f[h.cur], in, 9 * L * d.rs, cudaMemcpyDeviceToDevice, h.stream));
     if (h.S)
-        CK(cudaMemcpyAsync(h.g[h.cur], in + 9 * L, sizeof(double) * 5 * h.S * L, cudaMemcpyDeviceToDevice,
-                           h.stream));
+        CK(cudaMemcpyAsync(h.g[h.cur], in + 9 * L * d.rs, 5 * h.S * L * d.rs, cudaMemcpyDeviceToDevice, h.stream));
     CK(cudaGetLastError());
     diff_check_status(h, d);
     d.forwardDone = true;
@@ -1965,23 +1987,24 @@ static void diff_backward(Handle& h, DiffCtx& d) {
         const int base = s * d.K;
         const int len = std::min(d.K, d.T - base);
         // recompute states base+1 .. base+len-1 from the checkpoint
-        auto segState = [&](int j) -> double* {  // state base + j, 0 <= j < len
-            return j == 0 ? d.state(s) : d.seg + (size_t)(j - 1) * d.stateDoubles;
+        auto segState = [&](int j) -> char* {  // state base + j, 0 <= j < len
+            return j == 0 ? d.state(s) : d.seg + (size_t)(j - 1) * d.stateBytes;
         };
         for (int j = 1; j < len; ++j) diff_forward_step(h, d, segState(j - 1), segState(j), base + j);
         for (int t = base + len; t > base; --t) {
-            const double* prev = segState(t - 1 - base);
+            const char* prev = segState(t - 1 - base);
             a.fprev = prev;
-            a.gprev = prev + 9 * L;
+            a.gprev = prev + 9 * L * d.rs;
+            a.fp32 = d.rs == 4;
             const bool seedStep = t == d.T;
             // the adjoint planes are FP32 (in the first half of the state-sized buffers)
-            const float* pin = (const float*)d.P[(t + 1) & 1];
+            const float* pin = d.P[(t + 1) & 1];
             a.pf = seedStep ? nullptr : pin;
             a.pg = seedStep ? nullptr : pin + 9 * L;
             a.seed = seedStep ? d.seed : nullptr;
             a.seedF = seedStep && d.haveSeedF ? d.seedF : nullptr;
-            a.qf = (float*)d.P[t & 1];
-            a.qg = (float*)d.P[t & 1] + 9 * L;
+            a.qf = d.P[t & 1];
+            a.qg = d.P[t & 1] + 9 * L;
             a.iteration = d.it0 + (unsigned)(t - 1);
             launch_adjoint_step64(a, h.stream);
         }
@@ -2509,7 +2532,6 @@ int lbib_get_domain_count(lbib_handle* hh, int* n) {
 
 int lbib_diff_begin(lbib_handle* hh, int T, int K) {
     API_BEGIN(hh)
-    if (h.precision != LBIB_FP64) lbib::fail(LBIB_ERR_STATE, "differentiated runs need an FP64 handle");
     if (h.cross.nfTab != nullptr)
         lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover boundary solvers on connections");
     if (h.massNode != nullptr) lbib::fail(LBIB_ERR_STATE, "differentiated runs do not cover per-node mass sources");
@@ -2630,12 +2652,12 @@ int lbib_diff_end(lbib_handle* hh) {
     if (h.diff) {
         lbib::DiffCtx& d = *h.diff;
         const size_t L = h.L;
-        CK(cudaMemcpyAsync(h.f[h.cur], d.x0, sizeof(double) * 9 * L, cudaMemcpyDeviceToDevice, h.stream));
+        const size_t rs = d.rs;
+        CK(cudaMemcpyAsync(h.f[h.cur], d.x0, 9 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
         if (h.S)
-            CK(cudaMemcpyAsync(h.g[h.cur], d.x0 + 9 * L, sizeof(double) * 5 * h.S * L, cudaMemcpyDeviceToDevice,
-                               h.stream));
-        CK(cudaMemcpyAsync(h.u, d.u0, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
-        CK(cudaMemcpyAsync(h.force, d.u0 + 2 * L, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.g[h.cur], d.x0 + 9 * L * rs, 5 * h.S * L * rs, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.u, d.u0, 2 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.force, d.u0 + 2 * L * rs, 2 * L * rs, cudaMemcpyDeviceToDevice, h.stream));
         CK(cudaStreamSynchronize(h.stream));
         delete h.diff;
         h.diff = nullptr;

@@ -148,12 +148,23 @@ class Simulation:
         return c
 
     def areas(self) -> Dict[int, float]:
-        cap = max(1, self.sizes()["cells"])
-        d = np.zeros(cap, np.uint32); a = np.zeros(cap)
-        n = self._L.lbib_areas(self._h, _p(d), _p(a), cap)
-        if n < 0:
-            raise self._error()
-        return {int(d[i]): float(a[i]) for i in range(n)}
+        """GeometryHandler::computeAreas: {domain: area}.  The output buffers
+        are kept between calls (sized for the cell count plus room for
+        divisions), so a call is one round trip to the device."""
+        for _ in range(2):
+            cap = len(getattr(self, "_area_d", ()))
+            if cap == 0:
+                cap = max(1, self.sizes()["cells"]) + 64
+                self._area_d = np.zeros(cap, np.uint32)
+                self._area_a = np.zeros(cap)
+            n = self._L.lbib_areas(self._h, _p(self._area_d), _p(self._area_a), cap)
+            if n < 0:
+                raise self._error()
+            if n <= cap:
+                return {int(self._area_d[i]): float(self._area_a[i]) for i in range(n)}
+            self._area_d = np.zeros(n + 64, np.uint32)
+            self._area_a = np.zeros(n + 64)
+        raise RuntimeError("lbib_areas: the cell count keeps changing")
 
     def accumulated_concentrations(self, species: str) -> Dict[int, float]:
         """GeometryHandler::computeAccumulatedDomainConcentrations(species)."""

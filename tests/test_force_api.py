@@ -183,3 +183,36 @@ def test_range_queries(lbib, tmp_path):
         want = [_ref_order(ids, st[:, :2], dom_of, x, y, radius, cfg.nx, cfg.ny, avoid)[1] for x, y in pts]
         assert got.tolist() == want
     assert sum(len(sim.nodes_within_radius(x, y, 2.5)) for x, y in pts) > 50
+
+
+def test_force_types_4_and_5_match_reference(lbib, oracle_mod, tmp_path):
+    """The force types no other test loads: 4, the vertical slider (a spring
+    toward the line x = position), and 5, a pull of constant magnitude toward
+    a partner node (ForceStructs.hpp), read from the force file beside a
+    spring and an anchor; FP64 exact against the reference build up to
+    iteration 9 (the records are cleared at iteration 10)."""
+    if not os.path.exists(oracle_mod.REF_DRIVER):
+        pytest.skip("reference build not available")
+    cfg = configs.toy(n=48, r=8.0, nodes=80, iterations=9, report_step=3, species=1)
+    cfg.area = None
+    cfg.tension = None
+    cfg.forces = ["4\t5\t24.5\t0.001\t0.8", "5\t12\t40\t0.0003", "5\t40\t12\t0.0003",
+                  "4\t33\t23\t0.002\t1.25", "0\t20\t60\t0.001\t2.5", "1\t70\t24\t24\t0.0005\t0.5"]
+    paths = cfg.write(str(tmp_path / "cfg"))
+    ref = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    done = 0
+    for t in (3, 6, 9):
+        sim.step(t - done)
+        done = t
+        lat = sim.lattice()
+        st = ref[t]
+        for k in ("f", "g", "vel", "force", "dom"):
+            assert np.array_equal(getattr(lat, k), getattr(st, k)), (t, k)
+        ids, node = sim.membrane()
+        assert np.array_equal(node, st.node), t
+    # the records did act: the membrane moved otherwise without them
+    cfg.forces = []
+    plain = lbib.Simulation(cfg.write(str(tmp_path / "plain")), lbib.FP64)
+    plain.step(9)
+    assert np.abs(plain.membrane()[1][:, :2] - node[:, :2]).max() > 1e-3
