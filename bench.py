@@ -311,9 +311,27 @@ def large_block(args, tmp, rank, world, local):
                      "host_events": sim.sizes()["host_events"]}
     out["fp32_over_fp64"] = out["fp32"]["mlups"] / out["fp64"]["mlups"]
     a, b = runs["fp64"].lattice(), runs["fp32"].lattice()
+    # full steps: the trajectories separate where a membrane node's FP32
+    # position moves a crossing (a domain flip re-initialises a node), so the
+    # pointwise error is the flips'; the frozen-geometry comparison below is
+    # the lattice arithmetic's
     out["fp32_vs_fp64_rel_err"] = rel_errors(a, b)
     out["steps_compared"] = warm + K + prof
+    force = a.force
     del a, b
+    for sim in runs.values():
+        sim.close()
+    # fresh simulations (same initial state and domain ids), the FP64 run's
+    # force field, lattice steps only
+    fr = {p: runner.Simulation(paths, p, device=local) for p in (runner.FP64, runner.FP32_SHIFTED)}
+    for sim in fr.values():
+        sim.set_lattice(force=force)
+        sim.lattice_step(K, outlet=True)
+    out["fp32_vs_fp64_rel_err_frozen_geometry"] = rel_errors(fr[runner.FP64].lattice(), fr[runner.FP32_SHIFTED].lattice())
+    out["frozen_steps"] = K
+    for sim in fr.values():
+        sim.close()
+    runs = {}
     for sim in runs.values():
         sim.close()
     if rank == 0 and args.large_cpu and world == 1:

@@ -16,6 +16,21 @@
 
 namespace lbib {
 
+// Cache hints of the stream-collide kernel's distribution traffic (a tuning
+// knob, chosen by measurement): bit 0 loads the pulled inputs with the
+// evict-first policy (each is read once), bit 1 stores the outputs with it.
+#ifndef LBIB_COLLIDE_CACHE_HINTS
+#define LBIB_COLLIDE_CACHE_HINTS 0
+#endif
+__device__ __forceinline__ float ld_dist(const float* p) {
+    if (LBIB_COLLIDE_CACHE_HINTS & 1) return __ldcs(p);
+    return *p;
+}
+__device__ __forceinline__ void st_dist(float* p, float v) {
+    if (LBIB_COLLIDE_CACHE_HINTS & 2) __stcs(p, v);
+    else *p = v;
+}
+
 __device__ __forceinline__ float reaction32(int kind, float src, float decay, uint32_t dom, unsigned iteration,
                                             float C) {
     if (kind == RX_LINEAR) return src - decay * C;
@@ -90,15 +105,15 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     const unsigned rC = (unsigned)y * nx, rM = (unsigned)ym * nx, rP = (unsigned)yp * nx;
     const unsigned n = rC + x;
     const float* __restrict__ fin = a.fin;
-    const float hT = fin[0 * L + rC + x];
-    const float hE = fin[1 * L + rC + xm];
-    const float hN = fin[2 * L + rM + x];
-    const float hW = fin[3 * L + rC + xp];
-    const float hS = fin[4 * L + rP + x];
-    const float hNE = fin[5 * L + rM + xm];
-    const float hNW = fin[6 * L + rM + xp];
-    const float hSW = fin[7 * L + rP + xp];
-    const float hSE = fin[8 * L + rP + xm];
+    const float hT = ld_dist(&fin[0 * L + rC + x]);
+    const float hE = ld_dist(&fin[1 * L + rC + xm]);
+    const float hN = ld_dist(&fin[2 * L + rM + x]);
+    const float hW = ld_dist(&fin[3 * L + rC + xp]);
+    const float hS = ld_dist(&fin[4 * L + rP + x]);
+    const float hNE = ld_dist(&fin[5 * L + rM + xm]);
+    const float hNW = ld_dist(&fin[6 * L + rM + xp]);
+    const float hSW = ld_dist(&fin[7 * L + rP + xp]);
+    const float hSE = ld_dist(&fin[8 * L + rP + xm]);
     float gi[NS > 0 ? NS : 1][5];
     uint8_t bW = 0, bWe = 0, bS = 0, bSn = 0;
     if (BOUNCE) {
@@ -110,17 +125,17 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const float* __restrict__ gin = a.gin + (size_t)k * 5 * L;
-        gi[k][0] = gin[0 * L + rC + x];
+        gi[k][0] = ld_dist(&gin[0 * L + rC + x]);
         if (BOUNCE && a.sp[k].bounce) {
-            gi[k][1] = bW ? gin[3 * L + n] : gin[1 * L + rC + xm];
-            gi[k][2] = bS ? gin[4 * L + n] : gin[2 * L + rM + x];
-            gi[k][3] = bWe ? gin[1 * L + n] : gin[3 * L + rC + xp];
-            gi[k][4] = bSn ? gin[2 * L + n] : gin[4 * L + rP + x];
+            gi[k][1] = bW ? ld_dist(&gin[3 * L + n]) : ld_dist(&gin[1 * L + rC + xm]);
+            gi[k][2] = bS ? ld_dist(&gin[4 * L + n]) : ld_dist(&gin[2 * L + rM + x]);
+            gi[k][3] = bWe ? ld_dist(&gin[1 * L + n]) : ld_dist(&gin[3 * L + rC + xp]);
+            gi[k][4] = bSn ? ld_dist(&gin[2 * L + n]) : ld_dist(&gin[4 * L + rP + x]);
         } else {
-            gi[k][1] = gin[1 * L + rC + xm];
-            gi[k][2] = gin[2 * L + rM + x];
-            gi[k][3] = gin[3 * L + rC + xp];
-            gi[k][4] = gin[4 * L + rP + x];
+            gi[k][1] = ld_dist(&gin[1 * L + rC + xm]);
+            gi[k][2] = ld_dist(&gin[2 * L + rM + x]);
+            gi[k][3] = ld_dist(&gin[3 * L + rC + xp]);
+            gi[k][4] = ld_dist(&gin[4 * L + rP + x]);
         }
     }
     const uint32_t dom = a.dom[n];
@@ -217,7 +232,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
     }
     float* __restrict__ fo = a.fout;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) fo[q * L + n] = ho[q];
+    for (int q = 0; q < 9; ++q) st_dist(&fo[q * L + n], ho[q]);
 
     // Species: e0 = C - 4 e1 rather than C/3, so that the equilibrium sums to C
     // exactly up to one rounding: with C/3 and C/6 each rounded in FP32 the
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
             for (int q = 0; q < 5; ++q) go[q] *= rs[p];
         float* __restrict__ gop = a.gout + (size_t)k * 5 * L;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) gop[q * L + n] = go[q];
+        for (int q = 0; q < 5; ++q) st_dist(&gop[q * L + n], go[q]);
     }
 }
 

@@ -927,11 +927,17 @@ void SimulationRunner::runSimulation() {
             reportHandler_.writeReport(t - 1);
         }
     } catch (const std::exception& exp) {
-        // SimulationRunner.cpp:101-109: report everything, dump the state
+        // SimulationRunner.cpp:101-109: report everything, dump the state,
+        // print the error.  A device error leaves the handle refusing work, so
+        // the crash reports write what they can and their own failures are
+        // not reported over the original error.
         Parameters.setReportSteps(1);
         if (h_) {
             ActiveScope scope(h_);
-            reportHandler_.writeCrashReport(t);
+            try {
+                reportHandler_.writeCrashReport(t);
+            } catch (const std::exception&) {
+            }
             const std::string s = std::to_string(t);
             lbib_write_simulation(h_, ("output/CRASH_forceOut_" + s + ".txt").c_str(),
                                   ("output/CRASH_geoOut_" + s + ".txt").c_str(),

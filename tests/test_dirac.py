@@ -111,12 +111,12 @@ def test_dirac_with_membrane_matches_reference(lbib, oracle_mod, tmp_path):
 
 
 def test_dirac_refusals(lbib, tmp_path):
-    cfg = _far_cell(64, 10)
+    cfg = _far_cell(128, 10)
     cfg.force_model = "GuoZhengShi2002ForceModel"
     with pytest.raises(lbib.LbibError) as e:
         lbib.Simulation(cfg.write(str(tmp_path / "a")), lbib.FP64)
     assert e.value.code == 90
-    sim = lbib.Simulation(_far_cell(64, 10).write(str(tmp_path / "b")), lbib.FP64)
+    sim = lbib.Simulation(_far_cell(128, 10).write(str(tmp_path / "b")), lbib.FP64)
     with pytest.raises(lbib.LbibError) as e:
         sim.diff_begin(4, 2)
     assert e.value.code == 91

@@ -98,7 +98,10 @@ def test_lbib_division_per_cell_threshold_matches_reference(lbib, oracle_mod, tm
         lat = sim.lattice()
         for field in ("f", "g", "vel", "force", "dom", "ctype"):
             a, b = getattr(lat, field), getattr(ref, field)
-            assert np.array_equal(a, b), f"t={t} {field}: max |diff| {np.abs(a.astype(float) - b.astype(float)).max()}"
+            # the reference's re-initialisation writes NaN (0/0) for nodes
+            # trapped between the daughters' membranes: equal positions required
+            assert np.array_equal(a, b, equal_nan=True), \
+                f"t={t} {field}: max |diff| {np.nanmax(np.abs(a.astype(float) - b.astype(float)))}"
         ids, node = sim.membrane()
         assert np.array_equal(ids, ref.ids) and np.array_equal(node, ref.node), f"t={t}: membrane differs"
         assert np.array_equal(sim.connections(), ref.conn), f"t={t}: connections differ"

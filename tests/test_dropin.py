@@ -108,11 +108,15 @@ def test_user_plugin_app_matches_reference_build(dropin_lib, oracle_mod, tmp_pat
 def _tutorial01_dir(tmp_path, lbib):
     """config/ for tutorial_01: parameters (64x64, 20 iterations, reports
     every 10), the geometry as the .vtm the app loads (one cell, written by
-    the cell reporter) and the force file."""
+    the cell reporter) and the force file.  The cell (area ~314) stays below
+    the division threshold (380): a larger one, divided at iteration 0 from
+    the Float32 positions of the .vtm, makes the reference's cell division
+    join two coincident nodes and fail (Connection.cpp:315-323), in the
+    reference build as here."""
     run = tmp_path / "run"
     (run / "config" / "vtk").mkdir(parents=True)
-    cfg = configs.toy(n=64, r=12.0, nodes=120, iterations=20, report_step=10, species=0)
-    cfg.cells = [(1, configs.circle(32.0, 32.0, 12.0, 120, phase=0.1))]
+    cfg = configs.toy(n=64, r=10.0, nodes=100, iterations=20, report_step=10, species=0)
+    cfg.cells = [(1, configs.circle(32.0, 32.0, 10.0, 100, phase=0.1))]
     cfg.species = [configs.Species("tutorial_01_CDESolverD2Q5_SIGNAL", 2.0)]
     cfg.tau_fluid = 2.0
     cfg.area = None

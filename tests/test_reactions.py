@@ -97,9 +97,9 @@ def test_reactions_fp32_shifted(lbib, tmp_path):
 
 
 def test_unsupported_cde_solver_is_refused(lbib, tmp_path):
-    """DiracD2Q5 keeps the populations of boundary links in its advect and is
-    not built; a create call that names it fails."""
-    paths = _cfg([("DiracD2Q5", 1.0)], 20).write(str(tmp_path))
+    """The D2Q4 solvers (CDESolverD2Q4, DiracD2Q4, SchnakenbergD2Q4u/v) are
+    not built; a create call that names one fails."""
+    paths = _cfg([("CDESolverD2Q4", 1.0)], 20).write(str(tmp_path))
     with pytest.raises(lbib.LbibError) as e:
         lbib.Simulation(paths, lbib.FP64)
     assert e.value.code == 90
