@@ -500,7 +500,12 @@ def main():
         for d, r in sp.source.items():
             pinned[k, d] = r
     src = pinned.numpy()
+    # the areas come back into pinned host arrays (the caller's buffers)
+    cap = sim.sizes()["cells"] + 64
+    area_dom = torch.zeros(cap, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    area_val = torch.zeros(cap, dtype=torch.float64).pin_memory().numpy()
     e2e_steps = min(args.steps, 200)
+    host_events_before = sim.sizes()["host_events"]
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -509,12 +514,12 @@ def main():
         for k in range(S):
             sim.set_species_source(k, src[k])
         sim.step(1)
-        nareas = len(sim.areas())
+        nareas = sim.areas_into(area_dom, area_val)
     torch.cuda.synchronize()
     e2e_s = dist_max(time.perf_counter() - t0, world)
     e2e = {"value": world * L * e2e_steps / e2e_s / 1e6, "unit": "MLUPS",
            "h2d_bytes_per_step": int(S * nd * 8), "d2h_bytes_per_step": int(nareas * 8 + nareas * 4),
-           "steps": e2e_steps}
+           "steps": e2e_steps, "host_events": sim.sizes()["host_events"] - host_events_before}
     sim.close()
 
     # ---- FP64 path and the FP32-vs-FP64 error --------------------------------

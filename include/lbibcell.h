@@ -243,9 +243,31 @@ int lbib_diff_mass(lbib_handle* h, const double* mass, double* gMass, int n);
  * it.  Must be called after lbib_diff_begin. */
 int lbib_diff_fluid_seed(lbib_handle* h, const double* dLdf);
 
+/* dL/d of the force records' parameters, through the node forces
+ * (ForceSolver::calculateForce, ForceSolver.cpp:42-85 with the forces of
+ * ForceStructs.hpp:49-588): after lbib_diff_backward, with its dL/dF_i and
+ * the handle's current records and positions.  Each record adds to its own
+ * node's force only, so dL/dp = dL/dF_i . dF_i/dp.  gPar[4 r + q] for record
+ * r (lbib_download_forces' order) and parameter q (lbib_add_forces' meaning;
+ * 0 for parameters the type does not read; the spring's k and l0, the
+ * anchor's x, y, k, l0, the constant force, the slider's position, k, l0 and
+ * the tension's f).  The gradient is that of the run's loss when the run's
+ * node forces are these records' forces (memForce of lbib_diff_forward, or
+ * the default when the records did not change since the last force
+ * evaluation).  Returns the record count (fills min(count, cap) records) or
+ * a negative LBIB_ERR_*. */
+int lbib_diff_force_params(lbib_handle* h, double* gPar, int cap);
+
 /* Restores the snapshot taken by lbib_diff_begin (distributions, velocity and
  * force planes) and frees the run's device memory. */
 int lbib_diff_end(lbib_handle* h);
+
+/* The ForceSolver's records in the device's order: by node (ascending id),
+ * each node's records in insertion order (forcemap_[id] order, ForceSolver.cpp:
+ * 42-85).  type[r], id1[r] (the node), id2[r] (the partner's id for types 0,
+ * 5, 6, 7; 0 otherwise), par[4 r .. 4 r + 3] as lbib_add_forces takes them.
+ * Returns the record count (fills min(count, cap)) or a negative LBIB_ERR_*. */
+int lbib_download_forces(lbib_handle* h, int* type, unsigned* id1, unsigned* id2, double* par, int cap);
 
 /* ForceSolver::addForce for n records at once (ForceSolver.cpp:107-139), in
  * place of one text line each.  Record k has type[k] (0-7, ForceStructs.hpp),

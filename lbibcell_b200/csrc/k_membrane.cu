@@ -141,6 +141,74 @@ __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration,
     if (slots) tile_slot_node(m, t, i, true, nx, ny, st);
 }
 
+// dL/d of every force record's parameters from dL/dF of the node forces
+// (the membrane-force gradient of a differentiated run), through the
+// record's force as force_eval_kernel forms it (ForceStructs.hpp:49-588):
+// each record of node i adds to F_i only, so
+// dL/dp = (dL/dF_i) . dF_i/dp, with the positions fixed.  Parameters a type
+// does not read get 0.  gpar: 4 per record, in record order.
+__global__ void force_param_grad_kernel(MembraneDev m, const double* gfx, const double* gfy, double* gpar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.topo->M) return;
+    const double x1 = m.x[i], y1 = m.y[i], gx = gfx[i], gy = gfy[i];
+    for (int r = m.foff[i]; r < m.foff[i + 1]; ++r) {
+        const int type = m.ftype[r];
+        const double* p = m.fpar + 4 * (size_t)r;
+        const int j = m.fpartner[r];
+        double g[4] = {0.0, 0.0, 0.0, 0.0};
+        switch (type) {
+            case 0: case 7: case 5: case 6: {
+                if (j < 0 || j >= m.topo->M) break;
+                const double dx = m.x[j] - x1, dy = m.y[j] - y1;
+                const double dist = sqrt(dx * dx + dy * dy);
+                const double gd = (gx * dx + gy * dy) / dist;  // (dL/dF) . d / |d|
+                if (type == 5 || type == 6) {
+                    g[0] = gd;                      // F = f d/|d|
+                } else {
+                    g[0] = (dist - p[1]) * gd;      // F = k (|d| - l0) d/|d|
+                    g[1] = -p[0] * gd;
+                }
+                break;
+            }
+            case 1: {  // F = k (|d| - l0) d/|d|, d = (tx, ty) - x; none at |d| = 0
+                const double dx = p[0] - x1, dy = p[1] - y1;
+                const double dist = sqrt(dx * dx + dy * dy);
+                if (dist == 0.0) break;
+                const double gdd = gx * dx + gy * dy;
+                const double a = 1.0 - p[3] / dist, b = p[3] * gdd / (dist * dist * dist);
+                g[0] = p[2] * (a * gx + b * dx);  // dF/dtx: k [(1 - l0/|d|) I + l0 d d^T / |d|^3]
+                g[1] = p[2] * (a * gy + b * dy);
+                g[2] = (dist - p[3]) * gdd / dist;
+                g[3] = -p[2] * gdd / dist;
+                break;
+            }
+            case 2:  // F = (fx, fy)
+                g[0] = gx;
+                g[1] = gy;
+                break;
+            case 3: case 4: {  // sliders: F_y (3) or F_x (4) = +-k (|c - y| - l0), + below c
+                const double pos = type == 3 ? y1 : x1, gc = type == 3 ? gy : gx;
+                const double dist = fabs(p[0] - pos);
+                const double sgn = pos < p[0] ? 1.0 : -1.0;
+                const double dd = p[0] > pos ? 1.0 : (p[0] < pos ? -1.0 : 0.0);  // d|c - pos| / dc
+                g[0] = gc * sgn * p[1] * dd;
+                g[1] = gc * sgn * (dist - p[2]);
+                g[2] = -gc * sgn * p[1];
+                break;
+            }
+            default:
+                break;
+        }
+        for (int q = 0; q < 4; ++q) gpar[4 * (size_t)r + q] = g[q];
+    }
+}
+
+void launch_force_param_grad(const MembraneDev& m, const double* gfx, const double* gfy, double* gpar,
+                             cudaStream_t s) {
+    if (m.Mcap == 0) return;
+    force_param_grad_kernel<<<(m.Mcap + 127) / 128, 128, 0, s>>>(m, gfx, gfy, gpar);
+}
+
 template <typename Real>
 void launch_force_eval(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, bool begin,
                        TileDev* tiles, int nx, int ny) {
@@ -932,7 +1000,8 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     const int blocks = (m.Ccap + 127) / 128;
     if (c.nfTab != nullptr) launch_pdl(noflux_reset_kernel, 1, 1024, 0, s, c);
     if (c.bounceW != nullptr) launch_pdl(bounce_reset_kernel, 1, 1024, 0, s, c);
-    cudaMemsetAsync(&st->pad[2], 0, sizeof(int), s);
+    // the record count (st->pad[2]) is zero here: cleared with the status
+    // word before a run and by step_end_kernel after each step
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
     launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
     launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, ny, st);
@@ -1488,6 +1557,23 @@ __global__ void areas_fixed_kernel(MembraneDev m, const int* cellOfDom, int nDom
 void launch_areas(const MembraneDev& m, double* area, Status* st, cudaStream_t s) {
     if (m.nCells == 0) return;
     launch_pdl(areas_kernel, m.nCells, 256, 0, s, m, area, st);
+}
+
+// The fixed-point sums as areas (the conversion of area_regulator_kernel),
+// the sums cleared for their next use.
+__global__ void areas_fixed_finish_kernel(int nCells, unsigned long long* acc, double* area) {
+    pdl_wait();
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= nCells) return;
+    area[cell] = (double)(long long)acc[cell] * (1.0 / kAreaFix) / 2.0;
+    acc[cell] = 0ull;
+}
+
+void launch_areas_fixed(const MembraneDev& m, const int* cellOfDom, int nDomains, unsigned long long* acc,
+                        double* area, cudaStream_t s) {
+    if (m.nCells == 0) return;
+    if (m.Ccap > 0) launch_pdl(areas_fixed_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, cellOfDom, nDomains, acc);
+    launch_pdl(areas_fixed_finish_kernel, (m.nCells + 127) / 128, 128, 0, s, m.nCells, acc, area);
 }
 
 // The fixed device array of lbib_areas_static: the per-cell sums of one call.

@@ -1,7 +1,7 @@
 // k_topology.cu — membrane topology edits on the device.
 //
 //   remesh    GeometryHandler::remeshBoundary (GeometryHandler.cpp:385-431) as
-//             scan + scatter: every connection longer than MAXLENGTH gets a new
+//             count + scatter (block counts and their prefix in one kernel): every connection longer than MAXLENGTH gets a new
 //             node at its midpoint; the new node ids continue from the largest
 //             id in connection order (Geometry::addGeometryNode,
 //             Geometry.cpp:382-400); the split connection leaves the vector and
@@ -67,43 +67,86 @@ __device__ __forceinline__ void agg_min(int* addr, int key, int v) {
 // ---------------------------------------------------------------------------
 // Remesh
 
-__global__ void remesh_flag_kernel(MembraneDev m, TopoDev t, Status* st, int* nRng) {
-    pdl_wait();
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > m.Ccap) return;
-    int f = 0;
-    if (!st->halt && c < m.topo->C) {
-        const int a = m.ca[c], b = m.cb[c];
-        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-        // Connection::getLength (Connection.cpp:389-394)
-        const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
-        if (len > kMAXLENGTH) {
-            f = 1;
-            if (new_node_needs_rng((x1 + x2) / 2, (y1 + y2) / 2)) atomicAdd(nRng, 1);
-        }
-    }
-    t.flag[c] = f;
+constexpr int kRemeshBlock = 256;  // connections per block of the count and apply kernels
+
+// Connection c is split: longer than MAXLENGTH (Connection::getLength,
+// Connection.cpp:389-394).  `rng`: its new node needs the random perturbation.
+__device__ __forceinline__ bool remesh_split(const MembraneDev& m, int c, bool& rng) {
+    const int a = m.ca[c], b = m.cb[c];
+    const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+    const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
+    rng = len > kMAXLENGTH && new_node_needs_rng((x1 + x2) / 2, (y1 + y2) / 2);
+    return len > kMAXLENGTH;
 }
 
-// Decides the pass (K = number of splits) and applies it.  A pass that would
-// overflow a buffer or needs the random generator goes to the host; so does
-// a third pass (remesh_again_kernel).  Every thread takes the same decision;
-// the first one records it for the copy that follows.
-__global__ void remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st, const int* nRng) {
+// Pass decision.  Each block counts its connections to split (t.flag[block])
+// and the new nodes that need the random generator (T->nRng); the last block
+// to finish forms the exclusive prefix of the block counts (t.rank[block]),
+// and decides: K = the total, or 0 with a halt when the pass would overflow
+// a buffer or needs the random generator (the host runs it then; so it does
+// a third pass, remesh_again_kernel).
+__global__ void __launch_bounds__(kRemeshBlock) remesh_count_kernel(MembraneDev m, TopoDev t, Status* st) {
     pdl_wait();
-    if (st->halt) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     Topo* T = m.topo;
-    const int C = T->C, M = T->M;
-    const int K = t.rank[m.Ccap];  // exclusive scan over Ccap + 1 flags: the total
-    const bool run = K > 0 && *nRng == 0 && M + K <= m.Mcap && C + K <= m.Ccap;
-    if (c == 0) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool f = false, rng = false;
+    if (!st->halt && c < T->C) f = remesh_split(m, c, rng);
+    const int cnt = __syncthreads_count(f);
+    const int nr = __syncthreads_count(rng);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        t.flag[blockIdx.x] = cnt;
+        if (nr) atomicAdd(&T->nRng, nr);
+        __threadfence();
+        last = atomicAdd(&T->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    typedef cub::BlockScan<int, kRemeshBlock> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    int carry = 0;
+    for (int b0 = 0; b0 < (int)gridDim.x; b0 += kRemeshBlock) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < (int)gridDim.x ? __ldcg(&t.flag[b]) : 0;
+        int ex, total;
+        Scan(tmp).ExclusiveSum(v, ex, total);
+        if (b < (int)gridDim.x) t.rank[b] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int K = carry, C = T->C, M = T->M;
+        const int needRng = atomicExch(&T->nRng, 0);
+        const bool run = K > 0 && needRng == 0 && M + K <= m.Mcap && C + K <= m.Ccap;
         T->K = run ? K : 0;
+        T->done = 0;
         if (K > 0 && !run) raise_halt(st, ST_REMESH);
     }
-    if (!run || c >= C) return;
-    const int r = t.rank[c];
-    if (!t.flag[c]) {
+}
+
+// Applies the pass: connection c's rank among the split ones is its block's
+// prefix plus the split connections before it in the block (the same test
+// on the same positions as the count).
+__global__ void __launch_bounds__(kRemeshBlock) remesh_apply_kernel(MembraneDev m, TopoDev t, Status* st) {
+    pdl_wait();
+    if (st->halt) return;
+    Topo* T = m.topo;
+    const int K = T->K;
+    if (K == 0) return;
+    const int C = T->C, M = T->M;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool rng = false;
+    const bool f = c < C && remesh_split(m, c, rng);
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ int wsum[kRemeshBlock / 32];
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    if (c >= C) return;
+    int r = t.rank[blockIdx.x] + __popc(bal & ((1u << lane) - 1u));
+    for (int i = 0; i < w; ++i) r += wsum[i];
+    if (!f) {
         const int dst = c - r;
         t.ca2[dst] = m.ca[c]; t.cb2[dst] = m.cb[c]; t.cdom2[dst] = m.cdom[c]; t.cdesc2[dst] = m.cdesc[c];
         return;
@@ -181,15 +224,13 @@ __global__ void remesh_again_kernel(MembraneDev m, int nx, int ny, Status* st) {
 
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
     if (m.Ccap == 0) return 0;
-    int* nRng = &st->pad[1];
-    const int cb = (m.Ccap + 1 + 255) / 256;
-    cudaMemsetAsync(nRng, 0, sizeof(int), s);
-    launch_pdl(remesh_flag_kernel, cb, 256, 0, s, m, t, st, nRng);
-    cub::DeviceScan::ExclusiveSum(t.scanTmp, t.scanTmpBytes, t.flag, t.rank, m.Ccap + 1, s);
-    launch_pdl(remesh_apply_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st, (const int*)nRng);
+    // the count and the apply kernel partition the connections alike
+    const int cb = (m.Ccap + kRemeshBlock - 1) / kRemeshBlock;
+    launch_pdl(remesh_count_kernel, cb, kRemeshBlock, 0, s, m, t, st);
+    launch_pdl(remesh_apply_kernel, cb, kRemeshBlock, 0, s, m, t, st);
     launch_pdl(remesh_copy_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
     launch_pdl(remesh_again_kernel, (std::max(m.Ccap, m.Mcap) + 255) / 256, 256, 0, s, m, nx, ny, st);
-    return 6;
+    return 4;
 }
 
 // ---------------------------------------------------------------------------

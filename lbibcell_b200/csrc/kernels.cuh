@@ -15,7 +15,8 @@ struct Topo {
     int K;            // connections split by the current remesh pass
     int removed;      // nodes removed by the current coarsening
     int nCand;        // coarsening candidates
-    unsigned done;    // blocks of the remesh copy that have finished (the last one commits)
+    unsigned done;    // blocks of the remesh count / copy that have finished (the last one decides / commits)
+    int nRng;         // new nodes of the remesh pass that need the random perturbation
 };
 
 // Membrane state on the device (nodes in ascending id order).
@@ -224,6 +225,13 @@ void launch_area_regulator(const MembraneDev& m, double* area, double* target, d
                            const Status* st, cudaStream_t s);
 // st != nullptr: a ring longer than the kernel's limit raises ERR_CAPACITY there.
 void launch_areas(const MembraneDev& m, double* area, Status* st, cudaStream_t s);
+// dL/d of each force record's 4 parameters from the node-force gradient (gfx, gfy).
+void launch_force_param_grad(const MembraneDev& m, const double* gfx, const double* gfy, double* gpar,
+                             cudaStream_t s);
+// GeometryHandler::computeAreas from exact fixed-point shoelace sums (FP32-shifted
+// runs): independent of the summation order, so no ring order is needed.
+void launch_areas_fixed(const MembraneDev& m, const int* cellOfDom, int nDomains, unsigned long long* acc,
+                        double* area, cudaStream_t s);
 // FP32-shifted runs: areas from the connections in fixed point (no ring order
 // needed), then the regulator.  acc (nCells) must start at zero; it is left zero.
 void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, unsigned long long* acc, double* area,

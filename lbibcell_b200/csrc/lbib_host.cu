@@ -162,6 +162,7 @@ struct DiffCtx {
     int outlet = 0;
     unsigned it0 = 0;
     bool forwardDone = false;
+    bool backwardDone = false;  // gfx / gfy hold the last reverse pass's membrane-force gradient
     char* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateBytes; }
     ~DiffCtx() {
         auto fr = [](void* p) { if (p) cudaFree(p); };
@@ -243,7 +244,11 @@ struct Handle {
     Status* stHost = nullptr;
     Topo* topoHost = nullptr;   // pinned copy of the device counts, read with the status word
     bool ringsCurrent = false;  // the device's ring order matches the topology (no rebuild needed)
-    std::vector<double> areaHost;  // staging of lbib_areas' read-back
+    // per-cell areas read back at the end of lbib_step when its bio stage
+    // formed them (the area regulator), in pinned memory; areaFresh: they
+    // are the areas of the current state (any other API call clears it)
+    double* areaPinned = nullptr;
+    bool areaFresh = false;
     cudaStream_t stream = nullptr;
 
     std::mt19937 genNode{1};
@@ -317,6 +322,7 @@ Handle::~Handle() {
     fr(st);
     if (stHost) cudaFreeHost(stHost);
     if (topoHost) cudaFreeHost(topoHost);
+    if (areaPinned) cudaFreeHost(areaPinned);
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
     for (auto e : kEvents) cudaEventDestroy(e);
@@ -908,6 +914,9 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.area = dalloc<double>(h.cellCap); h.target = dalloc<double>(h.cellCap);
         h.areaAcc = dalloc<unsigned long long>(h.cellCap);
         CK(cudaMemset(h.areaAcc, 0, sizeof(unsigned long long) * h.cellCap));
+        if (h.areaPinned) CK(cudaFreeHost(h.areaPinned));
+        h.areaPinned = nullptr;
+        CK(cudaMallocHost(&h.areaPinned, sizeof(double) * h.cellCap));
         h.td.cellCount = dalloc<int>(h.cellCap + 1); h.td.cellStart = dalloc<int>(h.cellCap + 1);
         h.td.cellFill = dalloc<int>(h.cellCap); h.td.startNode = dalloc<int>(h.cellCap);
     }
@@ -1083,6 +1092,7 @@ __global__ void step_begin_kernel(Status* st) {
 
 __global__ void step_end_kernel(Status* st) {
     pdl_wait();
+    st->pad[2] = 0;  // the crossing records of this step are consumed
     if (st->halt) return;
     st->pad[0] += 1;  // steps completed in this batch
     st->iteration += 1;  // Parameters++ (SimulationRunner.cpp:98)
@@ -1221,6 +1231,34 @@ static void read_status(Handle& h) {
 
 static void write_status(Handle& h) {
     CK(cudaMemcpyAsync(h.st, h.stHost, sizeof(Status), cudaMemcpyHostToDevice, h.stream));
+}
+
+// The bio stage of a step leaves the cell areas of the new state in h.area
+// when the area regulator is registered: in ring order in FP64 runs, from
+// the exact fixed-point sums in FP32-shifted runs (the values lbib_areas
+// forms).  Their read-back rides on the status word's.
+static bool step_leaves_areas(const Handle& h) {
+    if (h.m.nCells == 0 || h.m.Ccap == 0 || h.areaPinned == nullptr) return false;
+    for (int b : h.bio)
+        if (b == 2) return true;
+    return false;
+}
+
+// GeometryHandler::computeAreas into the device array `area`: in ring order in
+// FP64 runs (the ring order is rebuilt only when the topology changed since
+// it was last built), from the fixed-point sums in FP32-shifted runs.
+static void queue_areas(Handle& h, double* area) {
+    if (h.precision == LBIB_FP64) {
+        if (!h.ringsCurrent) launch_rings(h.m, h.td, h.st, h.stream);
+        launch_areas(h.m, area, h.st, h.stream);
+    } else {
+        launch_areas_fixed(h.m, h.td.cellOfDom, h.nDomains, h.areaAcc, area, h.stream);
+    }
+}
+
+static void queue_step_areas(Handle& h) {
+    if (step_leaves_areas(h))
+        CK(cudaMemcpyAsync(h.areaPinned, h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost, h.stream));
 }
 
 // Clears the status word for a run that starts at Parameters' iteration `it`.
@@ -1411,6 +1449,7 @@ static void run_steps(Handle& h, int n) {
                 launch_step_graph<Real>(h, parity, it % 10 == 0, step_bio_ops(h, it));
         }
         CK(cudaGetLastError());
+        queue_step_areas(h);
         read_status(h);
         const Status st = *h.stHost;
         const int done = st.pad[0];
@@ -1447,6 +1486,7 @@ static void run_steps(Handle& h, int n) {
             if (from < 0) fail(ERR_STATE, "unexpected halt stage");
             reset_status(h, it, h.cellTypesCopied);
             h.launches += launch_stages<Real>(h, it % 10 == 0, step_bio_ops(h, it), h.cur, from, nullptr, nullptr);
+            queue_step_areas(h);
             read_status(h);
             if (h.stHost->err) {
                 h.err = h.stHost->err;
@@ -2030,6 +2070,7 @@ struct lbib_handle {
     if (!(hh)) return LBIB_ERR_STATE;                    \
     Handle& h = (hh)->h;                                 \
     if (h.err) return h.err;                             \
+    h.areaFresh = false;                                 \
     try {                                                \
         cudaSetDevice(h.device);
 #define API_END                                          \
@@ -2079,6 +2120,9 @@ int lbib_step(lbib_handle* hh, int n) {
     CK(cudaEventRecord(h.evA, h.stream));
     if (h.precision == LBIB_FP64) lbib::run_steps<double>(h, n);
     else lbib::run_steps<float>(h, n);
+    // the areas read back with the last status word are those of the state
+    // now, unless a host bio solver edited the geometry after the last step
+    h.areaFresh = n > 0 && lbib::step_leaves_areas(h) && !lbib::host_bio_at(h, h.iteration - 1);
     CK(cudaEventRecord(h.evB, h.stream));
     CK(cudaEventSynchronize(h.evB));
     float ms = 0;
@@ -2306,27 +2350,27 @@ int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
     }
     try {
         CK(cudaSetDevice(h.device));
-        lbib::reset_status(h, h.iteration, h.cellTypesCopied);
-        // the ring order is rebuilt only when the topology changed since it was
-        // last built (FP32-shifted steps and remeshing leave it stale)
-        if (!h.ringsCurrent) lbib::launch_rings(h.m, h.td, h.st, h.stream);
-        lbib::launch_areas(h.m, h.area, h.st, h.stream);
-        CK(cudaGetLastError());
-        h.areaHost.resize(h.m.nCells);
-        if (h.m.nCells)
-            CK(cudaMemcpyAsync(h.areaHost.data(), h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost,
-                               h.stream));
-        lbib::read_status(h);
-        if (h.stHost->err) {
-            const long long idx = h.stHost->errIndex;
+        // after lbib_step, the areas its bio stage formed are already on the
+        // host; otherwise one round trip forms and reads them
+        if (!h.areaFresh && h.m.nCells > 0) {
             lbib::reset_status(h, h.iteration, h.cellTypesCopied);
-            h.msg = "lbib_areas: cell " + std::to_string(idx) + " has more membrane nodes than one ring may hold";
-            h.errIndex = idx;
-            return -LBIB_ERR_CAPACITY;
+            lbib::queue_areas(h, h.area);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(h.areaPinned, h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost,
+                               h.stream));
+            lbib::read_status(h);
+            if (h.stHost->err) {
+                const long long idx = h.stHost->errIndex;
+                lbib::reset_status(h, h.iteration, h.cellTypesCopied);
+                h.msg = "lbib_areas: cell " + std::to_string(idx) + " has more membrane nodes than one ring may hold";
+                h.errIndex = idx;
+                return -LBIB_ERR_CAPACITY;
+            }
+            h.areaFresh = true;
         }
         for (int c = 0; c < h.m.nCells && c < cap; ++c) {
             dom[c] = h.ringDomHost[c];
-            area[c] = h.areaHost[c];
+            area[c] = h.areaPinned[c];
         }
         return h.m.nCells;
     } catch (const HostFail& e) {
@@ -2386,8 +2430,7 @@ int lbib_areas_static(lbib_handle* hh, unsigned* dom, double* area, int cap) {
         // all-ones bytes read back as NaN: a cell the kernel leaves out shows
         // no value of an earlier call (or of another handle sharing the array)
         if (h.m.nCells > 0) CK(cudaMemsetAsync(scratch, 0xFF, sizeof(double) * h.m.nCells, h.stream));
-        if (!h.ringsCurrent) lbib::launch_rings(h.m, h.td, h.st, h.stream);
-        lbib::launch_areas(h.m, scratch, h.st, h.stream);
+        lbib::queue_areas(h, scratch);
         CK(cudaGetLastError());
         const int n = std::min(h.m.nCells, cap);
         if (n > 0) CK(cudaMemcpyAsync(area, scratch, sizeof(double) * n, cudaMemcpyDeviceToHost, h.stream));
@@ -2568,6 +2611,7 @@ int lbib_diff_forward(lbib_handle* hh, const double* memForce, const double* tau
         CK(cudaStreamSynchronize(h.stream));
     }
     d.outlet = outlet ? 1 : 0;
+    d.backwardDone = false;
     CK(cudaEventRecord(h.evA, h.stream));
     lbib::diff_forward(h, d);
     CK(cudaEventRecord(h.evB, h.stream));
@@ -2590,6 +2634,7 @@ int lbib_diff_backward(lbib_handle* hh, const double* dLdC, double* gForce, doub
     lbib::diff_backward(h, d);
     CK(cudaEventRecord(h.evB, h.stream));
     CK(cudaEventSynchronize(h.evB));
+    d.backwardDone = true;
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
     h.lastTotalMs = ms;
@@ -2613,6 +2658,74 @@ int lbib_diff_backward(lbib_handle* hh, const double* dLdC, double* gForce, doub
     API_END
 }
 
+int lbib_diff_force_params(lbib_handle* hh, double* gPar, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    try {
+        CK(cudaSetDevice(h.device));
+        if (!h.diff || !h.diff->backwardDone)
+            lbib::fail(LBIB_ERR_STATE, "lbib_diff_force_params before lbib_diff_backward");
+        if (cap < 0 || (cap > 0 && !gPar)) lbib::fail(LBIB_ERR_INPUT, "lbib_diff_force_params: bad output buffer");
+        lbib::pull_topology(h);
+        const int M = h.m.M;
+        int nrec = 0;
+        if (M) CK(cudaMemcpy(&nrec, h.m.foff + M, sizeof(int), cudaMemcpyDeviceToHost));
+        const int n = std::min(nrec, cap);
+        if (n > 0) {
+            double* g = nullptr;
+            CK(cudaMallocAsync((void**)&g, sizeof(double) * 4 * (size_t)nrec, h.stream));
+            lbib::launch_force_param_grad(h.m, h.diff->gfx, h.diff->gfy, g, h.stream);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(gPar, g, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaFreeAsync(g, h.stream));
+            CK(cudaStreamSynchronize(h.stream));
+        }
+        return nrec;
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index;
+        return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
+    }
+}
+
+int lbib_download_forces(lbib_handle* hh, int* type, unsigned* id1, unsigned* id2, double* par, int cap) {
+    if (!hh) return -LBIB_ERR_STATE;
+    Handle& h = hh->h;
+    if (h.err) return -h.err;
+    try {
+        CK(cudaSetDevice(h.device));
+        if (cap < 0 || (cap > 0 && (!type || !id1 || !id2 || !par)))
+            lbib::fail(LBIB_ERR_INPUT, "lbib_download_forces: bad output buffers");
+        lbib::pull_topology(h);
+        const int M = h.m.M;
+        std::vector<int> foff(M + 1, 0);
+        if (M) CK(cudaMemcpy(foff.data(), h.m.foff, sizeof(int) * (M + 1), cudaMemcpyDeviceToHost));
+        const int nrec = foff[M];
+        const int n = std::min(nrec, cap);
+        if (n > 0) {
+            std::vector<int> part(n);
+            CK(cudaMemcpy(type, h.m.ftype, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(part.data(), h.m.fpartner, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(par, h.m.fpar, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToHost));
+            for (int i = 0, r = 0; i < M && r < n; ++i)
+                for (; r < foff[i + 1] && r < n; ++r) {
+                    id1[r] = h.ids[i];
+                    id2[r] = part[r] >= 0 && part[r] < M ? h.ids[part[r]] : 0u;
+                }
+        }
+        return nrec;
+    } catch (const HostFail& e) {
+        h.err = e.code; h.msg = e.msg; h.errIndex = e.index;
+        return -e.code;
+    } catch (const std::exception& e) {
+        h.err = LBIB_ERR_INPUT; h.msg = e.what();
+        return -h.err;
+    }
+}
+
 int lbib_diff_mass(lbib_handle* hh, const double* mass, double* gMass, int n) {
     API_BEGIN(hh)
     if (!h.diff) lbib::fail(LBIB_ERR_STATE, "lbib_diff_mass outside a differentiated run");
@@ -2623,6 +2736,7 @@ int lbib_diff_mass(lbib_handle* hh, const double* mass, double* gMass, int n) {
         CK(cudaStreamSynchronize(h.stream));
         d.massUsed = true;
         d.forwardDone = false;
+        d.backwardDone = false;
     }
     if (gMass)
         for (int i = 0; i < n; ++i) gMass[i] = d.massUsed && i < (int)d.gmass.size() ? d.gmass[i] : 0.0;

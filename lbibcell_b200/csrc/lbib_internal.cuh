@@ -85,7 +85,7 @@ struct Status {
     int nFailedReinit; // reinit without any neighbour (division by zero)
     unsigned iteration;   // Parameters' current iteration of the step being run
     int cellTypesCopied;  // copyCellTypeToPhysicalNodes has run (after the first step)
-    int pad[4];           // [0] steps completed in a batch, [1] remesh RNG needs, [2] crossing records
+    int pad[4];           // [0] steps completed in a batch, [2] crossing records of the step
 };
 
 // Stage numbers (halt points), in the reference's order of
@@ -167,6 +167,9 @@ struct SpeciesConst {
     double dt;      // the solver's deltaT (SchnakenbergD2Q5u/v: 20 / Iterations; BMP: 1)
     double hill;    // RX_BMP: pow(k_hill, n_hill) as the host's pow gives it
     int bounce;     // DiracD2Q5: advect keeps the populations of links with a boundary node
+    // FP32 forms for the FP32-shifted kernel, set by its launcher from the
+    // fields above: (float)(1 / tau), (float)decay, (float)dt, (float)hill
+    float tIf, decayf, dtf, hillf;
 };
 
 // Boundary solvers on connections (the "bsolver cdesolver" pairs of a
@@ -205,6 +208,7 @@ struct LatticeArgs {
     const double* srcTab;      // [S][nDomains] production per step
     const uint32_t* ctypeTab;  // per-domain cell type (read by RX_BMP)
     double tauF;
+    float tauIf, gff;          // FP32-shifted kernel: (float)(1 / tauF), (float)(1 - 1 / (2 tauF)), set by its launcher
     int forceModel;            // FM_LUO, FM_GUO (as the reference writes it), FM_GUO_CORRECTED
     SpeciesConst sp[kMaxSpecies];
     int coupled;               // some species has a coupled_kind reaction

@@ -19,7 +19,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
-from typing import Dict, Optional
+from typing import Dict, Optional, Tuple
 
 import numpy as np
 
@@ -148,23 +148,39 @@ class Simulation:
         return c
 
     def areas(self) -> Dict[int, float]:
-        """GeometryHandler::computeAreas: {domain: area}.  The output buffers
-        are kept between calls (sized for the cell count plus room for
-        divisions), so a call is one round trip to the device."""
+        """GeometryHandler::computeAreas: {domain: area}."""
+        dom, area = self.areas_array()
+        return dict(zip(dom.tolist(), area.tolist()))
+
+    def areas_array(self) -> Tuple[np.ndarray, np.ndarray]:
+        """The same as two arrays (domain ids, areas) in the handle's cell
+        order, views of buffers kept between calls (sized for the cell count
+        plus room for divisions): valid until the next call.  Right after
+        step() with an area regulator registered the areas are already on
+        the host; otherwise the call is one round trip to the device."""
         for _ in range(2):
             cap = len(getattr(self, "_area_d", ()))
             if cap == 0:
                 cap = max(1, self.sizes()["cells"]) + 64
                 self._area_d = np.zeros(cap, np.uint32)
                 self._area_a = np.zeros(cap)
-            n = self._L.lbib_areas(self._h, _p(self._area_d), _p(self._area_a), cap)
-            if n < 0:
-                raise self._error()
+            n = self.areas_into(self._area_d, self._area_a)
             if n <= cap:
-                return {int(self._area_d[i]): float(self._area_a[i]) for i in range(n)}
+                return self._area_d[:n], self._area_a[:n]
             self._area_d = np.zeros(n + 64, np.uint32)
             self._area_a = np.zeros(n + 64)
         raise RuntimeError("lbib_areas: the cell count keeps changing")
+
+    def areas_into(self, dom: np.ndarray, area: np.ndarray) -> int:
+        """lbib_areas into caller-owned contiguous uint32 / float64 arrays
+        (pinned or not): fills min(count, len) entries, returns the count."""
+        if dom.dtype != np.uint32 or area.dtype != np.float64 or not (dom.flags.c_contiguous and
+                                                                     area.flags.c_contiguous):
+            raise ValueError("areas_into needs contiguous uint32 and float64 arrays")
+        n = self._L.lbib_areas(self._h, _p(dom), _p(area), min(len(dom), len(area)))
+        if n < 0:
+            raise self._error()
+        return n
 
     def accumulated_concentrations(self, species: str) -> Dict[int, float]:
         """GeometryHandler::computeAccumulatedDomainConcentrations(species)."""
@@ -312,6 +328,30 @@ class Simulation:
         the next backward passes; None removes it."""
         a = None if dLdf is None else np.ascontiguousarray(dLdf, np.float64)
         self._check(self._L.lbib_diff_fluid_seed(self._h, _p(a)))
+
+    def diff_force_params(self) -> np.ndarray:
+        """dL/d of every force record's four parameters ((n, 4), the order of
+        forces()) from the last backward pass's membrane-force gradient."""
+        n = self._L.lbib_diff_force_params(self._h, None, 0)
+        if n < 0:
+            raise self._error()
+        g = np.zeros((n, 4))
+        got = self._L.lbib_diff_force_params(self._h, _p(g), n)
+        if got < 0:
+            raise self._error()
+        return g
+
+    def forces(self) -> Dict[str, np.ndarray]:
+        """The ForceSolver's records in device order (by node, then insertion):
+        type, id1, id2 (partner id or 0) and par (n, 4)."""
+        n = self._L.lbib_download_forces(self._h, None, None, None, None, 0)
+        if n < 0:
+            raise self._error()
+        t = np.zeros(n, np.int32); a = np.zeros(n, np.uint32); b = np.zeros(n, np.uint32); par = np.zeros((n, 4))
+        got = self._L.lbib_download_forces(self._h, _p(t), _p(a), _p(b), _p(par), n)
+        if got < 0:
+            raise self._error()
+        return {"type": t, "id1": a, "id2": b, "par": par}
 
     def diff_end(self) -> None:
         """Restore the snapshot and free the run's checkpoints."""

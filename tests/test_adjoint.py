@@ -416,3 +416,93 @@ def test_mass_source_and_flow_loss_gradients(lbib, tmp_path):
     _close(float((g["force"] * v).sum()), fd, np.abs(g["force"] * v).sum(), "dL/dF . v")
     P.sim.diff_fluid_seed(None)
     P.sim.diff_end()
+
+
+def _node_forces(ids, xy, rec):
+    """ForceSolver::calculateForce restated for the test (ForceStructs.hpp
+    49-588): each record adds to its own node's force."""
+    index = {int(i): k for k, i in enumerate(ids)}
+    F = np.zeros((len(ids), 2))
+    for t, a, b, p in zip(rec["type"], rec["id1"], rec["id2"], rec["par"]):
+        i = index[int(a)]
+        x1, y1 = xy[i]
+        if t in (0, 7, 5, 6):
+            dx, dy = xy[index[int(b)]] - xy[i]
+            dist = np.sqrt(dx * dx + dy * dy)
+            f = p[0] * (dist - p[1]) if t in (0, 7) else p[0]
+            F[i] += (dx * f / dist, dy * f / dist)
+        elif t == 1:
+            dx, dy = p[0] - x1, p[1] - y1
+            dist = np.sqrt(dx * dx + dy * dy)
+            if dist != 0.0:
+                f = p[2] * (dist - p[3])
+                F[i] += (dx * f / dist, dy * f / dist)
+        elif t == 2:
+            F[i] += p[:2]
+        elif t == 3:
+            f = p[1] * (abs(p[0] - y1) - p[2])
+            F[i, 1] += f if y1 < p[0] else -f
+        elif t == 4:
+            f = p[1] * (abs(p[0] - x1) - p[2])
+            F[i, 0] += f if x1 < p[0] else -f
+    return F
+
+
+def test_force_record_parameter_gradients(lbib, tmp_path):
+    """The a11 chain rule: dL/d of force-record parameters (lbib_diff_force_params)
+    equals dL/dF . dF/dp of a numpy restatement of the force types (all eight),
+    and central differences of the whole run in the parameter (the node forces
+    re-formed from the perturbed records and passed as the run's forces)."""
+    cfg = _cfg()
+    cfg.tension = (0.05, 10)  # LbibMembraneTension: type-6 records on every node
+    paths = cfg.write(str(tmp_path))
+    P = _Problem(lbib, paths, T=20, K=5, steps_before=2)
+    sim = P.sim
+    ids, node = sim.membrane()
+    xy = node[:, :2].copy()
+    n = len(ids)
+    # one record of each other type on a few nodes (partners two nodes on)
+    extra = [(0, 0, 2, (0.02, 1.5, 0, 0)), (7, 5, 9, (0.01, 3.0, 0, 0)),
+             (1, 11, 0, (xy[11, 0] + 3.0, xy[11, 1] - 2.0, 0.02, 1.0)), (2, 17, 0, (1e-3, -2e-3, 0, 0)),
+             (3, 23, 0, (xy[23, 1] + 4.0, 0.02, 1.0, 0)), (4, 29, 0, (xy[29, 0] - 3.0, 0.015, 0.5, 0)),
+             (5, 31, 33, (2e-3, 0, 0, 0))]
+    sim.add_forces([e[0] for e in extra], [ids[e[1] % n] for e in extra], [ids[e[2] % n] for e in extra],
+                   np.array([e[3] for e in extra], float))
+    rec = sim.forces()
+    assert set(rec["type"].tolist()) == set(range(8))
+    F0 = _node_forces(ids, xy, rec)
+
+    def loss(par):
+        r = dict(rec, par=par)
+        return P.loss(F=_node_forces(ids, xy, r))
+
+    L0 = loss(rec["par"])
+    g = sim.diff_backward(P.w)
+    gp = sim.diff_force_params()
+    assert gp.shape == (len(rec["type"]), 4)
+    # the chain rule against a numpy differentiation of the restated forces
+    index = {int(i): k for k, i in enumerate(ids)}
+    for r in range(len(rec["type"])):
+        i = index[int(rec["id1"][r])]
+        for q in range(4):
+            h = 1e-6 * max(1.0, abs(rec["par"][r, q]))
+            pp, pm = rec["par"].copy(), rec["par"].copy()
+            pp[r, q] += h
+            pm[r, q] -= h
+            dF = (_node_forces(ids, xy, dict(rec, par=pp))[i] - _node_forces(ids, xy, dict(rec, par=pm))[i]) / (2 * h)
+            want = float(g["force"][i] @ dF)
+            assert abs(gp[r, q] - want) <= 1e-6 * abs(want) + 1e-12 * np.abs(gp).max(), (r, q, gp[r, q], want)
+    # central differences of the run in one parameter of each type
+    assert np.abs(F0 - _node_forces(ids, xy, rec)).max() == 0.0
+    checked = 0
+    for t, q in ((6, 0), (0, 0), (0, 1), (7, 1), (1, 0), (1, 2), (2, 1), (3, 0), (3, 1), (4, 2), (5, 0)):
+        r = int(np.nonzero(rec["type"] == t)[0][0])
+        h = 1e-6 * max(1.0, abs(rec["par"][r, q]))
+        pp, pm = rec["par"].copy(), rec["par"].copy()
+        pp[r, q] += h
+        pm[r, q] -= h
+        fd = (loss(pp) - loss(pm)) / (2 * h)
+        _close(gp[r, q], fd, np.abs(gp).max(), f"dL/dpar[type {t}, {q}]")
+        checked += 1
+    assert checked == 11 and np.isfinite(L0)
+    sim.diff_end()
