@@ -493,8 +493,9 @@ def main():
 
     # ---- end to end through the public API, host buffers each step ---------
     # every step: H2D of both species' per-domain secretion tables (what a host
-    # plugin pushes) from pinned memory, lbib_step(1), D2H of the per-cell areas.
-    nd = max(d for d, _ in cfg.cells) + 1
+    # plugin pushes) from pinned memory in one copy, lbib_step(1), D2H of the
+    # per-cell areas into pinned host arrays.
+    nd = sim.domain_count()
     pinned = torch.zeros((S, nd), dtype=torch.float64).pin_memory()
     for k, sp in enumerate(cfg.species):
         for d, r in sp.source.items():
@@ -511,8 +512,7 @@ def main():
     t0 = time.perf_counter()
     nareas = 0
     for _ in range(e2e_steps):
-        for k in range(S):
-            sim.set_species_source(k, src[k])
+        sim.set_species_sources(src)
         sim.step(1)
         nareas = sim.areas_into(area_dom, area_val)
     torch.cuda.synchronize()

@@ -108,9 +108,15 @@ int lbib_download_membrane(lbib_handle* h, unsigned* ids, double* state);
 int lbib_download_connections(lbib_handle* h, unsigned* conn);
 
 /* Cell areas (GeometryHandler::computeAreas, GeometryHandler.cpp:101-134):
- * dom[k], area[k] for k < return value (capped at cap). Negative on error:
- * -LBIB_ERR_CAPACITY (the handle stays usable) when a cell's ring holds more
- * than 4096 membrane nodes, the most one ring sum takes. */
+ * dom[k], area[k] for k < return value (capped at cap).  FP64 handles sum each
+ * ring in the reference's order; FP32-shifted handles sum each shoelace term
+ * rounded to 2^-24 in any order (exact, so deterministic; at most n 2^-26 from
+ * the ring-order sum for a cell of n nodes).  Right after lbib_step with an
+ * area regulator registered, the areas its bio stage formed were read back
+ * with the step's status word and the call does no device work.  Negative on
+ * error: -LBIB_ERR_CAPACITY (the handle stays usable) when, on an FP64
+ * handle, a cell's ring holds more than 4096 membrane nodes, the most one
+ * ring sum takes. */
 int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
 
 /* The same cell areas as lbib_areas, computed without any allocation: no
@@ -126,8 +132,8 @@ int lbib_areas(lbib_handle* h, unsigned* dom, double* area, int cap);
  * no value of an earlier call can come back, but calls that overlap in time
  * (two threads, or two handles on different streams) race on it and must be
  * serialised by the caller.  A cell whose ring holds more than 4096 nodes
- * gives -LBIB_ERR_CAPACITY with the cell's index in lbib_last_error (the
- * handle stays usable; area[] may then hold NaN).  The first call on a
+ * gives -LBIB_ERR_CAPACITY on an FP64 handle, with the cell's index in
+ * lbib_last_error (the handle stays usable; area[] may then hold NaN).  The first call on a
  * device looks up the array's address; make that call before any stream
  * capture.  Returns the number of cells, as lbib_areas. */
 int lbib_areas_static(lbib_handle* h, unsigned* dom, double* area, int cap);
@@ -158,6 +164,11 @@ int lbib_get_cell_types(lbib_handle* h, unsigned* dom, unsigned* type, int cap);
  * CDESolver state (e.g. tutorial_01_CDESolverD2Q5_SIGNAL.cpp:92-100, where the
  * production depends on the node's domain id). */
 int lbib_set_species_source(lbib_handle* h, int k, const double* rates, int n);
+
+/* The same for every species at once, in one host-to-device copy:
+ * rates[k * n + d] for species k (parameter-file order) and domain id d,
+ * n = lbib_get_domain_count. */
+int lbib_set_species_sources(lbib_handle* h, const double* rates, int n);
 
 /* Writes the simulation in the reference's four text formats, as
  * SimulationRunner::writeSimulation does (SimulationRunner.cpp:112-149):

@@ -66,8 +66,9 @@ def build_dropin(force: bool = False) -> str:
     srcs = sorted(f for f in dropin_sources() if f.endswith(".cpp"))
     cmd = [CXX, "-std=gnu++11", "-O2", "-fPIC", "-shared", "-Wall", "-I" + os.path.join(DROPIN, "include"),
            "-I" + os.path.join(os.path.dirname(HERE), "include")] + srcs + [
-        "-L" + HERE, "-llbibcuda", "-Wl,-rpath,$ORIGIN", "-o", DROPIN_LIB]
+        "-L" + HERE, "-llbibcuda", "-Wl,-rpath,$ORIGIN", "-o", DROPIN_LIB + ".tmp"]
     subprocess.run(cmd, check=True)
+    os.replace(DROPIN_LIB + ".tmp", DROPIN_LIB)
     return DROPIN_LIB
 
 
@@ -88,12 +89,16 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
         for r in [pool.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
             r.result()
     objs = [obj for _, obj in jobs]
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
+    # linked beside the library and renamed over it: a process that has the
+    # old one loaded keeps its mapping, and no reader sees a partial file
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + [
         "-Xcompiler", "-static-libstdc++", "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-Bsymbolic", "-Xlinker", "--no-undefined",
         "-cudart", "static"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
     build_dropin(force=True)
     return LIB
 

@@ -72,11 +72,14 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 
 }  // namespace
 
-// NS = number of species (compile-time, so that every input of a node is
-// loaded before any arithmetic).  Grid (ceil(nx / 256), ny).  The kernel
-// holds a node's whole forward and reverse state; LBIB_ADJOINT_MIN_BLOCKS
-// (blocks per SM the register budget is sized for) trades occupancy against
-// register spills.
+// NS = number of species (compile-time, so that the species' inputs are
+// loaded together with the fluid state).  Grid (ceil(nx / 256), ny).  The
+// fluid's adjoint inputs are loaded after the species' reverse pass and the
+// gradient accumulators where they are updated, so that a node's values are
+// not all live at once: with one species no register spills at the 128
+// registers of two blocks per SM.  LBIB_ADJOINT_MIN_BLOCKS (blocks per SM the
+// register budget is sized for) trades occupancy against spills (measured:
+// 2 is fastest).
 #ifndef LBIB_ADJOINT_MIN_BLOCKS
 #define LBIB_ADJOINT_MIN_BLOCKS 2
 #endif
@@ -95,26 +98,30 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const unsigned rC = (unsigned)y * nx, rM = (unsigned)ym * nx, rP = (unsigned)yp * nx;
     const unsigned n = rC + x;
-    // forward pull sources x - c_q and adjoint gather sources x + c_q (offsets within a plane)
-    const unsigned pull[9] = {rC + x, rC + xm, rM + x, rC + xp, rP + x, rM + xm, rM + xp, rP + xp, rP + xm};
-    const unsigned push[9] = {rC + x, rC + xp, rP + x, rC + xm, rM + x, rP + xp, rP + xm, rM + xm, rM + xp};
+    // forward pull sources x - c_q and adjoint gather sources x + c_q (offsets
+    // within a plane), formed where they are used
+    auto pull = [&](int q) -> unsigned {
+        const unsigned row = kCY[q] > 0 ? rM : (kCY[q] < 0 ? rP : rC);
+        return row + (kCX[q] > 0 ? xm : (kCX[q] < 0 ? xp : x));
+    };
+    auto push = [&](int q) -> unsigned {
+        const unsigned row = kCY[q] > 0 ? rP : (kCY[q] < 0 ? rM : rC);
+        return row + (kCX[q] > 0 ? xp : (kCX[q] < 0 ? xm : x));
+    };
 
-    // ---- every input of the node, loaded before any arithmetic -----------
+    // ---- the inputs of the forward recomputation and of the species ------
     const Real* __restrict__ fprev = (const Real*)a.fprev;
     double f[9], lf[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q)
-        f[q] = sizeof(Real) == 8 ? (double)fprev[(size_t)q * L + pull[q]]
-                                 : (double)fprev[(size_t)q * L + pull[q]] + weight9(q);
-#pragma unroll
-    for (int q = 0; q < 9; ++q)
-        lf[q] = a.seed ? (a.seedF ? a.seedF[(size_t)q * L + n] : 0.0) : (double)a.pf[(size_t)q * L + push[q]];
+        f[q] = sizeof(Real) == 8 ? (double)fprev[(size_t)q * L + pull(q)]
+                                 : (double)fprev[(size_t)q * L + pull(q)] + weight9(q);
     double gA[NS > 0 ? NS : 1][5], muA[NS > 0 ? NS : 1][5];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const Real* gp = (const Real*)a.gprev + (size_t)k * 5 * L;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) gA[k][q] = gp[(size_t)q * L + pull[q]];
+        for (int q = 0; q < 5; ++q) gA[k][q] = gp[(size_t)q * L + pull(q)];
         if (a.seed) {
             const double sd = a.seed[(size_t)k * L + n];
 #pragma unroll
@@ -122,23 +129,18 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
         } else {
             const float* pg = a.pg + (size_t)k * 5 * L;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) muA[k][q] = (double)pg[(size_t)q * L + push[q]];
+            for (int q = 0; q < 5; ++q) muA[k][q] = (double)pg[(size_t)q * L + push(q)];
         }
     }
     const uint32_t dom = a.dom[n];
     // The force field of a differentiated run is zero outside the force tiles,
     // so it and G are read and written everywhere: no load waits on another.
     const double fx = a.force[n], fy = a.force[L + n];
-    const double Gx = a.G[n], Gy = a.G[L + n];
-    double raccA[NS > 0 ? NS : 1];
-#pragma unroll
-    for (int k = 0; k < NS; ++k) raccA[k] = a.racc[(size_t)k * L + n];
     double gTauK[NS > 0 ? NS : 1];
     double rta = 0.0;
     if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
     const bool hasMass = a.macc != nullptr && a.massTab != nullptr && dom < (uint32_t)a.nDomains && isfinite(rta);
     if (!isfinite(rta)) rta = 0.0;
-    const double maccA = hasMass ? a.macc[n] : 0.0;
 
     // ---- forward recomputation of the fluid collision --------------------
     const double tauI = a.tauIF;
@@ -254,8 +256,14 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
             for (int q = 0; q < 5; ++q) qg[(size_t)q * L + n] = (float)((1.0 - tauIk) * mu[q] + mC);
         }
         gTauK[k] = valid ? gTau : 0.0;
-        if (valid && sp.kind == RX_LINEAR) a.racc[(size_t)k * L + n] = raccA[k] + mR;
+        if (valid && sp.kind == RX_LINEAR) a.racc[(size_t)k * L + n] += mR;
     }
+
+    // ---- the fluid's adjoint inputs, loaded once the species are done (the
+    // node's values are not all held at once: no register spills) ----------
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+        lf[q] = a.seed ? (a.seedF ? a.seedF[(size_t)q * L + n] : 0.0) : (double)a.pf[(size_t)q * L + push(q)];
 
     // ---- fluid: outlet, velocity output and collide, backwards -----------
     if (passes == 2) {
@@ -300,13 +308,13 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
     mrho -= (ux * mux + uy * muy) * rhoI;
     mrhoF += mrho;
     // rho = sum f + rhoToAdd: dL/d rhoToAdd = dL/d rho
-    if (valid && hasMass) a.macc[n] = maccA + mrho;
+    if (valid && hasMass) a.macc[n] += mrho;
     if (valid) {
 #pragma unroll
         for (int q = 0; q < 9; ++q)
             a.qf[(size_t)q * L + n] = (float)((1.0 - tauI) * lf[q] + mrhoF + kCX[q] * mjx + kCY[q] * mjy);
-        a.G[n] = Gx + mfx;
-        a.G[L + n] = Gy + mfy;
+        a.G[n] += mfx;
+        a.G[L + n] += mfy;
     }
     // relaxation-time gradients: block sums into this block's own slots (the
     // same slots every step), reduced over blocks once at the end of the pass

@@ -90,8 +90,16 @@ __device__ __forceinline__ void reaction_terms32(const SpeciesConst& sp, float s
 //   u'    = (sum c_q h_q' + F/2) / rho
 // with the reference's NE coefficient (-3 v_y in place of +6 v_y in the F_y
 // factor) for FM_GUO: G_NE * 9 v_y F_y less on NE.
+// Blocks per SM the kernel's register budget is sized for (a tuning knob,
+// chosen by measurement).  6 (40 registers, no spills, 48 warps per SM)
+// against the compiler's own 48 registers (5 blocks): tissue_1024 step
+// 177.0 -> 174.5 us, the kernel 37.4 -> 35.2 us inside the step; 8 (32
+// registers) spills and is slower.
+#ifndef LBIB_COLLIDE_MIN_BLOCKS
+#define LBIB_COLLIDE_MIN_BLOCKS 6
+#endif
 template <int NS, int MODE>
-__global__ void __launch_bounds__(256) stream_collide32(LatticeArgs<float> a) {
+__global__ void __launch_bounds__(256, LBIB_COLLIDE_MIN_BLOCKS) stream_collide32(LatticeArgs<float> a) {
     constexpr bool COUPLED = (MODE & 1) != 0;   // coupled species reactions
     constexpr bool MASSNODE = (MODE & 2) != 0;  // per-node mass source
     constexpr bool GUO = (MODE & 4) != 0;       // Guo force model

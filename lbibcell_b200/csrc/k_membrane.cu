@@ -62,21 +62,14 @@ __device__ __forceinline__ double dirac(const double dx, const double dy) {
 __device__ __forceinline__ int tile_agg_add(int* arr, int tile, bool valid);
 __device__ void tile_slot_node(const MembraneDev& m, TileDev& t, int i, bool ok, int nx, int ny, Status* st);
 
-// `begin`: also reset the step's counters (the first kernel of a step).
+// `begin`: the first kernel of a step (begin_step).
 // `slots`: also enter the node in the per-tile lists of the FP32-shifted
 // spread (the tile counts were cleared before the launch).
 __global__ void force_eval_kernel(MembraneDev m, Status* st, unsigned iteration, int begin, TileDev t, int nx,
                                   int ny, int slots) {
     pdl_wait();
     if (st->halt) return;
-    if (begin && blockIdx.x == 0 && threadIdx.x == 0) {
-        st->nPerturbNode = 0;
-        st->nPerturbConn = 0;
-        st->nChanged = 0;
-        st->nRecords = 0;
-        st->remesh = 0;
-        st->coarsen = 0;
-    }
+    if (begin && blockIdx.x == 0 && threadIdx.x == 0) begin_step(st);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.topo->M) return;
     const double x1 = m.x[i], y1 = m.y[i];
@@ -522,33 +515,41 @@ __global__ void __launch_bounds__(256) spread_fixed_kernel(MembraneDev m, TileDe
             sF[1][e] = m.fy[i];
         }
         __syncthreads();
-        for (int j = threadIdx.x; j < 16 * nc; j += blockDim.x) {
-            const int e = j >> 4, k = j & 15;
+        // one item per (node, slot row r): slots k = 4 r .. 4 r + 3 of the
+        // node's 16 (in a 4 x 4 stencil, column dx = r, rows dy = 0..3)
+        for (int j = threadIdx.x; j < 4 * nc; j += blockDim.x) {
+            const int e = j >> 2, r = j & 3;
             const int c = org[e];
             const int ox = (c & 0xff) - 4, oy = ((c >> 8) & 0xff) - 4, hx = (c >> 16) & 0xf, hy = (c >> 20) & 0xf;
-            int dx, dy;  // node of item k relative to the stencil origin
-            if (hx == 3 && hy == 3) {
-                dx = k >> 2;
-                dy = k & 3;
-            } else {
-                // wider stencil: the node bound to slot k (last writer of the slot)
-                const Stencil sc{ox + tileX0, ox + tileX0 + hx, oy + tileY0, oy + tileY0 + hy};
-                int xk, yk;
-                stencil_slot(sc, k, xk, yk);
-                if (xk < 0) continue;
-                dx = xk - sc.x0;
-                dy = yk - sc.y0;
+            const bool plain = hx == 3 && hy == 3;
+            if (plain && (unsigned)(ox + r) >= (unsigned)kTile) continue;  // the column lies outside the tile
+            const Stencil sc{ox + tileX0, ox + tileX0 + hx, oy + tileY0, oy + tileY0 + hy};
+            const double Fx = sF[0][e], Fy = sF[1][e];
+#pragma unroll
+            for (int t4 = 0; t4 < 4; ++t4) {
+                int dx, dy;  // node of slot k relative to the stencil origin
+                if (plain) {
+                    dx = r;
+                    dy = t4;
+                } else {
+                    // wider stencil: the node bound to slot k (last writer of the slot)
+                    int xk, yk;
+                    stencil_slot(sc, 4 * r + t4, xk, yk);
+                    if (xk < 0) continue;
+                    dx = xk - sc.x0;
+                    dy = yk - sc.y0;
+                }
+                const int lx = ox + dx, ly = oy + dy;
+                if ((unsigned)lx >= (unsigned)kTile || (unsigned)ly >= (unsigned)kTile) continue;
+                const double dl = (fa[e][dx] * fb[e][dy]) / 16.0;
+                const long long vx = __double2ll_rn(Fx * dl * kForceFix);
+                const long long vy = __double2ll_rn(Fy * dl * kForceFix);
+                const int node = ly * kTile + lx;
+                atomicAdd(&accHi[0][node], (int)(vx >> 22));
+                atomicAdd(&accLo[0][node], (unsigned)(vx & 0x3fffff));
+                atomicAdd(&accHi[1][node], (int)(vy >> 22));
+                atomicAdd(&accLo[1][node], (unsigned)(vy & 0x3fffff));
             }
-            const int lx = ox + dx, ly = oy + dy;
-            if ((unsigned)lx >= (unsigned)kTile || (unsigned)ly >= (unsigned)kTile) continue;
-            const double dl = (fa[e][dx] * fb[e][dy]) / 16.0;
-            const long long vx = __double2ll_rn(sF[0][e] * dl * kForceFix);
-            const long long vy = __double2ll_rn(sF[1][e] * dl * kForceFix);
-            const int node = ly * kTile + lx;
-            atomicAdd(&accHi[0][node], (int)(vx >> 22));
-            atomicAdd(&accLo[0][node], (unsigned)(vx & 0x3fffff));
-            atomicAdd(&accHi[1][node], (int)(vy >> 22));
-            atomicAdd(&accLo[1][node], (unsigned)(vy & 0x3fffff));
         }
     }
     __syncthreads();
@@ -1001,7 +1002,7 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     if (c.nfTab != nullptr) launch_pdl(noflux_reset_kernel, 1, 1024, 0, s, c);
     if (c.bounceW != nullptr) launch_pdl(bounce_reset_kernel, 1, 1024, 0, s, c);
     // the record count (st->pad[2]) is zero here: cleared with the status
-    // word before a run and by step_end_kernel after each step
+    // word before a run and by the first kernel of each step
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
     launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
     launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, ny, st);

@@ -84,7 +84,7 @@ __device__ __forceinline__ bool remesh_split(const MembraneDev& m, int c, bool& 
 // to finish forms the exclusive prefix of the block counts (t.rank[block]),
 // and decides: K = the total, or 0 with a halt when the pass would overflow
 // a buffer or needs the random generator (the host runs it then; so it does
-// a third pass, remesh_again_kernel).
+// a third pass, remesh_commit_kernel).
 __global__ void __launch_bounds__(kRemeshBlock) remesh_count_kernel(MembraneDev m, TopoDev t, Status* st) {
     pdl_wait();
     Topo* T = m.topo;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_apply_kernel(MembraneDev 
     const double x = (m.x[a] + m.x[b]) / 2, y = (m.y[a] + m.y[b]) / 2;
     m.x[j] = x; m.y[j] = y;
     m.ox[j] = x - 5.0; m.oy[j] = y - 5.0;   // GeometryNode.cpp:98-103
-    m.bx[j] = x; m.by[j] = y;               // bound by remesh_again_kernel
+    m.bx[j] = x; m.by[j] = y;               // bound at once (remesh_commit_kernel tests the edges)
     m.vx[j] = 0.0; m.vy[j] = 0.0; m.fx[j] = 0.0; m.fy[j] = 0.0;
     m.id[j] = T->maxId + 1 + (unsigned)r;
     m.next[a] = j; m.prev[j] = a; m.next[j] = b; m.prev[b] = j;
@@ -166,17 +166,39 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_apply_kernel(MembraneDev 
     t.ca2[base + 1] = j; t.cb2[base + 1] = b; t.cdom2[base + 1] = m.cdom[c]; t.cdesc2[base + 1] = m.cdesc[c];
 }
 
-// Copies the new connection list back; the last block to finish commits the
-// pass (every block has read K and C before any block counts itself done).
-__global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
+// Commits the pass: copies the new connection list back (the last block to
+// finish updates the counts; every block has read K, C and M before any block
+// counts itself done), and checks what comes next in the reference:
+//  - a connection of the new list still longer than MAXLENGTH (a split half
+//    of one longer than 2 * MAXLENGTH) needs another pass
+//    (SimulationRunner.cpp:190-199 repeats the remeshing); that rare case goes
+//    to the host;
+//  - the new nodes are bound to the lattice at once (GeometryHandler.cpp:
+//    427-428): their old position is 5 lu away, so they are never in their
+//    old unit cell, take their binding from the current position (set by the
+//    apply kernel) and the edge test of connectGeometryNodesToPhysicalNodes
+//    (GeometryHandler.cpp:618-644).  The nodes that existed before the pass
+//    were bound, and tested, by the crossing stage from the same positions.
+__global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, Status* st) {
     pdl_wait();
-    if (st->halt) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     Topo* T = m.topo;
-    const int K = T->K, C = T->C;
+    const int K = T->K;
     if (K == 0) return;
+    const int C = T->C, M = T->M;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < C + K) {
-        m.ca[c] = t.ca2[c]; m.cb[c] = t.cb2[c]; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
+        const int a = t.ca2[c], b = t.cb2[c];
+        m.ca[c] = a; m.cb[c] = b; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
+        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
+        if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
+    }
+    if (c < K) {
+        const int i = M + c;
+        const double X = m.x[i], Y = m.y[i];
+        if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
+        else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
+        else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
+        else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -192,45 +214,15 @@ __global__ void remesh_copy_kernel(MembraneDev m, TopoDev t, Status* st) {
     }
 }
 
-// After the device pass: a connection still longer than MAXLENGTH (a split
-// half of one longer than 2 * MAXLENGTH) needs another pass; that rare case
-// goes to the host, which repeats passes like SimulationRunner.cpp:190-199.
-// Then the new nodes are bound to the lattice at once
-// (GeometryHandler.cpp:427-428): their old position is 5 lu away, so the edge
-// test of connectGeometryNodesToPhysicalNodes applies (GeometryHandler.cpp:
-// 618-636); the other nodes pass it as they did after the move.
-__global__ void remesh_again_kernel(MembraneDev m, int nx, int ny, Status* st) {
-    pdl_wait();
-    if (st->halt) return;
-    const int stride = gridDim.x * blockDim.x;
-    const int C = m.topo->C, M = m.topo->M;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += stride) {
-        const int a = m.ca[c], b = m.cb[c];
-        const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-        if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
-    }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
-        const double X = m.x[i], Y = m.y[i], ox = m.ox[i], oy = m.oy[i];
-        const bool within = (X >= floor(ox)) && (X < ceil(ox)) && (Y <= ceil(oy)) && (Y > floor(oy));
-        if (within || st->halt) continue;
-        m.bx[i] = X;  // bound from the current position (GeometryHandler.cpp:637-643)
-        m.by[i] = Y;
-        if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
-        else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
-        else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
-        else if (Y + 2.0 > ny) raise_error(st, ERR_EDGE_N, i, ST_REMESH);
-    }
-}
-
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
     if (m.Ccap == 0) return 0;
     // the count and the apply kernel partition the connections alike
     const int cb = (m.Ccap + kRemeshBlock - 1) / kRemeshBlock;
     launch_pdl(remesh_count_kernel, cb, kRemeshBlock, 0, s, m, t, st);
     launch_pdl(remesh_apply_kernel, cb, kRemeshBlock, 0, s, m, t, st);
-    launch_pdl(remesh_copy_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, st);
-    launch_pdl(remesh_again_kernel, (std::max(m.Ccap, m.Mcap) + 255) / 256, 256, 0, s, m, nx, ny, st);
-    return 4;
+    // a pass runs only when C + K <= Ccap: this grid covers the new list
+    launch_pdl(remesh_commit_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, nx, ny, st);
+    return 3;
 }
 
 // ---------------------------------------------------------------------------

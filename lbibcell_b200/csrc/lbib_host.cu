@@ -172,6 +172,9 @@ struct DiffCtx {
     }
 };
 
+// Offset of the membrane counts (Topo) in the status allocation.
+constexpr size_t kTopoOffset = (sizeof(Status) + 63) / 64 * 64;
+
 struct Handle {
     // parameters
     int nx = 0, ny = 0, S = 0;
@@ -313,15 +316,14 @@ Handle::~Handle() {
     fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys); fr(cross.nfD);
     fr(cross.nfSpec); fr(cross.nfU); fr(cross.nfN); fr(nfTabDev);
     fr(cross.bounceW); fr(cross.bounceS); fr(cross.bounceKeys); fr(cross.bounceN);
-    fr(m.topo); fr(m.cdesc);
+    fr(m.cdesc);  // m.topo lives in the status allocation
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
     fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
     fr(td.connAlive); fr(td.ncA); fr(td.ncB); fr(td.ncDom); fr(td.ncDesc); fr(td.ncAlive); fr(td.cellOfDom);
     fr(td.firstConn); fr(td.cellCount); fr(td.cellStart); fr(td.cellFill); fr(td.members); fr(td.succ);
     fr(td.dist); fr(td.startNode); fr(td.scanTmp);
     fr(st);
-    if (stHost) cudaFreeHost(stHost);
-    if (topoHost) cudaFreeHost(topoHost);
+    if (stHost) cudaFreeHost(stHost);  // topoHost lives in the same block
     if (areaPinned) cudaFreeHost(areaPinned);
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
@@ -1079,24 +1081,11 @@ static LatticeArgs<Real> lattice_args(Handle& h, unsigned iteration, int parity)
     return a;
 }
 
+// The first kernel of a step without a membrane (with one, the force kernel).
 __global__ void step_begin_kernel(Status* st) {
     pdl_wait();
     if (st->halt) return;
-    st->nPerturbNode = 0;
-    st->nPerturbConn = 0;
-    st->nChanged = 0;
-    st->nRecords = 0;
-    st->remesh = 0;
-    st->coarsen = 0;
-}
-
-__global__ void step_end_kernel(Status* st) {
-    pdl_wait();
-    st->pad[2] = 0;  // the crossing records of this step are consumed
-    if (st->halt) return;
-    st->pad[0] += 1;  // steps completed in this batch
-    st->iteration += 1;  // Parameters++ (SimulationRunner.cpp:98)
-    st->cellTypesCopied = 1;
+    begin_step(st);
 }
 
 __global__ void iteration_inc_kernel(Status* st) {
@@ -1204,8 +1193,6 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
             }
         }
     }
-    launch_pdl(step_end_kernel, 1, 1, 0, s, h.st);
-    nl += 1;
     return nl;
 }
 
@@ -1223,8 +1210,7 @@ static int resume_stage(int stage) {
 // their `changed` flag says whether the ring order of the cell areas is stale
 // (remeshing or coarsening on the device set it; a ring rebuild clears it).
 static void read_status(Handle& h) {
-    CK(cudaMemcpyAsync(h.stHost, h.st, sizeof(Status), cudaMemcpyDeviceToHost, h.stream));
-    if (h.m.topo) CK(cudaMemcpyAsync(h.topoHost, h.m.topo, sizeof(Topo), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(h.stHost, h.st, kTopoOffset + sizeof(Topo), cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
     if (h.m.topo) h.ringsCurrent = h.topoHost->changed == 0;
 }
@@ -1266,6 +1252,7 @@ static void reset_status(Handle& h, unsigned it, bool cellTypesCopied) {
     std::memset(h.stHost, 0, sizeof(Status));
     h.stHost->iteration = it;
     h.stHost->cellTypesCopied = cellTypesCopied ? 1 : 0;
+    h.stHost->pad[3] = 1;  // the next step begins a run
     write_status(h);
 }
 
@@ -1391,6 +1378,12 @@ static void launch_step_graph(Handle& h, int parity, bool coarsenStep, int bioOp
         CK(cudaGraphDestroy(graph));
     }
     CK(cudaGraphLaunch(g.exec, h.stream));
+    if (check_launches()) {
+        const cudaError_t e = cudaStreamSynchronize(h.stream);
+        if (e != cudaSuccess)
+            std::fprintf(stderr, "lbib: step graph (parity %d, coarsen %d, bio ops %d) at iteration %u failed: %s\n",
+                         parity, coarsenStep ? 1 : 0, bioOps, h.iteration, cudaGetErrorString(e));
+    }
     h.launches += g.launches;
 }
 
@@ -1452,7 +1445,9 @@ static void run_steps(Handle& h, int n) {
         queue_step_areas(h);
         read_status(h);
         const Status st = *h.stHost;
-        const int done = st.pad[0];
+        // the first kernel of each step counted the step before it; the last
+        // step of the batch completed unless a halt is pending
+        const int done = st.pad[0] + (st.halt ? 0 : 1);
         if (prof) {
             for (int b = 0; b < std::min(done, B); ++b) {
                 float ms = 0;
@@ -1611,10 +1606,13 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.force, 0, 2 * h.L * rs, h.stream));
     h.dom = dalloc<uint32_t>(h.L);
     CK(cudaMemsetAsync(h.dom, 0, sizeof(uint32_t) * h.L, h.stream));
-    CK(cudaMalloc(&h.st, sizeof(Status)));
-    CK(cudaMallocHost(&h.stHost, sizeof(Status)));
-    CK(cudaMallocHost(&h.topoHost, sizeof(Topo)));
-    std::memset(h.topoHost, 0, sizeof(Topo));
+    // the status word and the membrane counts share one allocation (and one
+    // pinned host copy), so that one copy reads both back after a step
+    CK(cudaMalloc(&h.st, kTopoOffset + sizeof(Topo)));
+    CK(cudaMemsetAsync(h.st, 0, kTopoOffset + sizeof(Topo), h.stream));
+    CK(cudaMallocHost(&h.stHost, kTopoOffset + sizeof(Topo)));
+    std::memset(h.stHost, 0, kTopoOffset + sizeof(Topo));
+    h.topoHost = (Topo*)((char*)h.stHost + kTopoOffset);
     init_kernel_attributes();
     // LBIB_NO_GRAPHS=1 launches every stage kernel directly (no CUDA graphs)
     if (const char* e = std::getenv("LBIB_NO_GRAPHS")) h.useGraphs = !(e[0] == '1');
@@ -1659,7 +1657,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
         CK(cudaMemsetAsync(h.cross.bounceN, 0, sizeof(int), h.stream));
     }
 
-    h.m.topo = dalloc<Topo>(1);
+    h.m.topo = (Topo*)((char*)h.st + kTopoOffset);
 
     // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160), or for a
     // ".vtm" file loadGeometryVTK (Geometry.cpp:162-306, the choice made at
@@ -2532,6 +2530,15 @@ int lbib_set_species_source(lbib_handle* hh, int k, const double* rates, int n) 
         lbib::fail(LBIB_ERR_INPUT, "bad species index or table size");
     if (n > 0)
         CK(cudaMemcpyAsync(h.srcTab + (size_t)k * h.nDomains, rates, sizeof(double) * n, cudaMemcpyHostToDevice,
+                           h.stream));
+    API_END
+}
+
+int lbib_set_species_sources(lbib_handle* hh, const double* rates, int n) {
+    API_BEGIN(hh)
+    if (n != h.nDomains || (h.S > 0 && !rates)) lbib::fail(LBIB_ERR_INPUT, "rates must be S x domain count");
+    if (h.S > 0)
+        CK(cudaMemcpyAsync(h.srcTab, rates, sizeof(double) * (size_t)h.S * h.nDomains, cudaMemcpyHostToDevice,
                            h.stream));
     API_END
 }

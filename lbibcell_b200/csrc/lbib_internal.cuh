@@ -20,6 +20,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <utility>
 #include <cuda_runtime.h>
@@ -44,6 +45,18 @@ inline bool pdl_enabled() {
     return on;
 }
 
+// LBIB_CHECK_LAUNCHES=1, a fault diagnostic (off by default): every stage
+// kernel launched outside a graph (all of them with LBIB_NO_GRAPHS=1), and
+// every step graph, is waited for where it is launched, and a failure names
+// the kernel or the step on stderr.
+inline bool check_launches() {
+    static const bool on = [] {
+        const char* e = std::getenv("LBIB_CHECK_LAUNCHES");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                        Args&&... args) {
@@ -58,6 +71,19 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    if (check_launches()) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        if (cs == cudaStreamCaptureStatusNone) {
+            const cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) {
+                const char* name = "?";
+                cudaFuncGetName(&name, (const void*)kernel);
+                std::fprintf(stderr, "lbib: kernel %s (grid %u x %u, block %u) failed: %s\n", name, grid.x, grid.y,
+                             block.x, cudaGetErrorString(e));
+            }
+        }
+    }
 }
 
 // Direction tables: libs/LbmLib/include/Direction.hpp:34-44 and
@@ -85,7 +111,7 @@ struct Status {
     int nFailedReinit; // reinit without any neighbour (division by zero)
     unsigned iteration;   // Parameters' current iteration of the step being run
     int cellTypesCopied;  // copyCellTypeToPhysicalNodes has run (after the first step)
-    int pad[4];           // [0] steps completed in a batch, [2] crossing records of the step
+    int pad[4];           // [0] steps of a run completed before its current one, [2] crossing records of the step, [3] first step of a run
 };
 
 // Stage numbers (halt points), in the reference's order of
@@ -125,6 +151,30 @@ __device__ __forceinline__ void raise_error(Status* st, int code, int index, int
     if (atomicCAS(&st->err, 0, code) == 0) st->errIndex = index;
     atomicExch(&st->halt, 1);
     atomicCAS(&st->haltStage, 0, stage);
+}
+
+// The start of a step, run by thread 0 of the step's first kernel when no halt
+// is pending: the step before it in the same run is then complete, so it is
+// counted (Parameters++, SimulationRunner.cpp:98) before this step's kernels
+// read the iteration; then the step's counters are cleared.  pad[3], set with
+// the status word, marks the first step of a run, which has no predecessor
+// there.  (The host counts the run's last step itself: it completed unless a
+// halt is pending.)
+__device__ __forceinline__ void begin_step(Status* st) {
+    if (st->pad[3]) {
+        st->pad[3] = 0;
+    } else {
+        st->pad[0] += 1;
+        st->iteration += 1;
+        st->cellTypesCopied = 1;
+    }
+    st->pad[2] = 0;
+    st->nPerturbNode = 0;
+    st->nPerturbConn = 0;
+    st->nChanged = 0;
+    st->nRecords = 0;
+    st->remesh = 0;
+    st->coarsen = 0;
 }
 
 __device__ __forceinline__ void raise_halt(Status* st, int stage) {

@@ -101,6 +101,13 @@ class Simulation:
         r = np.ascontiguousarray(rates, np.float64)
         self._check(self._L.lbib_set_species_source(self._h, int(k), _p(r), int(r.size)))
 
+    def set_species_sources(self, rates: np.ndarray) -> None:
+        """Every species' per-domain production rate at once ((S, n_domains)),
+        one host-to-device copy; pinned host memory makes it asynchronous."""
+        r = np.ascontiguousarray(rates, np.float64)
+        n = r.shape[-1] if r.ndim else 0
+        self._check(self._L.lbib_set_species_sources(self._h, _p(r), int(n)))
+
     def set_profiling(self, on: bool) -> None:
         self._check(self._L.lbib_set_profiling(self._h, 1 if on else 0))
 
