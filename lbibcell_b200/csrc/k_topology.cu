@@ -82,15 +82,21 @@ __device__ __forceinline__ bool remesh_split(const MembraneDev& m, int c, bool& 
 // Pass decision.  Each block counts its connections to split (t.flag[block])
 // and the new nodes that need the random generator (T->nRng); the last block
 // to finish forms the exclusive prefix of the block counts (t.rank[block]),
-// and decides: K = the total, or 0 with a halt when the pass would overflow
-// a buffer or needs the random generator (the host runs it then; so it does
-// a third pass, remesh_commit_kernel).
+// and decides: K = the total, or 0 with a halt when the pass would overflow a
+// buffer (the host runs it then; so it does a third pass,
+// remesh_commit_kernel).  New nodes that need the random perturbation are
+// made on the device all the same and listed for the host, which perturbs
+// them before the pass is committed (remesh_commit_kernel).
 __global__ void __launch_bounds__(kRemeshBlock) remesh_count_kernel(MembraneDev m, TopoDev t, Status* st) {
     pdl_wait();
+    // a halted step leaves the counts alone (a pass may wait for the host's
+    // perturbation of its new nodes); no block of this kernel raises a halt
+    // before every block has read it, so all blocks return together
+    if (st->halt) return;
     Topo* T = m.topo;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool f = false, rng = false;
-    if (!st->halt && c < T->C) f = remesh_split(m, c, rng);
+    if (c < T->C) f = remesh_split(m, c, rng);
     const int cnt = __syncthreads_count(f);
     const int nr = __syncthreads_count(rng);
     __shared__ bool last;
@@ -117,9 +123,10 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_count_kernel(MembraneDev 
     }
     if (threadIdx.x == 0) {
         const int K = carry, C = T->C, M = T->M;
-        const int needRng = atomicExch(&T->nRng, 0);
-        const bool run = K > 0 && needRng == 0 && M + K <= m.Mcap && C + K <= m.Ccap;
+        const bool run = K > 0 && M + K <= m.Mcap && C + K <= m.Ccap;
         T->K = run ? K : 0;
+        if (!run) T->nRng = 0;  // kept for the apply and commit kernels of a pass that runs
+        T->rngFill = 0;
         T->done = 0;
         if (K > 0 && !run) raise_halt(st, ST_REMESH);
     }
@@ -161,6 +168,9 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_apply_kernel(MembraneDev 
     m.id[j] = T->maxId + 1 + (unsigned)r;
     m.next[a] = j; m.prev[j] = a; m.next[j] = b; m.prev[b] = j;
     m.foff[j + 1] = m.foff[M];              // new nodes carry no forces
+    // GeometryNode's constructor perturbs a node made on a lattice line or
+    // diagonal (GeometryNode.cpp:98-117): the host draws it, in id order
+    if (rng) t.rngList[atomicAdd(&T->rngFill, 1)] = j;
     const int base = C - K + 2 * r;
     t.ca2[base] = a; t.cb2[base] = j; t.cdom2[base] = m.cdom[c]; t.cdesc2[base] = m.cdesc[c];
     t.ca2[base + 1] = j; t.cb2[base + 1] = b; t.cdom2[base + 1] = m.cdom[c]; t.cdesc2[base + 1] = m.cdesc[c];
@@ -175,8 +185,8 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_apply_kernel(MembraneDev 
 //    to the host;
 //  - the new nodes are bound to the lattice at once (GeometryHandler.cpp:
 //    427-428): their old position is 5 lu away, so they are never in their
-//    old unit cell, take their binding from the current position (set by the
-//    apply kernel) and the edge test of connectGeometryNodesToPhysicalNodes
+//    old unit cell, take their binding from the current position (perturbed
+//    by the host where needed) and the edge test of connectGeometryNodesToPhysicalNodes
 //    (GeometryHandler.cpp:618-644).  The nodes that existed before the pass
 //    were bound, and tested, by the crossing stage from the same positions.
 __global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, Status* st) {
@@ -184,6 +194,11 @@ __global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, S
     Topo* T = m.topo;
     const int K = T->K;
     if (K == 0) return;
+    if (T->nRng > 0) {
+        // new nodes wait for the host's perturbation; the step resumes here
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_halt(st, ST_REMESH_RNG);
+        return;
+    }
     const int C = T->C, M = T->M;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < C + K) {
@@ -195,6 +210,8 @@ __global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, S
     if (c < K) {
         const int i = M + c;
         const double X = m.x[i], Y = m.y[i];
+        m.bx[i] = X;  // bound at its (perturbed) position
+        m.by[i] = Y;
         if (X - 2.0 < 0) raise_error(st, ERR_EDGE_W, i, ST_REMESH);
         else if (Y - 2.0 < 0) raise_error(st, ERR_EDGE_S, i, ST_REMESH);
         else if (X + 2.0 > nx) raise_error(st, ERR_EDGE_E, i, ST_REMESH);
@@ -214,15 +231,19 @@ __global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, S
     }
 }
 
-int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s) {
+int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s, bool commitOnly) {
     if (m.Ccap == 0) return 0;
-    // the count and the apply kernel partition the connections alike
-    const int cb = (m.Ccap + kRemeshBlock - 1) / kRemeshBlock;
-    launch_pdl(remesh_count_kernel, cb, kRemeshBlock, 0, s, m, t, st);
-    launch_pdl(remesh_apply_kernel, cb, kRemeshBlock, 0, s, m, t, st);
+    int n = 0;
+    if (!commitOnly) {
+        // the count and the apply kernel partition the connections alike
+        const int cb = (m.Ccap + kRemeshBlock - 1) / kRemeshBlock;
+        launch_pdl(remesh_count_kernel, cb, kRemeshBlock, 0, s, m, t, st);
+        launch_pdl(remesh_apply_kernel, cb, kRemeshBlock, 0, s, m, t, st);
+        n = 2;
+    }
     // a pass runs only when C + K <= Ccap: this grid covers the new list
     launch_pdl(remesh_commit_kernel, (m.Ccap + 255) / 256, 256, 0, s, m, t, nx, ny, st);
-    return 3;
+    return n + 1;
 }
 
 // ---------------------------------------------------------------------------

@@ -17,6 +17,7 @@ struct Topo {
     int nCand;        // coarsening candidates
     unsigned done;    // blocks of the remesh count / copy that have finished (the last one decides / commits)
     int nRng;         // new nodes of the remesh pass that need the random perturbation
+    int rngFill;      // entries of TopoDev::rngList (those nodes' indices)
 };
 
 // Membrane state on the device (nodes in ascending id order).
@@ -149,6 +150,7 @@ struct TopoDev {
     int* cellFill;      // nCells
     int* members;       // Mcap
     int* succ; int* dist;                                 // Mcap
+    int* rngList;       // Mcap: new nodes of a remesh pass that need the host's random perturbation
     int* startNode;     // nCells
     void* scanTmp; size_t scanTmpBytes;
     int nDomains;
@@ -252,7 +254,9 @@ cudaError_t static_area_scratch(double** ptr);
 
 // Device-side topology edits (k_topology.cu).  Each returns the number of
 // kernels it launched.
-int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s);
+// A remesh pass (count, apply, commit); commitOnly: the commit alone, after
+// the host perturbed the pass's new nodes (halt ST_REMESH_RNG).
+int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s, bool commitOnly = false);
 int launch_coarsen(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s);
 size_t topo_scan_bytes(int n);

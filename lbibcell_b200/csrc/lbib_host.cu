@@ -12,7 +12,9 @@
 // order and resumes the step at the stage after the one that halted.  Steps
 // without such events run with no host round trip.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -162,6 +164,7 @@ struct DiffCtx {
     int outlet = 0;
     unsigned it0 = 0;
     bool forwardDone = false;
+    bool lastSegKept = false;   // the forward left the last segment's states in seg
     bool backwardDone = false;  // gfx / gfy hold the last reverse pass's membrane-force gradient
     char* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateBytes; }
     ~DiffCtx() {
@@ -320,7 +323,7 @@ Handle::~Handle() {
     fr(td.flag); fr(td.rank); fr(td.nflag); fr(td.nrank); fr(td.ca2); fr(td.cb2); fr(td.cdom2); fr(td.cdesc2);
     fr(td.dalt); fr(td.id2); fr(td.prev2); fr(td.next2); fr(td.inConn); fr(td.outConn); fr(td.removed);
     fr(td.connAlive); fr(td.ncA); fr(td.ncB); fr(td.ncDom); fr(td.ncDesc); fr(td.ncAlive); fr(td.cellOfDom);
-    fr(td.firstConn); fr(td.cellCount); fr(td.cellStart); fr(td.cellFill); fr(td.members); fr(td.succ);
+    fr(td.firstConn); fr(td.cellCount); fr(td.cellStart); fr(td.cellFill); fr(td.members); fr(td.succ); fr(td.rngList);
     fr(td.dist); fr(td.startNode); fr(td.scanTmp);
     fr(st);
     if (stHost) cudaFreeHost(stHost);  // topoHost lives in the same block
@@ -845,7 +848,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         fr(h.m.foff); fr(h.m.ringNode); fr(h.tiles.list);
         fr(h.td.nflag); fr(h.td.nrank); fr(h.td.dalt); fr(h.td.id2); fr(h.td.prev2); fr(h.td.next2);
         fr(h.td.inConn); fr(h.td.outConn); fr(h.td.removed); fr(h.td.ncA); fr(h.td.ncB); fr(h.td.ncDom);
-        fr(h.td.ncDesc); fr(h.td.ncAlive); fr(h.td.members); fr(h.td.succ); fr(h.td.dist);
+        fr(h.td.ncDesc); fr(h.td.ncAlive); fr(h.td.members); fr(h.td.succ); fr(h.td.dist); fr(h.td.rngList);
         const int n = h.Mcap;
         h.td.nflag = dalloc<int>(n + 1); h.td.nrank = dalloc<int>(n + 1);
         h.td.dalt = dalloc<double>(10 * (size_t)n);
@@ -857,6 +860,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.td.ncDesc = dalloc<int>(n); h.td.ncAlive = dalloc<int>(n + 1);
         CK(cudaMemsetAsync(h.td.ncAlive, 0, sizeof(int) * (n + 1), h.stream));
         h.td.members = dalloc<int>(n); h.td.succ = dalloc<int>(n + 1); h.td.dist = dalloc<int>(n + 1);
+        h.td.rngList = dalloc<int>(n);
         h.m.x = dalloc<double>(n); h.m.y = dalloc<double>(n); h.m.ox = dalloc<double>(n); h.m.oy = dalloc<double>(n);
         h.m.bx = dalloc<double>(n); h.m.by = dalloc<double>(n);
         h.m.vx = dalloc<double>(n); h.m.vy = dalloc<double>(n); h.m.fx = dalloc<double>(n); h.m.fy = dalloc<double>(n);
@@ -1151,7 +1155,8 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
         launch_domain_fill(h.cross, h.dom, h.nx, h.ny, h.L, h.st, it, s);
         nl += 1;
     }
-    if (fromStage <= ST_REMESH) nl += launch_remesh(h.m, h.td, h.nx, h.ny, h.st, s);
+    if (fromStage <= ST_REMESH_COMMIT)
+        nl += launch_remesh(h.m, h.td, h.nx, h.ny, h.st, s, fromStage == ST_REMESH_COMMIT);
     if (fromStage <= ST_COARSEN && coarsenStep) {
         // SimulationRunner.cpp:84-87: ForceSolver::deleteAllForces, then coarsenBoundary
         launch_clear_forces(h.m, s);
@@ -1202,6 +1207,7 @@ static int resume_stage(int stage) {
         case ST_INTERP_MOVE: return ST_PERTURB_CONN;
         case ST_PERTURB_CONN: return ST_CROSSINGS;
         case ST_REMESH: return ST_COARSEN;
+        case ST_REMESH_RNG: return ST_REMESH_COMMIT;
         default: return -1;
     }
 }
@@ -1301,23 +1307,80 @@ static int step_bio_ops(const Handle& h, unsigned it) {
     return ops;
 }
 
+// The new nodes of a remesh pass that were made on a lattice line or
+// diagonal: GeometryNode's constructor perturbs them when remeshBoundary
+// creates them (GeometryNode.cpp:98-117, GeometryHandler.cpp:385-431), drawing
+// from the node generator in creation (= id) order.  The device made the
+// pass's nodes and listed these; the host draws their perturbation from the
+// same generator and the device then commits the pass.  Only the pass's new
+// positions cross the bus.
+static void perturb_new_nodes(Handle& h) {
+    const Topo tp = *h.topoHost;  // read back with the status word
+    const int M = tp.M, K = tp.K, n = tp.rngFill;
+    if (K <= 0 || n <= 0 || n > K || M + K > h.Mcap) fail(ERR_STATE, "remesh: bad list of new nodes to perturb");
+    std::vector<int> list(n);
+    std::vector<double> x(K), y(K);
+    CK(cudaMemcpyAsync(list.data(), h.td.rngList, sizeof(int) * n, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(x.data(), h.m.x + M, sizeof(double) * K, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaMemcpyAsync(y.data(), h.m.y + M, sizeof(double) * K, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    std::sort(list.begin(), list.end());
+    for (int j : list) {
+        if (j < M || j >= M + K) fail(ERR_STATE, "remesh: new node index out of the pass", j);
+        perturbate(h, x[j - M], y[j - M]);
+    }
+    CK(cudaMemcpyAsync(h.m.x + M, x.data(), sizeof(double) * K, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.m.y + M, y.data(), sizeof(double) * K, cudaMemcpyHostToDevice, h.stream));
+    const int zero[2] = {0, 0};  // nRng, rngFill: the commit goes ahead
+    static_assert(offsetof(Topo, rngFill) == offsetof(Topo, nRng) + sizeof(int), "Topo field order");
+    CK(cudaMemcpyAsync((char*)h.m.topo + offsetof(Topo, nRng), zero, sizeof zero, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+// LBIB_LOG_HOST_EVENTS=1 prints each host event's stage and duration to
+// stderr (a diagnostic, off by default).
+static bool log_host_events() {
+    static const bool on = [] {
+        const char* e = std::getenv("LBIB_LOG_HOST_EVENTS");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 // The host side of a halted stage, in the reference's order.
 static void handle_halt(Handle& h, int stage) {
     h.hostEvents++;
-    pull_topology(h);
-    HostMembrane hm;
+    if (stage == ST_REMESH_RNG) {
+        perturb_new_nodes(h);
+        return;
+    }
     if (stage == ST_INTERP_MOVE) {
-        // positions that need GeometryNode::perturbatePosition, in id order
+        // positions that need GeometryNode::perturbatePosition, in id order;
+        // only those nodes' positions cross the bus
         const int cnt = h.stHost->nPerturbNode;
         if (cnt > h.cross.perturbCap) fail(ERR_CAPACITY, "perturbation list overflow");
         std::vector<int> list(cnt);
         if (cnt) CK(cudaMemcpyAsync(list.data(), h.cross.perturbList, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h.stream));
-        download_membrane(h, hm);
+        CK(cudaStreamSynchronize(h.stream));
         std::sort(list.begin(), list.end());
-        for (int i : list) perturbate(h, hm.x[i], hm.y[i]);
-        CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
-        CK(cudaMemcpyAsync(h.m.y, hm.y.data(), sizeof(double) * hm.y.size(), cudaMemcpyHostToDevice, h.stream));
-    } else if (stage == ST_PERTURB_CONN) {
+        std::vector<double> xy(2 * (size_t)cnt);
+        for (int k = 0; k < cnt; ++k) {
+            if (list[k] < 0 || list[k] >= h.Mcap) fail(ERR_STATE, "perturbation list entry out of range", list[k]);
+            CK(cudaMemcpyAsync(&xy[2 * k], h.m.x + list[k], sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+            CK(cudaMemcpyAsync(&xy[2 * k + 1], h.m.y + list[k], sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+        }
+        CK(cudaStreamSynchronize(h.stream));
+        for (int k = 0; k < cnt; ++k) perturbate(h, xy[2 * k], xy[2 * k + 1]);
+        for (int k = 0; k < cnt; ++k) {
+            CK(cudaMemcpyAsync(h.m.x + list[k], &xy[2 * k], sizeof(double), cudaMemcpyHostToDevice, h.stream));
+            CK(cudaMemcpyAsync(h.m.y + list[k], &xy[2 * k + 1], sizeof(double), cudaMemcpyHostToDevice, h.stream));
+        }
+        CK(cudaStreamSynchronize(h.stream));
+        return;
+    }
+    pull_topology(h);
+    HostMembrane hm;
+    if (stage == ST_PERTURB_CONN) {
         download_membrane(h, hm);
         perturb_connections(h, hm);
         CK(cudaMemcpyAsync(h.m.x, hm.x.data(), sizeof(double) * hm.x.size(), cudaMemcpyHostToDevice, h.stream));
@@ -1476,7 +1539,11 @@ static void run_steps(Handle& h, int n) {
         int stage = st.haltStage;
         const unsigned it = h.iteration;
         for (;;) {
+            const auto t0 = std::chrono::steady_clock::now();
             handle_halt(h, stage);
+            if (log_host_events())
+                std::fprintf(stderr, "lbib: host event at stage %d, iteration %u: %.3f ms\n", stage, it,
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
             const int from = resume_stage(stage);
             if (from < 0) fail(ERR_STATE, "unexpected halt stage");
             reset_status(h, it, h.cellTypesCopied);
@@ -1975,13 +2042,20 @@ static void diff_forward(Handle& h, DiffCtx& d) {
     // buffer, free during the forward pass; with K = 2 one is enough, with
     // K = 1 every state but the last is a checkpoint)
     char* scratch[2] = {d.seg, d.K > 2 ? d.seg + d.stateBytes : d.seg};
+    // the last segment's states go where the reverse pass reads them, so that
+    // it need not recompute that segment
+    const int lastBase = (d.nSeg - 1) * d.K;
     const char* in = d.x0;
     char* out = nullptr;
     for (int t = 1; t <= d.T; ++t) {
-        out = (t % d.K == 0 && t < d.T) ? d.state(t / d.K) : (t == d.T ? d.fin : scratch[t & 1]);
+        if (t % d.K == 0 && t < d.T) out = d.state(t / d.K);
+        else if (t == d.T) out = d.fin;
+        else if (t > lastBase) out = d.seg + (size_t)(t - lastBase - 1) * d.stateBytes;
+        else out = scratch[t & 1];
         diff_forward_step(h, d, in, out, t);
         in = out;
     }
+    d.lastSegKept = true;
     // the final state and the force field become the handle's lattice, for
     // lbib_download_lattice
     if (d.rs == 8) CK(cudaMemcpyAsync(h.force, d.force, sizeof(double) * 2 * L, cudaMemcpyDeviceToDevice, h.stream));
@@ -2028,7 +2102,9 @@ static void diff_backward(Handle& h, DiffCtx& d) {
         auto segState = [&](int j) -> char* {  // state base + j, 0 <= j < len
             return j == 0 ? d.state(s) : d.seg + (size_t)(j - 1) * d.stateBytes;
         };
-        for (int j = 1; j < len; ++j) diff_forward_step(h, d, segState(j - 1), segState(j), base + j);
+        if (!(s == d.nSeg - 1 && d.lastSegKept))
+            for (int j = 1; j < len; ++j) diff_forward_step(h, d, segState(j - 1), segState(j), base + j);
+        if (s < d.nSeg - 1) d.lastSegKept = false;  // seg now holds an earlier segment
         for (int t = base + len; t > base; --t) {
             const char* prev = segState(t - 1 - base);
             a.fprev = prev;

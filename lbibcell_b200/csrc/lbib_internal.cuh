@@ -126,10 +126,12 @@ enum Stage {
     ST_REINIT = 7,
     ST_DOMAIN = 8,
     ST_REMESH = 9,
-    ST_COARSEN = 10,
-    ST_OUTLET = 11,
-    ST_BIO = 12,
-    ST_DONE = 13,
+    ST_REMESH_COMMIT = 10,  // the remesh pass's commit (resumed at after the host perturbed its new nodes)
+    ST_COARSEN = 11,
+    ST_OUTLET = 12,
+    ST_BIO = 13,
+    ST_DONE = 14,
+    ST_REMESH_RNG = 15,     // halt only: new nodes of the remesh pass need the host's random perturbation
 };
 
 // Error codes (also returned through the C ABI, include/lbibcell.h).

@@ -3,6 +3,7 @@ reference build).  FP64 results must be identical; FP32-shifted results are
 checked against the FP64 path with stated tolerances."""
 import json
 import hashlib
+import math
 import os
 
 import numpy as np
@@ -115,6 +116,34 @@ def test_stencil_binding_kept_in_unit_cell_fp64(lbib, oracle_mod, tmp_path):
         dumps = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
         done = 20
         for t in (20, 40, 60):
+            sim.step(t - done)
+            done = t
+            _compare_state(sim, dumps[t])
+
+
+def test_remesh_new_nodes_on_lattice_lines_fp64(lbib, oracle_mod, tmp_path):
+    """A circle whose first remeshing makes new nodes on lattice lines: 120
+    nodes at odd multiples of pi/120 around a lattice node put the midpoints
+    at angles 0 and pi on the line y = 32 (to rounding), so GeometryNode's
+    constructor perturbs them from the node generator.  The device makes the
+    pass, the host draws those nodes' perturbation, the device commits it:
+    identical to the oracle after each of the first 5 steps and to the
+    reference build at t = 10 and 20."""
+    cfg = configs.toy(n=64, r=12.0, nodes=120, iterations=20, report_step=10, species=1)
+    cfg.cells = [(1, configs.circle(32.0, 32.0, 12.0, 120, phase=math.pi / 120))]
+    paths = cfg.write(str(tmp_path / "cfg"))
+    sim = lbib.Simulation(paths, lbib.FP64)
+    o = oracle_mod.Oracle(paths)
+    events = sim.sizes()["host_events"]
+    for _ in range(5):
+        sim.step(1)
+        o.step(1)
+        _compare_state(sim, o.state())
+    assert sim.sizes()["host_events"] > events  # the perturbation handoff ran
+    if os.path.exists(oracle_mod.REF_DRIVER):
+        dumps = oracle_mod.run_reference(paths, str(tmp_path / "ref"))
+        done = 5
+        for t in (10, 20):
             sim.step(t - done)
             done = t
             _compare_state(sim, dumps[t])
