@@ -703,21 +703,27 @@ void launch_force_adjoint(const MembraneDev& m, const double* G, int nx, int ny,
 }
 
 // Connection::perturbConnection's tests (Connection.cpp:339, 363).
-__global__ void perturb_conn_kernel(MembraneDev m, Status* st) {
+// Connections whose end points share an x or a y to within EPSILON
+// (Connection::perturbConnection's tests, Connection.cpp:339-340, 363-364) are
+// counted and listed (up to cap); the crossing kernel, the next, raises the
+// halt, so that every block here sees the same halt word and the list is
+// complete.
+__global__ void perturb_conn_kernel(MembraneDev m, Status* st, int* list, int cap) {
     pdl_wait();
     if (st->halt) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.topo->C) return;
     const int a = m.ca[c], b = m.cb[c];
     if (fabs(m.x[a] - m.x[b]) < kEPSILON || fabs(m.y[a] - m.y[b]) < kEPSILON) {
-        atomicAdd(&st->nPerturbConn, 1);
-        raise_halt(st, ST_PERTURB_CONN);
+        const int k = atomicAdd(&st->nPerturbConn, 1);
+        if (k < cap) list[k] = c;
     }
 }
 
-void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s) {
+void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, int* list,
+                               int cap) {
     if (m.Ccap == 0) return;
-    launch_pdl(perturb_conn_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, st);
+    launch_pdl(perturb_conn_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, st, list, cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -832,6 +838,11 @@ __device__ __forceinline__ int for_each_record(const MembraneDev& m, int cn, int
 __global__ void crossings_kernel(MembraneDev m, CrossDev c, int nx, int ny, Status* st) {
     pdl_wait();
     if (st->halt) return;
+    if (st->nPerturbConn > 0) {
+        // connections to perturb first (perturb_conn_kernel): the host does it
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_halt(st, ST_PERTURB_CONN);
+        return;
+    }
     const int cn = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = cn < m.topo->C;
     int nrec = 0;

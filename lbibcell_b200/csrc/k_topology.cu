@@ -574,6 +574,44 @@ __global__ void ring_done_kernel(MembraneDev m, TopoDev t) {
     if (d == 0) m.topo->changed = 0;
 }
 
+// The listed connections to perturb (perturb_conn_kernel, t.rngList), each
+// with its place in its cell's ring walk (the rings are current: the host
+// rebuilds them first when the topology changed).  The walk visits the
+// connection leaving the ring's last node first (the domain's first
+// connection), then those leaving ranks 0, 1, ..., len - 2.
+__global__ void conn_perturb_gather_kernel(MembraneDev m, TopoDev t, int n, ConnPerturbRec* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int c = t.rngList[k];
+    ConnPerturbRec r{};
+    r.a = m.ca[c];
+    r.b = m.cb[c];
+    r.dom = (int)m.cdom[c];
+    r.xa = m.x[r.a]; r.ya = m.y[r.a]; r.xb = m.x[r.b]; r.yb = m.y[r.b];
+    r.walk = -1;
+    r.z = -1;
+    const int cell = (uint32_t)r.dom < (uint32_t)t.nDomains ? t.cellOfDom[r.dom] : -1;
+    if (cell >= 0 && cell < m.nCells) {
+        const int s0 = m.ringStart[cell], len = m.ringStart[cell + 1] - s0;
+        int rank = -1;
+        for (int j = 0; j < len; ++j)
+            if (m.ringNode[s0 + j] == r.a) { rank = j; break; }
+        if (rank >= 0 && len >= 2) {
+            r.len = len;
+            r.walk = rank == len - 1 ? 0 : rank + 1;
+            r.z = m.ringNode[s0 + len - 2];
+            r.xz = m.x[r.z];
+            r.yz = m.y[r.z];
+        }
+    }
+    out[k] = r;
+}
+
+void launch_conn_perturb_gather(const MembraneDev& m, const TopoDev& t, int n, ConnPerturbRec* out, cudaStream_t s) {
+    if (n <= 0) return;
+    conn_perturb_gather_kernel<<<(n + 127) / 128, 128, 0, s>>>(m, t, n, out);
+}
+
 int launch_rings(MembraneDev& m, TopoDev& t, Status* st, cudaStream_t s) {
     const int nCells = t.nCellsCap;
     if (m.Mcap == 0 || nCells == 0) return 0;
@@ -595,6 +633,9 @@ namespace lbib {
 
 void init_kernel_attributes_topology() {
     cudaFuncSetAttribute(coarsen_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarsenSmem);
+    // loaded now rather than at a host event's first use (modules load lazily)
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, conn_perturb_gather_kernel);
 }
 
 }  // namespace lbib

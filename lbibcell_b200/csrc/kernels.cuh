@@ -184,7 +184,8 @@ void launch_spread(const MembraneDev& m, TileDev& t, Real* force, int nx, int ny
 template <typename Real>
 void launch_interp_move(const MembraneDev& m, const Real* u, int nx, int ny, size_t L, CrossDev& c, Status* st,
                         unsigned iteration, cudaStream_t s);
-void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s);
+void launch_perturb_conn_check(const MembraneDev& m, Status* st, unsigned iteration, cudaStream_t s, int* list,
+                               int cap);
 template <typename Real>
 void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, int nx, int ny, size_t L, Status* st,
                       unsigned iteration, cudaStream_t s);
@@ -254,6 +255,19 @@ cudaError_t static_area_scratch(double** ptr);
 
 // Device-side topology edits (k_topology.cu).  Each returns the number of
 // kernels it launched.
+// A connection to perturb (Connection::perturbConnection), with what the host
+// needs to do it in GeometryHandler::perturbConnections' order
+// (GeometryHandler.cpp:326-356): its cell's ring walk starts at the domain's
+// first connection in vector order and follows the second node's outgoing
+// connection; walk = the connection's place in that walk (-1: no ring found),
+// len = the ring's length, z = the first node of the walk's last connection
+// (whose second node is the walk's first node).
+struct ConnPerturbRec {
+    int dom, walk, len, a, b, z;
+    double xa, ya, xb, yb, xz, yz;
+};
+void launch_conn_perturb_gather(const MembraneDev& m, const TopoDev& t, int n, ConnPerturbRec* out, cudaStream_t s);
+
 // A remesh pass (count, apply, commit); commitOnly: the commit alone, after
 // the host perturbed the pass's new nodes (halt ST_REMESH_RNG).
 int launch_remesh(MembraneDev& m, TopoDev& t, int nx, int ny, Status* st, cudaStream_t s, bool commitOnly = false);

@@ -255,6 +255,11 @@ struct Handle {
     // are the areas of the current state (any other API call clears it)
     double* areaPinned = nullptr;
     bool areaFresh = false;
+    // LBIB_FULL_HOST_EVENTS=1 at creation: host events take the whole
+    // membrane to the host (the reference's algorithms on a full copy) instead
+    // of the listed nodes and connections only (a cross-check of the latter)
+    bool fullHostEvents = false;
+    bool workAfterEvB = false;  // GPU work was issued after the step loop's last timing event
     cudaStream_t stream = nullptr;
 
     std::mt19937 genNode{1};
@@ -1137,7 +1142,7 @@ static long long launch_stages(Handle& h, bool coarsenStep, int bioOps, int pari
         nl += hasM;
     }
     if (fromStage <= ST_PERTURB_CONN) {
-        launch_perturb_conn_check(h.m, h.st, it, s);
+        launch_perturb_conn_check(h.m, h.st, it, s, h.td.rngList, h.Mcap);
         nl += hasM;
     }
     if (fromStage <= ST_CROSSINGS) {
@@ -1337,23 +1342,97 @@ static void perturb_new_nodes(Handle& h) {
     CK(cudaStreamSynchronize(h.stream));
 }
 
+// GeometryHandler::perturbConnections (GeometryHandler.cpp:326-356) from the
+// device's list of connections that need it, without the whole membrane.  A
+// perturbation moves only the first node of its connection, which is the
+// second node of the connection before it in the ring walk: that one was
+// visited already, except for the walk's last connection (into the walk's
+// first node), which is tested again here when the first one moved.  So the
+// listed connections, visited in (domain, walk) order, with the ring-closing
+// test, draw exactly what the reference's full walk draws.  Returns false
+// (the caller takes the full path) when the list overflowed or a connection's
+// ring was not found.
+static bool perturb_listed_connections(Handle& h) {
+    const int n = h.stHost->nPerturbConn;
+    if (n <= 0 || n > h.Mcap) return false;
+    launch_rings(h.m, h.td, h.st, h.stream);  // a no-op when they are current
+    // the records go to the coarsening's node scratch (10 doubles per node of
+    // capacity), free until this step's coarsening
+    static_assert(sizeof(ConnPerturbRec) <= 10 * sizeof(double), "record larger than the scratch per node");
+    ConnPerturbRec* dev = reinterpret_cast<ConnPerturbRec*>(h.td.dalt);
+    launch_conn_perturb_gather(h.m, h.td, n, dev, h.stream);
+    CK(cudaGetLastError());
+    std::vector<ConnPerturbRec> rec(n);
+    CK(cudaMemcpyAsync(rec.data(), dev, sizeof(ConnPerturbRec) * n, cudaMemcpyDeviceToHost, h.stream));
+    read_status(h);
+    if (h.stHost->err) fail(h.stHost->err, "ring order for the connection perturbation", h.stHost->errIndex);
+    for (const ConnPerturbRec& r : rec)
+        if (r.walk < 0) return false;
+    std::sort(rec.begin(), rec.end(), [](const ConnPerturbRec& p, const ConnPerturbRec& q) {
+        return p.dom != q.dom ? p.dom < q.dom : p.walk < q.walk;
+    });
+    std::map<int, std::pair<double, double>> pos;  // node index -> current position
+    for (const ConnPerturbRec& r : rec) {
+        pos.emplace(r.a, std::make_pair(r.xa, r.ya));
+        pos.emplace(r.b, std::make_pair(r.xb, r.yb));
+        pos.emplace(r.z, std::make_pair(r.xz, r.yz));
+    }
+    std::map<int, std::pair<double, double>> moved;
+    auto perturb = [&](int a, int b) {  // Connection::perturbConnection (Connection.cpp:332-387)
+        auto& pa = pos.at(a);
+        const auto& pb = pos.at(b);
+        double r;
+        if (std::abs(pa.first - pb.first) < kEPSILON) {
+            r = 0.0;
+            while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genConn);
+            pa.first = pa.first + r;
+            perturbate(h, pa.first, pa.second);
+            moved[a] = pa;
+        }
+        if (std::abs(pa.second - pos.at(b).second) < kEPSILON) {
+            r = 0.0;
+            while (std::abs(r) < 5.0 * kEPSILON) r = h.dis(h.genConn);
+            pa.second = pa.second + r;
+            perturbate(h, pa.first, pa.second);
+            moved[a] = pa;
+        }
+    };
+    for (size_t i = 0; i < rec.size();) {
+        size_t j = i;
+        bool closingListed = false;
+        while (j < rec.size() && rec[j].dom == rec[i].dom) {
+            perturb(rec[j].a, rec[j].b);
+            closingListed |= rec[j].walk == rec[j].len - 1;
+            ++j;
+        }
+        // the walk's last connection (z -> first node), when the first moved
+        if (rec[i].walk == 0 && !closingListed && moved.count(rec[i].a)) perturb(rec[i].z, rec[i].a);
+        i = j;
+    }
+    for (const auto& kv : moved) {
+        CK(cudaMemcpyAsync(h.m.x + kv.first, &kv.second.first, sizeof(double), cudaMemcpyHostToDevice, h.stream));
+        CK(cudaMemcpyAsync(h.m.y + kv.first, &kv.second.second, sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    }
+    CK(cudaStreamSynchronize(h.stream));
+    return true;
+}
+
 // LBIB_LOG_HOST_EVENTS=1 prints each host event's stage and duration to
 // stderr (a diagnostic, off by default).
 static bool log_host_events() {
-    static const bool on = [] {
-        const char* e = std::getenv("LBIB_LOG_HOST_EVENTS");
-        return e && e[0] == '1';
-    }();
-    return on;
+    const char* e = std::getenv("LBIB_LOG_HOST_EVENTS");
+    return e && e[0] == '1';
 }
 
-// The host side of a halted stage, in the reference's order.
-static void handle_halt(Handle& h, int stage) {
+// The host side of a halted stage, in the reference's order.  Returns true
+// when only the listed nodes or connections crossed the bus.
+static bool handle_halt(Handle& h, int stage) {
     h.hostEvents++;
     if (stage == ST_REMESH_RNG) {
         perturb_new_nodes(h);
-        return;
+        return true;
     }
+    if (stage == ST_PERTURB_CONN && !h.fullHostEvents && perturb_listed_connections(h)) return true;
     if (stage == ST_INTERP_MOVE) {
         // positions that need GeometryNode::perturbatePosition, in id order;
         // only those nodes' positions cross the bus
@@ -1376,7 +1455,7 @@ static void handle_halt(Handle& h, int stage) {
             CK(cudaMemcpyAsync(h.m.y + list[k], &xy[2 * k + 1], sizeof(double), cudaMemcpyHostToDevice, h.stream));
         }
         CK(cudaStreamSynchronize(h.stream));
-        return;
+        return true;
     }
     pull_topology(h);
     HostMembrane hm;
@@ -1421,6 +1500,7 @@ static void handle_halt(Handle& h, int stage) {
     } else {
         fail(ERR_STATE, "unexpected halt stage");
     }
+    return false;
 }
 
 template <typename Real>
@@ -1506,6 +1586,8 @@ static void run_steps(Handle& h, int n) {
         }
         CK(cudaGetLastError());
         queue_step_areas(h);
+        CK(cudaEventRecord(h.evB, h.stream));  // the end of the call's GPU work, unless more follows
+        h.workAfterEvB = false;
         read_status(h);
         const Status st = *h.stHost;
         // the first kernel of each step counted the step before it; the last
@@ -1525,7 +1607,10 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += done;
         if (done > 0) h.cellTypesCopied = true;
         n -= done;
-        if (hostBio && done > 0) run_host_bio(h, h.iteration - 1);
+        if (hostBio && done > 0) {
+            run_host_bio(h, h.iteration - 1);
+            h.workAfterEvB = true;
+        }
         if (!st.halt) continue;
         if (st.err) {
             h.err = st.err;
@@ -1540,15 +1625,18 @@ static void run_steps(Handle& h, int n) {
         const unsigned it = h.iteration;
         for (;;) {
             const auto t0 = std::chrono::steady_clock::now();
-            handle_halt(h, stage);
+            const bool listed = handle_halt(h, stage);
             if (log_host_events())
-                std::fprintf(stderr, "lbib: host event at stage %d, iteration %u: %.3f ms\n", stage, it,
+                std::fprintf(stderr, "lbib: host event at stage %d, iteration %u (%s): %.3f ms\n", stage, it,
+                             listed ? "listed" : "full membrane",
                              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
             const int from = resume_stage(stage);
             if (from < 0) fail(ERR_STATE, "unexpected halt stage");
             reset_status(h, it, h.cellTypesCopied);
             h.launches += launch_stages<Real>(h, it % 10 == 0, step_bio_ops(h, it), h.cur, from, nullptr, nullptr);
             queue_step_areas(h);
+            CK(cudaEventRecord(h.evB, h.stream));
+            h.workAfterEvB = false;
             read_status(h);
             if (h.stHost->err) {
                 h.err = h.stHost->err;
@@ -1563,7 +1651,10 @@ static void run_steps(Handle& h, int n) {
         h.stepsDone += 1;
         h.cellTypesCopied = true;
         n -= 1;
-        if (hostBio) run_host_bio(h, h.iteration - 1);
+        if (hostBio) {
+            run_host_bio(h, h.iteration - 1);
+            h.workAfterEvB = true;
+        }
     }
 }
 
@@ -1681,6 +1772,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     std::memset(h.stHost, 0, kTopoOffset + sizeof(Topo));
     h.topoHost = (Topo*)((char*)h.stHost + kTopoOffset);
     init_kernel_attributes();
+    if (const char* e = std::getenv("LBIB_FULL_HOST_EVENTS")) h.fullHostEvents = e[0] == '1';
     // LBIB_NO_GRAPHS=1 launches every stage kernel directly (no CUDA graphs)
     if (const char* e = std::getenv("LBIB_NO_GRAPHS")) h.useGraphs = !(e[0] == '1');
     std::memset(h.stHost, 0, sizeof(Status));
@@ -2197,8 +2289,12 @@ int lbib_step(lbib_handle* hh, int n) {
     // the areas read back with the last status word are those of the state
     // now, unless a host bio solver edited the geometry after the last step
     h.areaFresh = n > 0 && lbib::step_leaves_areas(h) && !lbib::host_bio_at(h, h.iteration - 1);
-    CK(cudaEventRecord(h.evB, h.stream));
-    CK(cudaEventSynchronize(h.evB));
+    // evB was recorded before the last status read (whose synchronisation
+    // completed it) unless host work followed
+    if (n == 0 || h.workAfterEvB) {
+        CK(cudaEventRecord(h.evB, h.stream));
+        CK(cudaEventSynchronize(h.evB));
+    }
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, h.evA, h.evB));
     h.lastTotalMs = ms;

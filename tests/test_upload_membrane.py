@@ -176,3 +176,45 @@ def test_upload_rejects_bad_lists(lbib, tmp_path):
     bad[0, 1] = ids.max() + 100
     with pytest.raises(lbib.LbibError):
         sim2.upload_membrane(ids, st[:, :2], bad)
+
+
+def test_connection_perturbation_listed_equals_full(lbib, tmp_path, monkeypatch, capfd):
+    """GeometryHandler::perturbConnections inside a step (GeometryHandler.cpp:
+    326-356): connections whose end points share an x or a y are perturbed
+    by the host from the device's list of them (and the ring-closing test),
+    without the membrane crossing the bus.  The same run with
+    LBIB_FULL_HOST_EVENTS=1 (the reference's full ring walk on a host copy of
+    the membrane) gives identical states.  The connections are made vertical
+    and horizontal by an upload with the fluid at rest and no forces, so the
+    first step's move keeps them: the walk's first connection (node 0 -> 1),
+    the walk's last (node n-1 -> 0) and one at the top (30 -> 31)."""
+    paths = _cfg(10).write(str(tmp_path))
+    monkeypatch.setenv("LBIB_LOG_HOST_EVENTS", "1")
+
+    def run(full):
+        if full:
+            monkeypatch.setenv("LBIB_FULL_HOST_EVENTS", "1")
+        else:
+            monkeypatch.delenv("LBIB_FULL_HOST_EVENTS", raising=False)
+        sim = lbib.Simulation(paths, lbib.FP64)
+        ids, st = sim.membrane()
+        xy = st[:, :2].copy()
+        n = len(ids)
+        xy[1, 0] = xy[0, 0]
+        xy[n - 1, 0] = xy[0, 0]
+        xy[31, 1] = xy[30, 1]
+        sim.upload_membrane(ids, xy, sim.connections())
+        sim.step(1)
+        _, moved = sim.membrane()
+        sim.step(4)
+        return sim, moved
+
+    capfd.readouterr()
+    a, moved_a = run(False)
+    log_a = capfd.readouterr().err
+    b, moved_b = run(True)
+    log_b = capfd.readouterr().err
+    assert "stage 5" in log_a and "listed" in log_a.split("stage 5")[1].splitlines()[0], log_a
+    assert "stage 5" in log_b and "full membrane" in log_b.split("stage 5")[1].splitlines()[0], log_b
+    assert np.array_equal(moved_a, moved_b)
+    _same(a, b, "listed vs full connection perturbation")
