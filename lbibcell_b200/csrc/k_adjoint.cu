@@ -73,21 +73,29 @@ __device__ __forceinline__ void warp_keyed_add(double* grad, int key, double v) 
 }  // namespace
 
 // NS = number of species (compile-time, so that the species' inputs are
-// loaded together with the fluid state).  Grid (ceil(nx / 256), ny).  The
-// fluid's adjoint inputs are loaded after the species' reverse pass and the
-// gradient accumulators where they are updated, so that a node's values are
-// not all live at once: with one species no register spills at the 128
-// registers of two blocks per SM.  LBIB_ADJOINT_MIN_BLOCKS (blocks per SM the
-// register budget is sized for) trades occupancy against spills (measured:
-// 2 is fastest).
+// loaded together with the fluid state).  Grid (ceil(nx / kAdjBlock), ny).
+// The fluid's adjoint inputs are loaded after the species' reverse pass and
+// the gradient accumulators where they are updated, so that a node's values
+// are not all live at once (one species: 24 B of spills at 128 registers).
+// LBIB_ADJOINT_MIN_BLOCKS (blocks per SM the register budget is sized for)
+// trades occupancy against spills.
 #ifndef LBIB_ADJOINT_MIN_BLOCKS
-#define LBIB_ADJOINT_MIN_BLOCKS 2
+#define LBIB_ADJOINT_MIN_BLOCKS 4
 #endif
+// Threads per block (nodes of one row segment); with the blocks per SM above
+// it sets the register budget: 128 x 4 -> 128 registers.  Measured on
+// adjoint_512 (T = 2000, K = 100): 256 x 2 backward 75.6 ms, 128 x 4 73.1 ms,
+// 64 x 8 73.2 ms; 256 x 1 (no spills, 8 warps per SM) and 128 x 5 (96
+// registers, 300 B of spills) are slower.
+#ifndef LBIB_ADJOINT_BLOCK
+#define LBIB_ADJOINT_BLOCK 128
+#endif
+constexpr int kAdjBlock = LBIB_ADJOINT_BLOCK;
 // Real: the precision the states are stored in.  An FP32-shifted run stores
 // f_q - w_q in FP32 (and its species as they are); the reverse step reads
 // them back as f and runs its arithmetic in FP64 all the same.
 template <int NS, typename Real>
-__global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
+__global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
     pdl_wait();
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(256, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(A
     }
     // relaxation-time gradients: block sums into this block's own slots (the
     // same slots every step), reduced over blocks once at the end of the pass
-    __shared__ double red[8][1 + kMaxSpecies];
+    __shared__ double red[kAdjBlock / 32][1 + kMaxSpecies];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double v0 = warp_sum(valid ? gTauF : 0.0);
     if (lane == 0) red[warp][0] = v0;
@@ -371,19 +379,19 @@ __global__ void adjoint_rate_reduce(const double* racc, const uint32_t* dom, siz
 __global__ void set_iteration_kernel(Status* st, unsigned it) {
     pdl_wait(); st->iteration = it; }
 
-int adjoint_blocks(int nx, int ny) { return ((nx + 255) / 256) * ny; }
+int adjoint_blocks(int nx, int ny) { return ((nx + kAdjBlock - 1) / kAdjBlock) * ny; }
 
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
-    const dim3 grid((unsigned)((a.nx + 255) / 256), (unsigned)a.ny);
+    const dim3 grid((unsigned)((a.nx + kAdjBlock - 1) / kAdjBlock), (unsigned)a.ny);
     switch (a.S + (a.fp32 ? 4 : 0)) {
-        case 0: launch_pdl(adjoint_step64<0, double>, grid, 256, 0, s, a); break;
-        case 1: launch_pdl(adjoint_step64<1, double>, grid, 256, 0, s, a); break;
-        case 2: launch_pdl(adjoint_step64<2, double>, grid, 256, 0, s, a); break;
-        case 3: launch_pdl(adjoint_step64<3, double>, grid, 256, 0, s, a); break;
-        case 4: launch_pdl(adjoint_step64<0, float>, grid, 256, 0, s, a); break;
-        case 5: launch_pdl(adjoint_step64<1, float>, grid, 256, 0, s, a); break;
-        case 6: launch_pdl(adjoint_step64<2, float>, grid, 256, 0, s, a); break;
-        default: launch_pdl(adjoint_step64<3, float>, grid, 256, 0, s, a); break;
+        case 0: launch_pdl(adjoint_step64<0, double>, grid, kAdjBlock, 0, s, a); break;
+        case 1: launch_pdl(adjoint_step64<1, double>, grid, kAdjBlock, 0, s, a); break;
+        case 2: launch_pdl(adjoint_step64<2, double>, grid, kAdjBlock, 0, s, a); break;
+        case 3: launch_pdl(adjoint_step64<3, double>, grid, kAdjBlock, 0, s, a); break;
+        case 4: launch_pdl(adjoint_step64<0, float>, grid, kAdjBlock, 0, s, a); break;
+        case 5: launch_pdl(adjoint_step64<1, float>, grid, kAdjBlock, 0, s, a); break;
+        case 6: launch_pdl(adjoint_step64<2, float>, grid, kAdjBlock, 0, s, a); break;
+        default: launch_pdl(adjoint_step64<3, float>, grid, kAdjBlock, 0, s, a); break;
     }
 }
 
