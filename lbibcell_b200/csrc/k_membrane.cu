@@ -1015,8 +1015,11 @@ void launch_crossings(const MembraneDev& m, CrossDev& c, const uint32_t* dom, in
     // the record count (st->pad[2]) is zero here: cleared with the status
     // word before a run and by the first kernel of each step
     launch_pdl(crossings_kernel, blocks, 128, 0, s, m, c, nx, ny, st);
-    launch_pdl(cross_tie_kernel, 296, 256, 0, s, c, st);
-    launch_pdl(cross_win_kernel, 296, 256, 0, s, c, m, dom, nx, ny, st);
+    // grid-stride over the step's records (their count is known on the device
+    // only): 8 blocks per SM, so that each thread's chain of dependent loads
+    // overlaps many others
+    launch_pdl(cross_tie_kernel, 148 * 8, 256, 0, s, c, st);
+    launch_pdl(cross_win_kernel, 148 * 8, 256, 0, s, c, m, dom, nx, ny, st);
 }
 template void launch_crossings<double>(const MembraneDev&, CrossDev&, const uint32_t*, int, int, size_t, Status*,
                                        unsigned, cudaStream_t);

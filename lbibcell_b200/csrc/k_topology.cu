@@ -35,6 +35,24 @@ size_t topo_scan_bytes(int n) {
     return b;
 }
 
+// |d| < MAXLENGTH and |d| > MAXLENGTH for a squared length d2, as the
+// reference tests them (the correctly rounded sqrt, Connection::getLength,
+// Connection.cpp:389-394), with the root taken only within a few ulps of
+// MAXLENGTH^2: the rounded root is monotonic, so well below it is below
+// MAXLENGTH and at or above it is not (and the other way round).
+__device__ __forceinline__ bool shorter_than_max(double d2) {
+    constexpr double m2 = kMAXLENGTH * kMAXLENGTH;
+    if (d2 < m2 * (1.0 - 1e-12)) return true;
+    if (d2 >= m2) return false;
+    return sqrt(d2) < kMAXLENGTH;
+}
+__device__ __forceinline__ bool longer_than_max(double d2) {
+    constexpr double m2 = kMAXLENGTH * kMAXLENGTH;
+    if (d2 > m2 * (1.0 + 1e-12)) return true;
+    if (d2 <= m2) return false;
+    return sqrt(d2) > kMAXLENGTH;
+}
+
 // Perturbation tests of a new node (GeometryNode.cpp:160, 174, 189, 202).
 __device__ __forceinline__ bool new_node_needs_rng(double X, double Y) {
     if (fabs((double)(int)X - X) <= kEPSILON) return true;
@@ -74,9 +92,9 @@ constexpr int kRemeshBlock = 256;  // connections per block of the count and app
 __device__ __forceinline__ bool remesh_split(const MembraneDev& m, int c, bool& rng) {
     const int a = m.ca[c], b = m.cb[c];
     const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-    const double len = sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
-    rng = len > kMAXLENGTH && new_node_needs_rng((x1 + x2) / 2, (y1 + y2) / 2);
-    return len > kMAXLENGTH;
+    const bool split = longer_than_max((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2));
+    rng = split && new_node_needs_rng((x1 + x2) / 2, (y1 + y2) / 2);
+    return split;
 }
 
 // Pass decision.  Each block counts its connections to split (t.flag[block])
@@ -109,17 +127,20 @@ __global__ void __launch_bounds__(kRemeshBlock) remesh_count_kernel(MembraneDev 
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // each thread sums a run of consecutive block counts, one block-wide scan
+    // of the runs, then each thread writes its run's prefixes
     typedef cub::BlockScan<int, kRemeshBlock> Scan;
     __shared__ typename Scan::TempStorage tmp;
-    int carry = 0;
-    for (int b0 = 0; b0 < (int)gridDim.x; b0 += kRemeshBlock) {
-        const int b = b0 + threadIdx.x;
-        const int v = b < (int)gridDim.x ? __ldcg(&t.flag[b]) : 0;
-        int ex, total;
-        Scan(tmp).ExclusiveSum(v, ex, total);
-        if (b < (int)gridDim.x) t.rank[b] = carry + ex;
-        carry += total;
-        __syncthreads();
+    const int nb = (int)gridDim.x;
+    const int per = (nb + kRemeshBlock - 1) / kRemeshBlock;
+    const int beg = threadIdx.x * per, end = min(beg + per, nb);
+    int local = 0;
+    for (int b = beg; b < end; ++b) local += __ldcg(&t.flag[b]);
+    int ex, carry;
+    Scan(tmp).ExclusiveSum(local, ex, carry);
+    for (int b = beg; b < end; ++b) {
+        t.rank[b] = ex;
+        ex += __ldcg(&t.flag[b]);
     }
     if (threadIdx.x == 0) {
         const int K = carry, C = T->C, M = T->M;
@@ -205,7 +226,7 @@ __global__ void remesh_commit_kernel(MembraneDev m, TopoDev t, int nx, int ny, S
         const int a = t.ca2[c], b = t.cb2[c];
         m.ca[c] = a; m.cb[c] = b; m.cdom[c] = t.cdom2[c]; m.cdesc[c] = t.cdesc2[c];
         const double x1 = m.x[a], y1 = m.y[a], x2 = m.x[b], y2 = m.y[b];
-        if (sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) > kMAXLENGTH) raise_halt(st, ST_REMESH);
+        if (longer_than_max((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2))) raise_halt(st, ST_REMESH);
     }
     if (c < K) {
         const int i = M + c;
@@ -269,14 +290,15 @@ __global__ void coarsen_cand_kernel(MembraneDev m, TopoDev t, Status* st) {
     t.ncAlive[i] = 0;
     const int p = m.prev[i], q = m.next[i];
     const double dx = m.x[q] - m.x[p], dy = m.y[q] - m.y[p];
-    const bool cand = sqrt(dx * dx + dy * dy) < kMAXLENGTH;
+    const bool cand = shorter_than_max(dx * dx + dy * dy);
     const unsigned bal = __ballot_sync(__activemask(), cand);
     if (cand && (threadIdx.x & 31) == __ffs(bal) - 1) atomicAdd(&m.topo->nCand, __popc(bal));
 }
 
 constexpr int kCoarsenMax = 2048;  // nodes of one ring held in shared memory
 constexpr size_t kCoarsenSmem = (size_t)kCoarsenMax * (2 * sizeof(double) + sizeof(unsigned long long) +
-                                                       5 * sizeof(int) + 2);
+                                                       6 * sizeof(int) + 2) +
+                                 (size_t)kCoarsenMax / 32 * sizeof(unsigned);
 
 // One block per cell.  The ring (in ring order, rebuilt just before) is
 // loaded into shared memory as a circular list; thread 0 then visits the
@@ -303,7 +325,9 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
     int* nl = pl + kCoarsenMax;
     int* hin = nl + kCoarsenMax;
     int* hout = hin + kCoarsenMax;
-    unsigned char* dirty = (unsigned char*)(hout + kCoarsenMax);
+    int* rankOf = hout + kCoarsenMax;                   // ring position -> place in id order
+    unsigned* visit = (unsigned*)(rankOf + kCoarsenMax); // bit j: the node at place j is a candidate
+    unsigned char* dirty = (unsigned char*)(visit + kCoarsenMax / 32);
     unsigned char* gone = dirty + kCoarsenMax;
     __shared__ int anyDirty;
     if (threadIdx.x == 0) anyDirty = 0;
@@ -330,7 +354,7 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
     for (int k = threadIdx.x; k < len; k += blockDim.x) {
         const int p = pl[k], q = nl[k];
         const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
-        dirty[k] = sqrt(dx * dx + dy * dy) < kMAXLENGTH;
+        dirty[k] = shorter_than_max(dx * dx + dy * dy);
         if (dirty[k]) anyDirty = 1;
     }
     __syncthreads();
@@ -352,15 +376,32 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
             __syncthreads();
         }
     }
+    // the candidates as bits in id order, so that the serial visit below
+    // jumps from one to the next instead of stepping over every node
+    const int nw = (len + 31) >> 5;
+    for (int j = threadIdx.x; j < nw * 32; j += blockDim.x) {
+        const bool cand = j < len && dirty[(int)(ord[j] & 0xffffffffu)];
+        if (j < len) rankOf[(int)(ord[j] & 0xffffffffu)] = j;
+        const unsigned bits = __ballot_sync(0xffffffffu, cand);
+        if ((threadIdx.x & 31) == 0) visit[j >> 5] = bits;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         const int Ccap = m.Ccap;
         int removedHere = 0;
-        for (int j = 0; j < len; ++j) {
+        for (int j = 0;; ++j) {
+            // the next candidate at place >= j (a node that becomes one at an
+            // earlier place is not visited again, as in the id-order loop)
+            int w = j >> 5;
+            unsigned bits = w < nw ? visit[w] & (~0u << (j & 31)) : 0u;
+            while (bits == 0u && ++w < nw) bits = visit[w];
+            if (bits == 0u) break;
+            j = (w << 5) + __ffs(bits) - 1;
             const int k = (int)(ord[j] & 0xffffffffu);
             if (!dirty[k]) continue;
             const int p = pl[k], q = nl[k];
             const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
-            if (!(sqrt(dx * dx + dy * dy) < kMAXLENGTH)) continue;
+            if (!shorter_than_max(dx * dx + dy * dy)) continue;
             gone[k] = 1;
             ++removedHere;
             const int i = node[k];
@@ -375,6 +416,8 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
             nl[p] = q; pl[q] = p;
             hout[p] = Ccap + i; hin[q] = Ccap + i;
             dirty[p] = 1; dirty[q] = 1;
+            visit[rankOf[p] >> 5] |= 1u << (rankOf[p] & 31);
+            visit[rankOf[q] >> 5] |= 1u << (rankOf[q] & 31);
         }
         if (removedHere) atomicAdd(&m.topo->removed, removedHere);
     }

@@ -175,8 +175,11 @@ struct DiffCtx {
     }
 };
 
-// Offset of the membrane counts (Topo) in the status allocation.
+// The status allocation (device, and its pinned host copy): the status word,
+// the membrane counts (Topo) and the per-cell areas, so that one copy reads
+// all three back after a step.
 constexpr size_t kTopoOffset = (sizeof(Status) + 63) / 64 * 64;
+constexpr size_t kAreaOffset = kTopoOffset + (sizeof(Topo) + 63) / 64 * 64;
 
 struct Handle {
     // parameters
@@ -250,11 +253,14 @@ struct Handle {
     Status* stHost = nullptr;
     Topo* topoHost = nullptr;   // pinned copy of the device counts, read with the status word
     bool ringsCurrent = false;  // the device's ring order matches the topology (no rebuild needed)
-    // per-cell areas read back at the end of lbib_step when its bio stage
-    // formed them (the area regulator), in pinned memory; areaFresh: they
-    // are the areas of the current state (any other API call clears it)
+    // per-cell areas read back with the status word at the end of lbib_step
+    // when its bio stage formed them (the area regulator): the host copy's
+    // area part; areaFresh: they are the areas of the current state (any
+    // other API call clears it); statusWithAreas: the next status read takes
+    // the areas along
     double* areaPinned = nullptr;
     bool areaFresh = false;
+    bool statusWithAreas = false;
     // LBIB_FULL_HOST_EVENTS=1 at creation: host events take the whole
     // membrane to the host (the reference's algorithms on a full copy) instead
     // of the listed nodes and connections only (a cross-check of the latter)
@@ -317,7 +323,7 @@ Handle::~Handle() {
     fr(m.x); fr(m.y); fr(m.ox); fr(m.oy); fr(m.vx); fr(m.vy); fr(m.fx); fr(m.fy); fr(m.id); fr(m.bx); fr(m.by);
     fr(m.prev); fr(m.next); fr(m.ca); fr(m.cb); fr(m.cdom); fr(m.foff); fr(m.ftype); fr(m.fpartner); fr(m.fpar);
     fr(m.ringStart); fr(m.ringNode); fr(m.ringDom);
-    fr(outPos); fr(inPos); fr(area); fr(target); fr(areaAcc);
+    fr(outPos); fr(inPos); fr(target); fr(areaAcc);  // area lives in the status allocation
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp); fr(tiles.slots);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
     fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
@@ -332,7 +338,6 @@ Handle::~Handle() {
     fr(td.dist); fr(td.startNode); fr(td.scanTmp);
     fr(st);
     if (stHost) cudaFreeHost(stHost);  // topoHost lives in the same block
-    if (areaPinned) cudaFreeHost(areaPinned);
     if (evA) cudaEventDestroy(evA);
     if (evB) cudaEventDestroy(evB);
     for (auto e : kEvents) cudaEventDestroy(e);
@@ -836,6 +841,32 @@ static void ensure_force_scratch(Handle& h, bool need = false) {
     h.graphEpoch++;
 }
 
+// Sizes the status allocation for cellCap areas, keeping the status word and
+// the counts (device and host copies).
+static void resize_status_block(Handle& h) {
+    const size_t bytes = kAreaOffset + sizeof(double) * (size_t)h.cellCap;
+    char* dev = dalloc<char>(bytes);
+    char* host = nullptr;
+    CK(cudaMallocHost(&host, bytes));
+    std::memset(host, 0, bytes);
+    if (h.st) {
+        CK(cudaMemcpyAsync(dev, h.st, kAreaOffset, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        std::memcpy(host, h.stHost, kAreaOffset);
+        cudaFree(h.st);
+        cudaFreeHost(h.stHost);
+    } else {
+        CK(cudaMemsetAsync(dev, 0, kAreaOffset, h.stream));
+    }
+    h.st = (Status*)dev;
+    h.m.topo = (Topo*)(dev + kTopoOffset);
+    h.area = (double*)(dev + kAreaOffset);
+    h.stHost = (Status*)host;
+    h.topoHost = (Topo*)(host + kTopoOffset);
+    h.areaPinned = (double*)(host + kAreaOffset);
+    h.graphEpoch++;  // kernels captured with the old addresses
+}
+
 static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     // headroom for remeshing on the device: node and connection buffers hold
     // twice the current counts before the host has to grow them
@@ -919,15 +950,13 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(cells, h.cellCap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ringStart); fr(h.m.ringDom); fr(h.area); fr(h.target); fr(h.areaAcc);
+        fr(h.m.ringStart); fr(h.m.ringDom); fr(h.target); fr(h.areaAcc);
         fr(h.td.cellCount); fr(h.td.cellStart); fr(h.td.cellFill); fr(h.td.startNode);
         h.m.ringStart = dalloc<int>(h.cellCap + 1); h.m.ringDom = dalloc<uint32_t>(h.cellCap);
-        h.area = dalloc<double>(h.cellCap); h.target = dalloc<double>(h.cellCap);
+        resize_status_block(h);
+        h.target = dalloc<double>(h.cellCap);
         h.areaAcc = dalloc<unsigned long long>(h.cellCap);
         CK(cudaMemset(h.areaAcc, 0, sizeof(unsigned long long) * h.cellCap));
-        if (h.areaPinned) CK(cudaFreeHost(h.areaPinned));
-        h.areaPinned = nullptr;
-        CK(cudaMallocHost(&h.areaPinned, sizeof(double) * h.cellCap));
         h.td.cellCount = dalloc<int>(h.cellCap + 1); h.td.cellStart = dalloc<int>(h.cellCap + 1);
         h.td.cellFill = dalloc<int>(h.cellCap); h.td.startNode = dalloc<int>(h.cellCap);
     }
@@ -1221,7 +1250,9 @@ static int resume_stage(int stage) {
 // their `changed` flag says whether the ring order of the cell areas is stale
 // (remeshing or coarsening on the device set it; a ring rebuild clears it).
 static void read_status(Handle& h) {
-    CK(cudaMemcpyAsync(h.stHost, h.st, kTopoOffset + sizeof(Topo), cudaMemcpyDeviceToHost, h.stream));
+    const size_t areas = h.statusWithAreas ? sizeof(double) * (size_t)h.m.nCells : 0;
+    h.statusWithAreas = false;
+    CK(cudaMemcpyAsync(h.stHost, h.st, kAreaOffset + areas, cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
     if (h.m.topo) h.ringsCurrent = h.topoHost->changed == 0;
 }
@@ -1254,8 +1285,7 @@ static void queue_areas(Handle& h, double* area) {
 }
 
 static void queue_step_areas(Handle& h) {
-    if (step_leaves_areas(h))
-        CK(cudaMemcpyAsync(h.areaPinned, h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost, h.stream));
+    if (step_leaves_areas(h)) h.statusWithAreas = true;
 }
 
 // Clears the status word for a run that starts at Parameters' iteration `it`.
@@ -1766,11 +1796,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
     CK(cudaMemsetAsync(h.dom, 0, sizeof(uint32_t) * h.L, h.stream));
     // the status word and the membrane counts share one allocation (and one
     // pinned host copy), so that one copy reads both back after a step
-    CK(cudaMalloc(&h.st, kTopoOffset + sizeof(Topo)));
-    CK(cudaMemsetAsync(h.st, 0, kTopoOffset + sizeof(Topo), h.stream));
-    CK(cudaMallocHost(&h.stHost, kTopoOffset + sizeof(Topo)));
-    std::memset(h.stHost, 0, kTopoOffset + sizeof(Topo));
-    h.topoHost = (Topo*)((char*)h.stHost + kTopoOffset);
+    resize_status_block(h);
     init_kernel_attributes();
     if (const char* e = std::getenv("LBIB_FULL_HOST_EVENTS")) h.fullHostEvents = e[0] == '1';
     // LBIB_NO_GRAPHS=1 launches every stage kernel directly (no CUDA graphs)
@@ -1816,7 +1842,7 @@ static void create(Handle& h, const std::string& params, const std::string& geom
         CK(cudaMemsetAsync(h.cross.bounceN, 0, sizeof(int), h.stream));
     }
 
-    h.m.topo = (Topo*)((char*)h.st + kTopoOffset);
+    // (h.m.topo points into the status allocation, set with it)
 
     // geometry: Geometry::loadGeometryTXT (Geometry.cpp:99-160), or for a
     // ".vtm" file loadGeometryVTK (Geometry.cpp:162-306, the choice made at
@@ -2526,8 +2552,7 @@ int lbib_areas(lbib_handle* hh, unsigned* dom, double* area, int cap) {
             lbib::reset_status(h, h.iteration, h.cellTypesCopied);
             lbib::queue_areas(h, h.area);
             CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(h.areaPinned, h.area, sizeof(double) * h.m.nCells, cudaMemcpyDeviceToHost,
-                               h.stream));
+            h.statusWithAreas = true;
             lbib::read_status(h);
             if (h.stHost->err) {
                 const long long idx = h.stHost->errIndex;
