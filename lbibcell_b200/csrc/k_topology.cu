@@ -297,7 +297,7 @@ __global__ void coarsen_cand_kernel(MembraneDev m, TopoDev t, Status* st) {
 
 constexpr int kCoarsenMax = 2048;  // nodes of one ring held in shared memory
 constexpr size_t kCoarsenSmem = (size_t)kCoarsenMax * (2 * sizeof(double) + sizeof(unsigned long long) +
-                                                       6 * sizeof(int) + 2) +
+                                                       7 * sizeof(int) + 2) +
                                  (size_t)kCoarsenMax / 32 * sizeof(unsigned);
 
 // One block per cell.  The ring (in ring order, rebuilt just before) is
@@ -325,12 +325,22 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
     int* nl = pl + kCoarsenMax;
     int* hin = nl + kCoarsenMax;
     int* hout = hin + kCoarsenMax;
-    int* rankOf = hout + kCoarsenMax;                   // ring position -> place in id order
+    // boundary descriptor of each position's incoming connection, and the
+    // ring's domain (one per cell), so that the serial visit below reads no
+    // global memory (it does where a ring mixes domains)
+    int* inDesc = hout + kCoarsenMax;
+    __shared__ uint32_t ringDomS;
+    __shared__ int mixedDom;
+    int* rankOf = inDesc + kCoarsenMax;                 // ring position -> place in id order
     unsigned* visit = (unsigned*)(rankOf + kCoarsenMax); // bit j: the node at place j is a candidate
     unsigned char* dirty = (unsigned char*)(visit + kCoarsenMax / 32);
     unsigned char* gone = dirty + kCoarsenMax;
     __shared__ int anyDirty;
-    if (threadIdx.x == 0) anyDirty = 0;
+    if (threadIdx.x == 0) {
+        anyDirty = 0;
+        mixedDom = 0;
+        ringDomS = len > 0 ? m.cdom[t.inConn[m.ringNode[b]]] : 0u;
+    }
     int p2 = 1;
     while (p2 < len) p2 <<= 1;
     __syncthreads();
@@ -343,6 +353,8 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
             pl[k] = k == 0 ? len - 1 : k - 1;
             nl[k] = k == len - 1 ? 0 : k + 1;
             hin[k] = t.inConn[i];
+            if (m.cdom[hin[k]] != ringDomS) mixedDom = 1;
+            inDesc[k] = m.cdesc[hin[k]];
             hout[k] = t.outConn[i];
             ord[k] = ((unsigned long long)i << 32) | (unsigned)k;
             gone[k] = 0;
@@ -406,15 +418,21 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
             ++removedHere;
             const int i = node[k];
             const int h1 = hin[k], h2 = hout[k];
-            uint32_t dom;
-            int desc;
-            if (h1 < Ccap) { t.connAlive[h1] = 0; dom = m.cdom[h1]; desc = m.cdesc[h1]; }
-            else { t.ncAlive[h1 - Ccap] = 0; dom = t.ncDom[h1 - Ccap]; desc = t.ncDesc[h1 - Ccap]; }
+            uint32_t dom = ringDomS;
+            const int desc = inDesc[k];
+            if (h1 < Ccap) {
+                t.connAlive[h1] = 0;
+                if (mixedDom) dom = m.cdom[h1];
+            } else {
+                t.ncAlive[h1 - Ccap] = 0;
+                if (mixedDom) dom = t.ncDom[h1 - Ccap];
+            }
             if (h2 < Ccap) t.connAlive[h2] = 0;
             else t.ncAlive[h2 - Ccap] = 0;
             t.ncA[i] = node[p]; t.ncB[i] = node[q]; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
             nl[p] = q; pl[q] = p;
             hout[p] = Ccap + i; hin[q] = Ccap + i;
+            inDesc[q] = desc;
             dirty[p] = 1; dirty[q] = 1;
             visit[rankOf[p] >> 5] |= 1u << (rankOf[p] & 31);
             visit[rankOf[q] >> 5] |= 1u << (rankOf[q] & 31);
