@@ -1189,7 +1189,14 @@ __global__ void reinit_free_kernel(CrossDev c, uint32_t* dom, Real* g, const Rea
         bool free = true;
 #pragma unroll
         for (int d = 0; d < kReinitDeps; ++d) free &= deps[d] < 0;
-        c.reinitDone[k] = free ? 1 : 0;
+        if (!free) {
+            // listed for the one-block pass; the mark says where
+            const int w = atomicAdd(c.nWait, 1);
+            c.waitList[w] = k;
+            c.reinitDone[k] = 2 + w;
+        } else {
+            c.reinitDone[k] = 1;
+        }
         if (free)
             reinit_node<Real>(n, c.changedDom[k], dom, g, u, nS, sp, srcTab, nDomains, ctypeTab, st->cellTypesCopied,
                               c, nx, ny, L, st, st->iteration);
@@ -1203,11 +1210,16 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
                                                       int cellTypesCopied, int nx, int ny, size_t L, Status* st,
                                                       unsigned iteration) {
     pdl_wait();
-    if (st->halt) return;
     const int cnt = st->nChanged;
-    if (cnt == 0) return;
+    if (st->halt || cnt == 0) {
+        if (threadIdx.x == 0) *c.nWait = 0;
+        return;
+    }
     if (cnt > kReinitMax || cnt > c.changedCap) {
-        if (threadIdx.x == 0) raise_error(st, ERR_CAPACITY, cnt, ST_REINIT);
+        if (threadIdx.x == 0) {
+            raise_error(st, ERR_CAPACITY, cnt, ST_REINIT);
+            *c.nWait = 0;
+        }
         return;
     }
     const SpeciesConst sp[3] = {sp0, sp1, sp2};
@@ -1216,15 +1228,17 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
     int(*deps)[kReinitDeps] = (int(*)[kReinitDeps])(key + kReinitMax);
     unsigned char* done = (unsigned char*)(deps + kReinitMax);
     __shared__ int remaining;
-    // Step 2, one block: the nodes that wait for others, in dependency rounds
-    // (the marks and the free nodes' results come from steps 1 and 2)
-    if (threadIdx.x == 0) remaining = 0;
-    __syncthreads();
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-        key[k] = (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k];
-        reinit_deps(c, (size_t)c.changedNode[k], nx, ny, deps[k]);
-        done[k] = c.reinitDone[k];
-        if (!done[k]) atomicAdd(&remaining, 1);
+    // Step 2, one block: only the nodes that wait for others (listed by the
+    // wide pass, usually few or none), in dependency rounds.  A dependency is
+    // done when the wide pass re-initialised it (reinitDone 1) or when this
+    // pass did (done[w] of its place w in the wait list, reinitDone 2 + w).
+    const int nw = min(*c.nWait, cnt);
+    if (threadIdx.x == 0) remaining = nw;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        const int k = c.waitList[w];
+        key[w] = (((unsigned long long)c.changedNode[k]) << 32) | c.changedDom[k];
+        reinit_deps(c, (size_t)c.changedNode[k], nx, ny, deps[w]);
+        done[w] = 0;
     }
     __syncthreads();
     int rounds = 0;
@@ -1232,29 +1246,34 @@ __global__ void __launch_bounds__(1024) reinit_kernel(CrossDev c, uint32_t* dom,
         __shared__ int nowDone;
         if (threadIdx.x == 0) nowDone = 0;
         __syncthreads();
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-            if (done[k]) continue;
+        for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+            if (done[w]) continue;
             bool ready = true;
-            for (int d = 0; d < kReinitDeps; ++d)
-                if (deps[k][d] >= 0 && done[deps[k][d]] != 1) ready = false;
-            if (ready) done[k] = 2;  // processing this round
+            for (int d = 0; d < kReinitDeps; ++d) {
+                const int p = deps[w][d];
+                if (p < 0) continue;
+                const int v = c.reinitDone[p];
+                if (v != 1 && done[v - 2] != 1) ready = false;
+            }
+            if (ready) done[w] = 2;  // processing this round
         }
         __syncthreads();
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-            if (done[k] == 2) {
-                reinit_node<Real>((size_t)(key[k] >> 32), (uint32_t)(key[k] & 0xffffffffu), dom, g, u, nS, sp, srcTab,
+        for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+            if (done[w] == 2) {
+                reinit_node<Real>((size_t)(key[w] >> 32), (uint32_t)(key[w] & 0xffffffffu), dom, g, u, nS, sp, srcTab,
                                   nDomains, ctypeTab, st->cellTypesCopied, c, nx, ny, L, st, st->iteration);
                 atomicAdd(&nowDone, 1);
             }
         }
         __syncthreads();
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x)
-            if (done[k] == 2) done[k] = 1;
+        for (int w = threadIdx.x; w < nw; w += blockDim.x)
+            if (done[w] == 2) done[w] = 1;
         if (threadIdx.x == 0) remaining -= nowDone;
         __syncthreads();
         ++rounds;
     }
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) c.mark[(size_t)(key[k] >> 32)] = 0;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) c.mark[(size_t)c.changedNode[k]] = 0;
+    if (threadIdx.x == 0) *c.nWait = 0;
 }
 
 template <typename Real>

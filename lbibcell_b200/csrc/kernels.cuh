@@ -84,7 +84,9 @@ struct CrossDev {
     uint32_t* bnDom;             // 4*L
     uint32_t* wDom;              // L, W-slot winner domain + 1 (0: none)
     int* mark;                   // L, position + 1 of a node in this step's changed list (0: none)
-    unsigned char* reinitDone;   // changedCap: re-initialised by the wide pass
+    int* reinitDone;             // changedCap: 1 = re-initialised by the wide pass, 2 + w = waiting at waitList[w]
+    int* waitList;               // changedCap: list positions of the nodes that wait for another
+    int* nWait;                  // entries of waitList
     uint32_t* changedNode;       // capacity: nodes whose domain changes
     uint32_t* changedDom;
     int changedCap;

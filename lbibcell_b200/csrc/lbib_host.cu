@@ -326,7 +326,8 @@ Handle::~Handle() {
     fr(outPos); fr(inPos); fr(target); fr(areaAcc);  // area lives in the status allocation
     fr(tiles.count); fr(tiles.fill); fr(tiles.start); fr(tiles.list); fr(tiles.scanTmp); fr(tiles.slots);
     fr(cross.bnDist); fr(cross.bnConn); fr(cross.bnDom); fr(cross.wDom); fr(cross.mark);
-    fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone);
+    fr(cross.changedNode); fr(cross.changedDom); fr(cross.perturbList); fr(cross.reinitDone); fr(cross.waitList);
+    fr(cross.nWait);
     fr(cross.recKey); fr(cross.recConn); fr(cross.recDom); fr(cross.recDist); fr(cross.nfKeys); fr(cross.nfD);
     fr(cross.nfSpec); fr(cross.nfU); fr(cross.nfN); fr(nfTabDev);
     fr(cross.bounceW); fr(cross.bounceS); fr(cross.bounceKeys); fr(cross.bounceN);
@@ -910,7 +911,7 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
     }
     if (grow(C, h.Ccap)) {
         auto fr = [](void* p) { if (p) cudaFree(p); };
-        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode); fr(h.cross.reinitDone);
+        fr(h.m.ca); fr(h.m.cb); fr(h.m.cdom); fr(h.m.cdesc); fr(h.cross.changedNode); fr(h.cross.reinitDone); fr(h.cross.waitList);
         fr(h.cross.recKey); fr(h.cross.recConn); fr(h.cross.recDom); fr(h.cross.recDist);
         fr(h.cross.changedDom);
         // the boundary-node list of the last crossings is still to be used by
@@ -940,7 +941,12 @@ static void ensure_capacity(Handle& h, int M, int C, int F, int cells) {
         h.cross.recDom = dalloc<uint32_t>(h.cross.recCap);
         h.cross.recDist = dalloc<unsigned long long>(h.cross.recCap);
         h.cross.changedNode = dalloc<uint32_t>(h.cross.changedCap);
-        h.cross.reinitDone = dalloc<unsigned char>(h.cross.changedCap);
+        h.cross.reinitDone = dalloc<int>(h.cross.changedCap);
+        h.cross.waitList = dalloc<int>(h.cross.changedCap);
+        if (!h.cross.nWait) {
+            h.cross.nWait = dalloc<int>(1);
+            CK(cudaMemsetAsync(h.cross.nWait, 0, sizeof(int), h.stream));
+        }
         h.cross.changedDom = dalloc<uint32_t>(h.cross.changedCap);
     }
     if (grow(F, h.Fcap)) {
