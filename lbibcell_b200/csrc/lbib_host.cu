@@ -266,6 +266,11 @@ struct Handle {
     // of the listed nodes and connections only (a cross-check of the latter)
     bool fullHostEvents = false;
     bool workAfterEvB = false;  // GPU work was issued after the step loop's last timing event
+    // the device status word carries on from the last batch of steps (no
+    // halt, nothing wrote it since): the next batch needs no reset; its
+    // first step counts the batch's last step (pad[0] was lastPad0)
+    bool statusContinues = false;
+    int lastPad0 = 0;
     cudaStream_t stream = nullptr;
 
     std::mt19937 genNode{1};
@@ -1264,6 +1269,7 @@ static void read_status(Handle& h) {
 }
 
 static void write_status(Handle& h) {
+    h.statusContinues = false;
     CK(cudaMemcpyAsync(h.st, h.stHost, sizeof(Status), cudaMemcpyHostToDevice, h.stream));
 }
 
@@ -1602,7 +1608,12 @@ static void run_steps(Handle& h, int n) {
                     break;
                 }
         }
-        reset_status(h, h.iteration, h.cellTypesCopied);
+        // a status word that carries on from the last batch needs no reset
+        // (one host-to-device copy less per call); its steps' count starts
+        // at lastPad0 and the first step counts the last batch's last step
+        int pad0 = -1;
+        if (h.statusContinues) pad0 = h.lastPad0;
+        else reset_status(h, h.iteration, h.cellTypesCopied);
         const bool prof = h.profiling;
         while ((int)h.kEvents.size() < 2 * B) {
             cudaEvent_t e;
@@ -1628,7 +1639,11 @@ static void run_steps(Handle& h, int n) {
         const Status st = *h.stHost;
         // the first kernel of each step counted the step before it; the last
         // step of the batch completed unless a halt is pending
-        const int done = st.pad[0] + (st.halt ? 0 : 1);
+        const int done = pad0 < 0 ? st.pad[0] + (st.halt ? 0 : 1) : st.pad[0] - pad0 - (st.halt ? 1 : 0);
+        if (!st.halt) {
+            h.statusContinues = true;
+            h.lastPad0 = st.pad[0];
+        }
         if (prof) {
             for (int b = 0; b < std::min(done, B); ++b) {
                 float ms = 0;
