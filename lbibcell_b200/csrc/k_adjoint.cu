@@ -96,7 +96,6 @@ constexpr int kAdjBlock = LBIB_ADJOINT_BLOCK;
 // them back as f and runs its arithmetic in FP64 all the same.
 template <int NS, typename Real>
 __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
-    pdl_wait();
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
     const int xr = blockIdx.x * blockDim.x + threadIdx.x;
@@ -118,6 +117,12 @@ __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_st
     };
 
     // ---- the inputs of the forward recomputation and of the species ------
+    // The stored state, the domain ids, the force field and the mass table
+    // are written by no kernel of the reverse pass, and every kernel before
+    // the previous launch has completed (the previous launch, an adjoint step
+    // of the same pass with a.chained, let this one start only after its own
+    // wait): they are loaded before the wait, during the previous step's last
+    // wave.  The adjoint planes and the accumulators are read after it.
     const Real* __restrict__ fprev = (const Real*)a.fprev;
     double f[9], lf[9];
 #pragma unroll
@@ -130,6 +135,17 @@ __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_st
         const Real* gp = (const Real*)a.gprev + (size_t)k * 5 * L;
 #pragma unroll
         for (int q = 0; q < 5; ++q) gA[k][q] = gp[(size_t)q * L + pull(q)];
+    }
+    const uint32_t dom = a.dom[n];
+    // The force field of a differentiated run is zero outside the force tiles,
+    // so it and G are read and written everywhere: no load waits on another.
+    const double fx = a.force[n], fy = a.force[L + n];
+    double rta = 0.0;
+    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
+    pdl_wait();
+    pdl_launch_dependents();
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
         if (a.seed) {
             const double sd = a.seed[(size_t)k * L + n];
 #pragma unroll
@@ -140,13 +156,7 @@ __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_st
             for (int q = 0; q < 5; ++q) muA[k][q] = (double)pg[(size_t)q * L + push(q)];
         }
     }
-    const uint32_t dom = a.dom[n];
-    // The force field of a differentiated run is zero outside the force tiles,
-    // so it and G are read and written everywhere: no load waits on another.
-    const double fx = a.force[n], fy = a.force[L + n];
     double gTauK[NS > 0 ? NS : 1];
-    double rta = 0.0;
-    if (a.massTab != nullptr && dom < (uint32_t)a.nDomains) rta = a.massTab[dom];
     const bool hasMass = a.macc != nullptr && a.massTab != nullptr && dom < (uint32_t)a.nDomains && isfinite(rta);
     if (!isfinite(rta)) rta = 0.0;
 
@@ -384,14 +394,14 @@ int adjoint_blocks(int nx, int ny) { return ((nx + kAdjBlock - 1) / kAdjBlock) *
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.nx + kAdjBlock - 1) / kAdjBlock), (unsigned)a.ny);
     switch (a.S + (a.fp32 ? 4 : 0)) {
-        case 0: launch_pdl(adjoint_step64<0, double>, grid, kAdjBlock, 0, s, a); break;
-        case 1: launch_pdl(adjoint_step64<1, double>, grid, kAdjBlock, 0, s, a); break;
-        case 2: launch_pdl(adjoint_step64<2, double>, grid, kAdjBlock, 0, s, a); break;
-        case 3: launch_pdl(adjoint_step64<3, double>, grid, kAdjBlock, 0, s, a); break;
-        case 4: launch_pdl(adjoint_step64<0, float>, grid, kAdjBlock, 0, s, a); break;
-        case 5: launch_pdl(adjoint_step64<1, float>, grid, kAdjBlock, 0, s, a); break;
-        case 6: launch_pdl(adjoint_step64<2, float>, grid, kAdjBlock, 0, s, a); break;
-        default: launch_pdl(adjoint_step64<3, float>, grid, kAdjBlock, 0, s, a); break;
+        case 0: launch_ex(a.chained != 0, adjoint_step64<0, double>, grid, kAdjBlock, 0, s, a); break;
+        case 1: launch_ex(a.chained != 0, adjoint_step64<1, double>, grid, kAdjBlock, 0, s, a); break;
+        case 2: launch_ex(a.chained != 0, adjoint_step64<2, double>, grid, kAdjBlock, 0, s, a); break;
+        case 3: launch_ex(a.chained != 0, adjoint_step64<3, double>, grid, kAdjBlock, 0, s, a); break;
+        case 4: launch_ex(a.chained != 0, adjoint_step64<0, float>, grid, kAdjBlock, 0, s, a); break;
+        case 5: launch_ex(a.chained != 0, adjoint_step64<1, float>, grid, kAdjBlock, 0, s, a); break;
+        case 6: launch_ex(a.chained != 0, adjoint_step64<2, float>, grid, kAdjBlock, 0, s, a); break;
+        default: launch_ex(a.chained != 0, adjoint_step64<3, float>, grid, kAdjBlock, 0, s, a); break;
     }
 }
 

@@ -301,6 +301,8 @@ struct AdjointArgs {
     SpeciesConst sp[kMaxSpecies];
     unsigned iteration;    // iteration counter during step t
     int outlet;
+    int chained;           // the previous launch on the stream is an adjoint step of the same pass
+                           // (programmatic launch); 0: a plain launch after whatever came before
     double* G;             // 2*L      dL/dF(x), summed over steps
     double* racc;          // S*L      dL/d source at each node, summed over steps
     double* macc;          // L        dL/d rhoToAdd at each node, summed over steps (with massTab)

@@ -138,6 +138,15 @@ struct DiffCtx {
     char* u0 = nullptr;       // velocity and force planes at step 0 (restored by lbib_diff_end), 4*L values
     char* ck = nullptr;       // states at steps K, 2K, ... (nSeg - 1 of them)
     char* seg = nullptr;      // states base+1 .. base+K-1 of the segment being reversed
+    // A second segment buffer for FP32 states, when the device has room for
+    // it: the reverse pass then recomputes the next segment on `recStream`
+    // while the adjoint steps of the current one run on `adjStream` (higher
+    // priority).  adjoint_512, T = 2000, K = 100: FP32 states 58.5 -> 52.6 ms
+    // per reverse pass; FP64 states 72.7 -> 76.5 ms (the FP64 recompute slows
+    // the FP64 adjoint steps more than it saves), so FP64 runs stay serial.
+    char* seg2 = nullptr;
+    cudaStream_t recStream = nullptr, adjStream = nullptr;
+    cudaEvent_t evRec[2] = {nullptr, nullptr}, evAdj[2] = {nullptr, nullptr}, evFork = nullptr, evJoin[2] = {nullptr, nullptr};
     char* fin = nullptr;      // the final state of the forward pass
     float* P[2] = {nullptr, nullptr};  // adjoint planes, (9 + 5 S) L each
     double* G = nullptr;      // 2*L
@@ -171,7 +180,11 @@ struct DiffCtx {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(x0); fr(u0); fr(ck); fr(seg); fr(fin); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(force32); fr(fxp);
         fr(fyp); fr(gfx); fr(gfy);
-        fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st); fr(massTab); fr(macc); fr(seedF);
+        fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st); fr(massTab); fr(macc); fr(seedF); fr(seg2);
+        for (cudaEvent_t e : {evRec[0], evRec[1], evAdj[0], evAdj[1], evFork, evJoin[0], evJoin[1]})
+            if (e) cudaEventDestroy(e);
+        if (recStream) cudaStreamDestroy(recStream);
+        if (adjStream) cudaStreamDestroy(adjStream);
     }
 };
 
@@ -2112,6 +2125,22 @@ static void diff_begin(Handle& h, int T, int K) {
     }
     d->part = dalloc<double>(nPart);
     d->st = dalloc<Status>(1);
+    const char* serial = std::getenv("LBIB_DIFF_SERIAL");  // diagnostic: one segment buffer
+    if (rs == 4 && nSeg >= 2 && K >= 2 && !(serial && serial[0] == '1')) {
+        // the second segment buffer only where it leaves 2 GiB free
+        const size_t segBytes = (size_t)(K - 1) * stateBytes;
+        CK(cudaMemGetInfo(&freeB, &totalB));
+        if (segBytes + (size_t(2) << 30) <= freeB) {
+            d->seg2 = dalloc<char>(segBytes);
+            int least = 0, greatest = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            CK(cudaStreamCreateWithPriority(&d->recStream, cudaStreamNonBlocking, least));
+            CK(cudaStreamCreateWithPriority(&d->adjStream, cudaStreamNonBlocking, greatest));
+            for (cudaEvent_t* e : {&d->evRec[0], &d->evRec[1], &d->evAdj[0], &d->evAdj[1], &d->evFork, &d->evJoin[0],
+                                   &d->evJoin[1]})
+                CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        }
+    }
     CK(cudaMemsetAsync(d->st, 0, sizeof(Status), h.stream));
     CK(cudaMemsetAsync(d->force, 0, sizeof(double) * 2 * L, h.stream));
     // snapshot of the lattice and the run's default parameters
@@ -2141,9 +2170,9 @@ static bool diff_needs_iteration(const Handle& h) {
 // Forward step t of the differentiated run: state `in` (after step t-1) to
 // `out`, in the handle's lattice precision.
 template <typename Real>
-static void diff_forward_step_t(Handle& h, DiffCtx& d, const char* in, char* out, int t) {
+static void diff_forward_step_t(Handle& h, DiffCtx& d, const char* in, char* out, int t, cudaStream_t stream) {
     const unsigned it = d.it0 + (unsigned)(t - 1);
-    if (diff_needs_iteration(h)) launch_set_iteration(d.st, it, h.stream);
+    if (diff_needs_iteration(h)) launch_set_iteration(d.st, it, stream);
     LatticeArgs<Real> a = lattice_args<Real>(h, it, h.cur);
     a.fin = (const Real*)in; a.fout = (Real*)out;
     a.gin = (const Real*)in + 9 * h.L; a.gout = (Real*)out + 9 * h.L;
@@ -2154,13 +2183,13 @@ static void diff_forward_step_t(Handle& h, DiffCtx& d, const char* in, char* out
     for (int k = 0; k < h.S; ++k) a.sp[k].tau = d.tau[k];
     a.status = d.st;
     a.outlet = d.outlet;
-    if (sizeof(Real) == 8) launch_stream_collide64(*(const LatticeArgs<double>*)&a, h.stream);
-    else launch_stream_collide32(*(const LatticeArgs<float>*)&a, h.stream);
+    if (sizeof(Real) == 8) launch_stream_collide64(*(const LatticeArgs<double>*)&a, stream);
+    else launch_stream_collide32(*(const LatticeArgs<float>*)&a, stream);
 }
 
-static void diff_forward_step(Handle& h, DiffCtx& d, const char* in, char* out, int t) {
-    if (d.rs == 8) diff_forward_step_t<double>(h, d, in, out, t);
-    else diff_forward_step_t<float>(h, d, in, out, t);
+static void diff_forward_step(Handle& h, DiffCtx& d, const char* in, char* out, int t, cudaStream_t stream) {
+    if (d.rs == 8) diff_forward_step_t<double>(h, d, in, out, t, stream);
+    else diff_forward_step_t<float>(h, d, in, out, t, stream);
 }
 
 static void diff_check_status(Handle& h, DiffCtx& d) {
@@ -2191,7 +2220,7 @@ static void diff_forward(Handle& h, DiffCtx& d) {
         else if (t == d.T) out = d.fin;
         else if (t > lastBase) out = d.seg + (size_t)(t - lastBase - 1) * d.stateBytes;
         else out = scratch[t & 1];
-        diff_forward_step(h, d, in, out, t);
+        diff_forward_step(h, d, in, out, t, h.stream);
         in = out;
     }
     d.lastSegKept = true;
@@ -2234,18 +2263,23 @@ static void diff_backward(Handle& h, DiffCtx& d) {
     a.racc = d.racc;
     a.part = d.part;
     a.grad = d.grad;
-    for (int s = d.nSeg - 1; s >= 0; --s) {
+    // Segment s (steps base+1 .. base+len) is reversed from the states
+    // base .. base+len-1: the checkpoint, then its recomputed states in a
+    // segment buffer (d.seg always, or alternately d.seg and d.seg2).
+    const bool two = d.seg2 != nullptr;
+    auto bufOf = [&](int s) -> char* { return two && ((d.nSeg - 1 - s) & 1) ? d.seg2 : d.seg; };
+    auto segState = [&](int s, int j) -> char* {  // state s*K + j, 0 <= j < len
+        return j == 0 ? d.state(s) : bufOf(s) + (size_t)(j - 1) * d.stateBytes;
+    };
+    auto segLen = [&](int s) { return std::min(d.K, d.T - s * d.K); };
+    auto recompute = [&](int s, cudaStream_t stream) {
+        for (int j = 1; j < segLen(s); ++j)
+            diff_forward_step(h, d, segState(s, j - 1), segState(s, j), s * d.K + j, stream);
+    };
+    auto reverse = [&](int s, cudaStream_t stream) {
         const int base = s * d.K;
-        const int len = std::min(d.K, d.T - base);
-        // recompute states base+1 .. base+len-1 from the checkpoint
-        auto segState = [&](int j) -> char* {  // state base + j, 0 <= j < len
-            return j == 0 ? d.state(s) : d.seg + (size_t)(j - 1) * d.stateBytes;
-        };
-        if (!(s == d.nSeg - 1 && d.lastSegKept))
-            for (int j = 1; j < len; ++j) diff_forward_step(h, d, segState(j - 1), segState(j), base + j);
-        if (s < d.nSeg - 1) d.lastSegKept = false;  // seg now holds an earlier segment
-        for (int t = base + len; t > base; --t) {
-            const char* prev = segState(t - 1 - base);
+        for (int t = base + segLen(s); t > base; --t) {
+            const char* prev = segState(s, t - 1 - base);
             a.fprev = prev;
             a.gprev = prev + 9 * L * d.rs;
             a.fp32 = d.rs == 4;
@@ -2259,8 +2293,44 @@ static void diff_backward(Handle& h, DiffCtx& d) {
             a.qf = d.P[t & 1];
             a.qg = d.P[t & 1] + 9 * L;
             a.iteration = d.it0 + (unsigned)(t - 1);
-            launch_adjoint_step64(a, h.stream);
+            a.chained = t < base + segLen(s);  // the segment's first step follows its recompute
+            launch_adjoint_step64(a, stream);
         }
+    };
+    const bool keptLast = d.lastSegKept;
+    if (!two) {
+        for (int s = d.nSeg - 1; s >= 0; --s) {
+            if (!(s == d.nSeg - 1 && keptLast)) recompute(s, h.stream);
+            if (s < d.nSeg - 1) d.lastSegKept = false;  // seg now holds an earlier segment
+            reverse(s, h.stream);
+        }
+    } else {
+        // Segment s-1 is recomputed while segment s is reversed.  Its buffer
+        // was last read by the reverse pass of segment s+1, which it waits for.
+        CK(cudaEventRecord(d.evFork, h.stream));
+        CK(cudaStreamWaitEvent(d.recStream, d.evFork, 0));
+        CK(cudaStreamWaitEvent(d.adjStream, d.evFork, 0));
+        auto issueRecompute = [&](int s) {
+            const int b = (d.nSeg - 1 - s) & 1;
+            if (s + 2 <= d.nSeg - 1) CK(cudaStreamWaitEvent(d.recStream, d.evAdj[b], 0));
+            if (!(s == d.nSeg - 1 && keptLast)) recompute(s, d.recStream);
+            CK(cudaEventRecord(d.evRec[b], d.recStream));
+        };
+        issueRecompute(d.nSeg - 1);
+        issueRecompute(d.nSeg - 2);
+        for (int s = d.nSeg - 1; s >= 0; --s) {
+            const int b = (d.nSeg - 1 - s) & 1;
+            CK(cudaStreamWaitEvent(d.adjStream, d.evRec[b], 0));
+            reverse(s, d.adjStream);
+            CK(cudaEventRecord(d.evAdj[b], d.adjStream));
+            if (s - 2 >= 0) issueRecompute(s - 2);
+        }
+        CK(cudaEventRecord(d.evJoin[0], d.recStream));
+        CK(cudaEventRecord(d.evJoin[1], d.adjStream));
+        CK(cudaStreamWaitEvent(h.stream, d.evJoin[0], 0));
+        CK(cudaStreamWaitEvent(h.stream, d.evJoin[1], 0));
+        // d.seg holds the last segment unless an earlier one went there
+        d.lastSegKept = d.nSeg < 3;
     }
     launch_adjoint_finish(a, h.stream);
     launch_force_adjoint(h.m, d.G, h.nx, h.ny, L, d.gfx, d.gfy, h.stream);

@@ -30,12 +30,17 @@ namespace lbib {
 // Programmatic dependent launch.  The stage kernels of a step are short and
 // many; launching each with programmatic stream serialization lets the
 // launch and block scheduling of a kernel overlap the end of the previous
-// one.  No kernel triggers its dependents early, so a kernel's blocks start
-// only once every block of the previous kernel has exited, and each kernel
-// begins with griddepcontrol.wait, which returns once the previous grid has
-// completed and its memory operations are visible.  Ordering is therefore the
-// same as plain stream order.  LBIB_NO_PDL=1 launches without the attribute.
+// one.  Every kernel except the adjoint step begins with griddepcontrol.wait,
+// which returns once the previous grid has completed and its memory
+// operations are visible, and none of those triggers its dependents early, so
+// their blocks start only once every block of the previous kernel has exited.
+// The adjoint step (k_adjoint.cu) triggers its dependents right after its own
+// wait, and loads the inputs that no kernel of the reverse pass writes before
+// that wait; a kernel launched after it therefore starts during its last wave,
+// while every kernel before it has completed.  Ordering is the same as plain
+// stream order.  LBIB_NO_PDL=1 launches without the attribute.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 inline bool pdl_enabled() {
     static const bool on = [] {
@@ -57,9 +62,10 @@ inline bool check_launches() {
     return on;
 }
 
+// A launch with (programmatic) or without programmatic stream serialization.
 template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       Args&&... args) {
+inline void launch_ex(bool programmatic, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                      cudaStream_t s, Args&&... args) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = grid;
     cfg.blockDim = block;
@@ -69,7 +75,7 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cfg.numAttrs = programmatic && pdl_enabled() ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
     if (check_launches()) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -84,6 +90,12 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
             }
         }
     }
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    launch_ex(true, kernel, grid, block, smem, s, std::forward<Args>(args)...);
 }
 
 // Direction tables: libs/LbmLib/include/Direction.hpp:34-44 and

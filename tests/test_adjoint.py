@@ -506,3 +506,39 @@ def test_force_record_parameter_gradients(lbib, tmp_path):
         checked += 1
     assert checked == 11 and np.isfinite(L0)
     sim.diff_end()
+
+
+@pytest.mark.parametrize("T,K", [(13, 4), (12, 6), (15, 3), (9, 5)])
+def test_overlapped_recompute_equals_serial(lbib, tmp_path, monkeypatch, T, K):
+    """The reverse pass of an FP32-shifted run with two segment buffers (the
+    next segment recomputed on a second stream while the current one is
+    reversed) gives bit for bit
+    the gradients of the one-buffer pass, on the first backward call after a
+    forward (the last segment kept) and on a repeated one (every segment
+    recomputed).  The per-domain rate gradients are sums by atomic adds over
+    the lattice (their order varies from run to run): within 1e-12 relative."""
+    paths = _cfg(species=2).write(str(tmp_path))
+    out = {}
+    for serial in ("1", "0"):
+        monkeypatch.setenv("LBIB_DIFF_SERIAL", serial)
+        P = _Problem(lbib, paths, T=T, K=K, steps_before=2)
+        P.sim.close()
+        P.sim = lbib.Simulation(paths, lbib.FP32_SHIFTED)  # FP32 states: the overlapped pass
+        P.sim.step(2)
+        P.sim.diff_begin(T, K)
+        g1 = P.grads()
+        g2 = P.sim.diff_backward(P.w)
+        out[serial] = (g1, g2)
+        P.sim.diff_end()
+        P.sim.close()
+    monkeypatch.delenv("LBIB_DIFF_SERIAL", raising=False)
+    def same(x, y, k, what):
+        if k == "rates":
+            np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-300, err_msg=what)
+        else:
+            np.testing.assert_array_equal(x, y, err_msg=what)
+    for i in range(2):
+        for k in ("force", "tau", "rates"):
+            same(out["0"][i][k], out["1"][i][k], k, f"call {i} {k}")
+    for k in ("force", "tau", "rates"):
+        same(out["0"][1][k], out["0"][0][k], k, f"repeat {k}")
