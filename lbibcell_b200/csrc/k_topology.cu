@@ -40,6 +40,24 @@ size_t topo_scan_bytes(int n) {
 // Connection.cpp:389-394), with the root taken only within a few ulps of
 // MAXLENGTH^2: the rounded root is monotonic, so well below it is below
 // MAXLENGTH and at or above it is not (and the other way round).
+// Position of the n-th (from 0) set bit of w; w has more than n set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned w, int n) {
+    int base = 0;
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        const unsigned low = (1u << sh) - 1u;
+        const int c = __popc(w & low);
+        if (n >= c) {
+            n -= c;
+            w >>= sh;
+            base += sh;
+        } else {
+            w &= low;
+        }
+    }
+    return base;
+}
+
 __device__ __forceinline__ bool shorter_than_max(double d2) {
     constexpr double m2 = kMAXLENGTH * kMAXLENGTH;
     if (d2 < m2 * (1.0 - 1e-12)) return true;
@@ -388,8 +406,8 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
             __syncthreads();
         }
     }
-    // the candidates as bits in id order, so that the serial visit below
-    // jumps from one to the next instead of stepping over every node
+    // the candidates as bits in id order, so that the visit below jumps from
+    // one to the next instead of stepping over every node
     const int nw = (len + 31) >> 5;
     for (int j = threadIdx.x; j < nw * 32; j += blockDim.x) {
         const bool cand = j < len && dirty[(int)(ord[j] & 0xffffffffu)];
@@ -397,47 +415,107 @@ __global__ void __launch_bounds__(256) coarsen_cell_kernel(MembraneDev m, TopoDe
         const unsigned bits = __ballot_sync(0xffffffffu, cand);
         if ((threadIdx.x & 31) == 0) visit[j >> 5] = bits;
     }
+    __shared__ unsigned wantBits[kCoarsenMax / 32];
+    for (int w = threadIdx.x; w < kCoarsenMax / 32; w += blockDim.x) wantBits[w] = 0u;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // The visit in id order, 32 candidates per round.  Each lane takes the
+        // next candidate place and tests it against the state at the start of
+        // the round.  The round keeps the places before T, where T is the
+        // first place whose outcome an earlier removal of the round changes:
+        // a candidate next to a removed node (its neighbour link changes), or
+        // a node that a removal makes a candidate at a later place (the id
+        // order visits it there).  The kept removals touch disjoint links, so
+        // they are applied together, and the next round starts at T.  The
+        // result is the one of the one-by-one visit.
+        const int lane = threadIdx.x;
         const int Ccap = m.Ccap;
         int removedHere = 0;
-        for (int j = 0;; ++j) {
-            // the next candidate at place >= j (a node that becomes one at an
-            // earlier place is not visited again, as in the id-order loop)
-            int w = j >> 5;
-            unsigned bits = w < nw ? visit[w] & (~0u << (j & 31)) : 0u;
-            while (bits == 0u && ++w < nw) bits = visit[w];
-            if (bits == 0u) break;
-            j = (w << 5) + __ffs(bits) - 1;
-            const int k = (int)(ord[j] & 0xffffffffu);
-            if (!dirty[k]) continue;
-            const int p = pl[k], q = nl[k];
-            const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
-            if (!shorter_than_max(dx * dx + dy * dy)) continue;
-            gone[k] = 1;
-            ++removedHere;
-            const int i = node[k];
-            const int h1 = hin[k], h2 = hout[k];
-            uint32_t dom = ringDomS;
-            const int desc = inDesc[k];
-            if (h1 < Ccap) {
-                t.connAlive[h1] = 0;
-                if (mixedDom) dom = m.cdom[h1];
-            } else {
-                t.ncAlive[h1 - Ccap] = 0;
-                if (mixedDom) dom = t.ncDom[h1 - Ccap];
+        int j0 = 0;
+        while (j0 < len) {
+            // the places of the next (up to) 32 candidates at or after j0
+            const int w0 = j0 >> 5;
+            unsigned word = w0 + lane < nw ? visit[w0 + lane] : 0u;
+            if (lane == 0) word &= ~0u << (j0 & 31);
+            const int cnt = __popc(word);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
             }
-            if (h2 < Ccap) t.connAlive[h2] = 0;
-            else t.ncAlive[h2 - Ccap] = 0;
-            t.ncA[i] = node[p]; t.ncB[i] = node[q]; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
-            nl[p] = q; pl[q] = p;
-            hout[p] = Ccap + i; hin[q] = Ccap + i;
-            inDesc[q] = desc;
-            dirty[p] = 1; dirty[q] = 1;
-            visit[rankOf[p] >> 5] |= 1u << (rankOf[p] & 31);
-            visit[rankOf[q] >> 5] |= 1u << (rankOf[q] & 31);
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            if (total == 0) {
+                j0 = (w0 + 32) << 5;
+                continue;
+            }
+            // lane l takes candidate l: the word holding it, then its bit
+            int src = 0;
+#pragma unroll
+            for (int st2 = 16; st2 > 0; st2 >>= 1)
+                if (__shfl_sync(0xffffffffu, incl, src + st2 - 1) <= lane) src += st2;
+            const bool valid = lane < total;
+            const int srcS = valid ? src : 31;
+            const unsigned srcWord = __shfl_sync(0xffffffffu, word, srcS);
+            const int before = __shfl_sync(0xffffffffu, incl - cnt, srcS);
+            const int P = valid ? ((w0 + srcS) << 5) + nth_set_bit(srcWord, lane - before) : 0x7fffffff;
+            int k = 0, p = 0, q = 0;
+            bool want = false;
+            if (valid) {
+                k = (int)(ord[P] & 0xffffffffu);
+                p = pl[k];
+                q = nl[k];
+                if (dirty[k]) {
+                    const double dx = sx[q] - sx[p], dy = sy[q] - sy[p];
+                    want = shorter_than_max(dx * dx + dy * dy);
+                }
+            }
+            const int rp = valid ? rankOf[p] : 0, rq = valid ? rankOf[q] : 0;
+            if (want) atomicOr(&wantBits[P >> 5], 1u << (P & 31));
+            __syncwarp();
+            // a removal before this place takes away this node's neighbour
+            const bool conflict = valid && ((rp < P && ((wantBits[rp >> 5] >> (rp & 31)) & 1u)) ||
+                                            (rq < P && ((wantBits[rq >> 5] >> (rq & 31)) & 1u)));
+            int T = 0x7fffffff;
+            if (conflict) T = P;
+            if (want) {  // the neighbours become candidates at their places
+                if (rp > P) T = min(T, rp);
+                if (rq > P) T = min(T, rq);
+            }
+            T = (int)__reduce_min_sync(0xffffffffu, (unsigned)T);
+            const int lastP = __shfl_sync(0xffffffffu, P, min(total, 32) - 1);
+            if (T > lastP) T = lastP + 1;
+            __syncwarp();
+            if (want) atomicAnd(&wantBits[P >> 5], ~(1u << (P & 31)));
+            if (want && P < T) {
+                gone[k] = 1;
+                ++removedHere;
+                const int i = node[k];
+                const int h1 = hin[k], h2 = hout[k];
+                uint32_t dom = ringDomS;
+                const int desc = inDesc[k];
+                if (h1 < Ccap) {
+                    t.connAlive[h1] = 0;
+                    if (mixedDom) dom = m.cdom[h1];
+                } else {
+                    t.ncAlive[h1 - Ccap] = 0;
+                    if (mixedDom) dom = t.ncDom[h1 - Ccap];
+                }
+                if (h2 < Ccap) t.connAlive[h2] = 0;
+                else t.ncAlive[h2 - Ccap] = 0;
+                t.ncA[i] = node[p]; t.ncB[i] = node[q]; t.ncDom[i] = dom; t.ncDesc[i] = desc; t.ncAlive[i] = 1;
+                nl[p] = q; pl[q] = p;
+                hout[p] = Ccap + i; hin[q] = Ccap + i;
+                inDesc[q] = desc;
+                dirty[p] = 1; dirty[q] = 1;
+                atomicOr(&visit[rp >> 5], 1u << (rp & 31));
+                atomicOr(&visit[rq >> 5], 1u << (rq & 31));
+            }
+            __syncwarp();
+            j0 = T;
         }
-        if (removedHere) atomicAdd(&m.topo->removed, removedHere);
+        removedHere = __reduce_add_sync(0xffffffffu, removedHere);
+        if (lane == 0 && removedHere) atomicAdd(&m.topo->removed, removedHere);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < len; k += blockDim.x) {
