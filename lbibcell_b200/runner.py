@@ -53,6 +53,11 @@ class Simulation:
                                             paths.get("force", "").encode(), paths.get("plugins", "").encode(),
                                             int(precision), int(device), ctypes.byref(h))
         self._h = h
+        # the arrays of the last per-step calls and their data pointers: a call
+        # with the same array (its contents rewritten in place) skips the
+        # checks and the pointer lookup
+        self._src = (None, None, 0, None)
+        self._areas = (None, None, 0, 0, 0)
         if rc:
             err = self._error()
             self.close()
@@ -104,9 +109,14 @@ class Simulation:
     def set_species_sources(self, rates: np.ndarray) -> None:
         """Every species' per-domain production rate at once ((S, n_domains)),
         one host-to-device copy; pinned host memory makes it asynchronous."""
-        r = np.ascontiguousarray(rates, np.float64)
-        n = r.shape[-1] if r.ndim else 0
-        self._check(self._L.lbib_set_species_sources(self._h, _p(r), int(n)))
+        ref, ptr, n, shape = self._src
+        if rates is not ref or rates.shape != shape:
+            r = np.ascontiguousarray(rates, np.float64)
+            n = int(r.shape[-1]) if r.ndim else 0
+            ptr = r.ctypes.data
+            if r is rates:
+                self._src = (r, ptr, n, r.shape)
+        self._check(self._L.lbib_set_species_sources(self._h, ptr, n))
 
     def set_profiling(self, on: bool) -> None:
         self._check(self._L.lbib_set_profiling(self._h, 1 if on else 0))
@@ -181,10 +191,14 @@ class Simulation:
     def areas_into(self, dom: np.ndarray, area: np.ndarray) -> int:
         """lbib_areas into caller-owned contiguous uint32 / float64 arrays
         (pinned or not): fills min(count, len) entries, returns the count."""
-        if dom.dtype != np.uint32 or area.dtype != np.float64 or not (dom.flags.c_contiguous and
-                                                                     area.flags.c_contiguous):
-            raise ValueError("areas_into needs contiguous uint32 and float64 arrays")
-        n = self._L.lbib_areas(self._h, _p(dom), _p(area), min(len(dom), len(area)))
+        rd, ra, pd, pa, cap = self._areas
+        if dom is not rd or area is not ra or cap != min(len(dom), len(area)):
+            if dom.dtype != np.uint32 or area.dtype != np.float64 or not (dom.flags.c_contiguous and
+                                                                         area.flags.c_contiguous):
+                raise ValueError("areas_into needs contiguous uint32 and float64 arrays")
+            pd, pa, cap = dom.ctypes.data, area.ctypes.data, min(len(dom), len(area))
+            self._areas = (dom, area, pd, pa, cap)
+        n = self._L.lbib_areas(self._h, pd, pa, cap)
         if n < 0:
             raise self._error()
         return n

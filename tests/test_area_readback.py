@@ -81,3 +81,41 @@ def test_areas_fp32_close_to_fp64(lbib, tmp_path):
         # areas differ by at most n 2^-26 (3.7e-6 at 250 nodes) plus the
         # FP64 sum's own rounding (~1e-8 here)
         assert abs(ab[d] - aa[d]) <= 250 * 2.0 ** -26 + 1e-7, (d, ab[d], aa[d])
+
+
+def test_per_step_calls_with_reused_arrays(lbib, tmp_path):
+    """The per-step loop of a coupled driver (source rates in, areas out),
+    with the same host arrays rewritten in place every step, gives the state
+    and the areas of the same loop with fresh arrays each step."""
+    paths = _tissue(tmp_path)
+    a = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    b = lbib.Simulation(paths, lbib.FP32_SHIFTED)
+    nd = a.domain_count()
+    cap = a.sizes()["cells"] + 8
+    src = np.zeros((1, nd))
+    dom, area = np.zeros(cap, np.uint32), np.zeros(cap)
+    rng = np.random.default_rng(3)
+    for step in range(12):
+        r = rng.uniform(0.0, 2e-3, (1, nd))
+        src[...] = r
+        a.set_species_sources(src)
+        a.step(1)
+        n = a.areas_into(dom, area)
+        b.set_species_sources(r.copy())
+        b.step(1)
+        d2, a2 = np.zeros(cap, np.uint32), np.zeros(cap)
+        n2 = b.areas_into(d2, a2)
+        assert n == n2
+        np.testing.assert_array_equal(dom[:n], d2[:n])
+        np.testing.assert_array_equal(area[:n], a2[:n])
+    la, lb = a.lattice(), b.lattice()
+    np.testing.assert_array_equal(la.g, lb.g)
+    np.testing.assert_array_equal(la.f, lb.f)
+    # a smaller output array after the cached one: only its length is filled
+    small_d, small_a = np.zeros(3, np.uint32), np.zeros(3)
+    a.step(1)
+    assert a.areas_into(small_d, small_a) == n
+    with pytest.raises(ValueError):
+        a.areas_into(np.zeros(cap, np.int64), area)
+    a.close()
+    b.close()
