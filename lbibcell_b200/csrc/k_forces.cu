@@ -223,11 +223,37 @@ __device__ __forceinline__ int bin_first(const ForceScratch& fs, int mcap, unsig
 }
 
 
-// The query of node i: candidates in the order the cell list returns them
-// (bins by row, then column, within a bin in id order: the list is rebuilt from
-// the id-ordered node map after every move, Geometry.cpp:531-535); those
-// farther than the radius (distance > radius) or with i's domain are dropped;
-// the first of the smallest distance wins (std::min_element with <).
+// The junction step's cell list: every node linked into its bin's list (in
+// no particular order), the previous call's heads cleared first.  No sort: the
+// query below breaks ties by (bin, node index) itself.
+__global__ void junction_unlink_kernel(ForceScratch fs) {
+    pdl_wait();
+    const int n = *fs.linkPrevM;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        fs.binHead[fs.linkKey[i]] = -1;
+}
+
+__global__ void junction_link_kernel(MembraneDev m, ForceScratch fs, int nx, int ny, Status* st) {
+    pdl_wait();
+    const int M = m.topo->M;
+    const bool halt = st->halt != 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *fs.linkPrevM = halt ? 0 : M;
+    if (halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const unsigned key = (unsigned)bin_index(m.y[i], ny) * (unsigned)nx + (unsigned)bin_index(m.x[i], nx);
+    fs.linkKey[i] = key;
+    fs.binNext[i] = atomicExch(&fs.binHead[key], i);
+}
+
+// The query of node i: the reference visits the candidates in the order its
+// cell list returns them (bins by row, then column, within a bin in id order:
+// the list is rebuilt from the id-ordered node map after every move,
+// Geometry.cpp:531-535), drops those farther than the radius (distance >
+// radius) or with i's domain, and keeps the first of the smallest distance
+// (std::min_element with <).  Here the bins are visited in that order and a
+// candidate of the same distance replaces the best one only within its bin
+// and with a smaller node index: the same node wins.
 __global__ void junction_query_kernel(MembraneDev m, ForceScratch fs, int nx, int ny, double radius, Status* st) {
     pdl_wait();
     if (st->halt) return;
@@ -239,20 +265,26 @@ __global__ void junction_query_kernel(MembraneDev m, ForceScratch fs, int nx, in
     const int bx0 = bin_index(xi - radius, nx), bx1 = bin_index(xi + radius, nx);
     const int by0 = bin_index(yi - radius, ny), by1 = bin_index(yi + radius, ny);
     int best = -1;
+    unsigned bestKey = 0;
     double bestD = 0.0;
+    int steps = 0;  // a well-formed list holds each node once
     for (int by = by0; by <= by1; ++by)
         for (int bx = bx0; bx <= bx1; ++bx) {
             const unsigned key = (unsigned)by * (unsigned)nx + (unsigned)bx;
-            for (int q = bin_first(fs, m.Mcap, key); q < m.Mcap && fs.binKeySorted[q] == key;
-                 ++q) {
-                const int j = fs.binIdxSorted[q];
+            for (int j = fs.binHead[key]; j >= 0; j = fs.binNext[j]) {
+                if (++steps > M) {
+                    raise_error(st, ERR_STATE, i, ST_BIO);
+                    fs.closest[i] = -1;
+                    return;
+                }
                 const double xj = m.x[j], yj = m.y[j];
                 const double d = sqrt((xj - xi) * (xj - xi) + (yj - yi) * (yj - yi));
                 if (d > radius) continue;
                 if (m.cdom[fs.inPos[j]] == avoid) continue;
-                if (best < 0 || d < bestD) {
+                if (best < 0 || d < bestD || (d == bestD && key == bestKey && j < best)) {
                     best = j;
                     bestD = d;
+                    bestKey = key;
                 }
             }
         }
@@ -341,7 +373,9 @@ int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double ra
                      Status* st, cudaStream_t s) {
     if (m.Mcap == 0) return 0;
     const int n = m.Mcap;
-    launch_cell_list(m, fs, nx, ny, s);
+    launch_pdl(conn_pos_kernel, (m.Ccap + 127) / 128, 128, 0, s, m, fs);
+    launch_pdl(junction_unlink_kernel, 148 * 4, 256, 0, s, fs);
+    launch_pdl(junction_link_kernel, (n + 255) / 256, 256, 0, s, m, fs, nx, ny, st);
     launch_pdl(junction_query_kernel, (n + 127) / 128, 128, 0, s, m, fs, nx, ny, radius, st);
     cudaMemsetAsync(fs.inCnt, 0, sizeof(int) * (n + 1), s);
     cudaMemsetAsync(fs.inFill, 0, sizeof(int) * n, s);
@@ -349,7 +383,7 @@ int launch_junctions(MembraneDev& m, ForceScratch& fs, int nx, int ny, double ra
     cub::DeviceScan::ExclusiveSum(fs.scanTmp, fs.scanTmpBytes, fs.inCnt, fs.inOff, n + 1, s);
     launch_pdl(junction_infill_kernel, (n + 255) / 256, 256, 0, s, m, fs, st);
     // ForceSolver::deleteForceType(7), then the new springs
-    return 7 + launch_force_edit(m, fs, 7, GEN_JUNCTION, 0.0, K, L0, st, s);
+    return 8 + launch_force_edit(m, fs, 7, GEN_JUNCTION, 0.0, K, L0, st, s);
 }
 
 int launch_tension_edit(MembraneDev& m, ForceScratch& fs, double force, Status* st, cudaStream_t s) {

@@ -69,6 +69,11 @@ struct ForceScratch {
     int sortBits;               // key bits: bins 0..nx*ny-1, nx*ny for unused slots
     int* binStart;              // nx*ny: first sorted position of each bin (checked on use)
     unsigned binCap;            // nx*ny
+    // the junction step's own cell list: per bin a linked list of its nodes
+    int* binHead;               // nx*ny: first node of the bin's list, -1 empty
+    int* binNext;               // Mcap: next node of the same bin, -1 end
+    unsigned* linkKey;          // Mcap: the bin each node was linked into
+    int* linkPrevM;             // 1: nodes linked by the last call (their heads are cleared by the next)
     int* closest;               // Mcap: closest node of another cell within the radius, -1: none
     int* inCnt; int* inOff;     // Mcap+1: nodes that found node i, and their offsets
     int* inList; int* inFill;   // Mcap

@@ -364,7 +364,7 @@ Handle::~Handle() {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
     fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
-    fr(fs.binStart);
+    fr(fs.binStart); fr(fs.binHead); fr(fs.binNext); fr(fs.linkKey); fr(fs.linkPrevM);
     fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -826,7 +826,7 @@ static void ensure_force_scratch(Handle& h, bool need = false) {
     ForceScratch& fs = h.fs;
     fr(fs.foffS); fr(fs.ftypeS); fr(fs.fpartnerS); fr(fs.fparS); fr(fs.cnt); fr(fs.scanTmp);
     fr(fs.binKey); fr(fs.binKeySorted); fr(fs.binIdx); fr(fs.binIdxSorted); fr(fs.sortTmp); fr(fs.closest);
-    fr(fs.binStart);
+    fr(fs.binStart); fr(fs.binHead); fr(fs.binNext); fr(fs.linkKey); fr(fs.linkPrevM);
     fr(fs.inCnt); fr(fs.inOff); fr(fs.inList); fr(fs.inFill);
     fs = ForceScratch{};
     fs.outPos = h.outPos;
@@ -850,6 +850,12 @@ static void ensure_force_scratch(Handle& h, bool need = false) {
         fs.binCap = (unsigned)h.L;
         fs.binStart = dalloc<int>(h.L);
         CK(cudaMemsetAsync(fs.binStart, 0xff, sizeof(int) * h.L, h.stream));
+        fs.binHead = dalloc<int>(h.L);
+        CK(cudaMemsetAsync(fs.binHead, 0xff, sizeof(int) * h.L, h.stream));
+        fs.binNext = dalloc<int>(n);
+        fs.linkKey = dalloc<unsigned>(n);
+        fs.linkPrevM = dalloc<int>(1);
+        CK(cudaMemsetAsync(fs.linkPrevM, 0, sizeof(int), h.stream));
         fs.closest = dalloc<int>(n);
         fs.inCnt = dalloc<int>(n + 1); fs.inOff = dalloc<int>(n + 1);
         fs.inList = dalloc<int>(n); fs.inFill = dalloc<int>(n);
