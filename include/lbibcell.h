@@ -269,6 +269,33 @@ int lbib_diff_fluid_seed(lbib_handle* h, const double* dLdf);
  * a negative LBIB_ERR_*. */
 int lbib_diff_force_params(lbib_handle* h, double* gPar, int cap);
 
+/* Differentiated runs with moving membrane nodes (the adjoint of
+ * GeometryNode::collectVelocity + move, GeometryNode.cpp:216-226, 245-254;
+ * no counterpart in the reference).  on != 0, after lbib_diff_begin, makes
+ * every following lbib_diff_forward move the nodes: step t spreads the node
+ * forces F_i from the positions after step t-1, runs the lattice step, and
+ * moves each node by the post-collision velocity interpolated at those
+ * positions.  The stencil of a node is the 4x4 lattice nodes within 2 lu of
+ * its position at the step; the perturbation of nodes on lattice lines
+ * (GeometryNode.cpp:155-214) is left out (its random jumps have no
+ * derivative).  The domain ids, the boundary nodes and the mass table stay
+ * those of lbib_diff_begin.  The positions of every step are stored:
+ * (T + 1) * M * 16 bytes more device memory.  dLdX[M][2], when non-NULL, is
+ * dL/dX of the final positions (a loss of the membrane's shape), joined to
+ * dLdC in lbib_diff_backward; the reverse pass then also carries dL/dX back
+ * through each step (the Dirac weights' derivative included), its gForce is
+ * dL/dF_i through both the lattice and the motion, and lbib_diff_positions
+ * gives dL/dX at the start.  Spreads use FP64 atomic adds: the last bits of
+ * the fields can differ between calls.  lbib_diff_force_params is refused in
+ * such a run.  on = 0 switches the motion off again. */
+int lbib_diff_motion(lbib_handle* h, int on, const double* dLdX);
+
+/* Of a run with moving nodes: xT[M][2] = the positions after the last
+ * lbib_diff_forward's final step, gX0[M][2] = dL/dX of the positions at the
+ * start from the last lbib_diff_backward (either may be NULL).  n must be the
+ * node count M. */
+int lbib_diff_positions(lbib_handle* h, double* xT, double* gX0, int n);
+
 /* Restores the snapshot taken by lbib_diff_begin (distributions, velocity and
  * force planes) and frees the run's device memory. */
 int lbib_diff_end(lbib_handle* h);

@@ -21,7 +21,7 @@ SYMBOLS = (
     "lbib_delete_all_forces", "lbib_nodes_within_radius", "lbib_closest_nodes", "lbib_write_vtk",
     "lbib_read_vtm_geometry", "lbib_upload_membrane", "lbib_cure_lattice", "lbib_accumulated_concentrations",
     "lbib_set_cell_types", "lbib_get_cell_types", "lbib_init_velocity", "lbib_diff_mass", "lbib_diff_fluid_seed",
-    "lbib_diff_force_params", "lbib_download_forces", "lbib_set_species_sources",
+    "lbib_diff_force_params", "lbib_diff_motion", "lbib_diff_positions", "lbib_download_forces", "lbib_set_species_sources",
 )
 
 _lib = None
@@ -101,6 +101,10 @@ def load() -> ctypes.CDLL:
     L.lbib_set_species_sources.argtypes = [vp, vp, ip]
     L.lbib_diff_force_params.restype = ip
     L.lbib_diff_force_params.argtypes = [vp, vp, ip]
+    L.lbib_diff_motion.restype = ip
+    L.lbib_diff_motion.argtypes = [vp, ip, vp]
+    L.lbib_diff_positions.restype = ip
+    L.lbib_diff_positions.argtypes = [vp, vp, vp, ip]
     L.lbib_download_forces.restype = ip
     L.lbib_download_forces.argtypes = [vp, vp, vp, vp, vp, ip]
     L.lbib_write_simulation.restype = ip

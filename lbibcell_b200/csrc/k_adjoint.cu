@@ -94,7 +94,11 @@ constexpr int kAdjBlock = LBIB_ADJOINT_BLOCK;
 // Real: the precision the states are stored in.  An FP32-shifted run stores
 // f_q - w_q in FP32 (and its species as they are); the reverse step reads
 // them back as f and runs its arithmetic in FP64 all the same.
-template <int NS, typename Real>
+// MOT: the motion form of a run with moving membrane nodes: the step's
+// velocity output has its own adjoint input a.gu (the nodes interpolate it),
+// the post-collision velocity is written to a.uo, and G holds this step's
+// dL/dF alone (the force field changes every step).
+template <int NS, typename Real, bool MOT = false>
 __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_step64(AdjointArgs a) {
     const int nx = a.nx, ny = a.ny;
     const size_t L = a.L;
@@ -299,6 +303,14 @@ __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_st
         for (int q = 0; q < 9; ++q) lf[q] = s1 * lf[q] - s1 * s1 * d;
     }
     // post-collision velocity uo = (sum c_q fs_q) / rho
+    if (MOT) {
+        muox += a.gu[n];
+        muoy += a.gu[L + n];
+        if (valid) {
+            a.uo[n] = uox;
+            a.uo[L + n] = uoy;
+        }
+    }
     double mrho = -(uox * muox + uoy * muoy) * rhoI;
     const double mjox = muox * rhoI, mjoy = muoy * rhoI;
 #pragma unroll
@@ -331,8 +343,13 @@ __global__ void __launch_bounds__(kAdjBlock, LBIB_ADJOINT_MIN_BLOCKS) adjoint_st
 #pragma unroll
         for (int q = 0; q < 9; ++q)
             a.qf[(size_t)q * L + n] = (float)((1.0 - tauI) * lf[q] + mrhoF + kCX[q] * mjx + kCY[q] * mjy);
-        a.G[n] += mfx;
-        a.G[L + n] += mfy;
+        if (MOT) {
+            a.G[n] = mfx;
+            a.G[L + n] = mfy;
+        } else {
+            a.G[n] += mfx;
+            a.G[L + n] += mfy;
+        }
     }
     // relaxation-time gradients: block sums into this block's own slots (the
     // same slots every step), reduced over blocks once at the end of the pass
@@ -402,6 +419,20 @@ void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s) {
         case 5: launch_ex(a.chained != 0, adjoint_step64<1, float>, grid, kAdjBlock, 0, s, a); break;
         case 6: launch_ex(a.chained != 0, adjoint_step64<2, float>, grid, kAdjBlock, 0, s, a); break;
         default: launch_ex(a.chained != 0, adjoint_step64<3, float>, grid, kAdjBlock, 0, s, a); break;
+    }
+}
+
+void launch_adjoint_step64_motion(const AdjointArgs& a, cudaStream_t s) {
+    const dim3 grid((unsigned)((a.nx + kAdjBlock - 1) / kAdjBlock), (unsigned)a.ny);
+    switch (a.S + (a.fp32 ? 4 : 0)) {
+        case 0: adjoint_step64<0, double, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 1: adjoint_step64<1, double, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 2: adjoint_step64<2, double, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 3: adjoint_step64<3, double, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 4: adjoint_step64<0, float, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 5: adjoint_step64<1, float, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        case 6: adjoint_step64<2, float, true><<<grid, kAdjBlock, 0, s>>>(a); break;
+        default: adjoint_step64<3, float, true><<<grid, kAdjBlock, 0, s>>>(a); break;
     }
 }
 

@@ -1636,6 +1636,146 @@ void launch_area_regulator_fixed(const MembraneDev& m, const int* cellOfDom, uns
                strength, maxsource, ctypeTab, acc, st);
 }
 
+// ---------------------------------------------------------------------------
+// Differentiated runs with moving membrane nodes.  The forward of one step is
+// the spread of the node forces from the step-start positions X, the lattice
+// step, then X' = X + (the post-collision velocity interpolated at X): the
+// reference's distributeForce, collide and collectVelocity + move
+// (GeometryNode.cpp:216-254) without the perturbation, whose random jumps
+// have no derivative.  The stencil follows from X (stencil_range of the
+// position itself: the 4x4 lattice nodes within 2 lu, the set the reference's
+// binding holds while the node stays in its unit cell).
+
+// d fast_cos / dx: the derivative of the approximation itself (its two
+// parabolas and the 0.225 correction), so that the gradients are those of
+// the forward as it is computed.
+__device__ __forceinline__ double fast_cos_deriv(const double x) {
+    const double halfPi = M_PI / 2.0;
+    const double doublePi = 2.0 * M_PI;
+    double tempx = x + halfPi;
+    if (tempx > M_PI) tempx -= doublePi;
+    double c, dc;
+    if (tempx < .00) {
+        c = 1.27323954 * tempx + 0.405284735 * tempx * tempx;
+        dc = 1.27323954 + 2.0 * 0.405284735 * tempx;
+    } else {
+        c = 1.27323954 * tempx - 0.405284735 * tempx * tempx;
+        dc = 1.27323954 - 2.0 * 0.405284735 * tempx;
+    }
+    // cs = 0.225 (c |c| - c) + c
+    return c < 0.0 ? dc * (1.0 + 0.225 * (-2.0 * c - 1.0)) : dc * (1.0 + 0.225 * (2.0 * c - 1.0));
+}
+
+__global__ void motion_spread_kernel(const double* X, const double* Y, const double* ax, const double* ay, int M,
+                                     int nx, int ny, size_t L, double* out, Status* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const double xi = X[i], yi = Y[i];
+    Stencil sc;
+    if (!stencil_range(xi, yi, nx, ny, sc)) {
+        raise_error(st, ERR_STENCIL, i, ST_SPREAD);
+        return;
+    }
+    const double vx = ax[i], vy = ay[i];
+    for (int k = 0; k < 16; ++k) {
+        int xk, yk;
+        stencil_slot(sc, k, xk, yk);
+        const size_t n = (size_t)yk * nx + xk;
+        const double dl = dirac((double)xk - xi, (double)yk - yi);
+        atomicAdd(out + n, dl * vx);
+        atomicAdd(out + L + n, dl * vy);
+    }
+}
+
+void launch_motion_spread(const double* X, const double* Y, const double* ax, const double* ay, int M, int nx,
+                          int ny, size_t L, double* out, Status* st, cudaStream_t s) {
+    if (M <= 0) return;
+    motion_spread_kernel<<<(M + 127) / 128, 128, 0, s>>>(X, Y, ax, ay, M, nx, ny, L, out, st);
+}
+
+template <typename Real>
+__global__ void motion_move_kernel(const double* X0, const double* Y0, double* X1, double* Y1, int M, const Real* u,
+                                   int nx, int ny, size_t L, Status* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const double xi = X0[i], yi = Y0[i];
+    Stencil sc;
+    if (!stencil_range(xi, yi, nx, ny, sc)) {
+        raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
+        X1[i] = xi;
+        Y1[i] = yi;
+        return;
+    }
+    double vx = 0.0, vy = 0.0;
+    for (int k = 0; k < 16; ++k) {
+        int xk, yk;
+        stencil_slot(sc, k, xk, yk);
+        const size_t n = (size_t)yk * nx + xk;
+        const double dl = dirac((double)xk - xi, (double)yk - yi);
+        vx += (double)u[n] * dl;
+        vy += (double)u[L + n] * dl;
+    }
+    const double CS = 1 / sqrt(3.0);
+    if (((vx * vx) + (vy * vy)) > CS) raise_error(st, ERR_SPEED, i, ST_INTERP_MOVE);
+    X1[i] = xi + vx;
+    Y1[i] = yi + vy;
+}
+
+template <typename Real>
+void launch_motion_move(const double* X0, const double* Y0, double* X1, double* Y1, int M, const Real* u, int nx,
+                        int ny, size_t L, Status* st, cudaStream_t s) {
+    if (M <= 0) return;
+    motion_move_kernel<Real><<<(M + 127) / 128, 128, 0, s>>>(X0, Y0, X1, Y1, M, u, nx, ny, L, st);
+}
+template void launch_motion_move<double>(const double*, const double*, double*, double*, int, const double*, int,
+                                         int, size_t, Status*, cudaStream_t);
+template void launch_motion_move<float>(const double*, const double*, double*, double*, int, const float*, int, int,
+                                        size_t, Status*, cudaStream_t);
+
+// With w(a) = 1 + fast_cos(pi/2 (a - X)) the weight of lattice node (a, b)
+// is w(a) w(b) / 16, and d/dX of it is -pi/2 fast_cos'(pi/2 (a - X)) w(b) / 16
+// (likewise in Y).  A node whose stencil leaves the lattice was refused by
+// the forward (ERR_STENCIL) and contributes nothing here.
+__global__ void motion_adjoint_kernel(const double* X, const double* Y, const double* fx, const double* fy,
+                                      double* lx, double* ly, const double* uo, const double* G, double* gfx,
+                                      double* gfy, int M, int nx, int ny, size_t L) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const double xi = X[i], yi = Y[i];
+    Stencil sc;
+    if (!stencil_range(xi, yi, nx, ny, sc)) return;
+    const double halfPi = M_PI / 2.0;
+    const double lamx = lx[i], lamy = ly[i], Fx = fx[i], Fy = fy[i];
+    double gX = 0.0, gY = 0.0, gx = 0.0, gy = 0.0;
+    for (int k = 0; k < 16; ++k) {
+        int xk, yk;
+        stencil_slot(sc, k, xk, yk);
+        const size_t n = (size_t)yk * nx + xk;
+        const double ax = halfPi * ((double)xk - xi), ay = halfPi * ((double)yk - yi);
+        const double wa = 1.0 + fast_cos(ax), wb = 1.0 + fast_cos(ay);
+        const double dl = (wa * wb) / 16.0;
+        const double dX = -halfPi * fast_cos_deriv(ax) * wb / 16.0;
+        const double dY = -halfPi * wa * fast_cos_deriv(ay) / 16.0;
+        const double Gx = G[n], Gy = G[L + n];
+        const double c = lamx * uo[n] + lamy * uo[L + n] + Fx * Gx + Fy * Gy;
+        gX += dX * c;
+        gY += dY * c;
+        gx += dl * Gx;
+        gy += dl * Gy;
+    }
+    lx[i] = lamx + gX;
+    ly[i] = lamy + gY;
+    gfx[i] += gx;
+    gfy[i] += gy;
+}
+
+void launch_motion_adjoint(const double* X, const double* Y, const double* fx, const double* fy, double* lx,
+                           double* ly, const double* uo, const double* G, double* gfx, double* gfy, int M, int nx,
+                           int ny, size_t L, cudaStream_t s) {
+    if (M <= 0) return;
+    motion_adjoint_kernel<<<(M + 127) / 128, 128, 0, s>>>(X, Y, fx, fy, lx, ly, uo, G, gfx, gfy, M, nx, ny, L);
+}
+
 }  // namespace lbib
 
 namespace lbib {

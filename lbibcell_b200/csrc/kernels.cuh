@@ -313,8 +313,13 @@ struct AdjointArgs {
     double* macc;          // L        dL/d rhoToAdd at each node, summed over steps (with massTab)
     double* part;          // adjoint_blocks * (1 + S): per-block relaxation-time partials
     double* grad;          // 1 + S + S*nDomains + nDomains (written by launch_adjoint_finish)
+    // moving-membrane runs only (the kernel is launched in its motion form):
+    const double* gu;      // 2*L      dL/d(post-collision velocity) of step t
+    double* uo;            // 2*L      the post-collision velocity of step t (output)
 };
 void launch_adjoint_step64(const AdjointArgs& a, cudaStream_t s);
+// The same step in its motion form (a.gu, a.uo; G overwritten), a plain launch.
+void launch_adjoint_step64_motion(const AdjointArgs& a, cudaStream_t s);
 // Converts n doubles to floats (the force field of an FP32-shifted run).
 void launch_to_float(const double* in, float* out, size_t n, cudaStream_t s);
 // Thread blocks of one adjoint launch (the rows of AdjointArgs::part).
@@ -327,6 +332,27 @@ void launch_set_iteration(Status* st, unsigned it, cudaStream_t s);
 // stencil slots of dirac * G(x) (k_membrane.cu).
 void launch_force_adjoint(const MembraneDev& m, const double* G, int nx, int ny, size_t L, double* gfx,
                           double* gfy, cudaStream_t s);
+
+// Differentiated runs with moving membrane nodes (k_membrane.cu).  The
+// stencil of each node follows from its position at the step (the 4x4
+// lattice nodes within 2 lu), its weights are calculateDiscreteDeltaDirac's.
+// out[n] += dirac(x_n - X_i) * (ax_i, ay_i) over every node's stencil (FP64
+// atomics: the spread of the node forces, or of dL/dX onto dL/du).
+void launch_motion_spread(const double* X, const double* Y, const double* ax, const double* ay, int M, int nx,
+                          int ny, size_t L, double* out, Status* st, cudaStream_t s);
+// X1 = X0 + the velocity interpolated from u at X0 (GeometryNode::collectVelocity
+// then move, GeometryNode.cpp:216-226, 245-254, without the perturbation).
+template <typename Real>
+void launch_motion_move(const double* X0, const double* Y0, double* X1, double* Y1, int M, const Real* u, int nx,
+                        int ny, size_t L, Status* st, cudaStream_t s);
+// Reverse of one step's spread, interpolation and move for node i at its
+// step-start position X: with lambda = dL/dX_after,
+//   lambda += sum_n grad_X dirac * (lambda . uo(n) + F_i . G(n)),
+//   gF_i   += sum_n dirac * G(n),
+// G = dL/d(force field) of the step, uo its post-collision velocity.
+void launch_motion_adjoint(const double* X, const double* Y, const double* fx, const double* fy, double* lx,
+                           double* ly, const double* uo, const double* G, double* gfx, double* gfy, int M, int nx,
+                           int ny, size_t L, cudaStream_t s);
 
 // Opt-in shared-memory sizes of the kernels that need more than 48 KB; called
 // once before any launch (and so before any stream capture).

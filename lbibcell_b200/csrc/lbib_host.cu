@@ -175,12 +175,25 @@ struct DiffCtx {
     bool forwardDone = false;
     bool lastSegKept = false;   // the forward left the last segment's states in seg
     bool backwardDone = false;  // gfx / gfy hold the last reverse pass's membrane-force gradient
+    // Moving membrane nodes (lbib_diff_motion): the positions after every
+    // step, pos + t * 2 * M = X after step t then Y (t = 0: the snapshot's),
+    // and the reverse pass's per-node and per-step planes.
+    bool motion = false;
+    int M = 0;                  // the membrane's node count at lbib_diff_begin
+    double* pos = nullptr;      // (T + 1) * 2 * M
+    double* lam = nullptr;      // 2 * M: dL/dX after the step being reversed
+    double* seedX = nullptr;    // 2 * M: dL/dX after the final step
+    bool haveSeedX = false;
+    double* gu = nullptr;       // 2 * L: dL/d(post-collision velocity) of one step
+    double* uo = nullptr;       // 2 * L: the post-collision velocity of one step
+    double* posAt(int t) const { return pos + (size_t)t * 2 * M; }
     char* state(int i) const { return i == 0 ? x0 : ck + (size_t)(i - 1) * stateBytes; }
     ~DiffCtx() {
         auto fr = [](void* p) { if (p) cudaFree(p); };
         fr(x0); fr(u0); fr(ck); fr(seg); fr(fin); fr(P[0]); fr(P[1]); fr(G); fr(force); fr(force32); fr(fxp);
         fr(fyp); fr(gfx); fr(gfy);
         fr(srcTab); fr(seed); fr(grad); fr(racc); fr(part); fr(st); fr(massTab); fr(macc); fr(seedF); fr(seg2);
+        fr(pos); fr(lam); fr(seedX); fr(gu); fr(uo);
         for (cudaEvent_t e : {evRec[0], evRec[1], evAdj[0], evAdj[1], evFork, evJoin[0], evJoin[1]})
             if (e) cudaEventDestroy(e);
         if (recStream) cudaStreamDestroy(recStream);
@@ -2193,9 +2206,32 @@ static void diff_forward_step_t(Handle& h, DiffCtx& d, const char* in, char* out
     else launch_stream_collide32(*(const LatticeArgs<float>*)&a, stream);
 }
 
-static void diff_forward_step(Handle& h, DiffCtx& d, const char* in, char* out, int t, cudaStream_t stream) {
+// Step t of a run with moving membrane nodes: the node forces spread from
+// the positions after step t-1, the lattice step, then (move) the positions
+// after step t.  The reverse pass replays it without the move: the positions
+// of every step are stored.
+static void diff_motion_spread(Handle& h, DiffCtx& d, int t, cudaStream_t stream) {
+    const double* X = d.posAt(t - 1);
+    CK(cudaMemsetAsync(d.force, 0, sizeof(double) * 2 * h.L, stream));
+    launch_motion_spread(X, X + d.M, d.fxp, d.fyp, d.M, h.nx, h.ny, h.L, d.force, d.st, stream);
+    if (d.rs == 4) launch_to_float(d.force, d.force32, 2 * h.L, stream);
+}
+
+static void diff_forward_step(Handle& h, DiffCtx& d, const char* in, char* out, int t, cudaStream_t stream,
+                              bool move = false) {
+    if (d.motion) diff_motion_spread(h, d, t, stream);
     if (d.rs == 8) diff_forward_step_t<double>(h, d, in, out, t, stream);
     else diff_forward_step_t<float>(h, d, in, out, t, stream);
+    if (d.motion && move) {
+        const double* X0 = d.posAt(t - 1);
+        double* X1 = d.posAt(t);
+        if (d.rs == 8)
+            launch_motion_move<double>(X0, X0 + d.M, X1, X1 + d.M, d.M, (const double*)h.u, h.nx, h.ny, h.L, d.st,
+                                       stream);
+        else
+            launch_motion_move<float>(X0, X0 + d.M, X1, X1 + d.M, d.M, (const float*)h.u, h.nx, h.ny, h.L, d.st,
+                                      stream);
+    }
 }
 
 static void diff_check_status(Handle& h, DiffCtx& d) {
@@ -2210,8 +2246,12 @@ static void diff_forward(Handle& h, DiffCtx& d) {
     MembraneDev mp = h.m;
     mp.fx = d.fxp;
     mp.fy = d.fyp;
-    launch_spread<double>(mp, h.tiles, d.force, h.nx, h.ny, L, d.st, d.it0, h.stream);
-    if (d.rs == 4) launch_to_float(d.force, d.force32, 2 * L, h.stream);
+    if (!d.motion) {
+        // after a moving-node pass the field holds values outside the force tiles
+        if (d.pos != nullptr) CK(cudaMemsetAsync(d.force, 0, sizeof(double) * 2 * L, h.stream));
+        launch_spread<double>(mp, h.tiles, d.force, h.nx, h.ny, L, d.st, d.it0, h.stream);
+        if (d.rs == 4) launch_to_float(d.force, d.force32, 2 * L, h.stream);
+    }
     // two scratch states for the steps between checkpoints (the segment
     // buffer, free during the forward pass; with K = 2 one is enough, with
     // K = 1 every state but the last is a checkpoint)
@@ -2226,7 +2266,7 @@ static void diff_forward(Handle& h, DiffCtx& d) {
         else if (t == d.T) out = d.fin;
         else if (t > lastBase) out = d.seg + (size_t)(t - lastBase - 1) * d.stateBytes;
         else out = scratch[t & 1];
-        diff_forward_step(h, d, in, out, t, h.stream);
+        diff_forward_step(h, d, in, out, t, h.stream, true);
         in = out;
     }
     d.lastSegKept = true;
@@ -2272,7 +2312,17 @@ static void diff_backward(Handle& h, DiffCtx& d) {
     // Segment s (steps base+1 .. base+len) is reversed from the states
     // base .. base+len-1: the checkpoint, then its recomputed states in a
     // segment buffer (d.seg always, or alternately d.seg and d.seg2).
-    const bool two = d.seg2 != nullptr;
+    // (a run with moving nodes refills the one force field every step: serial)
+    const bool two = d.seg2 != nullptr && !d.motion;
+    if (d.motion) {
+        if (d.haveSeedX)
+            CK(cudaMemcpyAsync(d.lam, d.seedX, sizeof(double) * 2 * d.M, cudaMemcpyDeviceToDevice, h.stream));
+        else CK(cudaMemsetAsync(d.lam, 0, sizeof(double) * 2 * d.M, h.stream));
+        if (d.M) {
+            CK(cudaMemsetAsync(d.gfx, 0, sizeof(double) * d.M, h.stream));
+            CK(cudaMemsetAsync(d.gfy, 0, sizeof(double) * d.M, h.stream));
+        }
+    }
     auto bufOf = [&](int s) -> char* { return two && ((d.nSeg - 1 - s) & 1) ? d.seg2 : d.seg; };
     auto segState = [&](int s, int j) -> char* {  // state s*K + j, 0 <= j < len
         return j == 0 ? d.state(s) : bufOf(s) + (size_t)(j - 1) * d.stateBytes;
@@ -2300,7 +2350,25 @@ static void diff_backward(Handle& h, DiffCtx& d) {
             a.qg = d.P[t & 1] + 9 * L;
             a.iteration = d.it0 + (unsigned)(t - 1);
             a.chained = t < base + segLen(s);  // the segment's first step follows its recompute
-            launch_adjoint_step64(a, stream);
+            if (!d.motion) {
+                launch_adjoint_step64(a, stream);
+                continue;
+            }
+            // moving nodes: dL/du of this step is the spread of dL/dX after
+            // it (the interpolation's transpose), the force field is the one
+            // spread from the step-start positions, and the step's G and
+            // velocity then carry dL/dX back to those positions
+            const double* X = d.posAt(t - 1);
+            CK(cudaMemsetAsync(d.gu, 0, sizeof(double) * 2 * L, stream));
+            launch_motion_spread(X, X + d.M, d.lam, d.lam + d.M, d.M, h.nx, h.ny, L, d.gu, d.st, stream);
+            CK(cudaMemsetAsync(d.force, 0, sizeof(double) * 2 * L, stream));
+            launch_motion_spread(X, X + d.M, d.fxp, d.fyp, d.M, h.nx, h.ny, L, d.force, d.st, stream);
+            a.gu = d.gu;
+            a.uo = d.uo;
+            a.chained = 0;
+            launch_adjoint_step64_motion(a, stream);
+            launch_motion_adjoint(X, X + d.M, d.fxp, d.fyp, d.lam, d.lam + d.M, d.uo, d.G, d.gfx, d.gfy, d.M, h.nx,
+                                  h.ny, L, stream);
         }
     };
     const bool keptLast = d.lastSegKept;
@@ -2339,8 +2407,43 @@ static void diff_backward(Handle& h, DiffCtx& d) {
         d.lastSegKept = d.nSeg < 3;
     }
     launch_adjoint_finish(a, h.stream);
-    launch_force_adjoint(h.m, d.G, h.nx, h.ny, L, d.gfx, d.gfy, h.stream);
+    if (!d.motion) launch_force_adjoint(h.m, d.G, h.nx, h.ny, L, d.gfx, d.gfy, h.stream);
     CK(cudaGetLastError());
+}
+
+// Switches a differentiated run to moving membrane nodes (lbib_diff_motion).
+static void diff_set_motion(Handle& h, DiffCtx& d, bool on) {
+    if (!on) {
+        d.motion = false;
+        return;
+    }
+    if (d.motion) return;
+    if (d.pos != nullptr) {  // switched on before: the buffers and the snapshot positions are kept
+        d.motion = true;
+        d.forwardDone = false;
+        return;
+    }
+    const size_t L = h.L;
+    const int M = h.m.M;
+    const size_t bytes = sizeof(double) * ((size_t)(d.T + 1) * 2 * M + 4 * (size_t)M + 4 * L);
+    size_t freeB = 0, totalB = 0;
+    CK(cudaMemGetInfo(&freeB, &totalB));
+    if (bytes + (256u << 20) > freeB)
+        fail(ERR_CAPACITY, "moving-node differentiated run needs " + std::to_string(bytes >> 20) +
+                               " MiB of device memory, " + std::to_string(freeB >> 20) + " MiB free");
+    d.M = M;
+    d.pos = dalloc<double>((size_t)(d.T + 1) * 2 * M + 1);
+    d.lam = dalloc<double>(2 * (size_t)M + 1);
+    d.seedX = dalloc<double>(2 * (size_t)M + 1);
+    d.gu = dalloc<double>(2 * L);
+    d.uo = dalloc<double>(2 * L);
+    if (M) {
+        CK(cudaMemcpyAsync(d.pos, h.m.x, sizeof(double) * M, cudaMemcpyDeviceToDevice, h.stream));
+        CK(cudaMemcpyAsync(d.pos + M, h.m.y, sizeof(double) * M, cudaMemcpyDeviceToDevice, h.stream));
+    }
+    CK(cudaStreamSynchronize(h.stream));
+    d.motion = true;
+    d.forwardDone = false;
 }
 
 }  // namespace lbib
@@ -2967,6 +3070,8 @@ int lbib_diff_force_params(lbib_handle* hh, double* gPar, int cap) {
         CK(cudaSetDevice(h.device));
         if (!h.diff || !h.diff->backwardDone)
             lbib::fail(LBIB_ERR_STATE, "lbib_diff_force_params before lbib_diff_backward");
+        if (h.diff->motion)
+            lbib::fail(LBIB_ERR_STATE, "lbib_diff_force_params: the records' positions move in this run");
         if (cap < 0 || (cap > 0 && !gPar)) lbib::fail(LBIB_ERR_INPUT, "lbib_diff_force_params: bad output buffer");
         lbib::pull_topology(h);
         const int M = h.m.M;
@@ -3059,6 +3164,41 @@ int lbib_diff_fluid_seed(lbib_handle* hh, const double* dLdf) {
         CK(cudaMemcpyAsync(d.seedF, nat.data(), sizeof(double) * 9 * L, cudaMemcpyHostToDevice, h.stream));
         CK(cudaStreamSynchronize(h.stream));
     }
+    API_END
+}
+
+int lbib_diff_motion(lbib_handle* hh, int on, const double* dLdX) {
+    API_BEGIN(hh)
+    if (!h.diff) lbib::fail(LBIB_ERR_STATE, "lbib_diff_motion before lbib_diff_begin");
+    lbib::DiffCtx& d = *h.diff;
+    if (on && h.m.M == 0) lbib::fail(LBIB_ERR_STATE, "lbib_diff_motion: the geometry has no membrane nodes");
+    lbib::diff_set_motion(h, d, on != 0);
+    d.haveSeedX = false;
+    if (on && dLdX) {
+        const int M = d.M;
+        std::vector<double> v(2 * (size_t)M);
+        for (int i = 0; i < M; ++i) { v[i] = dLdX[2 * i]; v[M + i] = dLdX[2 * i + 1]; }
+        CK(cudaMemcpyAsync(d.seedX, v.data(), sizeof(double) * 2 * M, cudaMemcpyHostToDevice, h.stream));
+        CK(cudaStreamSynchronize(h.stream));
+        d.haveSeedX = true;
+    }
+    API_END
+}
+
+int lbib_diff_positions(lbib_handle* hh, double* xT, double* gX0, int n) {
+    API_BEGIN(hh)
+    if (!h.diff || !h.diff->motion) lbib::fail(LBIB_ERR_STATE, "lbib_diff_positions outside a moving-node run");
+    lbib::DiffCtx& d = *h.diff;
+    if (n != d.M) lbib::fail(LBIB_ERR_INPUT, "lbib_diff_positions: n must be the membrane's node count");
+    if (xT && !d.forwardDone) lbib::fail(LBIB_ERR_STATE, "lbib_diff_positions: no forward pass yet");
+    if (gX0 && !d.backwardDone) lbib::fail(LBIB_ERR_STATE, "lbib_diff_positions: no reverse pass yet");
+    std::vector<double> v(2 * (size_t)n);
+    auto put = [&](const double* dev, double* out) {
+        CK(cudaMemcpy(v.data(), dev, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) { out[2 * i] = v[i]; out[2 * i + 1] = v[n + i]; }
+    };
+    if (n && xT) put(d.posAt(d.T), xT);
+    if (n && gX0) put(d.lam, gX0);
     API_END
 }
 

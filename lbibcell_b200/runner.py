@@ -362,6 +362,21 @@ class Simulation:
             raise self._error()
         return g
 
+    def diff_motion(self, on: bool = True, dLdX=None) -> None:
+        """Moving membrane nodes in the next forward passes (the motion and its
+        adjoint); dLdX (M, 2) is dL/d of the final positions, or None."""
+        a = None if dLdX is None else np.ascontiguousarray(dLdX, np.float64)
+        self._check(self._L.lbib_diff_motion(self._h, 1 if on else 0, _p(a)))
+
+    def diff_positions(self, grad: bool = False):
+        """Final positions (M, 2) of the last forward pass; with grad, also
+        dL/dX (M, 2) of the starting positions from the last backward pass."""
+        M = self.sizes()["M"]
+        xT = np.zeros((M, 2))
+        g0 = np.zeros((M, 2)) if grad else None
+        self._check(self._L.lbib_diff_positions(self._h, _p(xT), _p(g0), M))
+        return (xT, g0) if grad else xT
+
     def forces(self) -> Dict[str, np.ndarray]:
         """The ForceSolver's records in device order (by node, then insertion):
         type, id1, id2 (partner id or 0) and par (n, 4)."""
