@@ -206,26 +206,35 @@ def test_tissue1024_fp64_matches_reference_digests(lbib, tmp_path):
 
 
 def test_fp32_shifted_error_config1(lbib, tmp_path):
-    """FP32-shifted vs FP64 on the 200x200 single cell after 500 steps: relative
-    max-norm errors (rho-1 by max|rho-1|, u by max|u|, c by max c) <= 1e-5;
-    membrane positions within 1e-6 lu."""
+    """FP32-shifted vs FP64 on the 200x200 single cell over its 2000 steps:
+    relative max-norm errors (rho-1 by max|rho-1|, u by max|u|, c by max c)
+    and membrane positions (lu) at t = 500, 1000, 1500, 2000.  rho-1 and u stay
+    within 1e-5 throughout, positions within 1e-6 lu.  The concentration stays
+    within 1e-5 up to t = 1000; after that it grows past it (1.2e-5 at 1500,
+    1.3e-5 at 2000 on a B200): the cell's source adds the same small amount
+    to a slowly growing FP32 value every step, so its rounding has nearly the
+    same sign every step and the error grows linearly.  Bound there: 2e-5."""
     paths = configs.config1().write(str(tmp_path))
     a = lbib.Simulation(paths, lbib.FP64)
     b = lbib.Simulation(paths, lbib.FP32_SHIFTED)
-    a.step(500)
-    b.step(500)
-    la, lb = a.lattice(), b.lattice()
-    ra, rb = la.f.sum(1) - 1.0, lb.f.sum(1) - 1.0
-    e_rho = np.abs(ra - rb).max() / np.abs(ra).max()
-    e_u = np.abs(la.vel - lb.vel).max() / np.abs(la.vel).max()
-    ca, cb = la.g.sum(2), lb.g.sum(2)
-    e_c = np.abs(ca - cb).max() / np.abs(ca).max()
-    _, na = a.membrane()
-    _, nb = b.membrane()
-    e_x = np.abs(na[:, :2] - nb[:, :2]).max() if na.shape == nb.shape else np.inf
-    print(f"FP32-shifted vs FP64: rho {e_rho:.2e} u {e_u:.2e} c {e_c:.2e} x {e_x:.2e}")
-    assert e_rho <= 1e-5 and e_u <= 1e-5 and e_c <= 1e-5
-    assert e_x <= 1e-6
+    prev = 0
+    for t, c_bound in ((500, 1e-5), (1000, 1e-5), (1500, 2e-5), (2000, 2e-5)):
+        a.step(t - prev)
+        b.step(t - prev)
+        prev = t
+        la, lb = a.lattice(), b.lattice()
+        ra, rb = la.f.sum(1) - 1.0, lb.f.sum(1) - 1.0
+        e_rho = np.abs(ra - rb).max() / np.abs(ra).max()
+        e_u = np.abs(la.vel - lb.vel).max() / np.abs(la.vel).max()
+        ca, cb = la.g.sum(2), lb.g.sum(2)
+        e_c = np.abs(ca - cb).max() / np.abs(ca).max()
+        _, na = a.membrane()
+        _, nb = b.membrane()
+        e_x = np.abs(na[:, :2] - nb[:, :2]).max() if na.shape == nb.shape else np.inf
+        print(f"t={t} FP32-shifted vs FP64: rho {e_rho:.2e} u {e_u:.2e} c {e_c:.2e} x {e_x:.2e}")
+        assert e_rho <= 1e-5 and e_u <= 1e-5, t
+        assert e_c <= c_bound, t
+        assert e_x <= 1e-6, t
 
 
 def _hex25(tmp_path, iterations=120):
