@@ -576,6 +576,22 @@ def main():
         fwd_ms = dist_max(d.last_timing()["total_ms"], world)
         g = d.diff_backward(seed)
         bwd_ms = dist_max(d.last_timing()["total_ms"], world)
+        # the same run with moving membrane nodes (the motion and its adjoint),
+        # a loss of the final positions joined to the concentrations' seed
+        _, st0 = d.membrane()
+        d.diff_motion(True, np.random.default_rng(1).normal(size=(st0.shape[0], 2)))
+        d.diff_forward()  # untimed: first touch of the position store
+        d.diff_backward(seed)
+        torch.cuda.synchronize()
+        d.diff_forward()
+        fwdm = dist_max(d.last_timing()["total_ms"], world)
+        gm = d.diff_backward(seed)
+        bwdm = dist_max(d.last_timing()["total_ms"], world)
+        xT, gx0 = d.diff_positions(grad=True)
+        moving = {"forward_ms": fwdm, "backward_ms": bwdm, "adjoint_over_forward": bwdm / fwdm,
+                  "membrane_nodes": int(st0.shape[0]),
+                  "max_displacement_lu": float(np.abs(xT - st0[:, :2]).max()),
+                  "grad_finite": bool(np.isfinite(gm["force"]).all() and np.isfinite(gx0).all())}
         d.diff_end()
         d.close()
         # the same run on an FP32-shifted handle (FP32 forward and states)
@@ -602,7 +618,7 @@ def main():
                    "forward_mlups": world * AL * T / (fwd_ms / 1e3) / 1e6,
                    "backward_note": "segment recompute from checkpoints + adjoint steps",
                    "grad_finite": bool(np.isfinite(g["force"]).all() and np.isfinite(g["tau"]).all()),
-                   "fp32": adjoint_fp32}
+                   "fp32": adjoint_fp32, "moving_nodes": moving}
 
     # ---- FP32-shifted error at fixed horizons (independent of --steps) -------
     horizons = None

@@ -1666,54 +1666,73 @@ __device__ __forceinline__ double fast_cos_deriv(const double x) {
     return c < 0.0 ? dc * (1.0 + 0.225 * (-2.0 * c - 1.0)) : dc * (1.0 + 0.225 * (2.0 * c - 1.0));
 }
 
+// Sixteen lanes per membrane node, one per stencil slot (two nodes per warp):
+// a node's 16 scattered lattice reads are issued at once instead of one
+// after another, and the sums over the slots are shuffles within the lanes'
+// group of 16 (every lane of the warp takes part, in range or not).
+constexpr int kMotionBlock = 128;
+
+__device__ __forceinline__ double group16_sum(double v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void motion_spread_kernel(const double* X, const double* Y, const double* ax, const double* ay, int M,
                                      int nx, int ny, size_t L, double* out, Status* st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t >> 4), k = (int)(t & 15);
     if (i >= M) return;
     const double xi = X[i], yi = Y[i];
     Stencil sc;
     if (!stencil_range(xi, yi, nx, ny, sc)) {
-        raise_error(st, ERR_STENCIL, i, ST_SPREAD);
+        if (k == 0) raise_error(st, ERR_STENCIL, i, ST_SPREAD);
         return;
     }
-    const double vx = ax[i], vy = ay[i];
-    for (int k = 0; k < 16; ++k) {
-        int xk, yk;
-        stencil_slot(sc, k, xk, yk);
-        const size_t n = (size_t)yk * nx + xk;
-        const double dl = dirac((double)xk - xi, (double)yk - yi);
-        atomicAdd(out + n, dl * vx);
-        atomicAdd(out + L + n, dl * vy);
-    }
+    int xk, yk;
+    stencil_slot(sc, k, xk, yk);
+    const size_t n = (size_t)yk * nx + xk;
+    const double dl = dirac((double)xk - xi, (double)yk - yi);
+    atomicAdd(out + n, dl * ax[i]);
+    atomicAdd(out + L + n, dl * ay[i]);
 }
 
 void launch_motion_spread(const double* X, const double* Y, const double* ax, const double* ay, int M, int nx,
                           int ny, size_t L, double* out, Status* st, cudaStream_t s) {
     if (M <= 0) return;
-    motion_spread_kernel<<<(M + 127) / 128, 128, 0, s>>>(X, Y, ax, ay, M, nx, ny, L, out, st);
+    const unsigned blocks = (unsigned)(((long long)M * 16 + kMotionBlock - 1) / kMotionBlock);
+    motion_spread_kernel<<<blocks, kMotionBlock, 0, s>>>(X, Y, ax, ay, M, nx, ny, L, out, st);
 }
 
 template <typename Real>
 __global__ void motion_move_kernel(const double* X0, const double* Y0, double* X1, double* Y1, int M, const Real* u,
                                    int nx, int ny, size_t L, Status* st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
-    const double xi = X0[i], yi = Y0[i];
-    Stencil sc;
-    if (!stencil_range(xi, yi, nx, ny, sc)) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t >> 4), k = (int)(t & 15);
+    double xi = 0.0, yi = 0.0, vx = 0.0, vy = 0.0;
+    bool ok = false;
+    if (i < M) {
+        xi = X0[i];
+        yi = Y0[i];
+        Stencil sc;
+        ok = stencil_range(xi, yi, nx, ny, sc);
+        if (ok) {
+            int xk, yk;
+            stencil_slot(sc, k, xk, yk);
+            const size_t n = (size_t)yk * nx + xk;
+            const double dl = dirac((double)xk - xi, (double)yk - yi);
+            vx = (double)u[n] * dl;
+            vy = (double)u[L + n] * dl;
+        }
+    }
+    vx = group16_sum(vx);
+    vy = group16_sum(vy);
+    if (i >= M || k != 0) return;
+    if (!ok) {
         raise_error(st, ERR_STENCIL, i, ST_INTERP_MOVE);
         X1[i] = xi;
         Y1[i] = yi;
         return;
-    }
-    double vx = 0.0, vy = 0.0;
-    for (int k = 0; k < 16; ++k) {
-        int xk, yk;
-        stencil_slot(sc, k, xk, yk);
-        const size_t n = (size_t)yk * nx + xk;
-        const double dl = dirac((double)xk - xi, (double)yk - yi);
-        vx += (double)u[n] * dl;
-        vy += (double)u[L + n] * dl;
     }
     const double CS = 1 / sqrt(3.0);
     if (((vx * vx) + (vy * vy)) > CS) raise_error(st, ERR_SPEED, i, ST_INTERP_MOVE);
@@ -1725,7 +1744,8 @@ template <typename Real>
 void launch_motion_move(const double* X0, const double* Y0, double* X1, double* Y1, int M, const Real* u, int nx,
                         int ny, size_t L, Status* st, cudaStream_t s) {
     if (M <= 0) return;
-    motion_move_kernel<Real><<<(M + 127) / 128, 128, 0, s>>>(X0, Y0, X1, Y1, M, u, nx, ny, L, st);
+    const unsigned blocks = (unsigned)(((long long)M * 16 + kMotionBlock - 1) / kMotionBlock);
+    motion_move_kernel<Real><<<blocks, kMotionBlock, 0, s>>>(X0, Y0, X1, Y1, M, u, nx, ny, L, st);
 }
 template void launch_motion_move<double>(const double*, const double*, double*, double*, int, const double*, int,
                                          int, size_t, Status*, cudaStream_t);
@@ -1739,30 +1759,39 @@ template void launch_motion_move<float>(const double*, const double*, double*, d
 __global__ void motion_adjoint_kernel(const double* X, const double* Y, const double* fx, const double* fy,
                                       double* lx, double* ly, const double* uo, const double* G, double* gfx,
                                       double* gfy, int M, int nx, int ny, size_t L) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
-    const double xi = X[i], yi = Y[i];
-    Stencil sc;
-    if (!stencil_range(xi, yi, nx, ny, sc)) return;
-    const double halfPi = M_PI / 2.0;
-    const double lamx = lx[i], lamy = ly[i], Fx = fx[i], Fy = fy[i];
-    double gX = 0.0, gY = 0.0, gx = 0.0, gy = 0.0;
-    for (int k = 0; k < 16; ++k) {
-        int xk, yk;
-        stencil_slot(sc, k, xk, yk);
-        const size_t n = (size_t)yk * nx + xk;
-        const double ax = halfPi * ((double)xk - xi), ay = halfPi * ((double)yk - yi);
-        const double wa = 1.0 + fast_cos(ax), wb = 1.0 + fast_cos(ay);
-        const double dl = (wa * wb) / 16.0;
-        const double dX = -halfPi * fast_cos_deriv(ax) * wb / 16.0;
-        const double dY = -halfPi * wa * fast_cos_deriv(ay) / 16.0;
-        const double Gx = G[n], Gy = G[L + n];
-        const double c = lamx * uo[n] + lamy * uo[L + n] + Fx * Gx + Fy * Gy;
-        gX += dX * c;
-        gY += dY * c;
-        gx += dl * Gx;
-        gy += dl * Gy;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t >> 4), k = (int)(t & 15);
+    double gX = 0.0, gY = 0.0, gx = 0.0, gy = 0.0, lamx = 0.0, lamy = 0.0;
+    bool ok = false;
+    if (i < M) {
+        const double xi = X[i], yi = Y[i];
+        Stencil sc;
+        ok = stencil_range(xi, yi, nx, ny, sc);
+        if (ok) {
+            const double halfPi = M_PI / 2.0;
+            lamx = lx[i];
+            lamy = ly[i];
+            int xk, yk;
+            stencil_slot(sc, k, xk, yk);
+            const size_t n = (size_t)yk * nx + xk;
+            const double ax = halfPi * ((double)xk - xi), ay = halfPi * ((double)yk - yi);
+            const double wa = 1.0 + fast_cos(ax), wb = 1.0 + fast_cos(ay);
+            const double dl = (wa * wb) / 16.0;
+            const double dX = -halfPi * fast_cos_deriv(ax) * wb / 16.0;
+            const double dY = -halfPi * wa * fast_cos_deriv(ay) / 16.0;
+            const double Gx = G[n], Gy = G[L + n];
+            const double c = lamx * uo[n] + lamy * uo[L + n] + fx[i] * Gx + fy[i] * Gy;
+            gX = dX * c;
+            gY = dY * c;
+            gx = dl * Gx;
+            gy = dl * Gy;
+        }
     }
+    gX = group16_sum(gX);
+    gY = group16_sum(gY);
+    gx = group16_sum(gx);
+    gy = group16_sum(gy);
+    if (!ok || k != 0) return;
     lx[i] = lamx + gX;
     ly[i] = lamy + gY;
     gfx[i] += gx;
@@ -1773,7 +1802,8 @@ void launch_motion_adjoint(const double* X, const double* Y, const double* fx, c
                            double* ly, const double* uo, const double* G, double* gfx, double* gfy, int M, int nx,
                            int ny, size_t L, cudaStream_t s) {
     if (M <= 0) return;
-    motion_adjoint_kernel<<<(M + 127) / 128, 128, 0, s>>>(X, Y, fx, fy, lx, ly, uo, G, gfx, gfy, M, nx, ny, L);
+    const unsigned blocks = (unsigned)(((long long)M * 16 + kMotionBlock - 1) / kMotionBlock);
+    motion_adjoint_kernel<<<blocks, kMotionBlock, 0, s>>>(X, Y, fx, fy, lx, ly, uo, G, gfx, gfy, M, nx, ny, L);
 }
 
 }  // namespace lbib
