@@ -576,8 +576,15 @@ def main():
         fwd_ms = dist_max(d.last_timing()["total_ms"], world)
         g = d.diff_backward(seed)
         bwd_ms = dist_max(d.last_timing()["total_ms"], world)
-        # the same run with moving membrane nodes (the motion and its adjoint),
-        # a loss of the final positions joined to the concentrations' seed
+        d.diff_end()
+        # The same workload with moving membrane nodes (the motion and its
+        # adjoint), a loss of the final positions joined to the concentrations'
+        # seed.  The node forces stay those of one force evaluation for the
+        # whole run, so over long runs they push nodes to the lattice's edge
+        # (a refused stencil at T = 2000); 200 steps move them up to 0.65 lu.
+        Tm = min(T, 200)
+        Km = max(1, Tm // 20)
+        d.diff_begin(Tm, Km)
         _, st0 = d.membrane()
         d.diff_motion(True, np.random.default_rng(1).normal(size=(st0.shape[0], 2)))
         d.diff_forward()  # untimed: first touch of the position store
@@ -588,7 +595,7 @@ def main():
         gm = d.diff_backward(seed)
         bwdm = dist_max(d.last_timing()["total_ms"], world)
         xT, gx0 = d.diff_positions(grad=True)
-        moving = {"forward_ms": fwdm, "backward_ms": bwdm, "adjoint_over_forward": bwdm / fwdm,
+        moving = {"T": Tm, "K": Km, "forward_ms": fwdm, "backward_ms": bwdm, "adjoint_over_forward": bwdm / fwdm,
                   "membrane_nodes": int(st0.shape[0]),
                   "max_displacement_lu": float(np.abs(xT - st0[:, :2]).max()),
                   "grad_finite": bool(np.isfinite(gm["force"]).all() and np.isfinite(gx0).all())}

@@ -1735,7 +1735,7 @@ __global__ void motion_move_kernel(const double* X0, const double* Y0, double* X
         return;
     }
     const double CS = 1 / sqrt(3.0);
-    if (((vx * vx) + (vy * vy)) > CS) raise_error(st, ERR_SPEED, i, ST_INTERP_MOVE);
+    if (!(((vx * vx) + (vy * vy)) <= CS)) raise_error(st, ERR_SPEED, i, ST_INTERP_MOVE);  // NaN too
     X1[i] = xi + vx;
     Y1[i] = yi + vy;
 }
