@@ -199,7 +199,8 @@ int lbib_get_domain_count(lbib_handle* h, int* n);
  * gradients accumulate in FP64.
  *
  * A differentiated run advances the lattice T steps with the geometry frozen
- * at its state when lbib_diff_begin is called: the membrane positions (so the
+ * (unless lbib_diff_motion moves the nodes) at its state when lbib_diff_begin
+ * is called: the membrane positions (so the
  * Dirac weights of the spread), the domain ids and the per-domain mass table
  * stay fixed, exactly as in lbib_lattice_step.  Each step is the pull-stream
  * + collide of the fluid (Luo force) and the species (with their reaction),
